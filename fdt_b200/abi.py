@@ -1,0 +1,113 @@
+"""ctypes mirror of include/bpx.h (the structs and option defaults).
+
+Kept free of any library loading so that tests can build option structs without a GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+BPX_MAX_FIBRES = 3
+BPX_NSTATE = 15
+
+BPX_OK = 0
+BPX_ERR_INVALID_ARG = 1
+BPX_ERR_CUDA = 2
+BPX_ERR_NO_DEVICE = 3
+BPX_ERR_UNSUPPORTED = 4
+BPX_ERR_IO = 5
+BPX_ERR_BAD_DATA = 6
+
+BPX_VOX_NONFINITE_DATA = 1
+BPX_VOX_F0_REFIT = 2
+BPX_VOX_NONFINITE_ENERGY = 4
+
+
+def nrec(nfib: int) -> int:
+    return 6 + 3 * nfib
+
+
+class Options(C.Structure):
+    """bpx_options: the xfibresOptions fields acting on the per-voxel path."""
+
+    _fields_ = [
+        ("model", C.c_int32),
+        ("nfibres", C.c_int32),
+        ("fudge", C.c_float),
+        ("njumps", C.c_int32),
+        ("nburn", C.c_int32),
+        ("sampleevery", C.c_int32),
+        ("updateproposalevery", C.c_int32),
+        ("no_ard", C.c_int32),
+        ("all_ard", C.c_int32),
+        ("nonlin", C.c_int32),
+        ("cnonlin", C.c_int32),
+        ("rician", C.c_int32),
+        ("f0", C.c_int32),
+        ("ardf0", C.c_int32),
+        ("R_prior_mean", C.c_float),
+        ("R_prior_std", C.c_float),
+        ("R_prior_fudge", C.c_float),
+        ("gradnonlin", C.c_int32),
+        ("seed", C.c_uint64),
+        ("mcmc_tpv", C.c_int32),
+        ("mcmc_mpl", C.c_int32),
+        ("reserved", C.c_int32 * 6),
+    ]
+
+    @classmethod
+    def make(cls, **kw) -> "Options":
+        """xfibres defaults (xfibresoptions.h:104-149), overridden by ``kw``."""
+        o = cls()
+        o.model = 1
+        o.nfibres = 1
+        o.fudge = 1.0
+        o.njumps = 1250
+        o.nburn = 1000
+        o.sampleevery = 25
+        o.updateproposalevery = 40
+        o.R_prior_mean = 0.13
+        o.R_prior_std = 0.03
+        o.R_prior_fudge = 0.0
+        o.seed = 8665904
+        for k, v in kw.items():
+            if not hasattr(o, k):
+                raise KeyError(k)
+            setattr(o, k, v)
+        return o
+
+    @property
+    def nparams_fit(self) -> int:
+        return 2 + 3 * self.nfibres + (1 if self.model >= 2 else 0) + (1 if self.f0 else 0)
+
+    @property
+    def nsamples(self) -> int:
+        return self.njumps // self.sampleevery
+
+
+class Volume(C.Structure):
+    _fields_ = [
+        ("nvox", C.c_int32),
+        ("ndir", C.c_int32),
+        ("data", C.c_void_p),
+        ("bvecs", C.c_void_p),
+        ("bvals", C.c_void_p),
+        ("grad", C.c_void_p),
+        ("voxel_offset", C.c_uint64),
+    ]
+
+
+class Outputs(C.Structure):
+    _fields_ = [
+        ("th", C.c_void_p),
+        ("ph", C.c_void_p),
+        ("f", C.c_void_p),
+        ("mean_d", C.c_void_p),
+        ("mean_dstd", C.c_void_p),
+        ("mean_R", C.c_void_p),
+        ("mean_f0", C.c_void_p),
+        ("mean_tau", C.c_void_p),
+        ("mean_S0", C.c_void_p),
+        ("mean_f", C.c_void_p),
+        ("dyads", C.c_void_p),
+        ("status", C.c_void_p),
+    ]

@@ -1,0 +1,601 @@
+// bpx_api.cu -- the C-ABI of libbpx.so (declared in include/bpx.h).
+//
+// Host code: option validation, launch dispatch, the per-device workspace cache and the
+// host-buffer drop-in for xfibres_gpu() (CUDA/xfibres_gpu.cu:29-146).  No entry point calls
+// exit(); failures return a bpx_status and leave a message for bpx_last_error().
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "bpx.h"
+#include "bpx_device.cuh"
+#include "bpx_internal.h"
+
+namespace bpx {
+
+cudaError_t launch_mcmc_m1(const McmcArgs&, int, bool, McmcLayout, cudaStream_t);
+cudaError_t launch_mcmc_m2(const McmcArgs&, int, bool, McmcLayout, cudaStream_t);
+cudaError_t launch_mcmc_m3(const McmcArgs&, int, bool, McmcLayout, cudaStream_t);
+cudaError_t launch_energy_m1(const EnergyArgs&, int, bool, McmcLayout, cudaStream_t);
+cudaError_t launch_energy_m2(const EnergyArgs&, int, bool, McmcLayout, cudaStream_t);
+cudaError_t launch_energy_m3(const EnergyArgs&, int, bool, McmcLayout, cudaStream_t);
+
+namespace {
+thread_local std::string g_last_error;
+
+constexpr int kMaxDevices = 64;
+int g_sm_count[kMaxDevices] = {0};
+
+// compiled (tpv, mpl) layouts, in order of preference for a given capacity
+const McmcLayout kLayouts[] = {{4, 9}, {8, 8}, {8, 9}, {16, 9}, {32, 9}, {32, 16}};
+constexpr int kNumLayouts = sizeof(kLayouts) / sizeof(kLayouts[0]);
+constexpr int kMaxNdir = 512;
+
+bpx_status fail(bpx_status st, const std::string& msg) {
+  g_last_error = msg;
+  return st;
+}
+
+bpx_status cuda_fail(cudaError_t e, const char* where) {
+  g_last_error = std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  return BPX_ERR_CUDA;
+}
+
+#define BPX_CUDA(call)                                   \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+bpx_status check_device() {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(BPX_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  int major = 0;
+  e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+  if (major != 10) return fail(BPX_ERR_NO_DEVICE, "libbpx is built for sm_100a only (found compute capability " + std::to_string(major) + ".x)");
+  return BPX_OK;
+}
+
+bpx_status check_opts(const bpx_options* o) {
+  if (!o) return fail(BPX_ERR_INVALID_ARG, "opts is NULL");
+  if (o->model < 1 || o->model > 3) return fail(BPX_ERR_INVALID_ARG, "model must be 1, 2 or 3");
+  if (o->nfibres < 1 || o->nfibres > BPX_MAX_FIBRES) return fail(BPX_ERR_INVALID_ARG, "nfibres must be 1..3");
+  if (o->njumps < 0 || o->nburn < 0) return fail(BPX_ERR_INVALID_ARG, "njumps and nburn must be >= 0");
+  if (o->sampleevery < 1) return fail(BPX_ERR_INVALID_ARG, "sampleevery must be >= 1");
+  if (o->updateproposalevery < 1) return fail(BPX_ERR_INVALID_ARG, "updateproposalevery must be >= 1");
+  if (o->njumps / o->sampleevery > 255 * 256 * 256) return fail(BPX_ERR_INVALID_ARG, "too many samples");
+  if (o->updateproposalevery > 255) return fail(BPX_ERR_UNSUPPORTED, "updateproposalevery > 255 is not supported (acceptance counters are 8-bit)");
+  return BPX_OK;
+}
+
+bpx_status check_vol(const bpx_volume* v, bool need_data) {
+  if (!v) return fail(BPX_ERR_INVALID_ARG, "vol is NULL");
+  if (v->nvox < 0) return fail(BPX_ERR_INVALID_ARG, "nvox < 0");
+  if (v->ndir < 7 || v->ndir > kMaxNdir) return fail(BPX_ERR_UNSUPPORTED, "ndir must be in 7.." + std::to_string(kMaxNdir));
+  if (v->nvox > 0 && need_data && (!v->data || !v->bvecs || !v->bvals)) return fail(BPX_ERR_INVALID_ARG, "data/bvecs/bvals is NULL");
+  return BPX_OK;
+}
+
+struct Workspace {
+  void* ptr = nullptr;
+  size_t cap = 0;
+};
+std::mutex g_ws_mutex;
+Workspace g_ws[kMaxDevices];
+
+// grow-only per-device scratch (not thread-safe across concurrent users of one device)
+bpx_status workspace(size_t bytes, void** out) {
+  int dev = 0;
+  BPX_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_ws_mutex);
+  Workspace& w = g_ws[dev % kMaxDevices];
+  if (w.cap < bytes) {
+    if (w.ptr) BPX_CUDA(cudaFree(w.ptr));
+    w.ptr = nullptr;
+    w.cap = 0;
+    BPX_CUDA(cudaMalloc(&w.ptr, bytes));
+    w.cap = bytes;
+  }
+  *out = w.ptr;
+  return BPX_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+McmcLayout pick_layout(const bpx_options* o, int ndir) {
+  if (o->mcmc_tpv > 0 && o->mcmc_mpl > 0) return McmcLayout{o->mcmc_tpv, o->mcmc_mpl};
+  return choose_layout(o->model, o->nfibres, o->rician != 0, ndir);
+}
+
+}  // namespace
+
+int sm_count() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+  dev %= kMaxDevices;
+  if (g_sm_count[dev] == 0) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    g_sm_count[dev] = n > 0 ? n : 1;
+  }
+  return g_sm_count[dev];
+}
+
+McmcLayout choose_layout(int model, int nfib, bool rician, int ndir) {
+  (void)model;
+  (void)nfib;
+  (void)rician;
+  for (int i = 0; i < kNumLayouts; ++i)
+    if (kLayouts[i].tpv * kLayouts[i].mpl >= ndir) return kLayouts[i];
+  return McmcLayout{0, 0};
+}
+
+bool layout_supported(int, int, bool, McmcLayout lay) {
+  for (int i = 0; i < kNumLayouts; ++i)
+    if (kLayouts[i].tpv == lay.tpv && kLayouts[i].mpl == lay.mpl) return true;
+  return false;
+}
+
+cudaError_t launch_mcmc(const McmcArgs& a, int model, int nfib, bool rician, McmcLayout lay, cudaStream_t s) {
+  if (a.nvox == 0) return cudaSuccess;
+  switch (model) {
+    case 1: return launch_mcmc_m1(a, nfib, rician, lay, s);
+    case 2: return launch_mcmc_m2(a, nfib, rician, lay, s);
+    case 3: return launch_mcmc_m3(a, nfib, rician, lay, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_energy(const EnergyArgs& a, int model, int nfib, bool rician, cudaStream_t s) {
+  if (a.nvox == 0) return cudaSuccess;
+  const McmcLayout lay = choose_layout(model, nfib, rician, a.ndir);
+  switch (model) {
+    case 1: return launch_energy_m1(a, nfib, rician, lay, s);
+    case 2: return launch_energy_m2(a, nfib, rician, lay, s);
+    case 3: return launch_energy_m3(a, nfib, rician, lay, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// correct_bvals_bvecs (CUDA/xfibres_gpu.cu:151-170) for every (voxel, measurement)
+__global__ void gradnonlin_kernel(int nvox, int ndir, const float* grad, const float* bvecs, const float* bvals,
+                                  float* bvecs_out, float* bvals_out) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)nvox * ndir) return;
+  const int v = (int)(i / ndir), m = (int)(i % ndir);
+  const float* L = grad + (size_t)v * 9;  // column-major 3x3: L(r,c) = L[c*3 + r]
+  float g[3] = {bvecs[m], bvecs[ndir + m], bvecs[2 * ndir + m]};
+  float b = bvals[m];
+  if (b > 0.f) {
+    float h[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) h[r] = g[r] + L[0 * 3 + r] * g[0] + L[1 * 3 + r] * g[1] + L[2 * 3 + r] * g[2];
+    const float mag = sqrtf(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+    if (mag != 0.f) {
+#pragma unroll
+      for (int r = 0; r < 3; ++r) h[r] /= mag;
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) g[r] = h[r];
+    b = mag * mag * b;
+  }
+  float* go = bvecs_out + (size_t)v * 3 * ndir;
+  go[m] = g[0];
+  go[ndir + m] = g[1];
+  go[2 * ndir + m] = g[2];
+  bvals_out[(size_t)v * ndir + m] = b;
+}
+
+// Pipe calibration: 8 independent dependency chains per thread so issue rate, not latency,
+// bounds both kernels; the grid fills every SM several times over.
+__global__ void mufu_rate_kernel(float* out, int iters) {
+  float a[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) a[j] = 1e-3f * (threadIdx.x + j);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = ex2_approx(-a[j]);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) s += a[j];
+  if (s == 12345.f) out[threadIdx.x] = s;
+}
+
+__global__ void fma_rate_kernel(float* out, int iters) {
+  float a[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) a[j] = 1e-3f * (threadIdx.x + j);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = fmaf(a[j], 0.9999f, 1e-4f);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) s += a[j];
+  if (s == 12345.f) out[threadIdx.x] = s;
+}
+
+}  // namespace bpx
+
+using namespace bpx;
+
+extern "C" {
+
+int32_t bpx_abi_version(void) { return BPX_ABI_VERSION; }
+
+void bpx_options_default(bpx_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->model = 1;
+  o->nfibres = 1;
+  o->fudge = 1.0f;
+  o->njumps = 1250;
+  o->nburn = 1000;
+  o->sampleevery = 25;
+  o->updateproposalevery = 40;
+  o->R_prior_mean = 0.13f;
+  o->R_prior_std = 0.03f;
+  o->R_prior_fudge = 0.0f;
+  o->seed = 8665904ull;
+}
+
+int32_t bpx_nparams_fit(const bpx_options* o) {
+  if (!o) return -1;
+  return 2 + 3 * o->nfibres + (o->model >= 2 ? 1 : 0) + (o->f0 ? 1 : 0);
+}
+
+int32_t bpx_nsamples(const bpx_options* o) {
+  if (!o || o->sampleevery < 1) return -1;
+  return o->njumps / o->sampleevery;
+}
+
+int32_t bpx_max_ndir(void) { return kMaxNdir; }
+
+const char* bpx_last_error(void) { return g_last_error.c_str(); }
+
+int32_t bpx_mcmc_layouts(int32_t* tpv, int32_t* mpl, int32_t max) {
+  for (int i = 0; i < kNumLayouts && i < max; ++i) {
+    if (tpv) tpv[i] = kLayouts[i].tpv;
+    if (mpl) mpl[i] = kLayouts[i].mpl;
+  }
+  return kNumLayouts;
+}
+
+bpx_status bpx_prepare_data_dev(int32_t nvox, int32_t ndir, float* data, void* stream) {
+  if (nvox < 0 || ndir < 1 || (nvox > 0 && !data)) return fail(BPX_ERR_INVALID_ARG, "bad arguments to bpx_prepare_data_dev");
+  if (nvox == 0) return BPX_OK;
+  bpx_status st = check_device();
+  if (st != BPX_OK) return st;
+  BPX_CUDA(launch_prepare(nvox, ndir, data, (cudaStream_t)stream));
+  return BPX_OK;
+}
+
+bpx_status bpx_gradnonlin_dev(int32_t nvox, int32_t ndir, const float* grad, const float* bvecs, const float* bvals,
+                              float* bvecs_out, float* bvals_out, void* stream) {
+  if (nvox < 0 || ndir < 1) return fail(BPX_ERR_INVALID_ARG, "bad sizes to bpx_gradnonlin_dev");
+  if (nvox == 0) return BPX_OK;
+  if (!grad || !bvecs || !bvals || !bvecs_out || !bvals_out) return fail(BPX_ERR_INVALID_ARG, "NULL pointer to bpx_gradnonlin_dev");
+  bpx_status st = check_device();
+  if (st != BPX_OK) return st;
+  const size_t n = (size_t)nvox * ndir;
+  const int threads = 256;
+  gradnonlin_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, (cudaStream_t)stream>>>(nvox, ndir, grad, bvecs, bvals, bvecs_out, bvals_out);
+  BPX_CUDA(cudaGetLastError());
+  return BPX_OK;
+}
+
+bpx_status bpx_fit_dev(const bpx_options* opts, const bpx_volume* vol, float* params, float* tau, uint32_t* status,
+                       void* stream) {
+  bpx_status st = check_opts(opts);
+  if (st == BPX_OK) st = check_vol(vol, true);
+  if (st != BPX_OK) return st;
+  if (vol->nvox == 0) return BPX_OK;
+  if (!params) return fail(BPX_ERR_INVALID_ARG, "params is NULL");
+  if (opts->rician && !tau) return fail(BPX_ERR_INVALID_ARG, "tau is NULL under rician");
+  st = check_device();
+  if (st != BPX_OK) return st;
+  FitArgs a;
+  a.nvox = vol->nvox;
+  a.ndir = vol->ndir;
+  a.data = vol->data;
+  a.bvecs = vol->bvecs;
+  a.bvals = vol->bvals;
+  a.gradnonlin = opts->gradnonlin;
+  a.params = params;
+  a.np_out = bpx_nparams_fit(opts);
+  a.tau = tau;
+  a.status = status;
+  a.model = opts->model;
+  a.rician = opts->rician;
+  a.nonlin = opts->nonlin;
+  a.R = opts->R_prior_mean;
+  BPX_CUDA(launch_fit(a, opts->nfibres, opts->f0 != 0, (cudaStream_t)stream));
+  return BPX_OK;
+}
+
+bpx_status bpx_mcmc_dev(const bpx_options* opts, const bpx_volume* vol, const float* params, const float* tau,
+                        float* records, uint32_t* status, void* stream) {
+  bpx_status st = check_opts(opts);
+  if (st == BPX_OK) st = check_vol(vol, true);
+  if (st != BPX_OK) return st;
+  if (vol->nvox == 0) return BPX_OK;
+  if (!params || !records) return fail(BPX_ERR_INVALID_ARG, "params/records is NULL");
+  if (opts->rician && !tau) return fail(BPX_ERR_INVALID_ARG, "tau is NULL under rician");
+  st = check_device();
+  if (st != BPX_OK) return st;
+  const McmcLayout lay = pick_layout(opts, vol->ndir);
+  if (lay.tpv == 0 || !layout_supported(opts->model, opts->nfibres, opts->rician != 0, lay) || lay.tpv * lay.mpl < vol->ndir)
+    return fail(BPX_ERR_UNSUPPORTED, "no compiled MCMC layout for ndir=" + std::to_string(vol->ndir));
+  McmcArgs a;
+  a.nvox = vol->nvox;
+  a.ndir = vol->ndir;
+  a.data = vol->data;
+  a.bvecs = vol->bvecs;
+  a.bvals = vol->bvals;
+  a.gradnonlin = opts->gradnonlin;
+  a.params = params;
+  a.np_fit = bpx_nparams_fit(opts);
+  a.tau = tau;
+  a.records = records;
+  a.nsamples = bpx_nsamples(opts);
+  a.status = status;
+  a.nburn = opts->nburn;
+  a.njumps = opts->njumps;
+  a.sampleevery = opts->sampleevery;
+  a.upe = opts->updateproposalevery;
+  a.f0 = opts->f0;
+  a.ardf0 = opts->ardf0;
+  a.no_ard = opts->no_ard;
+  a.all_ard = opts->all_ard;
+  a.fudge = opts->fudge;
+  a.R_mean = opts->R_prior_mean;
+  a.R_std = opts->R_prior_std;
+  a.R_fudge = opts->R_prior_fudge;
+  a.seed = opts->seed;
+  a.voxel_offset = vol->voxel_offset;
+  BPX_CUDA(launch_mcmc(a, opts->model, opts->nfibres, opts->rician != 0, lay, (cudaStream_t)stream));
+  return BPX_OK;
+}
+
+bpx_status bpx_finish_dev(const bpx_options* opts, int32_t nvox, const float* records, bpx_outputs* out, void* stream) {
+  bpx_status st = check_opts(opts);
+  if (st != BPX_OK) return st;
+  if (nvox < 0 || !out) return fail(BPX_ERR_INVALID_ARG, "bad arguments to bpx_finish_dev");
+  if (nvox == 0) return BPX_OK;
+  if (!records) return fail(BPX_ERR_INVALID_ARG, "records is NULL");
+  const int ns = bpx_nsamples(opts);
+  if (ns < 1) return fail(BPX_ERR_INVALID_ARG, "no samples (njumps < sampleevery)");
+  st = check_device();
+  if (st != BPX_OK) return st;
+  FinishArgs a;
+  a.nvox = nvox;
+  a.nsamples = ns;
+  a.nfib = opts->nfibres;
+  a.records = records;
+  a.out = *out;
+  BPX_CUDA(launch_finish(a, (cudaStream_t)stream));
+  return BPX_OK;
+}
+
+bpx_status bpx_energy_dev(const bpx_options* opts, const bpx_volume* vol, const float* states, float* lik, float* prior,
+                          void* stream) {
+  bpx_status st = check_opts(opts);
+  if (st == BPX_OK) st = check_vol(vol, true);
+  if (st != BPX_OK) return st;
+  if (vol->nvox == 0) return BPX_OK;
+  if (!states) return fail(BPX_ERR_INVALID_ARG, "states is NULL");
+  st = check_device();
+  if (st != BPX_OK) return st;
+  EnergyArgs a;
+  a.nvox = vol->nvox;
+  a.ndir = vol->ndir;
+  a.data = vol->data;
+  a.bvecs = vol->bvecs;
+  a.bvals = vol->bvals;
+  a.gradnonlin = opts->gradnonlin;
+  a.states = states;
+  a.lik = lik;
+  a.prior = prior;
+  a.f0 = opts->f0;
+  a.ardf0 = opts->ardf0;
+  a.no_ard = opts->no_ard;
+  a.all_ard = opts->all_ard;
+  a.fudge = opts->fudge;
+  a.R_mean = opts->R_prior_mean;
+  a.R_std = opts->R_prior_std;
+  a.R_fudge = opts->R_prior_fudge;
+  BPX_CUDA(launch_energy(a, opts->model, opts->nfibres, opts->rician != 0, (cudaStream_t)stream));
+  return BPX_OK;
+}
+
+bpx_status bpx_xfibres_dev(const bpx_options* opts, const bpx_volume* vol, bpx_outputs* out, void* stream) {
+  bpx_status st = check_opts(opts);
+  if (st == BPX_OK) st = check_vol(vol, true);
+  if (st != BPX_OK) return st;
+  if (!out) return fail(BPX_ERR_INVALID_ARG, "out is NULL");
+  if (vol->nvox == 0) return BPX_OK;
+  const int ns = bpx_nsamples(opts);
+  if (ns < 1) return fail(BPX_ERR_INVALID_ARG, "no samples (njumps < sampleevery)");
+  st = check_device();
+  if (st != BPX_OK) return st;
+  const size_t nvox = vol->nvox;
+  const size_t np = bpx_nparams_fit(opts);
+  const size_t nrec = BPX_NREC(opts->nfibres);
+  const size_t b_params = align256(nvox * np * sizeof(float));
+  const size_t b_tau = align256(nvox * sizeof(float));
+  const size_t b_rec = align256(nrec * ns * nvox * sizeof(float));
+  const size_t b_status = align256(nvox * sizeof(uint32_t));
+  void* ws = nullptr;
+  st = workspace(b_params + b_tau + b_rec + b_status, &ws);
+  if (st != BPX_OK) return st;
+  char* p = (char*)ws;
+  float* params = (float*)p;
+  float* tau = (float*)(p + b_params);
+  float* rec = (float*)(p + b_params + b_tau);
+  uint32_t* status = out->status ? out->status : (uint32_t*)(p + b_params + b_tau + b_rec);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (opts->rician) {
+    st = bpx_prepare_data_dev(vol->nvox, vol->ndir, const_cast<float*>(vol->data), stream);
+    if (st != BPX_OK) return st;
+  }
+  st = bpx_fit_dev(opts, vol, params, tau, status, stream);
+  if (st != BPX_OK) return st;
+  st = bpx_mcmc_dev(opts, vol, params, tau, rec, status, stream);
+  if (st != BPX_OK) return st;
+  st = bpx_finish_dev(opts, vol->nvox, rec, out, stream);
+  if (st != BPX_OK) return st;
+  (void)s;
+  return BPX_OK;
+}
+
+bpx_status bpx_xfibres_host(const bpx_options* opts, const bpx_volume* vol, bpx_outputs* host_out) {
+  bpx_status st = check_opts(opts);
+  if (st == BPX_OK) st = check_vol(vol, true);
+  if (st != BPX_OK) return st;
+  if (!host_out) return fail(BPX_ERR_INVALID_ARG, "host_out is NULL");
+  if (vol->nvox == 0) return BPX_OK;
+  if (opts->gradnonlin && !vol->grad) return fail(BPX_ERR_INVALID_ARG, "gradnonlin set but grad is NULL");
+  const int ns = bpx_nsamples(opts);
+  if (ns < 1) return fail(BPX_ERR_INVALID_ARG, "no samples (njumps < sampleevery)");
+  st = check_device();
+  if (st != BPX_OK) return st;
+  const size_t nvox = vol->nvox, ndir = vol->ndir, K = opts->nfibres;
+  const bool gn = opts->gradnonlin != 0;
+  // device buffers: inputs, per-voxel b-matrix under gradnonlin, outputs
+  const size_t b_data = align256(nvox * ndir * 4);
+  const size_t b_bvec = align256(3 * ndir * 4), b_bval = align256(ndir * 4);
+  const size_t b_grad = gn ? align256(nvox * 9 * 4) : 0;
+  const size_t b_bvec_v = gn ? align256(nvox * 3 * ndir * 4) : 0, b_bval_v = gn ? align256(nvox * ndir * 4) : 0;
+  const size_t b_samp = align256(K * ns * nvox * 4);
+  const size_t b_vox = align256(nvox * 4);
+  const size_t b_vk = align256(K * nvox * 4), b_dy = align256(K * 3 * nvox * 4);
+  const size_t total = b_data + b_bvec + b_bval + b_grad + b_bvec_v + b_bval_v + 3 * b_samp + 7 * b_vox + b_vk + b_dy;
+  char* base = nullptr;
+  BPX_CUDA(cudaMalloc(&base, total));
+  cudaStream_t s = nullptr;
+  cudaError_t ce = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  if (ce != cudaSuccess) {
+    cudaFree(base);
+    return cuda_fail(ce, "cudaStreamCreate");
+  }
+  char* p = base;
+  auto take = [&](size_t b) {
+    char* r = p;
+    p += b;
+    return r;
+  };
+  float* d_data = (float*)take(b_data);
+  float* d_bvec = (float*)take(b_bvec);
+  float* d_bval = (float*)take(b_bval);
+  float* d_grad = gn ? (float*)take(b_grad) : nullptr;
+  float* d_bvec_v = gn ? (float*)take(b_bvec_v) : nullptr;
+  float* d_bval_v = gn ? (float*)take(b_bval_v) : nullptr;
+  bpx_outputs d_out;
+  std::memset(&d_out, 0, sizeof(d_out));
+  d_out.th = (float*)take(b_samp);
+  d_out.ph = (float*)take(b_samp);
+  d_out.f = (float*)take(b_samp);
+  d_out.mean_d = (float*)take(b_vox);
+  d_out.mean_dstd = (float*)take(b_vox);
+  d_out.mean_R = (float*)take(b_vox);
+  d_out.mean_f0 = (float*)take(b_vox);
+  d_out.mean_tau = (float*)take(b_vox);
+  d_out.mean_S0 = (float*)take(b_vox);
+  d_out.status = (uint32_t*)take(b_vox);
+  d_out.mean_f = (float*)take(b_vk);
+  d_out.dyads = (float*)take(b_dy);
+  auto run = [&]() -> bpx_status {
+    BPX_CUDA(cudaMemcpyAsync(d_data, vol->data, nvox * ndir * 4, cudaMemcpyHostToDevice, s));
+    BPX_CUDA(cudaMemcpyAsync(d_bvec, vol->bvecs, 3 * ndir * 4, cudaMemcpyHostToDevice, s));
+    BPX_CUDA(cudaMemcpyAsync(d_bval, vol->bvals, ndir * 4, cudaMemcpyHostToDevice, s));
+    bpx_volume dv = *vol;
+    dv.data = d_data;
+    dv.bvecs = d_bvec;
+    dv.bvals = d_bval;
+    dv.grad = nullptr;
+    if (gn) {
+      BPX_CUDA(cudaMemcpyAsync(d_grad, vol->grad, nvox * 9 * 4, cudaMemcpyHostToDevice, s));
+      bpx_status s2 = bpx_gradnonlin_dev(vol->nvox, vol->ndir, d_grad, d_bvec, d_bval, d_bvec_v, d_bval_v, s);
+      if (s2 != BPX_OK) return s2;
+      dv.bvecs = d_bvec_v;
+      dv.bvals = d_bval_v;
+    }
+    bpx_status s3 = bpx_xfibres_dev(opts, &dv, &d_out, s);
+    if (s3 != BPX_OK) return s3;
+    const bpx_outputs& h = *host_out;
+    const size_t samp = K * ns * nvox * 4, vox = nvox * 4;
+    if (h.th) BPX_CUDA(cudaMemcpyAsync(h.th, d_out.th, samp, cudaMemcpyDeviceToHost, s));
+    if (h.ph) BPX_CUDA(cudaMemcpyAsync(h.ph, d_out.ph, samp, cudaMemcpyDeviceToHost, s));
+    if (h.f) BPX_CUDA(cudaMemcpyAsync(h.f, d_out.f, samp, cudaMemcpyDeviceToHost, s));
+    if (h.mean_d) BPX_CUDA(cudaMemcpyAsync(h.mean_d, d_out.mean_d, vox, cudaMemcpyDeviceToHost, s));
+    if (h.mean_dstd) BPX_CUDA(cudaMemcpyAsync(h.mean_dstd, d_out.mean_dstd, vox, cudaMemcpyDeviceToHost, s));
+    if (h.mean_R) BPX_CUDA(cudaMemcpyAsync(h.mean_R, d_out.mean_R, vox, cudaMemcpyDeviceToHost, s));
+    if (h.mean_f0) BPX_CUDA(cudaMemcpyAsync(h.mean_f0, d_out.mean_f0, vox, cudaMemcpyDeviceToHost, s));
+    if (h.mean_tau) BPX_CUDA(cudaMemcpyAsync(h.mean_tau, d_out.mean_tau, vox, cudaMemcpyDeviceToHost, s));
+    if (h.mean_S0) BPX_CUDA(cudaMemcpyAsync(h.mean_S0, d_out.mean_S0, vox, cudaMemcpyDeviceToHost, s));
+    if (h.status) BPX_CUDA(cudaMemcpyAsync(h.status, d_out.status, vox, cudaMemcpyDeviceToHost, s));
+    if (h.mean_f) BPX_CUDA(cudaMemcpyAsync(h.mean_f, d_out.mean_f, K * vox, cudaMemcpyDeviceToHost, s));
+    if (h.dyads) BPX_CUDA(cudaMemcpyAsync(h.dyads, d_out.dyads, 3 * K * vox, cudaMemcpyDeviceToHost, s));
+    BPX_CUDA(cudaStreamSynchronize(s));
+    return BPX_OK;
+  };
+  st = run();
+  cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  cudaFree(base);
+  return st;
+}
+
+bpx_status bpx_measure_pipes(double* mufu_ops_per_s, double* fma_ops_per_s) {
+  bpx_status st = check_device();
+  if (st != BPX_OK) return st;
+  const int threads = 256, blocks = sm_count() * 8;
+  float* dummy = nullptr;
+  BPX_CUDA(cudaMalloc(&dummy, threads * sizeof(float)));
+  cudaEvent_t e0, e1;
+  BPX_CUDA(cudaEventCreate(&e0));
+  BPX_CUDA(cudaEventCreate(&e1));
+  auto time_it = [&](bool mufu, int iters, float* ms) -> cudaError_t {
+    for (int rep = 0; rep < 2; ++rep) {  // first repetition warms up clocks and caches
+      cudaEventRecord(e0, 0);
+      if (mufu)
+        mufu_rate_kernel<<<blocks, threads>>>(dummy, iters);
+      else
+        fma_rate_kernel<<<blocks, threads>>>(dummy, iters);
+      cudaEventRecord(e1, 0);
+      cudaError_t e = cudaEventSynchronize(e1);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaEventElapsedTime(ms, e0, e1);
+  };
+  float ms_m = 0.f, ms_f = 0.f;
+  const int it_m = 4096, it_f = 32768;
+  cudaError_t e = time_it(true, it_m, &ms_m);
+  if (e == cudaSuccess) e = time_it(false, it_f, &ms_f);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(dummy);
+  if (e != cudaSuccess) return cuda_fail(e, "bpx_measure_pipes");
+  const double lanes = (double)blocks * threads * 8.0;
+  if (mufu_ops_per_s) *mufu_ops_per_s = lanes * it_m / (ms_m * 1e-3);
+  if (fma_ops_per_s) *fma_ops_per_s = lanes * it_f / (ms_f * 1e-3);
+  return BPX_OK;
+}
+
+bpx_status bpx_release_workspace(void) {
+  int dev = 0;
+  BPX_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_ws_mutex);
+  Workspace& w = g_ws[dev % kMaxDevices];
+  if (w.ptr) BPX_CUDA(cudaFree(w.ptr));
+  w.ptr = nullptr;
+  w.cap = 0;
+  return BPX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1096 @@
+// bpx_fit.cu -- initial fits of the bedpostx path on the GPU.
+//
+// One warp fits one voxel.  Replaces, for every voxel at once:
+//   * the host DTI start values  (CUDA/diffmodels.cu:57-94,149-184; DTI::linfit diffmodels.cc:17-46),
+//   * PVM_single_c::fit_pvf      (diffmodels.cc:561-603),
+//   * fit_PVM_single_kernel / fit_PVM_single_c_kernel / fit_PVM_multi_kernel
+//     (CUDA/PVM_single.cu:387-473, CUDA/PVM_single_c.cu:516-616, CUDA/PVM_multi.cu:468-576)
+//     with their LM driver (CUDA/levenberg_marquardt.cu:17-333),
+//   * the f0 plausibility re-fit and mix_params (CUDA/xfibres_gpu.cu:207-339,552-576),
+//   * calculate_tau with its residual kernels (CUDA/diffmodels.cu:259-347).
+//
+// Design: measurements are strided over the 32 lanes; every lane keeps its Jacobian row and
+// its partial J^T J / J^T r sums in registers; sums are combined with xor-butterfly shuffles so
+// that every lane holds identical totals and takes identical LM decisions (no shared memory, no
+// block barriers).  The damped normal equations are solved in FP64 with rows spread over lanes.
+#include <cstdint>
+
+#include "bpx_device.cuh"
+#include "bpx_internal.h"
+
+namespace bpx {
+
+enum Kind { kSingle = 0, kSingleC = 1, kMulti = 2 };
+
+template <int KIND, int K, bool F0>
+struct LmShape {
+  static constexpr int P = 3 * K + 2 + (KIND == kMulti ? 1 : 0) + (F0 ? 1 : 0);
+  static constexpr int O = (KIND == kMulti) ? 3 : 2;  // offset of the first fibre's f
+  static constexpr int NH = P * (P + 1) / 2;
+};
+
+struct Meas {
+  const float* y;
+  const float* gx;
+  const float* gy;
+  const float* gz;
+  const float* b;
+  int M;
+};
+
+// ------------------------------------------------------------------------------------------
+// Row-distributed FP64 solve of A x = r for an SPD matrix (A = J^T J + lambda I): lane i holds
+// row i.  Gaussian elimination without pivoting (stable for SPD), then back substitution; every
+// lane returns the whole solution.
+// ------------------------------------------------------------------------------------------
+template <int P>
+__device__ __forceinline__ void warp_solve(double (&row)[P], double rhs, double (&x)[P], int lane) {
+#pragma unroll
+  for (int k = 0; k < P; ++k) {
+    const double akk = __shfl_sync(0xffffffffu, row[k], k);
+    const double rk = __shfl_sync(0xffffffffu, rhs, k);
+    const double m = row[k] / akk;
+    const bool below = lane > k;
+#pragma unroll
+    for (int j = k + 1; j < P; ++j) {
+      const double akj = __shfl_sync(0xffffffffu, row[j], k);
+      if (below) row[j] -= m * akj;
+    }
+    if (below) rhs -= m * rk;
+  }
+#pragma unroll
+  for (int i = P - 1; i >= 0; --i) {
+    double s = rhs;
+#pragma unroll
+    for (int j = i + 1; j < P; ++j) s -= row[j] * x[j];
+    x[i] = __shfl_sync(0xffffffffu, s / row[i], i);
+  }
+}
+
+// Symmetric eigen-decomposition of a small matrix (n <= 3) by cyclic Jacobi, FP64; eigenvalues
+// descending; each eigenvector signed so its largest-magnitude component is positive (the
+// oracle uses the same convention, so both start the fits from the same angles).
+template <int N>
+__device__ void jacobi_eig(double (&A)[N][N], double (&w)[N], double (&V)[N][N]) {
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) V[i][j] = (i == j) ? 1.0 : 0.0;
+  for (int sweep = 0; sweep < 50; ++sweep) {
+    double off = 0;
+#pragma unroll
+    for (int p = 0; p < N; ++p)
+#pragma unroll
+      for (int q = p + 1; q < N; ++q) off += A[p][q] * A[p][q];
+    if (off < 1e-300) break;
+#pragma unroll
+    for (int p = 0; p < N; ++p) {
+#pragma unroll
+      for (int q = p + 1; q < N; ++q) {
+        const double apq = A[p][q];
+        if (fabs(apq) < 1e-300) continue;
+        const double theta = (A[q][q] - A[p][p]) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          const double akp = A[k][p], akq = A[k][q];
+          A[k][p] = c * akp - s * akq;
+          A[k][q] = s * akp + c * akq;
+        }
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          const double apk = A[p][k], aqk = A[q][k];
+          A[p][k] = c * apk - s * aqk;
+          A[q][k] = s * apk + c * aqk;
+        }
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          const double vkp = V[k][p], vkq = V[k][q];
+          V[k][p] = c * vkp - s * vkq;
+          V[k][q] = s * vkp + c * vkq;
+        }
+      }
+    }
+  }
+  // sort descending (selection on indices), canonical signs
+  int idx[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) idx[i] = i;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = i + 1; j < N; ++j) {
+      double ai = 0, aj = 0;
+#pragma unroll
+      for (int t = 0; t < N; ++t) {
+        if (t == idx[i]) ai = A[t][t];
+        if (t == idx[j]) aj = A[t][t];
+      }
+      if (aj > ai) {
+        const int tmp = idx[i];
+        idx[i] = idx[j];
+        idx[j] = tmp;
+      }
+    }
+  double Vs[N][N];
+#pragma unroll
+  for (int c = 0; c < N; ++c) {
+    double col[N], wc = 0;
+#pragma unroll
+    for (int t = 0; t < N; ++t)
+      if (t == idx[c]) {
+        wc = A[t][t];
+#pragma unroll
+        for (int r = 0; r < N; ++r) col[r] = V[r][t];
+      }
+    int big = 0;
+#pragma unroll
+    for (int r = 1; r < N; ++r)
+      if (fabs(col[r]) > fabs(col[big])) big = r;
+    double sg = 1.0;
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+      if (r == big && col[r] < 0) sg = -1.0;
+    w[c] = wc;
+#pragma unroll
+    for (int r = 0; r < N; ++r) Vs[r][c] = sg * col[r];
+  }
+#pragma unroll
+  for (int r = 0; r < N; ++r)
+#pragma unroll
+    for (int c = 0; c < N; ++c) V[r][c] = Vs[r][c];
+}
+
+// spherical angles in the convention of FSL miscmaths cart2sph (called at CUDA/diffmodels.cu:70)
+__device__ void cart2sph(const double (&v)[3], float& th, float& ph) {
+  const double x = v[0], y = v[1], z = v[2];
+  const double mag = sqrt(x * x + y * y + z * z);
+  const double pi = 3.141592653589793;
+  if (mag == 0) {
+    th = (float)(pi / 2);
+    ph = (float)(pi / 2);
+    return;
+  }
+  double p;
+  if (x == 0 && y >= 0)
+    p = pi / 2;
+  else if (x == 0 && y < 0)
+    p = -pi / 2;
+  else if (x > 0)
+    p = atan(y / x);
+  else if (y > 0)
+    p = atan(y / x) + pi;
+  else
+    p = atan(y / x) - pi;
+  const double r = sqrt(x * x + y * y);
+  double t;
+  if (z == 0)
+    t = pi / 2;
+  else if (z > 0)
+    t = atan(r / z);
+  else
+    t = atan(r / z) + pi;
+  th = (float)t;
+  ph = (float)p;
+}
+
+struct Dti {
+  double s0, md, fa, l1, v[3][3];  // v[i] = i-th eigenvector (descending eigenvalue)
+};
+
+// DTI::linfit (diffmodels.cc:17-46): two log-linear least-squares passes through the normal
+// equations of the 7-column design matrix (form_Amat, diffmodels.h:148-163), then the
+// eigen-system of the tensor (calc_tensor_parameters, diffmodels.cc:239-266).
+__device__ void dti_fit(const Meas& ms, int lane, Dti& o) {
+  double G[28];
+  double r1[7];
+#pragma unroll
+  for (int i = 0; i < 28; ++i) G[i] = 0;
+#pragma unroll
+  for (int i = 0; i < 7; ++i) r1[i] = 0;
+  float ysum = 0.f, ymax = 0.f;
+  for (int m = lane; m < ms.M; m += 32) {
+    const double gx = ms.gx[m], gy = ms.gy[m], gz = ms.gz[m], b = ms.b[m];
+    const double a[7] = {b * gx * gx, 2 * b * gx * gy, 2 * b * gx * gz, b * gy * gy, 2 * b * gy * gz, b * gz * gz, 1.0};
+    const float y = ms.y[m];
+    const double ls = y > 0 ? log((double)y) : 0.0;
+    int e = 0;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+      r1[i] += a[i] * ls;
+#pragma unroll
+      for (int j = i; j < 7; ++j) G[e++] += a[i] * a[j];
+    }
+    ysum += y;
+    ymax = fmaxf(ymax, fabsf(y));
+  }
+#pragma unroll
+  for (int i = 0; i < 28; ++i) G[i] = group_sum<32>(G[i]);
+#pragma unroll
+  for (int i = 0; i < 7; ++i) r1[i] = group_sum<32>(r1[i]);
+  ysum = group_sum<32>(ysum);
+  ymax = group_max<32>(ymax);
+  const double ymean = (double)ysum / ms.M;
+  // distribute rows of G
+  double row[7];
+  {
+    int e = 0;
+    double full[7][7];
+#pragma unroll
+    for (int i = 0; i < 7; ++i)
+#pragma unroll
+      for (int j = i; j < 7; ++j) {
+        full[i][j] = G[e];
+        full[j][i] = G[e];
+        ++e;
+      }
+#pragma unroll
+    for (int j = 0; j < 7; ++j) {
+      row[j] = 0;
+#pragma unroll
+      for (int i = 0; i < 7; ++i)
+        if (lane == i) row[j] = full[i][j];
+    }
+  }
+  double rowc[7];
+#pragma unroll
+  for (int j = 0; j < 7; ++j) rowc[j] = row[j];
+  double rhs = 0;
+#pragma unroll
+  for (int i = 0; i < 7; ++i)
+    if (lane == i) rhs = r1[i];
+  double D[7];
+  warp_solve<7>(rowc, rhs, D, lane);  // D = (A^T A)^-1 A^T logS ; Dvec = -D
+  double s0 = (-D[6]) > -23 ? exp(D[6]) : (double)ymax;
+  if (s0 < ymean) s0 = ymax;
+  double r2[7];
+#pragma unroll
+  for (int i = 0; i < 7; ++i) r2[i] = 0;
+  for (int m = lane; m < ms.M; m += 32) {
+    const double gx = ms.gx[m], gy = ms.gy[m], gz = ms.gz[m], b = ms.b[m];
+    const double a[7] = {b * gx * gx, 2 * b * gx * gy, 2 * b * gx * gz, b * gy * gy, 2 * b * gy * gz, b * gz * gz, 1.0};
+    const double y = ms.y[m];
+    const double ls = (y / s0) > 0.01 ? log(y) : log(0.01 * s0);
+#pragma unroll
+    for (int i = 0; i < 7; ++i) r2[i] += a[i] * ls;
+  }
+#pragma unroll
+  for (int i = 0; i < 7; ++i) r2[i] = group_sum<32>(r2[i]);
+  rhs = 0;
+#pragma unroll
+  for (int i = 0; i < 7; ++i)
+    if (lane == i) rhs = r2[i];
+  warp_solve<7>(row, rhs, D, lane);
+  // Dvec = -D
+  s0 = exp(D[6]);
+  if (s0 < ymean) s0 = ymean;
+  double T[3][3] = {{-D[0], -D[1], -D[2]}, {-D[1], -D[3], -D[4]}, {-D[2], -D[4], -D[5]}};
+  double w[3], V[3][3];
+  jacobi_eig<3>(T, w, V);
+  o.s0 = s0;
+  o.l1 = w[0];
+  o.md = (w[0] + w[1] + w[2]) / 3.0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) o.v[i][r] = V[r][i];
+  const double numer = 1.5 * ((w[0] - o.md) * (w[0] - o.md) + (w[1] - o.md) * (w[1] - o.md) + (w[2] - o.md) * (w[2] - o.md));
+  const double denom = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+  const double fa = denom > 0 ? numer / denom : 0;
+  o.fa = fa > 0 ? sqrt(fa) : 0;
+}
+
+// ------------------------------------------------------------------------------------------
+// model evaluation
+// ------------------------------------------------------------------------------------------
+template <int KIND, int K, bool F0>
+struct Pre {
+  float fs[K], v[K][3], sth[K], cth[K], sph[K], cph[K], dfx[K];
+  float sumf, d, a, bb, S0, f0v, dfx0, sgn1, sgn2;
+  float deriv[K][K];
+};
+
+template <int KIND, int K, bool F0>
+__device__ __forceinline__ void precompute(const float (&p)[LmShape<KIND, K, F0>::P], Pre<KIND, K, F0>& q) {
+  constexpr int P = LmShape<KIND, K, F0>::P, O = LmShape<KIND, K, F0>::O;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    sincosf(p[O + 3 * k + 1], &q.sth[k], &q.cth[k]);
+    sincosf(p[O + 3 * k + 2], &q.sph[k], &q.cph[k]);
+    q.v[k][0] = q.sth[k] * q.cph[k];
+    q.v[k][1] = q.sth[k] * q.sph[k];
+    q.v[k][2] = q.cth[k];
+  }
+  q.sumf = 0.f;
+  if (KIND == kSingle) {
+    q.d = fabsf(p[1]);
+    q.S0 = p[0];
+    q.sgn1 = pm1(p[1]);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const float x = p[O + 3 * k];
+      q.fs[k] = x2f(x);
+      q.dfx[k] = kTwoPiGpu * sgnf(x) / (1.f + x * x);
+      q.sumf += q.fs[k];
+    }
+    if (F0) {
+      const float x0 = p[P - 1];
+      q.f0v = x2f(x0);
+      q.dfx0 = kTwoPiGpu * sgnf(x0) / (1.f + x0 * x0);
+    }
+  } else if (KIND == kSingleC) {
+    q.d = p[1] * p[1];
+    q.S0 = p[0];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      float pf = 1.f;
+#pragma unroll
+      for (int j = 0; j < k; ++j) pf -= q.fs[j];
+      q.fs[k] = beta2f(p[O + 3 * k]) * pf;
+      q.sumf += q.fs[k];
+    }
+    // fractions_deriv_PVM_single_c (CUDA/PVM_single_c.cu:104-139): d f_j / d beta_k
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const float s2k = sinf(2.f * p[O + 3 * k]);
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
+        if (j == k) {
+          float fsum = 1.f;
+#pragma unroll
+          for (int n = 0; n < j; ++n) fsum -= q.fs[n];
+          q.deriv[j][k] = s2k * fsum;
+        } else if (j > k) {
+          const float sp = sinf(p[O + 3 * j]);
+          float fsum = 0.f;
+#pragma unroll
+          for (int n = 0; n < j; ++n) fsum += q.deriv[n][k];
+          q.deriv[j][k] = -(sp * sp) * fsum;
+        } else {
+          q.deriv[j][k] = 0.f;
+        }
+      }
+    }
+    if (F0) {
+      const float pfs = 1.f - q.sumf;
+      q.f0v = beta2f(p[P - 1]) * pfs;
+      q.dfx0 = sinf(2.f * p[P - 1]) * pfs;
+    }
+  } else {
+    q.a = fabsf(p[1]);
+    q.bb = fabsf(p[2]);
+    q.S0 = fabsf(p[0]);
+    q.sgn1 = pm1(p[1]);
+    q.sgn2 = pm1(p[2]);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const float x = p[O + 3 * k];
+      q.fs[k] = x2f(x);
+      q.dfx[k] = kTwoPiGpu * sgnf(x) / (1.f + x * x);
+      q.sumf += q.fs[k];
+    }
+    if (F0) {
+      const float x0 = p[P - 1];
+      q.f0v = x2f(x0);
+      q.dfx0 = kTwoPiGpu * sgnf(x0) / (1.f + x0 * x0);
+    }
+  }
+  if (!F0) {
+    q.f0v = 0.f;
+    q.dfx0 = 0.f;
+  }
+}
+
+// Predicted signal of one measurement; with WANTJ also the Jacobian row Jg (the one the
+// reference uses for the gradient) and J0h, the S0 entry its Hessian uses (they differ only for
+// PVM_multi, CUDA/PVM_multi.cu:376 vs :452).
+template <int KIND, int K, bool F0, bool WANTJ>
+__device__ __forceinline__ float point(const Pre<KIND, K, F0>& q, const float (&p)[LmShape<KIND, K, F0>::P],
+                                       float gx, float gy, float gz, float b, int gbo, float R,
+                                       float invR, float (&J)[LmShape<KIND, K, F0>::P], float& J0h) {
+  constexpr int P = LmShape<KIND, K, F0>::P, O = LmShape<KIND, K, F0>::O;
+  float dp[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) dp[k] = gx * q.v[k][0] + gy * q.v[k][1] + gz * q.v[k][2];
+  if (KIND == kSingle || KIND == kSingleC) {
+    const float d = q.d;
+    const float iso = expf(-b * d);
+    float an[K], sig = 0.f;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      an[k] = expf(-b * d * dp[k] * dp[k]);
+      sig += q.fs[k] * an[k];
+    }
+    const float wiso = 1.f - q.sumf - q.f0v;
+    const float full = q.S0 * ((q.f0v + wiso * iso) + sig);
+    if (!WANTJ) return full;
+#pragma unroll
+    for (int i = 0; i < P; ++i) J[i] = 0.f;
+    if (KIND == kSingle) {
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        J[1] += q.sgn1 * q.S0 * q.fs[k] * (-b * dp[k] * dp[k] * an[k]);
+        J[O + 3 * k] = q.S0 * (an[k] - iso) * q.dfx[k];
+      }
+      J[1] += q.sgn1 * q.S0 * wiso * (-b * iso);
+    } else {
+      const float lam = p[1];
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        J[1] += q.S0 * q.fs[k] * (-2.f * b * lam * dp[k] * dp[k] * an[k]);
+        float s = 0.f;
+#pragma unroll
+        for (int j = 0; j < K; ++j) s += q.S0 * (an[j] - iso) * q.deriv[j][k];
+        J[O + 3 * k] = s;
+      }
+      J[1] += q.S0 * wiso * (-2.f * b * lam * iso);
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const float dp1 = q.cth[k] * (gx * q.cph[k] + gy * q.sph[k]) - gz * q.sth[k];
+      const float dp2 = q.sth[k] * (-gx * q.sph[k] + gy * q.cph[k]);
+      const float c = q.S0 * q.fs[k] * (-2.f * b * d * dp[k] * an[k]);
+      J[O + 3 * k + 1] = c * dp1;
+      J[O + 3 * k + 2] = c * dp2;
+    }
+    if (F0) J[P - 1] = q.S0 * (1.f - iso) * q.dfx0;
+    J[0] = full / p[0];
+    J0h = J[0];
+    return full;
+  } else {
+    const float a = q.a, bb = q.bb;
+    const float liso = log1pf(b * bb);
+    const float iso = expf(-a * liso);
+    float an[K], an_a[K], an_b[K], an_th[K], an_ph[K], sig = 0.f;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const float x2 = dp[k] * dp[k];
+      const float dp1 = q.cth[k] * (gx * q.cph[k] + gy * q.sph[k]) - gz * q.sth[k];
+      const float dpp = q.sth[k] * (-gx * q.sph[k] + gy * q.cph[k]);
+      if (gbo == 2) {
+        const float arg = (1.f - R) * x2 + R;
+        const float e = expf(-b * 3.f * a * bb * invR * arg);
+        an[k] = e;
+        if (WANTJ) {
+          const float da = b * 3.f * bb * invR * arg;
+          an_a[k] = -da * expf(-da * a);
+          const float db = b * 3.f * a * invR * arg;
+          an_b[k] = -db * expf(-db * bb);
+          // the zeppelin angle derivatives of CUDA/PVM_multi.cu:82-84,99-101 (no factor dp)
+          an_th[k] = -(2.f * b * 3.f * a * bb * invR * (1.f - R) * dp1) * e;
+          an_ph[k] = -(2.f * b * 3.f * a * bb * invR * (1.f - R) * dpp) * e;
+        }
+      } else {
+        const float l = log1pf(b * bb * x2);
+        an[k] = expf(-a * l);
+        if (WANTJ) {
+          const float inv = 1.f / (1.f + b * x2 * bb);
+          an_a[k] = -l * an[k];
+          an_b[k] = -a * b * x2 * inv * an[k];
+          const float t = -a * bb * b * inv * an[k] * 2.f * dp[k];
+          an_th[k] = t * dp1;
+          an_ph[k] = t * dpp;
+        }
+      }
+      sig += q.fs[k] * an[k];
+    }
+    const float wiso = 1.f - q.sumf - q.f0v;
+    const float full = q.S0 * ((q.f0v + wiso * iso) + sig);
+    if (!WANTJ) return full;
+#pragma unroll
+    for (int i = 0; i < P; ++i) J[i] = 0.f;
+    const float iso_a = -liso * iso;
+    const float iso_b = -a * b / (1.f + b * bb) * iso;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      J[1] += q.sgn1 * q.S0 * q.fs[k] * an_a[k];
+      J[2] += q.sgn2 * q.S0 * q.fs[k] * an_b[k];
+      J[O + 3 * k] = q.S0 * (an[k] - iso) * q.dfx[k];
+      J[O + 3 * k + 1] = q.S0 * q.fs[k] * an_th[k];
+      J[O + 3 * k + 2] = q.S0 * q.fs[k] * an_ph[k];
+    }
+    J[1] += q.sgn1 * q.S0 * wiso * iso_a;
+    J[2] += q.sgn2 * q.S0 * wiso * iso_b;
+    if (F0) J[P - 1] = q.S0 * (1.f - iso) * q.dfx0;
+    J0h = full / p[0];
+    J[0] = pm1(p[0]) * full / p[0];
+    return full;
+  }
+}
+
+template <int KIND, int K, bool F0>
+__device__ double cost(const Meas& ms, const float (&p)[LmShape<KIND, K, F0>::P], int lane, int gbo, float R,
+                       float invR) {
+  constexpr int P = LmShape<KIND, K, F0>::P;
+  Pre<KIND, K, F0> q;
+  precompute<KIND, K, F0>(p, q);
+  float acc = 0.f;
+  float Jd[P];
+  float j0;
+  for (int m = lane; m < ms.M; m += 32) {
+    const float e = point<KIND, K, F0, false>(q, p, ms.gx[m], ms.gy[m], ms.gz[m], ms.b[m], gbo, R, invR, Jd, j0) - ms.y[m];
+    acc += e * e;
+  }
+  return group_sum<32>((double)acc);
+}
+
+// LM driver (CUDA/levenberg_marquardt.cu:57-122): lambda0 = 0.1, x/÷ 10, converged when
+// 2|dcf| <= 1e-8 (|cf_old|+|cf_new|+2e-16), stopped when lambda > 1e20 or after 200 successful
+// iterations (the iteration counter advances only on success).
+template <int KIND, int K, bool F0>
+__device__ int lm_run(const Meas& ms, float (&p)[LmShape<KIND, K, F0>::P], int lane, int gbo, float R, float invR) {
+  constexpr int P = LmShape<KIND, K, F0>::P;
+  constexpr int NH = LmShape<KIND, K, F0>::NH;
+  double lambda = 0.1;
+  const double cftol = 1.0e-8, ltol = 1.0e20;
+  double pcf = cost<KIND, K, F0>(ms, p, lane, gbo, R, invR);
+  int niter = 0, iters = 0;
+  bool success = true;
+  double Hrow[P], grow = 0.0;
+  while (!(success && niter++ >= 200)) {
+    ++iters;
+    if (success) {
+      Pre<KIND, K, F0> q;
+      precompute<KIND, K, F0>(p, q);
+      float H[NH], g[P];
+#pragma unroll
+      for (int i = 0; i < NH; ++i) H[i] = 0.f;
+#pragma unroll
+      for (int i = 0; i < P; ++i) g[i] = 0.f;
+      for (int m = lane; m < ms.M; m += 32) {
+        float J[P], J0h;
+        const float sig = point<KIND, K, F0, true>(q, p, ms.gx[m], ms.gy[m], ms.gz[m], ms.b[m], gbo, R, invR, J, J0h);
+        const float diff = sig - ms.y[m];
+#pragma unroll
+        for (int i = 0; i < P; ++i) g[i] += 2.f * J[i] * diff;
+        float Jh[P];
+#pragma unroll
+        for (int i = 0; i < P; ++i) Jh[i] = J[i];
+        Jh[0] = J0h;
+        int e = 0;
+#pragma unroll
+        for (int i = 0; i < P; ++i)
+#pragma unroll
+          for (int j = i; j < P; ++j) H[e++] += 2.f * Jh[i] * Jh[j];
+      }
+#pragma unroll
+      for (int i = 0; i < NH; ++i) H[i] = group_sum<32>(H[i]);
+#pragma unroll
+      for (int i = 0; i < P; ++i) g[i] = group_sum<32>(g[i]);
+      // lane i keeps row i of the Hessian and g[i]
+      grow = 0.0;
+#pragma unroll
+      for (int j = 0; j < P; ++j) Hrow[j] = 0.0;
+      int e = 0;
+#pragma unroll
+      for (int i = 0; i < P; ++i)
+#pragma unroll
+        for (int j = i; j < P; ++j) {
+          if (lane == i) Hrow[j] = H[e];
+          if (lane == j) Hrow[i] = H[e];
+          ++e;
+        }
+#pragma unroll
+      for (int i = 0; i < P; ++i)
+        if (lane == i) grow = g[i];
+    }
+    double A[P];
+#pragma unroll
+    for (int j = 0; j < P; ++j) A[j] = Hrow[j] + ((lane == j) ? lambda : 0.0);
+    double x[P];
+    warp_solve<P>(A, grow, x, lane);
+    float step[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i) step[i] = (float)((double)p[i] - x[i]);
+    const double ncf = cost<KIND, K, F0>(ms, step, lane, gbo, R, invR);
+    bool end = false;
+    if ((success = (ncf < pcf))) {
+#pragma unroll
+      for (int i = 0; i < P; ++i) p[i] = step[i];
+      lambda /= 10.0;
+      if (2.0 * fabs(pcf - ncf) <= cftol * (fabs(pcf) + fabs(ncf) + 2.0e-16)) end = true;
+      pcf = ncf;
+    } else {
+      lambda *= 10.0;
+      if (lambda > ltol) end = true;
+    }
+    if (end) break;
+  }
+  return iters;
+}
+
+// adjacent-swap sort of fibres by decreasing f (sort_PVM_*, CUDA/PVM_single.cu:86-104)
+template <int K, int O, int P>
+__device__ __forceinline__ void sort_fibres(float (&p)[P]) {
+#pragma unroll
+  for (int i = 1; i < K; ++i)
+#pragma unroll
+    for (int j = 0; j < K - i; ++j)
+      if (p[O + j * 3] < p[O + (j + 1) * 3]) {
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+          const float tmp = p[O + j * 3 + t];
+          p[O + j * 3 + t] = p[O + (j + 1) * 3 + t];
+          p[O + (j + 1) * 3 + t] = tmp;
+        }
+      }
+}
+
+// finalise raw LM parameters (CUDA/PVM_single.cu:451-466, CUDA/PVM_single_c.cu:582-607,
+// CUDA/PVM_multi.cu:549-566)
+template <int KIND, int K, bool F0>
+__device__ __forceinline__ void finalise(float (&p)[LmShape<KIND, K, F0>::P]) {
+  constexpr int P = LmShape<KIND, K, F0>::P, O = LmShape<KIND, K, F0>::O;
+  if (KIND == kSingle) {
+    p[1] = fabsf(p[1]);
+#pragma unroll
+    for (int k = 0; k < K; ++k) p[O + 3 * k] = x2f(p[O + 3 * k]);
+    if (F0) p[P - 1] = x2f(p[P - 1]);
+    sort_fibres<K, O, P>(p);
+    float sum = F0 ? p[P - 1] : 0.f;
+    bool hit = false;
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      if (!hit) {
+        sum += p[O + 3 * i];
+        if (sum >= 1.f) hit = true;
+      }
+      if (hit) p[O + 3 * i] = kFSmall;
+    }
+  } else if (KIND == kSingleC) {
+    p[1] = p[1] * p[1];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      float pf = 1.f;
+#pragma unroll
+      for (int j = 0; j < k; ++j) pf -= p[O + 3 * j];
+      p[O + 3 * k] = beta2f(p[O + 3 * k]) * pf;
+    }
+    if (F0) {
+      float pf = 1.f;
+#pragma unroll
+      for (int j = 0; j < K; ++j) pf -= p[O + 3 * j];
+      p[P - 1] = beta2f(p[P - 1]) * pf;
+    }
+    sort_fibres<K, O, P>(p);
+  } else {
+    const float aux = p[1];
+    p[1] = fabsf(aux * p[2]);
+    p[2] = sqrtf(fabsf(aux * p[2] * p[2]));
+#pragma unroll
+    for (int k = 0; k < K; ++k) p[O + 3 * k] = x2f(p[O + 3 * k]);
+    if (F0) p[P - 1] = x2f(p[P - 1]);
+    sort_fibres<K, O, P>(p);
+    float sum = F0 ? p[P - 1] : 0.f;
+    bool hit = false;
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      if (!hit) {
+        if (p[O + 3 * i] == 0.f) p[O + 3 * i] = kFSmall;
+        sum += p[O + 3 * i];
+        if (sum >= 1.f) hit = true;
+      }
+      if (hit) p[O + 3 * i] = kFSmall;
+    }
+  }
+}
+
+// PVM_single start values (CUDA/diffmodels.cu:67-91)
+template <int K, bool F0>
+__device__ void start_single(const Dti& dt, float (&p)[LmShape<kSingle, K, F0>::P]) {
+  constexpr int P = LmShape<kSingle, K, F0>::P;
+  float th, ph;
+  cart2sph(dt.v[0], th, ph);
+  p[0] = (float)dt.s0;
+  p[1] = dt.md > 0 ? (float)(dt.md * 2) : 0.001f;
+  p[2] = dt.fa < 1 ? f2x((float)dt.fa) : f2x(0.95f);
+  p[3] = th;
+  p[4] = ph;
+  float sumf = x2f(p[2]);
+#pragma unroll
+  for (int ii = 2; ii <= K; ++ii) {
+    const int i = 5 + 3 * (ii - 2);
+    float denom = 2.f, tmpsumf;
+    do {
+      p[i] = f2x(x2f(p[i - 3]) / denom);
+      denom *= 2.f;
+      tmpsumf = sumf + x2f(p[i]);
+    } while (tmpsumf >= 1.f);
+    sumf += x2f(p[i]);
+    cart2sph(dt.v[ii - 1], th, ph);
+    p[i + 1] = th;
+    p[i + 2] = ph;
+  }
+  if (F0) p[P - 1] = f2x(kFSmall);
+}
+
+// PVM_single_c start values with fit_pvf (CUDA/diffmodels.cu:149-184, diffmodels.cc:561-603)
+template <int K, bool F0>
+__device__ void start_single_c(const Dti& dt, const Meas& ms, int lane, float (&x)[LmShape<kSingleC, K, F0>::P]) {
+  constexpr int P = LmShape<kSingleC, K, F0>::P;
+  float th, ph;
+#pragma unroll
+  for (int i = 0; i < P; ++i) x[i] = 0.f;
+  cart2sph(dt.v[0], th, ph);
+  x[0] = (float)dt.s0;
+  x[1] = sqrtf(dt.l1 > 0 ? (float)dt.l1 : 0.002f);
+  x[3] = th;
+  x[4] = ph;
+#pragma unroll
+  for (int ii = 2; ii <= K; ++ii) {
+    const int i = 5 + 3 * (ii - 2);
+    cart2sph(dt.v[ii - 1], th, ph);
+    x[i + 1] = th;
+    x[i + 2] = ph;
+  }
+  // linear least squares for the fractions: pinv(M) * (Y - S0 iso)
+  const double s0 = x[0], d = (double)x[1] * x[1];
+  double dir[K][3];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    dir[k][0] = sin((double)x[3 + 3 * k]) * cos((double)x[4 + 3 * k]);
+    dir[k][1] = sin((double)x[3 + 3 * k]) * sin((double)x[4 + 3 * k]);
+    dir[k][2] = cos((double)x[3 + 3 * k]);
+  }
+  double MtM[K][K], MtY[K];
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    MtY[i] = 0;
+#pragma unroll
+    for (int j = 0; j < K; ++j) MtM[i][j] = 0;
+  }
+  for (int m = lane; m < ms.M; m += 32) {
+    const double gx = ms.gx[m], gy = ms.gy[m], gz = ms.gz[m], b = ms.b[m];
+    const double iso = exp(-b * d);
+    const double yi = ms.y[m] - s0 * iso;
+    double row[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const double dp = gx * dir[k][0] + gy * dir[k][1] + gz * dir[k][2];
+      row[k] = s0 * (exp(-b * d * dp * dp) - iso);
+    }
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      MtY[i] += row[i] * yi;
+#pragma unroll
+      for (int j = 0; j < K; ++j) MtM[i][j] += row[i] * row[j];
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    MtY[i] = group_sum<32>(MtY[i]);
+#pragma unroll
+    for (int j = 0; j < K; ++j) MtM[i][j] = group_sum<32>(MtM[i][j]);
+  }
+  double w[K], V[K][K];
+  jacobi_eig<K>(MtM, w, V);
+  const double tol = w[0] * 1e-14 * (ms.M > K ? ms.M : K);
+  double fs[K];
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    double s = 0;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      double gij = 0;
+#pragma unroll
+      for (int c = 0; c < K; ++c)
+        if (w[c] > tol) gij += V[i][c] * V[j][c] / w[c];
+      s += gij * MtY[j];
+    }
+    fs[i] = s;
+  }
+  float fsf[K];
+  float f0v = 0.f;
+#pragma unroll
+  for (int k = 0; k < K; ++k) fsf[k] = (float)fs[k];
+  if (F0) {
+    f0v = kFSmall;
+    fsf[0] -= f0v;
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) fsf[k] = fabsf(fsf[k]);
+  {
+    float sumf = 0.f;
+    bool hit = false;
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      if (!hit) {
+        sumf += fsf[i];
+        if (sumf >= 1.f) hit = true;
+      }
+      if (hit) fsf[i] = kFSmall;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    float pf = 1.f;
+#pragma unroll
+    for (int j = 0; j < k; ++j) pf -= fsf[j];
+    float tmpr = fsf[k] / pf;
+    if (tmpr > 1.f) tmpr = 1.f;
+    x[2 + 3 * k] = f2beta(tmpr);
+  }
+  if (F0) {
+    float pf = 1.f;
+#pragma unroll
+    for (int j = 0; j < K; ++j) pf -= fsf[j];
+    float tmpr = f0v / pf;
+    if (tmpr > 1.f) tmpr = 1.f;
+    x[P - 1] = f2beta(tmpr);
+  }
+}
+
+// fit_PVM_multi_kernel start from the finalised PVM_single / PVM_single_c parameters
+// (CUDA/PVM_multi.cu:514-530)
+template <int K, bool F0>
+__device__ __forceinline__ void start_multi(const float (&s)[LmShape<kSingle, K, F0>::P], float (&p)[LmShape<kMulti, K, F0>::P]) {
+  constexpr int P = LmShape<kMulti, K, F0>::P;
+  p[0] = s[0];
+  p[1] = 1.0f;
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    const int ii = 3 + 3 * i;
+    p[ii] = f2x(s[ii - 1]);
+    p[ii + 1] = s[ii];
+    p[ii + 2] = s[ii + 1];
+  }
+  p[2] = s[1];
+  if (F0) p[P - 1] = f2x(s[P - 2]);
+}
+
+// predicted signal from finalised parameters (what get_residuals_*_kernel subtract)
+template <int K>
+__device__ __forceinline__ float predict_final(int model, const float* q, int o, bool use_f0, float f0,
+                                               float R, float gx, float gy, float gz, float b) {
+  float sumf = 0.f, val = 0.f, iso, S0 = q[0];
+  if (model == 1) {
+    const float d = q[1];
+    iso = expf(-b * d);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      float st, ct, sp, cp;
+      sincosf(q[o + 3 * k + 1], &st, &ct);
+      sincosf(q[o + 3 * k + 2], &sp, &cp);
+      const float dp = gx * st * cp + gy * st * sp + gz * ct;
+      val += q[o + 3 * k] * expf(-b * d * dp * dp);
+      sumf += q[o + 3 * k];
+    }
+  } else {
+    const float d = q[1], ds = q[2];
+    const float a = d * d / ds / ds, bb = ds * ds / d;
+    const float invR = 1.f / (2.f * R + 1.f);
+    iso = expf(-a * log1pf(b * bb));
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      float st, ct, sp, cp;
+      sincosf(q[o + 3 * k + 1], &st, &ct);
+      sincosf(q[o + 3 * k + 2], &sp, &cp);
+      const float dp = gx * st * cp + gy * st * sp + gz * ct;
+      float an;
+      if (model == 3)
+        an = expf(-b * 3.f * a * bb * invR * ((1.f - R) * dp * dp + R));
+      else
+        an = expf(-a * log1pf(b * bb * dp * dp));
+      val += q[o + 3 * k] * an;
+      sumf += q[o + 3 * k];
+    }
+    S0 = fabsf(S0);
+  }
+  if (use_f0) return S0 * (f0 + (1.f - sumf - f0) * iso + val);
+  return S0 * ((1.f - sumf) * iso + val);
+}
+
+// ------------------------------------------------------------------------------------------
+// the fit kernel: one warp per voxel, grid-stride over voxels
+// ------------------------------------------------------------------------------------------
+template <int K, bool F0>
+__device__ void fit_one(const FitArgs& a, int v, int lane) {
+  constexpr int NPOUT = 2 + 3 * K + (F0 ? 1 : 0);  // model 1 layout
+  const int M = a.ndir;
+  Meas ms;
+  ms.y = a.data + (size_t)v * M;
+  const float* bv = a.gradnonlin ? a.bvecs + (size_t)v * 3 * M : a.bvecs;
+  ms.gx = bv;
+  ms.gy = bv + M;
+  ms.gz = bv + 2 * M;
+  ms.b = a.gradnonlin ? a.bvals + (size_t)v * M : a.bvals;
+  ms.M = M;
+  const float R = a.R, invR = 1.f / (2.f * R + 1.f);
+  const int gbo = a.model == 3 ? 2 : 0;
+  // non-finite data: flag and emit zeros
+  bool bad = false;
+  for (int m = lane; m < M; m += 32) bad |= !isfinite(ms.y[m]);
+  bad = __any_sync(0xffffffffu, bad);
+  const int npo = a.np_out;
+  float* out = a.params + (size_t)v * npo;
+  if (bad) {
+    if (lane < npo) out[lane] = 0.f;
+    if (lane == 0) {
+      if (a.tau) a.tau[v] = 0.f;
+      if (a.status) a.status[v] = BPX_VOX_NONFINITE_DATA;
+    }
+    return;
+  }
+  Dti dt;
+  dti_fit(ms, lane, dt);
+  float res[16];
+  bool refit = false;
+  if (a.model == 1) {
+    if (a.nonlin) {
+      float p[LmShape<kSingle, K, F0>::P];
+      start_single<K, F0>(dt, p);
+      lm_run<kSingle, K, F0>(ms, p, lane, 0, R, invR);
+      finalise<kSingle, K, F0>(p);
+#pragma unroll
+      for (int i = 0; i < NPOUT; ++i) res[i] = p[i];
+      if (F0 && ((K > 0 && p[2] < 0.05f) || p[1] > 0.007f || p[NPOUT - 1] > 0.4f)) {
+        float p2[LmShape<kSingle, K, false>::P];
+        start_single<K, false>(dt, p2);
+        lm_run<kSingle, K, false>(ms, p2, lane, 0, R, invR);
+        finalise<kSingle, K, false>(p2);
+#pragma unroll
+        for (int i = 0; i < NPOUT - 1; ++i) res[i] = p2[i];
+        res[NPOUT - 1] = 0.001f;
+        refit = true;
+      }
+    } else {
+      float p[LmShape<kSingleC, K, F0>::P];
+      start_single_c<K, F0>(dt, ms, lane, p);
+      lm_run<kSingleC, K, F0>(ms, p, lane, 0, R, invR);
+      finalise<kSingleC, K, F0>(p);
+#pragma unroll
+      for (int i = 0; i < NPOUT; ++i) res[i] = p[i];
+      if (F0 && ((K > 0 && p[2] < 0.05f) || p[1] > 0.007f || p[NPOUT - 1] > 0.4f)) {
+        float p2[LmShape<kSingleC, K, false>::P];
+        start_single_c<K, false>(dt, ms, lane, p2);
+        lm_run<kSingleC, K, false>(ms, p2, lane, 0, R, invR);
+        finalise<kSingleC, K, false>(p2);
+#pragma unroll
+        for (int i = 0; i < NPOUT - 1; ++i) res[i] = p2[i];
+        res[NPOUT - 1] = 0.001f;
+        refit = true;
+      }
+    }
+  } else {
+    constexpr int NPM = LmShape<kMulti, K, F0>::P;
+    float s[LmShape<kSingle, K, F0>::P];
+    start_single<K, F0>(dt, s);
+    lm_run<kSingle, K, F0>(ms, s, lane, 0, R, invR);
+    finalise<kSingle, K, F0>(s);
+    float p[NPM];
+    start_multi<K, F0>(s, p);
+    lm_run<kMulti, K, F0>(ms, p, lane, gbo, R, invR);
+    finalise<kMulti, K, F0>(p);
+#pragma unroll
+    for (int i = 0; i < NPM; ++i) res[i] = p[i];
+    if (F0 && ((K > 0 && p[3] < 0.05f) || p[1] > 0.007f || p[NPM - 1] > 0.4f)) {
+      // GPU re-fit path: PVM_single_c then PVM_multi (CUDA/xfibres_gpu.cu:331-333)
+      float c[LmShape<kSingleC, K, false>::P];
+      start_single_c<K, false>(dt, ms, lane, c);
+      lm_run<kSingleC, K, false>(ms, c, lane, 0, R, invR);
+      finalise<kSingleC, K, false>(c);
+      float p2[LmShape<kMulti, K, false>::P];
+      start_multi<K, false>(c, p2);
+      lm_run<kMulti, K, false>(ms, p2, lane, gbo, R, invR);
+      finalise<kMulti, K, false>(p2);
+#pragma unroll
+      for (int i = 0; i < NPM - 1; ++i) res[i] = p2[i];
+      res[NPM - 1] = 0.001f;
+      refit = true;
+    }
+  }
+  // tau = 1 / var(y - prediction)   (sample variance, n-1)
+  if (a.rician) {
+    const int o = a.model >= 2 ? 3 : 2;
+    const bool use_f0 = F0 && !refit;
+    const float f0 = F0 ? res[npo - 1] : 0.f;
+    float s1 = 0.f;
+    for (int m = lane; m < M; m += 32)
+      s1 += ms.y[m] - predict_final<K>(a.model, res, o, use_f0, f0, R, ms.gx[m], ms.gy[m], ms.gz[m], ms.b[m]);
+    const double mean = group_sum<32>((double)s1) / M;
+    double s2 = 0.0;
+    for (int m = lane; m < M; m += 32) {
+      const double r = ms.y[m] - predict_final<K>(a.model, res, o, use_f0, f0, R, ms.gx[m], ms.gy[m], ms.gz[m], ms.b[m]) - mean;
+      s2 += r * r;
+    }
+    s2 = group_sum<32>(s2);
+    if (lane == 0 && a.tau) a.tau[v] = (float)(1.0 / (s2 / (M - 1)));
+  } else if (lane == 0 && a.tau) {
+    a.tau[v] = 0.f;
+  }
+#pragma unroll
+  for (int i = 0; i < 16; ++i)
+    if (i < npo && lane == i) out[i] = res[i];
+  if (lane == 0 && a.status) a.status[v] = refit ? BPX_VOX_F0_REFIT : 0u;
+}
+
+template <int K, bool F0>
+__global__ void __launch_bounds__(kFitThreads) fit_kernel(FitArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int warps = blockDim.x >> 5;
+  for (int v = blockIdx.x * warps + (threadIdx.x >> 5); v < a.nvox; v += gridDim.x * warps) fit_one<K, F0>(a, v, lane);
+}
+
+// remove_NonPositive_entries (CUDA/xfibres_gpu.cu:350-367), one warp per voxel
+__global__ void __launch_bounds__(kFitThreads) prepare_kernel(int nvox, int ndir, float* data) {
+  const int lane = threadIdx.x & 31;
+  const int warps = blockDim.x >> 5;
+  for (int v = blockIdx.x * warps + (threadIdx.x >> 5); v < nvox; v += gridDim.x * warps) {
+    float* y = data + (size_t)v * ndir;
+    float mn = INFINITY, mx = -INFINITY;
+    for (int m = lane; m < ndir; m += 32) {
+      mn = fminf(mn, y[m]);
+      mx = fmaxf(mx, y[m]);
+    }
+    mn = group_min<32>(mn);
+    mx = group_max<32>(mx);
+    if (mn <= 0.f && mx > 0.f) {
+      float mp = INFINITY;
+      for (int m = lane; m < ndir; m += 32)
+        if (y[m] > 0.f) mp = fminf(mp, y[m]);
+      mp = group_min<32>(mp);
+      for (int m = lane; m < ndir; m += 32)
+        if (y[m] <= 0.f) y[m] = mp;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// launchers
+// ------------------------------------------------------------------------------------------
+template <int K, bool F0>
+static cudaError_t launch_fit_kf(const FitArgs& a, cudaStream_t s) {
+  const int warps = kFitThreads / 32;
+  int grid = (a.nvox + warps - 1) / warps;
+  const int cap = sm_count() * 16;
+  if (grid > cap) grid = cap;
+  if (grid < 1) grid = 1;
+  fit_kernel<K, F0><<<grid, kFitThreads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fit(const FitArgs& a, int nfib, bool f0, cudaStream_t s) {
+  if (a.nvox == 0) return cudaSuccess;
+  switch (nfib * 2 + (f0 ? 1 : 0)) {
+    case 2: return launch_fit_kf<1, false>(a, s);
+    case 3: return launch_fit_kf<1, true>(a, s);
+    case 4: return launch_fit_kf<2, false>(a, s);
+    case 5: return launch_fit_kf<2, true>(a, s);
+    case 6: return launch_fit_kf<3, false>(a, s);
+    case 7: return launch_fit_kf<3, true>(a, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_prepare(int nvox, int ndir, float* data, cudaStream_t s) {
+  if (nvox == 0) return cudaSuccess;
+  const int warps = kFitThreads / 32;
+  int grid = (nvox + warps - 1) / warps;
+  const int cap = sm_count() * 16;
+  if (grid > cap) grid = cap;
+  prepare_kernel<<<grid, kFitThreads, 0, s>>>(nvox, ndir, data);
+  return cudaGetLastError();
+}
+
+}  // namespace bpx

@@ -1,0 +1,80 @@
+// bpx_internal.h -- launch descriptors shared by the kernels and the C-ABI layer.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "bpx.h"
+
+namespace bpx {
+
+constexpr int kFitThreads = 256;   // 8 warps, one voxel per warp
+constexpr int kMcmcThreads = 128;  // 4 warps
+
+int sm_count();  // multiprocessors of the current device (cached per device)
+
+struct FitArgs {
+  int nvox, ndir;
+  const float* data;
+  const float* bvecs;
+  const float* bvals;
+  int gradnonlin;
+  float* params;
+  int np_out;
+  float* tau;
+  uint32_t* status;
+  int model, rician, nonlin;
+  float R;
+};
+
+struct McmcArgs {
+  int nvox, ndir;
+  const float* data;
+  const float* bvecs;
+  const float* bvals;
+  int gradnonlin;
+  const float* params;
+  int np_fit;
+  const float* tau;
+  float* records;  // [nrec][nsamples][nvox]
+  int nsamples;
+  uint32_t* status;
+  int nburn, njumps, sampleevery, upe;
+  int f0, ardf0, no_ard, all_ard;
+  float fudge, R_mean, R_std, R_fudge;
+  uint64_t seed, voxel_offset;
+};
+
+struct EnergyArgs {
+  int nvox, ndir;
+  const float* data;
+  const float* bvecs;
+  const float* bvals;
+  int gradnonlin;
+  const float* states;  // [nvox][BPX_NSTATE]
+  float* lik;
+  float* prior;
+  int f0, ardf0, no_ard, all_ard;
+  float fudge, R_mean, R_std, R_fudge;
+};
+
+struct FinishArgs {
+  int nvox, nsamples, nfib;
+  const float* records;
+  bpx_outputs out;
+};
+
+// Launch layout of the MCMC kernel: TPV lanes per voxel, at most MPL measurements per lane.
+struct McmcLayout {
+  int tpv, mpl;
+};
+
+cudaError_t launch_fit(const FitArgs& a, int nfib, bool f0, cudaStream_t s);
+cudaError_t launch_prepare(int nvox, int ndir, float* data, cudaStream_t s);
+cudaError_t launch_mcmc(const McmcArgs& a, int model, int nfib, bool rician, McmcLayout lay, cudaStream_t s);
+McmcLayout choose_layout(int model, int nfib, bool rician, int ndir);
+bool layout_supported(int model, int nfib, bool rician, McmcLayout lay);
+cudaError_t launch_energy(const EnergyArgs& a, int model, int nfib, bool rician, cudaStream_t s);
+cudaError_t launch_finish(const FinishArgs& a, cudaStream_t s);
+
+}  // namespace bpx

@@ -1,0 +1,764 @@
+// bpx_mcmc_impl.cuh -- the MCMC kernel of the bedpostx path (template; instantiated per model
+// in bpx_mcmc_m{1,2,3}.cu).
+//
+// Replaces init_Fibres_Multifibres_kernel + runmcmc_kernel (burn-in and recording launches)
+// of CUDA/runmcmc_kernels.cu:193-1474 with one launch that runs each voxel's whole chain.
+//
+// Layout: a group of TPV lanes owns one voxel; lane l of the group holds measurements
+// l, l+TPV, ... (at most MPL of them) in registers: data y, b-value, the squared projections
+// c_k = (g.v_k)^2 of every fibre, the per-fibre signals s_k and the isotropic signal.  The scalar
+// chain state (parameters, priors, proposal widths, acceptance counts) is replicated in every
+// lane of the group, so the accept/reject logic needs no broadcast; likelihood sums use an
+// xor-butterfly over the group.  Proposals evaluate new signals into registers and commit them
+// with selects, so groups sharing a warp never diverge.
+//
+// Random numbers: slot s of iteration it of voxel v uses Philox-4x32-10 with counter
+// (it, s, v) and key = seed.  At the start of each iteration lane l computes slots l, l+TPV, ...
+// once, and proposals fetch theirs with a shuffle.
+//
+// Deviations from the reference, all of which leave the chain's target distribution unchanged:
+//   * FP32 signals and likelihoods (the reference uses FP64); energy differences are formed as
+//     (M/2) ln(SS_old/SS_new) (Gaussian) or M ln(tau_new/tau_old) + sum(t_new - t_old) (Rician)
+//     with the Rician terms written as log y - tau (y-p)^2/2 + [logI0(z) - z], so no large
+//     cancelling sums appear in FP32.
+//   * a proposal rejected by its prior skips the likelihood (the reference evaluates and
+//     discards it); its random numbers are consumed either way, being slot-keyed.
+//   * fibre directions enter as dot products (g.v)^2 instead of the reference's three cosines of
+//     spherical angles (CUDA/runmcmc_kernels.cu:389-398, same quantity).
+#pragma once
+
+#include <cstdint>
+
+#include "bpx_device.cuh"
+#include "bpx_internal.h"
+
+namespace bpx {
+
+template <int MODEL>
+struct SigParams {
+  // model 1 (or model 2 with d_std < 1e-5): s = 2^(e1 * b * c), iso = 2^(e1 * b)
+  // model 2: s = 2^(-alpha * log2(1 + beta * b * c))
+  // model 3: s = 2^(e3 * b * ((1-R) c + R))
+  float e1, alpha, beta, e3, omR, R;
+  bool mono;
+};
+
+template <int MODEL>
+__device__ __forceinline__ SigParams<MODEL> sig_params(float d, float dstd, float R) {
+  SigParams<MODEL> sp;
+  sp.e1 = -d * kLog2e;
+  sp.mono = (MODEL == 1) || (dstd < 1e-5f);
+  if (MODEL >= 2) {
+    const float s2 = dstd * dstd;
+    sp.alpha = d * d / s2;
+    sp.beta = s2 / d;
+  } else {
+    sp.alpha = 0.f;
+    sp.beta = 0.f;
+  }
+  if (MODEL == 3) {
+    const float invR = 1.0f / (2.0f * R + 1.0f);
+    sp.e3 = -3.0f * d * invR * kLog2e;
+    sp.omR = 1.0f - R;
+    sp.R = R;
+  } else {
+    sp.e3 = 0.f;
+    sp.omR = 0.f;
+    sp.R = 0.f;
+  }
+  return sp;
+}
+
+// compute_signal (CUDA/runmcmc_kernels.cu:67-83)
+template <int MODEL>
+__device__ __forceinline__ float stick_signal(const SigParams<MODEL>& sp, float b, float c) {
+  if (MODEL == 1) return ex2_approx(sp.e1 * b * c);
+  if (MODEL == 2) {
+    if (sp.mono) return ex2_approx(sp.e1 * b * c);
+    return ex2_approx(-sp.alpha * lg2_approx(1.0f + sp.beta * b * c));
+  }
+  return ex2_approx(sp.e3 * b * (sp.omR * c + sp.R));
+}
+
+// compute_iso_signal (CUDA/runmcmc_kernels.cu:84-95)
+template <int MODEL>
+__device__ __forceinline__ float iso_signal(const SigParams<MODEL>& sp, float b) {
+  if (MODEL == 1 || sp.mono) return ex2_approx(sp.e1 * b);
+  return ex2_approx(-sp.alpha * lg2_approx(1.0f + sp.beta * b));
+}
+
+struct Priors {
+  float fudge, R_mean, R_std, R_fudge;
+  int ardf0, can_use_ard;
+};
+
+// theta prior -log|sin(th)/2| (CUDA/runmcmc_kernels.cu:1142-1147)
+__device__ __forceinline__ float th_prior(float th) {
+  return th == 0.f ? 0.f : -logf(fabsf(sinf(th) * 0.5f));
+}
+
+// R prior (CUDA/runmcmc_kernels.cu:1058-1083); returns true if R is rejected
+__device__ __forceinline__ bool r_prior(const Priors& pr, float R, float d, float& prior) {
+  float upper_R = 2.0f * pr.R_mean;
+  float lower_R = pr.R_mean - 2.0f * pr.R_std;
+  if (pr.R_mean > 0.5f) upper_R = 1.0f;
+  if (lower_R < 0.0f) lower_R = 1e-8f;
+  if (pr.R_fudge > 0.0f && d > kUpperDiff / 2.0f) {
+    if (R < 1e-8f || R > upper_R) return true;
+    prior = pr.R_fudge * logf(R);
+    return false;
+  }
+  if (R <= lower_R || R > upper_R) return true;
+  prior = (R - pr.R_mean) * (R - pr.R_mean) / (pr.R_std * pr.R_std);
+  return false;
+}
+
+template <int MODEL, int K, bool RIC, int TPV, int MPL>
+struct Lanes {
+  float y[MPL], b[MPL], c[K][MPL], s[K][MPL], iso[MPL];
+  int nj;  // measurements held by this lane
+};
+
+// likelihood statistic of one state: SS (Gaussian) or sum_m [-tau (y-p)^2/2 + logI0(z)-z] (Rician),
+// summed over the group.  Signals: s_k for k != kr, snew for fibre kr (kr = -1: none), iso array.
+template <int MODEL, int K, bool RIC, int TPV, int MPL>
+__device__ __forceinline__ float lik_stat(const Lanes<MODEL, K, RIC, TPV, MPL>& L, const float (&isoa)[MPL],
+                                          const float (&sk)[K][MPL], float S0, const float (&f)[K],
+                                          float f0, float tau) {
+  float fsum = f0;
+#pragma unroll
+  for (int k = 0; k < K; ++k) fsum += f[k];
+  const float wiso = 1.0f - fsum;
+  float acc = 0.f;
+#pragma unroll
+  for (int j = 0; j < MPL; ++j) {
+    if (j < L.nj) {
+      float base = f0 + wiso * isoa[j];
+#pragma unroll
+      for (int k = 0; k < K; ++k) base += f[k] * sk[k][j];
+      const float pred = S0 * base;
+      const float r = L.y[j] - pred;
+      if (!RIC) {
+        acc += r * r;
+      } else {
+        const float z = tau * pred * L.y[j];
+        acc += -0.5f * tau * r * r + logI0_minus_z(z);
+      }
+    }
+  }
+  return group_sum<TPV>(acc);
+}
+
+// energy difference E_old - E_new of the likelihood part
+template <bool RIC>
+__device__ __forceinline__ float dlik(float st_old, float st_new, float tau_old, float tau_new, float halfM, float M) {
+  if (!RIC) return halfM * logf(st_old / st_new);
+  return M * logf(tau_new / tau_old) + (st_new - st_old);
+}
+
+template <int MODEL, int K, bool RIC, int TPV, int MPL>
+__global__ void __launch_bounds__(kMcmcThreads) mcmc_kernel(McmcArgs a) {
+  constexpr int NS = 6 + 3 * K;                 // proposal slots
+  constexpr int NR = (NS + TPV - 1) / TPV;      // Philox blocks per lane per iteration
+  constexpr int GPW = 32 / TPV;                 // groups (voxels) per warp
+  const int lane = threadIdx.x & 31;
+  const int gl = lane % TPV;
+  const int gw = lane / TPV;
+  const int warps_total = gridDim.x * (blockDim.x >> 5);
+  const int warp_id = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int M = a.ndir;
+  const float halfM = 0.5f * (float)M, fM = (float)M;
+  const int total = a.nburn + a.njumps;
+  const int ns = a.nsamples;
+  Priors pr;
+  pr.fudge = a.fudge;
+  pr.R_mean = a.R_mean;
+  pr.R_std = a.R_std;
+  pr.R_fudge = a.R_fudge;
+  pr.ardf0 = a.ardf0;
+  pr.can_use_ard = !a.no_ard;
+  const bool use_f0 = a.f0 != 0;
+
+  for (int round = 0;; ++round) {
+    const int first = (warp_id + round * warps_total) * GPW;
+    if (first >= a.nvox) break;
+    const int vreal = first + gw;
+    const bool valid = vreal < a.nvox;
+    const int v = valid ? vreal : a.nvox - 1;
+    const uint64_t gvox = a.voxel_offset + (uint64_t)v;
+
+    // ---- load this lane's measurements ----
+    Lanes<MODEL, K, RIC, TPV, MPL> L;
+    const float* yv = a.data + (size_t)v * M;
+    const float* bv = a.gradnonlin ? a.bvecs + (size_t)v * 3 * M : a.bvecs;
+    const float* bl = a.gradnonlin ? a.bvals + (size_t)v * M : a.bvals;
+    L.nj = 0;
+    bool bad = false;
+#pragma unroll
+    for (int j = 0; j < MPL; ++j) {
+      const int m = gl + j * TPV;
+      if (m < M) {
+        L.y[j] = __ldg(yv + m);
+        L.b[j] = __ldg(bl + m);
+        L.nj = j + 1;
+        bad |= !isfinite(L.y[j]);
+      } else {
+        L.y[j] = 0.f;
+        L.b[j] = 0.f;
+      }
+    }
+    bad = group_sum<TPV>(bad ? 1.f : 0.f) > 0.f;
+
+    // ---- init_Fibres_Multifibres (CUDA/runmcmc_kernels.cu:255-504) ----
+    const float* prm = a.params + (size_t)v * a.np_fit;
+    float S0 = prm[0];
+    float d = prm[1];
+    if (d < 0.f || d > kUpperDiff) d = 2e-3f;
+    float dstd = 0.f, R = 0.f;
+    if (MODEL >= 2) {
+      dstd = prm[2];
+      const float upper = MODEL == 3 ? 0.004f : 0.01f;
+      if (dstd < 0.f || dstd > upper) dstd = d / 10.f;
+      R = MODEL == 3 ? a.R_mean : 0.f;
+    }
+    float f0 = use_f0 ? prm[a.np_fit - 1] : 0.f;
+    float tau = (RIC && a.tau) ? a.tau[v] : 0.f;
+    constexpr int add = MODEL >= 2 ? 1 : 0;
+    float th[K], ph[K], f[K], vx[K], vy[K], vz[K], p_th[K], p_f[K];
+    bool lam[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      th[k] = prm[2 + 3 * k + 1 + add];
+      ph[k] = prm[2 + 3 * k + 2 + add];
+      f[k] = prm[2 + 3 * k + add];
+      lam[k] = (k == 0) ? (a.all_ard != 0) : (a.no_ard == 0);
+      p_th[k] = th_prior(th[k]);
+      float fp = 0.f;
+      if (!(f[k] <= 0.f || f[k] >= 1.f)) fp = pr.fudge * (lam[k] ? logf(f[k]) : 0.f);
+      p_f[k] = fp;
+      float st, ct, sp, cp;
+      sincosf(th[k], &st, &ct);
+      sincosf(ph[k], &sp, &cp);
+      vx[k] = st * cp;
+      vy[k] = st * sp;
+      vz[k] = ct;
+    }
+    float p_d = 0.f, p_dstd = 0.f, p_R = 0.f, p_f0 = 0.f;
+    if (MODEL == 3 && d >= 0.f && d <= kUpperDiff) p_d = (1.0f - 3.0f) * logf(d) + 4000.0f * d;
+    if (MODEL >= 2) {
+      const float upper = MODEL == 3 ? 0.004f : 0.01f;
+      if (dstd > 0.f && dstd <= upper) p_dstd = logf(dstd);
+      if (MODEL == 3) {
+        float prr = 0.f;
+        if (!r_prior(pr, R, d, prr)) p_R = prr;
+      }
+    }
+    if (use_f0 && !(f0 <= 0.f || f0 >= 1.f) && a.ardf0) p_f0 = logf(f0);
+    auto prior_sum = [&]() {
+      float p = p_d + p_dstd + p_R + p_f0;
+#pragma unroll
+      for (int k = 0; k < K; ++k) p += p_th[k] + p_f[k];
+      return p;
+    };
+    float prior = prior_sum();
+    {
+      const SigParams<MODEL> sp = sig_params<MODEL>(d, dstd, R);
+#pragma unroll
+      for (int j = 0; j < MPL; ++j) {
+        const int m = gl + j * TPV;
+        float gx = 0.f, gy = 0.f, gz = 0.f;
+        if (m < M) {
+          gx = __ldg(bv + m);
+          gy = __ldg(bv + M + m);
+          gz = __ldg(bv + 2 * M + m);
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          const float dp = gx * vx[k] + gy * vy[k] + gz * vz[k];
+          L.c[k][j] = dp * dp;
+          L.s[k][j] = stick_signal<MODEL>(sp, L.b[j], L.c[k][j]);
+        }
+        L.iso[j] = iso_signal<MODEL>(sp, L.b[j]);
+      }
+    }
+    float lik = lik_stat<MODEL, K, RIC, TPV, MPL>(L, L.iso, L.s, S0, f, f0, tau);
+    // initialise_props
+    float prop[NS];
+#pragma unroll
+    for (int q = 0; q < NS; ++q) prop[q] = 0.2f;
+    prop[kSlotS0] = S0 / 10.f;
+    prop[kSlotD] = d / 10.f;
+    prop[kSlotDstd] = dstd / 10.f;
+    prop[kSlotTau] = tau / 2.f;
+    prop[kSlotF0] = 0.2f;
+    prop[kSlotR] = R / 10.f;
+    uint32_t accw[(NS + 3) / 4];
+#pragma unroll
+    for (int q = 0; q < (NS + 3) / 4; ++q) accw[q] = 0u;
+#define BPX_ACC(slot, ok) accw[(slot) / 4] += (ok) ? (1u << (8 * ((slot) % 4))) : 0u
+#define BPX_ACCN(slot) ((accw[(slot) / 4] >> (8 * ((slot) % 4))) & 0xffu)
+
+    int sample = 0;
+    for (int it = 0; it < total; ++it) {
+      // randoms of this iteration: lane gl holds slots gl, gl+TPV, ...
+      float rn[NR], rl[NR];
+#pragma unroll
+      for (int q = 0; q < NR; ++q) {
+        const int slot = gl + q * TPV;
+        rn[q] = 0.f;
+        rl[q] = 0.f;
+        if (slot < NS) slot_randoms(a.seed, gvox, (uint32_t)it, (uint32_t)slot, rn[q], rl[q]);
+      }
+#define BPX_RAND(slot, n, lu)                                                   \
+  const float n = __shfl_sync(0xffffffffu, rn[(slot) / TPV], (slot) % TPV, TPV); \
+  const float lu = __shfl_sync(0xffffffffu, rl[(slot) / TPV], (slot) % TPV, TPV)
+
+      // ---------------- f0 ----------------
+      if (use_f0) {
+        BPX_RAND(kSlotF0, n, lu);
+        const float f0n = f0 + n * prop[kSlotF0];
+        bool rej = (f0n <= 0.f || f0n >= 1.f);
+        const float pf0n = rej ? p_f0 : (a.ardf0 ? logf(f0n) : 0.f);
+        float fs = f0n;
+#pragma unroll
+        for (int k = 0; k < K; ++k) fs += f[k];
+        rej = rej || (fs > 1.f);
+        const float priorn = prior - p_f0 + pf0n;
+        float likn = lik;
+        if (__any_sync(0xffffffffu, !rej)) likn = lik_stat<MODEL, K, RIC, TPV, MPL>(L, L.iso, L.s, S0, f, f0n, tau);
+        const bool ok = !rej && ((prior - priorn) + dlik<RIC>(lik, likn, tau, tau, halfM, fM) > lu);
+        if (ok) {
+          f0 = f0n;
+          p_f0 = pf0n;
+          prior = priorn;
+          lik = likn;
+        }
+        BPX_ACC(kSlotF0, ok);
+      }
+      // ---------------- tau ----------------
+      if (RIC) {
+        BPX_RAND(kSlotTau, n, lu);
+        const float taun = tau + n * prop[kSlotTau];
+        const bool rej = taun <= 0.f;
+        float likn = lik;
+        if (__any_sync(0xffffffffu, !rej)) likn = lik_stat<MODEL, K, RIC, TPV, MPL>(L, L.iso, L.s, S0, f, f0, rej ? tau : taun);
+        const bool ok = !rej && (dlik<RIC>(lik, likn, tau, taun, halfM, fM) > lu);
+        if (ok) {
+          tau = taun;
+          lik = likn;
+        }
+        BPX_ACC(kSlotTau, ok);
+      }
+      // ---------------- d ----------------
+      {
+        BPX_RAND(kSlotD, n, lu);
+        const float dn = d + n * prop[kSlotD];
+        const bool rej = (dn < 0.f || dn > kUpperDiff);
+        const float pdn = rej ? p_d : (MODEL == 3 ? (1.0f - 3.0f) * logf(dn) + 4000.0f * dn : 0.f);
+        const float priorn = prior - p_d + pdn;
+        float likn = lik;
+        float ns_[K][MPL], ni[MPL];
+        if (__any_sync(0xffffffffu, !rej)) {
+          const SigParams<MODEL> sp = sig_params<MODEL>(rej ? d : dn, dstd, R);
+#pragma unroll
+          for (int j = 0; j < MPL; ++j) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) ns_[k][j] = stick_signal<MODEL>(sp, L.b[j], L.c[k][j]);
+            ni[j] = iso_signal<MODEL>(sp, L.b[j]);
+          }
+          likn = lik_stat<MODEL, K, RIC, TPV, MPL>(L, ni, ns_, S0, f, f0, tau);
+        } else {
+#pragma unroll
+          for (int j = 0; j < MPL; ++j) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) ns_[k][j] = L.s[k][j];
+            ni[j] = L.iso[j];
+          }
+        }
+        const bool ok = !rej && ((prior - priorn) + dlik<RIC>(lik, likn, tau, tau, halfM, fM) > lu);
+        if (ok) {
+          d = dn;
+          p_d = pdn;
+          prior = priorn;
+          lik = likn;
+        }
+#pragma unroll
+        for (int j = 0; j < MPL; ++j) {
+#pragma unroll
+          for (int k = 0; k < K; ++k) L.s[k][j] = ok ? ns_[k][j] : L.s[k][j];
+          L.iso[j] = ok ? ni[j] : L.iso[j];
+        }
+        BPX_ACC(kSlotD, ok);
+      }
+      // ---------------- d_std ----------------
+      if (MODEL >= 2) {
+        BPX_RAND(kSlotDstd, n, lu);
+        const float dsn = dstd + n * prop[kSlotDstd];
+        const float upper = MODEL == 3 ? 0.004f : 0.01f;
+        const bool rej = (dsn <= 0.f || dsn > upper);
+        const float pdsn = rej ? p_dstd : logf(dsn);
+        const float priorn = prior - p_dstd + pdsn;
+        float likn = lik;
+        float ns_[K][MPL], ni[MPL];
+        if (__any_sync(0xffffffffu, !rej)) {
+          const SigParams<MODEL> sp = sig_params<MODEL>(d, rej ? dstd : dsn, R);
+#pragma unroll
+          for (int j = 0; j < MPL; ++j) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) ns_[k][j] = (MODEL == 2) ? stick_signal<MODEL>(sp, L.b[j], L.c[k][j]) : L.s[k][j];
+            ni[j] = iso_signal<MODEL>(sp, L.b[j]);
+          }
+          likn = lik_stat<MODEL, K, RIC, TPV, MPL>(L, ni, ns_, S0, f, f0, tau);
+        } else {
+#pragma unroll
+          for (int j = 0; j < MPL; ++j) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) ns_[k][j] = L.s[k][j];
+            ni[j] = L.iso[j];
+          }
+        }
+        const bool ok = !rej && ((prior - priorn) + dlik<RIC>(lik, likn, tau, tau, halfM, fM) > lu);
+        if (ok) {
+          dstd = dsn;
+          p_dstd = pdsn;
+          prior = priorn;
+          lik = likn;
+        }
+#pragma unroll
+        for (int j = 0; j < MPL; ++j) {
+#pragma unroll
+          for (int k = 0; k < K; ++k) L.s[k][j] = ok ? ns_[k][j] : L.s[k][j];
+          L.iso[j] = ok ? ni[j] : L.iso[j];
+        }
+        BPX_ACC(kSlotDstd, ok);
+      }
+      // ---------------- R ----------------
+      if (MODEL == 3) {
+        BPX_RAND(kSlotR, n, lu);
+        const float Rn = R + n * prop[kSlotR];
+        float pRn = p_R;
+        const bool rej = r_prior(pr, Rn, d, pRn);
+        if (rej) pRn = p_R;
+        const float priorn = prior - p_R + pRn;
+        float likn = lik;
+        float ns_[K][MPL];
+        if (__any_sync(0xffffffffu, !rej)) {
+          const SigParams<MODEL> sp = sig_params<MODEL>(d, dstd, rej ? R : Rn);
+#pragma unroll
+          for (int j = 0; j < MPL; ++j)
+#pragma unroll
+            for (int k = 0; k < K; ++k) ns_[k][j] = stick_signal<MODEL>(sp, L.b[j], L.c[k][j]);
+          likn = lik_stat<MODEL, K, RIC, TPV, MPL>(L, L.iso, ns_, S0, f, f0, tau);
+        } else {
+#pragma unroll
+          for (int j = 0; j < MPL; ++j)
+#pragma unroll
+            for (int k = 0; k < K; ++k) ns_[k][j] = L.s[k][j];
+        }
+        const bool ok = !rej && ((prior - priorn) + dlik<RIC>(lik, likn, tau, tau, halfM, fM) > lu);
+        if (ok) {
+          R = Rn;
+          p_R = pRn;
+          prior = priorn;
+          lik = likn;
+        }
+#pragma unroll
+        for (int j = 0; j < MPL; ++j)
+#pragma unroll
+          for (int k = 0; k < K; ++k) L.s[k][j] = ok ? ns_[k][j] : L.s[k][j];
+        BPX_ACC(kSlotR, ok);
+      }
+      // ---------------- S0 ----------------
+      {
+        BPX_RAND(kSlotS0, n, lu);
+        const float S0n = S0 + n * prop[kSlotS0];
+        const bool rej = S0n < 0.f;
+        float likn = lik;
+        if (__any_sync(0xffffffffu, !rej)) likn = lik_stat<MODEL, K, RIC, TPV, MPL>(L, L.iso, L.s, rej ? S0 : S0n, f, f0, tau);
+        const bool ok = !rej && (dlik<RIC>(lik, likn, tau, tau, halfM, fM) > lu);
+        if (ok) {
+          S0 = S0n;
+          lik = likn;
+        }
+        BPX_ACC(kSlotS0, ok);
+      }
+      // ---------------- fibres ----------------
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        // theta and phi
+#pragma unroll
+        for (int ang = 0; ang < 2; ++ang) {
+          const int slot = kSlotFibre0 + 3 * k + ang;
+          BPX_RAND(slot, n, lu);
+          float thn = th[k], phn = ph[k];
+          if (ang == 0)
+            thn = th[k] + n * prop[slot];
+          else
+            phn = ph[k] + n * prop[slot];
+          const float pthn = (ang == 0) ? th_prior(thn) : p_th[k];
+          const float priorn = prior - p_th[k] + pthn;
+          float st, ct, sp_, cp;
+          sincosf(thn, &st, &ct);
+          sincosf(phn, &sp_, &cp);
+          const float nvx = st * cp, nvy = st * sp_, nvz = ct;
+          const SigParams<MODEL> sp = sig_params<MODEL>(d, dstd, R);
+          float nc[MPL], ns_[K][MPL];
+#pragma unroll
+          for (int j = 0; j < MPL; ++j) {
+            const int m = gl + j * TPV;
+            float gx = 0.f, gy = 0.f, gz = 0.f;
+            if (m < M) {
+              gx = __ldg(bv + m);
+              gy = __ldg(bv + M + m);
+              gz = __ldg(bv + 2 * M + m);
+            }
+            const float dp = gx * nvx + gy * nvy + gz * nvz;
+            nc[j] = dp * dp;
+#pragma unroll
+            for (int kk = 0; kk < K; ++kk) ns_[kk][j] = (kk == k) ? stick_signal<MODEL>(sp, L.b[j], nc[j]) : L.s[kk][j];
+          }
+          const float likn = lik_stat<MODEL, K, RIC, TPV, MPL>(L, L.iso, ns_, S0, f, f0, tau);
+          const bool ok = ((prior - priorn) + dlik<RIC>(lik, likn, tau, tau, halfM, fM) > lu);
+          if (ok) {
+            th[k] = thn;
+            ph[k] = phn;
+            p_th[k] = pthn;
+            vx[k] = nvx;
+            vy[k] = nvy;
+            vz[k] = nvz;
+            prior = priorn;
+            lik = likn;
+          }
+#pragma unroll
+          for (int j = 0; j < MPL; ++j) {
+            L.c[k][j] = ok ? nc[j] : L.c[k][j];
+            L.s[k][j] = ok ? ns_[k][j] : L.s[k][j];
+          }
+          BPX_ACC(slot, ok);
+        }
+        // f
+        {
+          const int slot = kSlotFibre0 + 3 * k + 2;
+          BPX_RAND(slot, n, lu);
+          const float fkn = f[k] + n * prop[slot];
+          bool rej = (fkn <= 0.f || fkn >= 1.f);
+          float pfn = p_f[k];
+          if (!rej) pfn = pr.fudge * ((pr.can_use_ard && lam[k]) ? logf(fkn) : 0.f);
+          float fn[K];
+#pragma unroll
+          for (int kk = 0; kk < K; ++kk) fn[kk] = (kk == k) ? fkn : f[kk];
+          float fs = f0;
+#pragma unroll
+          for (int kk = 0; kk < K; ++kk) fs += fn[kk];
+          rej = rej || (fs > 1.f);
+          const float priorn = prior - p_f[k] + pfn;
+          float likn = lik;
+          if (__any_sync(0xffffffffu, !rej)) likn = lik_stat<MODEL, K, RIC, TPV, MPL>(L, L.iso, L.s, S0, rej ? f : fn, f0, tau);
+          const bool ok = !rej && ((prior - priorn) + dlik<RIC>(lik, likn, tau, tau, halfM, fM) > lu);
+          if (ok) {
+            f[k] = fkn;
+            p_f[k] = pfn;
+            prior = priorn;
+            lik = likn;
+          }
+          BPX_ACC(slot, ok);
+        }
+      }
+#undef BPX_RAND
+      // ---------------- record (CUDA/runmcmc_kernels.cu:1326-1339) ----------------
+      if (it >= a.nburn && ((it - a.nburn + 1) % a.sampleevery) == 0 && sample < ns) {
+        if (valid && gl == 0) {
+          const size_t stride = (size_t)ns * a.nvox;
+          float* r = a.records + (size_t)sample * a.nvox + v;
+          r[0 * stride] = d;
+          r[1 * stride] = f0;
+          r[2 * stride] = tau;
+          r[3 * stride] = dstd;
+          r[4 * stride] = R;
+          r[5 * stride] = S0;
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            r[(6 + 3 * k) * stride] = th[k];
+            r[(7 + 3 * k) * stride] = ph[k];
+            r[(8 + 3 * k) * stride] = f[k];
+          }
+        }
+        ++sample;
+      }
+      // ---------------- update_proposals (CUDA/runmcmc_kernels.cu:1341-1395) ----------------
+      // every slot is proposed once per iteration, so since the last update acc + rej = upe
+      if (((it + 1) % a.upe) == 0) {
+        const float upe = (float)a.upe;
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+          const bool on = (q == kSlotD) || (q == kSlotS0) || (q >= kSlotFibre0) || (q == kSlotTau && RIC) ||
+                          (q == kSlotF0 && use_f0) || (q == kSlotDstd && MODEL >= 2) || (q == kSlotR && MODEL == 3);
+          if (on) {
+            const float acc = (float)BPX_ACCN(q);
+            prop[q] *= sqrtf((acc + 1.0f) / (upe - acc + 1.0f));
+            prop[q] = fminf(prop[q], kMaxProp);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < (NS + 3) / 4; ++q) accw[q] = 0u;
+      }
+    }
+#undef BPX_ACC
+#undef BPX_ACCN
+    if (valid && gl == 0 && a.status) {
+      uint32_t st = a.status[v];
+      if (!isfinite(lik)) st |= BPX_VOX_NONFINITE_ENERGY;
+      if (bad) st |= BPX_VOX_NONFINITE_DATA;
+      a.status[v] = st;
+    }
+  }
+}
+
+// Energies of given states (for the FP32-vs-FP64 likelihood check): one group per voxel.
+template <int MODEL, int K, bool RIC, int TPV, int MPL>
+__global__ void __launch_bounds__(kMcmcThreads) energy_kernel(EnergyArgs a) {
+  constexpr int GPW = 32 / TPV;
+  const int lane = threadIdx.x & 31;
+  const int gl = lane % TPV;
+  const int gw = lane / TPV;
+  const int warps_total = gridDim.x * (blockDim.x >> 5);
+  const int warp_id = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int M = a.ndir;
+  for (int round = 0;; ++round) {
+    const int first = (warp_id + round * warps_total) * GPW;
+    if (first >= a.nvox) break;
+    const int vreal = first + gw;
+    const bool valid = vreal < a.nvox;
+    const int v = valid ? vreal : a.nvox - 1;
+    const float* st = a.states + (size_t)v * BPX_NSTATE;
+    const float S0 = st[0], d = st[1], dstd = st[2], R = st[3], tau = st[4];
+    const float f0 = a.f0 ? st[5] : 0.f;
+    float f[K];
+    Lanes<MODEL, K, RIC, TPV, MPL> L;
+    const float* yv = a.data + (size_t)v * M;
+    const float* bv = a.gradnonlin ? a.bvecs + (size_t)v * 3 * M : a.bvecs;
+    const float* bl = a.gradnonlin ? a.bvals + (size_t)v * M : a.bvals;
+    const SigParams<MODEL> sp = sig_params<MODEL>(d, dstd, R);
+    L.nj = 0;
+    float logy_part = 0.f;
+#pragma unroll
+    for (int j = 0; j < MPL; ++j) {
+      const int m = gl + j * TPV;
+      L.y[j] = m < M ? yv[m] : 0.f;
+      L.b[j] = m < M ? bl[m] : 0.f;
+      if (m < M) {
+        L.nj = j + 1;
+        if (RIC) logy_part += logf(L.y[j]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      f[k] = st[8 + 3 * k];
+      float s_, c_, sp_, cp_;
+      sincosf(st[6 + 3 * k], &s_, &c_);
+      sincosf(st[7 + 3 * k], &sp_, &cp_);
+#pragma unroll
+      for (int j = 0; j < MPL; ++j) {
+        const int m = gl + j * TPV;
+        float dp = 0.f;
+        if (m < M) dp = bv[m] * s_ * cp_ + bv[M + m] * s_ * sp_ + bv[2 * M + m] * c_;
+        L.c[k][j] = dp * dp;
+        L.s[k][j] = stick_signal<MODEL>(sp, L.b[j], L.c[k][j]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < MPL; ++j) L.iso[j] = iso_signal<MODEL>(sp, L.b[j]);
+    const float stat = lik_stat<MODEL, K, RIC, TPV, MPL>(L, L.iso, L.s, S0, f, f0, tau);
+    float lik;
+    if (!RIC)
+      lik = 0.5f * (float)M * logf(stat / 2.0f);
+    else
+      lik = -(float)M * logf(tau) - (group_sum<TPV>(logy_part) + stat);
+    // prior energy as init_Fibres_Multifibres_kernel composes it
+    Priors pr;
+    pr.fudge = a.fudge;
+    pr.R_mean = a.R_mean;
+    pr.R_std = a.R_std;
+    pr.R_fudge = a.R_fudge;
+    float p = 0.f;
+    if (MODEL == 3 && d >= 0.f && d <= kUpperDiff) p += (1.0f - 3.0f) * logf(d) + 4000.0f * d;
+    if (MODEL >= 2) {
+      const float upper = MODEL == 3 ? 0.004f : 0.01f;
+      if (dstd > 0.f && dstd <= upper) p += logf(dstd);
+      if (MODEL == 3) {
+        float prr = 0.f;
+        if (!r_prior(pr, R, d, prr)) p += prr;
+      }
+    }
+    if (a.f0 && !(f0 <= 0.f || f0 >= 1.f) && a.ardf0) p += logf(f0);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const bool lj = (k == 0) ? (a.all_ard != 0) : (a.no_ard == 0);
+      float fp = 0.f;
+      if (!(f[k] <= 0.f || f[k] >= 1.f)) fp = a.fudge * (lj ? logf(f[k]) : 0.f);
+      p += th_prior(st[6 + 3 * k]) + fp;
+    }
+    if (valid && gl == 0) {
+      if (a.lik) a.lik[v] = lik;
+      if (a.prior) a.prior[v] = p;
+    }
+  }
+}
+
+template <int MODEL, int K, bool RIC, int TPV, int MPL>
+cudaError_t launch_mcmc_t(const McmcArgs& a, cudaStream_t s) {
+  auto kern = mcmc_kernel<MODEL, K, RIC, TPV, MPL>;
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kMcmcThreads, 0);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  const int vox_per_block = (kMcmcThreads / 32) * (32 / TPV);
+  int grid = (a.nvox + vox_per_block - 1) / vox_per_block;
+  const int cap = sm_count() * per_sm;
+  if (grid > cap) grid = cap;
+  if (grid < 1) grid = 1;
+  kern<<<grid, kMcmcThreads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int MODEL, int K, bool RIC, int TPV, int MPL>
+cudaError_t launch_energy_t(const EnergyArgs& a, cudaStream_t s) {
+  const int vox_per_block = (kMcmcThreads / 32) * (32 / TPV);
+  int grid = (a.nvox + vox_per_block - 1) / vox_per_block;
+  const int cap = sm_count() * 8;
+  if (grid > cap) grid = cap;
+  if (grid < 1) grid = 1;
+  energy_kernel<MODEL, K, RIC, TPV, MPL><<<grid, kMcmcThreads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+// Layouts compiled for every (model, K, rician): (TPV, MPL) with capacity TPV*MPL.
+#define BPX_LAYOUTS(X) X(4, 9) X(8, 8) X(8, 9) X(16, 9) X(32, 9) X(32, 16)
+
+template <int MODEL>
+cudaError_t launch_mcmc_model(const McmcArgs& a, int nfib, bool ric, McmcLayout lay, cudaStream_t s) {
+#define BPX_TRY(T, P)                                                              \
+  if (lay.tpv == T && lay.mpl == P) {                                              \
+    if (nfib == 1) return ric ? launch_mcmc_t<MODEL, 1, true, T, P>(a, s) : launch_mcmc_t<MODEL, 1, false, T, P>(a, s); \
+    if (nfib == 2) return ric ? launch_mcmc_t<MODEL, 2, true, T, P>(a, s) : launch_mcmc_t<MODEL, 2, false, T, P>(a, s); \
+    if (nfib == 3) return ric ? launch_mcmc_t<MODEL, 3, true, T, P>(a, s) : launch_mcmc_t<MODEL, 3, false, T, P>(a, s); \
+  }
+  BPX_LAYOUTS(BPX_TRY)
+#undef BPX_TRY
+  return cudaErrorInvalidValue;
+}
+
+template <int MODEL>
+cudaError_t launch_energy_model(const EnergyArgs& a, int nfib, bool ric, McmcLayout lay, cudaStream_t s) {
+#define BPX_TRY(T, P)                                                              \
+  if (lay.tpv == T && lay.mpl == P) {                                              \
+    if (nfib == 1) return ric ? launch_energy_t<MODEL, 1, true, T, P>(a, s) : launch_energy_t<MODEL, 1, false, T, P>(a, s); \
+    if (nfib == 2) return ric ? launch_energy_t<MODEL, 2, true, T, P>(a, s) : launch_energy_t<MODEL, 2, false, T, P>(a, s); \
+    if (nfib == 3) return ric ? launch_energy_t<MODEL, 3, true, T, P>(a, s) : launch_energy_t<MODEL, 3, false, T, P>(a, s); \
+  }
+  BPX_LAYOUTS(BPX_TRY)
+#undef BPX_TRY
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace bpx

@@ -1,0 +1,257 @@
+"""Python binding of libbpx.so (the sm_100a CUDA library) through its C-ABI.
+
+Host-side mirror of the xfibres_gpu interface for tests, benchmarks and Python users.  Device
+memory comes from torch (plumbing only); every computation runs in the library's CUDA kernels.
+There is no CPU fallback: if the library is missing or the device is not sm_100, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .abi import BPX_NSTATE, Options, Outputs, Volume, nrec
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libbpx.so")
+
+# exported functions: name -> (restype, argtypes)
+_SIGS = {
+    "bpx_abi_version": (C.c_int32, []),
+    "bpx_options_default": (None, [C.POINTER(Options)]),
+    "bpx_nparams_fit": (C.c_int32, [C.POINTER(Options)]),
+    "bpx_nsamples": (C.c_int32, [C.POINTER(Options)]),
+    "bpx_max_ndir": (C.c_int32, []),
+    "bpx_last_error": (C.c_char_p, []),
+    "bpx_fit_dev": (C.c_int, [C.POINTER(Options), C.POINTER(Volume), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "bpx_prepare_data_dev": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
+    "bpx_mcmc_dev": (C.c_int, [C.POINTER(Options), C.POINTER(Volume), C.c_void_p, C.c_void_p, C.c_void_p,
+                               C.c_void_p, C.c_void_p]),
+    "bpx_finish_dev": (C.c_int, [C.POINTER(Options), C.c_int32, C.c_void_p, C.POINTER(Outputs), C.c_void_p]),
+    "bpx_xfibres_dev": (C.c_int, [C.POINTER(Options), C.POINTER(Volume), C.POINTER(Outputs), C.c_void_p]),
+    "bpx_xfibres_host": (C.c_int, [C.POINTER(Options), C.POINTER(Volume), C.POINTER(Outputs)]),
+    "bpx_energy_dev": (C.c_int, [C.POINTER(Options), C.POINTER(Volume), C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_void_p]),
+    "bpx_gradnonlin_dev": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p]),
+    "bpx_mcmc_layouts": (C.c_int32, [C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32]),
+    "bpx_release_workspace": (C.c_int, []),
+    "bpx_measure_pipes": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+}
+
+_lib = None
+
+
+class BpxError(RuntimeError):
+    pass
+
+
+def load(path: str | None = None):
+    """Load libbpx.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise BpxError(f"{p} not found: build it with `python -m fdt_b200.build`")
+    L = C.CDLL(p)
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != 0:
+        msg = load().bpx_last_error().decode(errors="replace")
+        raise BpxError(f"{what} failed with status {rc}: {msg}")
+
+
+def _torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        raise BpxError("CUDA device required")
+    return torch
+
+
+def _stream(torch):
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def make_volume(data, bvecs, bvals, voxel_offset: int = 0) -> Volume:
+    v = Volume()
+    v.nvox, v.ndir = int(data.shape[0]), int(data.shape[1])
+    v.data, v.bvecs, v.bvals = _ptr(data), _ptr(bvecs), _ptr(bvals)
+    v.grad = None
+    v.voxel_offset = voxel_offset
+    return v
+
+
+def to_device(x, torch=None):
+    torch = torch or _torch()
+    if isinstance(x, np.ndarray):
+        x = torch.from_numpy(np.ascontiguousarray(x, np.float32))
+    return x.to(device="cuda", dtype=torch.float32).contiguous()
+
+
+def prepare_data(data) -> None:
+    """remove_NonPositive_entries in place on a device tensor [nvox][ndir]."""
+    torch = _torch()
+    _check(load().bpx_prepare_data_dev(data.shape[0], data.shape[1], _ptr(data), _stream(torch)), "bpx_prepare_data_dev")
+
+
+def fit(opts: Options, data, bvecs, bvals):
+    """LM initial fits (+ tau under rician).  Returns (params, tau, status) device tensors."""
+    torch = _torch()
+    nvox = data.shape[0]
+    params = torch.zeros((nvox, opts.nparams_fit), device="cuda", dtype=torch.float32)
+    tau = torch.zeros(nvox, device="cuda", dtype=torch.float32)
+    status = torch.zeros(nvox, device="cuda", dtype=torch.int32)
+    vol = make_volume(data, bvecs, bvals)
+    _check(load().bpx_fit_dev(C.byref(opts), C.byref(vol), _ptr(params), _ptr(tau), _ptr(status), _stream(torch)),
+           "bpx_fit_dev")
+    return params, tau, status
+
+
+def mcmc(opts: Options, data, bvecs, bvals, params, tau=None, voxel_offset: int = 0, status=None):
+    """Burn-in + recording.  Returns records [nrec][nsamples][nvox] (device)."""
+    torch = _torch()
+    nvox = data.shape[0]
+    rec = torch.zeros((nrec(opts.nfibres), opts.nsamples, nvox), device="cuda", dtype=torch.float32)
+    vol = make_volume(data, bvecs, bvals, voxel_offset)
+    _check(load().bpx_mcmc_dev(C.byref(opts), C.byref(vol), _ptr(params), _ptr(tau), _ptr(rec), _ptr(status),
+                               _stream(torch)), "bpx_mcmc_dev")
+    return rec
+
+
+OUT_KEYS = ["th", "ph", "f", "mean_d", "mean_dstd", "mean_R", "mean_f0", "mean_tau", "mean_S0", "mean_f", "dyads",
+            "status"]
+
+
+def alloc_outputs(opts: Options, nvox: int, device: str = "cuda", pin: bool = False):
+    """Output arrays (torch tensors on `device`) and the Outputs struct pointing at them."""
+    import torch
+
+    K, ns = opts.nfibres, opts.nsamples
+    shapes = dict(th=(K, ns, nvox), ph=(K, ns, nvox), f=(K, ns, nvox), mean_d=(nvox,), mean_dstd=(nvox,),
+                  mean_R=(nvox,), mean_f0=(nvox,), mean_tau=(nvox,), mean_S0=(nvox,), mean_f=(K, nvox),
+                  dyads=(K, 3, nvox), status=(nvox,))
+    t = {}
+    for k, s in shapes.items():
+        dt = torch.int32 if k == "status" else torch.float32
+        t[k] = torch.zeros(s, device=device, dtype=dt, pin_memory=(pin and device == "cpu"))
+    o = Outputs()
+    for k in OUT_KEYS:
+        setattr(o, k, t[k].data_ptr())
+    return t, o
+
+
+def finish(opts: Options, records):
+    torch = _torch()
+    nvox = records.shape[2]
+    t, o = alloc_outputs(opts, nvox)
+    _check(load().bpx_finish_dev(C.byref(opts), nvox, _ptr(records), C.byref(o), _stream(torch)), "bpx_finish_dev")
+    return t
+
+
+def xfibres_dev(opts: Options, data, bvecs, bvals, voxel_offset: int = 0, out=None):
+    """Whole pipeline on device tensors; returns the output dict (device tensors)."""
+    torch = _torch()
+    nvox = data.shape[0]
+    if out is None:
+        t, o = alloc_outputs(opts, nvox)
+    else:
+        t, o = out
+    vol = make_volume(data, bvecs, bvals, voxel_offset)
+    _check(load().bpx_xfibres_dev(C.byref(opts), C.byref(vol), C.byref(o), _stream(torch)), "bpx_xfibres_dev")
+    return t
+
+
+def xfibres_host(opts: Options, data: np.ndarray, bvecs: np.ndarray, bvals: np.ndarray, grad: np.ndarray | None = None,
+                 voxel_offset: int = 0, out=None):
+    """Drop-in for xfibres_gpu() with host arrays (synchronous).  Returns dict of host tensors."""
+    data = np.ascontiguousarray(data, np.float32)
+    bvecs = np.ascontiguousarray(bvecs, np.float32)
+    bvals = np.ascontiguousarray(bvals, np.float32)
+    nvox = data.shape[0]
+    if out is None:
+        t, o = alloc_outputs(opts, nvox, device="cpu")
+    else:
+        t, o = out
+    vol = Volume()
+    vol.nvox, vol.ndir = data.shape
+    vol.data, vol.bvecs, vol.bvals = data.ctypes.data, bvecs.ctypes.data, bvals.ctypes.data
+    g = None
+    if grad is not None:
+        g = np.ascontiguousarray(grad, np.float32)
+        vol.grad = g.ctypes.data
+    vol.voxel_offset = voxel_offset
+    _check(load().bpx_xfibres_host(C.byref(opts), C.byref(vol), C.byref(o)), "bpx_xfibres_host")
+    return t
+
+
+def energy(opts: Options, data, bvecs, bvals, states):
+    """FP32 likelihood and prior energies of states [nvox][15] (device)."""
+    torch = _torch()
+    nvox = data.shape[0]
+    lik = torch.zeros(nvox, device="cuda", dtype=torch.float32)
+    prior = torch.zeros(nvox, device="cuda", dtype=torch.float32)
+    vol = make_volume(data, bvecs, bvals)
+    _check(load().bpx_energy_dev(C.byref(opts), C.byref(vol), _ptr(states), _ptr(lik), _ptr(prior), _stream(torch)),
+           "bpx_energy_dev")
+    return lik, prior
+
+
+def gradnonlin(grad, bvecs, bvals):
+    """Per-voxel corrected b-matrix on the device: returns (bvecs [nvox][3][ndir], bvals [nvox][ndir])."""
+    torch = _torch()
+    nvox, ndir = grad.shape[0], bvals.shape[0]
+    bv = torch.zeros((nvox, 3, ndir), device="cuda", dtype=torch.float32)
+    bl = torch.zeros((nvox, ndir), device="cuda", dtype=torch.float32)
+    _check(load().bpx_gradnonlin_dev(nvox, ndir, _ptr(grad), _ptr(bvecs), _ptr(bvals), _ptr(bv), _ptr(bl),
+                                     _stream(torch)), "bpx_gradnonlin_dev")
+    return bv, bl
+
+
+def mcmc_layouts() -> list[tuple[int, int]]:
+    L = load()
+    n = L.bpx_mcmc_layouts(None, None, 0)
+    tpv = (C.c_int32 * n)()
+    mpl = (C.c_int32 * n)()
+    L.bpx_mcmc_layouts(tpv, mpl, n)
+    return list(zip(list(tpv), list(mpl)))
+
+
+def measure_pipes() -> tuple[float, float]:
+    """(MUFU ops/s, FP32 FMA ops/s) measured on the current device."""
+    _torch()
+    m, f = C.c_double(), C.c_double()
+    _check(load().bpx_measure_pipes(C.byref(m), C.byref(f)), "bpx_measure_pipes")
+    return m.value, f.value
+
+
+def states_from_records(opts: Options, records, sample: int):
+    """Chain states [nvox][15] (S0, d, d_std, R, tau, f0, (th, ph, f)*3) of one recorded sample."""
+    torch = _torch()
+    nvox = records.shape[2]
+    st = torch.zeros((nvox, BPX_NSTATE), device=records.device, dtype=torch.float32)
+    r = records[:, sample, :]
+    st[:, 0] = r[5]
+    st[:, 1] = r[0]
+    st[:, 2] = r[3]
+    st[:, 3] = r[4]
+    st[:, 4] = r[2]
+    st[:, 5] = r[1]
+    for k in range(opts.nfibres):
+        st[:, 6 + 3 * k] = r[6 + 3 * k]
+        st[:, 7 + 3 * k] = r[7 + 3 * k]
+        st[:, 8 + 3 * k] = r[8 + 3 * k]
+    return st

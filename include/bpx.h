@@ -1,0 +1,217 @@
+/*
+ * bpx.h -- C-ABI of the B200 bedpostx per-voxel path (libbpx.so).
+ *
+ * The library replaces the GPU half of FSL FDT's xfibres_gpu:
+ *   - the host entry  void xfibres_gpu(Matrix datam, Matrix bvecs, Matrix bvals,
+ *       Matrix gradm, int idpart, int idSubpart, float seed, string subjdir)
+ *     (CUDA/xfibres_gpu.h:15-23, implemented in CUDA/xfibres_gpu.cu:29-146),
+ *   - the kernel-level entries of libbedpostx_cuda.so
+ *     (CUDA/fit_gpu_kernels.h:9-102, CUDA/runmcmc_kernels.cu:26,193,507),
+ *   - the host sample finishing (CUDA/xfibres_gpu.cu:659-738, CUDA/samples.cu:134-347).
+ *
+ * Plain pointers and sizes only.  Every function returns a bpx_status; nothing calls exit().
+ * Functions named *_dev take DEVICE pointers and a cudaStream_t passed as void*; they are
+ * asynchronous with respect to the host unless stated.  bpx_xfibres_host takes HOST pointers
+ * and is synchronous.  Options are passed explicitly (the reference reads a process-wide
+ * xfibresOptions singleton), so calls with different options may run concurrently on
+ * different streams.
+ *
+ * Array layouts (row-major, C order):
+ *   data      [nvox][ndir]                 (voxel-major; CUDA/xfibres_gpu.cu:390-399)
+ *   bvecs     [3][ndir], bvals [ndir]      (or [nvox][3][ndir], [nvox][ndir] with gradnonlin;
+ *                                           CUDA/xfibres_gpu.cu:411-446)
+ *   params    [nvox][bpx_nparams_fit()]    LM output, layout
+ *             [S0, d, (d_std,) (f,th,ph)*nfib, (f0)]   (CUDA/PVM_multi.cu:549-566)
+ *   records   [BPX_NREC(nfib)][nsamples][nvox]   one row per recorded parameter, in the
+ *             order d, f0, tau, d_std, R, S0, then th_k, ph_k, f_k for k = 0..nfib-1
+ *             (the records of CUDA/runmcmc_kernels.cu:1326-1339, transposed so that every
+ *             row has the [nsamples][nvox] layout of the part files)
+ *   samples   th/ph/f [nfib][nsamples][nvox]: the th{k}samples/ph{k}samples/f{k}samples
+ *             part files of Samples::save (CUDA/samples.cu:262-347), fibres sorted by
+ *             decreasing sum of f over samples.
+ */
+#ifndef BPX_H
+#define BPX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BPX_ABI_VERSION 1
+#define BPX_MAX_FIBRES 3
+/* number of recorded parameters: d, f0, tau, d_std, R, S0 + (th, ph, f) per fibre */
+#define BPX_NREC(nfib) (6 + 3 * (nfib))
+
+typedef enum bpx_status {
+  BPX_OK = 0,
+  BPX_ERR_INVALID_ARG = 1, /* a size, pointer or option is out of range */
+  BPX_ERR_CUDA = 2,        /* a CUDA runtime call failed; see bpx_last_error() */
+  BPX_ERR_NO_DEVICE = 3,   /* no CUDA device, or the device is not sm_100 */
+  BPX_ERR_UNSUPPORTED = 4, /* option combination not built (e.g. ndir too large) */
+  BPX_ERR_IO = 5,          /* part-file read/write failed */
+  BPX_ERR_BAD_DATA = 6     /* non-finite input data */
+} bpx_status;
+
+/* Per-voxel status bits written by the pipeline (bpx_outputs.status). */
+#define BPX_VOX_NONFINITE_DATA 1u  /* data held NaN/Inf: voxel skipped, outputs zero */
+#define BPX_VOX_F0_REFIT 2u        /* the f0 plausibility rule re-fitted this voxel without f0 */
+#define BPX_VOX_NONFINITE_ENERGY 4u /* the chain met a non-finite energy */
+
+/*
+ * The xfibresOptions fields that act on the per-voxel path (xfibresoptions.h:104-149).
+ * Booleans are 0/1.  bpx_options_default() gives the xfibres defaults.
+ */
+typedef struct bpx_options {
+  int32_t model;               /* --model 1|2|3                       (default 1) */
+  int32_t nfibres;             /* --nf 1..3                           (default 1) */
+  float fudge;                 /* --fudge ARD weight                  (default 1) */
+  int32_t njumps;              /* --nj                                (default 1250) */
+  int32_t nburn;               /* --bi                                (default 1000) */
+  int32_t sampleevery;         /* --se                                (default 25) */
+  int32_t updateproposalevery; /* --upe                               (default 40) */
+  int32_t no_ard;              /* --noard */
+  int32_t all_ard;             /* --allard */
+  int32_t nonlin;              /* --nonlinear: model 1 fitted with PVM_single */
+  int32_t cnonlin;             /* --cnonlinear: model 1 fitted with PVM_single_c (the GPU default) */
+  int32_t rician;              /* --rician */
+  int32_t f0;                  /* --f0 */
+  int32_t ardf0;               /* --ardf0 */
+  float R_prior_mean;          /* --Rmean                             (default 0.13) */
+  float R_prior_std;           /* --Rstd                              (default 0.03) */
+  float R_prior_fudge;         /* --Rfudge                            (default 0) */
+  int32_t gradnonlin;          /* --gradnonlin given: per-voxel b-matrix */
+  uint64_t seed;               /* --seed                              (default 8665904) */
+  int32_t mcmc_tpv;            /* MCMC launch layout: lanes per voxel (0 = automatic) */
+  int32_t mcmc_mpl;            /* MCMC launch layout: measurements per lane (0 = automatic) */
+  int32_t reserved[6];         /* zero */
+} bpx_options;
+
+/* One volume (a part or subpart of xfibres_gpu). */
+typedef struct bpx_volume {
+  int32_t nvox;          /* voxels (may be 0) */
+  int32_t ndir;          /* measurements per voxel, 1..BPX max (bpx_max_ndir()) */
+  const float* data;     /* [nvox][ndir] */
+  const float* bvecs;    /* [3][ndir], unit vectors; [nvox][3][ndir] with gradnonlin */
+  const float* bvals;    /* [ndir]; [nvox][ndir] with gradnonlin */
+  const float* grad;     /* host entry only: [nvox][9] gradient-nonlinearity tensors or NULL */
+  uint64_t voxel_offset; /* global index of voxel 0: keys the counter-based RNG, so a voxel's
+                            chain does not depend on how the volume is split */
+} bpx_volume;
+
+/* Outputs of the full pipeline.  Any pointer may be NULL to skip that output. */
+typedef struct bpx_outputs {
+  float* th;        /* [nfib][nsamples][nvox]  merged_th{k}samples */
+  float* ph;        /* [nfib][nsamples][nvox]  merged_ph{k}samples */
+  float* f;         /* [nfib][nsamples][nvox]  merged_f{k}samples  */
+  float* mean_d;    /* [nvox] mean_dsamples */
+  float* mean_dstd; /* [nvox] mean_d_stdsamples (model >= 2) */
+  float* mean_R;    /* [nvox] mean_Rsamples (model 3) */
+  float* mean_f0;   /* [nvox] mean_f0samples (--f0) */
+  float* mean_tau;  /* [nvox] mean_tausamples (--rician) */
+  float* mean_S0;   /* [nvox] mean_S0samples */
+  float* mean_f;    /* [nfib][nvox] mean_f{k}samples */
+  float* dyads;     /* [nfib][3][nvox] principal eigenvector of the mean dyadic tensor */
+  uint32_t* status; /* [nvox] BPX_VOX_* bits */
+} bpx_outputs;
+
+/* ---- library facts ---- */
+int32_t bpx_abi_version(void);
+void bpx_options_default(bpx_options* opts);
+/* LM parameter count: 2+3*nf (+1 model>=2) (+1 f0)  (CUDA/xfibres_gpu.cu:190-193) */
+int32_t bpx_nparams_fit(const bpx_options* opts);
+int32_t bpx_nsamples(const bpx_options* opts); /* njumps / sampleevery */
+int32_t bpx_max_ndir(void);
+/* Message of the last failing call on this host thread ("" if none). */
+const char* bpx_last_error(void);
+
+/* ---- stage entry points (device pointers, asynchronous on `stream`) ---- */
+
+/*
+ * Initial fits, replacing fit() (CUDA/xfibres_gpu.cu:173-348) and calculate_tau
+ * (CUDA/diffmodels.cu:259-347): DTI start values, LM fit of PVM_single / PVM_single_c /
+ * PVM_multi, the f0 plausibility re-fit with mix_params, and tau = 1/var(residuals) when
+ * opts->rician.  params: [nvox][bpx_nparams_fit]; tau: [nvox] (may be NULL unless rician);
+ * status: [nvox] or NULL.  Under --rician the data must already have had non-positive
+ * entries replaced (bpx_prepare_data_dev).
+ */
+bpx_status bpx_fit_dev(const bpx_options* opts, const bpx_volume* vol, float* params, float* tau,
+                       uint32_t* status, void* stream);
+
+/*
+ * remove_NonPositive_entries for every voxel (CUDA/xfibres_gpu.cu:350-367): non-positive
+ * samples of a voxel with a positive maximum are replaced by its smallest positive sample.
+ * In place on data [nvox][ndir].
+ */
+bpx_status bpx_prepare_data_dev(int32_t nvox, int32_t ndir, float* data, void* stream);
+
+/*
+ * MCMC: init_Fibres_Multifibres_kernel + runmcmc_kernel burn-in and recording
+ * (CUDA/runmcmc.cu:27-316).  records: [BPX_NREC(nfib)][nsamples][nvox].
+ * tau may be NULL unless rician.  status may be NULL.
+ */
+bpx_status bpx_mcmc_dev(const bpx_options* opts, const bpx_volume* vol, const float* params,
+                        const float* tau, float* records, uint32_t* status, void* stream);
+
+/*
+ * Sample finishing: Samples::record/finish_voxel/save (CUDA/samples.cu:134-347).
+ * Sorts fibres by sum of f, writes th/ph/f sample arrays, means and dyads.
+ */
+bpx_status bpx_finish_dev(const bpx_options* opts, int32_t nvox, const float* records,
+                          bpx_outputs* out, void* stream);
+
+/*
+ * Whole pipeline on device buffers: prepare (rician) -> fit -> mcmc -> finish, for one volume.
+ * `data` is modified in place under --rician.  Workspace comes from a per-device cache
+ * owned by the library (grown on demand, freed by bpx_release_workspace).
+ */
+bpx_status bpx_xfibres_dev(const bpx_options* opts, const bpx_volume* vol, bpx_outputs* out,
+                           void* stream);
+
+/*
+ * Drop-in for xfibres_gpu() with HOST buffers: copies data/bvecs/bvals (and grad under
+ * gradnonlin) to the current device, corrects the b-matrix per voxel when vol->grad is given
+ * (correct_bvals_bvecs, CUDA/xfibres_gpu.cu:151-170), runs the pipeline and copies the
+ * outputs back into host buffers.  Synchronous.
+ */
+bpx_status bpx_xfibres_host(const bpx_options* opts, const bpx_volume* vol, bpx_outputs* host_out);
+
+/*
+ * Energies of given chain states, for checking the FP32 likelihood against an FP64 evaluation
+ * (compute_likelihood + compute_prior, CUDA/runmcmc_kernels.cu:140-191).
+ * states: [nvox][BPX_NSTATE] = S0, d, d_std, R, tau, f0, (th, ph, f) * 3.
+ * lik, prior: [nvox] outputs (either may be NULL).
+ */
+#define BPX_NSTATE 15
+bpx_status bpx_energy_dev(const bpx_options* opts, const bpx_volume* vol, const float* states,
+                          float* lik, float* prior, void* stream);
+
+/*
+ * Gradient-nonlinearity correction on the device (correct_bvals_bvecs, CUDA/xfibres_gpu.cu:151-170):
+ * for every voxel and every b>0 measurement, g' = (I+L) g / |(I+L) g| and b' = |(I+L) g|^2 b, with
+ * L the voxel's 3x3 coil tensor stored column-major in grad [nvox][9].
+ * bvecs [3][ndir], bvals [ndir] in; bvecs_out [nvox][3][ndir], bvals_out [nvox][ndir] out.
+ */
+bpx_status bpx_gradnonlin_dev(int32_t nvox, int32_t ndir, const float* grad, const float* bvecs,
+                              const float* bvals, float* bvecs_out, float* bvals_out, void* stream);
+
+/* MCMC launch layouts compiled into the library: writes up to `max` (tpv, mpl) pairs and returns
+ * how many exist. */
+int32_t bpx_mcmc_layouts(int32_t* tpv, int32_t* mpl, int32_t max);
+
+/*
+ * Measures the current device's MUFU (ex2.approx) and FP32 FMA issue rates with two
+ * throughput-bound microkernels (synchronous, ~20 ms).  Results in operations per second,
+ * one operation = one lane-instruction.  These are the denominators of the MCMC roofline.
+ */
+bpx_status bpx_measure_pipes(double* mufu_ops_per_s, double* fma_ops_per_s);
+
+/* Free the per-device workspace cache of the current device. */
+bpx_status bpx_release_workspace(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BPX_H */

@@ -1,0 +1,295 @@
+"""GPU parity tests: the CUDA path (through the C-ABI) against the FP64 oracle on the same inputs.
+
+Tolerances (stated per criterion):
+  (a) LM fits: S0, d, d_std and f1 within 1e-3 relative (f1 within 1e-3 absolute) and the first
+      fibre's direction within 0.1 degree, in at least 95% of voxels (FP32 GPU vs FP64 oracle
+      from the same data; the remaining voxels are ill-conditioned fits, e.g. near-zero fractions).
+  (b) FP32 log-likelihood energies within 2e-5 relative of the FP64 oracle on the same states;
+      prior energies within 1e-4 absolute.
+  (c) chains share the counter-based random stream with the oracle, so short chains agree step by
+      step until an accept decision falls within FP32 rounding of its threshold; posterior means
+      agree within 2 Monte-Carlo standard errors in at least 95% of voxels.
+"""
+import numpy as np
+import pytest
+
+from fdt_b200 import synth
+from fdt_b200.abi import Options
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+@pytest.fixture(scope="module")
+def lib(torch):
+    from fdt_b200 import lib as L
+
+    L.load()
+    return L
+
+
+def _dev(torch, *arrs):
+    return [torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda() for a in arrs]
+
+
+def _dirs(p, o, k):
+    th, ph = p[:, o + 3 * k + 1], p[:, o + 3 * k + 2]
+    return np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], 1)
+
+
+def _fit_agreement(o, pg, po):
+    off = 3 if o.model >= 2 else 2
+    rel = lambda a, b: np.abs(a - b) / np.maximum(np.abs(b), 1e-12)
+    ok = rel(pg[:, 0], po[:, 0]) < 1e-3
+    ok &= rel(pg[:, 1], po[:, 1]) < 1e-3
+    if o.model >= 2:
+        ok &= rel(pg[:, 2], po[:, 2]) < 1e-3
+    ok &= np.abs(pg[:, off] - po[:, off]) < 1e-3
+    cosang = np.abs(np.sum(_dirs(pg, off, 0) * _dirs(po, off, 0), 1))
+    ok &= np.degrees(np.arccos(np.clip(cosang, 0, 1))) < 0.1
+    return ok
+
+
+FIT_CASES = [
+    ("m1_cnonlin_K2", dict(model=1, nfibres=2), "small", 20.0),
+    ("m1_nonlin_K2_f0", dict(model=1, nfibres=2, nonlin=1, f0=1), "small", 20.0),
+    ("m1_cnonlin_K3_f0_rician", dict(model=1, nfibres=3, f0=1, rician=1), "small", 20.0),
+    ("m2_K3", dict(model=2, nfibres=3), "multi", 25.0),
+    ("m2_K3_f0_rician_ardf0", dict(model=2, nfibres=3, f0=1, rician=1, ardf0=1), "brain", 25.0),
+    ("m3_K2", dict(model=3, nfibres=2), "multi", 25.0),
+]
+
+
+def _protocol(name):
+    return {"small": synth.single_shell_64(), "multi": synth.three_shell(9, 90),
+            "brain": synth.three_shell(18, 90)}[name]
+
+
+@pytest.mark.parametrize("name,kw,protname,snr", FIT_CASES, ids=[c[0] for c in FIT_CASES])
+def test_fit_parity(torch, lib, oracle, name, kw, protname, snr):
+    prot = _protocol(protname)
+    o = Options.make(**kw)
+    gamma = o.model >= 2
+    y, tr = synth.make_volume(256, prot, o.nfibres, gamma, snr, seed=100 + len(name))
+    if o.rician:
+        y = oracle.prepare_data(y)
+    po, to, so = oracle.fit(o, y, prot.bvecs, prot.bvals)
+    d, bv, bl = _dev(torch, y, prot.bvecs, prot.bvals)
+    pg, tg, sg = lib.fit(o, d, bv, bl)
+    torch.cuda.synchronize()
+    pg, tg, sg = pg.cpu().numpy(), tg.cpu().numpy(), sg.cpu().numpy()
+    assert np.all(np.isfinite(pg))
+    ok = _fit_agreement(o, pg, po)
+    # the f0 re-fit decision must agree wherever the fits agree
+    assert np.all((((sg & 2) != 0) == ((so & 2) != 0))[ok])
+    assert ok.mean() >= 0.95, f"{name}: only {ok.mean():.3f} of voxels agree"
+    if o.rician:
+        rt = np.abs(tg - to) / to
+        assert np.median(rt[ok]) < 1e-3
+
+
+def test_fit_handles_nonfinite_and_empty(torch, lib):
+    prot = synth.single_shell_64()
+    y, _ = synth.make_volume(8, prot, 2, False, 20.0, seed=3)
+    y[3, 5] = np.nan
+    o = Options.make(model=1, nfibres=2)
+    d, bv, bl = _dev(torch, y, prot.bvecs, prot.bvals)
+    p, t, s = lib.fit(o, d, bv, bl)
+    s = s.cpu().numpy()
+    assert s[3] & 1 and not (s[np.arange(8) != 3] & 1).any()
+    assert np.all(p.cpu().numpy()[3] == 0)
+    e = torch.zeros((0, 64), device="cuda")
+    p0, _, _ = lib.fit(o, e, bv, bl)
+    assert p0.shape[0] == 0
+
+
+def _state_sample(o, prot, n, seed):
+    rng = np.random.default_rng(seed)
+    tr = synth.sample_truth(rng, n, o.nfibres, o.model >= 2)
+    st = np.zeros((n, 15))
+    st[:, 0] = tr.S0 * rng.uniform(0.95, 1.05, n)
+    st[:, 1] = tr.d * rng.uniform(0.8, 1.2, n)
+    st[:, 2] = tr.dstd if tr.dstd is not None else 0.0
+    st[:, 3] = 0.13
+    st[:, 4] = (20.0 / 1000.0) ** 2 * rng.uniform(0.5, 2.0, n)
+    st[:, 5] = 0.02 if o.f0 else 0.0
+    for k in range(o.nfibres):
+        v = tr.v[:, k, :]
+        st[:, 6 + 3 * k] = np.arccos(np.clip(v[:, 2], -1, 1)) + rng.normal(0, 0.05, n)
+        st[:, 7 + 3 * k] = np.arctan2(v[:, 1], v[:, 0]) + rng.normal(0, 0.05, n)
+        st[:, 8 + 3 * k] = np.clip(tr.f[:, k], 0.01, None)
+    y = synth.add_rician(rng, synth.predict(tr, prot, o.model >= 2), tr.S0 / 25.0).astype(np.float32)
+    return st, y
+
+
+ENERGY_CASES = [
+    dict(model=1, nfibres=2),
+    dict(model=1, nfibres=3, rician=1, f0=1, ardf0=1),
+    dict(model=2, nfibres=3),
+    dict(model=2, nfibres=3, rician=1, f0=1, ardf0=1),
+    dict(model=3, nfibres=2, rician=1),
+]
+
+
+@pytest.mark.parametrize("kw", ENERGY_CASES, ids=[str(i) for i in range(len(ENERGY_CASES))])
+def test_energy_parity(torch, lib, oracle, kw):
+    """criterion (b): FP32 energies against FP64 on identical states."""
+    o = Options.make(**kw)
+    prot = synth.three_shell(18, 90) if o.model >= 2 else synth.single_shell_64()
+    st, y = _state_sample(o, prot, 512, seed=7)
+    if o.rician:
+        y = oracle.prepare_data(y)
+    lo, pri_o = oracle.energy(o, y, prot.bvecs, prot.bvals, st)
+    d, bv, bl, sd = _dev(torch, y, prot.bvecs, prot.bvals, st)
+    lg, pri_g = lib.energy(o, d, bv, bl, sd)
+    lg, pri_g = lg.cpu().numpy().astype(np.float64), pri_g.cpu().numpy().astype(np.float64)
+    rel = np.abs(lg - lo) / np.abs(lo)
+    assert np.max(rel) < 2e-5, f"max rel err {np.max(rel):.3g}"
+    assert np.max(np.abs(pri_g - pri_o)) < 1e-4
+
+
+def _run_both(torch, lib, oracle, o, y, prot, n_vox, voxel_offset=0):
+    d, bv, bl = _dev(torch, y, prot.bvecs, prot.bvals)
+    p, t, s = lib.fit(o, d, bv, bl)
+    rec_g = lib.mcmc(o, d, bv, bl, p, t, voxel_offset=voxel_offset).cpu().numpy()
+    p64 = p.cpu().numpy().astype(np.float64)
+    t64 = t.cpu().numpy().astype(np.float64)
+    rec_o = oracle.mcmc(o, y, prot.bvecs, prot.bvals, p64, t64, voxel_offset=voxel_offset)
+    return rec_g, rec_o, p64, t64
+
+
+@pytest.mark.parametrize("kw", [dict(model=1, nfibres=2), dict(model=2, nfibres=3, rician=1, f0=1, ardf0=1)],
+                         ids=["m1", "m2_ric_f0"])
+def test_short_chains_track_the_oracle(torch, lib, oracle, kw):
+    """Same random stream: the GPU chain reproduces the FP64 chain step by step (se=1) until an
+    accept decision lands within FP32 rounding of its threshold."""
+    o = Options.make(nburn=0, njumps=30, sampleevery=1, **kw)
+    prot = synth.three_shell(18, 90) if o.model >= 2 else synth.single_shell_64()
+    y, _ = synth.make_volume(64, prot, o.nfibres, o.model >= 2, 25.0, seed=21)
+    if o.rician:
+        y = oracle.prepare_data(y)
+    rec_g, rec_o, _, _ = _run_both(torch, lib, oracle, o, y, prot, 64)
+    rows = [0, 5] + [6 + i for i in range(3 * o.nfibres)]
+    if o.model >= 2:
+        rows.append(3)
+    agree_until = np.zeros(64, int)
+    for v in range(64):
+        n = 0
+        for s in range(o.nsamples):
+            a, b = rec_g[rows, s, v], rec_o[rows, s, v]
+            if np.all(np.abs(a - b) <= 1e-3 * np.abs(b) + 1e-6):
+                n += 1
+            else:
+                break
+        agree_until[v] = n
+    assert np.mean(agree_until >= 10) >= 0.9, agree_until
+    assert np.median(agree_until) >= 20
+
+
+def test_chain_is_deterministic_and_split_invariant(torch, lib):
+    o = Options.make(model=2, nfibres=3, nburn=40, njumps=80, sampleevery=8)
+    prot = synth.three_shell(9, 90)
+    y, _ = synth.make_volume(96, prot, 3, True, 25.0, seed=31)
+    d, bv, bl = _dev(torch, y, prot.bvecs, prot.bvals)
+    p, t, s = lib.fit(o, d, bv, bl)
+    r1 = lib.mcmc(o, d, bv, bl, p, t).cpu().numpy()
+    r2 = lib.mcmc(o, d, bv, bl, p, t).cpu().numpy()
+    assert np.array_equal(r1, r2)
+    a = lib.mcmc(o, d[:40].contiguous(), bv, bl, p[:40].contiguous(), t[:40].contiguous(), voxel_offset=0).cpu().numpy()
+    b = lib.mcmc(o, d[40:].contiguous(), bv, bl, p[40:].contiguous(), t[40:].contiguous(), voxel_offset=40).cpu().numpy()
+    assert np.array_equal(np.concatenate([a, b], axis=2), r1)
+    # a different launch layout runs the same chains
+    lays = [l for l in lib.mcmc_layouts() if l[0] * l[1] >= prot.ndir]
+    if len(lays) > 1:
+        o2 = Options.make(model=2, nfibres=3, nburn=40, njumps=80, sampleevery=8, mcmc_tpv=lays[-1][0],
+                          mcmc_mpl=lays[-1][1])
+        r3 = lib.mcmc(o2, d, bv, bl, p, t).cpu().numpy()
+        assert np.allclose(r3, r1, rtol=1e-4, atol=1e-6) or np.mean(np.isclose(r3, r1, rtol=1e-4)) > 0.9
+
+
+def test_finish_matches_oracle_on_same_records(torch, lib, oracle):
+    o = Options.make(model=2, nfibres=3, nburn=20, njumps=100, sampleevery=5, f0=1, rician=1)
+    prot = synth.three_shell(18, 90)
+    y, _ = synth.make_volume(64, prot, 3, True, 25.0, seed=41)
+    y = oracle.prepare_data(y)
+    d, bv, bl = _dev(torch, y, prot.bvecs, prot.bvals)
+    p, t, s = lib.fit(o, d, bv, bl)
+    rec = lib.mcmc(o, d, bv, bl, p, t)
+    fg = {k: v.cpu().numpy() for k, v in lib.finish(o, rec).items()}
+    fo = oracle.finish(o, rec.cpu().numpy().astype(np.float64))
+    for k in ("th", "ph", "f"):
+        assert np.array_equal(fg[k], fo[k].astype(np.float32)), k
+    for k in ("mean_d", "mean_dstd", "mean_f0", "mean_tau", "mean_S0", "mean_f"):
+        assert np.allclose(fg[k], fo[k], rtol=1e-5, atol=1e-9), k
+    dots = np.abs(np.einsum("kiv,kiv->kv", fg["dyads"], fo["dyads"]))
+    assert np.all(dots > 1 - 1e-5)
+
+
+def _mcse(x):
+    """Monte-Carlo standard error of the mean of a chain (batch means, 5 batches)."""
+    n = x.shape[0] // 5 * 5
+    b = x[:n].reshape(5, n // 5, *x.shape[1:]).mean(1)
+    return b.std(0, ddof=1) / np.sqrt(5)
+
+
+def test_posterior_means_agree_with_oracle_small_config(torch, lib, oracle):
+    """criterion (c) on the CPU-runnable configuration (model 1, 2 fibres, 64 measurements)."""
+    vol = synth.config_small_model1(nvox=128)
+    o = Options.make(model=1, nfibres=2)  # burnin 1000, njumps 1250, sampleevery 25
+    rec_g, rec_o, _, _ = _run_both(torch, lib, oracle, o, vol.data, vol.prot, 128)
+    fg = oracle.finish(o, rec_g.astype(np.float64))
+    fo = oracle.finish(o, rec_o)
+    se = np.sqrt(_mcse(fg["f"][0]) ** 2 + _mcse(fo["f"][0]) ** 2) + 1e-6
+    within = np.abs(fg["mean_f"][0] - fo["mean_f"][0]) <= 2 * se + 1e-3
+    assert within.mean() >= 0.95, within.mean()
+    dots = np.abs(np.einsum("iv,iv->v", fg["dyads"][0], fo["dyads"][0]))
+    assert np.median(np.degrees(np.arccos(np.clip(dots, 0, 1)))) < 1.0
+
+
+def test_host_entry_matches_device_entry(torch, lib):
+    o = Options.make(model=2, nfibres=2, nburn=50, njumps=100, sampleevery=10, rician=1, f0=1)
+    prot = synth.three_shell(9, 90)
+    y, _ = synth.make_volume(50, prot, 2, True, 25.0, seed=51)
+    h = lib.xfibres_host(o, y, prot.bvecs, prot.bvals)
+    d, bv, bl = _dev(torch, y, prot.bvecs, prot.bvals)
+    g = lib.xfibres_dev(o, d, bv, bl)
+    for k in ("th", "ph", "f", "mean_d", "mean_S0", "mean_f", "dyads", "status"):
+        assert np.array_equal(h[k].numpy(), g[k].cpu().numpy()), k
+
+
+def test_gradnonlin_zero_tensor_is_identity(torch, lib):
+    o = Options.make(model=1, nfibres=2, nburn=30, njumps=60, sampleevery=6)
+    prot = synth.single_shell_64()
+    y, _ = synth.make_volume(20, prot, 2, False, 20.0, seed=61)
+    a = lib.xfibres_host(o, y, prot.bvecs, prot.bvals)
+    og = Options.make(model=1, nfibres=2, nburn=30, njumps=60, sampleevery=6, gradnonlin=1)
+    b = lib.xfibres_host(og, y, prot.bvecs, prot.bvals, grad=np.zeros((20, 9), np.float32))
+    for k in ("th", "f", "mean_d"):
+        assert np.allclose(a[k].numpy(), b[k].numpy(), rtol=1e-5, atol=1e-6), k
+
+
+def test_gradnonlin_correction_matches_numpy(torch, lib):
+    prot = synth.single_shell_64()
+    rng = np.random.default_rng(0)
+    grad = rng.normal(0, 0.02, (7, 9)).astype(np.float32)
+    g, bv, bl = _dev(torch, grad, prot.bvecs, prot.bvals)
+    obv, obl = lib.gradnonlin(g, bv, bl)
+    obv, obl = obv.cpu().numpy(), obl.cpu().numpy()
+    for v in range(7):
+        L = grad[v].reshape(3, 3).T  # column-major
+        for m in range(prot.ndir):
+            if prot.bvals[m] > 0:
+                h = (np.eye(3) + L) @ prot.bvecs[:, m]
+                mag = np.linalg.norm(h)
+                assert np.allclose(obv[v, :, m], h / mag, atol=1e-6)
+                assert abs(obl[v, m] - mag * mag * prot.bvals[m]) < 1e-3
+            else:
+                assert obl[v, m] == 0.0
