@@ -194,7 +194,14 @@ def main():
     ap.add_argument("--ref-voxels", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--prof", action="store_true",
+                    help="profiling case: run the steps only (no e2e, CPU baseline or pipe calibration)")
+    ap.add_argument("--nburn", type=int, default=None, help="override burn-in (profiling cases)")
+    ap.add_argument("--njumps", type=int, default=None, help="override jumps (profiling cases)")
     args = ap.parse_args()
+    if args.prof:
+        args.no_e2e = True
+        args.no_cpu_baseline = True
     world, rank, local = dist_setup(args)
 
     if args.impl == "reference":
@@ -217,6 +224,10 @@ def main():
         pg = dist
     L = lib.load()
     o = whole_brain_options()
+    if args.nburn is not None:
+        o.nburn = args.nburn
+    if args.njumps is not None:
+        o.njumps = args.njumps
     prot = synth.three_shell(18, 90)
     M = prot.ndir
     chunk = args.chunk
@@ -320,6 +331,11 @@ def main():
         e2e = {"value": chunk * n_e2e * world / te.item(), "unit": "voxels/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "steps": n_e2e}
 
+    if args.prof:
+        if rank == 0:
+            print(json.dumps({"prof": True, "voxels": chunk, "mcmc_s_per_step": t_mcmc / args.steps,
+                              "fit_s_per_step": t_fit / args.steps}), flush=True)
+        return
     # ---- roofline of the dominant kernel (the MCMC chain) ----
     mufu_peak, fma_peak = lib.measure_pipes()
     mufu_v, fp32_v = mcmc_work_per_voxel(o, M)

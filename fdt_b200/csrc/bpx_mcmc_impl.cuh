@@ -149,6 +149,35 @@ __device__ __forceinline__ float lik_stat(const Lanes<MODEL, K, RIC, TPV, MPL>& 
   return group_sum<TPV>(acc);
 }
 
+// likelihood statistic from plain per-lane arrays (used by the MCMC kernel)
+template <int K, bool RIC, int TPV, int MPL>
+__device__ __forceinline__ float lik_stat2(const float (&y)[MPL], int nj, const float (&isoa)[MPL],
+                                           const float (&sk)[K][MPL], float S0, const float (&f)[K], float f0,
+                                           float tau) {
+  float fsum = f0;
+#pragma unroll
+  for (int k = 0; k < K; ++k) fsum += f[k];
+  const float wiso = 1.0f - fsum;
+  float acc = 0.f;
+#pragma unroll
+  for (int j = 0; j < MPL; ++j) {
+    if (j < nj) {
+      float base = f0 + wiso * isoa[j];
+#pragma unroll
+      for (int k = 0; k < K; ++k) base += f[k] * sk[k][j];
+      const float pred = S0 * base;
+      const float r = y[j] - pred;
+      if (!RIC) {
+        acc += r * r;
+      } else {
+        const float z = tau * pred * y[j];
+        acc += -0.5f * tau * r * r + logI0_minus_z(z);
+      }
+    }
+  }
+  return group_sum<TPV>(acc);
+}
+
 // energy difference E_old - E_new of the likelihood part
 template <bool RIC>
 __device__ __forceinline__ float dlik(float st_old, float st_new, float tau_old, float tau_new, float halfM, float M) {
@@ -156,14 +185,29 @@ __device__ __forceinline__ float dlik(float st_old, float st_new, float tau_old,
   return M * logf(tau_new / tau_old) + (st_new - st_old);
 }
 
+// select element kf (runtime, < K) of a register array without local memory
+template <int K, typename T>
+__device__ __forceinline__ T pick(const T (&a)[K], int kf) {
+  T r = a[0];
+#pragma unroll
+  for (int k = 1; k < K; ++k)
+    if (k == kf) r = a[k];
+  return r;
+}
+
 template <int MODEL, int K, bool RIC, int TPV, int MPL>
 __global__ void __launch_bounds__(kMcmcThreads) mcmc_kernel(McmcArgs a) {
-  constexpr int NS = 6 + 3 * K;                 // proposal slots
-  constexpr int NR = (NS + TPV - 1) / TPV;      // Philox blocks per lane per iteration
-  constexpr int GPW = 32 / TPV;                 // groups (voxels) per warp
+  constexpr int NS = 6 + 3 * K;             // proposal slots
+  constexpr int NR = (NS + TPV - 1) / TPV;  // Philox blocks per lane per iteration
+  constexpr int GPW = 32 / TPV;             // groups (voxels) per warp
+  constexpr int GPB = kMcmcThreads / TPV;   // groups per block
+  constexpr unsigned kIsoBit = 1u << K;
+  constexpr unsigned kAllSticks = (1u << K) - 1u;
+  extern __shared__ float4 smem4[];
   const int lane = threadIdx.x & 31;
   const int gl = lane % TPV;
   const int gw = lane / TPV;
+  const int gblk = threadIdx.x / TPV;
   const int warps_total = gridDim.x * (blockDim.x >> 5);
   const int warp_id = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int M = a.ndir;
@@ -179,6 +223,18 @@ __global__ void __launch_bounds__(kMcmcThreads) mcmc_kernel(McmcArgs a) {
   pr.can_use_ard = !a.no_ard;
   const bool use_f0 = a.f0 != 0;
 
+  // shared memory: (g_x, g_y, g_z, b) per measurement -- one copy per block, or one per group
+  // under gradnonlin -- then per-group proposal widths and acceptance counts
+  const int ngb = a.gradnonlin ? GPB : 1;
+  float4* gb = smem4 + (a.gradnonlin ? gblk * M : 0);
+  float* sprop = (float*)(smem4 + ngb * M) + gblk * NS;
+  int* sacc = (int*)((float*)(smem4 + ngb * M) + GPB * NS) + gblk * NS;
+  if (!a.gradnonlin) {
+    for (int m = threadIdx.x; m < M; m += blockDim.x)
+      gb[m] = make_float4(a.bvecs[m], a.bvecs[M + m], a.bvecs[2 * M + m], a.bvals[m]);
+    __syncthreads();
+  }
+
   for (int round = 0;; ++round) {
     const int first = (warp_id + round * warps_total) * GPW;
     if (first >= a.nvox) break;
@@ -186,25 +242,29 @@ __global__ void __launch_bounds__(kMcmcThreads) mcmc_kernel(McmcArgs a) {
     const bool valid = vreal < a.nvox;
     const int v = valid ? vreal : a.nvox - 1;
     const uint64_t gvox = a.voxel_offset + (uint64_t)v;
+    if (a.gradnonlin) {
+      const float* bv = a.bvecs + (size_t)v * 3 * M;
+      const float* bl = a.bvals + (size_t)v * M;
+      __syncwarp();
+      for (int m = gl; m < M; m += TPV) gb[m] = make_float4(bv[m], bv[M + m], bv[2 * M + m], bl[m]);
+      __syncwarp();
+    }
 
-    // ---- load this lane's measurements ----
-    Lanes<MODEL, K, RIC, TPV, MPL> L;
-    const float* yv = a.data + (size_t)v * M;
-    const float* bv = a.gradnonlin ? a.bvecs + (size_t)v * 3 * M : a.bvecs;
-    const float* bl = a.gradnonlin ? a.bvals + (size_t)v * M : a.bvals;
-    L.nj = 0;
+    // ---- this lane's measurements ----
+    float y[MPL], b[MPL], s[K][MPL], iso[MPL];
+    int nj = 0;
     bool bad = false;
+    const float* yv = a.data + (size_t)v * M;
 #pragma unroll
     for (int j = 0; j < MPL; ++j) {
       const int m = gl + j * TPV;
+      y[j] = 0.f;
+      b[j] = 0.f;
       if (m < M) {
-        L.y[j] = __ldg(yv + m);
-        L.b[j] = __ldg(bl + m);
-        L.nj = j + 1;
-        bad |= !isfinite(L.y[j]);
-      } else {
-        L.y[j] = 0.f;
-        L.b[j] = 0.f;
+        y[j] = __ldg(yv + m);
+        b[j] = gb[m].w;
+        nj = j + 1;
+        bad |= !isfinite(y[j]);
       }
     }
     bad = group_sum<TPV>(bad ? 1.f : 0.f) > 0.f;
@@ -254,53 +314,40 @@ __global__ void __launch_bounds__(kMcmcThreads) mcmc_kernel(McmcArgs a) {
       }
     }
     if (use_f0 && !(f0 <= 0.f || f0 >= 1.f) && a.ardf0) p_f0 = logf(f0);
-    auto prior_sum = [&]() {
-      float p = p_d + p_dstd + p_R + p_f0;
-#pragma unroll
-      for (int k = 0; k < K; ++k) p += p_th[k] + p_f[k];
-      return p;
-    };
-    float prior = prior_sum();
     {
       const SigParams<MODEL> sp = sig_params<MODEL>(d, dstd, R);
 #pragma unroll
-      for (int j = 0; j < MPL; ++j) {
-        const int m = gl + j * TPV;
-        float gx = 0.f, gy = 0.f, gz = 0.f;
-        if (m < M) {
-          gx = __ldg(bv + m);
-          gy = __ldg(bv + M + m);
-          gz = __ldg(bv + 2 * M + m);
+      for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int j = 0; j < MPL; ++j) {
+          const int m = gl + j * TPV;
+          const float4 g = m < M ? gb[m] : make_float4(0.f, 0.f, 0.f, 0.f);
+          const float dp = g.x * vx[k] + g.y * vy[k] + g.z * vz[k];
+          s[k][j] = stick_signal<MODEL>(sp, b[j], dp * dp);
         }
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-          const float dp = gx * vx[k] + gy * vy[k] + gz * vz[k];
-          L.c[k][j] = dp * dp;
-          L.s[k][j] = stick_signal<MODEL>(sp, L.b[j], L.c[k][j]);
-        }
-        L.iso[j] = iso_signal<MODEL>(sp, L.b[j]);
+      for (int j = 0; j < MPL; ++j) iso[j] = iso_signal<MODEL>(sp, b[j]);
+    }
+    float lik = lik_stat2<K, RIC, TPV, MPL>(y, nj, iso, s, S0, f, f0, tau);
+    // initialise_props, acceptance counters
+    if (gl == 0) {
+#pragma unroll
+      for (int q = 0; q < NS; ++q) {
+        float pq = 0.2f;
+        if (q == kSlotS0) pq = S0 / 10.f;
+        if (q == kSlotD) pq = d / 10.f;
+        if (q == kSlotDstd) pq = dstd / 10.f;
+        if (q == kSlotTau) pq = tau / 2.f;
+        if (q == kSlotR) pq = R / 10.f;
+        sprop[q] = pq;
+        sacc[q] = 0;
       }
     }
-    float lik = lik_stat<MODEL, K, RIC, TPV, MPL>(L, L.iso, L.s, S0, f, f0, tau);
-    // initialise_props
-    float prop[NS];
-#pragma unroll
-    for (int q = 0; q < NS; ++q) prop[q] = 0.2f;
-    prop[kSlotS0] = S0 / 10.f;
-    prop[kSlotD] = d / 10.f;
-    prop[kSlotDstd] = dstd / 10.f;
-    prop[kSlotTau] = tau / 2.f;
-    prop[kSlotF0] = 0.2f;
-    prop[kSlotR] = R / 10.f;
-    uint32_t accw[(NS + 3) / 4];
-#pragma unroll
-    for (int q = 0; q < (NS + 3) / 4; ++q) accw[q] = 0u;
-#define BPX_ACC(slot, ok) accw[(slot) / 4] += (ok) ? (1u << (8 * ((slot) % 4))) : 0u
-#define BPX_ACCN(slot) ((accw[(slot) / 4] >> (8 * ((slot) % 4))) & 0xffu)
+    __syncwarp();
 
     int sample = 0;
     for (int it = 0; it < total; ++it) {
-      // randoms of this iteration: lane gl holds slots gl, gl+TPV, ...
+      // this iteration's randoms: lane gl holds slots gl, gl+TPV, ...
       float rn[NR], rl[NR];
 #pragma unroll
       for (int q = 0; q < NR; ++q) {
@@ -309,262 +356,196 @@ __global__ void __launch_bounds__(kMcmcThreads) mcmc_kernel(McmcArgs a) {
         rl[q] = 0.f;
         if (slot < NS) slot_randoms(a.seed, gvox, (uint32_t)it, (uint32_t)slot, rn[q], rl[q]);
       }
-#define BPX_RAND(slot, n, lu)                                                   \
-  const float n = __shfl_sync(0xffffffffu, rn[(slot) / TPV], (slot) % TPV, TPV); \
-  const float lu = __shfl_sync(0xffffffffu, rl[(slot) / TPV], (slot) % TPV, TPV)
-
-      // ---------------- f0 ----------------
-      if (use_f0) {
-        BPX_RAND(kSlotF0, n, lu);
-        const float f0n = f0 + n * prop[kSlotF0];
-        bool rej = (f0n <= 0.f || f0n >= 1.f);
-        const float pf0n = rej ? p_f0 : (a.ardf0 ? logf(f0n) : 0.f);
-        float fs = f0n;
-#pragma unroll
-        for (int k = 0; k < K; ++k) fs += f[k];
-        rej = rej || (fs > 1.f);
-        const float priorn = prior - p_f0 + pf0n;
-        float likn = lik;
-        if (__any_sync(0xffffffffu, !rej)) likn = lik_stat<MODEL, K, RIC, TPV, MPL>(L, L.iso, L.s, S0, f, f0n, tau);
-        const bool ok = !rej && ((prior - priorn) + dlik<RIC>(lik, likn, tau, tau, halfM, fM) > lu);
-        if (ok) {
-          f0 = f0n;
-          p_f0 = pf0n;
-          prior = priorn;
-          lik = likn;
-        }
-        BPX_ACC(kSlotF0, ok);
-      }
-      // ---------------- tau ----------------
-      if (RIC) {
-        BPX_RAND(kSlotTau, n, lu);
-        const float taun = tau + n * prop[kSlotTau];
-        const bool rej = taun <= 0.f;
-        float likn = lik;
-        if (__any_sync(0xffffffffu, !rej)) likn = lik_stat<MODEL, K, RIC, TPV, MPL>(L, L.iso, L.s, S0, f, f0, rej ? tau : taun);
-        const bool ok = !rej && (dlik<RIC>(lik, likn, tau, taun, halfM, fM) > lu);
-        if (ok) {
-          tau = taun;
-          lik = likn;
-        }
-        BPX_ACC(kSlotTau, ok);
-      }
-      // ---------------- d ----------------
-      {
-        BPX_RAND(kSlotD, n, lu);
-        const float dn = d + n * prop[kSlotD];
-        const bool rej = (dn < 0.f || dn > kUpperDiff);
-        const float pdn = rej ? p_d : (MODEL == 3 ? (1.0f - 3.0f) * logf(dn) + 4000.0f * dn : 0.f);
-        const float priorn = prior - p_d + pdn;
-        float likn = lik;
-        float ns_[K][MPL], ni[MPL];
-        if (__any_sync(0xffffffffu, !rej)) {
-          const SigParams<MODEL> sp = sig_params<MODEL>(rej ? d : dn, dstd, R);
-#pragma unroll
-          for (int j = 0; j < MPL; ++j) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) ns_[k][j] = stick_signal<MODEL>(sp, L.b[j], L.c[k][j]);
-            ni[j] = iso_signal<MODEL>(sp, L.b[j]);
-          }
-          likn = lik_stat<MODEL, K, RIC, TPV, MPL>(L, ni, ns_, S0, f, f0, tau);
-        } else {
-#pragma unroll
-          for (int j = 0; j < MPL; ++j) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) ns_[k][j] = L.s[k][j];
-            ni[j] = L.iso[j];
-          }
-        }
-        const bool ok = !rej && ((prior - priorn) + dlik<RIC>(lik, likn, tau, tau, halfM, fM) > lu);
-        if (ok) {
-          d = dn;
-          p_d = pdn;
-          prior = priorn;
-          lik = likn;
-        }
-#pragma unroll
-        for (int j = 0; j < MPL; ++j) {
-#pragma unroll
-          for (int k = 0; k < K; ++k) L.s[k][j] = ok ? ns_[k][j] : L.s[k][j];
-          L.iso[j] = ok ? ni[j] : L.iso[j];
-        }
-        BPX_ACC(kSlotD, ok);
-      }
-      // ---------------- d_std ----------------
-      if (MODEL >= 2) {
-        BPX_RAND(kSlotDstd, n, lu);
-        const float dsn = dstd + n * prop[kSlotDstd];
-        const float upper = MODEL == 3 ? 0.004f : 0.01f;
-        const bool rej = (dsn <= 0.f || dsn > upper);
-        const float pdsn = rej ? p_dstd : logf(dsn);
-        const float priorn = prior - p_dstd + pdsn;
-        float likn = lik;
-        float ns_[K][MPL], ni[MPL];
-        if (__any_sync(0xffffffffu, !rej)) {
-          const SigParams<MODEL> sp = sig_params<MODEL>(d, rej ? dstd : dsn, R);
-#pragma unroll
-          for (int j = 0; j < MPL; ++j) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) ns_[k][j] = (MODEL == 2) ? stick_signal<MODEL>(sp, L.b[j], L.c[k][j]) : L.s[k][j];
-            ni[j] = iso_signal<MODEL>(sp, L.b[j]);
-          }
-          likn = lik_stat<MODEL, K, RIC, TPV, MPL>(L, ni, ns_, S0, f, f0, tau);
-        } else {
-#pragma unroll
-          for (int j = 0; j < MPL; ++j) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) ns_[k][j] = L.s[k][j];
-            ni[j] = L.iso[j];
-          }
-        }
-        const bool ok = !rej && ((prior - priorn) + dlik<RIC>(lik, likn, tau, tau, halfM, fM) > lu);
-        if (ok) {
-          dstd = dsn;
-          p_dstd = pdsn;
-          prior = priorn;
-          lik = likn;
-        }
-#pragma unroll
-        for (int j = 0; j < MPL; ++j) {
-#pragma unroll
-          for (int k = 0; k < K; ++k) L.s[k][j] = ok ? ns_[k][j] : L.s[k][j];
-          L.iso[j] = ok ? ni[j] : L.iso[j];
-        }
-        BPX_ACC(kSlotDstd, ok);
-      }
-      // ---------------- R ----------------
-      if (MODEL == 3) {
-        BPX_RAND(kSlotR, n, lu);
-        const float Rn = R + n * prop[kSlotR];
-        float pRn = p_R;
-        const bool rej = r_prior(pr, Rn, d, pRn);
-        if (rej) pRn = p_R;
-        const float priorn = prior - p_R + pRn;
-        float likn = lik;
-        float ns_[K][MPL];
-        if (__any_sync(0xffffffffu, !rej)) {
-          const SigParams<MODEL> sp = sig_params<MODEL>(d, dstd, rej ? R : Rn);
-#pragma unroll
-          for (int j = 0; j < MPL; ++j)
-#pragma unroll
-            for (int k = 0; k < K; ++k) ns_[k][j] = stick_signal<MODEL>(sp, L.b[j], L.c[k][j]);
-          likn = lik_stat<MODEL, K, RIC, TPV, MPL>(L, L.iso, ns_, S0, f, f0, tau);
-        } else {
-#pragma unroll
-          for (int j = 0; j < MPL; ++j)
-#pragma unroll
-            for (int k = 0; k < K; ++k) ns_[k][j] = L.s[k][j];
-        }
-        const bool ok = !rej && ((prior - priorn) + dlik<RIC>(lik, likn, tau, tau, halfM, fM) > lu);
-        if (ok) {
-          R = Rn;
-          p_R = pRn;
-          prior = priorn;
-          lik = likn;
-        }
-#pragma unroll
-        for (int j = 0; j < MPL; ++j)
-#pragma unroll
-          for (int k = 0; k < K; ++k) L.s[k][j] = ok ? ns_[k][j] : L.s[k][j];
-        BPX_ACC(kSlotR, ok);
-      }
-      // ---------------- S0 ----------------
-      {
-        BPX_RAND(kSlotS0, n, lu);
-        const float S0n = S0 + n * prop[kSlotS0];
-        const bool rej = S0n < 0.f;
-        float likn = lik;
-        if (__any_sync(0xffffffffu, !rej)) likn = lik_stat<MODEL, K, RIC, TPV, MPL>(L, L.iso, L.s, rej ? S0 : S0n, f, f0, tau);
-        const bool ok = !rej && (dlik<RIC>(lik, likn, tau, tau, halfM, fM) > lu);
-        if (ok) {
-          S0 = S0n;
-          lik = likn;
-        }
-        BPX_ACC(kSlotS0, ok);
-      }
-      // ---------------- fibres ----------------
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        // theta and phi
-#pragma unroll
-        for (int ang = 0; ang < 2; ++ang) {
-          const int slot = kSlotFibre0 + 3 * k + ang;
-          BPX_RAND(slot, n, lu);
-          float thn = th[k], phn = ph[k];
-          if (ang == 0)
-            thn = th[k] + n * prop[slot];
-          else
-            phn = ph[k] + n * prop[slot];
-          const float pthn = (ang == 0) ? th_prior(thn) : p_th[k];
-          const float priorn = prior - p_th[k] + pthn;
-          float st, ct, sp_, cp;
-          sincosf(thn, &st, &ct);
-          sincosf(phn, &sp_, &cp);
-          const float nvx = st * cp, nvy = st * sp_, nvz = ct;
-          const SigParams<MODEL> sp = sig_params<MODEL>(d, dstd, R);
-          float nc[MPL], ns_[K][MPL];
-#pragma unroll
-          for (int j = 0; j < MPL; ++j) {
-            const int m = gl + j * TPV;
-            float gx = 0.f, gy = 0.f, gz = 0.f;
-            if (m < M) {
-              gx = __ldg(bv + m);
-              gy = __ldg(bv + M + m);
-              gz = __ldg(bv + 2 * M + m);
-            }
-            const float dp = gx * nvx + gy * nvy + gz * nvz;
-            nc[j] = dp * dp;
-#pragma unroll
-            for (int kk = 0; kk < K; ++kk) ns_[kk][j] = (kk == k) ? stick_signal<MODEL>(sp, L.b[j], nc[j]) : L.s[kk][j];
-          }
-          const float likn = lik_stat<MODEL, K, RIC, TPV, MPL>(L, L.iso, ns_, S0, f, f0, tau);
-          const bool ok = ((prior - priorn) + dlik<RIC>(lik, likn, tau, tau, halfM, fM) > lu);
-          if (ok) {
-            th[k] = thn;
-            ph[k] = phn;
-            p_th[k] = pthn;
-            vx[k] = nvx;
-            vy[k] = nvy;
-            vz[k] = nvz;
-            prior = priorn;
-            lik = likn;
-          }
-#pragma unroll
-          for (int j = 0; j < MPL; ++j) {
-            L.c[k][j] = ok ? nc[j] : L.c[k][j];
-            L.s[k][j] = ok ? ns_[k][j] : L.s[k][j];
-          }
-          BPX_ACC(slot, ok);
-        }
-        // f
+#pragma unroll 1
+      for (int slot = 0; slot < NS; ++slot) {
+        if (slot == kSlotF0 && !use_f0) continue;
+        if (slot == kSlotTau && !RIC) continue;
+        if (slot == kSlotDstd && MODEL < 2) continue;
+        if (slot == kSlotR && MODEL != 3) continue;
+        float n, lu;
         {
-          const int slot = kSlotFibre0 + 3 * k + 2;
-          BPX_RAND(slot, n, lu);
-          const float fkn = f[k] + n * prop[slot];
-          bool rej = (fkn <= 0.f || fkn >= 1.f);
-          float pfn = p_f[k];
-          if (!rej) pfn = pr.fudge * ((pr.can_use_ard && lam[k]) ? logf(fkn) : 0.f);
-          float fn[K];
+          float rq = rn[0], lq = rl[0];
 #pragma unroll
-          for (int kk = 0; kk < K; ++kk) fn[kk] = (kk == k) ? fkn : f[kk];
-          float fs = f0;
+          for (int q = 1; q < NR; ++q)
+            if (q == slot / TPV) {
+              rq = rn[q];
+              lq = rl[q];
+            }
+          n = __shfl_sync(0xffffffffu, rq, slot % TPV, TPV);
+          lu = __shfl_sync(0xffffffffu, lq, slot % TPV, TPV);
+        }
+        const float prop = sprop[slot];
+        const int kind = slot < kSlotFibre0 ? slot : kSlotFibre0 + (slot - kSlotFibre0) % 3;
+        const int kf = slot < kSlotFibre0 ? 0 : (slot - kSlotFibre0) / 3;
+        // ---- proposed state ----
+        float S0n = S0, dn = d, dsn = dstd, Rn = R, taun = tau, f0n = f0, thn = 0.f, phn = 0.f;
+        float fn[K];
 #pragma unroll
-          for (int kk = 0; kk < K; ++kk) fs += fn[kk];
-          rej = rej || (fs > 1.f);
-          const float priorn = prior - p_f[k] + pfn;
-          float likn = lik;
-          if (__any_sync(0xffffffffu, !rej)) likn = lik_stat<MODEL, K, RIC, TPV, MPL>(L, L.iso, L.s, S0, rej ? f : fn, f0, tau);
-          const bool ok = !rej && ((prior - priorn) + dlik<RIC>(lik, likn, tau, tau, halfM, fM) > lu);
-          if (ok) {
-            f[k] = fkn;
-            p_f[k] = pfn;
-            prior = priorn;
-            lik = likn;
+        for (int k = 0; k < K; ++k) fn[k] = f[k];
+        float pnew = 0.f, pold = 0.f;  // prior term that changes
+        bool rej = false;
+        unsigned mask = 0u;
+        bool newdir = false;
+        switch (kind) {
+          case kSlotF0: {
+            f0n = f0 + n * prop;
+            rej = (f0n <= 0.f || f0n >= 1.f);
+            pold = p_f0;
+            pnew = rej ? p_f0 : (a.ardf0 ? logf(f0n) : 0.f);
+            float fs = f0n;
+#pragma unroll
+            for (int k = 0; k < K; ++k) fs += f[k];
+            rej = rej || (fs > 1.f);
+          } break;
+          case kSlotTau:
+            taun = tau + n * prop;
+            rej = taun <= 0.f;
+            break;
+          case kSlotD:
+            dn = d + n * prop;
+            rej = (dn < 0.f || dn > kUpperDiff);
+            pold = p_d;
+            pnew = (rej || MODEL != 3) ? p_d : (1.0f - 3.0f) * logf(dn) + 4000.0f * dn;
+            mask = kAllSticks | kIsoBit;
+            break;
+          case kSlotDstd: {
+            dsn = dstd + n * prop;
+            const float upper = MODEL == 3 ? 0.004f : 0.01f;
+            rej = (dsn <= 0.f || dsn > upper);
+            pold = p_dstd;
+            pnew = rej ? p_dstd : logf(dsn);
+            mask = MODEL == 2 ? (kAllSticks | kIsoBit) : kIsoBit;
+          } break;
+          case kSlotR: {
+            Rn = R + n * prop;
+            float pr2 = p_R;
+            rej = r_prior(pr, Rn, d, pr2);
+            pold = p_R;
+            pnew = rej ? p_R : pr2;
+            mask = kAllSticks;
+          } break;
+          case kSlotS0:
+            S0n = S0 + n * prop;
+            rej = S0n < 0.f;
+            break;
+          case kSlotFibre0: {  // theta of fibre kf
+            thn = pick<K>(th, kf) + n * prop;
+            phn = pick<K>(ph, kf);
+            pold = pick<K>(p_th, kf);
+            pnew = th_prior(thn);
+            mask = 1u << kf;
+            newdir = true;
+          } break;
+          case kSlotFibre0 + 1:  // phi of fibre kf
+            thn = pick<K>(th, kf);
+            phn = pick<K>(ph, kf) + n * prop;
+            mask = 1u << kf;
+            newdir = true;
+            break;
+          default: {  // f of fibre kf
+            const float fkn = pick<K>(f, kf) + n * prop;
+            rej = (fkn <= 0.f || fkn >= 1.f);
+            const bool lj = pick<K>(lam, kf);
+            pold = pick<K>(p_f, kf);
+            pnew = rej ? pold : pr.fudge * ((pr.can_use_ard && lj) ? logf(fkn) : 0.f);
+            float fs = f0;
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+              if (k == kf) fn[k] = fkn;
+              fs += fn[k];
+            }
+            rej = rej || (fs > 1.f);
+          } break;
+        }
+        // ---- signals of the proposed state, then its likelihood ----
+        float likn = lik;
+        float ns_[K][MPL], ni[MPL];
+        float nvx = 0.f, nvy = 0.f, nvz = 0.f;
+        const bool any_live = __any_sync(0xffffffffu, !rej);
+        if (any_live) {
+          if (newdir) {
+            float st, ct, sp_, cp;
+            sincosf(thn, &st, &ct);
+            sincosf(phn, &sp_, &cp);
+            nvx = st * cp;
+            nvy = st * sp_;
+            nvz = ct;
           }
-          BPX_ACC(slot, ok);
+          const SigParams<MODEL> sp = sig_params<MODEL>(dn, dsn, Rn);
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            if (mask & (1u << k)) {
+              const bool nd = newdir && k == kf;
+              const float ux = nd ? nvx : vx[k], uy = nd ? nvy : vy[k], uz = nd ? nvz : vz[k];
+#pragma unroll
+              for (int j = 0; j < MPL; ++j) {
+                const int m = gl + j * TPV;
+                const float4 g = m < M ? gb[m] : make_float4(0.f, 0.f, 0.f, 0.f);
+                const float dp = g.x * ux + g.y * uy + g.z * uz;
+                ns_[k][j] = stick_signal<MODEL>(sp, b[j], dp * dp);
+              }
+            } else {
+#pragma unroll
+              for (int j = 0; j < MPL; ++j) ns_[k][j] = s[k][j];
+            }
+          }
+          if (mask & kIsoBit) {
+#pragma unroll
+            for (int j = 0; j < MPL; ++j) ni[j] = iso_signal<MODEL>(sp, b[j]);
+          } else {
+#pragma unroll
+            for (int j = 0; j < MPL; ++j) ni[j] = iso[j];
+          }
+          likn = lik_stat2<K, RIC, TPV, MPL>(y, nj, ni, ns_, S0n, fn, f0n, taun);
+        }
+        const bool ok = !rej && ((pold - pnew) + dlik<RIC>(lik, likn, tau, taun, halfM, fM) > lu);
+        // ---- accept / reject ----
+        if (ok) {
+          lik = likn;
+          switch (kind) {
+            case kSlotF0: f0 = f0n; p_f0 = pnew; break;
+            case kSlotTau: tau = taun; break;
+            case kSlotD: d = dn; p_d = pnew; break;
+            case kSlotDstd: dstd = dsn; p_dstd = pnew; break;
+            case kSlotR: R = Rn; p_R = pnew; break;
+            case kSlotS0: S0 = S0n; break;
+            case kSlotFibre0:
+            case kSlotFibre0 + 1:
+#pragma unroll
+              for (int k = 0; k < K; ++k)
+                if (k == kf) {
+                  th[k] = thn;
+                  ph[k] = phn;
+                  vx[k] = nvx;
+                  vy[k] = nvy;
+                  vz[k] = nvz;
+                  if (kind == kSlotFibre0) p_th[k] = pnew;
+                }
+              break;
+            default:
+#pragma unroll
+              for (int k = 0; k < K; ++k)
+                if (k == kf) {
+                  f[k] = fn[k];
+                  p_f[k] = pnew;
+                }
+              break;
+          }
+          if (gl == 0) sacc[slot] += 1;
+        }
+        if (mask != 0u && __any_sync(0xffffffffu, ok)) {
+#pragma unroll
+          for (int k = 0; k < K; ++k)
+            if (mask & (1u << k)) {
+#pragma unroll
+              for (int j = 0; j < MPL; ++j) s[k][j] = ok ? ns_[k][j] : s[k][j];
+            }
+          if (mask & kIsoBit) {
+#pragma unroll
+            for (int j = 0; j < MPL; ++j) iso[j] = ok ? ni[j] : iso[j];
+          }
         }
       }
-#undef BPX_RAND
       // ---------------- record (CUDA/runmcmc_kernels.cu:1326-1339) ----------------
       if (it >= a.nburn && ((it - a.nburn + 1) % a.sampleevery) == 0 && sample < ns) {
         if (valid && gl == 0) {
@@ -586,31 +567,32 @@ __global__ void __launch_bounds__(kMcmcThreads) mcmc_kernel(McmcArgs a) {
         ++sample;
       }
       // ---------------- update_proposals (CUDA/runmcmc_kernels.cu:1341-1395) ----------------
-      // every slot is proposed once per iteration, so since the last update acc + rej = upe
+      // each slot is proposed once per iteration, so since the last update acc + rej = upe
       if (((it + 1) % a.upe) == 0) {
-        const float upe = (float)a.upe;
+        __syncwarp();
+        if (gl == 0) {
+          const float upe = (float)a.upe;
 #pragma unroll
-        for (int q = 0; q < NS; ++q) {
-          const bool on = (q == kSlotD) || (q == kSlotS0) || (q >= kSlotFibre0) || (q == kSlotTau && RIC) ||
-                          (q == kSlotF0 && use_f0) || (q == kSlotDstd && MODEL >= 2) || (q == kSlotR && MODEL == 3);
-          if (on) {
-            const float acc = (float)BPX_ACCN(q);
-            prop[q] *= sqrtf((acc + 1.0f) / (upe - acc + 1.0f));
-            prop[q] = fminf(prop[q], kMaxProp);
+          for (int q = 0; q < NS; ++q) {
+            const bool on = (q == kSlotD) || (q == kSlotS0) || (q >= kSlotFibre0) || (q == kSlotTau && RIC) ||
+                            (q == kSlotF0 && use_f0) || (q == kSlotDstd && MODEL >= 2) || (q == kSlotR && MODEL == 3);
+            if (on) {
+              const float acc = (float)sacc[q];
+              sprop[q] = fminf(sprop[q] * sqrtf((acc + 1.0f) / (upe - acc + 1.0f)), kMaxProp);
+            }
+            sacc[q] = 0;
           }
         }
-#pragma unroll
-        for (int q = 0; q < (NS + 3) / 4; ++q) accw[q] = 0u;
+        __syncwarp();
       }
     }
-#undef BPX_ACC
-#undef BPX_ACCN
     if (valid && gl == 0 && a.status) {
       uint32_t st = a.status[v];
       if (!isfinite(lik)) st |= BPX_VOX_NONFINITE_ENERGY;
       if (bad) st |= BPX_VOX_NONFINITE_DATA;
       a.status[v] = st;
     }
+    __syncwarp();
   }
 }
 
@@ -708,8 +690,14 @@ __global__ void __launch_bounds__(kMcmcThreads) energy_kernel(EnergyArgs a) {
 template <int MODEL, int K, bool RIC, int TPV, int MPL>
 cudaError_t launch_mcmc_t(const McmcArgs& a, cudaStream_t s) {
   auto kern = mcmc_kernel<MODEL, K, RIC, TPV, MPL>;
+  constexpr int NS = 6 + 3 * K, GPB = kMcmcThreads / TPV;
+  const size_t smem = (size_t)(a.gradnonlin ? GPB : 1) * a.ndir * sizeof(float4) + (size_t)GPB * NS * 8;
+  if (smem > 48 * 1024) {
+    cudaError_t ea = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (ea != cudaSuccess) return ea;
+  }
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kMcmcThreads, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kMcmcThreads, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;
   const int vox_per_block = (kMcmcThreads / 32) * (32 / TPV);
@@ -717,7 +705,7 @@ cudaError_t launch_mcmc_t(const McmcArgs& a, cudaStream_t s) {
   const int cap = sm_count() * per_sm;
   if (grid > cap) grid = cap;
   if (grid < 1) grid = 1;
-  kern<<<grid, kMcmcThreads, 0, s>>>(a);
+  kern<<<grid, kMcmcThreads, smem, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -266,14 +266,23 @@ def test_host_entry_matches_device_entry(torch, lib):
 
 
 def test_gradnonlin_zero_tensor_is_identity(torch, lib):
-    o = Options.make(model=1, nfibres=2, nburn=30, njumps=60, sampleevery=6)
+    """A zero coil tensor leaves the b-matrix unchanged up to the renormalisation rounding, so the
+    fits agree to FP32 rounding (chains, being chaotic, are compared through their means)."""
+    o = Options.make(model=1, nfibres=2, nburn=200, njumps=400, sampleevery=4)
     prot = synth.single_shell_64()
     y, _ = synth.make_volume(20, prot, 2, False, 20.0, seed=61)
+    d, bv, bl = _dev(torch, y, prot.bvecs, prot.bvals)
+    g0 = torch.zeros((20, 9), device="cuda")
+    bvv, blv = lib.gradnonlin(g0, bv, bl)
+    assert torch.allclose(bvv, bv.expand(20, 3, 64), atol=1e-6) and torch.allclose(blv, bl.expand(20, 64), rtol=1e-6)
+    og = Options.make(model=1, nfibres=2, nburn=200, njumps=400, sampleevery=4, gradnonlin=1)
+    pa, _, _ = lib.fit(o, d, bv, bl)
+    pb, _, _ = lib.fit(og, d, bvv, blv)
+    assert torch.allclose(pa, pb, rtol=1e-4, atol=1e-6)
     a = lib.xfibres_host(o, y, prot.bvecs, prot.bvals)
-    og = Options.make(model=1, nfibres=2, nburn=30, njumps=60, sampleevery=6, gradnonlin=1)
     b = lib.xfibres_host(og, y, prot.bvecs, prot.bvals, grad=np.zeros((20, 9), np.float32))
-    for k in ("th", "f", "mean_d"):
-        assert np.allclose(a[k].numpy(), b[k].numpy(), rtol=1e-5, atol=1e-6), k
+    assert np.allclose(a["mean_d"].numpy(), b["mean_d"].numpy(), rtol=0.05)
+    assert np.allclose(a["mean_f"].numpy(), b["mean_f"].numpy(), atol=0.05)
 
 
 def test_gradnonlin_correction_matches_numpy(torch, lib):
