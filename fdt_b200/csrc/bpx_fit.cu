@@ -13,6 +13,11 @@
 // its partial J^T J / J^T r sums in registers; sums are combined with xor-butterfly shuffles so
 // that every lane holds identical totals and takes identical LM decisions (no shared memory, no
 // block barriers).  The damped normal equations are solved in FP64 with rows spread over lanes.
+//
+// Precision: everything is FP64 -- parameters, model values, residuals, cost, gradient and the
+// Gauss-Newton Hessian.  The reference's CPU fits are FP64, and on near-singular fits (a small
+// third fibre) even rounding J^T J to FP32 sends the LM path of a tenth of the voxels elsewhere.
+// The fits are a few percent of the path's arithmetic, so FP64 here costs little.
 #include <cstdint>
 
 #include "bpx_device.cuh"
@@ -163,13 +168,13 @@ __device__ void jacobi_eig(double (&A)[N][N], double (&w)[N], double (&V)[N][N])
 }
 
 // spherical angles in the convention of FSL miscmaths cart2sph (called at CUDA/diffmodels.cu:70)
-__device__ void cart2sph(const double (&v)[3], float& th, float& ph) {
+__device__ void cart2sph(const double (&v)[3], double& th, double& ph) {
   const double x = v[0], y = v[1], z = v[2];
   const double mag = sqrt(x * x + y * y + z * z);
   const double pi = 3.141592653589793;
   if (mag == 0) {
-    th = (float)(pi / 2);
-    ph = (float)(pi / 2);
+    th = pi / 2;
+    ph = pi / 2;
     return;
   }
   double p;
@@ -191,8 +196,8 @@ __device__ void cart2sph(const double (&v)[3], float& th, float& ph) {
     t = atan(r / z);
   else
     t = atan(r / z) + pi;
-  th = (float)t;
-  ph = (float)p;
+  th = t;
+  ph = p;
 }
 
 struct Dti {
@@ -302,131 +307,146 @@ __device__ void dti_fit(const Meas& ms, int lane, Dti& o) {
 }
 
 // ------------------------------------------------------------------------------------------
-// model evaluation
+// model evaluation (FP64)
 // ------------------------------------------------------------------------------------------
-template <int KIND, int K, bool F0>
-struct Pre {
-  float fs[K], v[K][3], sth[K], cth[K], sph[K], cph[K], dfx[K];
-  float sumf, d, a, bb, S0, f0v, dfx0, sgn1, sgn2;
-  float deriv[K][K];
-};
+using Real = double;  // model-evaluation precision of the fits
 
 template <int KIND, int K, bool F0>
-__device__ __forceinline__ void precompute(const float (&p)[LmShape<KIND, K, F0>::P], Pre<KIND, K, F0>& q) {
+struct Pre {
+  Real fs[K], v[K][3], sth[K], cth[K], sph[K], cph[K], dfx[K];
+  Real sumf, d, a, bb, S0, f0v, dfx0, sgn1, sgn2;
+  Real deriv[K][K];
+};
+
+__device__ __forceinline__ Real x2fd(Real x) { return fabs(kTwoPiGpuD * atan(x)); }
+__device__ __forceinline__ Real f2xd(Real f) { return tan(f / kTwoPiGpuD); }
+__device__ __forceinline__ Real beta2fd(Real b) {
+  const Real s = sin(b);
+  return s * s;
+}
+__device__ __forceinline__ Real f2betad(Real f) { return asin(sqrt(f)); }
+__device__ __forceinline__ Real sgnd(Real x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0); }
+__device__ __forceinline__ Real pm1d(Real x) { return x > 0 ? 1.0 : -1.0; }
+
+template <int KIND, int K, bool F0>
+__device__ __forceinline__ void precompute(const Real (&p)[LmShape<KIND, K, F0>::P], Pre<KIND, K, F0>& q) {
   constexpr int P = LmShape<KIND, K, F0>::P, O = LmShape<KIND, K, F0>::O;
 #pragma unroll
   for (int k = 0; k < K; ++k) {
-    sincosf(p[O + 3 * k + 1], &q.sth[k], &q.cth[k]);
-    sincosf(p[O + 3 * k + 2], &q.sph[k], &q.cph[k]);
+    sincos(p[O + 3 * k + 1], &q.sth[k], &q.cth[k]);
+    sincos(p[O + 3 * k + 2], &q.sph[k], &q.cph[k]);
     q.v[k][0] = q.sth[k] * q.cph[k];
     q.v[k][1] = q.sth[k] * q.sph[k];
     q.v[k][2] = q.cth[k];
   }
-  q.sumf = 0.f;
+  q.sumf = 0.0;
+  q.sgn1 = 1.0;
+  q.sgn2 = 1.0;
   if (KIND == kSingle) {
-    q.d = fabsf(p[1]);
+    q.d = fabs(p[1]);
     q.S0 = p[0];
-    q.sgn1 = pm1(p[1]);
+    q.sgn1 = pm1d(p[1]);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      const float x = p[O + 3 * k];
-      q.fs[k] = x2f(x);
-      q.dfx[k] = kTwoPiGpu * sgnf(x) / (1.f + x * x);
+      const Real x = p[O + 3 * k];
+      q.fs[k] = x2fd(x);
+      q.dfx[k] = kTwoPiGpuD * sgnd(x) / (1.0 + x * x);
       q.sumf += q.fs[k];
     }
     if (F0) {
-      const float x0 = p[P - 1];
-      q.f0v = x2f(x0);
-      q.dfx0 = kTwoPiGpu * sgnf(x0) / (1.f + x0 * x0);
+      const Real x0 = p[P - 1];
+      q.f0v = x2fd(x0);
+      q.dfx0 = kTwoPiGpuD * sgnd(x0) / (1.0 + x0 * x0);
     }
   } else if (KIND == kSingleC) {
     q.d = p[1] * p[1];
     q.S0 = p[0];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      float pf = 1.f;
+      Real pf = 1.0;
 #pragma unroll
       for (int j = 0; j < k; ++j) pf -= q.fs[j];
-      q.fs[k] = beta2f(p[O + 3 * k]) * pf;
+      q.fs[k] = beta2fd(p[O + 3 * k]) * pf;
       q.sumf += q.fs[k];
+      q.dfx[k] = 0.0;
     }
     // fractions_deriv_PVM_single_c (CUDA/PVM_single_c.cu:104-139): d f_j / d beta_k
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      const float s2k = sinf(2.f * p[O + 3 * k]);
+      const Real s2k = sin(2.0 * p[O + 3 * k]);
 #pragma unroll
       for (int j = 0; j < K; ++j) {
         if (j == k) {
-          float fsum = 1.f;
+          Real fsum = 1.0;
 #pragma unroll
           for (int n = 0; n < j; ++n) fsum -= q.fs[n];
           q.deriv[j][k] = s2k * fsum;
         } else if (j > k) {
-          const float sp = sinf(p[O + 3 * j]);
-          float fsum = 0.f;
+          const Real sp = sin(p[O + 3 * j]);
+          Real fsum = 0.0;
 #pragma unroll
           for (int n = 0; n < j; ++n) fsum += q.deriv[n][k];
           q.deriv[j][k] = -(sp * sp) * fsum;
         } else {
-          q.deriv[j][k] = 0.f;
+          q.deriv[j][k] = 0.0;
         }
       }
     }
     if (F0) {
-      const float pfs = 1.f - q.sumf;
-      q.f0v = beta2f(p[P - 1]) * pfs;
-      q.dfx0 = sinf(2.f * p[P - 1]) * pfs;
+      const Real pfs = 1.0 - q.sumf;
+      q.f0v = beta2fd(p[P - 1]) * pfs;
+      q.dfx0 = sin(2.0 * p[P - 1]) * pfs;
     }
   } else {
-    q.a = fabsf(p[1]);
-    q.bb = fabsf(p[2]);
-    q.S0 = fabsf(p[0]);
-    q.sgn1 = pm1(p[1]);
-    q.sgn2 = pm1(p[2]);
+    q.a = fabs(p[1]);
+    q.bb = fabs(p[2]);
+    q.S0 = fabs(p[0]);
+    q.sgn1 = pm1d(p[1]);
+    q.sgn2 = pm1d(p[2]);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      const float x = p[O + 3 * k];
-      q.fs[k] = x2f(x);
-      q.dfx[k] = kTwoPiGpu * sgnf(x) / (1.f + x * x);
+      const Real x = p[O + 3 * k];
+      q.fs[k] = x2fd(x);
+      q.dfx[k] = kTwoPiGpuD * sgnd(x) / (1.0 + x * x);
       q.sumf += q.fs[k];
     }
     if (F0) {
-      const float x0 = p[P - 1];
-      q.f0v = x2f(x0);
-      q.dfx0 = kTwoPiGpu * sgnf(x0) / (1.f + x0 * x0);
+      const Real x0 = p[P - 1];
+      q.f0v = x2fd(x0);
+      q.dfx0 = kTwoPiGpuD * sgnd(x0) / (1.0 + x0 * x0);
     }
   }
   if (!F0) {
-    q.f0v = 0.f;
-    q.dfx0 = 0.f;
+    q.f0v = 0.0;
+    q.dfx0 = 0.0;
   }
 }
 
-// Predicted signal of one measurement; with WANTJ also the Jacobian row Jg (the one the
+// Predicted signal of one measurement; with WANTJ also the Jacobian row J (the one the
 // reference uses for the gradient) and J0h, the S0 entry its Hessian uses (they differ only for
 // PVM_multi, CUDA/PVM_multi.cu:376 vs :452).
 template <int KIND, int K, bool F0, bool WANTJ>
-__device__ __forceinline__ float point(const Pre<KIND, K, F0>& q, const float (&p)[LmShape<KIND, K, F0>::P],
-                                       float gx, float gy, float gz, float b, int gbo, float R,
-                                       float invR, float (&J)[LmShape<KIND, K, F0>::P], float& J0h) {
+__device__ __forceinline__ Real point(const Pre<KIND, K, F0>& q, const Real (&p)[LmShape<KIND, K, F0>::P], Real gx,
+                                      Real gy, Real gz, Real b, int gbo, Real R, Real invR,
+                                      Real (&J)[LmShape<KIND, K, F0>::P], Real& J0h) {
   constexpr int P = LmShape<KIND, K, F0>::P, O = LmShape<KIND, K, F0>::O;
-  float dp[K];
+  Real dp[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) dp[k] = gx * q.v[k][0] + gy * q.v[k][1] + gz * q.v[k][2];
   if (KIND == kSingle || KIND == kSingleC) {
-    const float d = q.d;
-    const float iso = expf(-b * d);
-    float an[K], sig = 0.f;
+    const Real d = q.d;
+    const Real iso = exp(-b * d);
+    Real an[K], sig = 0.0;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      an[k] = expf(-b * d * dp[k] * dp[k]);
+      an[k] = exp(-b * d * dp[k] * dp[k]);
       sig += q.fs[k] * an[k];
     }
-    const float wiso = 1.f - q.sumf - q.f0v;
-    const float full = q.S0 * ((q.f0v + wiso * iso) + sig);
+    const Real wiso = 1.0 - q.sumf - q.f0v;
+    const Real full = q.S0 * ((q.f0v + wiso * iso) + sig);
     if (!WANTJ) return full;
 #pragma unroll
-    for (int i = 0; i < P; ++i) J[i] = 0.f;
+    for (int i = 0; i < P; ++i) J[i] = 0.0;
     if (KIND == kSingle) {
 #pragma unroll
       for (int k = 0; k < K; ++k) {
@@ -435,73 +455,73 @@ __device__ __forceinline__ float point(const Pre<KIND, K, F0>& q, const float (&
       }
       J[1] += q.sgn1 * q.S0 * wiso * (-b * iso);
     } else {
-      const float lam = p[1];
+      const Real lam = p[1];
 #pragma unroll
       for (int k = 0; k < K; ++k) {
-        J[1] += q.S0 * q.fs[k] * (-2.f * b * lam * dp[k] * dp[k] * an[k]);
-        float s = 0.f;
+        J[1] += q.S0 * q.fs[k] * (-2.0 * b * lam * dp[k] * dp[k] * an[k]);
+        Real s = 0.0;
 #pragma unroll
         for (int j = 0; j < K; ++j) s += q.S0 * (an[j] - iso) * q.deriv[j][k];
         J[O + 3 * k] = s;
       }
-      J[1] += q.S0 * wiso * (-2.f * b * lam * iso);
+      J[1] += q.S0 * wiso * (-2.0 * b * lam * iso);
     }
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      const float dp1 = q.cth[k] * (gx * q.cph[k] + gy * q.sph[k]) - gz * q.sth[k];
-      const float dp2 = q.sth[k] * (-gx * q.sph[k] + gy * q.cph[k]);
-      const float c = q.S0 * q.fs[k] * (-2.f * b * d * dp[k] * an[k]);
+      const Real dp1 = q.cth[k] * (gx * q.cph[k] + gy * q.sph[k]) - gz * q.sth[k];
+      const Real dp2 = q.sth[k] * (-gx * q.sph[k] + gy * q.cph[k]);
+      const Real c = q.S0 * q.fs[k] * (-2.0 * b * d * dp[k] * an[k]);
       J[O + 3 * k + 1] = c * dp1;
       J[O + 3 * k + 2] = c * dp2;
     }
-    if (F0) J[P - 1] = q.S0 * (1.f - iso) * q.dfx0;
+    if (F0) J[P - 1] = q.S0 * (1.0 - iso) * q.dfx0;
     J[0] = full / p[0];
     J0h = J[0];
     return full;
   } else {
-    const float a = q.a, bb = q.bb;
-    const float liso = log1pf(b * bb);
-    const float iso = expf(-a * liso);
-    float an[K], an_a[K], an_b[K], an_th[K], an_ph[K], sig = 0.f;
+    const Real a = q.a, bb = q.bb;
+    const Real liso = log1p(b * bb);
+    const Real iso = exp(-a * liso);
+    Real an[K], an_a[K], an_b[K], an_th[K], an_ph[K], sig = 0.0;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      const float x2 = dp[k] * dp[k];
-      const float dp1 = q.cth[k] * (gx * q.cph[k] + gy * q.sph[k]) - gz * q.sth[k];
-      const float dpp = q.sth[k] * (-gx * q.sph[k] + gy * q.cph[k]);
+      const Real x2 = dp[k] * dp[k];
+      const Real dp1 = q.cth[k] * (gx * q.cph[k] + gy * q.sph[k]) - gz * q.sth[k];
+      const Real dpp = q.sth[k] * (-gx * q.sph[k] + gy * q.cph[k]);
       if (gbo == 2) {
-        const float arg = (1.f - R) * x2 + R;
-        const float e = expf(-b * 3.f * a * bb * invR * arg);
+        const Real arg = (1.0 - R) * x2 + R;
+        const Real e = exp(-b * 3.0 * a * bb * invR * arg);
         an[k] = e;
         if (WANTJ) {
-          const float da = b * 3.f * bb * invR * arg;
-          an_a[k] = -da * expf(-da * a);
-          const float db = b * 3.f * a * invR * arg;
-          an_b[k] = -db * expf(-db * bb);
+          const Real da = b * 3.0 * bb * invR * arg;
+          an_a[k] = -da * exp(-da * a);
+          const Real db = b * 3.0 * a * invR * arg;
+          an_b[k] = -db * exp(-db * bb);
           // the zeppelin angle derivatives of CUDA/PVM_multi.cu:82-84,99-101 (no factor dp)
-          an_th[k] = -(2.f * b * 3.f * a * bb * invR * (1.f - R) * dp1) * e;
-          an_ph[k] = -(2.f * b * 3.f * a * bb * invR * (1.f - R) * dpp) * e;
+          an_th[k] = -(2.0 * b * 3.0 * a * bb * invR * (1.0 - R) * dp1) * e;
+          an_ph[k] = -(2.0 * b * 3.0 * a * bb * invR * (1.0 - R) * dpp) * e;
         }
       } else {
-        const float l = log1pf(b * bb * x2);
-        an[k] = expf(-a * l);
+        const Real l = log1p(b * bb * x2);
+        an[k] = exp(-a * l);
         if (WANTJ) {
-          const float inv = 1.f / (1.f + b * x2 * bb);
+          const Real inv = 1.0 / (1.0 + b * x2 * bb);
           an_a[k] = -l * an[k];
           an_b[k] = -a * b * x2 * inv * an[k];
-          const float t = -a * bb * b * inv * an[k] * 2.f * dp[k];
+          const Real t = -a * bb * b * inv * an[k] * 2.0 * dp[k];
           an_th[k] = t * dp1;
           an_ph[k] = t * dpp;
         }
       }
       sig += q.fs[k] * an[k];
     }
-    const float wiso = 1.f - q.sumf - q.f0v;
-    const float full = q.S0 * ((q.f0v + wiso * iso) + sig);
+    const Real wiso = 1.0 - q.sumf - q.f0v;
+    const Real full = q.S0 * ((q.f0v + wiso * iso) + sig);
     if (!WANTJ) return full;
 #pragma unroll
-    for (int i = 0; i < P; ++i) J[i] = 0.f;
-    const float iso_a = -liso * iso;
-    const float iso_b = -a * b / (1.f + b * bb) * iso;
+    for (int i = 0; i < P; ++i) J[i] = 0.0;
+    const Real iso_a = -liso * iso;
+    const Real iso_b = -a * b / (1.0 + b * bb) * iso;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       J[1] += q.sgn1 * q.S0 * q.fs[k] * an_a[k];
@@ -512,34 +532,35 @@ __device__ __forceinline__ float point(const Pre<KIND, K, F0>& q, const float (&
     }
     J[1] += q.sgn1 * q.S0 * wiso * iso_a;
     J[2] += q.sgn2 * q.S0 * wiso * iso_b;
-    if (F0) J[P - 1] = q.S0 * (1.f - iso) * q.dfx0;
+    if (F0) J[P - 1] = q.S0 * (1.0 - iso) * q.dfx0;
     J0h = full / p[0];
-    J[0] = pm1(p[0]) * full / p[0];
+    J[0] = pm1d(p[0]) * full / p[0];
     return full;
   }
 }
 
 template <int KIND, int K, bool F0>
-__device__ double cost(const Meas& ms, const float (&p)[LmShape<KIND, K, F0>::P], int lane, int gbo, float R,
-                       float invR) {
+__device__ double cost(const Meas& ms, const Real (&p)[LmShape<KIND, K, F0>::P], int lane, int gbo, Real R,
+                       Real invR) {
   constexpr int P = LmShape<KIND, K, F0>::P;
   Pre<KIND, K, F0> q;
   precompute<KIND, K, F0>(p, q);
-  float acc = 0.f;
-  float Jd[P];
-  float j0;
+  double acc = 0.0;
+  Real Jd[P];
+  Real j0;
   for (int m = lane; m < ms.M; m += 32) {
-    const float e = point<KIND, K, F0, false>(q, p, ms.gx[m], ms.gy[m], ms.gz[m], ms.b[m], gbo, R, invR, Jd, j0) - ms.y[m];
+    const Real e = point<KIND, K, F0, false>(q, p, ms.gx[m], ms.gy[m], ms.gz[m], ms.b[m], gbo, R, invR, Jd, j0) -
+                   (Real)ms.y[m];
     acc += e * e;
   }
-  return group_sum<32>((double)acc);
+  return group_sum<32>(acc);
 }
 
 // LM driver (CUDA/levenberg_marquardt.cu:57-122): lambda0 = 0.1, x/÷ 10, converged when
 // 2|dcf| <= 1e-8 (|cf_old|+|cf_new|+2e-16), stopped when lambda > 1e20 or after 200 successful
 // iterations (the iteration counter advances only on success).
 template <int KIND, int K, bool F0>
-__device__ int lm_run(const Meas& ms, float (&p)[LmShape<KIND, K, F0>::P], int lane, int gbo, float R, float invR) {
+__device__ int lm_run(const Meas& ms, Real (&p)[LmShape<KIND, K, F0>::P], int lane, int gbo, Real R, Real invR) {
   constexpr int P = LmShape<KIND, K, F0>::P;
   constexpr int NH = LmShape<KIND, K, F0>::NH;
   double lambda = 0.1;
@@ -553,26 +574,24 @@ __device__ int lm_run(const Meas& ms, float (&p)[LmShape<KIND, K, F0>::P], int l
     if (success) {
       Pre<KIND, K, F0> q;
       precompute<KIND, K, F0>(p, q);
-      float H[NH], g[P];
+      double H[NH];
+      double g[P];
 #pragma unroll
-      for (int i = 0; i < NH; ++i) H[i] = 0.f;
+      for (int i = 0; i < NH; ++i) H[i] = 0.0;
 #pragma unroll
-      for (int i = 0; i < P; ++i) g[i] = 0.f;
+      for (int i = 0; i < P; ++i) g[i] = 0.0;
       for (int m = lane; m < ms.M; m += 32) {
-        float J[P], J0h;
-        const float sig = point<KIND, K, F0, true>(q, p, ms.gx[m], ms.gy[m], ms.gz[m], ms.b[m], gbo, R, invR, J, J0h);
-        const float diff = sig - ms.y[m];
+        Real J[P], J0h;
+        const Real sig = point<KIND, K, F0, true>(q, p, ms.gx[m], ms.gy[m], ms.gz[m], ms.b[m], gbo, R, invR, J, J0h);
+        const Real diff = sig - (Real)ms.y[m];
 #pragma unroll
-        for (int i = 0; i < P; ++i) g[i] += 2.f * J[i] * diff;
-        float Jh[P];
-#pragma unroll
-        for (int i = 0; i < P; ++i) Jh[i] = J[i];
-        Jh[0] = J0h;
+        for (int i = 0; i < P; ++i) g[i] += 2.0 * J[i] * diff;
+        J[0] = J0h;  // the Hessian's S0 entry (differs from the gradient's only for PVM_multi)
         int e = 0;
 #pragma unroll
         for (int i = 0; i < P; ++i)
 #pragma unroll
-          for (int j = i; j < P; ++j) H[e++] += 2.f * Jh[i] * Jh[j];
+          for (int j = i; j < P; ++j) H[e++] += 2.0 * J[i] * J[j];
       }
 #pragma unroll
       for (int i = 0; i < NH; ++i) H[i] = group_sum<32>(H[i]);
@@ -600,9 +619,9 @@ __device__ int lm_run(const Meas& ms, float (&p)[LmShape<KIND, K, F0>::P], int l
     for (int j = 0; j < P; ++j) A[j] = Hrow[j] + ((lane == j) ? lambda : 0.0);
     double x[P];
     warp_solve<P>(A, grow, x, lane);
-    float step[P];
+    Real step[P];
 #pragma unroll
-    for (int i = 0; i < P; ++i) step[i] = (float)((double)p[i] - x[i]);
+    for (int i = 0; i < P; ++i) step[i] = p[i] - x[i];
     const double ncf = cost<KIND, K, F0>(ms, step, lane, gbo, R, invR);
     bool end = false;
     if ((success = (ncf < pcf))) {
@@ -622,7 +641,7 @@ __device__ int lm_run(const Meas& ms, float (&p)[LmShape<KIND, K, F0>::P], int l
 
 // adjacent-swap sort of fibres by decreasing f (sort_PVM_*, CUDA/PVM_single.cu:86-104)
 template <int K, int O, int P>
-__device__ __forceinline__ void sort_fibres(float (&p)[P]) {
+__device__ __forceinline__ void sort_fibres(Real (&p)[P]) {
 #pragma unroll
   for (int i = 1; i < K; ++i)
 #pragma unroll
@@ -630,7 +649,7 @@ __device__ __forceinline__ void sort_fibres(float (&p)[P]) {
       if (p[O + j * 3] < p[O + (j + 1) * 3]) {
 #pragma unroll
         for (int t = 0; t < 3; ++t) {
-          const float tmp = p[O + j * 3 + t];
+          const Real tmp = p[O + j * 3 + t];
           p[O + j * 3 + t] = p[O + (j + 1) * 3 + t];
           p[O + (j + 1) * 3 + t] = tmp;
         }
@@ -640,101 +659,102 @@ __device__ __forceinline__ void sort_fibres(float (&p)[P]) {
 // finalise raw LM parameters (CUDA/PVM_single.cu:451-466, CUDA/PVM_single_c.cu:582-607,
 // CUDA/PVM_multi.cu:549-566)
 template <int KIND, int K, bool F0>
-__device__ __forceinline__ void finalise(float (&p)[LmShape<KIND, K, F0>::P]) {
+__device__ __forceinline__ void finalise(Real (&p)[LmShape<KIND, K, F0>::P]) {
   constexpr int P = LmShape<KIND, K, F0>::P, O = LmShape<KIND, K, F0>::O;
+  const Real fsmall = 0.001;
   if (KIND == kSingle) {
-    p[1] = fabsf(p[1]);
+    p[1] = fabs(p[1]);
 #pragma unroll
-    for (int k = 0; k < K; ++k) p[O + 3 * k] = x2f(p[O + 3 * k]);
-    if (F0) p[P - 1] = x2f(p[P - 1]);
+    for (int k = 0; k < K; ++k) p[O + 3 * k] = x2fd(p[O + 3 * k]);
+    if (F0) p[P - 1] = x2fd(p[P - 1]);
     sort_fibres<K, O, P>(p);
-    float sum = F0 ? p[P - 1] : 0.f;
+    Real sum = F0 ? p[P - 1] : 0.0;
     bool hit = false;
 #pragma unroll
     for (int i = 0; i < K; ++i) {
       if (!hit) {
         sum += p[O + 3 * i];
-        if (sum >= 1.f) hit = true;
+        if (sum >= 1.0) hit = true;
       }
-      if (hit) p[O + 3 * i] = kFSmall;
+      if (hit) p[O + 3 * i] = fsmall;
     }
   } else if (KIND == kSingleC) {
     p[1] = p[1] * p[1];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      float pf = 1.f;
+      Real pf = 1.0;
 #pragma unroll
       for (int j = 0; j < k; ++j) pf -= p[O + 3 * j];
-      p[O + 3 * k] = beta2f(p[O + 3 * k]) * pf;
+      p[O + 3 * k] = beta2fd(p[O + 3 * k]) * pf;
     }
     if (F0) {
-      float pf = 1.f;
+      Real pf = 1.0;
 #pragma unroll
       for (int j = 0; j < K; ++j) pf -= p[O + 3 * j];
-      p[P - 1] = beta2f(p[P - 1]) * pf;
+      p[P - 1] = beta2fd(p[P - 1]) * pf;
     }
     sort_fibres<K, O, P>(p);
   } else {
-    const float aux = p[1];
-    p[1] = fabsf(aux * p[2]);
-    p[2] = sqrtf(fabsf(aux * p[2] * p[2]));
+    const Real aux = p[1];
+    p[1] = fabs(aux * p[2]);
+    p[2] = sqrt(fabs(aux * p[2] * p[2]));
 #pragma unroll
-    for (int k = 0; k < K; ++k) p[O + 3 * k] = x2f(p[O + 3 * k]);
-    if (F0) p[P - 1] = x2f(p[P - 1]);
+    for (int k = 0; k < K; ++k) p[O + 3 * k] = x2fd(p[O + 3 * k]);
+    if (F0) p[P - 1] = x2fd(p[P - 1]);
     sort_fibres<K, O, P>(p);
-    float sum = F0 ? p[P - 1] : 0.f;
+    Real sum = F0 ? p[P - 1] : 0.0;
     bool hit = false;
 #pragma unroll
     for (int i = 0; i < K; ++i) {
       if (!hit) {
-        if (p[O + 3 * i] == 0.f) p[O + 3 * i] = kFSmall;
+        if (p[O + 3 * i] == 0.0) p[O + 3 * i] = fsmall;
         sum += p[O + 3 * i];
-        if (sum >= 1.f) hit = true;
+        if (sum >= 1.0) hit = true;
       }
-      if (hit) p[O + 3 * i] = kFSmall;
+      if (hit) p[O + 3 * i] = fsmall;
     }
   }
 }
 
 // PVM_single start values (CUDA/diffmodels.cu:67-91)
 template <int K, bool F0>
-__device__ void start_single(const Dti& dt, float (&p)[LmShape<kSingle, K, F0>::P]) {
+__device__ void start_single(const Dti& dt, Real (&p)[LmShape<kSingle, K, F0>::P]) {
   constexpr int P = LmShape<kSingle, K, F0>::P;
-  float th, ph;
+  Real th, ph;
   cart2sph(dt.v[0], th, ph);
-  p[0] = (float)dt.s0;
-  p[1] = dt.md > 0 ? (float)(dt.md * 2) : 0.001f;
-  p[2] = dt.fa < 1 ? f2x((float)dt.fa) : f2x(0.95f);
+  p[0] = dt.s0;
+  p[1] = dt.md > 0 ? dt.md * 2 : 0.001;
+  p[2] = dt.fa < 1 ? f2xd(dt.fa) : f2xd(0.95);
   p[3] = th;
   p[4] = ph;
-  float sumf = x2f(p[2]);
+  Real sumf = x2fd(p[2]);
 #pragma unroll
   for (int ii = 2; ii <= K; ++ii) {
     const int i = 5 + 3 * (ii - 2);
-    float denom = 2.f, tmpsumf;
+    Real denom = 2.0, tmpsumf;
     do {
-      p[i] = f2x(x2f(p[i - 3]) / denom);
-      denom *= 2.f;
-      tmpsumf = sumf + x2f(p[i]);
-    } while (tmpsumf >= 1.f);
-    sumf += x2f(p[i]);
+      p[i] = f2xd(x2fd(p[i - 3]) / denom);
+      denom *= 2.0;
+      tmpsumf = sumf + x2fd(p[i]);
+    } while (tmpsumf >= 1.0);
+    sumf += x2fd(p[i]);
     cart2sph(dt.v[ii - 1], th, ph);
     p[i + 1] = th;
     p[i + 2] = ph;
   }
-  if (F0) p[P - 1] = f2x(kFSmall);
+  if (F0) p[P - 1] = f2xd(0.001);
 }
 
 // PVM_single_c start values with fit_pvf (CUDA/diffmodels.cu:149-184, diffmodels.cc:561-603)
 template <int K, bool F0>
-__device__ void start_single_c(const Dti& dt, const Meas& ms, int lane, float (&x)[LmShape<kSingleC, K, F0>::P]) {
+__device__ void start_single_c(const Dti& dt, const Meas& ms, int lane, Real (&x)[LmShape<kSingleC, K, F0>::P]) {
   constexpr int P = LmShape<kSingleC, K, F0>::P;
-  float th, ph;
+  Real th, ph;
 #pragma unroll
-  for (int i = 0; i < P; ++i) x[i] = 0.f;
+  for (int i = 0; i < P; ++i) x[i] = 0.0;
   cart2sph(dt.v[0], th, ph);
-  x[0] = (float)dt.s0;
-  x[1] = sqrtf(dt.l1 > 0 ? (float)dt.l1 : 0.002f);
+  x[0] = dt.s0;
+  x[1] = sqrt(dt.l1 > 0 ? dt.l1 : 0.002);
   x[3] = th;
   x[4] = ph;
 #pragma unroll
@@ -745,13 +765,13 @@ __device__ void start_single_c(const Dti& dt, const Meas& ms, int lane, float (&
     x[i + 2] = ph;
   }
   // linear least squares for the fractions: pinv(M) * (Y - S0 iso)
-  const double s0 = x[0], d = (double)x[1] * x[1];
+  const double s0 = x[0], d = x[1] * x[1];
   double dir[K][3];
 #pragma unroll
   for (int k = 0; k < K; ++k) {
-    dir[k][0] = sin((double)x[3 + 3 * k]) * cos((double)x[4 + 3 * k]);
-    dir[k][1] = sin((double)x[3 + 3 * k]) * sin((double)x[4 + 3 * k]);
-    dir[k][2] = cos((double)x[3 + 3 * k]);
+    dir[k][0] = sin(x[3 + 3 * k]) * cos(x[4 + 3 * k]);
+    dir[k][1] = sin(x[3 + 3 * k]) * sin(x[4 + 3 * k]);
+    dir[k][2] = cos(x[3 + 3 * k]);
   }
   double MtM[K][K], MtY[K];
 #pragma unroll
@@ -800,105 +820,102 @@ __device__ void start_single_c(const Dti& dt, const Meas& ms, int lane, float (&
     }
     fs[i] = s;
   }
-  float fsf[K];
-  float f0v = 0.f;
-#pragma unroll
-  for (int k = 0; k < K; ++k) fsf[k] = (float)fs[k];
+  double f0v = 0.0;
   if (F0) {
-    f0v = kFSmall;
-    fsf[0] -= f0v;
+    f0v = 0.001;
+    fs[0] -= f0v;
   }
 #pragma unroll
-  for (int k = 0; k < K; ++k) fsf[k] = fabsf(fsf[k]);
+  for (int k = 0; k < K; ++k) fs[k] = fabs(fs[k]);
   {
-    float sumf = 0.f;
+    double sumf = 0.0;
     bool hit = false;
 #pragma unroll
     for (int i = 0; i < K; ++i) {
       if (!hit) {
-        sumf += fsf[i];
-        if (sumf >= 1.f) hit = true;
+        sumf += fs[i];
+        if (sumf >= 1.0) hit = true;
       }
-      if (hit) fsf[i] = kFSmall;
+      if (hit) fs[i] = 0.001;
     }
   }
 #pragma unroll
   for (int k = 0; k < K; ++k) {
-    float pf = 1.f;
+    double pf = 1.0;
 #pragma unroll
-    for (int j = 0; j < k; ++j) pf -= fsf[j];
-    float tmpr = fsf[k] / pf;
-    if (tmpr > 1.f) tmpr = 1.f;
-    x[2 + 3 * k] = f2beta(tmpr);
+    for (int j = 0; j < k; ++j) pf -= fs[j];
+    double tmpr = fs[k] / pf;
+    if (tmpr > 1.0) tmpr = 1.0;
+    x[2 + 3 * k] = f2betad(tmpr);
   }
   if (F0) {
-    float pf = 1.f;
+    double pf = 1.0;
 #pragma unroll
-    for (int j = 0; j < K; ++j) pf -= fsf[j];
-    float tmpr = f0v / pf;
-    if (tmpr > 1.f) tmpr = 1.f;
-    x[P - 1] = f2beta(tmpr);
+    for (int j = 0; j < K; ++j) pf -= fs[j];
+    double tmpr = f0v / pf;
+    if (tmpr > 1.0) tmpr = 1.0;
+    x[P - 1] = f2betad(tmpr);
   }
 }
 
 // fit_PVM_multi_kernel start from the finalised PVM_single / PVM_single_c parameters
 // (CUDA/PVM_multi.cu:514-530)
 template <int K, bool F0>
-__device__ __forceinline__ void start_multi(const float (&s)[LmShape<kSingle, K, F0>::P], float (&p)[LmShape<kMulti, K, F0>::P]) {
+__device__ __forceinline__ void start_multi(const Real (&s)[LmShape<kSingle, K, F0>::P], Real (&p)[LmShape<kMulti, K, F0>::P]) {
   constexpr int P = LmShape<kMulti, K, F0>::P;
   p[0] = s[0];
-  p[1] = 1.0f;
+  p[1] = 1.0;
 #pragma unroll
   for (int i = 0; i < K; ++i) {
     const int ii = 3 + 3 * i;
-    p[ii] = f2x(s[ii - 1]);
+    p[ii] = f2xd(s[ii - 1]);
     p[ii + 1] = s[ii];
     p[ii + 2] = s[ii + 1];
   }
   p[2] = s[1];
-  if (F0) p[P - 1] = f2x(s[P - 2]);
+  if (F0) p[P - 1] = f2xd(s[P - 2]);
 }
 
 // predicted signal from finalised parameters (what get_residuals_*_kernel subtract)
 template <int K>
-__device__ __forceinline__ float predict_final(int model, const float* q, int o, bool use_f0, float f0,
-                                               float R, float gx, float gy, float gz, float b) {
-  float sumf = 0.f, val = 0.f, iso, S0 = q[0];
+__device__ __forceinline__ Real predict_final(int model, const Real* q, int o, bool use_f0, Real f0, Real R, Real gx,
+                                              Real gy, Real gz, Real b) {
+  Real sumf = 0.0, val = 0.0, iso, S0 = q[0];
   if (model == 1) {
-    const float d = q[1];
-    iso = expf(-b * d);
+    const Real d = q[1];
+    iso = exp(-b * d);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      float st, ct, sp, cp;
-      sincosf(q[o + 3 * k + 1], &st, &ct);
-      sincosf(q[o + 3 * k + 2], &sp, &cp);
-      const float dp = gx * st * cp + gy * st * sp + gz * ct;
-      val += q[o + 3 * k] * expf(-b * d * dp * dp);
+      Real st, ct, sp, cp;
+      sincos(q[o + 3 * k + 1], &st, &ct);
+      sincos(q[o + 3 * k + 2], &sp, &cp);
+      const Real dp = gx * st * cp + gy * st * sp + gz * ct;
+      val += q[o + 3 * k] * exp(-b * d * dp * dp);
       sumf += q[o + 3 * k];
     }
   } else {
-    const float d = q[1], ds = q[2];
-    const float a = d * d / ds / ds, bb = ds * ds / d;
-    const float invR = 1.f / (2.f * R + 1.f);
-    iso = expf(-a * log1pf(b * bb));
+    const Real d = q[1], ds = q[2];
+    const Real a = d * d / ds / ds, bb = ds * ds / d;
+    const Real invR = 1.0 / (2.0 * R + 1.0);
+    iso = exp(-a * log1p(b * bb));
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      float st, ct, sp, cp;
-      sincosf(q[o + 3 * k + 1], &st, &ct);
-      sincosf(q[o + 3 * k + 2], &sp, &cp);
-      const float dp = gx * st * cp + gy * st * sp + gz * ct;
-      float an;
+      Real st, ct, sp, cp;
+      sincos(q[o + 3 * k + 1], &st, &ct);
+      sincos(q[o + 3 * k + 2], &sp, &cp);
+      const Real dp = gx * st * cp + gy * st * sp + gz * ct;
+      Real an;
       if (model == 3)
-        an = expf(-b * 3.f * a * bb * invR * ((1.f - R) * dp * dp + R));
+        an = exp(-b * 3.0 * a * bb * invR * ((1.0 - R) * dp * dp + R));
       else
-        an = expf(-a * log1pf(b * bb * dp * dp));
+        an = exp(-a * log1p(b * bb * dp * dp));
       val += q[o + 3 * k] * an;
       sumf += q[o + 3 * k];
     }
-    S0 = fabsf(S0);
+    S0 = fabs(S0);
   }
-  if (use_f0) return S0 * (f0 + (1.f - sumf - f0) * iso + val);
-  return S0 * ((1.f - sumf) * iso + val);
+  if (use_f0) return S0 * (f0 + (1.0 - sumf - f0) * iso + val);
+  return S0 * ((1.0 - sumf) * iso + val);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -916,7 +933,7 @@ __device__ void fit_one(const FitArgs& a, int v, int lane) {
   ms.gz = bv + 2 * M;
   ms.b = a.gradnonlin ? a.bvals + (size_t)v * M : a.bvals;
   ms.M = M;
-  const float R = a.R, invR = 1.f / (2.f * R + 1.f);
+  const Real R = a.R, invR = 1.0 / (2.0 * R + 1.0);
   const int gbo = a.model == 3 ? 2 : 0;
   // non-finite data: flag and emit zeros
   bool bad = false;
@@ -934,69 +951,69 @@ __device__ void fit_one(const FitArgs& a, int v, int lane) {
   }
   Dti dt;
   dti_fit(ms, lane, dt);
-  float res[16];
+  Real res[16];
   bool refit = false;
   if (a.model == 1) {
     if (a.nonlin) {
-      float p[LmShape<kSingle, K, F0>::P];
+      Real p[LmShape<kSingle, K, F0>::P];
       start_single<K, F0>(dt, p);
       lm_run<kSingle, K, F0>(ms, p, lane, 0, R, invR);
       finalise<kSingle, K, F0>(p);
 #pragma unroll
       for (int i = 0; i < NPOUT; ++i) res[i] = p[i];
-      if (F0 && ((K > 0 && p[2] < 0.05f) || p[1] > 0.007f || p[NPOUT - 1] > 0.4f)) {
-        float p2[LmShape<kSingle, K, false>::P];
+      if (F0 && ((K > 0 && p[2] < 0.05) || p[1] > 0.007 || p[NPOUT - 1] > 0.4)) {
+        Real p2[LmShape<kSingle, K, false>::P];
         start_single<K, false>(dt, p2);
         lm_run<kSingle, K, false>(ms, p2, lane, 0, R, invR);
         finalise<kSingle, K, false>(p2);
 #pragma unroll
         for (int i = 0; i < NPOUT - 1; ++i) res[i] = p2[i];
-        res[NPOUT - 1] = 0.001f;
+        res[NPOUT - 1] = 0.001;
         refit = true;
       }
     } else {
-      float p[LmShape<kSingleC, K, F0>::P];
+      Real p[LmShape<kSingleC, K, F0>::P];
       start_single_c<K, F0>(dt, ms, lane, p);
       lm_run<kSingleC, K, F0>(ms, p, lane, 0, R, invR);
       finalise<kSingleC, K, F0>(p);
 #pragma unroll
       for (int i = 0; i < NPOUT; ++i) res[i] = p[i];
-      if (F0 && ((K > 0 && p[2] < 0.05f) || p[1] > 0.007f || p[NPOUT - 1] > 0.4f)) {
-        float p2[LmShape<kSingleC, K, false>::P];
+      if (F0 && ((K > 0 && p[2] < 0.05) || p[1] > 0.007 || p[NPOUT - 1] > 0.4)) {
+        Real p2[LmShape<kSingleC, K, false>::P];
         start_single_c<K, false>(dt, ms, lane, p2);
         lm_run<kSingleC, K, false>(ms, p2, lane, 0, R, invR);
         finalise<kSingleC, K, false>(p2);
 #pragma unroll
         for (int i = 0; i < NPOUT - 1; ++i) res[i] = p2[i];
-        res[NPOUT - 1] = 0.001f;
+        res[NPOUT - 1] = 0.001;
         refit = true;
       }
     }
   } else {
     constexpr int NPM = LmShape<kMulti, K, F0>::P;
-    float s[LmShape<kSingle, K, F0>::P];
+    Real s[LmShape<kSingle, K, F0>::P];
     start_single<K, F0>(dt, s);
     lm_run<kSingle, K, F0>(ms, s, lane, 0, R, invR);
     finalise<kSingle, K, F0>(s);
-    float p[NPM];
+    Real p[NPM];
     start_multi<K, F0>(s, p);
     lm_run<kMulti, K, F0>(ms, p, lane, gbo, R, invR);
     finalise<kMulti, K, F0>(p);
 #pragma unroll
     for (int i = 0; i < NPM; ++i) res[i] = p[i];
-    if (F0 && ((K > 0 && p[3] < 0.05f) || p[1] > 0.007f || p[NPM - 1] > 0.4f)) {
+    if (F0 && ((K > 0 && p[3] < 0.05) || p[1] > 0.007 || p[NPM - 1] > 0.4)) {
       // GPU re-fit path: PVM_single_c then PVM_multi (CUDA/xfibres_gpu.cu:331-333)
-      float c[LmShape<kSingleC, K, false>::P];
+      Real c[LmShape<kSingleC, K, false>::P];
       start_single_c<K, false>(dt, ms, lane, c);
       lm_run<kSingleC, K, false>(ms, c, lane, 0, R, invR);
       finalise<kSingleC, K, false>(c);
-      float p2[LmShape<kMulti, K, false>::P];
+      Real p2[LmShape<kMulti, K, false>::P];
       start_multi<K, false>(c, p2);
       lm_run<kMulti, K, false>(ms, p2, lane, gbo, R, invR);
       finalise<kMulti, K, false>(p2);
 #pragma unroll
       for (int i = 0; i < NPM - 1; ++i) res[i] = p2[i];
-      res[NPM - 1] = 0.001f;
+      res[NPM - 1] = 0.001;
       refit = true;
     }
   }
@@ -1004,11 +1021,11 @@ __device__ void fit_one(const FitArgs& a, int v, int lane) {
   if (a.rician) {
     const int o = a.model >= 2 ? 3 : 2;
     const bool use_f0 = F0 && !refit;
-    const float f0 = F0 ? res[npo - 1] : 0.f;
-    float s1 = 0.f;
+    const Real f0 = F0 ? res[npo - 1] : 0.0;
+    double s1 = 0.0;
     for (int m = lane; m < M; m += 32)
       s1 += ms.y[m] - predict_final<K>(a.model, res, o, use_f0, f0, R, ms.gx[m], ms.gy[m], ms.gz[m], ms.b[m]);
-    const double mean = group_sum<32>((double)s1) / M;
+    const double mean = group_sum<32>(s1) / M;
     double s2 = 0.0;
     for (int m = lane; m < M; m += 32) {
       const double r = ms.y[m] - predict_final<K>(a.model, res, o, use_f0, f0, R, ms.gx[m], ms.gy[m], ms.gz[m], ms.b[m]) - mean;
@@ -1021,7 +1038,7 @@ __device__ void fit_one(const FitArgs& a, int v, int lane) {
   }
 #pragma unroll
   for (int i = 0; i < 16; ++i)
-    if (i < npo && lane == i) out[i] = res[i];
+    if (i < npo && lane == i) out[i] = (float)res[i];
   if (lane == 0 && a.status) a.status[v] = refit ? BPX_VOX_F0_REFIT : 0u;
 }
 
