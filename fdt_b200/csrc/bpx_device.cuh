@@ -122,20 +122,21 @@ __device__ __forceinline__ float pm1(float x) { return x > 0.f ? 1.f : -1.f; }
 
 // log of the modified Bessel function I0 minus its argument, for z >= 0: the polynomial forms of
 // fibre.h:31-51 / CUDA/runmcmc_kernels.cu:126-145 (Abramowitz & Stegun 9.8.1, 9.8.2), written as
-// logI0(z) - z so that the Rician log-likelihood terms stay O(1).
+// logI0(z) - z so that the Rician log-likelihood terms stay O(1).  Branch-free: both polynomials
+// are evaluated and one log2 is taken of the selected one (measurements of one warp fall on
+// both sides of z = 3.75, so a branch would run both sides anyway).
 __device__ __forceinline__ float logI0_minus_z(float z) {
-  if (z < 3.75f) {
-    float a = z * (1.0f / 3.75f);
-    a *= a;
-    const float y =
-        1.0f + a * (3.5156229f + a * (3.0899424f + a * (1.2067492f + a * (0.2659732f + a * (0.0360768f + a * 0.0045813f)))));
-    return lg2_approx(y) * kLn2 - z;
-  }
-  const float rs = rsqrt_approx(z);
-  const float a = 3.75f * rs * rs;
+  const bool small = z < 3.75f;
+  float a = z * (1.0f / 3.75f);
+  a *= a;
+  const float q =
+      1.0f + a * (3.5156229f + a * (3.0899424f + a * (1.2067492f + a * (0.2659732f + a * (0.0360768f + a * 0.0045813f)))));
+  const float rs = rsqrt_approx(fmaxf(z, 3.75f));
+  const float c = 3.75f * rs * rs;
   const float p =
-      0.39894228f + a * (0.01328592f + a * (0.00225319f + a * (-0.00157565f + a * (0.00916281f + a * (-0.02057706f + a * (0.02635537f + a * (-0.01647633f + a * 0.00392377f)))))));
-  return lg2_approx(p * rs) * kLn2;
+      0.39894228f + c * (0.01328592f + c * (0.00225319f + c * (-0.00157565f + c * (0.00916281f + c * (-0.02057706f + c * (0.02635537f + c * (-0.01647633f + c * 0.00392377f)))))));
+  const float l = lg2_approx(small ? q : p * rs) * kLn2;
+  return small ? l - z : l;
 }
 
 }  // namespace bpx

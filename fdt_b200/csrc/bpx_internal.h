@@ -10,6 +10,7 @@ namespace bpx {
 
 constexpr int kFitThreads = 256;   // 8 warps, one voxel per warp
 constexpr int kMcmcThreads = 128;  // 4 warps
+constexpr int kMcmcMinBlocks = 3;  // register cap for 12 resident warps per SM
 
 int sm_count();  // multiprocessors of the current device (cached per device)
 

@@ -196,7 +196,7 @@ __device__ __forceinline__ T pick(const T (&a)[K], int kf) {
 }
 
 template <int MODEL, int K, bool RIC, int TPV, int MPL>
-__global__ void __launch_bounds__(kMcmcThreads) mcmc_kernel(McmcArgs a) {
+__global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(McmcArgs a) {
   constexpr int NS = 6 + 3 * K;             // proposal slots
   constexpr int NR = (NS + TPV - 1) / TPV;  // Philox blocks per lane per iteration
   constexpr int GPW = 32 / TPV;             // groups (voxels) per warp
@@ -223,12 +223,14 @@ __global__ void __launch_bounds__(kMcmcThreads) mcmc_kernel(McmcArgs a) {
   pr.can_use_ard = !a.no_ard;
   const bool use_f0 = a.f0 != 0;
 
-  // shared memory: (g_x, g_y, g_z, b) per measurement -- one copy per block, or one per group
-  // under gradnonlin -- then per-group proposal widths and acceptance counts
+  // shared memory: (g_x, g_y, g_z, b) per measurement (one copy per block, or per group under
+  // gradnonlin); per-thread backups of the signals a proposal overwrites; per-group proposal
+  // widths and acceptance counts
   const int ngb = a.gradnonlin ? GPB : 1;
   float4* gb = smem4 + (a.gradnonlin ? gblk * M : 0);
-  float* sprop = (float*)(smem4 + ngb * M) + gblk * NS;
-  int* sacc = (int*)((float*)(smem4 + ngb * M) + GPB * NS) + gblk * NS;
+  float* bk = (float*)(smem4 + ngb * M) + threadIdx.x;  // element c of this thread: bk[c * kMcmcThreads]
+  float* sprop = (float*)(smem4 + ngb * M) + (K + 1) * MPL * kMcmcThreads + gblk * NS;
+  int* sacc = (int*)((float*)(smem4 + ngb * M) + (K + 1) * MPL * kMcmcThreads + GPB * NS) + gblk * NS;
   if (!a.gradnonlin) {
     for (int m = threadIdx.x; m < M; m += blockDim.x)
       gb[m] = make_float4(a.bvecs[m], a.bvecs[M + m], a.bvecs[2 * M + m], a.bvals[m]);
@@ -251,7 +253,7 @@ __global__ void __launch_bounds__(kMcmcThreads) mcmc_kernel(McmcArgs a) {
     }
 
     // ---- this lane's measurements ----
-    float y[MPL], b[MPL], s[K][MPL], iso[MPL];
+    float y[MPL], s[K][MPL], iso[MPL];
     int nj = 0;
     bool bad = false;
     const float* yv = a.data + (size_t)v * M;
@@ -259,10 +261,8 @@ __global__ void __launch_bounds__(kMcmcThreads) mcmc_kernel(McmcArgs a) {
     for (int j = 0; j < MPL; ++j) {
       const int m = gl + j * TPV;
       y[j] = 0.f;
-      b[j] = 0.f;
       if (m < M) {
         y[j] = __ldg(yv + m);
-        b[j] = gb[m].w;
         nj = j + 1;
         bad |= !isfinite(y[j]);
       }
@@ -317,16 +317,16 @@ __global__ void __launch_bounds__(kMcmcThreads) mcmc_kernel(McmcArgs a) {
     {
       const SigParams<MODEL> sp = sig_params<MODEL>(d, dstd, R);
 #pragma unroll
-      for (int k = 0; k < K; ++k)
+      for (int j = 0; j < MPL; ++j) {
+        const int m = gl + j * TPV;
+        const float4 g = m < M ? gb[m] : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-        for (int j = 0; j < MPL; ++j) {
-          const int m = gl + j * TPV;
-          const float4 g = m < M ? gb[m] : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int k = 0; k < K; ++k) {
           const float dp = g.x * vx[k] + g.y * vy[k] + g.z * vz[k];
-          s[k][j] = stick_signal<MODEL>(sp, b[j], dp * dp);
+          s[k][j] = stick_signal<MODEL>(sp, g.w, dp * dp);
         }
-#pragma unroll
-      for (int j = 0; j < MPL; ++j) iso[j] = iso_signal<MODEL>(sp, b[j]);
+        iso[j] = iso_signal<MODEL>(sp, g.w);
+      }
     }
     float lik = lik_stat2<K, RIC, TPV, MPL>(y, nj, iso, s, S0, f, f0, tau);
     // initialise_props, acceptance counters
@@ -385,7 +385,6 @@ __global__ void __launch_bounds__(kMcmcThreads) mcmc_kernel(McmcArgs a) {
         float pnew = 0.f, pold = 0.f;  // prior term that changes
         bool rej = false;
         unsigned mask = 0u;
-        bool newdir = false;
         switch (kind) {
           case kSlotF0: {
             f0n = f0 + n * prop;
@@ -434,13 +433,11 @@ __global__ void __launch_bounds__(kMcmcThreads) mcmc_kernel(McmcArgs a) {
             pold = pick<K>(p_th, kf);
             pnew = th_prior(thn);
             mask = 1u << kf;
-            newdir = true;
           } break;
           case kSlotFibre0 + 1:  // phi of fibre kf
             thn = pick<K>(th, kf);
             phn = pick<K>(ph, kf) + n * prop;
             mask = 1u << kf;
-            newdir = true;
             break;
           default: {  // f of fibre kf
             const float fkn = pick<K>(f, kf) + n * prop;
@@ -457,49 +454,78 @@ __global__ void __launch_bounds__(kMcmcThreads) mcmc_kernel(McmcArgs a) {
             rej = rej || (fs > 1.f);
           } break;
         }
-        // ---- signals of the proposed state, then its likelihood ----
+        // ---- signals of the proposed state (in place, old values kept in bk), likelihood ----
         float likn = lik;
-        float ns_[K][MPL], ni[MPL];
         float nvx = 0.f, nvy = 0.f, nvz = 0.f;
-        const bool any_live = __any_sync(0xffffffffu, !rej);
-        if (any_live) {
-          if (newdir) {
-            float st, ct, sp_, cp;
-            sincosf(thn, &st, &ct);
-            sincosf(phn, &sp_, &cp);
-            nvx = st * cp;
-            nvy = st * sp_;
-            nvz = ct;
-          }
-          const SigParams<MODEL> sp = sig_params<MODEL>(dn, dsn, Rn);
+        const bool live = __any_sync(0xffffffffu, !rej);
+        const bool one_fibre = mask != 0u && (mask & kAllSticks) != kAllSticks && (mask & kAllSticks) != 0u;
+        if (live) {
+          if (mask != 0u) {
+            const SigParams<MODEL> sp = sig_params<MODEL>(dn, dsn, Rn);
+            if (one_fibre) {
+              float st, ct, sp_, cp;
+              sincosf(thn, &st, &ct);
+              sincosf(phn, &sp_, &cp);
+              nvx = st * cp;
+              nvy = st * sp_;
+              nvz = ct;
 #pragma unroll
-          for (int k = 0; k < K; ++k) {
-            if (mask & (1u << k)) {
-              const bool nd = newdir && k == kf;
-              const float ux = nd ? nvx : vx[k], uy = nd ? nvy : vy[k], uz = nd ? nvz : vz[k];
+              for (int k = 0; k < K; ++k)
+                if (k == kf) {
+#pragma unroll
+                  for (int j = 0; j < MPL; ++j) {
+                    const int m = gl + j * TPV;
+                    const float4 g = m < M ? gb[m] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    const float dp = g.x * nvx + g.y * nvy + g.z * nvz;
+                    bk[j * kMcmcThreads] = s[k][j];
+                    s[k][j] = stick_signal<MODEL>(sp, g.w, dp * dp);
+                  }
+                }
+            } else {
+              const bool sticks = (mask & kAllSticks) != 0u, isob = (mask & kIsoBit) != 0u;
 #pragma unroll
               for (int j = 0; j < MPL; ++j) {
                 const int m = gl + j * TPV;
                 const float4 g = m < M ? gb[m] : make_float4(0.f, 0.f, 0.f, 0.f);
-                const float dp = g.x * ux + g.y * uy + g.z * uz;
-                ns_[k][j] = stick_signal<MODEL>(sp, b[j], dp * dp);
-              }
-            } else {
+                if (sticks) {
 #pragma unroll
-              for (int j = 0; j < MPL; ++j) ns_[k][j] = s[k][j];
+                  for (int k = 0; k < K; ++k) {
+                    const float dp = g.x * vx[k] + g.y * vy[k] + g.z * vz[k];
+                    bk[(k * MPL + j) * kMcmcThreads] = s[k][j];
+                    s[k][j] = stick_signal<MODEL>(sp, g.w, dp * dp);
+                  }
+                }
+                if (isob) {
+                  bk[(K * MPL + j) * kMcmcThreads] = iso[j];
+                  iso[j] = iso_signal<MODEL>(sp, g.w);
+                }
+              }
             }
           }
-          if (mask & kIsoBit) {
-#pragma unroll
-            for (int j = 0; j < MPL; ++j) ni[j] = iso_signal<MODEL>(sp, b[j]);
-          } else {
-#pragma unroll
-            for (int j = 0; j < MPL; ++j) ni[j] = iso[j];
-          }
-          likn = lik_stat2<K, RIC, TPV, MPL>(y, nj, ni, ns_, S0n, fn, f0n, taun);
+          likn = lik_stat2<K, RIC, TPV, MPL>(y, nj, iso, s, S0n, fn, f0n, taun);
         }
         const bool ok = !rej && ((pold - pnew) + dlik<RIC>(lik, likn, tau, taun, halfM, fM) > lu);
-        // ---- accept / reject ----
+        // ---- accept, or restore the signals ----
+        if (live && mask != 0u && !__all_sync(0xffffffffu, ok)) {
+          if (one_fibre) {
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+              if (k == kf) {
+#pragma unroll
+                for (int j = 0; j < MPL; ++j) s[k][j] = ok ? s[k][j] : bk[j * kMcmcThreads];
+              }
+          } else {
+            const bool sticks = (mask & kAllSticks) != 0u, isob = (mask & kIsoBit) != 0u;
+#pragma unroll
+            for (int j = 0; j < MPL; ++j) {
+              if (sticks) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) s[k][j] = ok ? s[k][j] : bk[(k * MPL + j) * kMcmcThreads];
+              }
+              if (isob) iso[j] = ok ? iso[j] : bk[(K * MPL + j) * kMcmcThreads];
+            }
+          }
+        }
         if (ok) {
           lik = likn;
           switch (kind) {
@@ -532,18 +558,6 @@ __global__ void __launch_bounds__(kMcmcThreads) mcmc_kernel(McmcArgs a) {
               break;
           }
           if (gl == 0) sacc[slot] += 1;
-        }
-        if (mask != 0u && __any_sync(0xffffffffu, ok)) {
-#pragma unroll
-          for (int k = 0; k < K; ++k)
-            if (mask & (1u << k)) {
-#pragma unroll
-              for (int j = 0; j < MPL; ++j) s[k][j] = ok ? ns_[k][j] : s[k][j];
-            }
-          if (mask & kIsoBit) {
-#pragma unroll
-            for (int j = 0; j < MPL; ++j) iso[j] = ok ? ni[j] : iso[j];
-          }
         }
       }
       // ---------------- record (CUDA/runmcmc_kernels.cu:1326-1339) ----------------
@@ -691,7 +705,8 @@ template <int MODEL, int K, bool RIC, int TPV, int MPL>
 cudaError_t launch_mcmc_t(const McmcArgs& a, cudaStream_t s) {
   auto kern = mcmc_kernel<MODEL, K, RIC, TPV, MPL>;
   constexpr int NS = 6 + 3 * K, GPB = kMcmcThreads / TPV;
-  const size_t smem = (size_t)(a.gradnonlin ? GPB : 1) * a.ndir * sizeof(float4) + (size_t)GPB * NS * 8;
+  const size_t smem = (size_t)(a.gradnonlin ? GPB : 1) * a.ndir * sizeof(float4) +
+                      (size_t)(K + 1) * MPL * kMcmcThreads * sizeof(float) + (size_t)GPB * NS * 8;
   if (smem > 48 * 1024) {
     cudaError_t ea = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (ea != cudaSuccess) return ea;
