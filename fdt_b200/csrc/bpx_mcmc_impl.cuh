@@ -195,12 +195,121 @@ __device__ __forceinline__ T pick(const T (&a)[K], int kf) {
   return r;
 }
 
+// ---- scalar / packed-pair arithmetic ------------------------------------------------------
+// A lane's measurements are processed two at a time with the sm_100 packed FP32x2 instructions
+// (one issue slot for two FMAs); an odd measurement left over uses the scalar forms.
+__device__ __forceinline__ float vfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float vmul(float a, float b) { return a * b; }
+__device__ __forceinline__ float2 vmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float vadd(float a, float b) { return a + b; }
+__device__ __forceinline__ float2 vadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+template <typename V>
+__device__ __forceinline__ V vbc(float x);
+template <>
+__device__ __forceinline__ float vbc<float>(float x) { return x; }
+template <>
+__device__ __forceinline__ float2 vbc<float2>(float x) { return make_float2(x, x); }
+__device__ __forceinline__ float vex2(float x) { return ex2_approx(x); }
+__device__ __forceinline__ float2 vex2(float2 x) { return make_float2(ex2_approx(x.x), ex2_approx(x.y)); }
+__device__ __forceinline__ float vlg2(float x) { return lg2_approx(x); }
+__device__ __forceinline__ float2 vlg2(float2 x) { return make_float2(lg2_approx(x.x), lg2_approx(x.y)); }
+__device__ __forceinline__ float vhsum(float x) { return x; }
+__device__ __forceinline__ float vhsum(float2 x) { return x.x + x.y; }
+
+// Rician log-likelihood term without its log(y) part, -tau (y-p)^2/2 + [logI0(z) - z] with
+// z = tau p y, for one or two measurements (the branch-free logI0_minus_z of bpx_device.cuh;
+// the small-argument polynomial is taken in z^2 with its coefficients pre-divided by 3.75^(2i)).
+template <typename V>
+__device__ __forceinline__ V rician_term(V y, V pred, V r, V tau, V nhalf_tau);
+__device__ __forceinline__ float rician_pick(float z, float q, float pr, float& zs) {
+  const bool small = z < 3.75f;
+  zs = small ? -z : 0.f;
+  return small ? q : pr;
+}
+template <typename V>
+__device__ __forceinline__ V rician_term(V y, V pred, V r, V tau, V nhalf_tau) {
+  constexpr float s1 = 3.5156229f / 14.0625f, s2 = 3.0899424f / (14.0625f * 14.0625f),
+                  s3 = 1.2067492f / (14.0625f * 14.0625f * 14.0625f),
+                  s4 = 0.2659732f / (14.0625f * 14.0625f * 14.0625f * 14.0625f),
+                  s5 = 0.0360768f / (14.0625f * 14.0625f * 14.0625f * 14.0625f * 14.0625f),
+                  s6 = 0.0045813f / (14.0625f * 14.0625f * 14.0625f * 14.0625f * 14.0625f * 14.0625f);
+  const V z = vmul(vmul(tau, pred), y);
+  const V u = vmul(z, z);
+  V q = vfma(u, vbc<V>(s6), vbc<V>(s5));
+  q = vfma(u, q, vbc<V>(s4));
+  q = vfma(u, q, vbc<V>(s3));
+  q = vfma(u, q, vbc<V>(s2));
+  q = vfma(u, q, vbc<V>(s1));
+  q = vfma(u, q, vbc<V>(1.0f));
+  V rs;
+  if constexpr (sizeof(V) == 8) {
+    rs = make_float2(rsqrt_approx(fmaxf(z.x, 3.75f)), rsqrt_approx(fmaxf(z.y, 3.75f)));
+  } else {
+    rs = rsqrt_approx(fmaxf(z, 3.75f));
+  }
+  const V c = vmul(rs, vmul(rs, vbc<V>(3.75f)));
+  V p = vfma(c, vbc<V>(0.00392377f), vbc<V>(-0.01647633f));
+  p = vfma(c, p, vbc<V>(0.02635537f));
+  p = vfma(c, p, vbc<V>(-0.02057706f));
+  p = vfma(c, p, vbc<V>(0.00916281f));
+  p = vfma(c, p, vbc<V>(-0.00157565f));
+  p = vfma(c, p, vbc<V>(0.00225319f));
+  p = vfma(c, p, vbc<V>(0.01328592f));
+  p = vfma(c, p, vbc<V>(0.39894228f));
+  const V pr = vmul(p, rs);
+  V sel, zs;
+  if constexpr (sizeof(V) == 8) {
+    sel.x = rician_pick(z.x, q.x, pr.x, zs.x);
+    sel.y = rician_pick(z.y, q.y, pr.y, zs.y);
+  } else {
+    sel = rician_pick(z, q, pr, zs);
+  }
+  const V h = vfma(vlg2(sel), vbc<V>(kLn2), zs);
+  return vfma(vmul(nhalf_tau, r), r, h);
+}
+
+// signals of one or two measurements (compute_signal / compute_iso_signal, CUDA/runmcmc_kernels.cu:67-95)
+template <int MODEL, typename V>
+__device__ __forceinline__ V stick_v(const SigParams<MODEL>& sp, V b, V bbeta, V c) {
+  if (MODEL == 1) return vex2(vmul(vmul(vbc<V>(sp.e1), b), c));
+  if (MODEL == 2) {
+    if (sp.mono) return vex2(vmul(vmul(vbc<V>(sp.e1), b), c));
+    return vex2(vmul(vbc<V>(-sp.alpha), vlg2(vfma(bbeta, c, vbc<V>(1.0f)))));
+  }
+  return vex2(vmul(vmul(vbc<V>(sp.e3), b), vfma(vbc<V>(sp.omR), c, vbc<V>(sp.R))));
+}
+template <int MODEL, typename V>
+__device__ __forceinline__ V iso_v(const SigParams<MODEL>& sp, V b, V bbeta) {
+  if (MODEL == 1 || sp.mono) return vex2(vmul(vbc<V>(sp.e1), b));
+  return vex2(vmul(vbc<V>(-sp.alpha), vlg2(vadd(bbeta, vbc<V>(1.0f)))));
+}
+
+// per-measurement likelihood contribution (before the group sum), weighted by w (0 for padding)
+template <int K, bool RIC, typename V>
+__device__ __forceinline__ V lik_v(V y, V w, V isov, const V (&sk)[K], V S0, const V (&fk)[K], V f0, V wiso, V tau,
+                                   V nhalf_tau) {
+  V base = vfma(wiso, isov, f0);
+#pragma unroll
+  for (int k = 0; k < K; ++k) base = vfma(fk[k], sk[k], base);
+  const V pred = vmul(S0, base);
+  const V r = vfma(pred, vbc<V>(-1.0f), y);
+  if (!RIC) {
+    const V rw = vmul(r, w);
+    return vmul(rw, r);
+  }
+  return vmul(w, rician_term<V>(y, pred, r, tau, nhalf_tau));
+}
+
 template <int MODEL, int K, bool RIC, int TPV, int MPL>
 __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(McmcArgs a) {
   constexpr int NS = 6 + 3 * K;             // proposal slots
   constexpr int NR = (NS + TPV - 1) / TPV;  // Philox blocks per lane per iteration
   constexpr int GPW = 32 / TPV;             // groups (voxels) per warp
   constexpr int GPB = kMcmcThreads / TPV;   // groups per block
+  constexpr int NP = MPL / 2;               // measurement pairs per lane
+  constexpr bool TAIL = (MPL & 1) != 0;     // one unpaired measurement per lane
+  constexpr int NG = TPV * MPL;             // float4 (g, b) entries per copy
   constexpr unsigned kIsoBit = 1u << K;
   constexpr unsigned kAllSticks = (1u << K) - 1u;
   extern __shared__ float4 smem4[];
@@ -208,6 +317,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
   const int gl = lane % TPV;
   const int gw = lane / TPV;
   const int gblk = threadIdx.x / TPV;
+  const int tid = threadIdx.x;
   const int warps_total = gridDim.x * (blockDim.x >> 5);
   const int warp_id = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int M = a.ndir;
@@ -223,17 +333,38 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
   pr.can_use_ard = !a.no_ard;
   const bool use_f0 = a.f0 != 0;
 
-  // shared memory: (g_x, g_y, g_z, b) per measurement (one copy per block, or per group under
-  // gradnonlin); per-thread backups of the signals a proposal overwrites; per-group proposal
-  // widths and acceptance counts
-  const int ngb = a.gradnonlin ? GPB : 1;
-  float4* gb = smem4 + (a.gradnonlin ? gblk * M : 0);
-  float* bk = (float*)(smem4 + ngb * M) + threadIdx.x;  // element c of this thread: bk[c * kMcmcThreads]
-  float* sprop = (float*)(smem4 + ngb * M) + (K + 1) * MPL * kMcmcThreads + gblk * NS;
-  int* sacc = (int*)((float*)(smem4 + ngb * M) + (K + 1) * MPL * kMcmcThreads + GPB * NS) + gblk * NS;
+  // shared memory: the (g_x, g_y, g_z, b) table in pair order (one copy per block, or per group
+  // under gradnonlin); per-thread backups of the signals a proposal overwrites; per-group proposal
+  // widths and acceptance counts.  Pair p of lane l is entries 2(p*TPV+l) and 2(p*TPV+l)+1 =
+  // {gx0,gx1,gy0,gy1}, {gz0,gz1,b0,b1} for measurements l+2p*TPV and l+(2p+1)*TPV; the unpaired
+  // measurement l+(MPL-1)*TPV is entry 2*NP*TPV+l.  Measurements past M read zeros.
+  const int ncopy = a.gradnonlin ? GPB : 1;
+  float4* gb = smem4 + (a.gradnonlin ? gblk * NG : 0);
+  float* after = (float*)(smem4 + ncopy * NG);
+  float2* bkp = (float2*)after + tid;  // pair backup c: bkp[c * kMcmcThreads]
+  float* bkt = after + 2 * (K + 1) * NP * kMcmcThreads + tid;
+  float* sprop = after + (2 * NP + 1) * (K + 1) * kMcmcThreads + gblk * NS;
+  int* sacc = (int*)(after + (2 * NP + 1) * (K + 1) * kMcmcThreads + GPB * NS) + gblk * NS;
+  auto fill_gb = [&](float4* dst, const float* bv, const float* bl, int first_l, int step) {
+    for (int e = first_l; e < NP * TPV; e += step) {
+      const int p = e / TPV, l = e % TPV;
+      const int m0 = l + 2 * p * TPV, m1 = m0 + TPV;
+      const float gx0 = m0 < M ? bv[m0] : 0.f, gy0 = m0 < M ? bv[M + m0] : 0.f, gz0 = m0 < M ? bv[2 * M + m0] : 0.f;
+      const float b0 = m0 < M ? bl[m0] : 0.f;
+      const float gx1 = m1 < M ? bv[m1] : 0.f, gy1 = m1 < M ? bv[M + m1] : 0.f, gz1 = m1 < M ? bv[2 * M + m1] : 0.f;
+      const float b1 = m1 < M ? bl[m1] : 0.f;
+      dst[2 * e] = make_float4(gx0, gx1, gy0, gy1);
+      dst[2 * e + 1] = make_float4(gz0, gz1, b0, b1);
+    }
+    if (TAIL)
+      for (int l = first_l; l < TPV; l += step) {
+        const int m = l + (MPL - 1) * TPV;
+        dst[2 * NP * TPV + l] =
+            m < M ? make_float4(bv[m], bv[M + m], bv[2 * M + m], bl[m]) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+  };
   if (!a.gradnonlin) {
-    for (int m = threadIdx.x; m < M; m += blockDim.x)
-      gb[m] = make_float4(a.bvecs[m], a.bvecs[M + m], a.bvecs[2 * M + m], a.bvals[m]);
+    fill_gb(gb, a.bvecs, a.bvals, tid, blockDim.x);
     __syncthreads();
   }
 
@@ -245,27 +376,30 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
     const int v = valid ? vreal : a.nvox - 1;
     const uint64_t gvox = a.voxel_offset + (uint64_t)v;
     if (a.gradnonlin) {
-      const float* bv = a.bvecs + (size_t)v * 3 * M;
-      const float* bl = a.bvals + (size_t)v * M;
       __syncwarp();
-      for (int m = gl; m < M; m += TPV) gb[m] = make_float4(bv[m], bv[M + m], bv[2 * M + m], bl[m]);
+      fill_gb(gb, a.bvecs + (size_t)v * 3 * M, a.bvals + (size_t)v * M, gl, TPV);
       __syncwarp();
     }
 
-    // ---- this lane's measurements ----
-    float y[MPL], s[K][MPL], iso[MPL];
-    int nj = 0;
+    // ---- this lane's measurements: pairs (y2, w2) and the unpaired one (yt, wt) ----
+    float2 y2[NP], w2[NP], i2[NP], s2[K][NP];
+    float yt = 0.f, wt = 0.f, it_ = 0.f, st[K];
     bool bad = false;
     const float* yv = a.data + (size_t)v * M;
 #pragma unroll
-    for (int j = 0; j < MPL; ++j) {
-      const int m = gl + j * TPV;
-      y[j] = 0.f;
-      if (m < M) {
-        y[j] = __ldg(yv + m);
-        nj = j + 1;
-        bad |= !isfinite(y[j]);
-      }
+    for (int p = 0; p < NP; ++p) {
+      const int m0 = gl + 2 * p * TPV, m1 = m0 + TPV;
+      y2[p].x = m0 < M ? __ldg(yv + m0) : 0.f;
+      y2[p].y = m1 < M ? __ldg(yv + m1) : 0.f;
+      w2[p].x = m0 < M ? 1.f : 0.f;
+      w2[p].y = m1 < M ? 1.f : 0.f;
+      bad |= !isfinite(y2[p].x) || !isfinite(y2[p].y);
+    }
+    if (TAIL) {
+      const int m = gl + (MPL - 1) * TPV;
+      yt = m < M ? __ldg(yv + m) : 0.f;
+      wt = m < M ? 1.f : 0.f;
+      bad |= !isfinite(yt);
     }
     bad = group_sum<TPV>(bad ? 1.f : 0.f) > 0.f;
 
@@ -296,12 +430,12 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
       float fp = 0.f;
       if (!(f[k] <= 0.f || f[k] >= 1.f)) fp = pr.fudge * (lam[k] ? logf(f[k]) : 0.f);
       p_f[k] = fp;
-      float st, ct, sp, cp;
-      sincosf(th[k], &st, &ct);
+      float sn, cs, sp, cp;
+      sincosf(th[k], &sn, &cs);
       sincosf(ph[k], &sp, &cp);
-      vx[k] = st * cp;
-      vy[k] = st * sp;
-      vz[k] = ct;
+      vx[k] = sn * cp;
+      vy[k] = sn * sp;
+      vz[k] = cs;
     }
     float p_d = 0.f, p_dstd = 0.f, p_R = 0.f, p_f0 = 0.f;
     if (MODEL == 3 && d >= 0.f && d <= kUpperDiff) p_d = (1.0f - 3.0f) * logf(d) + 4000.0f * d;
@@ -314,21 +448,75 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
       }
     }
     if (use_f0 && !(f0 <= 0.f || f0 >= 1.f) && a.ardf0) p_f0 = logf(f0);
-    {
-      const SigParams<MODEL> sp = sig_params<MODEL>(d, dstd, R);
+
+    // all signals of state (d, dstd, R, v_k) into s2/st/i2/it_, backing up when bk is true
+    auto all_signals = [&](float dd, float ds, float RR, bool sticks, bool isob, bool backup) {
+      const SigParams<MODEL> sp = sig_params<MODEL>(dd, ds, RR);
+      const float2 beta2 = make_float2(sp.beta, sp.beta);
 #pragma unroll
-      for (int j = 0; j < MPL; ++j) {
-        const int m = gl + j * TPV;
-        const float4 g = m < M ? gb[m] : make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int p = 0; p < NP; ++p) {
+        const float4 ga = gb[2 * (p * TPV + gl)], gc = gb[2 * (p * TPV + gl) + 1];
+        const float2 gx = make_float2(ga.x, ga.y), gy = make_float2(ga.z, ga.w), gz = make_float2(gc.x, gc.y);
+        const float2 b = make_float2(gc.z, gc.w);
+        const float2 bbeta = vmul(beta2, b);
+        if (sticks) {
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-          const float dp = g.x * vx[k] + g.y * vy[k] + g.z * vz[k];
-          s[k][j] = stick_signal<MODEL>(sp, g.w, dp * dp);
+          for (int k = 0; k < K; ++k) {
+            float2 dp = vmul(gx, vbc<float2>(vx[k]));
+            dp = vfma(gy, vbc<float2>(vy[k]), dp);
+            dp = vfma(gz, vbc<float2>(vz[k]), dp);
+            if (backup) bkp[(k * NP + p) * kMcmcThreads] = s2[k][p];
+            s2[k][p] = stick_v<MODEL, float2>(sp, b, bbeta, vmul(dp, dp));
+          }
         }
-        iso[j] = iso_signal<MODEL>(sp, g.w);
+        if (isob) {
+          if (backup) bkp[(K * NP + p) * kMcmcThreads] = i2[p];
+          i2[p] = iso_v<MODEL, float2>(sp, b, bbeta);
+        }
       }
-    }
-    float lik = lik_stat2<K, RIC, TPV, MPL>(y, nj, iso, s, S0, f, f0, tau);
+      if (TAIL) {
+        const float4 g = gb[2 * NP * TPV + gl];
+        const float bbeta = sp.beta * g.w;
+        if (sticks) {
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            const float dp = g.x * vx[k] + g.y * vy[k] + g.z * vz[k];
+            if (backup) bkt[k * kMcmcThreads] = st[k];
+            st[k] = stick_v<MODEL, float>(sp, g.w, bbeta, dp * dp);
+          }
+        }
+        if (isob) {
+          if (backup) bkt[K * kMcmcThreads] = it_;
+          it_ = iso_v<MODEL, float>(sp, g.w, bbeta);
+        }
+      }
+    };
+    // the likelihood statistic of a state, summed over the group
+    auto lik_of = [&](float S0x, const float (&fx)[K], float f0x, float taux) {
+      float fsum = f0x;
+#pragma unroll
+      for (int k = 0; k < K; ++k) fsum += fx[k];
+      const float wiso = 1.0f - fsum;
+      float2 fk2[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k) fk2[k] = vbc<float2>(fx[k]);
+      const float2 S02 = vbc<float2>(S0x), f02 = vbc<float2>(f0x), wiso2 = vbc<float2>(wiso);
+      const float2 tau2 = vbc<float2>(taux), nht2 = vbc<float2>(-0.5f * taux);
+      float2 acc2 = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        float2 sk[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) sk[k] = s2[k][p];
+        acc2 = vadd(acc2, lik_v<K, RIC, float2>(y2[p], w2[p], i2[p], sk, S02, fk2, f02, wiso2, tau2, nht2));
+      }
+      float acc = vhsum(acc2);
+      if (TAIL) acc += lik_v<K, RIC, float>(yt, wt, it_, st, S0x, fx, f0x, wiso, taux, -0.5f * taux);
+      return group_sum<TPV>(acc);
+    };
+
+    all_signals(d, dstd, R, true, true, false);
+    float lik = lik_of(S0, f, f0, tau);
     // initialise_props, acceptance counters
     if (gl == 0) {
 #pragma unroll
@@ -454,55 +642,46 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
             rej = rej || (fs > 1.f);
           } break;
         }
-        // ---- signals of the proposed state (in place, old values kept in bk), likelihood ----
+        // ---- signals of the proposed state (in place, old values backed up), likelihood ----
         float likn = lik;
         float nvx = 0.f, nvy = 0.f, nvz = 0.f;
         const bool live = __any_sync(0xffffffffu, !rej);
         const bool one_fibre = mask != 0u && (mask & kAllSticks) != kAllSticks && (mask & kAllSticks) != 0u;
         if (live) {
-          if (mask != 0u) {
-            const SigParams<MODEL> sp = sig_params<MODEL>(dn, dsn, Rn);
-            if (one_fibre) {
-              float st, ct, sp_, cp;
-              sincosf(thn, &st, &ct);
-              sincosf(phn, &sp_, &cp);
-              nvx = st * cp;
-              nvy = st * sp_;
-              nvz = ct;
+          if (one_fibre) {
+            float sn, cs, sp_, cp;
+            sincosf(thn, &sn, &cs);
+            sincosf(phn, &sp_, &cp);
+            nvx = sn * cp;
+            nvy = sn * sp_;
+            nvz = cs;
+            const SigParams<MODEL> sp = sig_params<MODEL>(d, dstd, R);
+            const float2 beta2 = make_float2(sp.beta, sp.beta);
+            const float2 nvx2 = vbc<float2>(nvx), nvy2 = vbc<float2>(nvy), nvz2 = vbc<float2>(nvz);
 #pragma unroll
-              for (int k = 0; k < K; ++k)
-                if (k == kf) {
+            for (int k = 0; k < K; ++k)
+              if (k == kf) {
 #pragma unroll
-                  for (int j = 0; j < MPL; ++j) {
-                    const int m = gl + j * TPV;
-                    const float4 g = m < M ? gb[m] : make_float4(0.f, 0.f, 0.f, 0.f);
-                    const float dp = g.x * nvx + g.y * nvy + g.z * nvz;
-                    bk[j * kMcmcThreads] = s[k][j];
-                    s[k][j] = stick_signal<MODEL>(sp, g.w, dp * dp);
-                  }
+                for (int p = 0; p < NP; ++p) {
+                  const float4 ga = gb[2 * (p * TPV + gl)], gc = gb[2 * (p * TPV + gl) + 1];
+                  float2 dp = vmul(make_float2(ga.x, ga.y), nvx2);
+                  dp = vfma(make_float2(ga.z, ga.w), nvy2, dp);
+                  dp = vfma(make_float2(gc.x, gc.y), nvz2, dp);
+                  const float2 b = make_float2(gc.z, gc.w);
+                  bkp[p * kMcmcThreads] = s2[k][p];
+                  s2[k][p] = stick_v<MODEL, float2>(sp, b, vmul(beta2, b), vmul(dp, dp));
                 }
-            } else {
-              const bool sticks = (mask & kAllSticks) != 0u, isob = (mask & kIsoBit) != 0u;
-#pragma unroll
-              for (int j = 0; j < MPL; ++j) {
-                const int m = gl + j * TPV;
-                const float4 g = m < M ? gb[m] : make_float4(0.f, 0.f, 0.f, 0.f);
-                if (sticks) {
-#pragma unroll
-                  for (int k = 0; k < K; ++k) {
-                    const float dp = g.x * vx[k] + g.y * vy[k] + g.z * vz[k];
-                    bk[(k * MPL + j) * kMcmcThreads] = s[k][j];
-                    s[k][j] = stick_signal<MODEL>(sp, g.w, dp * dp);
-                  }
-                }
-                if (isob) {
-                  bk[(K * MPL + j) * kMcmcThreads] = iso[j];
-                  iso[j] = iso_signal<MODEL>(sp, g.w);
+                if (TAIL) {
+                  const float4 g = gb[2 * NP * TPV + gl];
+                  const float dp = g.x * nvx + g.y * nvy + g.z * nvz;
+                  bkt[0] = st[k];
+                  st[k] = stick_v<MODEL, float>(sp, g.w, sp.beta * g.w, dp * dp);
                 }
               }
-            }
+          } else if (mask != 0u) {
+            all_signals(dn, dsn, Rn, (mask & kAllSticks) != 0u, (mask & kIsoBit) != 0u, true);
           }
-          likn = lik_stat2<K, RIC, TPV, MPL>(y, nj, iso, s, S0n, fn, f0n, taun);
+          likn = lik_of(S0n, fn, f0n, taun);
         }
         const bool ok = !rej && ((pold - pnew) + dlik<RIC>(lik, likn, tau, taun, halfM, fM) > lu);
         // ---- accept, or restore the signals ----
@@ -512,17 +691,37 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
             for (int k = 0; k < K; ++k)
               if (k == kf) {
 #pragma unroll
-                for (int j = 0; j < MPL; ++j) s[k][j] = ok ? s[k][j] : bk[j * kMcmcThreads];
+                for (int p = 0; p < NP; ++p) {
+                  const float2 old = bkp[p * kMcmcThreads];
+                  s2[k][p].x = ok ? s2[k][p].x : old.x;
+                  s2[k][p].y = ok ? s2[k][p].y : old.y;
+                }
+                if (TAIL) st[k] = ok ? st[k] : bkt[0];
               }
           } else {
             const bool sticks = (mask & kAllSticks) != 0u, isob = (mask & kIsoBit) != 0u;
 #pragma unroll
-            for (int j = 0; j < MPL; ++j) {
+            for (int p = 0; p < NP; ++p) {
               if (sticks) {
 #pragma unroll
-                for (int k = 0; k < K; ++k) s[k][j] = ok ? s[k][j] : bk[(k * MPL + j) * kMcmcThreads];
+                for (int k = 0; k < K; ++k) {
+                  const float2 old = bkp[(k * NP + p) * kMcmcThreads];
+                  s2[k][p].x = ok ? s2[k][p].x : old.x;
+                  s2[k][p].y = ok ? s2[k][p].y : old.y;
+                }
               }
-              if (isob) iso[j] = ok ? iso[j] : bk[(K * MPL + j) * kMcmcThreads];
+              if (isob) {
+                const float2 old = bkp[(K * NP + p) * kMcmcThreads];
+                i2[p].x = ok ? i2[p].x : old.x;
+                i2[p].y = ok ? i2[p].y : old.y;
+              }
+            }
+            if (TAIL) {
+              if (sticks) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) st[k] = ok ? st[k] : bkt[k * kMcmcThreads];
+              }
+              if (isob) it_ = ok ? it_ : bkt[K * kMcmcThreads];
             }
           }
         }
@@ -601,10 +800,10 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
       }
     }
     if (valid && gl == 0 && a.status) {
-      uint32_t st = a.status[v];
-      if (!isfinite(lik)) st |= BPX_VOX_NONFINITE_ENERGY;
-      if (bad) st |= BPX_VOX_NONFINITE_DATA;
-      a.status[v] = st;
+      uint32_t stt = a.status[v];
+      if (!isfinite(lik)) stt |= BPX_VOX_NONFINITE_ENERGY;
+      if (bad) stt |= BPX_VOX_NONFINITE_DATA;
+      a.status[v] = stt;
     }
     __syncwarp();
   }
@@ -705,8 +904,9 @@ template <int MODEL, int K, bool RIC, int TPV, int MPL>
 cudaError_t launch_mcmc_t(const McmcArgs& a, cudaStream_t s) {
   auto kern = mcmc_kernel<MODEL, K, RIC, TPV, MPL>;
   constexpr int NS = 6 + 3 * K, GPB = kMcmcThreads / TPV;
-  const size_t smem = (size_t)(a.gradnonlin ? GPB : 1) * a.ndir * sizeof(float4) +
-                      (size_t)(K + 1) * MPL * kMcmcThreads * sizeof(float) + (size_t)GPB * NS * 8;
+  constexpr int NP = MPL / 2;
+  const size_t smem = (size_t)(a.gradnonlin ? GPB : 1) * TPV * MPL * sizeof(float4) +
+                      (size_t)(2 * NP + 1) * (K + 1) * kMcmcThreads * sizeof(float) + (size_t)GPB * NS * 8;
   if (smem > 48 * 1024) {
     cudaError_t ea = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (ea != cudaSuccess) return ea;
