@@ -113,6 +113,8 @@ McmcLayout pick_layout(const bpx_options* o, int ndir) {
 
 }  // namespace
 
+void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
 int sm_count() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return 1;

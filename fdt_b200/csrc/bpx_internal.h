@@ -13,6 +13,7 @@ constexpr int kMcmcThreads = 128;  // 4 warps
 constexpr int kMcmcMinBlocks = 3;  // register cap for 12 resident warps per SM
 
 int sm_count();  // multiprocessors of the current device (cached per device)
+void set_last_error(const char* msg);  // message returned by bpx_last_error() on this thread
 
 struct FitArgs {
   int nvox, ndir;

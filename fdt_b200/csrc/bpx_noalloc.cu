@@ -1,0 +1,97 @@
+// bpx_noalloc.cu -- the allocation-free pipeline entry (bpx_xfibres_noalloc_dev).
+//
+// Same stages as bpx_xfibres_dev (bpx_api.cu), but the intermediates live in a file-scope
+// __device__ array instead of the grow-only workspace, so the call never allocates device memory.
+// Host code must not pass the array's name to a kernel (in host code it names a host-side stand-in);
+// its device address is resolved once per device with cudaGetSymbolAddress.
+#include <mutex>
+#include <string>
+
+#include "bpx.h"
+#include "bpx_internal.h"
+
+namespace {
+
+constexpr size_t kScratchBytes = BPX_NOALLOC_SCRATCH_BYTES;
+constexpr int kMaxDevices = 64;
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+std::mutex g_mutex;
+void* g_scratch_dev[kMaxDevices] = {nullptr};
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+size_t scratch_bytes(const bpx_options* o, size_t nvox, bool own_status) {
+  const size_t np = (size_t)bpx_nparams_fit(o), ns = (size_t)bpx_nsamples(o);
+  return align256(nvox * np * 4) + align256(nvox * 4) + align256((size_t)BPX_NREC(o->nfibres) * ns * nvox * 4) +
+         (own_status ? align256(nvox * 4) : 0);
+}
+
+}  // namespace
+
+extern "C" bpx_status bpx_xfibres_noalloc_dev(const bpx_options* opts, const bpx_volume* vol, bpx_outputs* out,
+                                              void* stream) {
+  if (!opts || !vol || !out) {
+    bpx::set_last_error("bpx_xfibres_noalloc_dev: NULL opts, vol or out");
+    return BPX_ERR_INVALID_ARG;
+  }
+  if (opts->nfibres < 1 || opts->nfibres > BPX_MAX_FIBRES || opts->sampleevery < 1 || vol->nvox < 0)
+    return bpx_xfibres_dev(opts, vol, out, stream);  // its argument checks report the error
+  if (vol->nvox == 0) return BPX_OK;
+  const bool own_status = out->status == nullptr;
+  const size_t need = scratch_bytes(opts, (size_t)vol->nvox, own_status);
+  if (need > kScratchBytes) {
+    size_t lo = 0, hi = (size_t)vol->nvox;  // largest voxel count that fits
+    while (lo < hi) {
+      const size_t mid = (lo + hi + 1) / 2;
+      if (scratch_bytes(opts, mid, own_status) <= kScratchBytes)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const std::string msg = "bpx_xfibres_noalloc_dev: " + std::to_string(vol->nvox) + " voxels need " +
+                            std::to_string(need) + " bytes of scratch; the allocation-free entry holds " +
+                            std::to_string(kScratchBytes) + " bytes, i.e. at most " + std::to_string(lo) +
+                            " voxels for these options";
+    bpx::set_last_error(msg.c_str());
+    return BPX_ERR_UNSUPPORTED;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    bpx::set_last_error("bpx_xfibres_noalloc_dev: no usable CUDA device");
+    return BPX_ERR_NO_DEVICE;
+  }
+  void* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_mutex);
+    if (!g_scratch_dev[dev]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || !p) {
+        const std::string msg = std::string("bpx_xfibres_noalloc_dev: cudaGetSymbolAddress failed: ") +
+                                cudaGetErrorString(e);
+        bpx::set_last_error(msg.c_str());
+        return BPX_ERR_CUDA;
+      }
+      g_scratch_dev[dev] = p;
+    }
+    base = g_scratch_dev[dev];
+  }
+  const size_t nvox = (size_t)vol->nvox;
+  const size_t np = (size_t)bpx_nparams_fit(opts), ns = (size_t)bpx_nsamples(opts);
+  char* p = (char*)base;
+  float* params = (float*)p;
+  p += align256(nvox * np * 4);
+  float* tau = (float*)p;
+  p += align256(nvox * 4);
+  float* rec = (float*)p;
+  p += align256((size_t)BPX_NREC(opts->nfibres) * ns * nvox * 4);
+  uint32_t* status = own_status ? (uint32_t*)p : out->status;
+  bpx_status st = BPX_OK;
+  if (opts->rician) st = bpx_prepare_data_dev(vol->nvox, vol->ndir, const_cast<float*>(vol->data), stream);
+  if (st == BPX_OK) st = bpx_fit_dev(opts, vol, params, tau, status, stream);
+  if (st == BPX_OK) st = bpx_mcmc_dev(opts, vol, params, tau, rec, status, stream);
+  if (st == BPX_OK) st = bpx_finish_dev(opts, vol->nvox, rec, out, stream);
+  return st;
+}

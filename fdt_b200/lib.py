@@ -38,6 +38,7 @@ _SIGS = {
     "bpx_mcmc_layouts": (C.c_int32, [C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32]),
     "bpx_release_workspace": (C.c_int, []),
     "bpx_measure_pipes": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "bpx_xfibres_noalloc_dev": (C.c_int, [C.POINTER(Options), C.POINTER(Volume), C.POINTER(Outputs), C.c_void_p]),
 }
 
 _lib = None

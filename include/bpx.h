@@ -208,6 +208,35 @@ int32_t bpx_mcmc_layouts(int32_t* tpv, int32_t* mpl, int32_t max);
  */
 bpx_status bpx_measure_pipes(double* mufu_ops_per_s, double* fma_ops_per_s);
 
+/*
+ * Allocation-free variant of bpx_xfibres_dev.  No counterpart in the reference: xfibres_gpu
+ * allocates its working memory (thrust vectors) on every call.
+ *
+ * Some callers cannot call cudaMalloc once they are running: frameworks that reserve the device
+ * memory up front for their own pool (a later cudaMalloc fails or fragments that pool), and
+ * latency-sensitive services for which cudaMalloc's implicit device synchronisation would stall
+ * every other stream.  This entry performs the whole pipeline (--rician data clean-up, fits, MCMC,
+ * finishing) with its intermediates (fit parameters, tau, MCMC records, status) in a file-scope
+ * __device__ array of BPX_NOALLOC_SCRATCH_BYTES (40 MiB), which every GPU that loads the library
+ * keeps until the process exits.  It calls no cudaMalloc, cudaFree or allocating library routine.
+ *
+ * Size limit: the intermediates take 4*(P + 2 + (6+3*nfib)*nsamples) bytes per voxel, each
+ * block rounded up to 256 bytes (P = bpx_nparams_fit); larger volumes are rejected with
+ * BPX_ERR_UNSUPPORTED and a message giving the maximum voxel count for the options.  At the
+ * whole-brain options (model 2, 3 fibres, f0, rician, 50 samples) that is 13,700 voxels, more than
+ * one 12,800-voxel subpart of xfibres_gpu.
+ *
+ * The first call on a device resolves the array's device address (cudaGetSymbolAddress, with that
+ * device current); make that first call before any stream capture.  All calls share the one array
+ * and it keeps the last call's contents; every element a call reads it has written first, so no
+ * clearing is needed, but calls that overlap on the GPU (different streams, or threads) race on
+ * the array and must be serialised by the caller.  Inputs and outputs are caller-owned device
+ * buffers as for bpx_xfibres_dev; `data` is modified in place under --rician.
+ */
+#define BPX_NOALLOC_SCRATCH_BYTES (40u * 1024u * 1024u)
+bpx_status bpx_xfibres_noalloc_dev(const bpx_options* opts, const bpx_volume* vol, bpx_outputs* out,
+                                   void* stream);
+
 /* Free the per-device workspace cache of the current device. */
 bpx_status bpx_release_workspace(void);
 
