@@ -9,10 +9,12 @@
 //   * the f0 plausibility re-fit and mix_params (CUDA/xfibres_gpu.cu:207-339,552-576),
 //   * calculate_tau with its residual kernels (CUDA/diffmodels.cu:259-347).
 //
-// Design: measurements are strided over the 32 lanes; every lane keeps its Jacobian row and
-// its partial J^T J / J^T r sums in registers; sums are combined with xor-butterfly shuffles so
-// that every lane holds identical totals and takes identical LM decisions (no shared memory, no
-// block barriers).  The damped normal equations are solved in FP64 with rows spread over lanes.
+// Design: measurements are strided over the 32 lanes.  Scalar sums (cost, DTI moments) are
+// combined with xor-butterfly shuffles so that every lane holds identical totals and takes
+// identical LM decisions.  The Gauss-Newton normal equations J^T J, J^T r are contracted on the
+// FP64 tensor cores (mma.sync m8n8k4 .f64) from Jacobian rows staged in a per-warp
+// shared-memory tile, and kept there between LM steps; the damped system is solved in FP64
+// with its rows spread over lanes.  Warps of a block take voxels from a shared counter.
 //
 // Precision: everything is FP64 -- parameters, model values, residuals, cost, gradient and the
 // Gauss-Newton Hessian.  The reference's CPU fits are FP64, and on near-singular fits (a small
@@ -50,11 +52,13 @@ struct Meas {
 // ------------------------------------------------------------------------------------------
 template <int P>
 __device__ __forceinline__ void warp_solve(double (&row)[P], double rhs, double (&x)[P], int lane) {
+  double inv_pivot = 0.0;  // lane k keeps 1 / (pivot k) for the back substitution
 #pragma unroll
   for (int k = 0; k < P; ++k) {
-    const double akk = __shfl_sync(0xffffffffu, row[k], k);
+    const double inv = 1.0 / __shfl_sync(0xffffffffu, row[k], k);
     const double rk = __shfl_sync(0xffffffffu, rhs, k);
-    const double m = row[k] / akk;
+    if (lane == k) inv_pivot = inv;
+    const double m = row[k] * inv;
     const bool below = lane > k;
 #pragma unroll
     for (int j = k + 1; j < P; ++j) {
@@ -68,8 +72,16 @@ __device__ __forceinline__ void warp_solve(double (&row)[P], double rhs, double 
     double s = rhs;
 #pragma unroll
     for (int j = i + 1; j < P; ++j) s -= row[j] * x[j];
-    x[i] = __shfl_sync(0xffffffffu, s / row[i], i);
+    x[i] = __shfl_sync(0xffffffffu, s * inv_pivot, i);
   }
+}
+
+// D += A B for one 8x8x4 FP64 tensor-core tile (mma.sync m8n8k4 .f64): lane l holds A[l/4][l%4],
+// B[l%4][l/4] and D[l/4][2(l%4) + {0,1}].
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
 }
 
 // Symmetric eigen-decomposition of a small matrix (n <= 3) by cyclic Jacobi, FP64; eigenvalues
@@ -556,67 +568,94 @@ __device__ double cost(const Meas& ms, const Real (&p)[LmShape<KIND, K, F0>::P],
   return group_sum<32>(acc);
 }
 
+// Gauss-Newton normal equations at p, left in the warp's staging area st as the 16x16 matrix
+// N = [J | r]^T [J | r] (row stride kNormLd): N[i][j] for i,j < P is (J^T J)_ij with the Hessian's
+// S0 column (J0h), N[i][P] is (J^T r)_i, r = S - y.  The rows of [J | r] are written to shared
+// memory 32 measurements at a time (one per lane, stored column-major with stride kStageLd, which
+// makes both the stores and the fragment loads bank-conflict free) and contracted on the FP64
+// tensor cores in 8x8x4 tiles: the upper 8x8 block alone when P+1 <= 8, else the three blocks of
+// the upper triangle.  Replaces the per-lane outer products and 32-lane butterflies of
+// P(P+1)/2 + P partial sums (CUDA/PVM_multi.cu:371-465 computes the same sums serially).
+constexpr int kStageLd = 36;                      // column stride (doubles) of the staged [J | r]
+constexpr int kNormLd = 17;                       // row stride (doubles) of N
+constexpr int kStageDoubles = 16 * kStageLd;      // per warp: 4.5 KB
+static_assert(16 * kNormLd <= 8 * kStageLd, "N must not overlap staged columns 8..15");
+
+template <int KIND, int K, bool F0>
+__device__ void normal_eqs(const Meas& ms, const Real (&p)[LmShape<KIND, K, F0>::P], int lane, int gbo, Real R,
+                           Real invR, double* st) {
+  constexpr int P = LmShape<KIND, K, F0>::P;
+  constexpr bool kWide = P + 1 > 8;
+  Pre<KIND, K, F0> q;
+  precompute<KIND, K, F0>(p, q);
+  double n00[2] = {0.0, 0.0}, n01[2] = {0.0, 0.0}, n11[2] = {0.0, 0.0};
+  const int fr = lane >> 2, fk = lane & 3;  // fragment row (parameter) and k (measurement) of this lane
+  for (int m0 = 0; m0 < ms.M; m0 += 32) {
+    const int m = m0 + lane;
+    Real J[P], J0h = 0.0, diff = 0.0;
+    if (m < ms.M) {
+      const Real sig = point<KIND, K, F0, true>(q, p, ms.gx[m], ms.gy[m], ms.gz[m], ms.b[m], gbo, R, invR, J, J0h);
+      diff = sig - (Real)ms.y[m];
+    } else {
+#pragma unroll
+      for (int i = 0; i < P; ++i) J[i] = 0.0;
+    }
+    J[0] = J0h;
+    __syncwarp();  // the previous chunk's fragment loads are done
+#pragma unroll
+    for (int c = 0; c < P; ++c) st[c * kStageLd + lane] = J[c];
+    st[P * kStageLd + lane] = diff;
+    __syncwarp();
+#pragma unroll
+    for (int k0 = 0; k0 < 32; k0 += 4) {
+      const double lo = st[fr * kStageLd + k0 + fk];
+      dmma_8x8x4(n00, lo, lo);
+      if (kWide) {
+        const double hi = st[(8 + fr) * kStageLd + k0 + fk];
+        dmma_8x8x4(n01, lo, hi);
+        dmma_8x8x4(n11, hi, hi);
+      }
+    }
+  }
+  __syncwarp();
+  const int c0 = 2 * fk;
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    st[fr * kNormLd + c0 + i] = n00[i];
+    if (kWide) {
+      st[fr * kNormLd + 8 + c0 + i] = n01[i];
+      st[(8 + c0 + i) * kNormLd + fr] = n01[i];
+      st[(8 + fr) * kNormLd + 8 + c0 + i] = n11[i];
+    }
+  }
+  __syncwarp();
+}
+
 // LM driver (CUDA/levenberg_marquardt.cu:57-122): lambda0 = 0.1, x/÷ 10, converged when
 // 2|dcf| <= 1e-8 (|cf_old|+|cf_new|+2e-16), stopped when lambda > 1e20 or after 200 successful
-// iterations (the iteration counter advances only on success).
+// iterations (the iteration counter advances only on success).  Gradient 2 J^T r and Hessian
+// 2 J^T J come from normal_eqs after every successful step and stay in st between steps.
 template <int KIND, int K, bool F0>
-__device__ int lm_run(const Meas& ms, Real (&p)[LmShape<KIND, K, F0>::P], int lane, int gbo, Real R, Real invR) {
+__device__ int lm_run(const Meas& ms, Real (&p)[LmShape<KIND, K, F0>::P], int lane, int gbo, Real R, Real invR,
+                      double* st) {
   constexpr int P = LmShape<KIND, K, F0>::P;
-  constexpr int NH = LmShape<KIND, K, F0>::NH;
   double lambda = 0.1;
   const double cftol = 1.0e-8, ltol = 1.0e20;
   double pcf = cost<KIND, K, F0>(ms, p, lane, gbo, R, invR);
   int niter = 0, iters = 0;
   bool success = true;
-  double Hrow[P], grow = 0.0;
+  double gsign = 1.0;  // PVM_multi's gradient S0 entry carries sign(S0) (CUDA/PVM_multi.cu:376)
+  const int row = lane < P ? lane : 0;
   while (!(success && niter++ >= 200)) {
     ++iters;
     if (success) {
-      Pre<KIND, K, F0> q;
-      precompute<KIND, K, F0>(p, q);
-      double H[NH];
-      double g[P];
-#pragma unroll
-      for (int i = 0; i < NH; ++i) H[i] = 0.0;
-#pragma unroll
-      for (int i = 0; i < P; ++i) g[i] = 0.0;
-      for (int m = lane; m < ms.M; m += 32) {
-        Real J[P], J0h;
-        const Real sig = point<KIND, K, F0, true>(q, p, ms.gx[m], ms.gy[m], ms.gz[m], ms.b[m], gbo, R, invR, J, J0h);
-        const Real diff = sig - (Real)ms.y[m];
-#pragma unroll
-        for (int i = 0; i < P; ++i) g[i] += 2.0 * J[i] * diff;
-        J[0] = J0h;  // the Hessian's S0 entry (differs from the gradient's only for PVM_multi)
-        int e = 0;
-#pragma unroll
-        for (int i = 0; i < P; ++i)
-#pragma unroll
-          for (int j = i; j < P; ++j) H[e++] += 2.0 * J[i] * J[j];
-      }
-#pragma unroll
-      for (int i = 0; i < NH; ++i) H[i] = group_sum<32>(H[i]);
-#pragma unroll
-      for (int i = 0; i < P; ++i) g[i] = group_sum<32>(g[i]);
-      // lane i keeps row i of the Hessian and g[i]
-      grow = 0.0;
-#pragma unroll
-      for (int j = 0; j < P; ++j) Hrow[j] = 0.0;
-      int e = 0;
-#pragma unroll
-      for (int i = 0; i < P; ++i)
-#pragma unroll
-        for (int j = i; j < P; ++j) {
-          if (lane == i) Hrow[j] = H[e];
-          if (lane == j) Hrow[i] = H[e];
-          ++e;
-        }
-#pragma unroll
-      for (int i = 0; i < P; ++i)
-        if (lane == i) grow = g[i];
+      normal_eqs<KIND, K, F0>(ms, p, lane, gbo, R, invR, st);
+      if (KIND == kMulti && lane == 0) gsign = pm1d(p[0]);
     }
     double A[P];
 #pragma unroll
-    for (int j = 0; j < P; ++j) A[j] = Hrow[j] + ((lane == j) ? lambda : 0.0);
+    for (int j = 0; j < P; ++j) A[j] = 2.0 * st[row * kNormLd + j] + ((lane == j) ? lambda : 0.0);
+    const double grow = 2.0 * gsign * st[row * kNormLd + P];
     double x[P];
     warp_solve<P>(A, grow, x, lane);
     Real step[P];
@@ -922,7 +961,7 @@ __device__ __forceinline__ Real predict_final(int model, const Real* q, int o, b
 // the fit kernel: one warp per voxel, grid-stride over voxels
 // ------------------------------------------------------------------------------------------
 template <int K, bool F0>
-__device__ void fit_one(const FitArgs& a, int v, int lane) {
+__device__ void fit_one(const FitArgs& a, int v, int lane, double* st) {
   constexpr int NPOUT = 2 + 3 * K + (F0 ? 1 : 0);  // model 1 layout
   const int M = a.ndir;
   Meas ms;
@@ -957,14 +996,14 @@ __device__ void fit_one(const FitArgs& a, int v, int lane) {
     if (a.nonlin) {
       Real p[LmShape<kSingle, K, F0>::P];
       start_single<K, F0>(dt, p);
-      lm_run<kSingle, K, F0>(ms, p, lane, 0, R, invR);
+      lm_run<kSingle, K, F0>(ms, p, lane, 0, R, invR, st);
       finalise<kSingle, K, F0>(p);
 #pragma unroll
       for (int i = 0; i < NPOUT; ++i) res[i] = p[i];
       if (F0 && ((K > 0 && p[2] < 0.05) || p[1] > 0.007 || p[NPOUT - 1] > 0.4)) {
         Real p2[LmShape<kSingle, K, false>::P];
         start_single<K, false>(dt, p2);
-        lm_run<kSingle, K, false>(ms, p2, lane, 0, R, invR);
+        lm_run<kSingle, K, false>(ms, p2, lane, 0, R, invR, st);
         finalise<kSingle, K, false>(p2);
 #pragma unroll
         for (int i = 0; i < NPOUT - 1; ++i) res[i] = p2[i];
@@ -974,14 +1013,14 @@ __device__ void fit_one(const FitArgs& a, int v, int lane) {
     } else {
       Real p[LmShape<kSingleC, K, F0>::P];
       start_single_c<K, F0>(dt, ms, lane, p);
-      lm_run<kSingleC, K, F0>(ms, p, lane, 0, R, invR);
+      lm_run<kSingleC, K, F0>(ms, p, lane, 0, R, invR, st);
       finalise<kSingleC, K, F0>(p);
 #pragma unroll
       for (int i = 0; i < NPOUT; ++i) res[i] = p[i];
       if (F0 && ((K > 0 && p[2] < 0.05) || p[1] > 0.007 || p[NPOUT - 1] > 0.4)) {
         Real p2[LmShape<kSingleC, K, false>::P];
         start_single_c<K, false>(dt, ms, lane, p2);
-        lm_run<kSingleC, K, false>(ms, p2, lane, 0, R, invR);
+        lm_run<kSingleC, K, false>(ms, p2, lane, 0, R, invR, st);
         finalise<kSingleC, K, false>(p2);
 #pragma unroll
         for (int i = 0; i < NPOUT - 1; ++i) res[i] = p2[i];
@@ -993,11 +1032,11 @@ __device__ void fit_one(const FitArgs& a, int v, int lane) {
     constexpr int NPM = LmShape<kMulti, K, F0>::P;
     Real s[LmShape<kSingle, K, F0>::P];
     start_single<K, F0>(dt, s);
-    lm_run<kSingle, K, F0>(ms, s, lane, 0, R, invR);
+    lm_run<kSingle, K, F0>(ms, s, lane, 0, R, invR, st);
     finalise<kSingle, K, F0>(s);
     Real p[NPM];
     start_multi<K, F0>(s, p);
-    lm_run<kMulti, K, F0>(ms, p, lane, gbo, R, invR);
+    lm_run<kMulti, K, F0>(ms, p, lane, gbo, R, invR, st);
     finalise<kMulti, K, F0>(p);
 #pragma unroll
     for (int i = 0; i < NPM; ++i) res[i] = p[i];
@@ -1005,11 +1044,11 @@ __device__ void fit_one(const FitArgs& a, int v, int lane) {
       // GPU re-fit path: PVM_single_c then PVM_multi (CUDA/xfibres_gpu.cu:331-333)
       Real c[LmShape<kSingleC, K, false>::P];
       start_single_c<K, false>(dt, ms, lane, c);
-      lm_run<kSingleC, K, false>(ms, c, lane, 0, R, invR);
+      lm_run<kSingleC, K, false>(ms, c, lane, 0, R, invR, st);
       finalise<kSingleC, K, false>(c);
       Real p2[LmShape<kMulti, K, false>::P];
       start_multi<K, false>(c, p2);
-      lm_run<kMulti, K, false>(ms, p2, lane, gbo, R, invR);
+      lm_run<kMulti, K, false>(ms, p2, lane, gbo, R, invR, st);
       finalise<kMulti, K, false>(p2);
 #pragma unroll
       for (int i = 0; i < NPM - 1; ++i) res[i] = p2[i];
@@ -1042,11 +1081,27 @@ __device__ void fit_one(const FitArgs& a, int v, int lane) {
   if (lane == 0 && a.status) a.status[v] = refit ? BPX_VOX_F0_REFIT : 0u;
 }
 
+// Each block owns kFitVoxPerBlock consecutive voxels; its warps take the next one from a
+// shared-memory counter as they finish, so a voxel whose fit runs 200 iterations holds up one
+// warp instead of a fixed share of the block's voxels.
 template <int K, bool F0>
-__global__ void __launch_bounds__(kFitThreads) fit_kernel(FitArgs a) {
-  const int lane = threadIdx.x & 31;
-  const int warps = blockDim.x >> 5;
-  for (int v = blockIdx.x * warps + (threadIdx.x >> 5); v < a.nvox; v += gridDim.x * warps) fit_one<K, F0>(a, v, lane);
+__global__ void __launch_bounds__(kFitThreads, kFitMinBlocks) fit_kernel(FitArgs a) {
+  __shared__ double stage[kFitThreads / 32][kStageDoubles];
+  __shared__ int next;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double* st = stage[w];
+  for (int i = lane; i < kStageDoubles; i += 32) st[i] = 0.0;
+  const int v0 = blockIdx.x * kFitVoxPerBlock;
+  const int v1 = min(v0 + kFitVoxPerBlock, a.nvox);
+  if (threadIdx.x == 0) next = v0 + kFitThreads / 32;
+  __syncthreads();
+  int v = v0 + w;
+  while (v < v1) {
+    fit_one<K, F0>(a, v, lane, st);
+    int nv = 0;
+    if (lane == 0) nv = atomicAdd(&next, 1);
+    v = __shfl_sync(0xffffffffu, nv, 0);
+  }
 }
 
 // remove_NonPositive_entries (CUDA/xfibres_gpu.cu:350-367), one warp per voxel
@@ -1078,11 +1133,7 @@ __global__ void __launch_bounds__(kFitThreads) prepare_kernel(int nvox, int ndir
 // ------------------------------------------------------------------------------------------
 template <int K, bool F0>
 static cudaError_t launch_fit_kf(const FitArgs& a, cudaStream_t s) {
-  const int warps = kFitThreads / 32;
-  int grid = (a.nvox + warps - 1) / warps;
-  const int cap = sm_count() * 16;
-  if (grid > cap) grid = cap;
-  if (grid < 1) grid = 1;
+  const int grid = (a.nvox + kFitVoxPerBlock - 1) / kFitVoxPerBlock;
   fit_kernel<K, F0><<<grid, kFitThreads, 0, s>>>(a);
   return cudaGetLastError();
 }

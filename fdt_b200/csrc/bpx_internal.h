@@ -8,7 +8,12 @@
 
 namespace bpx {
 
-constexpr int kFitThreads = 256;   // 8 warps, one voxel per warp
+constexpr int kFitThreads = 128;   // 4 warps, one voxel per warp at a time
+constexpr int kFitVoxPerBlock = 32;  // voxels a fit block shares out among its warps
+#ifndef BPX_FIT_MIN_BLOCKS
+#define BPX_FIT_MIN_BLOCKS 4
+#endif
+constexpr int kFitMinBlocks = BPX_FIT_MIN_BLOCKS;  // register cap: 65536 / (128 * 4) = 128 per thread
 constexpr int kMcmcThreads = 128;  // 4 warps
 constexpr int kMcmcMinBlocks = 3;  // register cap for 12 resident warps per SM
 
