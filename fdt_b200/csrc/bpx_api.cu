@@ -85,14 +85,14 @@ struct Workspace {
   size_t cap = 0;
 };
 std::mutex g_ws_mutex;
-Workspace g_ws[kMaxDevices];
+Workspace g_ws[kWorkspaceSlots][kMaxDevices];
 
 // grow-only per-device scratch (not thread-safe across concurrent users of one device)
-bpx_status workspace(size_t bytes, void** out) {
+bpx_status workspace(size_t bytes, void** out, int slot = kWsPipeline) {
   int dev = 0;
   BPX_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lk(g_ws_mutex);
-  Workspace& w = g_ws[dev % kMaxDevices];
+  Workspace& w = g_ws[slot][dev % kMaxDevices];
   if (w.cap < bytes) {
     if (w.ptr) BPX_CUDA(cudaFree(w.ptr));
     w.ptr = nullptr;
@@ -114,6 +114,12 @@ McmcLayout pick_layout(const bpx_options* o, int ndir) {
 }  // namespace
 
 void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+bpx_status api_fail(bpx_status st, const std::string& msg) { return fail(st, msg); }
+bpx_status api_cuda_fail(cudaError_t e, const char* where) { return cuda_fail(e, where); }
+bpx_status api_check_device() { return check_device(); }
+bpx_status api_check_opts(const bpx_options* o) { return check_opts(o); }
+bpx_status api_check_vol(const bpx_volume* v) { return check_vol(v, true); }
+bpx_status api_workspace(int slot, size_t bytes, void** out) { return workspace(bytes, out, slot); }
 
 int sm_count() {
   int dev = 0;
@@ -320,8 +326,9 @@ bpx_status bpx_fit_dev(const bpx_options* opts, const bpx_volume* vol, float* pa
   return BPX_OK;
 }
 
-bpx_status bpx_mcmc_dev(const bpx_options* opts, const bpx_volume* vol, const float* params, const float* tau,
-                        float* records, uint32_t* status, void* stream) {
+bpx_status bpx_mcmc_ex_dev(const bpx_options* opts, const bpx_volume* vol, const float* params, const float* tau,
+                           const float* props_in, float* props_out, int32_t freeze_props, float* records,
+                           uint32_t* status, void* stream) {
   bpx_status st = check_opts(opts);
   if (st == BPX_OK) st = check_vol(vol, true);
   if (st != BPX_OK) return st;
@@ -360,8 +367,16 @@ bpx_status bpx_mcmc_dev(const bpx_options* opts, const bpx_volume* vol, const fl
   a.R_fudge = opts->R_prior_fudge;
   a.seed = opts->seed;
   a.voxel_offset = vol->voxel_offset;
+  a.props_in = props_in;
+  a.props_out = props_out;
+  a.freeze_props = freeze_props;
   BPX_CUDA(launch_mcmc(a, opts->model, opts->nfibres, opts->rician != 0, lay, (cudaStream_t)stream));
   return BPX_OK;
+}
+
+bpx_status bpx_mcmc_dev(const bpx_options* opts, const bpx_volume* vol, const float* params, const float* tau,
+                        float* records, uint32_t* status, void* stream) {
+  return bpx_mcmc_ex_dev(opts, vol, params, tau, nullptr, nullptr, 0, records, status, stream);
 }
 
 bpx_status bpx_finish_dev(const bpx_options* opts, int32_t nvox, const float* records, bpx_outputs* out, void* stream) {
@@ -593,10 +608,12 @@ bpx_status bpx_release_workspace(void) {
   int dev = 0;
   BPX_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lk(g_ws_mutex);
-  Workspace& w = g_ws[dev % kMaxDevices];
-  if (w.ptr) BPX_CUDA(cudaFree(w.ptr));
-  w.ptr = nullptr;
-  w.cap = 0;
+  for (int slot = 0; slot < kWorkspaceSlots; ++slot) {
+    Workspace& w = g_ws[slot][dev % kMaxDevices];
+    if (w.ptr) BPX_CUDA(cudaFree(w.ptr));
+    w.ptr = nullptr;
+    w.cap = 0;
+  }
   return BPX_OK;
 }
 

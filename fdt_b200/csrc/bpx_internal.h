@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 #include "bpx.h"
@@ -19,6 +20,20 @@ constexpr int kMcmcMinBlocks = 3;  // register cap for 12 resident warps per SM
 
 int sm_count();  // multiprocessors of the current device (cached per device)
 void set_last_error(const char* msg);  // message returned by bpx_last_error() on this thread
+
+// C-ABI helpers shared by the entry-point files (bpx_api.cu): status with message, device and
+// argument checks, and the grow-only per-device workspaces (one per slot, so that a pipeline
+// stage can hold one while calling a stage that uses another).
+constexpr int kWorkspaceSlots = 3;
+constexpr int kWsPipeline = 0;  // fit parameters, tau, records, status of bpx_xfibres_dev
+constexpr int kWsNetwork = 1;   // the network's weights and activations
+constexpr int kWsLearned = 2;   // intermediates of the learned pipeline
+bpx_status api_fail(bpx_status st, const std::string& msg);
+bpx_status api_cuda_fail(cudaError_t e, const char* where);
+bpx_status api_check_device();
+bpx_status api_check_opts(const bpx_options* o);
+bpx_status api_check_vol(const bpx_volume* v);
+bpx_status api_workspace(int slot, size_t bytes, void** out);
 
 struct FitArgs {
   int nvox, ndir;
@@ -50,6 +65,9 @@ struct McmcArgs {
   int f0, ardf0, no_ard, all_ard;
   float fudge, R_mean, R_std, R_fudge;
   uint64_t seed, voxel_offset;
+  const float* props_in;  // [6+3K][nvox] initial proposal widths, or NULL for initialise_props
+  float* props_out;       // [6+3K][nvox] proposal widths after the last iteration, or NULL
+  int freeze_props;       // nonzero: no proposal adaptation (the widths stay as initialised)
 };
 
 struct EnergyArgs {

@@ -517,7 +517,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
 
     all_signals(d, dstd, R, true, true, false);
     float lik = lik_of(S0, f, f0, tau);
-    // initialise_props, acceptance counters
+    // initialise_props (or widths given per voxel), acceptance counters
     if (gl == 0) {
 #pragma unroll
       for (int q = 0; q < NS; ++q) {
@@ -527,6 +527,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
         if (q == kSlotDstd) pq = dstd / 10.f;
         if (q == kSlotTau) pq = tau / 2.f;
         if (q == kSlotR) pq = R / 10.f;
+        if (a.props_in) pq = a.props_in[(size_t)q * a.nvox + v];
         sprop[q] = pq;
         sacc[q] = 0;
       }
@@ -781,7 +782,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
       }
       // ---------------- update_proposals (CUDA/runmcmc_kernels.cu:1341-1395) ----------------
       // each slot is proposed once per iteration, so since the last update acc + rej = upe
-      if (((it + 1) % a.upe) == 0) {
+      if (!a.freeze_props && ((it + 1) % a.upe) == 0) {
         __syncwarp();
         if (gl == 0) {
           const float upe = (float)a.upe;
@@ -798,6 +799,10 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
         }
         __syncwarp();
       }
+    }
+    if (valid && gl == 0 && a.props_out) {
+#pragma unroll
+      for (int q = 0; q < NS; ++q) a.props_out[(size_t)q * a.nvox + v] = sprop[q];
     }
     if (valid && gl == 0 && a.status) {
       uint32_t stt = a.status[v];

@@ -39,6 +39,25 @@ _SIGS = {
     "bpx_release_workspace": (C.c_int, []),
     "bpx_measure_pipes": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "bpx_xfibres_noalloc_dev": (C.c_int, [C.POINTER(Options), C.POINTER(Volume), C.POINTER(Outputs), C.c_void_p]),
+    "bpx_mcmc_ex_dev": (C.c_int, [C.POINTER(Options), C.POINTER(Volume), C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "bpx_mlp_nin": (C.c_int32, [C.c_int32]),
+    "bpx_mlp_nparams": (C.c_int64, [C.c_int32]),
+    "bpx_mlp_features_dev": (C.c_int, [C.POINTER(Volume), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "bpx_mlp_forward_dev": (C.c_int, [C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "bpx_mlp_train_step_dev": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_void_p, C.c_void_p]),
+    "bpx_mlp_adam_dev": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
+                                   C.c_float, C.c_float, C.c_int32, C.c_void_p]),
+    "bpx_mlp_targets_dev": (C.c_int, [C.POINTER(Options), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p]),
+    "bpx_mlp_decode_dev": (C.c_int, [C.POINTER(Options), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_void_p]),
+    "bpx_xfibres_learned_dev": (C.c_int, [C.POINTER(Options), C.POINTER(Volume), C.c_void_p, C.POINTER(Outputs),
+                                          C.c_void_p]),
+    "bpx_gemm_bf16_dev": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
+                                    C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p]),
+    "bpx_mlp_poll_error": (C.c_int, [C.POINTER(C.c_int32)]),
 }
 
 _lib = None
@@ -120,6 +139,35 @@ def fit(opts: Options, data, bvecs, bvals):
     _check(load().bpx_fit_dev(C.byref(opts), C.byref(vol), _ptr(params), _ptr(tau), _ptr(status), _stream(torch)),
            "bpx_fit_dev")
     return params, tau, status
+
+
+def mcmc_ex(opts: Options, data, bvecs, bvals, params, tau=None, props_in=None, freeze: bool = False,
+            want_props: bool = False, voxel_offset: int = 0, status=None):
+    """MCMC with per-voxel proposal widths.  Returns (records, props_out or None)."""
+    torch = _torch()
+    nvox = data.shape[0]
+    rec = torch.zeros((nrec(opts.nfibres), opts.nsamples, nvox), device="cuda", dtype=torch.float32)
+    pout = torch.zeros((6 + 3 * opts.nfibres, nvox), device="cuda", dtype=torch.float32) if want_props else None
+    vol = make_volume(data, bvecs, bvals, voxel_offset)
+    _check(load().bpx_mcmc_ex_dev(C.byref(opts), C.byref(vol), _ptr(params), _ptr(tau), _ptr(props_in), _ptr(pout),
+                                  1 if freeze else 0, _ptr(rec), _ptr(status), _stream(torch)), "bpx_mcmc_ex_dev")
+    return rec, pout
+
+
+def gemm_bf16(a, b, M: int, N: int, K: int, a_mn: bool = False, b_mn: bool = False):
+    """C [M][N] fp32 = A B^T on the tcgen05 tensor cores; a, b are bf16 device tensors (see bpx_gemm_bf16_dev)."""
+    torch = _torch()
+    c = torch.zeros((M, N), device="cuda", dtype=torch.float32)
+    _check(load().bpx_gemm_bf16_dev(M, N, K, _ptr(a), a.shape[1], 1 if a_mn else 0, _ptr(b), b.shape[1],
+                                    1 if b_mn else 0, _ptr(c), N, _stream(torch)), "bpx_gemm_bf16_dev")
+    return c
+
+
+def poll_error() -> int:
+    """Reads and clears the tensor-core kernels' device error word (synchronous)."""
+    code = C.c_int32()
+    _check(load().bpx_mlp_poll_error(C.byref(code)), "bpx_mlp_poll_error")
+    return code.value
 
 
 def mcmc(opts: Options, data, bvecs, bvals, params, tau=None, voxel_offset: int = 0, status=None):

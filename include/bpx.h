@@ -237,6 +237,74 @@ bpx_status bpx_measure_pipes(double* mufu_ops_per_s, double* fma_ops_per_s);
 bpx_status bpx_xfibres_noalloc_dev(const bpx_options* opts, const bpx_volume* vol, bpx_outputs* out,
                                    void* stream);
 
+/*
+ * MCMC with per-voxel proposal widths (no counterpart in the reference).  As bpx_mcmc_dev, plus:
+ *   props_in   [6+3*nfib][nvox] starting proposal widths in slot order f0, tau, d, d_std, R, S0,
+ *              (th, ph, f) per fibre; NULL = initialise_props (CUDA/runmcmc_kernels.cu:430-460).
+ *   props_out  [6+3*nfib][nvox] widths after the last iteration, or NULL.
+ *   freeze_props  nonzero: no adaptation (the chain keeps the starting widths; a fixed-width
+ *              random-walk chain has the same target distribution).
+ */
+bpx_status bpx_mcmc_ex_dev(const bpx_options* opts, const bpx_volume* vol, const float* params,
+                           const float* tau, const float* props_in, float* props_out,
+                           int32_t freeze_props, float* records, uint32_t* status, void* stream);
+
+/*
+ * ---- Learned initialiser (no counterpart in the reference) ----
+ * A network nin -> 256 x 4 (GELU) -> 32 maps a voxel's signals, divided by the mean of its
+ * b <= 50 s/mm^2 measurements (S0_hat) and zero-padded to nin = 8*ceil(ndir/8), to the MCMC's
+ * starting state and per-voxel proposal widths.  BF16 weights and activations, FP32 accumulation,
+ * all contractions on the tcgen05 tensor cores.  Parameters: one FP32 vector, for layer l = 0..4
+ * W_l [n_l][k_l] then b_l [n_l], k = {nin,256,256,256,256}, n = {256,256,256,256,32}.
+ * Outputs: 0-2 f_k, 3-11 fibre unit vectors, 12 d*1e3, 13 d_std*1e3, 14 S0/S0_hat, 15 f0*10,
+ * 16 ln(tau*S0_hat^2), 17+q ln(normalised proposal width of MCMC slot q).
+ */
+#define BPX_MLP_WIDTH 256
+#define BPX_MLP_HIDDEN 4
+#define BPX_MLP_NOUT 32
+int32_t bpx_mlp_nin(int32_t ndir);
+int64_t bpx_mlp_nparams(int32_t ndir);
+
+/* x [nvox][nin] (bf16 bits) and s0hat [nvox]; per_voxel_bvals: bvals is [nvox][ndir]. */
+bpx_status bpx_mlp_features_dev(const bpx_volume* vol, int32_t per_voxel_bvals, uint16_t* x,
+                                float* s0hat, void* stream);
+/* out [nvox][32] = network(x). */
+bpx_status bpx_mlp_forward_dev(int32_t ndir, const float* params, int32_t nvox, const uint16_t* x,
+                               float* out, void* stream);
+/* One forward + backward pass over a batch: grads (same layout as params) and the mean loss
+ * (device float) of targets/tweights [batch][32] (weighted squared error; the direction blocks use
+ * the sign-invariant loss |u u^T - v v^T|^2 weighted by tweights[3+3k]). */
+bpx_status bpx_mlp_train_step_dev(int32_t ndir, const float* params, float* grads, int32_t batch,
+                                  const uint16_t* x, const float* targets, const float* tweights,
+                                  float* loss, void* stream);
+/* Adam update (bias-corrected; step counts from 1). */
+bpx_status bpx_mlp_adam_dev(int64_t n, float* params, const float* grads, float* m, float* v,
+                            float lr, float beta1, float beta2, float eps, int32_t step, void* stream);
+/* Training targets and weights [nvox][32] from fitted states (fit layout), tau (may be NULL) and
+ * adapted proposal widths [6+3K][nvox] (may be NULL: no width targets). */
+bpx_status bpx_mlp_targets_dev(const bpx_options* opts, int32_t nvox, const float* params,
+                               const float* tau, const float* props, const float* s0hat,
+                               float* targets, float* tweights, void* stream);
+/* Network outputs -> starting state params [nvox][P] (fit layout), tau [nvox], proposal widths
+ * props [6+3K][nvox] (tau, props may be NULL); status [nvox] (may be NULL) is cleared. */
+bpx_status bpx_mlp_decode_dev(const bpx_options* opts, int32_t nvox, const float* out,
+                              const float* s0hat, float* params, float* tau, float* props,
+                              uint32_t* status, void* stream);
+/* Learned pipeline: features -> network -> decode -> MCMC with the network's proposal widths
+ * frozen, opts->nburn burn-in -> finishing.  Same outputs as bpx_xfibres_dev. */
+bpx_status bpx_xfibres_learned_dev(const bpx_options* opts, const bpx_volume* vol,
+                                   const float* mlp_params, bpx_outputs* out, void* stream);
+
+/* C[M][N] (fp32, row-major, ldc) = A B^T on the tcgen05 tensor cores, bf16 operands: A is
+ * [M][lda] (a_mn = 0) or [K][lda] (a_mn = 1), B is [N][ldb] (b_mn = 0) or [K][ldb] (b_mn = 1).
+ * Leading dimensions and the contiguous extents must be multiples of 8. */
+bpx_status bpx_gemm_bf16_dev(int32_t M, int32_t N, int32_t K, const uint16_t* A, int32_t lda,
+                             int32_t a_mn, const uint16_t* B, int32_t ldb, int32_t b_mn, float* C,
+                             int32_t ldc, void* stream);
+/* Synchronously reads and clears the device error word of the tensor-core kernels (0 = none;
+ * 1 or 2 = a bounded wait for a TMA copy or an MMA gave up). */
+bpx_status bpx_mlp_poll_error(int32_t* code);
+
 /* Free the per-device workspace cache of the current device. */
 bpx_status bpx_release_workspace(void);
 
