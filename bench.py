@@ -4,9 +4,12 @@
 Workload (the whole-brain configuration): model 2 (Gamma-distributed diffusivity), 3 fibres,
 --rician --f0 --ardf0, 288 measurements (18 b=0 + 90 directions at b=1000/2000/3000),
 burn-in 1000, 1250 jumps, sample every 25, seeded synthetic voxels with SNR 25 generated from the
-forward model (no dataset exists for this path).  One step = the whole path (Rician data clean-up,
-LM fits + tau, MCMC burn-in + recording, sample finishing) over one chunk of voxels already
-resident in HBM.  The chunk (131072 voxels x 288 x 4 B = 151 MB) is larger than the 126 MB L2 and
+forward model (no dataset exists for this path).  One step = the whole path over one chunk of voxels already resident in HBM: for the plain form
+Rician data clean-up, LM fits + tau, MCMC (burn-in 1000) and sample finishing; for the learned form
+the data clean-up, the initialiser network (features, 5 tensor-core layers, decode), MCMC from the
+network's state and widths (burn-in 200) and finishing.  The headline value is the learned form's
+voxels/s; the plain form is timed beside it on the same chunks, and the accuracy block compares
+their posteriors on the same voxels (with a second plain run at another seed as the yardstick).  The chunk (131072 voxels x 288 x 4 B = 151 MB) is larger than the 126 MB L2 and
 the L2 is also flushed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -36,6 +39,9 @@ from fdt_b200.abi import Options  # noqa: E402
 METRIC = "voxels/s, learned-init vs plain MCMC on 1 B200 at matched dyad error"
 WORKLOAD = ("whole-brain: model 2, 3 fibres, rician+f0+ardf0, 288 measurements, burnin 1000, njumps 1250, "
             "sampleevery 25, plain LM-initialised chain")
+WORKLOAD_LEARNED = ("whole-brain: model 2, 3 fibres, rician+f0+ardf0, 288 measurements, njumps 1250, sampleevery 25; "
+                    "learned form (network start state and proposal widths, burnin 200) against the plain "
+                    "LM-initialised chain (burnin 1000)")
 
 
 def whole_brain_options() -> Options:
@@ -184,6 +190,14 @@ def cpu_baseline(seconds: float = 12.0) -> dict:
             "sample": f"{done} voxels of the whole-brain workload (full chain), {t_all:.1f} s on {cores} threads"}
 
 
+def learned_options(o: Options) -> Options:
+    """Options of the learned form: the plain options with burn-in 200 and another RNG seed."""
+    lo = Options.make(**{f: getattr(o, f) for f, _ in Options._fields_ if f != "reserved"})
+    lo.nburn = 200
+    lo.seed = o.seed + 1
+    return lo
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -194,23 +208,32 @@ def main():
     ap.add_argument("--ref-voxels", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--form", default="both", choices=["both", "plain", "learned"],
+                    help="forms to time (the headline value is the learned form's)")
+    ap.add_argument("--freeze", type=int, default=0, choices=[0, 1, 2],
+                    help="learned form: 0 network widths adapt, 1 frozen, 2 frozen after burn-in")
+    ap.add_argument("--weights", default=None, help="initialiser weights (default: the committed whole-brain set)")
     ap.add_argument("--prof", action="store_true",
-                    help="profiling case: run the steps only (no e2e, CPU baseline or pipe calibration)")
+                    help="profiling case: run the steps only (no e2e, CPU baseline, accuracy or calibration)")
     ap.add_argument("--nburn", type=int, default=None, help="override burn-in (profiling cases)")
     ap.add_argument("--njumps", type=int, default=None, help="override jumps (profiling cases)")
     args = ap.parse_args()
     if args.prof:
         args.no_e2e = True
         args.no_cpu_baseline = True
+        args.no_accuracy = True
     world, rank, local = dist_setup(args)
 
     if args.impl == "reference":
         run_reference(args, world, rank)
         return
 
+    import ctypes as C
+
     import torch
 
-    from fdt_b200 import lib
+    from fdt_b200 import learned, lib
 
     torch.cuda.set_device(local)
     pg = None
@@ -228,9 +251,16 @@ def main():
         o.nburn = args.nburn
     if args.njumps is not None:
         o.njumps = args.njumps
+    lo = learned_options(o)
     prot = synth.three_shell(18, 90)
     M = prot.ndir
     chunk = args.chunk
+    forms = ["plain", "learned"] if args.form == "both" else [args.form]
+    wpath = args.weights or learned.default_weights_path("whole_brain")
+    mlp_h, meta = learned.load_weights(wpath) if "learned" in forms else (None, None)
+    if mlp_h is not None and int(meta["ndir"]) != M:
+        raise SystemExit(f"{wpath}: trained for {int(meta['ndir'])} measurements, the workload has {M}")
+    mlp_d = torch.from_numpy(mlp_h).cuda() if mlp_h is not None else None
     # two distinct chunks per rank, alternated between steps
     chunks_h = []
     for c in range(2):
@@ -239,67 +269,109 @@ def main():
     bvecs = lib.to_device(prot.bvecs)
     bvals = lib.to_device(prot.bvals)
     chunks_d = [lib.to_device(y) for y in chunks_h]
-    work = [torch.empty_like(chunks_d[0]) for _ in range(2)]
-    np_fit = o.nparams_fit
-    ns = o.nsamples
-    params = torch.empty((chunk, np_fit), device="cuda")
+    work = torch.empty_like(chunks_d[0])
+    nin = learned.nin(M)
+    params = torch.empty((chunk, o.nparams_fit), device="cuda")
     tau = torch.empty(chunk, device="cuda")
     status = torch.zeros(chunk, device="cuda", dtype=torch.int32)
-    rec = torch.empty((6 + 3 * o.nfibres, ns, chunk), device="cuda")
-    outs = lib.alloc_outputs(o, chunk)
+    rec = torch.empty((6 + 3 * o.nfibres, o.nsamples, chunk), device="cuda")
+    x = torch.empty((chunk, nin), device="cuda", dtype=torch.bfloat16)
+    s0hat = torch.empty(chunk, device="cuda")
+    netout = torch.empty((chunk, 32), device="cuda")
+    props = torch.empty((6 + 3 * o.nfibres, chunk), device="cuda")
+    outs = {f: lib.alloc_outputs(o, chunk) for f in forms}
     flush = torch.empty(256 * 1024 * 1024 // 4, device="cuda")
     stream = torch.cuda.current_stream()
-    sptr = lib.C.c_void_p(stream.cuda_stream)
+    sptr = C.c_void_p(stream.cuda_stream)
 
-    import ctypes as C
-
-    def step(i, ev=None):
-        src = chunks_d[i % 2]
-        w = work[i % 2]
-        w.copy_(src)  # the path cleans the data in place under --rician
-        vol = lib.make_volume(w, bvecs, bvals, voxel_offset=(rank * 1_000_000_000) + i * chunk)
+    def plain_step(i, ev=None, opts=o, out=None):
+        work.copy_(chunks_d[i % 2])  # the path cleans the data in place under --rician
+        vol = lib.make_volume(work, bvecs, bvals, voxel_offset=(rank * 1_000_000_000) + i * chunk)
         if ev:
             ev[0].record(stream)
-        lib._check(L.bpx_prepare_data_dev(chunk, M, w.data_ptr(), sptr), "prepare")
-        lib._check(L.bpx_fit_dev(C.byref(o), C.byref(vol), params.data_ptr(), tau.data_ptr(), status.data_ptr(), sptr),
-                   "fit")
+        lib._check(L.bpx_prepare_data_dev(chunk, M, work.data_ptr(), sptr), "prepare")
+        lib._check(L.bpx_fit_dev(C.byref(opts), C.byref(vol), params.data_ptr(), tau.data_ptr(), status.data_ptr(),
+                                 sptr), "fit")
         if ev:
             ev[1].record(stream)
-        lib._check(L.bpx_mcmc_dev(C.byref(o), C.byref(vol), params.data_ptr(), tau.data_ptr(), rec.data_ptr(),
+        lib._check(L.bpx_mcmc_dev(C.byref(opts), C.byref(vol), params.data_ptr(), tau.data_ptr(), rec.data_ptr(),
                                   status.data_ptr(), sptr), "mcmc")
         if ev:
             ev[2].record(stream)
-        lib._check(L.bpx_finish_dev(C.byref(o), chunk, rec.data_ptr(), C.byref(outs[1]), sptr), "finish")
+        lib._check(L.bpx_finish_dev(C.byref(opts), chunk, rec.data_ptr(), C.byref((out or outs["plain"])[1]), sptr),
+                   "finish")
         if ev:
             ev[3].record(stream)
 
-    for i in range(args.warmup):
-        flush.zero_()
-        step(i)
-    torch.cuda.synchronize()
-    if pg:
-        pg.barrier()
+    def learned_step(i, ev=None):
+        work.copy_(chunks_d[i % 2])
+        vol = lib.make_volume(work, bvecs, bvals, voxel_offset=(rank * 1_000_000_000) + i * chunk)
+        if ev:
+            ev[0].record(stream)
+        lib._check(L.bpx_prepare_data_dev(chunk, M, work.data_ptr(), sptr), "prepare")
+        lib._check(L.bpx_mlp_features_dev(C.byref(vol), 0, x.data_ptr(), s0hat.data_ptr(), sptr), "features")
+        lib._check(L.bpx_mlp_forward_dev(M, mlp_d.data_ptr(), chunk, x.data_ptr(), netout.data_ptr(), sptr), "network")
+        lib._check(L.bpx_mlp_decode_dev(C.byref(lo), chunk, netout.data_ptr(), s0hat.data_ptr(), params.data_ptr(),
+                                        tau.data_ptr(), props.data_ptr(), status.data_ptr(), sptr), "decode")
+        if ev:
+            ev[1].record(stream)
+        lib._check(L.bpx_mcmc_ex_dev(C.byref(lo), C.byref(vol), params.data_ptr(), tau.data_ptr(), props.data_ptr(),
+                                     None, args.freeze, rec.data_ptr(), status.data_ptr(), sptr), "mcmc")
+        if ev:
+            ev[2].record(stream)
+        lib._check(L.bpx_finish_dev(C.byref(lo), chunk, rec.data_ptr(), C.byref(outs["learned"][1]), sptr), "finish")
+        if ev:
+            ev[3].record(stream)
+
+    steps_fn = {"plain": plain_step, "learned": learned_step}
+    launches = {"plain": 4, "learned": 6 + 6}  # learned: prepare, features, cast + 5 GEMMs, decode, mcmc, finish
+    timing = {}
     clocks = ClockSampler(local)
     clocks.start()
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
-    torch.cuda.synchronize()
-    for i in range(args.steps):
-        flush.zero_()  # L2 flush (256 MB write), outside the timed events
-        step(args.warmup + i, evs[i])
-    torch.cuda.synchronize()
+    for f in forms:
+        for i in range(args.warmup):
+            flush.zero_()
+            steps_fn[f](i)
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+        for i in range(args.steps):
+            flush.zero_()  # L2 flush (256 MB write), outside the timed events
+            steps_fn[f](args.warmup + i, evs[i])
+        torch.cuda.synchronize()
+        t = [sum(e[a].elapsed_time(e[a + 1]) for e in evs) / 1e3 for a in range(3)]
+        tt = torch.tensor([sum(t)] + t, device="cuda", dtype=torch.float64)
+        if pg:
+            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        timing[f] = tt.tolist()
     ck = clocks.stop()
-    t_fit = sum(e[0].elapsed_time(e[1]) for e in evs) / 1e3
-    t_mcmc = sum(e[1].elapsed_time(e[2]) for e in evs) / 1e3
-    t_fin = sum(e[2].elapsed_time(e[3]) for e in evs) / 1e3
-    t_step = t_fit + t_mcmc + t_fin
-    times = torch.tensor([t_step, t_fit, t_mcmc, t_fin], device="cuda", dtype=torch.float64)
-    if pg:
-        pg.all_reduce(times, op=pg.ReduceOp.MAX)
-    t_step, t_fit, t_mcmc, t_fin = times.tolist()
+    head = "learned" if "learned" in forms else "plain"
+    t_step, t_init, t_mcmc, t_fin = timing[head]
     vox_total = chunk * args.steps * world
     value = vox_total / t_step
+    ho = lo if head == "learned" else o
 
-    # ---- end to end through the host-buffer public entry (pinned host memory) ----
+    # ---- accuracy of the learned form against the plain chain on the same voxels ----
+    accuracy = None
+    if not args.no_accuracy and len(forms) == 2:
+        # the last timed step of each form ran on the same chunk; a second plain run with another
+        # seed gives the plain-vs-plain agreement the learned form is measured against
+        o2 = Options.make(**{f: getattr(o, f) for f, _ in Options._fields_ if f != "reserved"})
+        o2.seed = o.seed + 7
+        plain2 = lib.alloc_outputs(o, chunk)
+        plain_step(args.warmup + args.steps - 1, opts=o2, out=plain2)
+        torch.cuda.synchronize()
+        n_acc = min(chunk, 32768)
+        sub = lambda d: {k: v[..., :n_acc] for k, v in d.items()}  # noqa: E731  (voxel axis is last)
+        accuracy = {
+            "voxels": n_acc,
+            "learned_vs_plain": learned.summary(o, sub(outs["learned"][0]), sub(outs["plain"][0])),
+            "plain_vs_plain_other_seed": learned.summary(o, sub(plain2[0]), sub(outs["plain"][0])),
+            "f_se": "Monte-Carlo SE of each chain's mean (Geyer initial positive sequence), combined",
+        }
+
+    # ---- end to end through the host-buffer public entries (pinned host memory) ----
     e2e = None
     if not args.no_e2e:
         hp = [torch.from_numpy(y).pin_memory() for y in chunks_h]
@@ -314,7 +386,11 @@ def main():
             v.data, v.bvecs, v.bvals = hp[i % 2].data_ptr(), bh.ctypes.data, lh.ctypes.data
             v.grad = None
             v.voxel_offset = rank * 1_000_000_000 + i * chunk
-            lib._check(L.bpx_xfibres_host(C.byref(o), C.byref(v), C.byref(hout[1])), "xfibres_host")
+            if head == "learned":
+                lib._check(L.bpx_xfibres_learned_host(C.byref(lo), C.byref(v), mlp_h.ctypes.data, args.freeze,
+                                                      C.byref(hout[1])), "xfibres_learned_host")
+            else:
+                lib._check(L.bpx_xfibres_host(C.byref(o), C.byref(v), C.byref(hout[1])), "xfibres_host")
 
         host_step(0)
         if pg:
@@ -326,42 +402,55 @@ def main():
         te = torch.tensor([time.perf_counter() - t0], device="cuda", dtype=torch.float64)
         if pg:
             pg.all_reduce(te, op=pg.ReduceOp.MAX)
-        h2d = chunk * M * 4 + 4 * 4 * M
+        h2d = chunk * M * 4 + 4 * 4 * M + (mlp_h.nbytes if head == "learned" else 0)
         d2h = sum(t.numel() * t.element_size() for t in hout[0].values())
         e2e = {"value": chunk * n_e2e * world / te.item(), "unit": "voxels/s", "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "steps": n_e2e}
+               "d2h_bytes_per_step": d2h, "steps": n_e2e, "entry": "bpx_xfibres_learned_host" if head == "learned"
+               else "bpx_xfibres_host"}
 
     if args.prof:
         if rank == 0:
-            print(json.dumps({"prof": True, "voxels": chunk, "mcmc_s_per_step": t_mcmc / args.steps,
-                              "fit_s_per_step": t_fit / args.steps}), flush=True)
+            print(json.dumps({"prof": True, "voxels": chunk, "timing": timing}), flush=True)
         return
     # ---- roofline of the dominant kernel (the MCMC chain) ----
     mufu_peak, fma_peak = lib.measure_pipes()
-    mufu_v, fp32_v = mcmc_work_per_voxel(o, M)
+    mufu_v, fp32_v = mcmc_work_per_voxel(ho, M)
     mcmc_per_launch_s = t_mcmc / args.steps
     achieved = mufu_v * chunk / mcmc_per_launch_s
     fp32_achieved = fp32_v * chunk / mcmc_per_launch_s
     roof_time = max(mufu_v * chunk / mufu_peak, fp32_v * chunk / fma_peak)
     roofline = {
         "bound": "sfu", "achieved": achieved / 1e9, "peak": mufu_peak / 1e9, "unit": "Gop/s",
-        "frac": achieved / mufu_peak, "traffic": None,
+        "frac": achieved / mufu_peak, "traffic": None, "kernel": "mcmc_kernel (burn-in + recording)",
         "fp32_achieved": fp32_achieved / 1e9, "fp32_peak": fma_peak / 1e9,
         "frac_of_roofline_time": roof_time / mcmc_per_launch_s,
         "peak_source": "measured on this GPU by bpx_measure_pipes (ex2.approx and FFMA issue-rate kernels)",
         "work_per_voxel": {"mufu": mufu_v, "fp32": fp32_v},
     }
     peaks = measured_peaks()
+    forms_out = {}
+    for f in forms:
+        ts_, ti, tm, tf = timing[f]
+        forms_out[f] = {"voxels_per_s": vox_total / ts_, "ms_per_step": 1e3 * ts_ / args.steps,
+                        "phases_s_per_step": {"init": ti / args.steps, "mcmc": tm / args.steps,
+                                              "finish": tf / args.steps},
+                        "nburn": (lo if f == "learned" else o).nburn, "gpu_launches_per_step": launches[f]}
     result = {
         "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_step / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "voxels_per_step_per_gpu": chunk, "ndir": M, "l2": "flushed between steps "
-                   "(256 MB write) and inputs (151 MB/step) larger than L2", "form": "plain (LM init, burnin 1000)"},
-        "phases_s_per_step": {"fit": t_fit / args.steps, "mcmc": t_mcmc / args.steps, "finish": t_fin / args.steps},
+        "config": {"workload": WORKLOAD_LEARNED if head == "learned" else WORKLOAD,
+                   "voxels_per_step_per_gpu": chunk, "ndir": M,
+                   "l2": "flushed between steps (256 MB write) and inputs (151 MB/step) larger than L2",
+                   "form": head, "freeze_props": args.freeze if head == "learned" else None,
+                   "weights": os.path.relpath(wpath, ROOT) if head == "learned" else None},
+        "forms": forms_out,
+        "learned_over_plain": (forms_out["learned"]["voxels_per_s"] / forms_out["plain"]["voxels_per_s"])
+        if len(forms) == 2 else None,
+        "accuracy": accuracy,
         "roofline": roofline,
         "e2e": e2e,
-        "gpu_launches": 4 * args.steps,
+        "gpu_launches": launches[head] * args.steps,
         "clocks": ck,
         "hbm_peak_gbs": peaks.get("hbm_gbs"),
     }

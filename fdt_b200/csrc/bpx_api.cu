@@ -369,6 +369,7 @@ bpx_status bpx_mcmc_ex_dev(const bpx_options* opts, const bpx_volume* vol, const
   a.voxel_offset = vol->voxel_offset;
   a.props_in = props_in;
   a.props_out = props_out;
+  if (freeze_props < 0 || freeze_props > 2) return fail(BPX_ERR_INVALID_ARG, "freeze_props must be 0, 1 or 2");
   a.freeze_props = freeze_props;
   BPX_CUDA(launch_mcmc(a, opts->model, opts->nfibres, opts->rician != 0, lay, (cudaStream_t)stream));
   return BPX_OK;
@@ -470,7 +471,14 @@ bpx_status bpx_xfibres_dev(const bpx_options* opts, const bpx_volume* vol, bpx_o
   return BPX_OK;
 }
 
-bpx_status bpx_xfibres_host(const bpx_options* opts, const bpx_volume* vol, bpx_outputs* host_out) {
+}  // extern "C"
+
+namespace {
+
+// Host-buffer pipeline: copies in, runs the plain (mlp == NULL) or the learned pipeline on a
+// private stream, copies the outputs back and synchronises.
+bpx_status xfibres_host_impl(const bpx_options* opts, const bpx_volume* vol, bpx_outputs* host_out, const float* mlp,
+                             int32_t freeze_props) {
   bpx_status st = check_opts(opts);
   if (st == BPX_OK) st = check_vol(vol, true);
   if (st != BPX_OK) return st;
@@ -491,7 +499,9 @@ bpx_status bpx_xfibres_host(const bpx_options* opts, const bpx_volume* vol, bpx_
   const size_t b_samp = align256(K * ns * nvox * 4);
   const size_t b_vox = align256(nvox * 4);
   const size_t b_vk = align256(K * nvox * 4), b_dy = align256(K * 3 * nvox * 4);
-  const size_t total = b_data + b_bvec + b_bval + b_grad + b_bvec_v + b_bval_v + 3 * b_samp + 7 * b_vox + b_vk + b_dy;
+  const size_t b_mlp = mlp ? align256((size_t)bpx_mlp_nparams(vol->ndir) * 4) : 0;
+  const size_t total =
+      b_data + b_bvec + b_bval + b_grad + b_bvec_v + b_bval_v + 3 * b_samp + 7 * b_vox + b_vk + b_dy + b_mlp;
   char* base = nullptr;
   BPX_CUDA(cudaMalloc(&base, total));
   cudaStream_t s = nullptr;
@@ -526,7 +536,9 @@ bpx_status bpx_xfibres_host(const bpx_options* opts, const bpx_volume* vol, bpx_
   d_out.status = (uint32_t*)take(b_vox);
   d_out.mean_f = (float*)take(b_vk);
   d_out.dyads = (float*)take(b_dy);
+  float* d_mlp = mlp ? (float*)take(b_mlp) : nullptr;
   auto run = [&]() -> bpx_status {
+    if (mlp) BPX_CUDA(cudaMemcpyAsync(d_mlp, mlp, (size_t)bpx_mlp_nparams(vol->ndir) * 4, cudaMemcpyHostToDevice, s));
     BPX_CUDA(cudaMemcpyAsync(d_data, vol->data, nvox * ndir * 4, cudaMemcpyHostToDevice, s));
     BPX_CUDA(cudaMemcpyAsync(d_bvec, vol->bvecs, 3 * ndir * 4, cudaMemcpyHostToDevice, s));
     BPX_CUDA(cudaMemcpyAsync(d_bval, vol->bvals, ndir * 4, cudaMemcpyHostToDevice, s));
@@ -542,7 +554,8 @@ bpx_status bpx_xfibres_host(const bpx_options* opts, const bpx_volume* vol, bpx_
       dv.bvecs = d_bvec_v;
       dv.bvals = d_bval_v;
     }
-    bpx_status s3 = bpx_xfibres_dev(opts, &dv, &d_out, s);
+    bpx_status s3 = mlp ? bpx_xfibres_learned_dev(opts, &dv, d_mlp, freeze_props, &d_out, s)
+                        : bpx_xfibres_dev(opts, &dv, &d_out, s);
     if (s3 != BPX_OK) return s3;
     const bpx_outputs& h = *host_out;
     const size_t samp = K * ns * nvox * 4, vox = nvox * 4;
@@ -566,6 +579,20 @@ bpx_status bpx_xfibres_host(const bpx_options* opts, const bpx_volume* vol, bpx_
   cudaStreamDestroy(s);
   cudaFree(base);
   return st;
+}
+
+}  // namespace
+
+extern "C" {
+
+bpx_status bpx_xfibres_host(const bpx_options* opts, const bpx_volume* vol, bpx_outputs* host_out) {
+  return xfibres_host_impl(opts, vol, host_out, nullptr, 0);
+}
+
+bpx_status bpx_xfibres_learned_host(const bpx_options* opts, const bpx_volume* vol, const float* mlp_params,
+                                    int32_t freeze_props, bpx_outputs* host_out) {
+  if (!mlp_params) return fail(BPX_ERR_INVALID_ARG, "mlp_params is NULL");
+  return xfibres_host_impl(opts, vol, host_out, mlp_params, freeze_props);
 }
 
 bpx_status bpx_measure_pipes(double* mufu_ops_per_s, double* fma_ops_per_s) {

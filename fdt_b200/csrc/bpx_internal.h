@@ -67,7 +67,7 @@ struct McmcArgs {
   uint64_t seed, voxel_offset;
   const float* props_in;  // [6+3K][nvox] initial proposal widths, or NULL for initialise_props
   float* props_out;       // [6+3K][nvox] proposal widths after the last iteration, or NULL
-  int freeze_props;       // nonzero: no proposal adaptation (the widths stay as initialised)
+  int freeze_props;       // 0: adapt (reference); 1: never adapt; 2: adapt during burn-in only
 };
 
 struct EnergyArgs {

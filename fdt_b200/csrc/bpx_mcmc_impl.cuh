@@ -782,7 +782,8 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
       }
       // ---------------- update_proposals (CUDA/runmcmc_kernels.cu:1341-1395) ----------------
       // each slot is proposed once per iteration, so since the last update acc + rej = upe
-      if (!a.freeze_props && ((it + 1) % a.upe) == 0) {
+      const bool adapt = a.freeze_props == 0 || (a.freeze_props == 2 && it < a.nburn);
+      if (adapt && ((it + 1) % a.upe) == 0) {
         __syncwarp();
         if (gl == 0) {
           const float upe = (float)a.upe;

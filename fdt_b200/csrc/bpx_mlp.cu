@@ -13,7 +13,7 @@
 // k = {nin, 256, 256, 256, 256}, n = {256, 256, 256, 256, 32}.
 //
 // Output vector (32): 0-2 f_k, 3-11 fibre unit vectors v_k, 12 d*1e3, 13 d_std*1e3, 14 S0/S0_hat,
-// 15 f0*10, 16 ln(tau*S0_hat^2), 17.. ln of the normalised proposal width of MCMC slot q
+// 15 f0*10, 16 ln(tau*S0_hat^2), 17.. ln of the normalised proposal width of MCMC slot q, in [-14, 2]
 // (q = 0..5+3K in the slot order f0, tau, d, d_std, R, S0, (th, ph, f)_k; widths of S0 are
 // divided by S0_hat, of d and d_std multiplied by 1e3, of tau divided by tau).
 #include <cuda_bf16.h>
@@ -36,6 +36,10 @@ constexpr int kWidth = BPX_MLP_WIDTH;
 constexpr int kLayers = BPX_MLP_HIDDEN + 1;
 constexpr int kOut = BPX_MLP_NOUT;
 constexpr int kOutProps = 17;  // first proposal-width output
+// Range of the normalised log widths.  A chain adapts the angle widths of a fibre whose fraction
+// is near zero without bound (every proposal is accepted; CUDA/runmcmc_kernels.cu caps them at
+// 1e10), but a width past e^2 (> 2 pi for an angle, > 1 for a fraction) proposes no differently.
+constexpr float kLogWidthMin = -14.f, kLogWidthMax = 2.f;
 constexpr int kMaxChunk = 32768;  // inference rows per pass (bounds the activation buffers)
 
 struct Geom {
@@ -250,7 +254,7 @@ __global__ void targets_kernel(Layout L, int nvox, const float* __restrict__ par
       if (q == kSlotD || q == kSlotDstd) pw *= 1e3f;
       if (q == kSlotTau) pw = tv > 0.f ? pw / tv : 0.f;
       if (on && pw > 0.f && isfinite(pw)) {
-        o[kOutProps + q] = logf(pw);
+        o[kOutProps + q] = fminf(fmaxf(logf(pw), kLogWidthMin), kLogWidthMax);
         w[kOutProps + q] = 0.1f;
       }
     }
@@ -305,7 +309,7 @@ __global__ void decode_kernel(Layout L, int nvox, const float* __restrict__ out,
   if (tau) tau[v] = tv;
   if (props) {
     for (int q = 0; q < L.ns; ++q) {
-      float pw = expf(fminf(fmaxf(o[kOutProps + q], -30.f), 10.f));
+      float pw = expf(fminf(fmaxf(o[kOutProps + q], kLogWidthMin), kLogWidthMax));
       if (q == kSlotS0) pw *= s0;
       if (q == kSlotD || q == kSlotDstd) pw *= 1e-3f;
       if (q == kSlotTau) pw *= tv;
@@ -597,11 +601,12 @@ bpx_status bpx_mlp_decode_dev(const bpx_options* opts, int32_t nvox, const float
 }
 
 bpx_status bpx_xfibres_learned_dev(const bpx_options* opts, const bpx_volume* vol, const float* mlp_params,
-                                   bpx_outputs* out, void* stream) {
+                                   int32_t freeze_props, bpx_outputs* out, void* stream) {
   bpx_status st = api_check_opts(opts);
   if (st == BPX_OK) st = api_check_vol(vol);
   if (st != BPX_OK) return st;
   if (!out || !mlp_params) return api_fail(BPX_ERR_INVALID_ARG, "out or mlp_params is NULL");
+  if (freeze_props < 0 || freeze_props > 2) return api_fail(BPX_ERR_INVALID_ARG, "freeze_props must be 0, 1 or 2");
   if (vol->nvox == 0) return BPX_OK;
   const int ns = bpx_nsamples(opts);
   if (ns < 1) return api_fail(BPX_ERR_INVALID_ARG, "no samples (njumps < sampleevery)");
@@ -639,7 +644,8 @@ bpx_status bpx_xfibres_learned_dev(const bpx_options* opts, const bpx_volume* vo
   if (st == BPX_OK) st = bpx_mlp_forward_dev(vol->ndir, mlp_params, vol->nvox, x, netout, stream);
   if (st == BPX_OK) st = bpx_mlp_decode_dev(opts, vol->nvox, netout, s0hat, params, tau, props, status, stream);
   if (st == BPX_OK)
-    st = bpx_mcmc_ex_dev(opts, vol, params, opts->rician ? tau : nullptr, props, nullptr, 1, rec, status, stream);
+    st = bpx_mcmc_ex_dev(opts, vol, params, opts->rician ? tau : nullptr, props, nullptr, freeze_props, rec, status,
+                         stream);
   if (st == BPX_OK) st = bpx_finish_dev(opts, vol->nvox, rec, out, stream);
   return st;
 }

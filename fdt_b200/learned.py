@@ -1,0 +1,368 @@
+"""The learned form: training the initialiser network on the GPU and running the learned pipeline.
+
+Training data are voxels the forward model generates on the GPU (bpx_synth_dev), labelled with
+their LM fits (bpx_fit_dev) and with the proposal widths a plain chain adapts to by the end of its
+burn-in (bpx_mcmc_ex_dev).  Every step of training -- forward, loss, backward, Adam -- runs in the
+library's own kernels (tcgen05 GEMMs with fused epilogues); PyTorch only holds device memory and
+gathers the mini-batches.
+
+The trained network replaces the LM initialiser and sets per-voxel proposal widths that are then
+frozen, so the chain needs a shorter burn-in; the plain LM-initialised chain with the full burn-in
+stays the fallback and the judge of its accuracy (see `compare`).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import math
+import os
+
+import numpy as np
+
+from . import lib
+from .abi import Options
+
+WIDTH, HIDDEN, NOUT = 256, 4, 32
+WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights")
+
+
+def nin(ndir: int) -> int:
+    return (ndir + 7) // 8 * 8
+
+
+def geometry(ndir: int):
+    k = [nin(ndir)] + [WIDTH] * HIDDEN
+    n = [WIDTH] * HIDDEN + [NOUT]
+    woff, boff, o = [], [], 0
+    for l in range(HIDDEN + 1):
+        woff.append(o)
+        o += k[l] * n[l]
+        boff.append(o)
+        o += n[l]
+    return k, n, woff, boff, o
+
+
+def init_params(ndir: int, seed: int = 0) -> np.ndarray:
+    """He-normal hidden weights, small output weights, zero biases (FP32 flat vector)."""
+    rng = np.random.default_rng(seed)
+    k, n, woff, boff, total = geometry(ndir)
+    p = np.zeros(total, np.float32)
+    for l in range(HIDDEN + 1):
+        std = math.sqrt(2.0 / k[l]) if l < HIDDEN else 0.1 * math.sqrt(1.0 / k[l])
+        p[woff[l] : woff[l] + n[l] * k[l]] = rng.normal(0.0, std, n[l] * k[l])
+    return p
+
+
+@dataclasses.dataclass
+class TrainingSet:
+    x: object  # [n][nin] bf16 device tensor
+    targets: object  # [n][32] float32 device tensor
+    tweights: object  # [n][32] float32 device tensor
+    ndir: int
+
+    @property
+    def n(self) -> int:
+        return int(self.x.shape[0])
+
+
+def label_options(opts: Options) -> Options:
+    """Options of the labelling chain: the plain chain's burn-in, one recorded sample."""
+    o = Options.make(**{f: getattr(opts, f) for f, _ in Options._fields_ if f != "reserved"})
+    o.njumps = o.sampleevery
+    return o
+
+
+def state_from_record(opts: Options, rec, sample: int = 0):
+    """(params [n][P] in the fit layout, tau [n]) of one recorded chain state."""
+    import torch
+
+    r = rec[:, sample, :]
+    K = opts.nfibres
+    cols = [r[5], r[0]] + ([r[3]] if opts.model >= 2 else [])
+    for k in range(K):
+        cols += [r[8 + 3 * k], r[6 + 3 * k], r[7 + 3 * k]]
+    if opts.f0:
+        cols.append(r[1])
+    return torch.stack(cols, 1).contiguous(), r[2].contiguous()
+
+
+def make_training_set(opts: Options, bvecs: np.ndarray, bvals: np.ndarray, n: int, seed: int = 1,
+                      snr=(10.0, 40.0), chunk: int = 131072, widths: bool = True,
+                      state_labels: str = "chain") -> TrainingSet:
+    """n forward-model voxels (SNR ~ U(snr)) with their labels.  The plain chain is run from each
+    voxel's LM fit through its full burn-in; its proposal widths at that point are the width
+    labels, and the state labels are either that chain state (state_labels="chain": the state the
+    LM-initialised chain reaches, which is where a chain with frozen widths must start) or the LM
+    fit itself ("lm")."""
+    import torch
+
+    L = lib.load()
+    ndir = bvals.shape[0]
+    bv, bl = lib.to_device(bvecs), lib.to_device(bvals)
+    x = torch.empty((n, nin(ndir)), device="cuda", dtype=torch.bfloat16)
+    t = torch.empty((n, NOUT), device="cuda", dtype=torch.float32)
+    w = torch.empty((n, NOUT), device="cuda", dtype=torch.float32)
+    lo = label_options(opts)
+    stream = lib._stream(torch)
+    for s in range(0, n, chunk):
+        m = min(chunk, n - s)
+        data, _ = lib.synth(opts.model, opts.nfibres, m, bv, bl, seed, snr, voxel_offset=s)
+        if opts.rician:
+            lib.prepare_data(data)
+        params, tau, status = lib.fit(opts, data, bv, bl)
+        s0hat = torch.empty(m, device="cuda", dtype=torch.float32)
+        vol = lib.make_volume(data, bv, bl)
+        lib._check(L.bpx_mlp_features_dev(C.byref(vol), 0, lib._ptr(x[s : s + m]), lib._ptr(s0hat), stream),
+                   "bpx_mlp_features_dev")
+        props = None
+        if widths or state_labels == "chain":
+            rec, props = lib.mcmc_ex(lo, data, bv, bl, params, tau if opts.rician else None, want_props=True,
+                                     voxel_offset=s, status=status)
+            if state_labels == "chain":
+                params, tau = state_from_record(opts, rec)
+            if not widths:
+                props = None
+        lib._check(L.bpx_mlp_targets_dev(C.byref(opts), m, lib._ptr(params), lib._ptr(tau if opts.rician else None),
+                                         lib._ptr(props), lib._ptr(s0hat), lib._ptr(t[s : s + m]),
+                                         lib._ptr(w[s : s + m]), stream), "bpx_mlp_targets_dev")
+        bad = (status & 1) != 0  # non-finite data: no targets
+        if bool(bad.any()):
+            w[s : s + m][bad] = 0.0
+    torch.cuda.synchronize()
+    return TrainingSet(x, t, w, ndir)
+
+
+def output_bias_from_targets(ts: TrainingSet, params: np.ndarray) -> np.ndarray:
+    """Set the output layer's bias to the weighted mean target (a better start than zero)."""
+    k, n, woff, boff, total = geometry(ts.ndir)
+    t, w = ts.targets, ts.tweights
+    mean = ((t * w).sum(0) / w.sum(0).clamp_min(1e-12)).cpu().numpy()
+    mean[3:12] = 0.0
+    p = params.copy()
+    p[boff[HIDDEN] : boff[HIDDEN] + NOUT] = mean
+    return p
+
+
+def train(ts: TrainingSet, steps: int, batch: int = 4096, lr: float = 1e-3, seed: int = 0,
+          params: np.ndarray | None = None, log_every: int = 0):
+    """Adam with a cosine learning-rate decay over `steps` mini-batches.  Returns (params, losses)."""
+    import torch
+
+    L = lib.load()
+    stream = lib._stream(torch)
+    p0 = params if params is not None else output_bias_from_targets(ts, init_params(ts.ndir, seed))
+    p = torch.from_numpy(np.ascontiguousarray(p0, np.float32)).cuda()
+    g = torch.zeros_like(p)
+    m = torch.zeros_like(p)
+    v = torch.zeros_like(p)
+    loss = torch.zeros(1, device="cuda", dtype=torch.float32)
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    perm = torch.randperm(ts.n, device="cuda", generator=gen)
+    pos = 0
+    losses = []
+    for step in range(1, steps + 1):
+        if pos + batch > ts.n:
+            perm = torch.randperm(ts.n, device="cuda", generator=gen)
+            pos = 0
+        idx = perm[pos : pos + batch]
+        pos += batch
+        xb, tb, wb = ts.x[idx].contiguous(), ts.targets[idx].contiguous(), ts.tweights[idx].contiguous()
+        bs = int(xb.shape[0])
+        lib._check(L.bpx_mlp_train_step_dev(ts.ndir, lib._ptr(p), lib._ptr(g), bs, lib._ptr(xb), lib._ptr(tb),
+                                            lib._ptr(wb), lib._ptr(loss), stream), "bpx_mlp_train_step_dev")
+        lr_t = lr * 0.5 * (1.0 + math.cos(math.pi * (step - 1) / max(1, steps)))
+        lib._check(L.bpx_mlp_adam_dev(p.numel(), lib._ptr(p), lib._ptr(g), lib._ptr(m), lib._ptr(v), lr_t, 0.9, 0.999,
+                                      1e-8, step, stream), "bpx_mlp_adam_dev")
+        if log_every and (step % log_every == 0 or step == 1 or step == steps):
+            losses.append((step, float(loss.item())))
+    torch.cuda.synchronize()
+    if lib.poll_error() != 0:
+        raise lib.BpxError("a tensor-core kernel gave up waiting during training")
+    return p.cpu().numpy(), losses
+
+
+def forward(params, ndir: int, x):
+    """Network outputs [n][32] (device) for bf16 inputs x [n][nin] (device)."""
+    import torch
+
+    n = int(x.shape[0])
+    out = torch.empty((n, NOUT), device="cuda", dtype=torch.float32)
+    p = params if hasattr(params, "data_ptr") else torch.from_numpy(np.ascontiguousarray(params, np.float32)).cuda()
+    lib._check(lib.load().bpx_mlp_forward_dev(ndir, lib._ptr(p), n, lib._ptr(x), lib._ptr(out), lib._stream(torch)),
+               "bpx_mlp_forward_dev")
+    return out
+
+
+def features(data, bvecs, bvals):
+    """(x [n][nin] bf16, s0hat [n]) on the device."""
+    import torch
+
+    n, ndir = int(data.shape[0]), int(data.shape[1])
+    x = torch.empty((n, nin(ndir)), device="cuda", dtype=torch.bfloat16)
+    s0 = torch.empty(n, device="cuda", dtype=torch.float32)
+    vol = lib.make_volume(data, bvecs, bvals)
+    lib._check(lib.load().bpx_mlp_features_dev(C.byref(vol), 0, lib._ptr(x), lib._ptr(s0), lib._stream(torch)),
+               "bpx_mlp_features_dev")
+    return x, s0
+
+
+def decode(opts: Options, out, s0hat):
+    """(params [n][P], tau [n], props [6+3K][n], status [n]) starting state from network outputs."""
+    import torch
+
+    n = int(out.shape[0])
+    params = torch.empty((n, opts.nparams_fit), device="cuda", dtype=torch.float32)
+    tau = torch.empty(n, device="cuda", dtype=torch.float32)
+    props = torch.empty((6 + 3 * opts.nfibres, n), device="cuda", dtype=torch.float32)
+    status = torch.empty(n, device="cuda", dtype=torch.int32)
+    lib._check(lib.load().bpx_mlp_decode_dev(C.byref(opts), n, lib._ptr(out), lib._ptr(s0hat), lib._ptr(params),
+                                             lib._ptr(tau), lib._ptr(props), lib._ptr(status), lib._stream(torch)),
+               "bpx_mlp_decode_dev")
+    return params, tau, props, status
+
+
+def xfibres_learned(opts: Options, data, bvecs, bvals, params, freeze: int = 2, out=None):
+    """The learned pipeline on device tensors (bpx_xfibres_learned_dev); returns the output dict.
+    freeze: 0 adapt the network's widths throughout, 1 never, 2 during the burn-in only."""
+    import torch
+
+    n = int(data.shape[0])
+    t, o = out if out is not None else lib.alloc_outputs(opts, n)
+    p = params if hasattr(params, "data_ptr") else torch.from_numpy(np.ascontiguousarray(params, np.float32)).cuda()
+    vol = lib.make_volume(data, bvecs, bvals)
+    lib._check(lib.load().bpx_xfibres_learned_dev(C.byref(opts), C.byref(vol), lib._ptr(p), int(freeze), C.byref(o),
+                                                  lib._stream(torch)), "bpx_xfibres_learned_dev")
+    return t
+
+
+def save(path: str, params: np.ndarray, **meta) -> None:
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    np.savez_compressed(path, params=np.asarray(params, np.float32), **{k: np.asarray(v) for k, v in meta.items()})
+
+
+def load_weights(path: str):
+    z = np.load(path)
+    return z["params"], {k: z[k] for k in z.files if k != "params"}
+
+
+def mc_se(x):
+    """Monte-Carlo standard error of the mean of each column of x [ns][n] (one chain's samples per
+    voxel): sd * sqrt(tau / ns), with the integrated autocorrelation time tau = -1 + 2 sum_m G_m,
+    G_m = rho_2m + rho_2m+1 summed up to the first non-positive G_m (Geyer's initial positive
+    sequence)."""
+    import torch
+
+    ns = x.shape[0]
+    c = x - x.mean(0)
+    g0 = (c * c).mean(0).clamp_min(1e-30)
+
+    def rho(k):
+        return (c[k:] * c[: ns - k]).mean(0) * ((ns - k) / ns) / g0 if k < ns else torch.zeros_like(g0)
+
+    tau = -torch.ones_like(g0)
+    alive = torch.ones_like(g0, dtype=torch.bool)
+    for m in range(ns // 2):
+        G = (torch.ones_like(g0) if m == 0 else rho(2 * m)) + rho(2 * m + 1)
+        alive = alive & (G > 0)
+        tau = tau + 2.0 * torch.where(alive, G, torch.zeros_like(G))
+    return torch.sqrt(g0 * tau.clamp_min(1.0) / ns)
+
+
+def compare(opts: Options, a: dict, b: dict):
+    """Agreement of two runs' posteriors per voxel: (dyad angle differences in degrees [K][n],
+    |mean f difference| / combined Monte-Carlo standard error [K][n], mean d relative difference
+    [n]).  Standard errors account for the autocorrelation of each chain's samples (mc_se)."""
+    import torch
+
+    ang, z = [], []
+    for k in range(opts.nfibres):
+        da, db = a["dyads"][k].float(), b["dyads"][k].float()
+        c = (da * db).sum(0).abs().clamp(max=1.0)
+        ang.append(torch.rad2deg(torch.acos(c)))
+        fa, fb = a["f"][k].float(), b["f"][k].float()
+        se = torch.sqrt(mc_se(fa) ** 2 + mc_se(fb) ** 2).clamp_min(1e-6)
+        z.append((fa.mean(0) - fb.mean(0)).abs() / se)
+    dd = (a["mean_d"] - b["mean_d"]).abs() / b["mean_d"].abs().clamp_min(1e-12)
+    return torch.stack(ang), torch.stack(z), dd
+
+
+def summary(opts: Options, a: dict, b: dict) -> dict:
+    """Median dyad angles, fraction of f within 2 MC standard errors, median d relative difference."""
+    ang, z, dd = compare(opts, a, b)
+    return {
+        "dyad_median_deg": [round(float(ang[k].median()), 3) for k in range(opts.nfibres)],
+        "f_within_2se": [round(float((z[k] <= 2).float().mean()), 3) for k in range(opts.nfibres)],
+        "d_rel_median": round(float(dd.median()), 4),
+    }
+
+
+PROTOCOLS = {
+    "whole_brain": lambda synth: synth.three_shell(18, 90),
+    "multishell": lambda synth: synth.three_shell(9, 90),
+}
+
+
+def default_weights_path(protocol: str) -> str:
+    return os.path.join(WEIGHTS_DIR, f"initialiser_model2_k3_{protocol}.npz")
+
+
+def main(argv=None) -> None:
+    """Train the initialiser for a protocol on the GPU and save it:
+
+        python -m fdt_b200.learned --protocol whole_brain --n 1000000 --steps 4000
+    """
+    import argparse
+    import time
+
+    import torch
+
+    from . import synth
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--protocol", default="whole_brain", choices=sorted(PROTOCOLS))
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--eval", type=int, default=8192, help="held-out voxels for the learned-vs-plain check")
+    ap.add_argument("--labels", default="chain", choices=["chain", "lm"])
+    ap.add_argument("--weights", default=None, help="evaluate these weights instead of training")
+    a = ap.parse_args(argv)
+    prot = PROTOCOLS[a.protocol](synth)
+    opts = Options.make(model=2, nfibres=3, rician=1, f0=1, ardf0=1)
+    if a.weights:
+        params, _ = load_weights(a.weights)
+    else:
+        t0 = time.time()
+        ts = make_training_set(opts, prot.bvecs, prot.bvals, a.n, seed=a.seed, state_labels=a.labels)
+        t1 = time.time()
+        params, losses = train(ts, a.steps, a.batch, a.lr, seed=a.seed, log_every=max(1, a.steps // 20))
+        t2 = time.time()
+        print(f"training set {a.n} voxels in {t1 - t0:.1f} s; {a.steps} steps in {t2 - t1:.1f} s")
+        for s, l in losses:
+            print(f"  step {s:6d} loss {l:.5f}")
+        out = a.out or default_weights_path(a.protocol)
+        save(out, params, ndir=prot.ndir, model=2, nfibres=3, protocol=a.protocol, n_train=a.n, steps=a.steps,
+             seed=a.seed, labels=a.labels, bvals=prot.bvals, bvecs=prot.bvecs)
+        print("saved", out)
+        del ts
+        torch.cuda.empty_cache()
+    if a.eval:
+        data, _ = synth.make_volume(a.eval, prot, 3, True, 25.0, seed=a.seed + 1000)
+        bv, bl = lib.to_device(prot.bvecs), lib.to_device(prot.bvals)
+        plain = lib.xfibres_dev(opts, lib.to_device(data), bv, bl)
+        o2 = Options.make(model=2, nfibres=3, rician=1, f0=1, ardf0=1, seed=opts.seed + 1)
+        print("plain vs plain (other seed):", summary(opts, lib.xfibres_dev(o2, lib.to_device(data), bv, bl), plain))
+        o3 = Options.make(model=2, nfibres=3, rician=1, f0=1, ardf0=1, nburn=200, seed=opts.seed + 1)
+        print("LM start, burn-in 200:", summary(opts, lib.xfibres_dev(o3, lib.to_device(data), bv, bl), plain))
+        for nb in (100, 200):
+            for fr in (0, 1, 2):
+                lo = Options.make(model=2, nfibres=3, rician=1, f0=1, ardf0=1, nburn=nb, seed=opts.seed + 1)
+                learned_out = xfibres_learned(lo, lib.to_device(data), bv, bl, params, freeze=fr)
+                print(f"learned, burn-in {nb}, freeze {fr}:", summary(opts, learned_out, plain))
+
+
+if __name__ == "__main__":
+    main()

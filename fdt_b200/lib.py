@@ -53,11 +53,15 @@ _SIGS = {
                                       C.c_void_p, C.c_void_p, C.c_void_p]),
     "bpx_mlp_decode_dev": (C.c_int, [C.POINTER(Options), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_void_p, C.c_void_p]),
-    "bpx_xfibres_learned_dev": (C.c_int, [C.POINTER(Options), C.POINTER(Volume), C.c_void_p, C.POINTER(Outputs),
-                                          C.c_void_p]),
+    "bpx_xfibres_learned_dev": (C.c_int, [C.POINTER(Options), C.POINTER(Volume), C.c_void_p, C.c_int32,
+                                          C.POINTER(Outputs), C.c_void_p]),
+    "bpx_xfibres_learned_host": (C.c_int, [C.POINTER(Options), C.POINTER(Volume), C.c_void_p, C.c_int32,
+                                           C.POINTER(Outputs)]),
     "bpx_gemm_bf16_dev": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
                                     C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p]),
     "bpx_mlp_poll_error": (C.c_int, [C.POINTER(C.c_int32)]),
+    "bpx_synth_dev": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_uint64, C.c_float,
+                                C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None
@@ -141,16 +145,17 @@ def fit(opts: Options, data, bvecs, bvals):
     return params, tau, status
 
 
-def mcmc_ex(opts: Options, data, bvecs, bvals, params, tau=None, props_in=None, freeze: bool = False,
+def mcmc_ex(opts: Options, data, bvecs, bvals, params, tau=None, props_in=None, freeze: int = 0,
             want_props: bool = False, voxel_offset: int = 0, status=None):
-    """MCMC with per-voxel proposal widths.  Returns (records, props_out or None)."""
+    """MCMC with per-voxel proposal widths (freeze: 0 adapt, 1 never, 2 burn-in only).
+    Returns (records, props_out or None)."""
     torch = _torch()
     nvox = data.shape[0]
     rec = torch.zeros((nrec(opts.nfibres), opts.nsamples, nvox), device="cuda", dtype=torch.float32)
     pout = torch.zeros((6 + 3 * opts.nfibres, nvox), device="cuda", dtype=torch.float32) if want_props else None
     vol = make_volume(data, bvecs, bvals, voxel_offset)
     _check(load().bpx_mcmc_ex_dev(C.byref(opts), C.byref(vol), _ptr(params), _ptr(tau), _ptr(props_in), _ptr(pout),
-                                  1 if freeze else 0, _ptr(rec), _ptr(status), _stream(torch)), "bpx_mcmc_ex_dev")
+                                  int(freeze), _ptr(rec), _ptr(status), _stream(torch)), "bpx_mcmc_ex_dev")
     return rec, pout
 
 
@@ -161,6 +166,17 @@ def gemm_bf16(a, b, M: int, N: int, K: int, a_mn: bool = False, b_mn: bool = Fal
     _check(load().bpx_gemm_bf16_dev(M, N, K, _ptr(a), a.shape[1], 1 if a_mn else 0, _ptr(b), b.shape[1],
                                     1 if b_mn else 0, _ptr(c), N, _stream(torch)), "bpx_gemm_bf16_dev")
     return c
+
+
+def synth(model: int, nfib: int, nvox: int, bvecs, bvals, seed: int, snr=(10.0, 40.0), voxel_offset: int = 0):
+    """Forward-model voxels with Rician noise on the device: (data [nvox][ndir], truth [nvox][15])."""
+    torch = _torch()
+    ndir = bvals.shape[0]
+    data = torch.empty((nvox, ndir), device="cuda", dtype=torch.float32)
+    truth = torch.empty((nvox, BPX_NSTATE), device="cuda", dtype=torch.float32)
+    _check(load().bpx_synth_dev(model, nfib, nvox, ndir, seed, voxel_offset, float(snr[0]), float(snr[1]),
+                                _ptr(bvecs), _ptr(bvals), _ptr(data), _ptr(truth), _stream(torch)), "bpx_synth_dev")
+    return data, truth
 
 
 def poll_error() -> int:

@@ -242,8 +242,10 @@ bpx_status bpx_xfibres_noalloc_dev(const bpx_options* opts, const bpx_volume* vo
  *   props_in   [6+3*nfib][nvox] starting proposal widths in slot order f0, tau, d, d_std, R, S0,
  *              (th, ph, f) per fibre; NULL = initialise_props (CUDA/runmcmc_kernels.cu:430-460).
  *   props_out  [6+3*nfib][nvox] widths after the last iteration, or NULL.
- *   freeze_props  nonzero: no adaptation (the chain keeps the starting widths; a fixed-width
- *              random-walk chain has the same target distribution).
+ *   freeze_props  0: adapt every updateproposalevery iterations (the reference's behaviour);
+ *              1: never adapt (the chain keeps the starting widths); 2: adapt during the burn-in
+ *              only, then record with the widths frozen.  A random-walk chain with fixed widths
+ *              has the same target distribution.
  */
 bpx_status bpx_mcmc_ex_dev(const bpx_options* opts, const bpx_volume* vol, const float* params,
                            const float* tau, const float* props_in, float* props_out,
@@ -290,10 +292,27 @@ bpx_status bpx_mlp_targets_dev(const bpx_options* opts, int32_t nvox, const floa
 bpx_status bpx_mlp_decode_dev(const bpx_options* opts, int32_t nvox, const float* out,
                               const float* s0hat, float* params, float* tau, float* props,
                               uint32_t* status, void* stream);
-/* Learned pipeline: features -> network -> decode -> MCMC with the network's proposal widths
- * frozen, opts->nburn burn-in -> finishing.  Same outputs as bpx_xfibres_dev. */
+/* Learned pipeline: features -> network -> decode -> MCMC started from the network's state with
+ * the network's proposal widths (freeze_props as for bpx_mcmc_ex_dev), opts->nburn burn-in ->
+ * finishing.  Same outputs as bpx_xfibres_dev. */
 bpx_status bpx_xfibres_learned_dev(const bpx_options* opts, const bpx_volume* vol,
-                                   const float* mlp_params, bpx_outputs* out, void* stream);
+                                   const float* mlp_params, int32_t freeze_props, bpx_outputs* out,
+                                   void* stream);
+/* The learned pipeline on host buffers (as bpx_xfibres_host; mlp_params is a host array). */
+bpx_status bpx_xfibres_learned_host(const bpx_options* opts, const bpx_volume* vol,
+                                    const float* mlp_params, int32_t freeze_props,
+                                    bpx_outputs* host_out);
+
+/*
+ * Voxels drawn from the forward model (training data of the learned initialiser; no counterpart
+ * in the reference).  model 1 or 2, nfib 1..3; S0 = 1000, d ~ U(0.5e-3, 2e-3), d_std = U(0.1,0.5) d,
+ * f1 ~ U(0.3, 0.7), f2 = U(0,1) min(0.3, 1-f1), f3 = U(0,1) min(0.15, 0.99-f1-f2), directions
+ * uniform, Rician noise at SNR ~ U(snr_lo, snr_hi) on S0.  Philox keyed by seed, counted by
+ * voxel_offset + voxel.  data [nvox][ndir]; truth [nvox][BPX_NSTATE] (tau = 1/sigma^2) or NULL.
+ */
+bpx_status bpx_synth_dev(int32_t model, int32_t nfib, int32_t nvox, int32_t ndir, uint64_t seed,
+                         uint64_t voxel_offset, float snr_lo, float snr_hi, const float* bvecs,
+                         const float* bvals, float* data, float* truth, void* stream);
 
 /* C[M][N] (fp32, row-major, ldc) = A B^T on the tcgen05 tensor cores, bf16 operands: A is
  * [M][lda] (a_mn = 0) or [K][lda] (a_mn = 1), B is [N][ldb] (b_mn = 0) or [K][ldb] (b_mn = 1).
