@@ -111,3 +111,14 @@ class Outputs(C.Structure):
         ("dyads", C.c_void_p),
         ("status", C.c_void_p),
     ]
+
+
+class Item(C.Structure):
+    """bpx_item: one volume of a batch."""
+
+    _fields_ = [
+        ("vol", Volume),
+        ("model", C.c_int32),
+        ("nfibres", C.c_int32),
+        ("out", Outputs),
+    ]

@@ -307,7 +307,7 @@ bpx_status bpx_fit_dev(const bpx_options* opts, const bpx_volume* vol, float* pa
   if (opts->rician && !tau) return fail(BPX_ERR_INVALID_ARG, "tau is NULL under rician");
   st = check_device();
   if (st != BPX_OK) return st;
-  FitArgs a;
+  FitArgs a{};
   a.nvox = vol->nvox;
   a.ndir = vol->ndir;
   a.data = vol->data;
@@ -340,7 +340,7 @@ bpx_status bpx_mcmc_ex_dev(const bpx_options* opts, const bpx_volume* vol, const
   const McmcLayout lay = pick_layout(opts, vol->ndir);
   if (lay.tpv == 0 || !layout_supported(opts->model, opts->nfibres, opts->rician != 0, lay) || lay.tpv * lay.mpl < vol->ndir)
     return fail(BPX_ERR_UNSUPPORTED, "no compiled MCMC layout for ndir=" + std::to_string(vol->ndir));
-  McmcArgs a;
+  McmcArgs a{};
   a.nvox = vol->nvox;
   a.ndir = vol->ndir;
   a.data = vol->data;
@@ -390,7 +390,7 @@ bpx_status bpx_finish_dev(const bpx_options* opts, int32_t nvox, const float* re
   if (ns < 1) return fail(BPX_ERR_INVALID_ARG, "no samples (njumps < sampleevery)");
   st = check_device();
   if (st != BPX_OK) return st;
-  FinishArgs a;
+  FinishArgs a{};
   a.nvox = nvox;
   a.nsamples = ns;
   a.nfib = opts->nfibres;
@@ -409,7 +409,7 @@ bpx_status bpx_energy_dev(const bpx_options* opts, const bpx_volume* vol, const 
   if (!states) return fail(BPX_ERR_INVALID_ARG, "states is NULL");
   st = check_device();
   if (st != BPX_OK) return st;
-  EnergyArgs a;
+  EnergyArgs a{};
   a.nvox = vol->nvox;
   a.ndir = vol->ndir;
   a.data = vol->data;

@@ -16,7 +16,10 @@ constexpr int kFitVoxPerBlock = 32;  // voxels a fit block shares out among its 
 #endif
 constexpr int kFitMinBlocks = BPX_FIT_MIN_BLOCKS;  // register cap: 65536 / (128 * 4) = 128 per thread
 constexpr int kMcmcThreads = 128;  // 4 warps
-constexpr int kMcmcMinBlocks = 3;  // register cap for 12 resident warps per SM
+#ifndef BPX_MCMC_MIN_BLOCKS
+#define BPX_MCMC_MIN_BLOCKS 3
+#endif
+constexpr int kMcmcMinBlocks = BPX_MCMC_MIN_BLOCKS;  // register cap: 3 blocks = 12 resident warps per SM
 
 int sm_count();  // multiprocessors of the current device (cached per device)
 void set_last_error(const char* msg);  // message returned by bpx_last_error() on this thread
@@ -68,6 +71,7 @@ struct McmcArgs {
   const float* props_in;  // [6+3K][nvox] initial proposal widths, or NULL for initialise_props
   float* props_out;       // [6+3K][nvox] proposal widths after the last iteration, or NULL
   int freeze_props;       // 0: adapt (reference); 1: never adapt; 2: adapt during burn-in only
+  const uint64_t* voxel_keys;  // [nvox] RNG voxel keys (packed batches), or NULL: voxel_offset + v
 };
 
 struct EnergyArgs {

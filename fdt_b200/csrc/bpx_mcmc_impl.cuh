@@ -335,9 +335,10 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
 
   // shared memory: the (g_x, g_y, g_z, b) table in pair order (one copy per block, or per group
   // under gradnonlin); per-thread backups of the signals a proposal overwrites; per-group proposal
-  // widths and acceptance counts.  Pair p of lane l is entries 2(p*TPV+l) and 2(p*TPV+l)+1 =
-  // {gx0,gx1,gy0,gy1}, {gz0,gz1,b0,b1} for measurements l+2p*TPV and l+(2p+1)*TPV; the unpaired
-  // measurement l+(MPL-1)*TPV is entry 2*NP*TPV+l.  Measurements past M read zeros.
+  // widths and acceptance counts.  Pair p of lane l is entries p*TPV+l = {gx0,gx1,gy0,gy1} and
+  // (NP+p)*TPV+l = {gz0,gz1,b0,b1} for measurements l+2p*TPV and l+(2p+1)*TPV (consecutive lanes
+  // read consecutive 16-byte entries, free of bank conflicts); the unpaired measurement
+  // l+(MPL-1)*TPV is entry 2*NP*TPV+l.  Measurements past M read zeros.
   const int ncopy = a.gradnonlin ? GPB : 1;
   float4* gb = smem4 + (a.gradnonlin ? gblk * NG : 0);
   float* after = (float*)(smem4 + ncopy * NG);
@@ -353,8 +354,8 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
       const float b0 = m0 < M ? bl[m0] : 0.f;
       const float gx1 = m1 < M ? bv[m1] : 0.f, gy1 = m1 < M ? bv[M + m1] : 0.f, gz1 = m1 < M ? bv[2 * M + m1] : 0.f;
       const float b1 = m1 < M ? bl[m1] : 0.f;
-      dst[2 * e] = make_float4(gx0, gx1, gy0, gy1);
-      dst[2 * e + 1] = make_float4(gz0, gz1, b0, b1);
+      dst[e] = make_float4(gx0, gx1, gy0, gy1);
+      dst[NP * TPV + e] = make_float4(gz0, gz1, b0, b1);
     }
     if (TAIL)
       for (int l = first_l; l < TPV; l += step) {
@@ -374,7 +375,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
     const int vreal = first + gw;
     const bool valid = vreal < a.nvox;
     const int v = valid ? vreal : a.nvox - 1;
-    const uint64_t gvox = a.voxel_offset + (uint64_t)v;
+    const uint64_t gvox = a.voxel_keys ? a.voxel_keys[v] : a.voxel_offset + (uint64_t)v;
     if (a.gradnonlin) {
       __syncwarp();
       fill_gb(gb, a.bvecs + (size_t)v * 3 * M, a.bvals + (size_t)v * M, gl, TPV);
@@ -455,7 +456,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
       const float2 beta2 = make_float2(sp.beta, sp.beta);
 #pragma unroll
       for (int p = 0; p < NP; ++p) {
-        const float4 ga = gb[2 * (p * TPV + gl)], gc = gb[2 * (p * TPV + gl) + 1];
+        const float4 ga = gb[p * TPV + gl], gc = gb[(NP + p) * TPV + gl];
         const float2 gx = make_float2(ga.x, ga.y), gy = make_float2(ga.z, ga.w), gz = make_float2(gc.x, gc.y);
         const float2 b = make_float2(gc.z, gc.w);
         const float2 bbeta = vmul(beta2, b);
@@ -664,7 +665,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
               if (k == kf) {
 #pragma unroll
                 for (int p = 0; p < NP; ++p) {
-                  const float4 ga = gb[2 * (p * TPV + gl)], gc = gb[2 * (p * TPV + gl) + 1];
+                  const float4 ga = gb[p * TPV + gl], gc = gb[(NP + p) * TPV + gl];
                   float2 dp = vmul(make_float2(ga.x, ga.y), nvx2);
                   dp = vfma(make_float2(ga.z, ga.w), nvy2, dp);
                   dp = vfma(make_float2(gc.x, gc.y), nvz2, dp);

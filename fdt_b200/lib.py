@@ -11,7 +11,7 @@ import os
 
 import numpy as np
 
-from .abi import BPX_NSTATE, Options, Outputs, Volume, nrec
+from .abi import BPX_NSTATE, Item, Options, Outputs, Volume, nrec
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libbpx.so")
@@ -60,6 +60,12 @@ _SIGS = {
     "bpx_gemm_bf16_dev": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
                                     C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p]),
     "bpx_mlp_poll_error": (C.c_int, [C.POINTER(C.c_int32)]),
+    "bpx_batch_create": (C.c_int, [C.POINTER(Options), C.POINTER(Item), C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
+    "bpx_batch_run": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "bpx_batch_buckets": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int32), C.c_int32]),
+    "bpx_batch_destroy": (C.c_int, [C.c_void_p]),
+    "bpx_autotune_layout": (C.c_int, [C.POINTER(Options), C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
+                                      C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_float), C.c_void_p]),
     "bpx_synth_dev": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_uint64, C.c_float,
                                 C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
@@ -320,3 +326,66 @@ def states_from_records(opts: Options, records, sample: int):
         st[:, 7 + 3 * k] = r[7 + 3 * k]
         st[:, 8 + 3 * k] = r[8 + 3 * k]
     return st
+
+
+class Batch:
+    """A batch of items run as one CUDA-graph launch (bpx_batch_*).  `items` is a list of dicts
+    with keys data, bvecs, bvals (device tensors), model, nfibres, voxel_offset (optional); the
+    outputs are allocated here (device) and returned by run() as a list of output dicts."""
+
+    def __init__(self, opts: Options, items: list, autotune: bool = True):
+        torch = _torch()
+        self.opts = opts
+        self._keep = []
+        arr = (Item * len(items))()
+        self.outputs = []
+        for i, it in enumerate(items):
+            o = Options.make(**{f: getattr(opts, f) for f, _ in Options._fields_ if f != "reserved"})
+            o.model, o.nfibres = it["model"], it["nfibres"]
+            t, out = alloc_outputs(o, int(it["data"].shape[0]))
+            self.outputs.append(t)
+            arr[i].vol = make_volume(it["data"], it["bvecs"], it["bvals"], int(it.get("voxel_offset", 0)))
+            arr[i].model, arr[i].nfibres = it["model"], it["nfibres"]
+            arr[i].out = out
+            self._keep.append((it["data"], it["bvecs"], it["bvals"]))
+        h = C.c_void_p()
+        _check(load().bpx_batch_create(C.byref(opts), arr, len(items), 1 if autotune else 0, C.byref(h)),
+               "bpx_batch_create")
+        self.handle = h
+        del torch
+
+    def buckets(self) -> list[dict]:
+        L = load()
+        n = L.bpx_batch_buckets(self.handle, None, 0)
+        d = (C.c_int32 * (7 * max(n, 1)))()
+        L.bpx_batch_buckets(self.handle, d, n)
+        keys = ["model", "nfibres", "ndir", "tpv", "mpl", "voxels", "items"]
+        return [dict(zip(keys, list(d[7 * i : 7 * i + 7]))) for i in range(n)]
+
+    def run(self):
+        torch = _torch()
+        _check(load().bpx_batch_run(self.handle, _stream(torch)), "bpx_batch_run")
+        return self.outputs
+
+    def close(self):
+        if getattr(self, "handle", None):
+            load().bpx_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune_layout(opts: Options, bvecs, bvals, sample: int = 2048):
+    """(tpv, mpl, {layout: seconds per voxel}) from bpx_autotune_layout."""
+    _torch()
+    L = load()
+    lays = mcmc_layouts()
+    t = (C.c_float * len(lays))()
+    tpv, mpl = C.c_int32(), C.c_int32()
+    _check(L.bpx_autotune_layout(C.byref(opts), int(bvals.shape[0]), _ptr(bvecs), _ptr(bvals), sample, C.byref(tpv),
+                                 C.byref(mpl), t, None), "bpx_autotune_layout")
+    return tpv.value, mpl.value, {lays[i]: t[i] for i in range(len(lays)) if t[i] >= 0}

@@ -324,6 +324,44 @@ bpx_status bpx_gemm_bf16_dev(int32_t M, int32_t N, int32_t K, const uint16_t* A,
  * 1 or 2 = a bounded wait for a TMA copy or an MMA gave up). */
 bpx_status bpx_mlp_poll_error(int32_t* code);
 
+/*
+ * ---- Batched form (no counterpart in the reference) ----
+ * Many volumes ("items") with their own voxel counts, measurement counts, models and fibre counts
+ * run as one CUDA-graph launch.  Items of equal (model, nfibres, ndir, bvecs, bvals) form a bucket
+ * whose voxels are packed so one fit, one MCMC and one finishing launch serve them all; the chains
+ * keep each item's RNG keys (vol.voxel_offset + voxel), so results equal per-item runs.  The other
+ * options (rician, f0, burn-in, ...) come from `opts` and are shared by all items.
+ * bpx_batch_create validates, picks each bucket's MCMC layout (opts->mcmc_tpv/mpl if set, else the
+ * autotuner when autotune != 0, else the default), allocates the packed buffers and captures the
+ * graph; the items' device buffers must stay valid for the batch's life.  bpx_batch_run launches
+ * the graph on `stream` (asynchronous).  Items with vol.grad (gradnonlin) are not batched.
+ */
+typedef struct bpx_item {
+  bpx_volume vol;       /* device buffers */
+  int32_t model;        /* 1..3 */
+  int32_t nfibres;      /* 1..3 */
+  bpx_outputs out;      /* device buffers; NULL fields are not written */
+} bpx_item;
+typedef struct bpx_batch bpx_batch;
+bpx_status bpx_batch_create(const bpx_options* opts, const bpx_item* items, int32_t nitems,
+                            int32_t autotune, bpx_batch** batch);
+bpx_status bpx_batch_run(bpx_batch* batch, void* stream);
+/* Bucket descriptions, 7 ints each: model, nfibres, ndir, tpv, mpl, voxels, items.  Returns the
+ * number of buckets (writes at most max). */
+int32_t bpx_batch_buckets(const bpx_batch* batch, int32_t* desc, int32_t max);
+bpx_status bpx_batch_destroy(bpx_batch* batch);
+
+/*
+ * Autotuner: times every compiled MCMC layout (threads per voxel tpv, measurements per lane mpl;
+ * 128/tpv voxels per block) that covers ndir on `sample` forward-model voxels with a 65-iteration
+ * chain and returns the fastest (cached per device and option set).  seconds_per_voxel, if not
+ * NULL, receives one entry per compiled layout (bpx_mcmc_layouts order; -1 = not a candidate).
+ * Synchronous.
+ */
+bpx_status bpx_autotune_layout(const bpx_options* opts, int32_t ndir, const float* bvecs,
+                               const float* bvals, int32_t sample, int32_t* tpv, int32_t* mpl,
+                               float* seconds_per_voxel, void* stream);
+
 /* Free the per-device workspace cache of the current device. */
 bpx_status bpx_release_workspace(void);
 
