@@ -190,6 +190,103 @@ def cpu_baseline(seconds: float = 12.0) -> dict:
             "sample": f"{done} voxels of the whole-brain workload (full chain), {t_all:.1f} s on {cores} threads"}
 
 
+def batched_workload(scale: float, seed: int = 31):
+    """Config C2: 16 volumes, voxel counts log-uniform in [5k, 300k] (times `scale`), measurement
+    counts from {33, 65, 129, 279} (the 279-volume three-shell scheme truncated), models 1 and 2
+    mixed across volumes, fibre count 1..3 per voxel, SNR ~ U(10, 40).  Returns a list of items
+    (host arrays), one per (volume, fibre count)."""
+    rng = np.random.default_rng(seed)
+    items = []
+    for v in range(16):
+        n = int(round(np.exp(rng.uniform(np.log(5000), np.log(300000))) * scale))
+        M = int(rng.choice([33, 65, 129, 279]))
+        model = int(rng.choice([1, 2]))
+        prot = synth.truncated_three_shell(M)
+        ks = rng.integers(1, 4, size=n)
+        off = 0
+        for K in (1, 2, 3):
+            m = int((ks == K).sum())
+            if m == 0:
+                continue
+            snr = rng.uniform(10.0, 40.0, size=m)
+            y, _ = synth.make_volume(m, prot, K, model == 2, snr, seed=seed * 1000 + 10 * v + K)
+            items.append(dict(host=y, prot=prot, model=model, nfibres=K, volume=v, voxel_offset=off))
+            off += m
+    return items
+
+
+def run_batched(args):
+    """Times the batched form (one graph launch over all volumes) against the same items run one
+    after another through bpx_xfibres_dev with the default layouts."""
+    import torch
+
+    from fdt_b200 import lib
+
+    o = whole_brain_options()
+    items = batched_workload(args.batch_scale)
+    protos = {}
+    dev_items = []
+    for it in items:
+        M = it["prot"].ndir
+        if M not in protos:
+            protos[M] = (lib.to_device(it["prot"].bvecs), lib.to_device(it["prot"].bvals))
+        bv, bl = protos[M]
+        dev_items.append(dict(data=lib.to_device(it["host"]), bvecs=bv, bvals=bl, model=it["model"],
+                              nfibres=it["nfibres"], voxel_offset=it["voxel_offset"]))
+    nvox = sum(int(it["host"].shape[0]) for it in items)
+    t0 = time.perf_counter()
+    batch = lib.Batch(o, dev_items, autotune=True)
+    t_create = time.perf_counter() - t0
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, k):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+        for e0, e1 in evs:
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        return sum(e0.elapsed_time(e1) for e0, e1 in evs) / 1e3 / k
+
+    for _ in range(args.warmup):
+        batch.run()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    t_batch = timed(batch.run, args.steps)
+    ck = clocks.stop()
+    work = [torch.empty_like(d["data"]) for d in dev_items]
+    outs = []
+    for it in items:
+        oi = Options.make(**{f: getattr(o, f) for f, _ in Options._fields_ if f != "reserved"})
+        oi.model, oi.nfibres = it["model"], it["nfibres"]
+        outs.append((oi, lib.alloc_outputs(oi, int(it["host"].shape[0]))))
+
+    def sequential():
+        for d, w, (oi, out) in zip(dev_items, work, outs):
+            w.copy_(d["data"])
+            lib.xfibres_dev(oi, w, d["bvecs"], d["bvals"], voxel_offset=d["voxel_offset"], out=out)
+
+    sequential()
+    torch.cuda.synchronize()
+    t_seq = timed(sequential, 1)
+    line = {
+        "metric": "voxels/s, batched form (16 mixed volumes in one CUDA-graph launch)", "value": nvox / t_batch,
+        "unit": "voxels/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_batch,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": "C2 batch: 16 volumes, voxels log-uniform in [5k, 300k] x %g, ndir from "
+                   "{33, 65, 129, 279}, models 1/2 per volume, 1..3 fibres per voxel, SNR U(10,40); "
+                   "rician+f0+ardf0, burnin 1000, njumps 1250" % args.batch_scale,
+                   "voxels": nvox, "items": len(items), "l2": "inputs larger than L2"},
+        "sequential_per_item": {"value": nvox / t_seq, "unit": "voxels/s", "launches": 4 * len(items)},
+        "batched_over_sequential": t_seq / t_batch,
+        "buckets": batch.buckets(), "create_s": t_create,
+        "gpu_launches": 1, "clocks": ck,
+    }
+    print(json.dumps(line), flush=True)
+    batch.close()
+
+
 def learned_options(o: Options) -> Options:
     """Options of the learned form: the plain options with burn-in 200 and another RNG seed."""
     lo = Options.make(**{f: getattr(o, f) for f, _ in Options._fields_ if f != "reserved"})
@@ -214,6 +311,9 @@ def main():
     ap.add_argument("--freeze", type=int, default=0, choices=[0, 1, 2],
                     help="learned form: 0 network widths adapt, 1 frozen, 2 frozen after burn-in")
     ap.add_argument("--weights", default=None, help="initialiser weights (default: the committed whole-brain set)")
+    ap.add_argument("--workload", default="whole_brain", choices=["whole_brain", "batched"],
+                    help="batched: the mixed 16-volume batch in one graph launch (one GPU)")
+    ap.add_argument("--batch-scale", type=float, default=0.25, help="batched: voxel-count scale")
     ap.add_argument("--prof", action="store_true",
                     help="profiling case: run the steps only (no e2e, CPU baseline, accuracy or calibration)")
     ap.add_argument("--nburn", type=int, default=None, help="override burn-in (profiling cases)")
@@ -227,6 +327,10 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.workload == "batched":
+        if rank == 0:
+            run_batched(args)
         return
 
     import ctypes as C
