@@ -185,6 +185,30 @@ __device__ __forceinline__ float dlik(float st_old, float st_new, float tau_old,
   return M * logf(tau_new / tau_old) + (st_new - st_old);
 }
 
+// likelihood energy difference when tau is unchanged (the Rician M ln(tau'/tau) term is zero)
+template <bool RIC>
+__device__ __forceinline__ float dlik_same_tau(float st_old, float st_new, float halfM) {
+  if (!RIC) return halfM * logf(st_old / st_new);
+  return st_new - st_old;
+}
+
+// all lanes of this lane's group agree on a group-uniform flag; with one group per warp the flag
+// is warp-uniform already, otherwise a vote over the warp tells whether any group disagrees
+template <int TPV>
+__device__ __forceinline__ bool group_all(bool x) {
+  if constexpr (TPV == 32) return x;
+  return __all_sync(0xffffffffu, x);
+}
+
+// a rejected proposal's signals go back to their backups: with one group per warp the decision
+// is warp-uniform and the caller only gets here on rejection, so the backup is taken as it is
+template <int TPV, typename T>
+__device__ __forceinline__ T keep_or_restore(bool ok, T cur, T old) {
+  if constexpr (TPV == 32) return old;
+  if constexpr (sizeof(T) == 8) return make_float2(ok ? cur.x : old.x, ok ? cur.y : old.y);
+  return ok ? cur : old;
+}
+
 // select element kf (runtime, < K) of a register array without local memory
 template <int K, typename T>
 __device__ __forceinline__ T pick(const T (&a)[K], int kf) {
@@ -565,71 +589,143 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
           lu = __shfl_sync(0xffffffffu, lq, slot % TPV, TPV);
         }
         const float prop = sprop[slot];
-        const int kind = slot < kSlotFibre0 ? slot : kSlotFibre0 + (slot - kSlotFibre0) % 3;
-        const int kf = slot < kSlotFibre0 ? 0 : (slot - kSlotFibre0) / 3;
-        // ---- proposed state ----
-        float S0n = S0, dn = d, dsn = dstd, Rn = R, taun = tau, f0n = f0, thn = 0.f, phn = 0.f;
-        float fn[K];
+        bool ok = false;
+        if (slot >= kSlotFibre0 && (slot - kSlotFibre0) % 3 != 2) {
+          // ---------- theta or phi of fibre kf: only that fibre's stick signals change ----------
+          const int kf = (slot - kSlotFibre0) / 3;
+          const bool is_th = (slot - kSlotFibre0) % 3 == 0;
+          const float tho = pick<K>(th, kf), pho = pick<K>(ph, kf);
+          const float thn = is_th ? tho + n * prop : tho;
+          const float phn = is_th ? pho : pho + n * prop;
+          const float pold = is_th ? pick<K>(p_th, kf) : 0.f;
+          const float pnew = is_th ? th_prior(thn) : 0.f;
+          float sn, cs, sp_, cp;
+          sincosf(thn, &sn, &cs);
+          sincosf(phn, &sp_, &cp);
+          const float nvx = sn * cp, nvy = sn * sp_, nvz = cs;
+          const SigParams<MODEL> sp = sig_params<MODEL>(d, dstd, R);
+          const float2 beta2 = make_float2(sp.beta, sp.beta);
+          const float2 nvx2 = vbc<float2>(nvx), nvy2 = vbc<float2>(nvy), nvz2 = vbc<float2>(nvz);
 #pragma unroll
-        for (int k = 0; k < K; ++k) fn[k] = f[k];
-        float pnew = 0.f, pold = 0.f;  // prior term that changes
-        bool rej = false;
-        unsigned mask = 0u;
-        switch (kind) {
-          case kSlotF0: {
-            f0n = f0 + n * prop;
-            rej = (f0n <= 0.f || f0n >= 1.f);
-            pold = p_f0;
-            pnew = rej ? p_f0 : (a.ardf0 ? logf(f0n) : 0.f);
-            float fs = f0n;
+          for (int k = 0; k < K; ++k)
+            if (k == kf) {
 #pragma unroll
-            for (int k = 0; k < K; ++k) fs += f[k];
-            rej = rej || (fs > 1.f);
-          } break;
-          case kSlotTau:
-            taun = tau + n * prop;
-            rej = taun <= 0.f;
-            break;
-          case kSlotD:
+              for (int p = 0; p < NP; ++p) {
+                const float4 ga = gb[p * TPV + gl], gc = gb[(NP + p) * TPV + gl];
+                float2 dp = vmul(make_float2(ga.x, ga.y), nvx2);
+                dp = vfma(make_float2(ga.z, ga.w), nvy2, dp);
+                dp = vfma(make_float2(gc.x, gc.y), nvz2, dp);
+                const float2 b = make_float2(gc.z, gc.w);
+                bkp[p * kMcmcThreads] = s2[k][p];
+                s2[k][p] = stick_v<MODEL, float2>(sp, b, vmul(beta2, b), vmul(dp, dp));
+              }
+              if (TAIL) {
+                const float4 g = gb[2 * NP * TPV + gl];
+                const float dp = g.x * nvx + g.y * nvy + g.z * nvz;
+                bkt[0] = st[k];
+                st[k] = stick_v<MODEL, float>(sp, g.w, sp.beta * g.w, dp * dp);
+              }
+            }
+          const float likn = lik_of(S0, f, f0, tau);
+          ok = (pold - pnew) + dlik_same_tau<RIC>(lik, likn, halfM) > lu;
+          if (!group_all<TPV>(ok)) {
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+              if (k == kf) {
+#pragma unroll
+                for (int p = 0; p < NP; ++p) s2[k][p] = keep_or_restore<TPV>(ok, s2[k][p], bkp[p * kMcmcThreads]);
+                if (TAIL) st[k] = keep_or_restore<TPV>(ok, st[k], bkt[0]);
+              }
+          }
+          if (ok) {
+            lik = likn;
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+              if (k == kf) {
+                th[k] = thn;
+                ph[k] = phn;
+                vx[k] = nvx;
+                vy[k] = nvy;
+                vz[k] = nvz;
+                if (is_th) p_th[k] = pnew;
+              }
+          }
+        } else if (slot == kSlotD || slot == kSlotDstd || slot == kSlotR) {
+          // ---------- d, d_std or R: every signal that depends on it changes ----------
+          float dn = d, dsn = dstd, Rn = R, pold, pnew;
+          bool rej, sticks, isob;
+          if (slot == kSlotD) {
             dn = d + n * prop;
             rej = (dn < 0.f || dn > kUpperDiff);
             pold = p_d;
             pnew = (rej || MODEL != 3) ? p_d : (1.0f - 3.0f) * logf(dn) + 4000.0f * dn;
-            mask = kAllSticks | kIsoBit;
-            break;
-          case kSlotDstd: {
+            sticks = true;
+            isob = true;
+          } else if (slot == kSlotDstd) {
             dsn = dstd + n * prop;
             const float upper = MODEL == 3 ? 0.004f : 0.01f;
             rej = (dsn <= 0.f || dsn > upper);
             pold = p_dstd;
             pnew = rej ? p_dstd : logf(dsn);
-            mask = MODEL == 2 ? (kAllSticks | kIsoBit) : kIsoBit;
-          } break;
-          case kSlotR: {
+            sticks = MODEL == 2;
+            isob = true;
+          } else {
             Rn = R + n * prop;
             float pr2 = p_R;
             rej = r_prior(pr, Rn, d, pr2);
             pold = p_R;
             pnew = rej ? p_R : pr2;
-            mask = kAllSticks;
-          } break;
-          case kSlotS0:
-            S0n = S0 + n * prop;
-            rej = S0n < 0.f;
-            break;
-          case kSlotFibre0: {  // theta of fibre kf
-            thn = pick<K>(th, kf) + n * prop;
-            phn = pick<K>(ph, kf);
-            pold = pick<K>(p_th, kf);
-            pnew = th_prior(thn);
-            mask = 1u << kf;
-          } break;
-          case kSlotFibre0 + 1:  // phi of fibre kf
-            thn = pick<K>(th, kf);
-            phn = pick<K>(ph, kf) + n * prop;
-            mask = 1u << kf;
-            break;
-          default: {  // f of fibre kf
+            sticks = true;
+            isob = false;
+          }
+          float likn = lik;
+          const bool live = !group_all<TPV>(rej);
+          if (live) {
+            all_signals(dn, dsn, Rn, sticks, isob, true);
+            likn = lik_of(S0, f, f0, tau);
+          }
+          ok = !rej && ((pold - pnew) + dlik_same_tau<RIC>(lik, likn, halfM) > lu);
+          if (live && !group_all<TPV>(ok)) {
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+              if (sticks) {
+#pragma unroll
+                for (int k = 0; k < K; ++k)
+                  s2[k][p] = keep_or_restore<TPV>(ok, s2[k][p], bkp[(k * NP + p) * kMcmcThreads]);
+              }
+              if (isob) i2[p] = keep_or_restore<TPV>(ok, i2[p], bkp[(K * NP + p) * kMcmcThreads]);
+            }
+            if (TAIL) {
+              if (sticks) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) st[k] = keep_or_restore<TPV>(ok, st[k], bkt[k * kMcmcThreads]);
+              }
+              if (isob) it_ = keep_or_restore<TPV>(ok, it_, bkt[K * kMcmcThreads]);
+            }
+          }
+          if (ok) {
+            lik = likn;
+            if (slot == kSlotD) {
+              d = dn;
+              p_d = pnew;
+            } else if (slot == kSlotDstd) {
+              dstd = dsn;
+              p_dstd = pnew;
+            } else {
+              R = Rn;
+              p_R = pnew;
+            }
+          }
+        } else {
+          // ---------- f0, tau, S0 or a fraction f_k: no signal changes ----------
+          const bool is_f = slot >= kSlotFibre0;
+          const int kf = is_f ? (slot - kSlotFibre0) / 3 : 0;
+          float S0n = S0, taun = tau, f0n = f0, fn[K];
+#pragma unroll
+          for (int k = 0; k < K; ++k) fn[k] = f[k];
+          float pold = 0.f, pnew = 0.f;
+          bool rej;
+          if (is_f) {
             const float fkn = pick<K>(f, kf) + n * prop;
             rej = (fkn <= 0.f || fkn >= 1.f);
             const bool lj = pick<K>(lam, kf);
@@ -642,124 +738,47 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
               fs += fn[k];
             }
             rej = rej || (fs > 1.f);
-          } break;
-        }
-        // ---- signals of the proposed state (in place, old values backed up), likelihood ----
-        float likn = lik;
-        float nvx = 0.f, nvy = 0.f, nvz = 0.f;
-        const bool live = __any_sync(0xffffffffu, !rej);
-        const bool one_fibre = mask != 0u && (mask & kAllSticks) != kAllSticks && (mask & kAllSticks) != 0u;
-        if (live) {
-          if (one_fibre) {
-            float sn, cs, sp_, cp;
-            sincosf(thn, &sn, &cs);
-            sincosf(phn, &sp_, &cp);
-            nvx = sn * cp;
-            nvy = sn * sp_;
-            nvz = cs;
-            const SigParams<MODEL> sp = sig_params<MODEL>(d, dstd, R);
-            const float2 beta2 = make_float2(sp.beta, sp.beta);
-            const float2 nvx2 = vbc<float2>(nvx), nvy2 = vbc<float2>(nvy), nvz2 = vbc<float2>(nvz);
+          } else if (slot == kSlotF0) {
+            f0n = f0 + n * prop;
+            rej = (f0n <= 0.f || f0n >= 1.f);
+            pold = p_f0;
+            pnew = rej ? p_f0 : (a.ardf0 ? logf(f0n) : 0.f);
+            float fs = f0n;
 #pragma unroll
-            for (int k = 0; k < K; ++k)
-              if (k == kf) {
-#pragma unroll
-                for (int p = 0; p < NP; ++p) {
-                  const float4 ga = gb[p * TPV + gl], gc = gb[(NP + p) * TPV + gl];
-                  float2 dp = vmul(make_float2(ga.x, ga.y), nvx2);
-                  dp = vfma(make_float2(ga.z, ga.w), nvy2, dp);
-                  dp = vfma(make_float2(gc.x, gc.y), nvz2, dp);
-                  const float2 b = make_float2(gc.z, gc.w);
-                  bkp[p * kMcmcThreads] = s2[k][p];
-                  s2[k][p] = stick_v<MODEL, float2>(sp, b, vmul(beta2, b), vmul(dp, dp));
-                }
-                if (TAIL) {
-                  const float4 g = gb[2 * NP * TPV + gl];
-                  const float dp = g.x * nvx + g.y * nvy + g.z * nvz;
-                  bkt[0] = st[k];
-                  st[k] = stick_v<MODEL, float>(sp, g.w, sp.beta * g.w, dp * dp);
-                }
-              }
-          } else if (mask != 0u) {
-            all_signals(dn, dsn, Rn, (mask & kAllSticks) != 0u, (mask & kIsoBit) != 0u, true);
-          }
-          likn = lik_of(S0n, fn, f0n, taun);
-        }
-        const bool ok = !rej && ((pold - pnew) + dlik<RIC>(lik, likn, tau, taun, halfM, fM) > lu);
-        // ---- accept, or restore the signals ----
-        if (live && mask != 0u && !__all_sync(0xffffffffu, ok)) {
-          if (one_fibre) {
-#pragma unroll
-            for (int k = 0; k < K; ++k)
-              if (k == kf) {
-#pragma unroll
-                for (int p = 0; p < NP; ++p) {
-                  const float2 old = bkp[p * kMcmcThreads];
-                  s2[k][p].x = ok ? s2[k][p].x : old.x;
-                  s2[k][p].y = ok ? s2[k][p].y : old.y;
-                }
-                if (TAIL) st[k] = ok ? st[k] : bkt[0];
-              }
+            for (int k = 0; k < K; ++k) fs += f[k];
+            rej = rej || (fs > 1.f);
+          } else if (slot == kSlotTau) {
+            taun = tau + n * prop;
+            rej = taun <= 0.f;
           } else {
-            const bool sticks = (mask & kAllSticks) != 0u, isob = (mask & kIsoBit) != 0u;
-#pragma unroll
-            for (int p = 0; p < NP; ++p) {
-              if (sticks) {
-#pragma unroll
-                for (int k = 0; k < K; ++k) {
-                  const float2 old = bkp[(k * NP + p) * kMcmcThreads];
-                  s2[k][p].x = ok ? s2[k][p].x : old.x;
-                  s2[k][p].y = ok ? s2[k][p].y : old.y;
-                }
-              }
-              if (isob) {
-                const float2 old = bkp[(K * NP + p) * kMcmcThreads];
-                i2[p].x = ok ? i2[p].x : old.x;
-                i2[p].y = ok ? i2[p].y : old.y;
-              }
-            }
-            if (TAIL) {
-              if (sticks) {
-#pragma unroll
-                for (int k = 0; k < K; ++k) st[k] = ok ? st[k] : bkt[k * kMcmcThreads];
-              }
-              if (isob) it_ = ok ? it_ : bkt[K * kMcmcThreads];
-            }
+            S0n = S0 + n * prop;
+            rej = S0n < 0.f;
           }
-        }
-        if (ok) {
-          lik = likn;
-          switch (kind) {
-            case kSlotF0: f0 = f0n; p_f0 = pnew; break;
-            case kSlotTau: tau = taun; break;
-            case kSlotD: d = dn; p_d = pnew; break;
-            case kSlotDstd: dstd = dsn; p_dstd = pnew; break;
-            case kSlotR: R = Rn; p_R = pnew; break;
-            case kSlotS0: S0 = S0n; break;
-            case kSlotFibre0:
-            case kSlotFibre0 + 1:
-#pragma unroll
-              for (int k = 0; k < K; ++k)
-                if (k == kf) {
-                  th[k] = thn;
-                  ph[k] = phn;
-                  vx[k] = nvx;
-                  vy[k] = nvy;
-                  vz[k] = nvz;
-                  if (kind == kSlotFibre0) p_th[k] = pnew;
-                }
-              break;
-            default:
+          float likn = lik;
+          if (!group_all<TPV>(rej)) likn = lik_of(S0n, fn, f0n, taun);
+          const float dl = slot == kSlotTau ? dlik<RIC>(lik, likn, tau, taun, halfM, fM)
+                                            : dlik_same_tau<RIC>(lik, likn, halfM);
+          ok = !rej && ((pold - pnew) + dl > lu);
+          if (ok) {
+            lik = likn;
+            if (is_f) {
 #pragma unroll
               for (int k = 0; k < K; ++k)
                 if (k == kf) {
                   f[k] = fn[k];
                   p_f[k] = pnew;
                 }
-              break;
+            } else if (slot == kSlotF0) {
+              f0 = f0n;
+              p_f0 = pnew;
+            } else if (slot == kSlotTau) {
+              tau = taun;
+            } else {
+              S0 = S0n;
+            }
           }
-          if (gl == 0) sacc[slot] += 1;
         }
+        if (ok && gl == 0) sacc[slot] += 1;
       }
       // ---------------- record (CUDA/runmcmc_kernels.cu:1326-1339) ----------------
       if (it >= a.nburn && ((it - a.nburn + 1) % a.sampleevery) == 0 && sample < ns) {
