@@ -40,8 +40,8 @@ METRIC = "voxels/s, learned-init vs plain MCMC on 1 B200 at matched dyad error"
 WORKLOAD = ("whole-brain: model 2, 3 fibres, rician+f0+ardf0, 288 measurements, burnin 1000, njumps 1250, "
             "sampleevery 25, plain LM-initialised chain")
 WORKLOAD_LEARNED = ("whole-brain: model 2, 3 fibres, rician+f0+ardf0, 288 measurements, njumps 1250, sampleevery 25; "
-                    "learned form (network start state and proposal widths, burnin 200) against the plain "
-                    "LM-initialised chain (burnin 1000)")
+                    "learned-init batched form (network start state and proposal widths, burnin 200, one CUDA-graph "
+                    "launch per step) against the plain LM-initialised chain (burnin 1000)")
 
 
 def whole_brain_options() -> Options:
@@ -306,8 +306,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
-    ap.add_argument("--form", default="both", choices=["both", "plain", "learned"],
-                    help="forms to time (the headline value is the learned form's)")
+    ap.add_argument("--form", default="all", choices=["all", "plain", "learned", "learned_batched"],
+                    help="forms to time (the headline value is the learned, batched form's)")
     ap.add_argument("--freeze", type=int, default=0, choices=[0, 1, 2],
                     help="learned form: 0 network widths adapt, 1 frozen, 2 frozen after burn-in")
     ap.add_argument("--weights", default=None, help="initialiser weights (default: the committed whole-brain set)")
@@ -359,9 +359,10 @@ def main():
     prot = synth.three_shell(18, 90)
     M = prot.ndir
     chunk = args.chunk
-    forms = ["plain", "learned"] if args.form == "both" else [args.form]
+    forms = ["plain", "learned", "learned_batched"] if args.form == "all" else [args.form]
     wpath = args.weights or learned.default_weights_path("whole_brain")
-    mlp_h, meta = learned.load_weights(wpath) if "learned" in forms else (None, None)
+    uses_net = "learned" in forms or "learned_batched" in forms
+    mlp_h, meta = learned.load_weights(wpath) if uses_net else (None, None)
     if mlp_h is not None and int(meta["ndir"]) != M:
         raise SystemExit(f"{wpath}: trained for {int(meta['ndir'])} measurements, the workload has {M}")
     mlp_d = torch.from_numpy(mlp_h).cuda() if mlp_h is not None else None
@@ -427,8 +428,28 @@ def main():
         if ev:
             ev[3].record(stream)
 
-    steps_fn = {"plain": plain_step, "learned": learned_step}
-    launches = {"plain": 4, "learned": 6 + 6}  # learned: prepare, features, cast + 5 GEMMs, decode, mcmc, finish
+    lbatches = None
+    if "learned_batched" in forms:
+        # one batch (one captured graph) per input chunk; the chunk's voxels form one bucket
+        lbatches = [lib.Batch(o, [dict(data=chunks_d[c], bvecs=bvecs, bvals=bvals, model=o.model, nfibres=o.nfibres,
+                                       mlp=mlp_d, nburn=lo.nburn, freeze=args.freeze,
+                                       voxel_offset=rank * 1_000_000_000 + (2 + c) * chunk)], autotune=False)
+                    for c in range(2)]
+
+    def learned_batched_step(i, ev=None):
+        if ev:
+            ev[0].record(stream)
+        lbatches[i % 2].run()
+        if ev:
+            ev[1].record(stream)
+            ev[2].record(stream)
+            ev[3].record(stream)
+
+    steps_fn = {"plain": plain_step, "learned": learned_step, "learned_batched": learned_batched_step}
+    # learned: prepare, features, weight cast + 5 GEMMs per 32768 voxels, decode, mcmc, finish;
+    # learned_batched: one CUDA-graph launch (gather, the same kernels, scatter)
+    n_gemm = 5 * ((chunk + 32767) // 32768)
+    launches = {"plain": 4, "learned": 6 + n_gemm, "learned_batched": 1}
     timing = {}
     clocks = ClockSampler(local)
     clocks.start()
@@ -450,15 +471,18 @@ def main():
             pg.all_reduce(tt, op=pg.ReduceOp.MAX)
         timing[f] = tt.tolist()
     ck = clocks.stop()
-    head = "learned" if "learned" in forms else "plain"
-    t_step, t_init, t_mcmc, t_fin = timing[head]
+    head = "learned_batched" if "learned_batched" in forms else ("learned" if "learned" in forms else "plain")
+    t_step = timing[head][0]
     vox_total = chunk * args.steps * world
     value = vox_total / t_step
-    ho = lo if head == "learned" else o
+    # the MCMC kernel time for the roofline: from a form whose phases are timed separately
+    rf = "learned" if "learned" in forms else ("plain" if "plain" in forms else head)
+    t_mcmc = timing[rf][2] if rf != "learned_batched" else timing[rf][0]
+    ho = o if rf == "plain" else lo
 
     # ---- accuracy of the learned form against the plain chain on the same voxels ----
     accuracy = None
-    if not args.no_accuracy and len(forms) == 2:
+    if not args.no_accuracy and "plain" in forms and ("learned" in forms or "learned_batched" in forms):
         # the last timed step of each form ran on the same chunk; a second plain run with another
         # seed gives the plain-vs-plain agreement the learned form is measured against
         o2 = Options.make(**{f: getattr(o, f) for f, _ in Options._fields_ if f != "reserved"})
@@ -468,9 +492,11 @@ def main():
         torch.cuda.synchronize()
         n_acc = min(chunk, 32768)
         sub = lambda d: {k: v[..., :n_acc] for k, v in d.items()}  # noqa: E731  (voxel axis is last)
+        lout = lbatches[(args.warmup + args.steps - 1) % 2].outputs[0] if lbatches else outs["learned"][0]
         accuracy = {
             "voxels": n_acc,
-            "learned_vs_plain": learned.summary(o, sub(outs["learned"][0]), sub(outs["plain"][0])),
+            "form": "learned_batched" if lbatches else "learned",
+            "learned_vs_plain": learned.summary(o, sub(lout), sub(outs["plain"][0])),
             "plain_vs_plain_other_seed": learned.summary(o, sub(plain2[0]), sub(outs["plain"][0])),
             "f_se": "Monte-Carlo SE of each chain's mean (Geyer initial positive sequence), combined",
         }
@@ -490,7 +516,7 @@ def main():
             v.data, v.bvecs, v.bvals = hp[i % 2].data_ptr(), bh.ctypes.data, lh.ctypes.data
             v.grad = None
             v.voxel_offset = rank * 1_000_000_000 + i * chunk
-            if head == "learned":
+            if head != "plain":
                 lib._check(L.bpx_xfibres_learned_host(C.byref(lo), C.byref(v), mlp_h.ctypes.data, args.freeze,
                                                       C.byref(hout[1])), "xfibres_learned_host")
             else:
@@ -506,10 +532,10 @@ def main():
         te = torch.tensor([time.perf_counter() - t0], device="cuda", dtype=torch.float64)
         if pg:
             pg.all_reduce(te, op=pg.ReduceOp.MAX)
-        h2d = chunk * M * 4 + 4 * 4 * M + (mlp_h.nbytes if head == "learned" else 0)
+        h2d = chunk * M * 4 + 4 * 4 * M + (mlp_h.nbytes if head != "plain" else 0)
         d2h = sum(t.numel() * t.element_size() for t in hout[0].values())
         e2e = {"value": chunk * n_e2e * world / te.item(), "unit": "voxels/s", "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "steps": n_e2e, "entry": "bpx_xfibres_learned_host" if head == "learned"
+               "d2h_bytes_per_step": d2h, "steps": n_e2e, "entry": "bpx_xfibres_learned_host" if head != "plain"
                else "bpx_xfibres_host"}
 
     if args.prof:
@@ -525,7 +551,8 @@ def main():
     roof_time = max(mufu_v * chunk / mufu_peak, fp32_v * chunk / fma_peak)
     roofline = {
         "bound": "sfu", "achieved": achieved / 1e9, "peak": mufu_peak / 1e9, "unit": "Gop/s",
-        "frac": achieved / mufu_peak, "traffic": None, "kernel": "mcmc_kernel (burn-in + recording)",
+        "frac": achieved / mufu_peak, "traffic": None,
+        "kernel": f"mcmc_kernel (burn-in + recording), timed in the {rf} form's step",
         "fp32_achieved": fp32_achieved / 1e9, "fp32_peak": fma_peak / 1e9,
         "frac_of_roofline_time": roof_time / mcmc_per_launch_s,
         "peak_source": "measured on this GPU by bpx_measure_pipes (ex2.approx and FFMA issue-rate kernels)",
@@ -536,21 +563,22 @@ def main():
     for f in forms:
         ts_, ti, tm, tf = timing[f]
         forms_out[f] = {"voxels_per_s": vox_total / ts_, "ms_per_step": 1e3 * ts_ / args.steps,
-                        "phases_s_per_step": {"init": ti / args.steps, "mcmc": tm / args.steps,
-                                              "finish": tf / args.steps},
-                        "nburn": (lo if f == "learned" else o).nburn, "gpu_launches_per_step": launches[f]}
+                        "nburn": (o if f == "plain" else lo).nburn, "gpu_launches_per_step": launches[f]}
+        if f != "learned_batched":
+            forms_out[f]["phases_s_per_step"] = {"init": ti / args.steps, "mcmc": tm / args.steps,
+                                                 "finish": tf / args.steps}
     result = {
         "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_step / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-        "config": {"workload": WORKLOAD_LEARNED if head == "learned" else WORKLOAD,
+        "config": {"workload": WORKLOAD_LEARNED if head != "plain" else WORKLOAD,
                    "voxels_per_step_per_gpu": chunk, "ndir": M,
                    "l2": "flushed between steps (256 MB write) and inputs (151 MB/step) larger than L2",
-                   "form": head, "freeze_props": args.freeze if head == "learned" else None,
-                   "weights": os.path.relpath(wpath, ROOT) if head == "learned" else None},
+                   "form": head, "freeze_props": args.freeze if head != "plain" else None,
+                   "weights": os.path.relpath(wpath, ROOT) if head != "plain" else None},
         "forms": forms_out,
-        "learned_over_plain": (forms_out["learned"]["voxels_per_s"] / forms_out["plain"]["voxels_per_s"])
-        if len(forms) == 2 else None,
+        "learned_over_plain": (forms_out[head]["voxels_per_s"] / forms_out["plain"]["voxels_per_s"])
+        if "plain" in forms and head != "plain" else None,
         "accuracy": accuracy,
         "roofline": roofline,
         "e2e": e2e,

@@ -121,4 +121,7 @@ class Item(C.Structure):
         ("model", C.c_int32),
         ("nfibres", C.c_int32),
         ("out", Outputs),
+        ("mlp_params", C.c_void_p),
+        ("nburn", C.c_int32),
+        ("freeze_props", C.c_int32),
     ]

@@ -3,12 +3,13 @@
 // No counterpart in the reference (xfibres_gpu runs one subpart of one volume per call,
 // CUDA/xfibres_gpu.cu:29-146, with one fixed launch shape).
 //
-// Items are grouped into buckets of equal (model, fibres, measurements, b-matrix).  A bucket's
+// Items are grouped into buckets of equal (model, fibres, measurements, b-matrix, start: LM fits
+// or an initialiser network, burn-in).  A bucket's
 // voxels are packed into one contiguous set of buffers, so one fit, one MCMC and one finishing
 // launch (each grid-stride over the whole bucket) process every voxel of every item in it; the
 // chains keep each item's own RNG keys (item voxel_offset + local index), so a batched run equals
 // the per-item runs bit for bit.  The batch is captured once into a CUDA graph -- gather, then
-// per bucket [Rician clean-up, fit, MCMC, finish] on its own branch, then scatter to the items'
+// per bucket [Rician clean-up, fit or network start, MCMC, finish] on its own branch, then scatter to the items'
 // output buffers -- and every bpx_batch_run is one cudaGraphLaunch.
 //
 // Autotuner: for a bucket, every compiled (threads-per-voxel, measurements-per-lane) layout that
@@ -81,6 +82,8 @@ struct Bucket {
   int model, K, M;
   const float* bvecs;
   const float* bvals;
+  const float* mlp = nullptr;  // initialiser network (learned start) or NULL (LM fits)
+  int nburn = 0, freeze = 0;
   McmcLayout lay;
   std::vector<int> items;
   int n = 0;
@@ -96,6 +99,15 @@ struct Bucket {
   int* local_of = nullptr;
   ItemOut* item_tab = nullptr;
   bpx_outputs packed{};
+  // learned start: network inputs, outputs and working buffers
+  uint16_t* x = nullptr;
+  float* s0hat = nullptr;
+  float* netout = nullptr;
+  float* props = nullptr;
+  uint16_t* wbf = nullptr;
+  uint16_t* act0 = nullptr;
+  uint16_t* act1 = nullptr;
+  int chunk = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
 };
@@ -204,6 +216,11 @@ McmcArgs mcmc_args(const bpx_options& o, const Bucket& b) {
   a.seed = o.seed;
   a.voxel_offset = 0;
   a.voxel_keys = b.keys;
+  a.nburn = b.nburn;
+  if (b.mlp) {
+    a.props_in = b.props;
+    a.freeze_props = b.freeze;
+  }
   return a;
 }
 
@@ -343,10 +360,13 @@ bpx_status bpx_batch_create(const bpx_options* opts, const bpx_item* items, int3
     if (st != BPX_OK) return st;
     if (it.vol.grad) return api_fail(BPX_ERR_UNSUPPORTED, "gradnonlin items are not batched");
     if (it.vol.nvox == 0) continue;
+    const int nburn = it.nburn >= 0 ? it.nburn : opts->nburn;
+    const int freeze = it.mlp_params ? it.freeze_props : 0;
+    if (freeze < 0 || freeze > 2) return api_fail(BPX_ERR_INVALID_ARG, "item freeze_props must be 0, 1 or 2");
     Bucket* bk = nullptr;
     for (Bucket& c : b->buckets)
       if (c.model == it.model && c.K == it.nfibres && c.M == it.vol.ndir && c.bvecs == it.vol.bvecs &&
-          c.bvals == it.vol.bvals)
+          c.bvals == it.vol.bvals && c.mlp == it.mlp_params && c.nburn == nburn && c.freeze == freeze)
         bk = &c;
     if (!bk) {
       b->buckets.emplace_back();
@@ -356,6 +376,9 @@ bpx_status bpx_batch_create(const bpx_options* opts, const bpx_item* items, int3
       bk->M = it.vol.ndir;
       bk->bvecs = it.vol.bvecs;
       bk->bvals = it.vol.bvals;
+      bk->mlp = it.mlp_params;
+      bk->nburn = nburn;
+      bk->freeze = freeze;
     }
     bk->items.push_back(i);
     bk->n += it.vol.nvox;
@@ -379,11 +402,17 @@ bpx_status bpx_batch_create(const bpx_options* opts, const bpx_item* items, int3
   // ---- arena ----
   size_t total = 0;
   std::vector<size_t> base(b->buckets.size());
+  auto learned_bytes = [&](const Bucket& bk) -> size_t {
+    if (!bk.mlp) return 0;
+    const size_t n = bk.n, nin = bpx_mlp_nin(bk.M), chunk = std::min<size_t>(n, 32768);
+    return a256(n * nin * 2) + a256(n * 4) + a256(n * BPX_MLP_NOUT * 4) + a256((6 + 3 * bk.K) * n * 4) +
+           a256(mlp_weight_elems(bk.M) * 2) + 2 * a256(chunk * BPX_MLP_WIDTH * 2);
+  };
   auto bucket_bytes = [&](const Bucket& bk) {
     const size_t n = bk.n, K = bk.K, P = 2 + 3 * K + (bk.model >= 2 ? 1 : 0) + (opts->f0 ? 1 : 0);
     return a256(n * bk.M * 4) + a256(n * P * 4) + 2 * a256(n * 4) + a256(BPX_NREC(K) * ns * n * 4) + a256(n * 8) +
            a256(n * 8) + 2 * a256(n * 4) + a256(bk.items.size() * sizeof(ItemOut)) + 3 * a256(K * ns * n * 4) +
-           6 * a256(n * 4) + a256(K * n * 4) + a256(3 * K * n * 4);
+           6 * a256(n * 4) + a256(K * n * 4) + a256(3 * K * n * 4) + learned_bytes(bk);
   };
   for (size_t i = 0; i < b->buckets.size(); ++i) {
     base[i] = total;
@@ -421,6 +450,16 @@ bpx_status bpx_batch_create(const bpx_options* opts, const bpx_item* items, int3
     bk.packed.status = bk.status;  // written by the fit and MCMC kernels
     bk.packed.mean_f = (float*)take(K * n * 4);
     bk.packed.dyads = (float*)take(3 * K * n * 4);
+    if (bk.mlp) {
+      bk.chunk = (int)std::min<size_t>(n, 32768);
+      bk.x = (uint16_t*)take(n * bpx_mlp_nin(bk.M) * 2);
+      bk.s0hat = (float*)take(n * 4);
+      bk.netout = (float*)take(n * BPX_MLP_NOUT * 4);
+      bk.props = (float*)take((6 + 3 * K) * n * 4);
+      bk.wbf = (uint16_t*)take(mlp_weight_elems(bk.M) * 2);
+      bk.act0 = (uint16_t*)take((size_t)bk.chunk * BPX_MLP_WIDTH * 2);
+      bk.act1 = (uint16_t*)take((size_t)bk.chunk * BPX_MLP_WIDTH * 2);
+    }
     // voxel maps
     std::vector<uint64_t> keys(n);
     std::vector<const float*> src(n);
@@ -446,6 +485,13 @@ bpx_status bpx_batch_create(const bpx_options* opts, const bpx_item* items, int3
     BAT_CUDA(cudaStreamCreateWithFlags(&bk.stream, cudaStreamNonBlocking));
     BAT_CUDA(cudaEventCreateWithFlags(&bk.done, cudaEventDisableTiming));
   }
+  for (const Bucket& bk : b->buckets)
+    if (bk.mlp) {  // create the network kernels' error word now, outside the capture
+      int32_t code = 0;
+      st = bpx_mlp_poll_error(&code);
+      if (st != BPX_OK) return st;
+      break;
+    }
   // ---- capture: fork one branch per bucket, join ----
   BAT_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
   BAT_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
@@ -459,7 +505,30 @@ bpx_status bpx_batch_create(const bpx_options* opts, const bpx_item* items, int3
     const int gblocks = std::min((bk.n + 7) / 8, sms * 16);
     gather_kernel<<<gblocks, 256, 0, bk.stream>>>(bk.n, bk.M, bk.src, bk.data);
     if (opts->rician && ce == cudaSuccess) ce = launch_prepare(bk.n, bk.M, bk.data, bk.stream);
-    if (ce == cudaSuccess) ce = launch_fit(fit_args(*opts, bk), bk.K, opts->f0 != 0, bk.stream);
+    if (ce == cudaSuccess && !bk.mlp) ce = launch_fit(fit_args(*opts, bk), bk.K, opts->f0 != 0, bk.stream);
+    if (ce == cudaSuccess && bk.mlp) {
+      // learned start: features -> network (tcgen05) -> state, tau and proposal widths
+      bpx_options oi = *opts;
+      oi.model = bk.model;
+      oi.nfibres = bk.K;
+      bpx_volume pv{};
+      pv.nvox = bk.n;
+      pv.ndir = bk.M;
+      pv.data = bk.data;
+      pv.bvecs = bk.bvecs;
+      pv.bvals = bk.bvals;
+      bpx_status ls = bpx_mlp_features_dev(&pv, 0, bk.x, bk.s0hat, bk.stream);
+      if (ls == BPX_OK)
+        ls = mlp_forward_buffers(bk.M, bk.mlp, bk.n, bk.x, bk.netout, bk.wbf, bk.act0, bk.act1, bk.chunk, bk.stream);
+      if (ls == BPX_OK)
+        ls = bpx_mlp_decode_dev(&oi, bk.n, bk.netout, bk.s0hat, bk.params, bk.tau, bk.props, bk.status, bk.stream);
+      if (ls != BPX_OK) {
+        cudaGraph_t junk = nullptr;
+        cudaStreamEndCapture(b->cap, &junk);
+        if (junk) cudaGraphDestroy(junk);
+        return ls;
+      }
+    }
     if (ce == cudaSuccess) ce = launch_mcmc(mcmc_args(*opts, bk), bk.model, bk.K, opts->rician != 0, bk.lay, bk.stream);
     if (ce == cudaSuccess) {
       FinishArgs fa{};

@@ -98,6 +98,12 @@ struct McmcLayout {
   int tpv, mpl;
 };
 
+// the initialiser network's forward pass on caller buffers (weights copy of mlp_weight_elems
+// bf16 values, two activation buffers of chunk_rows x 256 bf16); bpx_mlp.cu
+size_t mlp_weight_elems(int ndir);
+bpx_status mlp_forward_buffers(int ndir, const float* params, int nvox, const uint16_t* x, float* out, uint16_t* wbf,
+                               uint16_t* buf0, uint16_t* buf1, int chunk_rows, cudaStream_t s);
+
 cudaError_t launch_fit(const FitArgs& a, int nfib, bool f0, cudaStream_t s);
 cudaError_t launch_prepare(int nvox, int ndir, float* data, cudaStream_t s);
 cudaError_t launch_mcmc(const McmcArgs& a, int model, int nfib, bool rician, McmcLayout lay, cudaStream_t s);

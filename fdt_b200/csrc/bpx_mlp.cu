@@ -420,6 +420,26 @@ Layout layout_of(const bpx_options* o) {
 
 }  // namespace
 
+namespace bpx {
+
+size_t mlp_weight_elems(int ndir) { return geom(ndir).nw; }
+
+bpx_status mlp_forward_buffers(int ndir, const float* params, int nvox, const uint16_t* x, float* out, uint16_t* wbf,
+                               uint16_t* buf0, uint16_t* buf1, int chunk_rows, cudaStream_t s) {
+  const Geom G = geom(ndir);
+  int* err = nullptr;
+  bpx_status st = error_word(&err);
+  if (st == BPX_OK) st = cast_weights(G, params, wbf, s);
+  for (int r0 = 0; st == BPX_OK && r0 < nvox; r0 += chunk_rows) {
+    const int n = std::min(chunk_rows, nvox - r0);
+    st = forward(G, params, wbf, n, x + (size_t)r0 * G.nin, out + (size_t)r0 * kOut, buf0, buf1, nullptr, nullptr, err,
+                 s);
+  }
+  return st;
+}
+
+}  // namespace bpx
+
 extern "C" {
 
 int32_t bpx_mlp_nin(int32_t ndir) { return ndir < 1 ? -1 : (ndir + 7) / 8 * 8; }

@@ -330,8 +330,9 @@ def states_from_records(opts: Options, records, sample: int):
 
 class Batch:
     """A batch of items run as one CUDA-graph launch (bpx_batch_*).  `items` is a list of dicts
-    with keys data, bvecs, bvals (device tensors), model, nfibres, voxel_offset (optional); the
-    outputs are allocated here (device) and returned by run() as a list of output dicts."""
+    with keys data, bvecs, bvals (device tensors), model, nfibres, and optionally voxel_offset,
+    mlp (device FP32 initialiser parameters: learned start), nburn, freeze; the outputs are
+    allocated here (device) and returned by run() as a list of output dicts."""
 
     def __init__(self, opts: Options, items: list, autotune: bool = True):
         torch = _torch()
@@ -347,6 +348,11 @@ class Batch:
             arr[i].vol = make_volume(it["data"], it["bvecs"], it["bvals"], int(it.get("voxel_offset", 0)))
             arr[i].model, arr[i].nfibres = it["model"], it["nfibres"]
             arr[i].out = out
+            arr[i].mlp_params = _ptr(it.get("mlp"))
+            arr[i].nburn = int(it.get("nburn", -1))
+            arr[i].freeze_props = int(it.get("freeze", 0))
+            if it.get("mlp") is not None:
+                self._keep.append(it["mlp"])
             self._keep.append((it["data"], it["bvecs"], it["bvals"]))
         h = C.c_void_p()
         _check(load().bpx_batch_create(C.byref(opts), arr, len(items), 1 if autotune else 0, C.byref(h)),

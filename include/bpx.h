@@ -327,7 +327,9 @@ bpx_status bpx_mlp_poll_error(int32_t* code);
 /*
  * ---- Batched form (no counterpart in the reference) ----
  * Many volumes ("items") with their own voxel counts, measurement counts, models and fibre counts
- * run as one CUDA-graph launch.  Items of equal (model, nfibres, ndir, bvecs, bvals) form a bucket
+ * run as one CUDA-graph launch; an item may start its chains from the initialiser network
+ * (mlp_params) instead of LM fits.  Items of equal (model, nfibres, ndir, bvecs, bvals, network,
+ * burn-in, freeze mode) form a bucket
  * whose voxels are packed so one fit, one MCMC and one finishing launch serve them all; the chains
  * keep each item's RNG keys (vol.voxel_offset + voxel), so results equal per-item runs.  The other
  * options (rician, f0, burn-in, ...) come from `opts` and are shared by all items.
@@ -341,6 +343,9 @@ typedef struct bpx_item {
   int32_t model;        /* 1..3 */
   int32_t nfibres;      /* 1..3 */
   bpx_outputs out;      /* device buffers; NULL fields are not written */
+  const float* mlp_params;  /* device: initialiser network for vol.ndir (learned start), or NULL (LM fits) */
+  int32_t nburn;            /* burn-in of this item's chains; < 0: opts->nburn */
+  int32_t freeze_props;     /* learned items: as bpx_mcmc_ex_dev */
 } bpx_item;
 typedef struct bpx_batch bpx_batch;
 bpx_status bpx_batch_create(const bpx_options* opts, const bpx_item* items, int32_t nitems,

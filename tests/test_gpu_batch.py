@@ -83,3 +83,53 @@ def test_autotuner_picks_a_covering_layout(torch):
     assert tpv * mpl >= 129 and (tpv, mpl) in t
     assert all(v > 0 for v in t.values()) and len(t) >= 2
     assert t[(tpv, mpl)] == min(t.values())
+
+
+def test_learned_items_in_a_batch_equal_the_learned_pipeline(torch):
+    """Items started from the initialiser network run in the same graph as LM-started items and
+    give exactly what the standalone learned pipeline gives with the bucket's layout."""
+    from fdt_b200 import learned, lib, synth
+
+    params, meta = learned.load_weights(learned.default_weights_path("whole_brain"))
+    prot = synth.three_shell(18, 90)
+    mlp = torch.from_numpy(params).cuda()
+    bv, bl = lib.to_device(prot.bvecs), lib.to_device(prot.bvals)
+    ys = [synth.make_volume(n, prot, 3, True, 25.0, seed=400 + n)[0] for n in (700, 300)]
+    opts = Options.make(rician=1, f0=1, ardf0=1, nburn=300, njumps=100, sampleevery=10)
+    items = [
+        dict(data=lib.to_device(ys[0]), bvecs=bv, bvals=bl, model=2, nfibres=3, mlp=mlp, nburn=80, freeze=0),
+        dict(data=lib.to_device(ys[1]), bvecs=bv, bvals=bl, model=2, nfibres=3, voxel_offset=9000),
+        dict(data=lib.to_device(ys[1]), bvecs=bv, bvals=bl, model=2, nfibres=3, mlp=mlp, nburn=80, freeze=2,
+             voxel_offset=9000),
+    ]
+    batch = lib.Batch(opts, items, autotune=False)
+    bks = batch.buckets()
+    assert len(bks) == 3
+    outs = batch.run()
+    torch.cuda.synchronize()
+    assert lib.poll_error() == 0
+    lay = (bks[0]["tpv"], bks[0]["mpl"])
+    for i, (n_b, fr) in [(0, (80, 0)), (2, (80, 2))]:
+        o = Options.make(model=2, nfibres=3, rician=1, f0=1, ardf0=1, nburn=n_b, njumps=100, sampleevery=10,
+                         mcmc_tpv=lay[0], mcmc_mpl=lay[1])
+        off = items[i].get("voxel_offset", 0)
+        ref = learned.xfibres_learned(o, lib.to_device(ys[0 if i == 0 else 1]), bv, bl, mlp, freeze=fr,
+                                      out=None) if off == 0 else None
+        if off:
+            d = lib.to_device(ys[1])
+            t, oo = lib.alloc_outputs(o, d.shape[0])
+            import ctypes as C
+
+            vol = lib.make_volume(d, bv, bl, voxel_offset=off)
+            rc = lib.load().bpx_xfibres_learned_dev(C.byref(o), C.byref(vol), mlp.data_ptr(), fr, C.byref(oo),
+                                                    C.c_void_p(torch.cuda.current_stream().cuda_stream))
+            assert rc == 0
+            ref = t
+        for k in ("th", "ph", "f", "mean_d", "dyads", "status"):
+            assert np.array_equal(outs[i][k].cpu().numpy(), ref[k].cpu().numpy()), (i, k)
+    o = Options.make(model=2, nfibres=3, rician=1, f0=1, ardf0=1, nburn=300, njumps=100, sampleevery=10,
+                     mcmc_tpv=bks[1]["tpv"], mcmc_mpl=bks[1]["mpl"])
+    ref = lib.xfibres_dev(o, lib.to_device(ys[1]), bv, bl, voxel_offset=9000)
+    for k in ("th", "f", "dyads"):
+        assert np.array_equal(outs[1][k].cpu().numpy(), ref[k].cpu().numpy()), (1, k)
+    batch.close()
