@@ -125,3 +125,16 @@ class Item(C.Structure):
         ("nburn", C.c_int32),
         ("freeze_props", C.c_int32),
     ]
+
+
+class PostProc(C.Structure):
+    """bpx_postproc: the bedpostx_postproc arithmetic's outputs."""
+
+    _fields_ = [
+        ("mean_th", C.c_void_p),
+        ("mean_ph", C.c_void_p),
+        ("dispersion", C.c_void_p),
+        ("dyads_thr", C.c_void_p),
+        ("dyads_modf", C.c_void_p),
+        ("mean_fsum", C.c_void_p),
+    ]

@@ -400,6 +400,32 @@ bpx_status bpx_finish_dev(const bpx_options* opts, int32_t nvox, const float* re
   return BPX_OK;
 }
 
+bpx_status bpx_postproc_dev(const bpx_options* opts, int32_t nvox, const bpx_outputs* out, float thr,
+                            bpx_postproc* post, void* stream) {
+  bpx_status st = check_opts(opts);
+  if (st != BPX_OK) return st;
+  if (nvox < 0 || !out || !post) return fail(BPX_ERR_INVALID_ARG, "bad arguments to bpx_postproc_dev");
+  if (nvox == 0) return BPX_OK;
+  if (!out->th || !out->ph || !out->mean_f || !out->dyads)
+    return fail(BPX_ERR_INVALID_ARG, "bpx_postproc_dev needs out->th, ph, mean_f and dyads");
+  const int ns = bpx_nsamples(opts);
+  if (ns < 1) return fail(BPX_ERR_INVALID_ARG, "no samples (njumps < sampleevery)");
+  st = check_device();
+  if (st != BPX_OK) return st;
+  PostArgs a{};
+  a.nvox = nvox;
+  a.nsamples = ns;
+  a.nfib = opts->nfibres;
+  a.th = out->th;
+  a.ph = out->ph;
+  a.mean_f = out->mean_f;
+  a.dyads = out->dyads;
+  a.thr = thr;
+  a.post = *post;
+  BPX_CUDA(launch_postproc(a, (cudaStream_t)stream));
+  return BPX_OK;
+}
+
 bpx_status bpx_energy_dev(const bpx_options* opts, const bpx_volume* vol, const float* states, float* lik, float* prior,
                           void* stream) {
   bpx_status st = check_opts(opts);

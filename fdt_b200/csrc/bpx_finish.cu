@@ -13,8 +13,9 @@
 
 namespace bpx {
 
-// principal eigenvector of a symmetric 3x3 (cyclic Jacobi, FP64), largest |component| positive
-__device__ void principal_vector(double (&A)[3][3], double (&out)[3]) {
+// principal eigenvector of a symmetric 3x3 (cyclic Jacobi, FP64), largest |component| positive;
+// returns the largest eigenvalue
+__device__ double principal_vector(double (&A)[3][3], double (&out)[3]) {
   double V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
   for (int sweep = 0; sweep < 50; ++sweep) {
     const double off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
@@ -60,6 +61,7 @@ __device__ void principal_vector(double (&A)[3][3], double (&out)[3]) {
   const double sg = col[big] < 0 ? -1.0 : 1.0;
 #pragma unroll
   for (int r = 0; r < 3; ++r) out[r] = sg * col[r];
+  return A[best][best];
 }
 
 template <int K>
@@ -149,6 +151,73 @@ __global__ void finish_kernel(FinishArgs a) {
       for (int r = 0; r < 3; ++r) out.dyads[((size_t)o * 3 + r) * nvox + v] = (float)pv[r];
     }
   }
+}
+
+// bedpostx_postproc_gpu.sh arithmetic (CUDA/bedpostx_postproc_gpu.sh:20-49) on the finished
+// outputs, one thread per voxel: fslmaths -Tmean of merged_th/ph, the dispersion of each fibre's
+// mean dyadic tensor (make_dyadic_vectors.cc:60-92: 1 - max |eigenvalue|), maskdyads
+// (dyads{k} where mean_f{k} >= thr, fslmaths -thr -bin -mul), the _modf{k} scaling by
+// mean_f{k}/mean_f1 (fslmaths -div gives 0 where the divisor is 0) and mean_fsumsamples.
+template <int K>
+__global__ void postproc_kernel(PostArgs a) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= a.nvox) return;
+  const int ns = a.nsamples, nvox = a.nvox;
+  const bpx_postproc& p = a.post;
+  float mf[K];
+  double fsum = 0.0;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    mf[k] = a.mean_f[(size_t)k * nvox + v];
+    fsum += mf[k];
+    double sth = 0, sph = 0, A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int s = 0; s < ns; ++s) {
+      const size_t o = ((size_t)k * ns + s) * nvox + v;
+      const float th = a.th[o], ph = a.ph[o];
+      sth += th;
+      sph += ph;
+      float st, ct, sp, cp;
+      sincosf(th, &st, &ct);
+      sincosf(ph, &sp, &cp);
+      const double x[3] = {(double)st * cp, (double)st * sp, (double)ct};
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) A[i][j] += x[i] * x[j] / ns;
+    }
+    if (p.mean_th) p.mean_th[(size_t)k * nvox + v] = (float)(sth / ns);
+    if (p.mean_ph) p.mean_ph[(size_t)k * nvox + v] = (float)(sph / ns);
+    if (p.dispersion) {
+      double pv[3];
+      const double lmax = principal_vector(A, pv);  // the tensor is positive semi-definite
+      p.dispersion[(size_t)k * nvox + v] = (float)(1.0 - fabs(lmax));
+    }
+  }
+  if (p.mean_fsum) p.mean_fsum[v] = (float)fsum;
+#pragma unroll
+  for (int k = 1; k < K; ++k) {
+    const bool keep = mf[k] >= a.thr && mf[k] != 0.f;
+    const float ratio = mf[0] != 0.f ? mf[k] / mf[0] : 0.f;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const size_t o = ((size_t)k * 3 + r) * nvox + v;
+      const float dt = keep ? a.dyads[o] : 0.f;
+      if (p.dyads_thr) p.dyads_thr[o] = dt;
+      if (p.dyads_modf) p.dyads_modf[o] = dt * ratio;
+    }
+  }
+}
+
+cudaError_t launch_postproc(const PostArgs& a, cudaStream_t s) {
+  if (a.nvox == 0) return cudaSuccess;
+  const int threads = 128, grid = (a.nvox + threads - 1) / threads;
+  switch (a.nfib) {
+    case 1: postproc_kernel<1><<<grid, threads, 0, s>>>(a); break;
+    case 2: postproc_kernel<2><<<grid, threads, 0, s>>>(a); break;
+    case 3: postproc_kernel<3><<<grid, threads, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
 }
 
 cudaError_t launch_finish(const FinishArgs& a, cudaStream_t s) {

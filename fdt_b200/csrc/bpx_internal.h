@@ -93,6 +93,16 @@ struct FinishArgs {
   bpx_outputs out;
 };
 
+struct PostArgs {
+  int nvox, nsamples, nfib;
+  const float* th;      // [K][ns][nvox] (finished, fibres sorted)
+  const float* ph;
+  const float* mean_f;  // [K][nvox]
+  const float* dyads;   // [K][3][nvox]
+  float thr;
+  bpx_postproc post;
+};
+
 // Launch layout of the MCMC kernel: TPV lanes per voxel, at most MPL measurements per lane.
 struct McmcLayout {
   int tpv, mpl;
@@ -111,5 +121,6 @@ McmcLayout choose_layout(int model, int nfib, bool rician, int ndir);
 bool layout_supported(int model, int nfib, bool rician, McmcLayout lay);
 cudaError_t launch_energy(const EnergyArgs& a, int model, int nfib, bool rician, cudaStream_t s);
 cudaError_t launch_finish(const FinishArgs& a, cudaStream_t s);
+cudaError_t launch_postproc(const PostArgs& a, cudaStream_t s);
 
 }  // namespace bpx

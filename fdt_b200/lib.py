@@ -11,7 +11,7 @@ import os
 
 import numpy as np
 
-from .abi import BPX_NSTATE, Item, Options, Outputs, Volume, nrec
+from .abi import BPX_NSTATE, Item, Options, Outputs, PostProc, Volume, nrec
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libbpx.so")
@@ -66,6 +66,8 @@ _SIGS = {
     "bpx_batch_destroy": (C.c_int, [C.c_void_p]),
     "bpx_autotune_layout": (C.c_int, [C.POINTER(Options), C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
                                       C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_float), C.c_void_p]),
+    "bpx_postproc_dev": (C.c_int, [C.POINTER(Options), C.c_int32, C.POINTER(Outputs), C.c_float, C.POINTER(PostProc),
+                                   C.c_void_p]),
     "bpx_synth_dev": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_uint64, C.c_float,
                                 C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
@@ -395,3 +397,22 @@ def autotune_layout(opts: Options, bvecs, bvals, sample: int = 2048):
     _check(L.bpx_autotune_layout(C.byref(opts), int(bvals.shape[0]), _ptr(bvecs), _ptr(bvals), sample, C.byref(tpv),
                                  C.byref(mpl), t, None), "bpx_autotune_layout")
     return tpv.value, mpl.value, {lays[i]: t[i] for i in range(len(lays)) if t[i] >= 0}
+
+
+def postproc(opts: Options, outputs: dict, thr: float = 0.05) -> dict:
+    """bedpostx_postproc arithmetic on finished device outputs: mean_th, mean_ph, dispersion
+    [K][n], dyads_thr, dyads_modf [K][3][n] (fibres 2..K), mean_fsum [n] (device tensors)."""
+    torch = _torch()
+    K, n = opts.nfibres, int(outputs["mean_d"].shape[0])
+    r = dict(mean_th=torch.zeros((K, n), device="cuda"), mean_ph=torch.zeros((K, n), device="cuda"),
+             dispersion=torch.zeros((K, n), device="cuda"), dyads_thr=torch.zeros((K, 3, n), device="cuda"),
+             dyads_modf=torch.zeros((K, 3, n), device="cuda"), mean_fsum=torch.zeros(n, device="cuda"))
+    o = Outputs()
+    for k in OUT_KEYS:
+        setattr(o, k, outputs[k].data_ptr())
+    pp = PostProc()
+    for k in r:
+        setattr(pp, k, r[k].data_ptr())
+    _check(load().bpx_postproc_dev(C.byref(opts), n, C.byref(o), thr, C.byref(pp), _stream(torch)),
+           "bpx_postproc_dev")
+    return r

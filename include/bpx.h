@@ -367,6 +367,26 @@ bpx_status bpx_autotune_layout(const bpx_options* opts, int32_t ndir, const floa
                                const float* bvals, int32_t sample, int32_t* tpv, int32_t* mpl,
                                float* seconds_per_voxel, void* stream);
 
+/*
+ * bedpostx_postproc_gpu.sh arithmetic (CUDA/bedpostx_postproc_gpu.sh:20-49) from finished outputs
+ * (out->th, ph, mean_f, dyads on the device, as bpx_finish_dev leaves them): per fibre the
+ * sample means of th and ph (fslmaths -Tmean), the dispersion 1 - max|eigenvalue| of the mean
+ * dyadic tensor (make_dyadic_vectors.cc), for fibres 2..K the dyads masked where mean_f >= thr
+ * (maskdyads, thr 0.05 in bedpostx) and those scaled by mean_f{k}/mean_f1 (_modf{k}), and
+ * mean_fsumsamples.  Rows of fibre 1 in dyads_thr/dyads_modf are not written.  NULL outputs are
+ * skipped.
+ */
+typedef struct bpx_postproc {
+  float* mean_th;     /* [nfib][nvox] mean_th{k}samples */
+  float* mean_ph;     /* [nfib][nvox] mean_ph{k}samples */
+  float* dispersion;  /* [nfib][nvox] dyads{k}_dispersion */
+  float* dyads_thr;   /* [nfib][3][nvox] dyads{k}_thr0.05 (k >= 2) */
+  float* dyads_modf;  /* [nfib][3][nvox] dyads{k}_thr0.05_modf{k} (k >= 2) */
+  float* mean_fsum;   /* [nvox] mean_fsumsamples */
+} bpx_postproc;
+bpx_status bpx_postproc_dev(const bpx_options* opts, int32_t nvox, const bpx_outputs* out, float thr,
+                            bpx_postproc* post, void* stream);
+
 /* Free the per-device workspace cache of the current device. */
 bpx_status bpx_release_workspace(void);
 
