@@ -2,7 +2,8 @@
 
     python -m fdt_b200.bedpostx SUBJDIR [--nf 3] [--model 2] [--rician] [--f0] [--ardf0] ...
 
-Reads SUBJDIR/{data, nodif_brain_mask}.nii.gz, bvecs and bvals (the inputs bedpostx_gpu reads),
+Reads SUBJDIR/{data, nodif_brain_mask}.nii.gz, bvecs and bvals (the inputs bedpostx_gpu reads;
+grad_dev with --gradnonlin),
 runs the per-voxel path on the GPU (LM-initialised, or --learned WEIGHTS for the learned start),
 the bedpostx_postproc arithmetic on the GPU, and writes into SUBJDIR.bedpostX/ the files
 merge_parts_gpu and bedpostx_postproc_gpu.sh produce:
@@ -89,6 +90,19 @@ def read_subject(subjdir: str):
     return y, mask, hdr, bvecs.astype(np.float32), bvals.astype(np.float32)
 
 
+def read_grad_dev(subjdir: str, mask: np.ndarray) -> np.ndarray:
+    """grad_dev (X x Y x Z x 9, the gradient-nonlinearity tensor per voxel) at the mask's voxels:
+    [nvox][9], the rows split_parts_gpu takes with grad.matrix(mask) (CUDA/split_parts_gpu.cc:114-120)."""
+    for ext in (".nii.gz", ".nii"):
+        p = os.path.join(subjdir, "grad_dev" + ext)
+        if os.path.exists(p):
+            g, _ = nifti.read(p)
+            if g.shape[:3] != mask.shape or g.ndim != 4 or g.shape[3] != 9:
+                raise ValueError("grad_dev must be X x Y x Z x 9 over the mask's grid")
+            return nifti.to_matrix(g, mask).astype(np.float32)
+    raise FileNotFoundError(os.path.join(subjdir, "grad_dev.nii.gz"))
+
+
 def write_parts(outdir: str, outputs: dict, opts: Options, nparts: int) -> None:
     """The reference's part files: diff_parts/data_part_XXXX/<name>J, float64 [nt][part voxels]."""
     nvox = int(np.asarray(outputs["mean_d"]).shape[0])
@@ -167,6 +181,8 @@ def run(subjdir: str, opts: Options, learned_weights: str | None = None, nparts:
     os.makedirs(outdir, exist_ok=True)
     d = lib.to_device(y)
     bv, bl = lib.to_device(bvecs), lib.to_device(bvals)
+    if opts.gradnonlin:  # per-voxel corrected b-matrix on the device (correct_bvals_bvecs)
+        bv, bl = lib.gradnonlin(lib.to_device(read_grad_dev(subjdir, mask)), bv, bl)
     if learned_weights:
         params, meta = learned.load_weights(learned_weights)
         if int(meta["ndir"]) != y.shape[1]:
@@ -204,7 +220,7 @@ def options_from_args(a) -> Options:
     return Options.make(model=a.model, nfibres=a.nf, fudge=a.fudge, njumps=a.nj, nburn=a.bi, sampleevery=a.se,
                         updateproposalevery=a.upe, no_ard=int(a.noard), all_ard=int(a.allard), nonlin=int(a.nonlinear),
                         cnonlin=int(not a.nonlinear), rician=int(a.rician), f0=int(a.f0), ardf0=int(a.ardf0),
-                        seed=a.seed)
+                        gradnonlin=int(a.gradnonlin), seed=a.seed)
 
 
 def main(argv=None) -> None:
@@ -225,6 +241,7 @@ def main(argv=None) -> None:
     ap.add_argument("--rician", action="store_true")
     ap.add_argument("--f0", action="store_true")
     ap.add_argument("--ardf0", action="store_true")
+    ap.add_argument("--gradnonlin", action="store_true", help="per-voxel b-matrix from SUBJDIR/grad_dev")
     ap.add_argument("--learned", default=None, help="initialiser weights: learned start (use --bi 200)")
     ap.add_argument("--freeze", type=int, default=0, choices=[0, 1, 2])
     ap.add_argument("--parts", type=int, default=0, help="also write (run) or read (merge) this many part files")

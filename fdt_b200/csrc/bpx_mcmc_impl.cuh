@@ -589,20 +589,30 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
           lu = __shfl_sync(0xffffffffu, lq, slot % TPV, TPV);
         }
         const float prop = sprop[slot];
-        bool ok = false;
-        if (slot >= kSlotFibre0 && (slot - kSlotFibre0) % 3 != 2) {
-          // ---------- theta or phi of fibre kf: only that fibre's stick signals change ----------
-          const int kf = (slot - kSlotFibre0) / 3;
-          const bool is_th = (slot - kSlotFibre0) % 3 == 0;
+        // ---------- the proposal: state, prior, and the signals it changes (updated in place) ----------
+        // kind 0: f0, tau, S0 or a fraction (likelihood only); 1: theta/phi of fibre kf (one stick);
+        // 2: d, d_std or R (every signal that depends on it)
+        const int fib = slot - kSlotFibre0;
+        const int kind = (slot >= kSlotFibre0 && fib % 3 != 2) ? 1 : ((slot == kSlotD || slot == kSlotDstd || slot == kSlotR) ? 2 : 0);
+        const int kf = slot >= kSlotFibre0 ? fib / 3 : 0;
+        float S0n = S0, taun = tau, f0n = f0, fn[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) fn[k] = f[k];
+        float pold = 0.f, pnew = 0.f, thn = 0.f, phn = 0.f, nvx = 0.f, nvy = 0.f, nvz = 0.f, dn = d, dsn = dstd, Rn = R;
+        bool rej = false, sticks = false, isob = false;
+        if (kind == 1) {
+          const bool is_th = fib % 3 == 0;
           const float tho = pick<K>(th, kf), pho = pick<K>(ph, kf);
-          const float thn = is_th ? tho + n * prop : tho;
-          const float phn = is_th ? pho : pho + n * prop;
-          const float pold = is_th ? pick<K>(p_th, kf) : 0.f;
-          const float pnew = is_th ? th_prior(thn) : 0.f;
+          thn = is_th ? tho + n * prop : tho;
+          phn = is_th ? pho : pho + n * prop;
+          pold = is_th ? pick<K>(p_th, kf) : 0.f;
+          pnew = is_th ? th_prior(thn) : 0.f;
           float sn, cs, sp_, cp;
           sincosf(thn, &sn, &cs);
           sincosf(phn, &sp_, &cp);
-          const float nvx = sn * cp, nvy = sn * sp_, nvz = cs;
+          nvx = sn * cp;
+          nvy = sn * sp_;
+          nvz = cs;
           const SigParams<MODEL> sp = sig_params<MODEL>(d, dstd, R);
           const float2 beta2 = make_float2(sp.beta, sp.beta);
           const float2 nvx2 = vbc<float2>(nvx), nvy2 = vbc<float2>(nvy), nvz2 = vbc<float2>(nvz);
@@ -626,34 +636,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
                 st[k] = stick_v<MODEL, float>(sp, g.w, sp.beta * g.w, dp * dp);
               }
             }
-          const float likn = lik_of(S0, f, f0, tau);
-          ok = (pold - pnew) + dlik_same_tau<RIC>(lik, likn, halfM) > lu;
-          if (!group_all<TPV>(ok)) {
-#pragma unroll
-            for (int k = 0; k < K; ++k)
-              if (k == kf) {
-#pragma unroll
-                for (int p = 0; p < NP; ++p) s2[k][p] = keep_or_restore<TPV>(ok, s2[k][p], bkp[p * kMcmcThreads]);
-                if (TAIL) st[k] = keep_or_restore<TPV>(ok, st[k], bkt[0]);
-              }
-          }
-          if (ok) {
-            lik = likn;
-#pragma unroll
-            for (int k = 0; k < K; ++k)
-              if (k == kf) {
-                th[k] = thn;
-                ph[k] = phn;
-                vx[k] = nvx;
-                vy[k] = nvy;
-                vz[k] = nvz;
-                if (is_th) p_th[k] = pnew;
-              }
-          }
-        } else if (slot == kSlotD || slot == kSlotDstd || slot == kSlotR) {
-          // ---------- d, d_std or R: every signal that depends on it changes ----------
-          float dn = d, dsn = dstd, Rn = R, pold, pnew;
-          bool rej, sticks, isob;
+        } else if (kind == 2) {
           if (slot == kSlotD) {
             dn = d + n * prop;
             rej = (dn < 0.f || dn > kUpperDiff);
@@ -676,15 +659,55 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
             pold = p_R;
             pnew = rej ? p_R : pr2;
             sticks = true;
-            isob = false;
           }
-          float likn = lik;
-          const bool live = !group_all<TPV>(rej);
-          if (live) {
-            all_signals(dn, dsn, Rn, sticks, isob, true);
-            likn = lik_of(S0, f, f0, tau);
+          if (!group_all<TPV>(rej)) all_signals(dn, dsn, Rn, sticks, isob, true);
+        } else if (slot >= kSlotFibre0) {
+          const float fkn = pick<K>(f, kf) + n * prop;
+          rej = (fkn <= 0.f || fkn >= 1.f);
+          const bool lj = pick<K>(lam, kf);
+          pold = pick<K>(p_f, kf);
+          pnew = rej ? pold : pr.fudge * ((pr.can_use_ard && lj) ? logf(fkn) : 0.f);
+          float fs = f0;
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            if (k == kf) fn[k] = fkn;
+            fs += fn[k];
           }
-          ok = !rej && ((pold - pnew) + dlik_same_tau<RIC>(lik, likn, halfM) > lu);
+          rej = rej || (fs > 1.f);
+        } else if (slot == kSlotF0) {
+          f0n = f0 + n * prop;
+          rej = (f0n <= 0.f || f0n >= 1.f);
+          pold = p_f0;
+          pnew = rej ? p_f0 : (a.ardf0 ? logf(f0n) : 0.f);
+          float fs = f0n;
+#pragma unroll
+          for (int k = 0; k < K; ++k) fs += f[k];
+          rej = rej || (fs > 1.f);
+        } else if (slot == kSlotTau) {
+          taun = tau + n * prop;
+          rej = taun <= 0.f;
+        } else {
+          S0n = S0 + n * prop;
+          rej = S0n < 0.f;
+        }
+        // ---------- likelihood of the proposed state and the decision (one body for every kind) ----------
+        float likn = lik;
+        const bool live = !group_all<TPV>(rej);
+        if (live) likn = lik_of(S0n, fn, f0n, taun);
+        const float dl = slot == kSlotTau ? dlik<RIC>(lik, likn, tau, taun, halfM, fM) : dlik_same_tau<RIC>(lik, likn, halfM);
+        const bool ok = !rej && ((pold - pnew) + dl > lu);
+        // ---------- restore the signals of a rejected proposal, or commit an accepted one ----------
+        if (kind == 1) {
+          if (!group_all<TPV>(ok)) {
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+              if (k == kf) {
+#pragma unroll
+                for (int p = 0; p < NP; ++p) s2[k][p] = keep_or_restore<TPV>(ok, s2[k][p], bkp[p * kMcmcThreads]);
+                if (TAIL) st[k] = keep_or_restore<TPV>(ok, st[k], bkt[0]);
+              }
+          }
+        } else if (kind == 2) {
           if (live && !group_all<TPV>(ok)) {
 #pragma unroll
             for (int p = 0; p < NP; ++p) {
@@ -703,8 +726,21 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
               if (isob) it_ = keep_or_restore<TPV>(ok, it_, bkt[K * kMcmcThreads]);
             }
           }
-          if (ok) {
-            lik = likn;
+        }
+        if (ok) {
+          lik = likn;
+          if (kind == 1) {
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+              if (k == kf) {
+                th[k] = thn;
+                ph[k] = phn;
+                vx[k] = nvx;
+                vy[k] = nvy;
+                vz[k] = nvz;
+                if (fib % 3 == 0) p_th[k] = pnew;
+              }
+          } else if (kind == 2) {
             if (slot == kSlotD) {
               d = dn;
               p_d = pnew;
@@ -715,70 +751,23 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
               R = Rn;
               p_R = pnew;
             }
-          }
-        } else {
-          // ---------- f0, tau, S0 or a fraction f_k: no signal changes ----------
-          const bool is_f = slot >= kSlotFibre0;
-          const int kf = is_f ? (slot - kSlotFibre0) / 3 : 0;
-          float S0n = S0, taun = tau, f0n = f0, fn[K];
+          } else if (slot >= kSlotFibre0) {
 #pragma unroll
-          for (int k = 0; k < K; ++k) fn[k] = f[k];
-          float pold = 0.f, pnew = 0.f;
-          bool rej;
-          if (is_f) {
-            const float fkn = pick<K>(f, kf) + n * prop;
-            rej = (fkn <= 0.f || fkn >= 1.f);
-            const bool lj = pick<K>(lam, kf);
-            pold = pick<K>(p_f, kf);
-            pnew = rej ? pold : pr.fudge * ((pr.can_use_ard && lj) ? logf(fkn) : 0.f);
-            float fs = f0;
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-              if (k == kf) fn[k] = fkn;
-              fs += fn[k];
-            }
-            rej = rej || (fs > 1.f);
+            for (int k = 0; k < K; ++k)
+              if (k == kf) {
+                f[k] = fn[k];
+                p_f[k] = pnew;
+              }
           } else if (slot == kSlotF0) {
-            f0n = f0 + n * prop;
-            rej = (f0n <= 0.f || f0n >= 1.f);
-            pold = p_f0;
-            pnew = rej ? p_f0 : (a.ardf0 ? logf(f0n) : 0.f);
-            float fs = f0n;
-#pragma unroll
-            for (int k = 0; k < K; ++k) fs += f[k];
-            rej = rej || (fs > 1.f);
+            f0 = f0n;
+            p_f0 = pnew;
           } else if (slot == kSlotTau) {
-            taun = tau + n * prop;
-            rej = taun <= 0.f;
+            tau = taun;
           } else {
-            S0n = S0 + n * prop;
-            rej = S0n < 0.f;
+            S0 = S0n;
           }
-          float likn = lik;
-          if (!group_all<TPV>(rej)) likn = lik_of(S0n, fn, f0n, taun);
-          const float dl = slot == kSlotTau ? dlik<RIC>(lik, likn, tau, taun, halfM, fM)
-                                            : dlik_same_tau<RIC>(lik, likn, halfM);
-          ok = !rej && ((pold - pnew) + dl > lu);
-          if (ok) {
-            lik = likn;
-            if (is_f) {
-#pragma unroll
-              for (int k = 0; k < K; ++k)
-                if (k == kf) {
-                  f[k] = fn[k];
-                  p_f[k] = pnew;
-                }
-            } else if (slot == kSlotF0) {
-              f0 = f0n;
-              p_f0 = pnew;
-            } else if (slot == kSlotTau) {
-              tau = taun;
-            } else {
-              S0 = S0n;
-            }
-          }
+          if (gl == 0) sacc[slot] += 1;
         }
-        if (ok && gl == 0) sacc[slot] += 1;
       }
       // ---------------- record (CUDA/runmcmc_kernels.cu:1326-1339) ----------------
       if (it >= a.nburn && ((it - a.nburn + 1) % a.sampleevery) == 0 && sample < ns) {
