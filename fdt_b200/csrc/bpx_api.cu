@@ -297,8 +297,12 @@ bpx_status bpx_gradnonlin_dev(int32_t nvox, int32_t ndir, const float* grad, con
   return BPX_OK;
 }
 
-bpx_status bpx_fit_dev(const bpx_options* opts, const bpx_volume* vol, float* params, float* tau, uint32_t* status,
-                       void* stream) {
+}  // extern "C"
+
+namespace bpx {
+
+bpx_status fit_dev_scratch(const bpx_options* opts, const bpx_volume* vol, float* params, float* tau, uint32_t* status,
+                           void* scratch, void* stream) {
   bpx_status st = check_opts(opts);
   if (st == BPX_OK) st = check_vol(vol, true);
   if (st != BPX_OK) return st;
@@ -322,8 +326,25 @@ bpx_status bpx_fit_dev(const bpx_options* opts, const bpx_volume* vol, float* pa
   a.rician = opts->rician;
   a.nonlin = opts->nonlin;
   a.R = opts->R_prior_mean;
+  a.scratch = (double*)scratch;
+  a.flags = (uint32_t*)((char*)scratch + (size_t)vol->nvox * 16 * sizeof(double));
   BPX_CUDA(launch_fit(a, opts->nfibres, opts->f0 != 0, (cudaStream_t)stream));
   return BPX_OK;
+}
+
+}  // namespace bpx
+
+extern "C" {
+
+bpx_status bpx_fit_dev(const bpx_options* opts, const bpx_volume* vol, float* params, float* tau, uint32_t* status,
+                       void* stream) {
+  if (vol && vol->nvox > 0) {
+    void* scratch = nullptr;
+    const bpx_status st = workspace((size_t)vol->nvox * kFitScratchBytes, &scratch, kWsFit);
+    if (st != BPX_OK) return st;
+    return fit_dev_scratch(opts, vol, params, tau, status, scratch, stream);
+  }
+  return fit_dev_scratch(opts, vol, params, tau, status, nullptr, stream);
 }
 
 bpx_status bpx_mcmc_ex_dev(const bpx_options* opts, const bpx_volume* vol, const float* params, const float* tau,

@@ -93,6 +93,7 @@ struct Bucket {
   float* tau = nullptr;
   uint32_t* status = nullptr;
   float* rec = nullptr;
+  void* fit_scratch = nullptr;  // LM start: FP64 parameters between the fit stages
   uint64_t* keys = nullptr;
   const float** src = nullptr;
   int* item_of = nullptr;
@@ -181,6 +182,8 @@ FitArgs fit_args(const bpx_options& o, const Bucket& b) {
   a.rician = o.rician;
   a.nonlin = o.nonlin;
   a.R = o.R_prior_mean;
+  a.scratch = (double*)b.fit_scratch;
+  a.flags = (uint32_t*)((char*)b.fit_scratch + (size_t)b.n * 16 * sizeof(double));
   return a;
 }
 
@@ -412,7 +415,8 @@ bpx_status bpx_batch_create(const bpx_options* opts, const bpx_item* items, int3
     const size_t n = bk.n, K = bk.K, P = 2 + 3 * K + (bk.model >= 2 ? 1 : 0) + (opts->f0 ? 1 : 0);
     return a256(n * bk.M * 4) + a256(n * P * 4) + 2 * a256(n * 4) + a256(BPX_NREC(K) * ns * n * 4) + a256(n * 8) +
            a256(n * 8) + 2 * a256(n * 4) + a256(bk.items.size() * sizeof(ItemOut)) + 3 * a256(K * ns * n * 4) +
-           6 * a256(n * 4) + a256(K * n * 4) + a256(3 * K * n * 4) + learned_bytes(bk);
+           6 * a256(n * 4) + a256(K * n * 4) + a256(3 * K * n * 4) + learned_bytes(bk) +
+           (bk.mlp ? 0 : a256(n * kFitScratchBytes));
   };
   for (size_t i = 0; i < b->buckets.size(); ++i) {
     base[i] = total;
@@ -450,6 +454,7 @@ bpx_status bpx_batch_create(const bpx_options* opts, const bpx_item* items, int3
     bk.packed.status = bk.status;  // written by the fit and MCMC kernels
     bk.packed.mean_f = (float*)take(K * n * 4);
     bk.packed.dyads = (float*)take(3 * K * n * 4);
+    if (!bk.mlp) bk.fit_scratch = take(n * kFitScratchBytes);
     if (bk.mlp) {
       bk.chunk = (int)std::min<size_t>(n, 32768);
       bk.x = (uint16_t*)take(n * bpx_mlp_nin(bk.M) * 2);

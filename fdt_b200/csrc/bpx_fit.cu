@@ -958,29 +958,154 @@ __device__ __forceinline__ Real predict_final(int model, const Real* q, int o, b
 }
 
 // ------------------------------------------------------------------------------------------
-// the fit kernel: one warp per voxel, grid-stride over voxels
+// the fit as four kernels, one per stage, so each holds one or two LM instances and its warps
+// run the same code (the single kernel with every stage was instruction-fetch bound):
+//   A  non-finite check, DTI, the first LM fit (PVM_single or PVM_single_c, with f0 if asked)
+//   B  PVM_multi from A's fit (models 2 and 3)
+//   C  the f0 re-fit of the voxels the plausibility rule flags (CUDA/xfibres_gpu.cu:207-339)
+//   D  tau = 1/var(residuals) and the FP32 outputs
+// Between stages each voxel's FP64 parameters stay in scratch ([nvox][16] doubles) and its
+// state in a flag word.  One warp per voxel; the warps of a block take voxels from a
+// shared-memory counter.
 // ------------------------------------------------------------------------------------------
-template <int K, bool F0>
-__device__ void fit_one(const FitArgs& a, int v, int lane, double* st) {
-  constexpr int NPOUT = 2 + 3 * K + (F0 ? 1 : 0);  // model 1 layout
-  const int M = a.ndir;
+enum FitFlag : uint32_t { kFitBad = 1u, kFitRefit = 2u, kFitRefitted = 4u };
+
+struct VoxelMeas {
   Meas ms;
-  ms.y = a.data + (size_t)v * M;
-  const float* bv = a.gradnonlin ? a.bvecs + (size_t)v * 3 * M : a.bvecs;
-  ms.gx = bv;
-  ms.gy = bv + M;
-  ms.gz = bv + 2 * M;
-  ms.b = a.gradnonlin ? a.bvals + (size_t)v * M : a.bvals;
-  ms.M = M;
+  __device__ VoxelMeas(const FitArgs& a, int v) {
+    const int M = a.ndir;
+    ms.y = a.data + (size_t)v * M;
+    const float* bv = a.gradnonlin ? a.bvecs + (size_t)v * 3 * M : a.bvecs;
+    ms.gx = bv;
+    ms.gy = bv + M;
+    ms.gz = bv + 2 * M;
+    ms.b = a.gradnonlin ? a.bvals + (size_t)v * M : a.bvals;
+    ms.M = M;
+  }
+};
+
+template <int P>
+__device__ __forceinline__ void store_res(double* res, const Real (&p)[P], int lane) {
+  __syncwarp();
+  if (lane == 0)
+#pragma unroll
+    for (int i = 0; i < P; ++i) res[i] = p[i];
+  __syncwarp();
+}
+
+template <int P>
+__device__ __forceinline__ void load_res(const double* res, Real (&p)[P]) {
+#pragma unroll
+  for (int i = 0; i < P; ++i) p[i] = res[i];
+}
+
+// the f0 plausibility rule (CUDA/xfibres_gpu.cu:207-222): f1 < 0.05, d > 0.007 or f0 > 0.4
+template <int P>
+__device__ __forceinline__ bool needs_refit(const Real (&p)[P], int of1) {
+  return p[of1] < 0.05 || p[1] > 0.007 || p[P - 1] > 0.4;
+}
+
+template <int K, bool F0>
+__device__ void stage_start(const FitArgs& a, int v, int lane, double* st) {
+  const VoxelMeas vm(a, v);
+  const Meas& ms = vm.ms;
   const Real R = a.R, invR = 1.0 / (2.0 * R + 1.0);
-  const int gbo = a.model == 3 ? 2 : 0;
-  // non-finite data: flag and emit zeros
+  double* res = a.scratch + (size_t)v * 16;
   bool bad = false;
-  for (int m = lane; m < M; m += 32) bad |= !isfinite(ms.y[m]);
+  for (int m = lane; m < ms.M; m += 32) bad |= !isfinite(ms.y[m]);
   bad = __any_sync(0xffffffffu, bad);
-  const int npo = a.np_out;
-  float* out = a.params + (size_t)v * npo;
   if (bad) {
+    if (lane == 0) a.flags[v] = kFitBad;
+    return;
+  }
+  Dti dt;
+  dti_fit(ms, lane, dt);
+  uint32_t flag = 0;
+  if (a.model == 1 && !a.nonlin) {
+    Real p[LmShape<kSingleC, K, F0>::P];
+    start_single_c<K, F0>(dt, ms, lane, p);
+    lm_run<kSingleC, K, F0>(ms, p, lane, 0, R, invR, st);
+    finalise<kSingleC, K, F0>(p);
+    if (F0 && needs_refit(p, 2)) flag = kFitRefit;
+    store_res(res, p, lane);
+  } else {
+    Real p[LmShape<kSingle, K, F0>::P];
+    start_single<K, F0>(dt, p);
+    lm_run<kSingle, K, F0>(ms, p, lane, 0, R, invR, st);
+    finalise<kSingle, K, F0>(p);
+    if (a.model == 1 && F0 && needs_refit(p, 2)) flag = kFitRefit;
+    store_res(res, p, lane);
+  }
+  if (lane == 0) a.flags[v] = flag;
+}
+
+template <int K, bool F0>
+__device__ void stage_multi(const FitArgs& a, int v, int lane, double* st) {
+  if (a.flags[v] & kFitBad) return;
+  const VoxelMeas vm(a, v);
+  const Real R = a.R, invR = 1.0 / (2.0 * R + 1.0);
+  double* res = a.scratch + (size_t)v * 16;
+  Real s[LmShape<kSingle, K, F0>::P];
+  load_res(res, s);
+  Real p[LmShape<kMulti, K, F0>::P];
+  start_multi<K, F0>(s, p);
+  lm_run<kMulti, K, F0>(vm.ms, p, lane, a.model == 3 ? 2 : 0, R, invR, st);
+  finalise<kMulti, K, F0>(p);
+  store_res(res, p, lane);
+  if (lane == 0 && F0 && needs_refit(p, 3)) a.flags[v] = kFitRefit;
+}
+
+// re-fit without f0 (f0 := 0.001): model 1 with the same start as A; models 2 and 3 through
+// PVM_single_c then PVM_multi, as the GPU path does (CUDA/xfibres_gpu.cu:331-333)
+template <int K>
+__device__ void stage_refit(const FitArgs& a, int v, int lane, double* st) {
+  if (!(a.flags[v] & kFitRefit)) return;
+  const VoxelMeas vm(a, v);
+  const Meas& ms = vm.ms;
+  const Real R = a.R, invR = 1.0 / (2.0 * R + 1.0);
+  double* res = a.scratch + (size_t)v * 16;
+  Dti dt;
+  dti_fit(ms, lane, dt);
+  if (a.model == 1) {
+    constexpr int NPOUT = 2 + 3 * K + 1;
+    if (a.nonlin) {
+      Real p[LmShape<kSingle, K, false>::P];
+      start_single<K, false>(dt, p);
+      lm_run<kSingle, K, false>(ms, p, lane, 0, R, invR, st);
+      finalise<kSingle, K, false>(p);
+      store_res(res, p, lane);
+    } else {
+      Real p[LmShape<kSingleC, K, false>::P];
+      start_single_c<K, false>(dt, ms, lane, p);
+      lm_run<kSingleC, K, false>(ms, p, lane, 0, R, invR, st);
+      finalise<kSingleC, K, false>(p);
+      store_res(res, p, lane);
+    }
+    if (lane == 0) res[NPOUT - 1] = 0.001;
+  } else {
+    constexpr int NPM = LmShape<kMulti, K, true>::P;
+    Real c[LmShape<kSingleC, K, false>::P];
+    start_single_c<K, false>(dt, ms, lane, c);
+    lm_run<kSingleC, K, false>(ms, c, lane, 0, R, invR, st);
+    finalise<kSingleC, K, false>(c);
+    Real p[LmShape<kMulti, K, false>::P];
+    start_multi<K, false>(c, p);
+    lm_run<kMulti, K, false>(ms, p, lane, a.model == 3 ? 2 : 0, R, invR, st);
+    finalise<kMulti, K, false>(p);
+    store_res(res, p, lane);
+    if (lane == 0) res[NPM - 1] = 0.001;
+  }
+  __syncwarp();
+  if (lane == 0) a.flags[v] = kFitRefitted;
+}
+
+// tau = 1 / var(y - prediction) (sample variance, n-1) and the FP32 outputs
+template <int K, bool F0>
+__device__ void stage_finish(const FitArgs& a, int v, int lane, double*) {
+  const uint32_t flag = a.flags[v];
+  const int npo = a.np_out, M = a.ndir;
+  float* out = a.params + (size_t)v * npo;
+  if (flag & kFitBad) {
     if (lane < npo) out[lane] = 0.f;
     if (lane == 0) {
       if (a.tau) a.tau[v] = 0.f;
@@ -988,108 +1113,45 @@ __device__ void fit_one(const FitArgs& a, int v, int lane, double* st) {
     }
     return;
   }
-  Dti dt;
-  dti_fit(ms, lane, dt);
-  Real res[16];
-  bool refit = false;
-  if (a.model == 1) {
-    if (a.nonlin) {
-      Real p[LmShape<kSingle, K, F0>::P];
-      start_single<K, F0>(dt, p);
-      lm_run<kSingle, K, F0>(ms, p, lane, 0, R, invR, st);
-      finalise<kSingle, K, F0>(p);
+  const bool refit = (flag & kFitRefitted) != 0;
+  const double* res = a.scratch + (size_t)v * 16;
+  Real r[16];
 #pragma unroll
-      for (int i = 0; i < NPOUT; ++i) res[i] = p[i];
-      if (F0 && ((K > 0 && p[2] < 0.05) || p[1] > 0.007 || p[NPOUT - 1] > 0.4)) {
-        Real p2[LmShape<kSingle, K, false>::P];
-        start_single<K, false>(dt, p2);
-        lm_run<kSingle, K, false>(ms, p2, lane, 0, R, invR, st);
-        finalise<kSingle, K, false>(p2);
-#pragma unroll
-        for (int i = 0; i < NPOUT - 1; ++i) res[i] = p2[i];
-        res[NPOUT - 1] = 0.001;
-        refit = true;
-      }
-    } else {
-      Real p[LmShape<kSingleC, K, F0>::P];
-      start_single_c<K, F0>(dt, ms, lane, p);
-      lm_run<kSingleC, K, F0>(ms, p, lane, 0, R, invR, st);
-      finalise<kSingleC, K, F0>(p);
-#pragma unroll
-      for (int i = 0; i < NPOUT; ++i) res[i] = p[i];
-      if (F0 && ((K > 0 && p[2] < 0.05) || p[1] > 0.007 || p[NPOUT - 1] > 0.4)) {
-        Real p2[LmShape<kSingleC, K, false>::P];
-        start_single_c<K, false>(dt, ms, lane, p2);
-        lm_run<kSingleC, K, false>(ms, p2, lane, 0, R, invR, st);
-        finalise<kSingleC, K, false>(p2);
-#pragma unroll
-        for (int i = 0; i < NPOUT - 1; ++i) res[i] = p2[i];
-        res[NPOUT - 1] = 0.001;
-        refit = true;
-      }
-    }
-  } else {
-    constexpr int NPM = LmShape<kMulti, K, F0>::P;
-    Real s[LmShape<kSingle, K, F0>::P];
-    start_single<K, F0>(dt, s);
-    lm_run<kSingle, K, F0>(ms, s, lane, 0, R, invR, st);
-    finalise<kSingle, K, F0>(s);
-    Real p[NPM];
-    start_multi<K, F0>(s, p);
-    lm_run<kMulti, K, F0>(ms, p, lane, gbo, R, invR, st);
-    finalise<kMulti, K, F0>(p);
-#pragma unroll
-    for (int i = 0; i < NPM; ++i) res[i] = p[i];
-    if (F0 && ((K > 0 && p[3] < 0.05) || p[1] > 0.007 || p[NPM - 1] > 0.4)) {
-      // GPU re-fit path: PVM_single_c then PVM_multi (CUDA/xfibres_gpu.cu:331-333)
-      Real c[LmShape<kSingleC, K, false>::P];
-      start_single_c<K, false>(dt, ms, lane, c);
-      lm_run<kSingleC, K, false>(ms, c, lane, 0, R, invR, st);
-      finalise<kSingleC, K, false>(c);
-      Real p2[LmShape<kMulti, K, false>::P];
-      start_multi<K, false>(c, p2);
-      lm_run<kMulti, K, false>(ms, p2, lane, gbo, R, invR, st);
-      finalise<kMulti, K, false>(p2);
-#pragma unroll
-      for (int i = 0; i < NPM - 1; ++i) res[i] = p2[i];
-      res[NPM - 1] = 0.001;
-      refit = true;
-    }
-  }
-  // tau = 1 / var(y - prediction)   (sample variance, n-1)
+  for (int i = 0; i < 16; ++i) r[i] = i < npo ? res[i] : 0.0;
   if (a.rician) {
+    const VoxelMeas vm(a, v);
+    const Meas& ms = vm.ms;
     const int o = a.model >= 2 ? 3 : 2;
     const bool use_f0 = F0 && !refit;
     const Real f0 = F0 ? res[npo - 1] : 0.0;
     double s1 = 0.0;
     for (int m = lane; m < M; m += 32)
-      s1 += ms.y[m] - predict_final<K>(a.model, res, o, use_f0, f0, R, ms.gx[m], ms.gy[m], ms.gz[m], ms.b[m]);
+      s1 += ms.y[m] - predict_final<K>(a.model, r, o, use_f0, f0, a.R, ms.gx[m], ms.gy[m], ms.gz[m], ms.b[m]);
     const double mean = group_sum<32>(s1) / M;
     double s2 = 0.0;
     for (int m = lane; m < M; m += 32) {
-      const double r = ms.y[m] - predict_final<K>(a.model, res, o, use_f0, f0, R, ms.gx[m], ms.gy[m], ms.gz[m], ms.b[m]) - mean;
-      s2 += r * r;
+      const double e = ms.y[m] - predict_final<K>(a.model, r, o, use_f0, f0, a.R, ms.gx[m], ms.gy[m], ms.gz[m], ms.b[m]) -
+                       mean;
+      s2 += e * e;
     }
     s2 = group_sum<32>(s2);
     if (lane == 0 && a.tau) a.tau[v] = (float)(1.0 / (s2 / (M - 1)));
   } else if (lane == 0 && a.tau) {
     a.tau[v] = 0.f;
   }
-#pragma unroll
-  for (int i = 0; i < 16; ++i)
-    if (i < npo && lane == i) out[i] = (float)res[i];
+  if (lane < npo) out[lane] = (float)res[lane];
   if (lane == 0 && a.status) a.status[v] = refit ? BPX_VOX_F0_REFIT : 0u;
 }
 
 // Each block owns kFitVoxPerBlock consecutive voxels; its warps take the next one from a
 // shared-memory counter as they finish, so a voxel whose fit runs 200 iterations holds up one
 // warp instead of a fixed share of the block's voxels.
-template <int K, bool F0>
-__global__ void __launch_bounds__(kFitThreads, kFitMinBlocks) fit_kernel(FitArgs a) {
-  __shared__ double stage[kFitThreads / 32][kStageDoubles];
+template <typename Stage>
+__device__ __forceinline__ void run_stage(const FitArgs& a, Stage stage) {
+  __shared__ double stage_buf[kFitThreads / 32][kStageDoubles];
   __shared__ int next;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double* st = stage[w];
+  double* st = stage_buf[w];
   for (int i = lane; i < kStageDoubles; i += 32) st[i] = 0.0;
   const int v0 = blockIdx.x * kFitVoxPerBlock;
   const int v1 = min(v0 + kFitVoxPerBlock, a.nvox);
@@ -1097,11 +1159,28 @@ __global__ void __launch_bounds__(kFitThreads, kFitMinBlocks) fit_kernel(FitArgs
   __syncthreads();
   int v = v0 + w;
   while (v < v1) {
-    fit_one<K, F0>(a, v, lane, st);
+    stage(a, v, lane, st);
     int nv = 0;
     if (lane == 0) nv = atomicAdd(&next, 1);
     v = __shfl_sync(0xffffffffu, nv, 0);
   }
+}
+
+template <int K, bool F0>
+__global__ void __launch_bounds__(kFitThreads, kFitMinBlocks) fit_start_kernel(FitArgs a) {
+  run_stage(a, [](const FitArgs& x, int v, int lane, double* st) { stage_start<K, F0>(x, v, lane, st); });
+}
+template <int K, bool F0>
+__global__ void __launch_bounds__(kFitThreads, kFitMinBlocks) fit_multi_kernel(FitArgs a) {
+  run_stage(a, [](const FitArgs& x, int v, int lane, double* st) { stage_multi<K, F0>(x, v, lane, st); });
+}
+template <int K>
+__global__ void __launch_bounds__(kFitThreads, kFitMinBlocks) fit_refit_kernel(FitArgs a) {
+  run_stage(a, [](const FitArgs& x, int v, int lane, double* st) { stage_refit<K>(x, v, lane, st); });
+}
+template <int K, bool F0>
+__global__ void __launch_bounds__(kFitThreads, kFitMinBlocks) fit_finish_kernel(FitArgs a) {
+  run_stage(a, [](const FitArgs& x, int v, int lane, double* st) { stage_finish<K, F0>(x, v, lane, st); });
 }
 
 // remove_NonPositive_entries (CUDA/xfibres_gpu.cu:350-367), one warp per voxel
@@ -1134,12 +1213,16 @@ __global__ void __launch_bounds__(kFitThreads) prepare_kernel(int nvox, int ndir
 template <int K, bool F0>
 static cudaError_t launch_fit_kf(const FitArgs& a, cudaStream_t s) {
   const int grid = (a.nvox + kFitVoxPerBlock - 1) / kFitVoxPerBlock;
-  fit_kernel<K, F0><<<grid, kFitThreads, 0, s>>>(a);
+  fit_start_kernel<K, F0><<<grid, kFitThreads, 0, s>>>(a);
+  if (a.model >= 2) fit_multi_kernel<K, F0><<<grid, kFitThreads, 0, s>>>(a);
+  if (F0) fit_refit_kernel<K><<<grid, kFitThreads, 0, s>>>(a);
+  fit_finish_kernel<K, F0><<<grid, kFitThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t launch_fit(const FitArgs& a, int nfib, bool f0, cudaStream_t s) {
   if (a.nvox == 0) return cudaSuccess;
+  if (!a.scratch || !a.flags) return cudaErrorInvalidValue;
   switch (nfib * 2 + (f0 ? 1 : 0)) {
     case 2: return launch_fit_kf<1, false>(a, s);
     case 3: return launch_fit_kf<1, true>(a, s);

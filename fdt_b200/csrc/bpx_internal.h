@@ -27,16 +27,20 @@ void set_last_error(const char* msg);  // message returned by bpx_last_error() o
 // C-ABI helpers shared by the entry-point files (bpx_api.cu): status with message, device and
 // argument checks, and the grow-only per-device workspaces (one per slot, so that a pipeline
 // stage can hold one while calling a stage that uses another).
-constexpr int kWorkspaceSlots = 3;
+constexpr int kWorkspaceSlots = 4;
 constexpr int kWsPipeline = 0;  // fit parameters, tau, records, status of bpx_xfibres_dev
 constexpr int kWsNetwork = 1;   // the network's weights and activations
 constexpr int kWsLearned = 2;   // intermediates of the learned pipeline
+constexpr int kWsFit = 3;       // FP64 parameters between the fit stages
 bpx_status api_fail(bpx_status st, const std::string& msg);
 bpx_status api_cuda_fail(cudaError_t e, const char* where);
 bpx_status api_check_device();
 bpx_status api_check_opts(const bpx_options* o);
 bpx_status api_check_vol(const bpx_volume* v);
 bpx_status api_workspace(int slot, size_t bytes, void** out);
+// bpx_fit_dev with caller-provided stage scratch (nvox * kFitScratchBytes, 8-byte aligned)
+bpx_status fit_dev_scratch(const bpx_options* opts, const bpx_volume* vol, float* params, float* tau, uint32_t* status,
+                           void* scratch, void* stream);
 
 struct FitArgs {
   int nvox, ndir;
@@ -50,7 +54,10 @@ struct FitArgs {
   uint32_t* status;
   int model, rician, nonlin;
   float R;
+  double* scratch;   // [nvox][16] FP64 parameters between the fit stages (kFitScratchBytes per voxel)
+  uint32_t* flags;   // [nvox] stage flags (within kFitScratchBytes)
 };
+constexpr size_t kFitScratchBytes = 16 * sizeof(double) + sizeof(uint32_t);  // per voxel
 
 struct McmcArgs {
   int nvox, ndir;

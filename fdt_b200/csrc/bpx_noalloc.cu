@@ -25,7 +25,7 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 size_t scratch_bytes(const bpx_options* o, size_t nvox, bool own_status) {
   const size_t np = (size_t)bpx_nparams_fit(o), ns = (size_t)bpx_nsamples(o);
   return align256(nvox * np * 4) + align256(nvox * 4) + align256((size_t)BPX_NREC(o->nfibres) * ns * nvox * 4) +
-         (own_status ? align256(nvox * 4) : 0);
+         (own_status ? align256(nvox * 4) : 0) + align256(nvox * bpx::kFitScratchBytes);
 }
 
 }  // namespace
@@ -88,9 +88,11 @@ extern "C" bpx_status bpx_xfibres_noalloc_dev(const bpx_options* opts, const bpx
   float* rec = (float*)p;
   p += align256((size_t)BPX_NREC(opts->nfibres) * ns * nvox * 4);
   uint32_t* status = own_status ? (uint32_t*)p : out->status;
+  if (own_status) p += align256(nvox * 4);
+  void* fit_scratch = p;
   bpx_status st = BPX_OK;
   if (opts->rician) st = bpx_prepare_data_dev(vol->nvox, vol->ndir, const_cast<float*>(vol->data), stream);
-  if (st == BPX_OK) st = bpx_fit_dev(opts, vol, params, tau, status, stream);
+  if (st == BPX_OK) st = bpx::fit_dev_scratch(opts, vol, params, tau, status, fit_scratch, stream);
   if (st == BPX_OK) st = bpx_mcmc_dev(opts, vol, params, tau, rec, status, stream);
   if (st == BPX_OK) st = bpx_finish_dev(opts, vol->nvox, rec, out, stream);
   return st;

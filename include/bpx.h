@@ -220,11 +220,11 @@ bpx_status bpx_measure_pipes(double* mufu_ops_per_s, double* fma_ops_per_s);
  * __device__ array of BPX_NOALLOC_SCRATCH_BYTES (40 MiB), which every GPU that loads the library
  * keeps until the process exits.  It calls no cudaMalloc, cudaFree or allocating library routine.
  *
- * Size limit: the intermediates take 4*(P + 2 + (6+3*nfib)*nsamples) bytes per voxel, each
- * block rounded up to 256 bytes (P = bpx_nparams_fit); larger volumes are rejected with
- * BPX_ERR_UNSUPPORTED and a message giving the maximum voxel count for the options.  At the
- * whole-brain options (model 2, 3 fibres, f0, rician, 50 samples) that is 13,700 voxels, more than
- * one 12,800-voxel subpart of xfibres_gpu.
+ * Size limit: the intermediates take 4*(P + 2 + (6+3*nfib)*nsamples) + 132 bytes per voxel (the
+ * last 132 hold the fit stages' FP64 parameters), each block rounded up to 256 bytes
+ * (P = bpx_nparams_fit); larger volumes are rejected with BPX_ERR_UNSUPPORTED and a message giving
+ * the maximum voxel count for the options.  At the whole-brain options (model 2, 3 fibres, f0,
+ * rician, 50 samples) that is 13,100 voxels, more than one 12,800-voxel subpart of xfibres_gpu.
  *
  * The first call on a device resolves the array's device address (cudaGetSymbolAddress, with that
  * device current); make that first call before any stream capture.  All calls share the one array
