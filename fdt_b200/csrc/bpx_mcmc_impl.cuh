@@ -358,14 +358,17 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
   const bool use_f0 = a.f0 != 0;
 
   // shared memory: the (g_x, g_y, g_z, b) table in pair order (one copy per block, or per group
-  // under gradnonlin); per-thread backups of the signals a proposal overwrites; per-group proposal
-  // widths and acceptance counts.  Pair p of lane l is entries p*TPV+l = {gx0,gx1,gy0,gy1} and
+  // under gradnonlin); each thread's data y and padding weights w (read-only during the chain, so
+  // kept out of registers); per-thread backups of the signals a proposal overwrites; per-group
+  // proposal widths and acceptance counts.  Pair p of lane l is entries p*TPV+l = {gx0,gx1,gy0,gy1} and
   // (NP+p)*TPV+l = {gz0,gz1,b0,b1} for measurements l+2p*TPV and l+(2p+1)*TPV (consecutive lanes
   // read consecutive 16-byte entries, free of bank conflicts); the unpaired measurement
   // l+(MPL-1)*TPV is entry 2*NP*TPV+l.  Measurements past M read zeros.
   const int ncopy = a.gradnonlin ? GPB : 1;
   float4* gb = smem4 + (a.gradnonlin ? gblk * NG : 0);
-  float* after = (float*)(smem4 + ncopy * NG);
+  float4* ywp = smem4 + ncopy * NG;                      // {y0, y1, w0, w1} of pair p: ywp[p * threads + tid]
+  float2* ywt = (float2*)(ywp + NP * kMcmcThreads);      // {y, w} of the unpaired measurement: ywt[tid]
+  float* after = (float*)(ywt + kMcmcThreads);
   float2* bkp = (float2*)after + tid;  // pair backup c: bkp[c * kMcmcThreads]
   float* bkt = after + 2 * (K + 1) * NP * kMcmcThreads + tid;
   float* sprop = after + (2 * NP + 1) * (K + 1) * kMcmcThreads + gblk * NS;
@@ -407,7 +410,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
     }
 
     // ---- this lane's measurements: pairs (y2, w2) and the unpaired one (yt, wt) ----
-    float2 y2[NP], w2[NP], i2[NP], s2[K][NP];
+    float2 y2[NP], w2[NP], i2[NP], s2[K][NP];  // y2, w2: only until they are stored in shared memory
     float yt = 0.f, wt = 0.f, it_ = 0.f, st[K];
     bool bad = false;
     const float* yv = a.data + (size_t)v * M;
@@ -427,6 +430,9 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
       bad |= !isfinite(yt);
     }
     bad = group_sum<TPV>(bad ? 1.f : 0.f) > 0.f;
+#pragma unroll
+    for (int p = 0; p < NP; ++p) ywp[p * kMcmcThreads + tid] = make_float4(y2[p].x, y2[p].y, w2[p].x, w2[p].y);
+    if (TAIL) ywt[tid] = make_float2(yt, wt);
 
     // ---- init_Fibres_Multifibres (CUDA/runmcmc_kernels.cu:255-504) ----
     const float* prm = a.params + (size_t)v * a.np_fit;
@@ -533,10 +539,15 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
         float2 sk[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) sk[k] = s2[k][p];
-        acc2 = vadd(acc2, lik_v<K, RIC, float2>(y2[p], w2[p], i2[p], sk, S02, fk2, f02, wiso2, tau2, nht2));
+        const float4 yw = ywp[p * kMcmcThreads + tid];
+        acc2 = vadd(acc2, lik_v<K, RIC, float2>(make_float2(yw.x, yw.y), make_float2(yw.z, yw.w), i2[p], sk, S02, fk2,
+                                                 f02, wiso2, tau2, nht2));
       }
       float acc = vhsum(acc2);
-      if (TAIL) acc += lik_v<K, RIC, float>(yt, wt, it_, st, S0x, fx, f0x, wiso, taux, -0.5f * taux);
+      if (TAIL) {
+        const float2 ytw = ywt[tid];
+        acc += lik_v<K, RIC, float>(ytw.x, ytw.y, it_, st, S0x, fx, f0x, wiso, taux, -0.5f * taux);
+      }
       return group_sum<TPV>(acc);
     };
 
@@ -921,6 +932,7 @@ cudaError_t launch_mcmc_t(const McmcArgs& a, cudaStream_t s) {
   constexpr int NS = 6 + 3 * K, GPB = kMcmcThreads / TPV;
   constexpr int NP = MPL / 2;
   const size_t smem = (size_t)(a.gradnonlin ? GPB : 1) * TPV * MPL * sizeof(float4) +
+                      (size_t)NP * kMcmcThreads * sizeof(float4) + (size_t)kMcmcThreads * sizeof(float2) +
                       (size_t)(2 * NP + 1) * (K + 1) * kMcmcThreads * sizeof(float) + (size_t)GPB * NS * 8;
   if (smem > 48 * 1024) {
     cudaError_t ea = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
