@@ -301,16 +301,24 @@ bpx_status bpx_gradnonlin_dev(int32_t nvox, int32_t ndir, const float* grad, con
 
 namespace bpx {
 
-bpx_status fit_dev_scratch(const bpx_options* opts, const bpx_volume* vol, float* params, float* tau, uint32_t* status,
-                           void* scratch, void* stream) {
+namespace {
+// argument checks of the fit entries, made before any device call or allocation
+bpx_status fit_validate(const bpx_options* opts, const bpx_volume* vol, const float* params, const float* tau) {
   bpx_status st = check_opts(opts);
   if (st == BPX_OK) st = check_vol(vol, true);
   if (st != BPX_OK) return st;
   if (vol->nvox == 0) return BPX_OK;
   if (!params) return fail(BPX_ERR_INVALID_ARG, "params is NULL");
   if (opts->rician && !tau) return fail(BPX_ERR_INVALID_ARG, "tau is NULL under rician");
-  st = check_device();
-  if (st != BPX_OK) return st;
+  return check_device();
+}
+}  // namespace
+
+bpx_status fit_dev_scratch(const bpx_options* opts, const bpx_volume* vol, float* params, float* tau, uint32_t* status,
+                           void* scratch, void* stream) {
+  bpx_status st = fit_validate(opts, vol, params, tau);
+  if (st != BPX_OK || vol->nvox == 0) return st;
+  if (!scratch) return fail(BPX_ERR_INVALID_ARG, "fit stage scratch is NULL");
   FitArgs a{};
   a.nvox = vol->nvox;
   a.ndir = vol->ndir;
@@ -338,13 +346,12 @@ extern "C" {
 
 bpx_status bpx_fit_dev(const bpx_options* opts, const bpx_volume* vol, float* params, float* tau, uint32_t* status,
                        void* stream) {
-  if (vol && vol->nvox > 0) {
-    void* scratch = nullptr;
-    const bpx_status st = workspace((size_t)vol->nvox * kFitScratchBytes, &scratch, kWsFit);
-    if (st != BPX_OK) return st;
-    return fit_dev_scratch(opts, vol, params, tau, status, scratch, stream);
-  }
-  return fit_dev_scratch(opts, vol, params, tau, status, nullptr, stream);
+  bpx_status st = fit_validate(opts, vol, params, tau);
+  if (st != BPX_OK || vol->nvox == 0) return st;
+  void* scratch = nullptr;
+  st = workspace((size_t)vol->nvox * kFitScratchBytes, &scratch, kWsFit);
+  if (st != BPX_OK) return st;
+  return fit_dev_scratch(opts, vol, params, tau, status, scratch, stream);
 }
 
 bpx_status bpx_mcmc_ex_dev(const bpx_options* opts, const bpx_volume* vol, const float* params, const float* tau,
