@@ -44,6 +44,12 @@ WORKLOAD_LEARNED = ("whole-brain: model 2, 3 fibres, rician+f0+ardf0, 288 measur
                     "launch per step) against the plain LM-initialised chain (burnin 1000)")
 
 
+# DRAM bytes (read + write) of one mcmc_kernel launch per voxel on the whole-brain workload, from
+# an ncu capture of a 131072-voxel launch: 307,087,104 B read + 473,595,136 B written.  The kernel
+# keeps its chain state on chip, so its traffic scales with voxels, not with iterations.
+MCMC_DRAM_BYTES_PER_VOXEL = (307087104 + 473595136) / 131072
+
+
 def whole_brain_options() -> Options:
     return Options.make(model=2, nfibres=3, rician=1, f0=1, ardf0=1, nburn=1000, njumps=1250, sampleevery=25)
 
@@ -449,7 +455,10 @@ def main():
     # learned: prepare, features, weight cast + 5 GEMMs per 32768 voxels, decode, mcmc, finish;
     # learned_batched: one CUDA-graph launch (gather, the same kernels, scatter)
     n_gemm = 5 * ((chunk + 32767) // 32768)
-    launches = {"plain": 4, "learned": 6 + n_gemm, "learned_batched": 1}
+    # kernels per step: plain = Rician clean-up, 4 fit stages, MCMC, finishing; learned = clean-up,
+    # features, weight cast, the GEMMs, decode, MCMC, finishing; the graph form launches once and its
+    # graph holds gather, the learned form's kernels and scatter
+    launches = {"plain": 7, "learned": 6 + n_gemm, "learned_batched": 8 + n_gemm}
     timing = {}
     clocks = ClockSampler(local)
     clocks.start()
@@ -551,7 +560,10 @@ def main():
     roof_time = max(mufu_v * chunk / mufu_peak, fp32_v * chunk / fma_peak)
     roofline = {
         "bound": "sfu", "achieved": achieved / 1e9, "peak": mufu_peak / 1e9, "unit": "Gop/s",
-        "frac": achieved / mufu_peak, "traffic": None,
+        "frac": achieved / mufu_peak,
+        "traffic": MCMC_DRAM_BYTES_PER_VOXEL * chunk if (o.model, o.nfibres, M, o.nsamples) == (2, 3, 288, 50) else None,
+        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one mcmc_kernel launch "
+                          "(131072 voxels, this workload), scaled by voxels (profiles/mcmc_kernel_model2_k3_rician.md)",
         "kernel": f"mcmc_kernel (burn-in + recording), timed in the {rf} form's step",
         "fp32_achieved": fp32_achieved / 1e9, "fp32_peak": fma_peak / 1e9,
         "frac_of_roofline_time": roof_time / mcmc_per_launch_s,
