@@ -259,6 +259,19 @@ __global__ void targets_kernel(Layout L, int nvox, const float* __restrict__ par
       }
     }
   }
+  // a chain that met a non-finite state leaves non-finite labels: such targets get weight 0 and
+  // value 0 (a zero weight alone does not stop 0 * NaN from reaching the loss), a direction as a whole
+  for (int k = 0; k < 3; ++k)
+    if (!(isfinite(o[3 + 3 * k]) && isfinite(o[4 + 3 * k]) && isfinite(o[5 + 3 * k])))
+      for (int c = 0; c < 3; ++c) {
+        o[3 + 3 * k + c] = 0.f;
+        w[3 + 3 * k + c] = 0.f;
+      }
+  for (int j = 0; j < kOut; ++j)
+    if (!isfinite(o[j]) || !isfinite(w[j])) {
+      o[j] = 0.f;
+      w[j] = 0.f;
+    }
 }
 
 // Network outputs -> MCMC starting state (fit layout), tau and proposal widths [NS][nvox]; the

@@ -125,7 +125,7 @@ def make_training_set(opts: Options, bvecs: np.ndarray, bvals: np.ndarray, n: in
         lib._check(L.bpx_mlp_targets_dev(C.byref(opts), m, lib._ptr(params), lib._ptr(tau if opts.rician else None),
                                          lib._ptr(props), lib._ptr(s0hat), lib._ptr(t[s : s + m]),
                                          lib._ptr(w[s : s + m]), stream), "bpx_mlp_targets_dev")
-        bad = (status & 1) != 0  # non-finite data: no targets
+        bad = (status & 5) != 0  # non-finite data, or a chain that met a non-finite energy: no targets
         if bool(bad.any()):
             w[s : s + m][bad] = 0.0
     torch.cuda.synchronize()

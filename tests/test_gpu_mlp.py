@@ -200,3 +200,30 @@ def test_training_reduces_loss(torch):
     e0, e1 = errors(p0), errors(p1)
     assert e1[0] < 0.5 * e0[0] and e1[1] < 0.5 * e0[1], (e0, e1)
     assert e1[2] < 0.5 * e0[2], (e0, e1)
+
+
+def test_targets_drop_non_finite_labels(torch):
+    """A labelling chain that met a non-finite state must not poison training: its non-finite
+    labels become zero targets with zero weight (a direction as a whole)."""
+    import ctypes as C
+
+    from fdt_b200 import lib
+
+    opts = Options.make(model=2, nfibres=3, rician=1, f0=1, ardf0=1)
+    n = 4
+    p = torch.tensor([[1000.0, 1e-3, 3e-4, 0.5, 1.0, 2.0, 0.2, 0.5, 0.3, 0.05, 2.0, 1.0, 0.01]] * n, device="cuda")
+    p[1, 1] = float("nan")  # d
+    p[2, 4] = float("inf")  # theta of fibre 1
+    tau = torch.full((n,), 6e-4, device="cuda")
+    tau[3] = float("nan")
+    s0 = torch.full((n,), 1000.0, device="cuda")
+    t = torch.empty((n, 32), device="cuda")
+    w = torch.empty((n, 32), device="cuda")
+    rc = lib.load().bpx_mlp_targets_dev(C.byref(opts), n, p.data_ptr(), tau.data_ptr(), None, s0.data_ptr(),
+                                       t.data_ptr(), w.data_ptr(), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == 0
+    t, w = t.cpu().numpy(), w.cpu().numpy()
+    assert np.all(np.isfinite(t)) and np.all(np.isfinite(w))
+    assert w[0, 12] == 1.0 and w[1, 12] == 0.0 and t[1, 12] == 0.0
+    assert np.all(w[2, 3:6] == 0.0) and np.all(t[2, 3:6] == 0.0) and w[2, 6] > 0.0
+    assert w[3, 16] == 0.0 and w[0, 16] > 0.0
