@@ -166,8 +166,9 @@ def _run_both(torch, lib, oracle, o, y, prot, n_vox, voxel_offset=0):
     return rec_g, rec_o, p64, t64
 
 
-@pytest.mark.parametrize("kw", [dict(model=1, nfibres=2), dict(model=2, nfibres=3, rician=1, f0=1, ardf0=1)],
-                         ids=["m1", "m2_ric_f0"])
+@pytest.mark.parametrize("kw", [dict(model=1, nfibres=2), dict(model=2, nfibres=3, rician=1, f0=1, ardf0=1),
+                                dict(model=3, nfibres=2, rician=1), dict(model=3, nfibres=2, R_prior_fudge=1.0)],
+                         ids=["m1", "m2_ric_f0", "m3_ric", "m3_Rfudge"])
 def test_short_chains_track_the_oracle(torch, lib, oracle, kw):
     """Same random stream: the GPU chain reproduces the FP64 chain step by step (se=1) until an
     accept decision lands within FP32 rounding of its threshold."""
