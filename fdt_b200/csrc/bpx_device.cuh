@@ -66,6 +66,54 @@ __device__ __forceinline__ float rcp_approx(float x) {
 constexpr float kLog2e = 1.4426950408889634f;
 constexpr float kLn2 = 0.6931471805599453f;
 
+// ln(x) from the MUFU log2 (absolute error about 1e-7): the chain's prior energies.
+__device__ __forceinline__ float ln_approx(float x) { return kLn2 * lg2_approx(x); }
+
+// sin and cos of r for |r| <= pi/4 (slightly beyond): odd degree-7 and even degree-8 polynomials
+// whose coefficients were fitted for this library (relative minimax for sin, absolute for cos,
+// error below 4e-9 before FP32 rounding).
+__device__ __forceinline__ void sincos_quarter(float r, float& s, float& c) {
+  const float u = r * r;
+  float p = fmaf(u, -1.9515e-04f, 8.33216e-03f);
+  p = fmaf(u, p, -0.16666655f);
+  s = fmaf(r * u, p, r);
+  float q = fmaf(u, 2.443773e-05f, -1.3887362e-03f);
+  q = fmaf(u, q, 4.1666646e-02f);
+  q = fmaf(u, q, -0.5f);
+  c = fmaf(u, q, 1.0f);
+}
+
+// Quadrant q (mod 4) of a reduced argument: sin and cos of r + q pi/2.
+__device__ __forceinline__ void sincos_rotate(int q, float s, float c, float& sn, float& cs) {
+  const bool sw = (q & 1) != 0;
+  const float a = sw ? c : s, b = sw ? s : c;
+  sn = __int_as_float(__float_as_int(a) ^ ((q & 2) << 30));
+  cs = __int_as_float(__float_as_int(b) ^ (((q + 1) & 2) << 30));
+}
+
+// sin and cos of x in radians, within 2 ulp for |x| < 1e5: Cody-Waite reduction by pi/2 in three
+// FMA steps (Cody and Waite, Software Manual for the Elementary Functions, 1980), then
+// sincos_quarter.  pi/2 = 1.57079637f - 4.37113883e-08f - 1.71512451e-15f (to 1e-23).
+__device__ __forceinline__ void sincos_fast(float x, float& sn, float& cs) {
+  const float k = rintf(x * 0.636619772f);
+  float r = fmaf(-k, 1.57079637f, x);
+  r = fmaf(-k, -4.37113883e-08f, r);
+  r = fmaf(-k, -1.71512451e-15f, r);
+  float s, c;
+  sincos_quarter(r, s, c);
+  sincos_rotate((int)k, s, c, sn, cs);
+}
+
+// cos(2 pi u) for u = m 2^-24 in [0, 1): 4u - k is exact, so the reduction adds no error.
+__device__ __forceinline__ float cos_2pi_u24(float u) {
+  const float x4 = 4.0f * u;
+  const float k = rintf(x4);
+  float s, c, sn, cs;
+  sincos_quarter((x4 - k) * 1.57079637f, s, c);
+  sincos_rotate((int)k, s, c, sn, cs);
+  return cs;
+}
+
 // Random numbers of one proposal slot: a standard normal (Box-Muller on two 24-bit uniforms)
 // and ln(u) of the acceptance uniform u in (0,1].  The same 24-bit uniforms are exact in the
 // FP64 oracle, which therefore draws the same numbers.
@@ -76,9 +124,7 @@ __device__ __forceinline__ void slot_randoms(uint64_t seed, uint64_t vox, uint32
   const float u0 = (float)((r.x >> 8) + 1u) * (1.0f / 16777216.0f);
   const float u1 = (float)(r.y >> 8) * (1.0f / 16777216.0f);
   const float u2 = (float)((r.z >> 8) + 1u) * (1.0f / 16777216.0f);
-  float s, c;
-  sincospif(2.0f * u1, &s, &c);
-  normal = sqrtf(-2.0f * logf(u0)) * c;
+  normal = sqrtf(-2.0f * logf(u0)) * cos_2pi_u24(u1);
   log_u = logf(u2);
 }
 
@@ -119,24 +165,5 @@ __device__ __forceinline__ float beta2f(float b) {
 __device__ __forceinline__ float f2beta(float f) { return asinf(sqrtf(f)); }
 __device__ __forceinline__ float sgnf(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }
 __device__ __forceinline__ float pm1(float x) { return x > 0.f ? 1.f : -1.f; }
-
-// log of the modified Bessel function I0 minus its argument, for z >= 0: the polynomial forms of
-// fibre.h:31-51 / CUDA/runmcmc_kernels.cu:126-145 (Abramowitz & Stegun 9.8.1, 9.8.2), written as
-// logI0(z) - z so that the Rician log-likelihood terms stay O(1).  Branch-free: both polynomials
-// are evaluated and one log2 is taken of the selected one (measurements of one warp fall on
-// both sides of z = 3.75, so a branch would run both sides anyway).
-__device__ __forceinline__ float logI0_minus_z(float z) {
-  const bool small = z < 3.75f;
-  float a = z * (1.0f / 3.75f);
-  a *= a;
-  const float q =
-      1.0f + a * (3.5156229f + a * (3.0899424f + a * (1.2067492f + a * (0.2659732f + a * (0.0360768f + a * 0.0045813f)))));
-  const float rs = rsqrt_approx(fmaxf(z, 3.75f));
-  const float c = 3.75f * rs * rs;
-  const float p =
-      0.39894228f + c * (0.01328592f + c * (0.00225319f + c * (-0.00157565f + c * (0.00916281f + c * (-0.02057706f + c * (0.02635537f + c * (-0.01647633f + c * 0.00392377f)))))));
-  const float l = lg2_approx(small ? q : p * rs) * kLn2;
-  return small ? l - z : l;
-}
 
 }  // namespace bpx

@@ -92,9 +92,9 @@ struct Priors {
   int ardf0, can_use_ard;
 };
 
-// theta prior -log|sin(th)/2| (CUDA/runmcmc_kernels.cu:1142-1147)
-__device__ __forceinline__ float th_prior(float th) {
-  return th == 0.f ? 0.f : -logf(fabsf(sinf(th) * 0.5f));
+// theta prior -log|sin(th)/2| (CUDA/runmcmc_kernels.cu:1142-1147), given sin(th)
+__device__ __forceinline__ float th_prior(float th, float sin_th) {
+  return th == 0.f ? 0.f : -ln_approx(fabsf(sin_th * 0.5f));
 }
 
 // R prior (CUDA/runmcmc_kernels.cu:1058-1083); returns true if R is rejected
@@ -105,7 +105,7 @@ __device__ __forceinline__ bool r_prior(const Priors& pr, float R, float d, floa
   if (lower_R < 0.0f) lower_R = 1e-8f;
   if (pr.R_fudge > 0.0f && d > kUpperDiff / 2.0f) {
     if (R < 1e-8f || R > upper_R) return true;
-    prior = pr.R_fudge * logf(R);
+    prior = pr.R_fudge * ln_approx(R);
     return false;
   }
   if (R <= lower_R || R > upper_R) return true;
@@ -118,65 +118,6 @@ struct Lanes {
   float y[MPL], b[MPL], c[K][MPL], s[K][MPL], iso[MPL];
   int nj;  // measurements held by this lane
 };
-
-// likelihood statistic of one state: SS (Gaussian) or sum_m [-tau (y-p)^2/2 + logI0(z)-z] (Rician),
-// summed over the group.  Signals: s_k for k != kr, snew for fibre kr (kr = -1: none), iso array.
-template <int MODEL, int K, bool RIC, int TPV, int MPL>
-__device__ __forceinline__ float lik_stat(const Lanes<MODEL, K, RIC, TPV, MPL>& L, const float (&isoa)[MPL],
-                                          const float (&sk)[K][MPL], float S0, const float (&f)[K],
-                                          float f0, float tau) {
-  float fsum = f0;
-#pragma unroll
-  for (int k = 0; k < K; ++k) fsum += f[k];
-  const float wiso = 1.0f - fsum;
-  float acc = 0.f;
-#pragma unroll
-  for (int j = 0; j < MPL; ++j) {
-    if (j < L.nj) {
-      float base = f0 + wiso * isoa[j];
-#pragma unroll
-      for (int k = 0; k < K; ++k) base += f[k] * sk[k][j];
-      const float pred = S0 * base;
-      const float r = L.y[j] - pred;
-      if (!RIC) {
-        acc += r * r;
-      } else {
-        const float z = tau * pred * L.y[j];
-        acc += -0.5f * tau * r * r + logI0_minus_z(z);
-      }
-    }
-  }
-  return group_sum<TPV>(acc);
-}
-
-// likelihood statistic from plain per-lane arrays (used by the MCMC kernel)
-template <int K, bool RIC, int TPV, int MPL>
-__device__ __forceinline__ float lik_stat2(const float (&y)[MPL], int nj, const float (&isoa)[MPL],
-                                           const float (&sk)[K][MPL], float S0, const float (&f)[K], float f0,
-                                           float tau) {
-  float fsum = f0;
-#pragma unroll
-  for (int k = 0; k < K; ++k) fsum += f[k];
-  const float wiso = 1.0f - fsum;
-  float acc = 0.f;
-#pragma unroll
-  for (int j = 0; j < MPL; ++j) {
-    if (j < nj) {
-      float base = f0 + wiso * isoa[j];
-#pragma unroll
-      for (int k = 0; k < K; ++k) base += f[k] * sk[k][j];
-      const float pred = S0 * base;
-      const float r = y[j] - pred;
-      if (!RIC) {
-        acc += r * r;
-      } else {
-        const float z = tau * pred * y[j];
-        acc += -0.5f * tau * r * r + logI0_minus_z(z);
-      }
-    }
-  }
-  return group_sum<TPV>(acc);
-}
 
 // energy difference E_old - E_new of the likelihood part
 template <bool RIC>
@@ -241,24 +182,33 @@ __device__ __forceinline__ float2 vlg2(float2 x) { return make_float2(lg2_approx
 __device__ __forceinline__ float vhsum(float x) { return x; }
 __device__ __forceinline__ float vhsum(float2 x) { return x.x + x.y; }
 
-// Rician log-likelihood term without its log(y) part, -tau (y-p)^2/2 + [logI0(z) - z] with
-// z = tau p y, for one or two measurements (the branch-free logI0_minus_z of bpx_device.cuh;
-// the small-argument polynomial is taken in z^2 with its coefficients pre-divided by 3.75^(2i)).
-template <typename V>
-__device__ __forceinline__ V rician_term(V y, V pred, V r, V tau, V nhalf_tau);
-__device__ __forceinline__ float rician_pick(float z, float q, float pr, float& zs) {
+// Rician log-likelihood terms without their log(y) part, sum_m w (-tau (y-p)^2/2 + logI0(z) - z)
+// with p = S0 base and z = tau p y, for one or two measurements, accumulated as
+//   -tau/2 rr + ln2 lg2(prod) - zs,   rr += w r^2,
+// where each measurement multiplies prod by I0(z) (z < 3.75, and zs gains z) or by e^-z I0(z)
+// (z >= 3.75): the polynomial forms of logIo in fibre.h:31-51 / CUDA/runmcmc_kernels.cu:126-145
+// (Abramowitz & Stegun 9.8.1, 9.8.2).  Both are evaluated, branch-free, since the measurements of
+// one warp fall on both sides of z = 3.75.  Every
+// factor lies in (0, 9.2], so a product of five stays in FP32's normal range for z below ~1e14
+// and one log2 per product replaces one per measurement.  Padding measurements (y = 0, w = 0)
+// give z = 0 and the factor 1.  The small-argument polynomial is taken in z^2 with its
+// coefficients divided by 3.75^(2i), the large-argument one in 1/z with them multiplied by 3.75^i.
+__device__ __forceinline__ void rician_pick(float z, float q, float pr, float& sel, float& zs) {
   const bool small = z < 3.75f;
-  zs = small ? -z : 0.f;
-  return small ? q : pr;
+  sel = small ? q : pr;
+  zs = small ? z : 0.f;
 }
 template <typename V>
-__device__ __forceinline__ V rician_term(V y, V pred, V r, V tau, V nhalf_tau) {
+__device__ __forceinline__ void rician_acc(V y, V w, V base, V nS0, V tS0, V& rr, V& prod, V& zs) {
   constexpr float s1 = 3.5156229f / 14.0625f, s2 = 3.0899424f / (14.0625f * 14.0625f),
                   s3 = 1.2067492f / (14.0625f * 14.0625f * 14.0625f),
                   s4 = 0.2659732f / (14.0625f * 14.0625f * 14.0625f * 14.0625f),
                   s5 = 0.0360768f / (14.0625f * 14.0625f * 14.0625f * 14.0625f * 14.0625f),
                   s6 = 0.0045813f / (14.0625f * 14.0625f * 14.0625f * 14.0625f * 14.0625f * 14.0625f);
-  const V z = vmul(vmul(tau, pred), y);
+  constexpr float c1 = 3.75f, c2 = c1 * c1, c3 = c2 * c1, c4 = c3 * c1, c5 = c4 * c1, c6 = c5 * c1, c7 = c6 * c1,
+                  c8 = c7 * c1;
+  const V r = vfma(nS0, base, y);
+  const V z = vmul(tS0, vmul(y, base));
   const V u = vmul(z, z);
   V q = vfma(u, vbc<V>(s6), vbc<V>(s5));
   q = vfma(u, q, vbc<V>(s4));
@@ -272,25 +222,26 @@ __device__ __forceinline__ V rician_term(V y, V pred, V r, V tau, V nhalf_tau) {
   } else {
     rs = rsqrt_approx(fmaxf(z, 3.75f));
   }
-  const V c = vmul(rs, vmul(rs, vbc<V>(3.75f)));
-  V p = vfma(c, vbc<V>(0.00392377f), vbc<V>(-0.01647633f));
-  p = vfma(c, p, vbc<V>(0.02635537f));
-  p = vfma(c, p, vbc<V>(-0.02057706f));
-  p = vfma(c, p, vbc<V>(0.00916281f));
-  p = vfma(c, p, vbc<V>(-0.00157565f));
-  p = vfma(c, p, vbc<V>(0.00225319f));
-  p = vfma(c, p, vbc<V>(0.01328592f));
-  p = vfma(c, p, vbc<V>(0.39894228f));
+  const V v = vmul(rs, rs);
+  V p = vfma(v, vbc<V>(0.00392377f * c8), vbc<V>(-0.01647633f * c7));
+  p = vfma(v, p, vbc<V>(0.02635537f * c6));
+  p = vfma(v, p, vbc<V>(-0.02057706f * c5));
+  p = vfma(v, p, vbc<V>(0.00916281f * c4));
+  p = vfma(v, p, vbc<V>(-0.00157565f * c3));
+  p = vfma(v, p, vbc<V>(0.00225319f * c2));
+  p = vfma(v, p, vbc<V>(0.01328592f * c1));
+  p = vfma(v, p, vbc<V>(0.39894228f));
   const V pr = vmul(p, rs);
-  V sel, zs;
+  V sel, zz;
   if constexpr (sizeof(V) == 8) {
-    sel.x = rician_pick(z.x, q.x, pr.x, zs.x);
-    sel.y = rician_pick(z.y, q.y, pr.y, zs.y);
+    rician_pick(z.x, q.x, pr.x, sel.x, zz.x);
+    rician_pick(z.y, q.y, pr.y, sel.y, zz.y);
   } else {
-    sel = rician_pick(z, q, pr, zs);
+    rician_pick(z, q, pr, sel, zz);
   }
-  const V h = vfma(vlg2(sel), vbc<V>(kLn2), zs);
-  return vfma(vmul(nhalf_tau, r), r, h);
+  prod = vmul(prod, sel);
+  zs = vadd(zs, zz);
+  rr = vfma(vmul(r, w), r, rr);
 }
 
 // signals of one or two measurements (compute_signal / compute_iso_signal, CUDA/runmcmc_kernels.cu:67-95)
@@ -309,20 +260,14 @@ __device__ __forceinline__ V iso_v(const SigParams<MODEL>& sp, V b, V bbeta) {
   return vex2(vmul(vbc<V>(-sp.alpha), vlg2(vadd(bbeta, vbc<V>(1.0f)))));
 }
 
-// per-measurement likelihood contribution (before the group sum), weighted by w (0 for padding)
-template <int K, bool RIC, typename V>
-__device__ __forceinline__ V lik_v(V y, V w, V isov, const V (&sk)[K], V S0, const V (&fk)[K], V f0, V wiso, V tau,
-                                   V nhalf_tau) {
+// Gaussian likelihood contribution of one or two measurements, w (y - S0 base)^2
+template <int K, typename V>
+__device__ __forceinline__ V gauss_v(V y, V w, V isov, const V (&sk)[K], V nS0, const V (&fk)[K], V f0, V wiso) {
   V base = vfma(wiso, isov, f0);
 #pragma unroll
   for (int k = 0; k < K; ++k) base = vfma(fk[k], sk[k], base);
-  const V pred = vmul(S0, base);
-  const V r = vfma(pred, vbc<V>(-1.0f), y);
-  if (!RIC) {
-    const V rw = vmul(r, w);
-    return vmul(rw, r);
-  }
-  return vmul(w, rician_term<V>(y, pred, r, tau, nhalf_tau));
+  const V r = vfma(nS0, base, y);
+  return vmul(vmul(r, w), r);
 }
 
 template <int MODEL, int K, bool RIC, int TPV, int MPL>
@@ -457,28 +402,28 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
       ph[k] = prm[2 + 3 * k + 2 + add];
       f[k] = prm[2 + 3 * k + add];
       lam[k] = (k == 0) ? (a.all_ard != 0) : (a.no_ard == 0);
-      p_th[k] = th_prior(th[k]);
       float fp = 0.f;
-      if (!(f[k] <= 0.f || f[k] >= 1.f)) fp = pr.fudge * (lam[k] ? logf(f[k]) : 0.f);
+      if (!(f[k] <= 0.f || f[k] >= 1.f)) fp = pr.fudge * (lam[k] ? ln_approx(f[k]) : 0.f);
       p_f[k] = fp;
       float sn, cs, sp, cp;
-      sincosf(th[k], &sn, &cs);
-      sincosf(ph[k], &sp, &cp);
+      sincos_fast(th[k], sn, cs);
+      sincos_fast(ph[k], sp, cp);
+      p_th[k] = th_prior(th[k], sn);
       vx[k] = sn * cp;
       vy[k] = sn * sp;
       vz[k] = cs;
     }
     float p_d = 0.f, p_dstd = 0.f, p_R = 0.f, p_f0 = 0.f;
-    if (MODEL == 3 && d >= 0.f && d <= kUpperDiff) p_d = (1.0f - 3.0f) * logf(d) + 4000.0f * d;
+    if (MODEL == 3 && d >= 0.f && d <= kUpperDiff) p_d = (1.0f - 3.0f) * ln_approx(d) + 4000.0f * d;
     if (MODEL >= 2) {
       const float upper = MODEL == 3 ? 0.004f : 0.01f;
-      if (dstd > 0.f && dstd <= upper) p_dstd = logf(dstd);
+      if (dstd > 0.f && dstd <= upper) p_dstd = ln_approx(dstd);
       if (MODEL == 3) {
         float prr = 0.f;
         if (!r_prior(pr, R, d, prr)) p_R = prr;
       }
     }
-    if (use_f0 && !(f0 <= 0.f || f0 >= 1.f) && a.ardf0) p_f0 = logf(f0);
+    if (use_f0 && !(f0 <= 0.f || f0 >= 1.f) && a.ardf0) p_f0 = ln_approx(f0);
 
     // all signals of state (d, dstd, R, v_k) into s2/st/i2/it_, backing up when bk is true
     auto all_signals = [&](float dd, float ds, float RR, bool sticks, bool isob, bool backup) {
@@ -531,22 +476,48 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
       float2 fk2[K];
 #pragma unroll
       for (int k = 0; k < K; ++k) fk2[k] = vbc<float2>(fx[k]);
-      const float2 S02 = vbc<float2>(S0x), f02 = vbc<float2>(f0x), wiso2 = vbc<float2>(wiso);
-      const float2 tau2 = vbc<float2>(taux), nht2 = vbc<float2>(-0.5f * taux);
-      float2 acc2 = make_float2(0.f, 0.f);
+      const float2 nS02 = vbc<float2>(-S0x), f02 = vbc<float2>(f0x), wiso2 = vbc<float2>(wiso);
+      float acc;
+      if constexpr (RIC) {
+        const float2 tS02 = vbc<float2>(taux * S0x);
+        float2 rr = make_float2(0.f, 0.f), prod = make_float2(1.f, 1.f), zs = make_float2(0.f, 0.f);
+        float lgp = 0.f;  // log2 of the products already closed (at most five factors per product)
 #pragma unroll
-      for (int p = 0; p < NP; ++p) {
-        float2 sk[K];
+        for (int p = 0; p < NP; ++p) {
+          const float4 yw = ywp[p * kMcmcThreads + tid];
+          float2 base = vfma(wiso2, i2[p], f02);
 #pragma unroll
-        for (int k = 0; k < K; ++k) sk[k] = s2[k][p];
-        const float4 yw = ywp[p * kMcmcThreads + tid];
-        acc2 = vadd(acc2, lik_v<K, RIC, float2>(make_float2(yw.x, yw.y), make_float2(yw.z, yw.w), i2[p], sk, S02, fk2,
-                                                 f02, wiso2, tau2, nht2));
-      }
-      float acc = vhsum(acc2);
-      if (TAIL) {
-        const float2 ytw = ywt[tid];
-        acc += lik_v<K, RIC, float>(ytw.x, ytw.y, it_, st, S0x, fx, f0x, wiso, taux, -0.5f * taux);
+          for (int k = 0; k < K; ++k) base = vfma(fk2[k], s2[k][p], base);
+          rician_acc<float2>(make_float2(yw.x, yw.y), make_float2(yw.z, yw.w), base, nS02, tS02, rr, prod, zs);
+          if (p % 4 == 3 && p + 1 < NP) {
+            lgp += lg2_approx(prod.x) + lg2_approx(prod.y);
+            prod = make_float2(1.f, 1.f);
+          }
+        }
+        if (TAIL) {
+          const float2 ytw = ywt[tid];
+          float base = fmaf(wiso, it_, f0x);
+#pragma unroll
+          for (int k = 0; k < K; ++k) base = fmaf(fx[k], st[k], base);
+          rician_acc<float>(ytw.x, ytw.y, base, -S0x, taux * S0x, rr.x, prod.x, zs.x);
+        }
+        acc = -0.5f * taux * (rr.x + rr.y) + kLn2 * (lgp + lg2_approx(prod.x) + lg2_approx(prod.y)) - (zs.x + zs.y);
+      } else {
+        float2 acc2 = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+          float2 sk[K];
+#pragma unroll
+          for (int k = 0; k < K; ++k) sk[k] = s2[k][p];
+          const float4 yw = ywp[p * kMcmcThreads + tid];
+          acc2 = vadd(acc2, gauss_v<K, float2>(make_float2(yw.x, yw.y), make_float2(yw.z, yw.w), i2[p], sk, nS02, fk2,
+                                               f02, wiso2));
+        }
+        acc = vhsum(acc2);
+        if (TAIL) {
+          const float2 ytw = ywt[tid];
+          acc += gauss_v<K, float>(ytw.x, ytw.y, it_, st, -S0x, fx, f0x, wiso);
+        }
       }
       return group_sum<TPV>(acc);
     };
@@ -616,11 +587,11 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
           const float tho = pick<K>(th, kf), pho = pick<K>(ph, kf);
           thn = is_th ? tho + n * prop : tho;
           phn = is_th ? pho : pho + n * prop;
-          pold = is_th ? pick<K>(p_th, kf) : 0.f;
-          pnew = is_th ? th_prior(thn) : 0.f;
           float sn, cs, sp_, cp;
-          sincosf(thn, &sn, &cs);
-          sincosf(phn, &sp_, &cp);
+          sincos_fast(thn, sn, cs);
+          sincos_fast(phn, sp_, cp);
+          pold = is_th ? pick<K>(p_th, kf) : 0.f;
+          pnew = is_th ? th_prior(thn, sn) : 0.f;
           nvx = sn * cp;
           nvy = sn * sp_;
           nvz = cs;
@@ -652,7 +623,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
             dn = d + n * prop;
             rej = (dn < 0.f || dn > kUpperDiff);
             pold = p_d;
-            pnew = (rej || MODEL != 3) ? p_d : (1.0f - 3.0f) * logf(dn) + 4000.0f * dn;
+            pnew = (rej || MODEL != 3) ? p_d : (1.0f - 3.0f) * ln_approx(dn) + 4000.0f * dn;
             sticks = true;
             isob = true;
           } else if (slot == kSlotDstd) {
@@ -660,7 +631,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
             const float upper = MODEL == 3 ? 0.004f : 0.01f;
             rej = (dsn <= 0.f || dsn > upper);
             pold = p_dstd;
-            pnew = rej ? p_dstd : logf(dsn);
+            pnew = rej ? p_dstd : ln_approx(dsn);
             sticks = MODEL == 2;
             isob = true;
           } else {
@@ -677,7 +648,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
           rej = (fkn <= 0.f || fkn >= 1.f);
           const bool lj = pick<K>(lam, kf);
           pold = pick<K>(p_f, kf);
-          pnew = rej ? pold : pr.fudge * ((pr.can_use_ard && lj) ? logf(fkn) : 0.f);
+          pnew = rej ? pold : pr.fudge * ((pr.can_use_ard && lj) ? ln_approx(fkn) : 0.f);
           float fs = f0;
 #pragma unroll
           for (int k = 0; k < K; ++k) {
@@ -689,7 +660,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
           f0n = f0 + n * prop;
           rej = (f0n <= 0.f || f0n >= 1.f);
           pold = p_f0;
-          pnew = rej ? p_f0 : (a.ardf0 ? logf(f0n) : 0.f);
+          pnew = rej ? p_f0 : (a.ardf0 ? ln_approx(f0n) : 0.f);
           float fs = f0n;
 #pragma unroll
           for (int k = 0; k < K; ++k) fs += f[k];
@@ -835,6 +806,39 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
   }
 }
 
+// likelihood statistic of one state, summed over the group: SS (Gaussian) or
+// sum_m [-tau (y-p)^2/2 + logI0(z) - z] (Rician, accumulated as the MCMC kernel does)
+template <int MODEL, int K, bool RIC, int TPV, int MPL>
+__device__ __forceinline__ float lik_stat(const Lanes<MODEL, K, RIC, TPV, MPL>& L, const float (&isoa)[MPL],
+                                          const float (&sk)[K][MPL], float S0, const float (&f)[K],
+                                          float f0, float tau) {
+  float fsum = f0;
+#pragma unroll
+  for (int k = 0; k < K; ++k) fsum += f[k];
+  const float wiso = 1.0f - fsum;
+  float rr = 0.f, prod = 1.f, zs = 0.f, lgp = 0.f;
+#pragma unroll
+  for (int j = 0; j < MPL; ++j) {
+    if (j < L.nj) {
+      float base = fmaf(wiso, isoa[j], f0);
+#pragma unroll
+      for (int k = 0; k < K; ++k) base = fmaf(f[k], sk[k][j], base);
+      if (!RIC) {
+        const float r = fmaf(-S0, base, L.y[j]);
+        rr = fmaf(r, r, rr);
+      } else {
+        rician_acc<float>(L.y[j], 1.0f, base, -S0, tau * S0, rr, prod, zs);
+      }
+    }
+    if (RIC && j % 5 == 4) {
+      lgp += lg2_approx(prod);
+      prod = 1.f;
+    }
+  }
+  if (!RIC) return group_sum<TPV>(rr);
+  return group_sum<TPV>(-0.5f * tau * rr + kLn2 * (lgp + lg2_approx(prod)) - zs);
+}
+
 // Energies of given states (for the FP32-vs-FP64 likelihood check): one group per voxel.
 template <int MODEL, int K, bool RIC, int TPV, int MPL>
 __global__ void __launch_bounds__(kMcmcThreads) energy_kernel(EnergyArgs a) {
@@ -876,8 +880,8 @@ __global__ void __launch_bounds__(kMcmcThreads) energy_kernel(EnergyArgs a) {
     for (int k = 0; k < K; ++k) {
       f[k] = st[8 + 3 * k];
       float s_, c_, sp_, cp_;
-      sincosf(st[6 + 3 * k], &s_, &c_);
-      sincosf(st[7 + 3 * k], &sp_, &cp_);
+      sincos_fast(st[6 + 3 * k], s_, c_);
+      sincos_fast(st[7 + 3 * k], sp_, cp_);
 #pragma unroll
       for (int j = 0; j < MPL; ++j) {
         const int m = gl + j * TPV;
@@ -902,22 +906,24 @@ __global__ void __launch_bounds__(kMcmcThreads) energy_kernel(EnergyArgs a) {
     pr.R_std = a.R_std;
     pr.R_fudge = a.R_fudge;
     float p = 0.f;
-    if (MODEL == 3 && d >= 0.f && d <= kUpperDiff) p += (1.0f - 3.0f) * logf(d) + 4000.0f * d;
+    if (MODEL == 3 && d >= 0.f && d <= kUpperDiff) p += (1.0f - 3.0f) * ln_approx(d) + 4000.0f * d;
     if (MODEL >= 2) {
       const float upper = MODEL == 3 ? 0.004f : 0.01f;
-      if (dstd > 0.f && dstd <= upper) p += logf(dstd);
+      if (dstd > 0.f && dstd <= upper) p += ln_approx(dstd);
       if (MODEL == 3) {
         float prr = 0.f;
         if (!r_prior(pr, R, d, prr)) p += prr;
       }
     }
-    if (a.f0 && !(f0 <= 0.f || f0 >= 1.f) && a.ardf0) p += logf(f0);
+    if (a.f0 && !(f0 <= 0.f || f0 >= 1.f) && a.ardf0) p += ln_approx(f0);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const bool lj = (k == 0) ? (a.all_ard != 0) : (a.no_ard == 0);
       float fp = 0.f;
-      if (!(f[k] <= 0.f || f[k] >= 1.f)) fp = a.fudge * (lj ? logf(f[k]) : 0.f);
-      p += th_prior(st[6 + 3 * k]) + fp;
+      if (!(f[k] <= 0.f || f[k] >= 1.f)) fp = a.fudge * (lj ? ln_approx(f[k]) : 0.f);
+      float sn_, cs_;
+      sincos_fast(st[6 + 3 * k], sn_, cs_);
+      p += th_prior(st[6 + 3 * k], sn_) + fp;
     }
     if (valid && gl == 0) {
       if (a.lik) a.lik[v] = lik;
