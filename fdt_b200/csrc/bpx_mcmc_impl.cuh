@@ -28,6 +28,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 #include "bpx_device.cuh"
 #include "bpx_internal.h"
@@ -244,20 +245,29 @@ __device__ __forceinline__ void rician_acc(V y, V w, V base, V nS0, V tS0, V& rr
   rr = vfma(vmul(r, w), r, rr);
 }
 
-// signals of one or two measurements (compute_signal / compute_iso_signal, CUDA/runmcmc_kernels.cu:67-95)
-template <int MODEL, typename V>
+// signals of one or two measurements (compute_signal / compute_iso_signal, CUDA/runmcmc_kernels.cu:67-95).
+// MONO selects the model-2 mono-exponential form (d_std < 1e-5) at compile time: callers branch on
+// sp.mono once around their measurement loops, so each form costs only its own MUFU operations.
+template <int MODEL, bool MONO, typename V>
 __device__ __forceinline__ V stick_v(const SigParams<MODEL>& sp, V b, V bbeta, V c) {
-  if (MODEL == 1) return vex2(vmul(vmul(vbc<V>(sp.e1), b), c));
-  if (MODEL == 2) {
-    if (sp.mono) return vex2(vmul(vmul(vbc<V>(sp.e1), b), c));
-    return vex2(vmul(vbc<V>(-sp.alpha), vlg2(vfma(bbeta, c, vbc<V>(1.0f)))));
-  }
+  if (MODEL == 1 || (MODEL == 2 && MONO)) return vex2(vmul(vmul(vbc<V>(sp.e1), b), c));
+  if (MODEL == 2) return vex2(vmul(vbc<V>(-sp.alpha), vlg2(vfma(bbeta, c, vbc<V>(1.0f)))));
   return vex2(vmul(vmul(vbc<V>(sp.e3), b), vfma(vbc<V>(sp.omR), c, vbc<V>(sp.R))));
 }
-template <int MODEL, typename V>
+template <int MODEL, bool MONO, typename V>
 __device__ __forceinline__ V iso_v(const SigParams<MODEL>& sp, V b, V bbeta) {
-  if (MODEL == 1 || sp.mono) return vex2(vmul(vbc<V>(sp.e1), b));
+  if (MODEL == 1 || MONO) return vex2(vmul(vbc<V>(sp.e1), b));
   return vex2(vmul(vbc<V>(-sp.alpha), vlg2(vadd(bbeta, vbc<V>(1.0f)))));
+}
+
+// Runs body(std::true_type) for the mono-exponential form (model 1, or d_std < 1e-5: the model-2
+// sticks and the model-2/3 isotropic signal), body(std::false_type) otherwise.
+template <int MODEL, typename F>
+__device__ __forceinline__ void with_signal_form(const SigParams<MODEL>& sp, F&& body) {
+  if (MODEL >= 2 && !sp.mono)
+    body(std::false_type{});
+  else
+    body(std::true_type{});
 }
 
 // Gaussian likelihood contribution of one or two measurements, w (y - S0 base)^2
@@ -425,9 +435,11 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
     }
     if (use_f0 && !(f0 <= 0.f || f0 >= 1.f) && a.ardf0) p_f0 = ln_approx(f0);
 
-    // all signals of state (d, dstd, R, v_k) into s2/st/i2/it_, backing up when bk is true
-    auto all_signals = [&](float dd, float ds, float RR, bool sticks, bool isob, bool backup) {
-      const SigParams<MODEL> sp = sig_params<MODEL>(dd, ds, RR);
+    // all signals of the state with signal parameters sp and directions v_k into s2/st/i2/it_,
+    // backing up the overwritten ones when backup is true
+    auto all_signals = [&](const SigParams<MODEL>& sp, bool sticks, bool isob, bool backup) {
+      with_signal_form<MODEL>(sp, [&](auto form) {
+      constexpr bool MONO = decltype(form)::value;
       const float2 beta2 = make_float2(sp.beta, sp.beta);
 #pragma unroll
       for (int p = 0; p < NP; ++p) {
@@ -442,12 +454,12 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
             dp = vfma(gy, vbc<float2>(vy[k]), dp);
             dp = vfma(gz, vbc<float2>(vz[k]), dp);
             if (backup) bkp[(k * NP + p) * kMcmcThreads] = s2[k][p];
-            s2[k][p] = stick_v<MODEL, float2>(sp, b, bbeta, vmul(dp, dp));
+            s2[k][p] = stick_v<MODEL, MONO, float2>(sp, b, bbeta, vmul(dp, dp));
           }
         }
         if (isob) {
           if (backup) bkp[(K * NP + p) * kMcmcThreads] = i2[p];
-          i2[p] = iso_v<MODEL, float2>(sp, b, bbeta);
+          i2[p] = iso_v<MODEL, MONO, float2>(sp, b, bbeta);
         }
       }
       if (TAIL) {
@@ -458,14 +470,15 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
           for (int k = 0; k < K; ++k) {
             const float dp = g.x * vx[k] + g.y * vy[k] + g.z * vz[k];
             if (backup) bkt[k * kMcmcThreads] = st[k];
-            st[k] = stick_v<MODEL, float>(sp, g.w, bbeta, dp * dp);
+            st[k] = stick_v<MODEL, MONO, float>(sp, g.w, bbeta, dp * dp);
           }
         }
         if (isob) {
           if (backup) bkt[K * kMcmcThreads] = it_;
-          it_ = iso_v<MODEL, float>(sp, g.w, bbeta);
+          it_ = iso_v<MODEL, MONO, float>(sp, g.w, bbeta);
         }
       }
+      });
     };
     // the likelihood statistic of a state, summed over the group
     auto lik_of = [&](float S0x, const float (&fx)[K], float f0x, float taux) {
@@ -522,7 +535,9 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
       return group_sum<TPV>(acc);
     };
 
-    all_signals(d, dstd, R, true, true, false);
+    // signal parameters of the current state (changed only by accepted d, d_std or R proposals)
+    SigParams<MODEL> spc = sig_params<MODEL>(d, dstd, R);
+    all_signals(spc, true, true, false);
     float lik = lik_of(S0, f, f0, tau);
     // initialise_props (or widths given per voxel), acceptance counters
     if (gl == 0) {
@@ -595,7 +610,9 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
           nvx = sn * cp;
           nvy = sn * sp_;
           nvz = cs;
-          const SigParams<MODEL> sp = sig_params<MODEL>(d, dstd, R);
+          with_signal_form<MODEL>(spc, [&](auto form) {
+          constexpr bool MONO = decltype(form)::value;
+          const SigParams<MODEL>& sp = spc;
           const float2 beta2 = make_float2(sp.beta, sp.beta);
           const float2 nvx2 = vbc<float2>(nvx), nvy2 = vbc<float2>(nvy), nvz2 = vbc<float2>(nvz);
 #pragma unroll
@@ -609,15 +626,16 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
                 dp = vfma(make_float2(gc.x, gc.y), nvz2, dp);
                 const float2 b = make_float2(gc.z, gc.w);
                 bkp[p * kMcmcThreads] = s2[k][p];
-                s2[k][p] = stick_v<MODEL, float2>(sp, b, vmul(beta2, b), vmul(dp, dp));
+                s2[k][p] = stick_v<MODEL, MONO, float2>(sp, b, vmul(beta2, b), vmul(dp, dp));
               }
               if (TAIL) {
                 const float4 g = gb[2 * NP * TPV + gl];
                 const float dp = g.x * nvx + g.y * nvy + g.z * nvz;
                 bkt[0] = st[k];
-                st[k] = stick_v<MODEL, float>(sp, g.w, sp.beta * g.w, dp * dp);
+                st[k] = stick_v<MODEL, MONO, float>(sp, g.w, sp.beta * g.w, dp * dp);
               }
             }
+          });
         } else if (kind == 2) {
           if (slot == kSlotD) {
             dn = d + n * prop;
@@ -642,7 +660,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
             pnew = rej ? p_R : pr2;
             sticks = true;
           }
-          if (!group_all<TPV>(rej)) all_signals(dn, dsn, Rn, sticks, isob, true);
+          if (!group_all<TPV>(rej)) all_signals(sig_params<MODEL>(dn, dsn, Rn), sticks, isob, true);
         } else if (slot >= kSlotFibre0) {
           const float fkn = pick<K>(f, kf) + n * prop;
           rej = (fkn <= 0.f || fkn >= 1.f);
@@ -733,6 +751,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
               R = Rn;
               p_R = pnew;
             }
+            spc = sig_params<MODEL>(d, dstd, R);
           } else if (slot >= kSlotFibre0) {
 #pragma unroll
             for (int k = 0; k < K; ++k)
