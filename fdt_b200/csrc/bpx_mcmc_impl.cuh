@@ -280,6 +280,23 @@ __device__ __forceinline__ V gauss_v(V y, V w, V isov, const V (&sk)[K], V nS0, 
   return vmul(vmul(r, w), r);
 }
 
+// Proposal-slot descriptors, two bits per slot: kind (0: f0, tau, S0 or a fraction; 1: theta or
+// phi of a fibre; 2: d, d_std or R) and fibre index; one bit per slot: theta slots.
+constexpr int slot_kind(int s) {
+  return (s >= kSlotFibre0 && (s - kSlotFibre0) % 3 != 2) ? 1 : ((s == kSlotD || s == kSlotDstd || s == kSlotR) ? 2 : 0);
+}
+template <int K>
+constexpr uint32_t slot_bits(int what) {
+  uint32_t m = 0;
+  for (int s = 0; s < 6 + 3 * K; ++s) {
+    const int fib = s - kSlotFibre0;
+    if (what == 0) m |= (uint32_t)slot_kind(s) << (2 * s);
+    if (what == 1 && fib >= 0) m |= (uint32_t)(fib / 3) << (2 * s);
+    if (what == 2 && fib >= 0 && fib % 3 == 0) m |= 1u << s;
+  }
+  return m;
+}
+
 template <int MODEL, int K, bool RIC, int TPV, int MPL>
 __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(McmcArgs a) {
   constexpr int NS = 6 + 3 * K;             // proposal slots
@@ -289,8 +306,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
   constexpr int NP = MPL / 2;               // measurement pairs per lane
   constexpr bool TAIL = (MPL & 1) != 0;     // one unpaired measurement per lane
   constexpr int NG = TPV * MPL;             // float4 (g, b) entries per copy
-  constexpr unsigned kIsoBit = 1u << K;
-  constexpr unsigned kAllSticks = (1u << K) - 1u;
+  constexpr uint32_t kSlotKinds = slot_bits<K>(0), kSlotFibres = slot_bits<K>(1), kSlotTheta = slot_bits<K>(2);
   extern __shared__ float4 smem4[];
   const int lane = threadIdx.x & 31;
   const int gl = lane % TPV;
@@ -311,6 +327,9 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
   pr.ardf0 = a.ardf0;
   pr.can_use_ard = !a.no_ard;
   const bool use_f0 = a.f0 != 0;
+  // slots proposed by this model: f0 with --f0, tau when Rician, d_std for models 2-3, R for model 3
+  const uint32_t enabled = ((1u << NS) - 1u) & ~((use_f0 ? 0u : 1u << kSlotF0) | (RIC ? 0u : 1u << kSlotTau) |
+                                                  (MODEL >= 2 ? 0u : 1u << kSlotDstd) | (MODEL == 3 ? 0u : 1u << kSlotR));
 
   // shared memory: the (g_x, g_y, g_z, b) table in pair order (one copy per block, or per group
   // under gradnonlin); each thread's data y and padding weights w (read-only during the chain, so
@@ -569,10 +588,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
       }
 #pragma unroll 1
       for (int slot = 0; slot < NS; ++slot) {
-        if (slot == kSlotF0 && !use_f0) continue;
-        if (slot == kSlotTau && !RIC) continue;
-        if (slot == kSlotDstd && MODEL < 2) continue;
-        if (slot == kSlotR && MODEL != 3) continue;
+        if (!((enabled >> slot) & 1u)) continue;
         float n, lu;
         {
           float rq = rn[0], lq = rl[0];
@@ -589,16 +605,15 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
         // ---------- the proposal: state, prior, and the signals it changes (updated in place) ----------
         // kind 0: f0, tau, S0 or a fraction (likelihood only); 1: theta/phi of fibre kf (one stick);
         // 2: d, d_std or R (every signal that depends on it)
-        const int fib = slot - kSlotFibre0;
-        const int kind = (slot >= kSlotFibre0 && fib % 3 != 2) ? 1 : ((slot == kSlotD || slot == kSlotDstd || slot == kSlotR) ? 2 : 0);
-        const int kf = slot >= kSlotFibre0 ? fib / 3 : 0;
+        const int kind = (int)((kSlotKinds >> (2 * slot)) & 3u);
+        const int kf = (int)((kSlotFibres >> (2 * slot)) & 3u);
+        const bool is_th = (kSlotTheta >> slot) & 1u;
         float S0n = S0, taun = tau, f0n = f0, fn[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) fn[k] = f[k];
         float pold = 0.f, pnew = 0.f, thn = 0.f, phn = 0.f, nvx = 0.f, nvy = 0.f, nvz = 0.f, dn = d, dsn = dstd, Rn = R;
         bool rej = false, sticks = false, isob = false;
         if (kind == 1) {
-          const bool is_th = fib % 3 == 0;
           const float tho = pick<K>(th, kf), pho = pick<K>(ph, kf);
           thn = is_th ? tho + n * prop : tho;
           phn = is_th ? pho : pho + n * prop;
@@ -738,7 +753,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
                 vx[k] = nvx;
                 vy[k] = nvy;
                 vz[k] = nvz;
-                if (fib % 3 == 0) p_th[k] = pnew;
+                if (is_th) p_th[k] = pnew;
               }
           } else if (kind == 2) {
             if (slot == kSlotD) {
