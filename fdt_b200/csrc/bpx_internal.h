@@ -16,10 +16,17 @@ constexpr int kFitVoxPerBlock = 32;  // voxels a fit block shares out among its 
 #endif
 constexpr int kFitMinBlocks = BPX_FIT_MIN_BLOCKS;  // register cap: 65536 / (128 * 4) = 128 per thread
 constexpr int kMcmcThreads = 128;  // 4 warps
-#ifndef BPX_MCMC_MIN_BLOCKS
-#define BPX_MCMC_MIN_BLOCKS 3
+// Register cap of the MCMC kernel as resident blocks per SM: 4 (128 registers, 16 warps) for up to
+// 9 measurements per lane, 3 (168 registers, 12 warps) for more, where 128 registers spill in the
+// proposal loop.  BPX_MCMC_MIN_BLOCKS overrides both.
+template <int MPL>
+constexpr int mcmc_min_blocks() {
+#ifdef BPX_MCMC_MIN_BLOCKS
+  return BPX_MCMC_MIN_BLOCKS;
+#else
+  return MPL <= 9 ? 4 : 3;
 #endif
-constexpr int kMcmcMinBlocks = BPX_MCMC_MIN_BLOCKS;  // register cap: 3 blocks = 12 resident warps per SM
+}
 
 int sm_count();  // multiprocessors of the current device (cached per device)
 void set_last_error(const char* msg);  // message returned by bpx_last_error() on this thread

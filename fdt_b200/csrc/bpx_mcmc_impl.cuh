@@ -280,6 +280,9 @@ __device__ __forceinline__ V gauss_v(V y, V w, V isov, const V (&sk)[K], V nS0, 
   return vmul(vmul(r, w), r);
 }
 
+// Rows of the per-group fibre state in shared memory (K entries each).
+enum FibreStateRow : int { kFsTh = 0, kFsPh, kFsVx, kFsVy, kFsVz, kFsPth, kFsPf, kFsRows };
+
 // Proposal-slot descriptors, two bits per slot: kind (0: f0, tau, S0 or a fraction; 1: theta or
 // phi of a fibre; 2: d, d_std or R) and fibre index; one bit per slot: theta slots.
 constexpr int slot_kind(int s) {
@@ -298,7 +301,7 @@ constexpr uint32_t slot_bits(int what) {
 }
 
 template <int MODEL, int K, bool RIC, int TPV, int MPL>
-__global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(McmcArgs a) {
+__global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_kernel(McmcArgs a) {
   constexpr int NS = 6 + 3 * K;             // proposal slots
   constexpr int NR = (NS + TPV - 1) / TPV;  // Philox blocks per lane per iteration
   constexpr int GPW = 32 / TPV;             // groups (voxels) per warp
@@ -347,6 +350,9 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
   float* bkt = after + 2 * (K + 1) * NP * kMcmcThreads + tid;
   float* sprop = after + (2 * NP + 1) * (K + 1) * kMcmcThreads + gblk * NS;
   int* sacc = (int*)(after + (2 * NP + 1) * (K + 1) * kMcmcThreads + GPB * NS) + gblk * NS;
+  // per-group fibre state th, ph, v_x, v_y, v_z, theta prior and fraction prior (kFs* rows of K);
+  // every lane of a group writes the same values, so each lane reads back what it wrote
+  float* fst = after + (2 * NP + 1) * (K + 1) * kMcmcThreads + 2 * GPB * NS + gblk * kFsRows * K;
   auto fill_gb = [&](float4* dst, const float* bv, const float* bl, int first_l, int step) {
     for (int e = first_l; e < NP * TPV; e += step) {
       const int p = e / TPV, l = e % TPV;
@@ -423,24 +429,26 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
     float f0 = use_f0 ? prm[a.np_fit - 1] : 0.f;
     float tau = (RIC && a.tau) ? a.tau[v] : 0.f;
     constexpr int add = MODEL >= 2 ? 1 : 0;
-    float th[K], ph[K], f[K], vx[K], vy[K], vz[K], p_th[K], p_f[K];
-    bool lam[K];
+    float f[K];
+    uint32_t lam = 0;  // ARD flag of fibre k in bit k
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      th[k] = prm[2 + 3 * k + 1 + add];
-      ph[k] = prm[2 + 3 * k + 2 + add];
+      const float th0 = prm[2 + 3 * k + 1 + add], ph0 = prm[2 + 3 * k + 2 + add];
       f[k] = prm[2 + 3 * k + add];
-      lam[k] = (k == 0) ? (a.all_ard != 0) : (a.no_ard == 0);
+      const bool lk = (k == 0) ? (a.all_ard != 0) : (a.no_ard == 0);
+      lam |= lk ? 1u << k : 0u;
       float fp = 0.f;
-      if (!(f[k] <= 0.f || f[k] >= 1.f)) fp = pr.fudge * (lam[k] ? ln_approx(f[k]) : 0.f);
-      p_f[k] = fp;
+      if (!(f[k] <= 0.f || f[k] >= 1.f)) fp = pr.fudge * (lk ? ln_approx(f[k]) : 0.f);
       float sn, cs, sp, cp;
-      sincos_fast(th[k], sn, cs);
-      sincos_fast(ph[k], sp, cp);
-      p_th[k] = th_prior(th[k], sn);
-      vx[k] = sn * cp;
-      vy[k] = sn * sp;
-      vz[k] = cs;
+      sincos_fast(th0, sn, cs);
+      sincos_fast(ph0, sp, cp);
+      fst[kFsTh * K + k] = th0;
+      fst[kFsPh * K + k] = ph0;
+      fst[kFsVx * K + k] = sn * cp;
+      fst[kFsVy * K + k] = sn * sp;
+      fst[kFsVz * K + k] = cs;
+      fst[kFsPth * K + k] = th_prior(th0, sn);
+      fst[kFsPf * K + k] = fp;
     }
     float p_d = 0.f, p_dstd = 0.f, p_R = 0.f, p_f0 = 0.f;
     if (MODEL == 3 && d >= 0.f && d <= kUpperDiff) p_d = (1.0f - 3.0f) * ln_approx(d) + 4000.0f * d;
@@ -469,9 +477,9 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
         if (sticks) {
 #pragma unroll
           for (int k = 0; k < K; ++k) {
-            float2 dp = vmul(gx, vbc<float2>(vx[k]));
-            dp = vfma(gy, vbc<float2>(vy[k]), dp);
-            dp = vfma(gz, vbc<float2>(vz[k]), dp);
+            float2 dp = vmul(gx, vbc<float2>(fst[kFsVx * K + k]));
+            dp = vfma(gy, vbc<float2>(fst[kFsVy * K + k]), dp);
+            dp = vfma(gz, vbc<float2>(fst[kFsVz * K + k]), dp);
             if (backup) bkp[(k * NP + p) * kMcmcThreads] = s2[k][p];
             s2[k][p] = stick_v<MODEL, MONO, float2>(sp, b, bbeta, vmul(dp, dp));
           }
@@ -487,7 +495,7 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
         if (sticks) {
 #pragma unroll
           for (int k = 0; k < K; ++k) {
-            const float dp = g.x * vx[k] + g.y * vy[k] + g.z * vz[k];
+            const float dp = g.x * fst[kFsVx * K + k] + g.y * fst[kFsVy * K + k] + g.z * fst[kFsVz * K + k];
             if (backup) bkt[k * kMcmcThreads] = st[k];
             st[k] = stick_v<MODEL, MONO, float>(sp, g.w, bbeta, dp * dp);
           }
@@ -614,13 +622,13 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
         float pold = 0.f, pnew = 0.f, thn = 0.f, phn = 0.f, nvx = 0.f, nvy = 0.f, nvz = 0.f, dn = d, dsn = dstd, Rn = R;
         bool rej = false, sticks = false, isob = false;
         if (kind == 1) {
-          const float tho = pick<K>(th, kf), pho = pick<K>(ph, kf);
+          const float tho = fst[kFsTh * K + kf], pho = fst[kFsPh * K + kf];
           thn = is_th ? tho + n * prop : tho;
           phn = is_th ? pho : pho + n * prop;
           float sn, cs, sp_, cp;
           sincos_fast(thn, sn, cs);
           sincos_fast(phn, sp_, cp);
-          pold = is_th ? pick<K>(p_th, kf) : 0.f;
+          pold = is_th ? fst[kFsPth * K + kf] : 0.f;
           pnew = is_th ? th_prior(thn, sn) : 0.f;
           nvx = sn * cp;
           nvy = sn * sp_;
@@ -679,8 +687,8 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
         } else if (slot >= kSlotFibre0) {
           const float fkn = pick<K>(f, kf) + n * prop;
           rej = (fkn <= 0.f || fkn >= 1.f);
-          const bool lj = pick<K>(lam, kf);
-          pold = pick<K>(p_f, kf);
+          const bool lj = (lam >> kf) & 1u;
+          pold = fst[kFsPf * K + kf];
           pnew = rej ? pold : pr.fudge * ((pr.can_use_ard && lj) ? ln_approx(fkn) : 0.f);
           float fs = f0;
 #pragma unroll
@@ -745,16 +753,12 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
         if (ok) {
           lik = likn;
           if (kind == 1) {
-#pragma unroll
-            for (int k = 0; k < K; ++k)
-              if (k == kf) {
-                th[k] = thn;
-                ph[k] = phn;
-                vx[k] = nvx;
-                vy[k] = nvy;
-                vz[k] = nvz;
-                if (is_th) p_th[k] = pnew;
-              }
+            fst[kFsTh * K + kf] = thn;
+            fst[kFsPh * K + kf] = phn;
+            fst[kFsVx * K + kf] = nvx;
+            fst[kFsVy * K + kf] = nvy;
+            fst[kFsVz * K + kf] = nvz;
+            if (is_th) fst[kFsPth * K + kf] = pnew;
           } else if (kind == 2) {
             if (slot == kSlotD) {
               d = dn;
@@ -769,11 +773,8 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
             spc = sig_params<MODEL>(d, dstd, R);
           } else if (slot >= kSlotFibre0) {
 #pragma unroll
-            for (int k = 0; k < K; ++k)
-              if (k == kf) {
-                f[k] = fn[k];
-                p_f[k] = pnew;
-              }
+            for (int k = 0; k < K; ++k) f[k] = fn[k];
+            fst[kFsPf * K + kf] = pnew;
           } else if (slot == kSlotF0) {
             f0 = f0n;
             p_f0 = pnew;
@@ -798,8 +799,8 @@ __global__ void __launch_bounds__(kMcmcThreads, kMcmcMinBlocks) mcmc_kernel(Mcmc
           r[5 * stride] = S0;
 #pragma unroll
           for (int k = 0; k < K; ++k) {
-            r[(6 + 3 * k) * stride] = th[k];
-            r[(7 + 3 * k) * stride] = ph[k];
+            r[(6 + 3 * k) * stride] = fst[kFsTh * K + k];
+            r[(7 + 3 * k) * stride] = fst[kFsPh * K + k];
             r[(8 + 3 * k) * stride] = f[k];
           }
         }
@@ -973,7 +974,8 @@ cudaError_t launch_mcmc_t(const McmcArgs& a, cudaStream_t s) {
   constexpr int NP = MPL / 2;
   const size_t smem = (size_t)(a.gradnonlin ? GPB : 1) * TPV * MPL * sizeof(float4) +
                       (size_t)NP * kMcmcThreads * sizeof(float4) + (size_t)kMcmcThreads * sizeof(float2) +
-                      (size_t)(2 * NP + 1) * (K + 1) * kMcmcThreads * sizeof(float) + (size_t)GPB * NS * 8;
+                      (size_t)(2 * NP + 1) * (K + 1) * kMcmcThreads * sizeof(float) + (size_t)GPB * NS * 8 +
+                      (size_t)GPB * kFsRows * K * sizeof(float);
   if (smem > 48 * 1024) {
     cudaError_t ea = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (ea != cudaSuccess) return ea;
