@@ -69,16 +69,25 @@ constexpr float kLn2 = 0.6931471805599453f;
 // ln(x) from the MUFU log2 (absolute error about 1e-7): the chain's prior energies.
 __device__ __forceinline__ float ln_approx(float x) { return kLn2 * lg2_approx(x); }
 
-// sin and cos of r for |r| <= pi/4 (slightly beyond): odd degree-7 and even degree-8 polynomials
-// whose coefficients were fitted for this library (relative minimax for sin, absolute for cos,
-// error below 4e-9 before FP32 rounding).
+// Polynomial coefficients fitted for this library to the exact functions (fdt_b200/polyfit.py):
+// I0(z) in powers of z^2 below kI0Split, e^-z I0(z) sqrt(z) in powers of 1/z above it, and sin/cos
+// on [-pi/4, pi/4] (relative minimax for sin, absolute for cos, below 4e-9 before FP32 rounding).
+// BEGIN generated by python -m fdt_b200.polyfit
+constexpr float kI0Split = 4.75f;
+__host__ __device__ constexpr float kI0Small(int i) { return i == 0 ? 1.0f : i == 1 ? 0.24999896f : i == 2 ? 0.015626252f : i == 3 ? 0.00043356538f : i == 4 ? 6.8553645e-06f : i == 5 ? 6.218488e-08f : 6.707401e-10f; }
+__host__ __device__ constexpr float kI0Large(int i) { return i == 0 ? 0.39894244f : i == 1 ? 0.04983106f : i == 2 ? 0.029434934f : i == 3 ? 0.0128485765f : i == 4 ? 0.096278094f : 0.20845851f; }
+__host__ __device__ constexpr float kSinQ(int i) { return i == 0 ? -0.16666655f : i == 1 ? 0.008332156f : -0.00019514632f; }
+__host__ __device__ constexpr float kCosQ(int i) { return i == 0 ? 0.041666646f : i == 1 ? -0.0013887362f : 2.443773e-05f; }
+// END generated
+
+// sin and cos of r for |r| <= pi/4 (slightly beyond)
 __device__ __forceinline__ void sincos_quarter(float r, float& s, float& c) {
   const float u = r * r;
-  float p = fmaf(u, -1.9515e-04f, 8.33216e-03f);
-  p = fmaf(u, p, -0.16666655f);
+  float p = fmaf(u, kSinQ(2), kSinQ(1));
+  p = fmaf(u, p, kSinQ(0));
   s = fmaf(r * u, p, r);
-  float q = fmaf(u, 2.443773e-05f, -1.3887362e-03f);
-  q = fmaf(u, q, 4.1666646e-02f);
+  float q = fmaf(u, kCosQ(2), kCosQ(1));
+  q = fmaf(u, q, kCosQ(0));
   q = fmaf(u, q, -0.5f);
   c = fmaf(u, q, 1.0f);
 }

@@ -186,52 +186,38 @@ __device__ __forceinline__ float vhsum(float2 x) { return x.x + x.y; }
 // Rician log-likelihood terms without their log(y) part, sum_m w (-tau (y-p)^2/2 + logI0(z) - z)
 // with p = S0 base and z = tau p y, for one or two measurements, accumulated as
 //   -tau/2 rr + ln2 lg2(prod) - zs,   rr += w r^2,
-// where each measurement multiplies prod by I0(z) (z < 3.75, and zs gains z) or by e^-z I0(z)
-// (z >= 3.75): the polynomial forms of logIo in fibre.h:31-51 / CUDA/runmcmc_kernels.cu:126-145
-// (Abramowitz & Stegun 9.8.1, 9.8.2).  Both are evaluated, branch-free, since the measurements of
-// one warp fall on both sides of z = 3.75.  Every
-// factor lies in (0, 9.2], so a product of five stays in FP32's normal range for z below ~1e14
-// and one log2 per product replaces one per measurement.  Padding measurements (y = 0, w = 0)
-// give z = 0 and the factor 1.  The small-argument polynomial is taken in z^2 with its
-// coefficients divided by 3.75^(2i), the large-argument one in 1/z with them multiplied by 3.75^i.
+// where each measurement multiplies prod by I0(z) (z < kI0Split, and zs gains z) or by e^-z I0(z)
+// (z >= kI0Split).  The reference's logIo (fibre.h:31-51 / CUDA/runmcmc_kernels.cu:126-145) uses the
+// Abramowitz & Stegun 9.8.1/9.8.2 polynomials split at 3.75 (degrees 6 and 8); the kI0Small/kI0Large
+// polynomials of bpx_device.cuh, split at 4.75, have degrees 6 and 5 at the same accuracy (log I0
+// within 6e-7 after FP32 rounding).  Both branches are evaluated, branch-free, since the measurements
+// of one warp fall on both sides of the split; the unselected branch may be inf or NaN (rsqrt of a
+// small z), which the select discards.  Every factor lies in (0, 15], so a product of five stays in
+// FP32's normal range for z below ~1e14 and one log2 per product replaces one per measurement.
+// Padding measurements (y = 0, w = 0) give z = 0 and the factor kI0Small(0) = 1.
 __device__ __forceinline__ void rician_pick(float z, float q, float pr, float& sel, float& zs) {
-  const bool small = z < 3.75f;
+  const bool small = z < kI0Split;
   sel = small ? q : pr;
   zs = small ? z : 0.f;
 }
 template <typename V>
 __device__ __forceinline__ void rician_acc(V y, V w, V base, V nS0, V tS0, V& rr, V& prod, V& zs) {
-  constexpr float s1 = 3.5156229f / 14.0625f, s2 = 3.0899424f / (14.0625f * 14.0625f),
-                  s3 = 1.2067492f / (14.0625f * 14.0625f * 14.0625f),
-                  s4 = 0.2659732f / (14.0625f * 14.0625f * 14.0625f * 14.0625f),
-                  s5 = 0.0360768f / (14.0625f * 14.0625f * 14.0625f * 14.0625f * 14.0625f),
-                  s6 = 0.0045813f / (14.0625f * 14.0625f * 14.0625f * 14.0625f * 14.0625f * 14.0625f);
-  constexpr float c1 = 3.75f, c2 = c1 * c1, c3 = c2 * c1, c4 = c3 * c1, c5 = c4 * c1, c6 = c5 * c1, c7 = c6 * c1,
-                  c8 = c7 * c1;
   const V r = vfma(nS0, base, y);
   const V z = vmul(tS0, vmul(y, base));
   const V u = vmul(z, z);
-  V q = vfma(u, vbc<V>(s6), vbc<V>(s5));
-  q = vfma(u, q, vbc<V>(s4));
-  q = vfma(u, q, vbc<V>(s3));
-  q = vfma(u, q, vbc<V>(s2));
-  q = vfma(u, q, vbc<V>(s1));
-  q = vfma(u, q, vbc<V>(1.0f));
+  V q = vfma(u, vbc<V>(kI0Small(6)), vbc<V>(kI0Small(5)));
+#pragma unroll
+  for (int i = 4; i >= 0; --i) q = vfma(u, q, vbc<V>(kI0Small(i)));
   V rs;
   if constexpr (sizeof(V) == 8) {
-    rs = make_float2(rsqrt_approx(fmaxf(z.x, 3.75f)), rsqrt_approx(fmaxf(z.y, 3.75f)));
+    rs = make_float2(rsqrt_approx(z.x), rsqrt_approx(z.y));
   } else {
-    rs = rsqrt_approx(fmaxf(z, 3.75f));
+    rs = rsqrt_approx(z);
   }
   const V v = vmul(rs, rs);
-  V p = vfma(v, vbc<V>(0.00392377f * c8), vbc<V>(-0.01647633f * c7));
-  p = vfma(v, p, vbc<V>(0.02635537f * c6));
-  p = vfma(v, p, vbc<V>(-0.02057706f * c5));
-  p = vfma(v, p, vbc<V>(0.00916281f * c4));
-  p = vfma(v, p, vbc<V>(-0.00157565f * c3));
-  p = vfma(v, p, vbc<V>(0.00225319f * c2));
-  p = vfma(v, p, vbc<V>(0.01328592f * c1));
-  p = vfma(v, p, vbc<V>(0.39894228f));
+  V p = vfma(v, vbc<V>(kI0Large(5)), vbc<V>(kI0Large(4)));
+#pragma unroll
+  for (int i = 3; i >= 0; --i) p = vfma(v, p, vbc<V>(kI0Large(i)));
   const V pr = vmul(p, rs);
   V sel, zz;
   if constexpr (sizeof(V) == 8) {
