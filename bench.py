@@ -47,7 +47,7 @@ WORKLOAD_LEARNED = ("whole-brain: model 2, 3 fibres, rician+f0+ardf0, 288 measur
 # DRAM bytes (read + write) of one mcmc_kernel launch per voxel on the whole-brain workload, from
 # an ncu capture of a 131072-voxel launch: 307,087,104 B read + 473,595,136 B written.  The kernel
 # keeps its chain state on chip, so its traffic scales with voxels, not with iterations.
-MCMC_DRAM_BYTES_PER_VOXEL = (307087104 + 473595136) / 131072
+MCMC_DRAM_BYTES_PER_VOXEL = (313204224 + 441731584) / 131072
 
 
 def whole_brain_options() -> Options:
@@ -55,12 +55,14 @@ def whole_brain_options() -> Options:
 
 
 def mcmc_work_per_voxel(o: Options, ndir: int) -> tuple[float, float]:
-    """Algorithmic MUFU and FP32 operations of one voxel's chain (minimal formulation).
+    """Algorithmic MUFU and FP32 operations of one voxel's chain (the kernel's formulation).
 
     Per iteration: L likelihood evaluations over the M measurements and T signal-term updates.
     MUFU per signal term: 1 (models 1/3: exp2) or 2 (model 2: log2 + exp2 with the per-proposal
-    Gamma scale hoisted); per Rician likelihood term 2 (rsqrt + log2), Gaussian 0.  FP32 ops per
-    signal term 6, per likelihood term K+4 (+12 Rician).
+    Gamma scale hoisted); per Rician likelihood term 1.2 (an rsqrt, and one log2 per product of five
+    Bessel factors), Gaussian 0.  FP32 operations (an FMA counts as one) per signal term 6, per
+    likelihood term K+4 (prediction, residual, weighted square) plus 19 when Rician (the two log I0
+    polynomials of degrees 6 and 5, their arguments z, z^2, 1/z and the product/sum accumulations).
     """
     K, M = o.nfibres, ndir
     J = o.nburn + o.njumps
@@ -69,9 +71,9 @@ def mcmc_work_per_voxel(o: Options, ndir: int) -> tuple[float, float]:
     T = (K + 1) * M + (K + 1) * M * (1 if o.model == 2 else 0) + M * (1 if o.model == 3 else 0) \
         + K * M * (1 if o.model == 3 else 0) + 2 * K * M
     c_sig = 2 if o.model == 2 else 1
-    c_lik = 2 if o.rician else 0
+    c_lik = 1.2 if o.rician else 0.0
     mufu = J * (T * c_sig + L * M * c_lik)
-    fp32 = J * (T * 6 + L * M * (K + 4 + (12 if o.rician else 0)))
+    fp32 = J * (T * 6 + L * M * (K + 4 + (19 if o.rician else 0)))
     return float(mufu), float(fp32)
 
 
@@ -557,15 +559,20 @@ def main():
     mcmc_per_launch_s = t_mcmc / args.steps
     achieved = mufu_v * chunk / mcmc_per_launch_s
     fp32_achieved = fp32_v * chunk / mcmc_per_launch_s
-    roof_time = max(mufu_v * chunk / mufu_peak, fp32_v * chunk / fma_peak)
+    t_mufu, t_fp32 = mufu_v * chunk / mufu_peak, fp32_v * chunk / fma_peak
+    roof_time = max(t_mufu, t_fp32)
+    fp32_bound = t_fp32 >= t_mufu  # the pipe whose algorithmic work takes longer at its peak
     roofline = {
-        "bound": "sfu", "achieved": achieved / 1e9, "peak": mufu_peak / 1e9, "unit": "Gop/s",
-        "frac": achieved / mufu_peak,
+        "bound": "fp32" if fp32_bound else "sfu",
+        "achieved": (fp32_achieved if fp32_bound else achieved) / 1e9,
+        "peak": (fma_peak if fp32_bound else mufu_peak) / 1e9, "unit": "Gop/s",
+        "frac": (fp32_achieved / fma_peak) if fp32_bound else (achieved / mufu_peak),
+        "sfu_achieved": achieved / 1e9, "sfu_peak": mufu_peak / 1e9, "sfu_frac": achieved / mufu_peak,
         "traffic": MCMC_DRAM_BYTES_PER_VOXEL * chunk if (o.model, o.nfibres, M, o.nsamples) == (2, 3, 288, 50) else None,
         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one mcmc_kernel launch "
                           "(131072 voxels, this workload), scaled by voxels (profiles/mcmc_kernel_model2_k3_rician.md)",
         "kernel": f"mcmc_kernel (burn-in + recording), timed in the {rf} form's step",
-        "fp32_achieved": fp32_achieved / 1e9, "fp32_peak": fma_peak / 1e9,
+        "fp32_achieved": fp32_achieved / 1e9, "fp32_peak": fma_peak / 1e9, "fp32_frac": fp32_achieved / fma_peak,
         "frac_of_roofline_time": roof_time / mcmc_per_launch_s,
         "peak_source": "measured on this GPU by bpx_measure_pipes (ex2.approx and FFMA issue-rate kernels)",
         "work_per_voxel": {"mufu": mufu_v, "fp32": fp32_v},
