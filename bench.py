@@ -45,7 +45,7 @@ WORKLOAD_LEARNED = ("whole-brain: model 2, 3 fibres, rician+f0+ardf0, 288 measur
 
 
 # DRAM bytes (read + write) of one mcmc_kernel launch per voxel on the whole-brain workload, from
-# an ncu capture of a 131072-voxel launch: 307,087,104 B read + 473,595,136 B written.  The kernel
+# an ncu capture of a 131072-voxel launch: 313,204,224 B read + 441,731,584 B written.  The kernel
 # keeps its chain state on chip, so its traffic scales with voxels, not with iterations.
 MCMC_DRAM_BYTES_PER_VOXEL = (313204224 + 441731584) / 131072
 
