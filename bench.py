@@ -54,22 +54,39 @@ def whole_brain_options() -> Options:
     return Options.make(model=2, nfibres=3, rician=1, f0=1, ardf0=1, nburn=1000, njumps=1250, sampleevery=25)
 
 
-def mcmc_work_per_voxel(o: Options, ndir: int) -> tuple[float, float]:
-    """Algorithmic MUFU and FP32 operations of one voxel's chain (the kernel's formulation).
-
-    Per iteration: L likelihood evaluations over the M measurements and T signal-term updates.
-    MUFU per signal term: 1 (models 1/3: exp2) or 2 (model 2: log2 + exp2 with the per-proposal
-    Gamma scale hoisted); per Rician likelihood term 1.2 (an rsqrt, and one log2 per product of five
-    Bessel factors), Gaussian 0.  FP32 operations (an FMA counts as one) per signal term 6, per
-    likelihood term K+4 (prediction, residual, weighted square) plus 19 when Rician (the two log I0
-    polynomials of degrees 6 and 5, their arguments z, z^2, 1/z and the product/sum accumulations).
-    """
+def _mcmc_terms(o: Options, ndir: int) -> tuple[int, int, int, int, int]:
+    """(J, L, T, K, M): iterations, likelihood evaluations and signal-term updates per iteration."""
     K, M = o.nfibres, ndir
     J = o.nburn + o.njumps
     L = (1 if o.f0 else 0) + (1 if o.rician else 0) + 1 + (1 if o.model >= 2 else 0) + (1 if o.model == 3 else 0) \
         + 1 + 3 * K
     T = (K + 1) * M + (K + 1) * M * (1 if o.model == 2 else 0) + M * (1 if o.model == 3 else 0) \
         + K * M * (1 if o.model == 3 else 0) + 2 * K * M
+    return J, L, T, K, M
+
+
+def mcmc_work_canonical(o: Options, ndir: int) -> tuple[float, float]:
+    """Canonical algorithmic MUFU and FP32-FMA operations of one voxel's chain: the path's minimal
+    formulation with the reference's operations (model-2 signal terms rcp + log2 + exp2, Rician
+    likelihood terms log2 + rsqrt; FMA per signal term 6, per likelihood term K+4, +12 Rician)."""
+    J, L, T, K, M = _mcmc_terms(o, ndir)
+    c_sig = 3 if o.model == 2 else 1
+    c_lik = 2 if o.rician else 0
+    mufu = J * (T * c_sig + L * M * c_lik)
+    fp32 = J * (T * 6 + L * M * (K + 4 + (12 if o.rician else 0)))
+    return float(mufu), float(fp32)
+
+
+def mcmc_work_per_voxel(o: Options, ndir: int) -> tuple[float, float]:
+    """MUFU and FP32 operations of one voxel's chain as this kernel formulates it.
+
+    MUFU per signal term: 1 (models 1/3: exp2) or 2 (model 2: log2 + exp2 with the per-proposal
+    Gamma scale hoisted); per Rician likelihood term 1.2 (an rsqrt, and one log2 per product of five
+    Bessel factors), Gaussian 0.  FP32 operations (an FMA counts as one) per signal term 6, per
+    likelihood term K+4 (prediction, residual, weighted square) plus 19 when Rician (the two log I0
+    polynomials of degrees 6 and 5, their arguments z, z^2, 1/z and the product/sum accumulations).
+    """
+    J, L, T, K, M = _mcmc_terms(o, ndir)
     c_sig = 2 if o.model == 2 else 1
     c_lik = 1.2 if o.rician else 0.0
     mufu = J * (T * c_sig + L * M * c_lik)
@@ -555,27 +572,36 @@ def main():
         return
     # ---- roofline of the dominant kernel (the MCMC chain) ----
     mufu_peak, fma_peak = lib.measure_pipes()
-    mufu_v, fp32_v = mcmc_work_per_voxel(ho, M)
     mcmc_per_launch_s = t_mcmc / args.steps
-    achieved = mufu_v * chunk / mcmc_per_launch_s
-    fp32_achieved = fp32_v * chunk / mcmc_per_launch_s
-    t_mufu, t_fp32 = mufu_v * chunk / mufu_peak, fp32_v * chunk / fma_peak
-    roof_time = max(t_mufu, t_fp32)
-    fp32_bound = t_fp32 >= t_mufu  # the pipe whose algorithmic work takes longer at its peak
+
+    def pipe_fracs(mufu_v: float, fp32_v: float) -> dict:
+        t_mufu, t_fp32 = mufu_v * chunk / mufu_peak, fp32_v * chunk / fma_peak
+        sfu_a, fp32_a = mufu_v * chunk / mcmc_per_launch_s, fp32_v * chunk / mcmc_per_launch_s
+        fp32_bound = t_fp32 >= t_mufu  # the pipe whose work takes longer at its measured peak
+        return {"bound": "fp32" if fp32_bound else "sfu",
+                "achieved": (fp32_a if fp32_bound else sfu_a) / 1e9,
+                "peak": (fma_peak if fp32_bound else mufu_peak) / 1e9,
+                "frac": max(t_mufu, t_fp32) / mcmc_per_launch_s,
+                "sfu_achieved": sfu_a / 1e9, "sfu_frac": sfu_a / mufu_peak,
+                "fp32_achieved": fp32_a / 1e9, "fp32_frac": fp32_a / fma_peak,
+                "work_per_voxel": {"mufu": mufu_v, "fp32": fp32_v}}
+
+    canon = pipe_fracs(*mcmc_work_canonical(ho, M))
+    own = pipe_fracs(*mcmc_work_per_voxel(ho, M))
     roofline = {
-        "bound": "fp32" if fp32_bound else "sfu",
-        "achieved": (fp32_achieved if fp32_bound else achieved) / 1e9,
-        "peak": (fma_peak if fp32_bound else mufu_peak) / 1e9, "unit": "Gop/s",
-        "frac": (fp32_achieved / fma_peak) if fp32_bound else (achieved / mufu_peak),
-        "sfu_achieved": achieved / 1e9, "sfu_peak": mufu_peak / 1e9, "sfu_frac": achieved / mufu_peak,
+        "bound": canon["bound"], "achieved": canon["achieved"], "peak": canon["peak"], "unit": "Gop/s",
+        "frac": canon["frac"],
         "traffic": MCMC_DRAM_BYTES_PER_VOXEL * chunk if (o.model, o.nfibres, M, o.nsamples) == (2, 3, 288, 50) else None,
         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one mcmc_kernel launch "
                           "(131072 voxels, this workload), scaled by voxels (profiles/mcmc_kernel_model2_k3_rician.md)",
         "kernel": f"mcmc_kernel (burn-in + recording), timed in the {rf} form's step",
-        "fp32_achieved": fp32_achieved / 1e9, "fp32_peak": fma_peak / 1e9, "fp32_frac": fp32_achieved / fma_peak,
-        "frac_of_roofline_time": roof_time / mcmc_per_launch_s,
+        "counts": "canonical per-term counts (model-2 signal rcp+log2+exp2, Rician log2+rsqrt; FMA 6 per signal "
+                  "term, K+4(+12 Rician) per likelihood term)",
+        "sfu_peak": mufu_peak / 1e9, "fp32_peak": fma_peak / 1e9,
+        "sfu_frac": canon["sfu_frac"], "fp32_frac": canon["fp32_frac"],
+        "work_per_voxel": canon["work_per_voxel"],
+        "kernel_formulation": {k: own[k] for k in ("bound", "frac", "sfu_frac", "fp32_frac", "work_per_voxel")},
         "peak_source": "measured on this GPU by bpx_measure_pipes (ex2.approx and FFMA issue-rate kernels)",
-        "work_per_voxel": {"mufu": mufu_v, "fp32": fp32_v},
     }
     peaks = measured_peaks()
     forms_out = {}
