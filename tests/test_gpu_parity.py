@@ -111,7 +111,7 @@ def test_fit_handles_nonfinite_and_empty(torch, lib):
     assert p0.shape[0] == 0
 
 
-def _state_sample(o, prot, n, seed):
+def _state_sample(o, prot, n, seed, snr=25.0, snr_tau=20.0):
     rng = np.random.default_rng(seed)
     tr = synth.sample_truth(rng, n, o.nfibres, o.model >= 2)
     st = np.zeros((n, 15))
@@ -119,14 +119,14 @@ def _state_sample(o, prot, n, seed):
     st[:, 1] = tr.d * rng.uniform(0.8, 1.2, n)
     st[:, 2] = tr.dstd if tr.dstd is not None else 0.0
     st[:, 3] = 0.13
-    st[:, 4] = (20.0 / 1000.0) ** 2 * rng.uniform(0.5, 2.0, n)
+    st[:, 4] = (snr_tau / 1000.0) ** 2 * rng.uniform(0.5, 2.0, n)
     st[:, 5] = 0.02 if o.f0 else 0.0
     for k in range(o.nfibres):
         v = tr.v[:, k, :]
         st[:, 6 + 3 * k] = np.arccos(np.clip(v[:, 2], -1, 1)) + rng.normal(0, 0.05, n)
         st[:, 7 + 3 * k] = np.arctan2(v[:, 1], v[:, 0]) + rng.normal(0, 0.05, n)
         st[:, 8 + 3 * k] = np.clip(tr.f[:, k], 0.01, None)
-    y = synth.add_rician(rng, synth.predict(tr, prot, o.model >= 2), tr.S0 / 25.0).astype(np.float32)
+    y = synth.add_rician(rng, synth.predict(tr, prot, o.model >= 2), tr.S0 / snr).astype(np.float32)
     return st, y
 
 
@@ -154,6 +154,25 @@ def test_energy_parity(torch, lib, oracle, kw):
     rel = np.abs(lg - lo) / np.abs(lo)
     assert np.max(rel) < 2e-5, f"max rel err {np.max(rel):.3g}"
     assert np.max(np.abs(pri_g - pri_o)) < 1e-4
+
+
+@pytest.mark.parametrize("snr,tol", [(3.0, 2e-5), (1000.0, 1e-3)])
+def test_energy_parity_extreme_snr(torch, lib, oracle, snr, tol):
+    """Rician energies where every Bessel argument is small (SNR 3) or large (SNR 1000: z up to
+    ~1e6, products of five Bessel factors near 1e-15).  At SNR 1000 the energy of these perturbed
+    states is dominated by tau/2 sum r^2 with tau = 1 and residuals of tens; the FP32 signals
+    (exp2/log2 at Gamma shapes up to ~100, ~1e-5 relative) move each residual by ~1e-5 S0, hence
+    the wider relative tolerance there (the log I0 terms themselves are within 6e-7 each)."""
+    o = Options.make(model=2, nfibres=3, rician=1, f0=1, ardf0=1)
+    prot = synth.three_shell(18, 90)
+    st, y = _state_sample(o, prot, 256, seed=11, snr=snr, snr_tau=snr)
+    y = oracle.prepare_data(y)
+    lo, _ = oracle.energy(o, y, prot.bvecs, prot.bvals, st)
+    d, bv, bl, sd = _dev(torch, y, prot.bvecs, prot.bvals, st)
+    lg, _ = lib.energy(o, d, bv, bl, sd)
+    lg = lg.cpu().numpy().astype(np.float64)
+    assert np.all(np.isfinite(lg))
+    assert np.max(np.abs(lg - lo) / np.abs(lo)) < tol
 
 
 def _run_both(torch, lib, oracle, o, y, prot, n_vox, voxel_offset=0):
