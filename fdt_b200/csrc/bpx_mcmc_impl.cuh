@@ -5,12 +5,14 @@
 // of CUDA/runmcmc_kernels.cu:193-1474 with one launch that runs each voxel's whole chain.
 //
 // Layout: a group of TPV lanes owns one voxel; lane l of the group holds measurements
-// l, l+TPV, ... (at most MPL of them) in registers: data y, b-value, the squared projections
-// c_k = (g.v_k)^2 of every fibre, the per-fibre signals s_k and the isotropic signal.  The scalar
-// chain state (parameters, priors, proposal widths, acceptance counts) is replicated in every
-// lane of the group, so the accept/reject logic needs no broadcast; likelihood sums use an
-// xor-butterfly over the group.  Proposals evaluate new signals into registers and commit them
-// with selects, so groups sharing a warp never diverge.
+// l, l+TPV, ... (at most MPL of them) as packed pairs plus one unpaired tail.  Registers hold
+// what changes during the chain: the per-fibre stick signals and the isotropic signal.  Shared
+// memory holds what is read-only or rarely written: the (g, b) table, each thread's data y and
+// padding weights, the backups of signals a proposal overwrites, the group's proposal widths,
+// acceptance counts and fibre state (angles, directions, priors).  The scalar chain state is
+// replicated in every lane of the group, so the accept/reject logic needs no broadcast;
+// likelihood sums use an xor-butterfly over the group.  A proposal overwrites the signals it
+// changes in place (old values backed up in shared memory) and restores them if rejected.
 //
 // Random numbers: slot s of iteration it of voxel v uses Philox-4x32-10 with counter
 // (it, s, v) and key = seed.  At the start of each iteration lane l computes slots l, l+TPV, ...
@@ -21,6 +23,8 @@
 //     (M/2) ln(SS_old/SS_new) (Gaussian) or M ln(tau_new/tau_old) + sum(t_new - t_old) (Rician)
 //     with the Rician terms written as log y - tau (y-p)^2/2 + [logI0(z) - z], so no large
 //     cancelling sums appear in FP32.
+//   * log I0, sin and cos from polynomials fitted for this library (bpx_device.cuh), at FP32
+//     accuracy, in place of the reference's A&S polynomials and the CUDA math library.
 //   * a proposal rejected by its prior skips the likelihood (the reference evaluates and
 //     discards it); its random numbers are consumed either way, being slot-keyed.
 //   * fibre directions enter as dot products (g.v)^2 instead of the reference's three cosines of
@@ -114,6 +118,7 @@ __device__ __forceinline__ bool r_prior(const Priors& pr, float R, float d, floa
   return false;
 }
 
+// per-lane measurement arrays of the energy kernel (one state per voxel, no chain)
 template <int MODEL, int K, bool RIC, int TPV, int MPL>
 struct Lanes {
   float y[MPL], b[MPL], c[K][MPL], s[K][MPL], iso[MPL];
@@ -452,45 +457,45 @@ __global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_ker
     // backing up the overwritten ones when backup is true
     auto all_signals = [&](const SigParams<MODEL>& sp, bool sticks, bool isob, bool backup) {
       with_signal_form<MODEL>(sp, [&](auto form) {
-      constexpr bool MONO = decltype(form)::value;
-      const float2 beta2 = make_float2(sp.beta, sp.beta);
+        constexpr bool MONO = decltype(form)::value;
+        const float2 beta2 = make_float2(sp.beta, sp.beta);
 #pragma unroll
-      for (int p = 0; p < NP; ++p) {
-        const float4 ga = gb[p * TPV + gl], gc = gb[(NP + p) * TPV + gl];
-        const float2 gx = make_float2(ga.x, ga.y), gy = make_float2(ga.z, ga.w), gz = make_float2(gc.x, gc.y);
-        const float2 b = make_float2(gc.z, gc.w);
-        const float2 bbeta = vmul(beta2, b);
-        if (sticks) {
+        for (int p = 0; p < NP; ++p) {
+          const float4 ga = gb[p * TPV + gl], gc = gb[(NP + p) * TPV + gl];
+          const float2 gx = make_float2(ga.x, ga.y), gy = make_float2(ga.z, ga.w), gz = make_float2(gc.x, gc.y);
+          const float2 b = make_float2(gc.z, gc.w);
+          const float2 bbeta = vmul(beta2, b);
+          if (sticks) {
 #pragma unroll
-          for (int k = 0; k < K; ++k) {
-            float2 dp = vmul(gx, vbc<float2>(fst[kFsVx * K + k]));
-            dp = vfma(gy, vbc<float2>(fst[kFsVy * K + k]), dp);
-            dp = vfma(gz, vbc<float2>(fst[kFsVz * K + k]), dp);
-            if (backup) bkp[(k * NP + p) * kMcmcThreads] = s2[k][p];
-            s2[k][p] = stick_v<MODEL, MONO, float2>(sp, b, bbeta, vmul(dp, dp));
+            for (int k = 0; k < K; ++k) {
+              float2 dp = vmul(gx, vbc<float2>(fst[kFsVx * K + k]));
+              dp = vfma(gy, vbc<float2>(fst[kFsVy * K + k]), dp);
+              dp = vfma(gz, vbc<float2>(fst[kFsVz * K + k]), dp);
+              if (backup) bkp[(k * NP + p) * kMcmcThreads] = s2[k][p];
+              s2[k][p] = stick_v<MODEL, MONO, float2>(sp, b, bbeta, vmul(dp, dp));
+            }
+          }
+          if (isob) {
+            if (backup) bkp[(K * NP + p) * kMcmcThreads] = i2[p];
+            i2[p] = iso_v<MODEL, MONO, float2>(sp, b, bbeta);
           }
         }
-        if (isob) {
-          if (backup) bkp[(K * NP + p) * kMcmcThreads] = i2[p];
-          i2[p] = iso_v<MODEL, MONO, float2>(sp, b, bbeta);
-        }
-      }
-      if (TAIL) {
-        const float4 g = gb[2 * NP * TPV + gl];
-        const float bbeta = sp.beta * g.w;
-        if (sticks) {
+        if (TAIL) {
+          const float4 g = gb[2 * NP * TPV + gl];
+          const float bbeta = sp.beta * g.w;
+          if (sticks) {
 #pragma unroll
-          for (int k = 0; k < K; ++k) {
-            const float dp = g.x * fst[kFsVx * K + k] + g.y * fst[kFsVy * K + k] + g.z * fst[kFsVz * K + k];
-            if (backup) bkt[k * kMcmcThreads] = st[k];
-            st[k] = stick_v<MODEL, MONO, float>(sp, g.w, bbeta, dp * dp);
+            for (int k = 0; k < K; ++k) {
+              const float dp = g.x * fst[kFsVx * K + k] + g.y * fst[kFsVy * K + k] + g.z * fst[kFsVz * K + k];
+              if (backup) bkt[k * kMcmcThreads] = st[k];
+              st[k] = stick_v<MODEL, MONO, float>(sp, g.w, bbeta, dp * dp);
+            }
+          }
+          if (isob) {
+            if (backup) bkt[K * kMcmcThreads] = it_;
+            it_ = iso_v<MODEL, MONO, float>(sp, g.w, bbeta);
           }
         }
-        if (isob) {
-          if (backup) bkt[K * kMcmcThreads] = it_;
-          it_ = iso_v<MODEL, MONO, float>(sp, g.w, bbeta);
-        }
-      }
       });
     };
     // the likelihood statistic of a state, summed over the group
@@ -620,30 +625,30 @@ __global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_ker
           nvy = sn * sp_;
           nvz = cs;
           with_signal_form<MODEL>(spc, [&](auto form) {
-          constexpr bool MONO = decltype(form)::value;
-          const SigParams<MODEL>& sp = spc;
-          const float2 beta2 = make_float2(sp.beta, sp.beta);
-          const float2 nvx2 = vbc<float2>(nvx), nvy2 = vbc<float2>(nvy), nvz2 = vbc<float2>(nvz);
+            constexpr bool MONO = decltype(form)::value;
+            const SigParams<MODEL>& sp = spc;
+            const float2 beta2 = make_float2(sp.beta, sp.beta);
+            const float2 nvx2 = vbc<float2>(nvx), nvy2 = vbc<float2>(nvy), nvz2 = vbc<float2>(nvz);
 #pragma unroll
-          for (int k = 0; k < K; ++k)
-            if (k == kf) {
+            for (int k = 0; k < K; ++k)
+              if (k == kf) {
 #pragma unroll
-              for (int p = 0; p < NP; ++p) {
-                const float4 ga = gb[p * TPV + gl], gc = gb[(NP + p) * TPV + gl];
-                float2 dp = vmul(make_float2(ga.x, ga.y), nvx2);
-                dp = vfma(make_float2(ga.z, ga.w), nvy2, dp);
-                dp = vfma(make_float2(gc.x, gc.y), nvz2, dp);
-                const float2 b = make_float2(gc.z, gc.w);
-                bkp[p * kMcmcThreads] = s2[k][p];
-                s2[k][p] = stick_v<MODEL, MONO, float2>(sp, b, vmul(beta2, b), vmul(dp, dp));
+                for (int p = 0; p < NP; ++p) {
+                  const float4 ga = gb[p * TPV + gl], gc = gb[(NP + p) * TPV + gl];
+                  float2 dp = vmul(make_float2(ga.x, ga.y), nvx2);
+                  dp = vfma(make_float2(ga.z, ga.w), nvy2, dp);
+                  dp = vfma(make_float2(gc.x, gc.y), nvz2, dp);
+                  const float2 b = make_float2(gc.z, gc.w);
+                  bkp[p * kMcmcThreads] = s2[k][p];
+                  s2[k][p] = stick_v<MODEL, MONO, float2>(sp, b, vmul(beta2, b), vmul(dp, dp));
+                }
+                if (TAIL) {
+                  const float4 g = gb[2 * NP * TPV + gl];
+                  const float dp = g.x * nvx + g.y * nvy + g.z * nvz;
+                  bkt[0] = st[k];
+                  st[k] = stick_v<MODEL, MONO, float>(sp, g.w, sp.beta * g.w, dp * dp);
+                }
               }
-              if (TAIL) {
-                const float4 g = gb[2 * NP * TPV + gl];
-                const float dp = g.x * nvx + g.y * nvy + g.z * nvz;
-                bkt[0] = st[k];
-                st[k] = stick_v<MODEL, MONO, float>(sp, g.w, sp.beta * g.w, dp * dp);
-              }
-            }
           });
         } else if (kind == 2) {
           if (slot == kSlotD) {
