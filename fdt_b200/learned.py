@@ -65,11 +65,37 @@ class TrainingSet:
         return int(self.x.shape[0])
 
 
-def label_options(opts: Options) -> Options:
-    """Options of the labelling chain: the plain chain's burn-in, one recorded sample."""
+MEAN_LABEL_SAMPLES = 10
+
+
+def label_options(opts: Options, samples: int = 1) -> Options:
+    """Options of the labelling chain: the plain chain's burn-in, then `samples` recorded samples."""
     o = Options.make(**{f: getattr(opts, f) for f, _ in Options._fields_ if f != "reserved"})
-    o.njumps = o.sampleevery
+    o.njumps = o.sampleevery * samples
     return o
+
+
+def state_mean_from_records(opts: Options, rec):
+    """(params [n][P] in the fit layout, tau [n]) of the posterior mean over the recorded samples:
+    means of the scalars and fractions; for each fibre the principal eigenvector of the mean dyadic
+    tensor (v v^T over samples, so the sign of v does not matter), as angles with theta in [0, pi]."""
+    import torch
+
+    r = rec.double()
+    m = r.mean(1)  # [rows][n]
+    K = opts.nfibres
+    cols = [m[5], m[0]] + ([m[3]] if opts.model >= 2 else [])
+    for k in range(K):
+        th, ph = r[6 + 3 * k], r[7 + 3 * k]  # [ns][n]
+        v = torch.stack([torch.sin(th) * torch.cos(ph), torch.sin(th) * torch.sin(ph), torch.cos(th)], -1)
+        dyad = torch.nan_to_num(torch.einsum("sni,snj->nij", v, v) / v.shape[0], nan=0.0, posinf=0.0, neginf=0.0)
+        _, vecs = torch.linalg.eigh(dyad.cpu())  # host LAPACK: the batched device solver rejects large batches
+        e = vecs[..., 2].to(dyad.device)  # largest eigenvalue's vector
+        e = torch.where((e[:, 2:3] < 0), -e, e)
+        cols += [m[8 + 3 * k], torch.arccos(e[:, 2].clamp(-1.0, 1.0)), torch.atan2(e[:, 1], e[:, 0])]
+    if opts.f0:
+        cols.append(m[1])
+    return torch.stack(cols, 1).float().contiguous(), m[2].float().contiguous()
 
 
 def state_from_record(opts: Options, rec, sample: int = 0):
@@ -92,8 +118,9 @@ def make_training_set(opts: Options, bvecs: np.ndarray, bvals: np.ndarray, n: in
     """n forward-model voxels (SNR ~ U(snr)) with their labels.  The plain chain is run from each
     voxel's LM fit through its full burn-in; its proposal widths at that point are the width
     labels, and the state labels are either that chain state (state_labels="chain": the state the
-    LM-initialised chain reaches, which is where a chain with frozen widths must start) or the LM
-    fit itself ("lm")."""
+    LM-initialised chain reaches, which is where a chain with frozen widths must start), the
+    posterior mean over MEAN_LABEL_SAMPLES samples recorded after the burn-in ("mean", widths then
+    taken at the end of that recording) or the LM fit itself ("lm")."""
     import torch
 
     L = lib.load()
@@ -102,7 +129,7 @@ def make_training_set(opts: Options, bvecs: np.ndarray, bvals: np.ndarray, n: in
     x = torch.empty((n, nin(ndir)), device="cuda", dtype=torch.bfloat16)
     t = torch.empty((n, NOUT), device="cuda", dtype=torch.float32)
     w = torch.empty((n, NOUT), device="cuda", dtype=torch.float32)
-    lo = label_options(opts)
+    lo = label_options(opts, MEAN_LABEL_SAMPLES if state_labels == "mean" else 1)
     stream = lib._stream(torch)
     for s in range(0, n, chunk):
         m = min(chunk, n - s)
@@ -115,11 +142,13 @@ def make_training_set(opts: Options, bvecs: np.ndarray, bvals: np.ndarray, n: in
         lib._check(L.bpx_mlp_features_dev(C.byref(vol), 0, lib._ptr(x[s : s + m]), lib._ptr(s0hat), stream),
                    "bpx_mlp_features_dev")
         props = None
-        if widths or state_labels == "chain":
+        if widths or state_labels in ("chain", "mean"):
             rec, props = lib.mcmc_ex(lo, data, bv, bl, params, tau if opts.rician else None, want_props=True,
                                      voxel_offset=s, status=status)
             if state_labels == "chain":
                 params, tau = state_from_record(opts, rec)
+            elif state_labels == "mean":
+                params, tau = state_mean_from_records(opts, rec)
             if not widths:
                 props = None
         lib._check(L.bpx_mlp_targets_dev(C.byref(opts), m, lib._ptr(params), lib._ptr(tau if opts.rician else None),
@@ -327,7 +356,7 @@ def main(argv=None) -> None:
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--out", default=None)
     ap.add_argument("--eval", type=int, default=8192, help="held-out voxels for the learned-vs-plain check")
-    ap.add_argument("--labels", default="chain", choices=["chain", "lm"])
+    ap.add_argument("--labels", default="chain", choices=["chain", "mean", "lm"])
     ap.add_argument("--weights", default=None, help="evaluate these weights instead of training")
     a = ap.parse_args(argv)
     prot = PROTOCOLS[a.protocol](synth)
