@@ -197,7 +197,7 @@ __device__ __forceinline__ float vhsum(float2 x) { return x.x + x.y; }
 // polynomials of bpx_device.cuh, split at 4.75, have degrees 6 and 5 at the same accuracy (log I0
 // within 6e-7 after FP32 rounding).  Both branches are evaluated, branch-free, since the measurements
 // of one warp fall on both sides of the split; the unselected branch may be inf or NaN (rsqrt of a
-// small z), which the select discards.  Every factor lies in (0, 15], so a product of five stays in
+// small z), which the select discards.  Every factor lies in (0, 22] (I0(4.75) = 21.8), so a product of five stays in
 // FP32's normal range for z below ~1e14 and one log2 per product replaces one per measurement.
 // Padding measurements (y = 0, w = 0) give z = 0 and the factor kI0Small(0) = 1.
 __device__ __forceinline__ void rician_pick(float z, float q, float pr, float& sel, float& zs) {
