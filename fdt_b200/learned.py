@@ -114,7 +114,7 @@ def state_from_record(opts: Options, rec, sample: int = 0):
 
 def make_training_set(opts: Options, bvecs: np.ndarray, bvals: np.ndarray, n: int, seed: int = 1,
                       snr=(10.0, 40.0), chunk: int = 131072, widths: bool = True,
-                      state_labels: str = "chain") -> TrainingSet:
+                      state_labels: str = "mean") -> TrainingSet:
     """n forward-model voxels (SNR ~ U(snr)) with their labels.  The plain chain is run from each
     voxel's LM fit through its full burn-in; its proposal widths at that point are the width
     labels, and the state labels are either that chain state (state_labels="chain": the state the
@@ -338,7 +338,7 @@ def default_weights_path(protocol: str) -> str:
 def main(argv=None) -> None:
     """Train the initialiser for a protocol on the GPU and save it:
 
-        python -m fdt_b200.learned --protocol whole_brain --n 1000000 --steps 4000
+        python -m fdt_b200.learned --protocol whole_brain --n 10485760 --steps 40000
     """
     import argparse
     import time
@@ -356,7 +356,7 @@ def main(argv=None) -> None:
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--out", default=None)
     ap.add_argument("--eval", type=int, default=8192, help="held-out voxels for the learned-vs-plain check")
-    ap.add_argument("--labels", default="chain", choices=["chain", "mean", "lm"])
+    ap.add_argument("--labels", default="mean", choices=["chain", "mean", "lm"])
     ap.add_argument("--weights", default=None, help="evaluate these weights instead of training")
     a = ap.parse_args(argv)
     prot = PROTOCOLS[a.protocol](synth)

@@ -107,5 +107,8 @@ def test_learned_start_matches_plain_and_beats_no_network(torch, setup):
     rec, _ = lib.mcmc_ex(lo, d, s["bv"], s["bl"], p0, tau0, props_in=None, freeze=0, status=st0)
     naive = lib.finish(lo, rec)
     abl = learned.summary(o, naive, s["plain"])
-    assert abl["dyad_median_deg"][0] > 3.0 * acc["dyad_median_deg"][0], (abl, acc)
+    # the network's start beats the data-independent one on both dyads and on f1's agreement
+    assert abl["dyad_median_deg"][0] > 2.5 * acc["dyad_median_deg"][0], (abl, acc)
+    assert abl["dyad_median_deg"][1] > 2.0 * acc["dyad_median_deg"][1], (abl, acc)
+    assert acc["f_within_2se"][0] > abl["f_within_2se"][0] + 0.15, (abl, acc)
     assert t_learned < 0.75 * t_plain, (t_learned, t_plain)

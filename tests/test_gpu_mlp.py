@@ -173,8 +173,8 @@ def test_decode_inverts_targets(torch):
 def test_training_reduces_loss(torch):
     """A short training run on forward-model voxels: the loss falls, and on held-out voxels the
     error of the well-determined outputs (f1, d, the first fibre's direction) drops well below
-    that of the untrained network.  (The total loss keeps a floor: the state and width labels are
-    single chain draws.)"""
+    that of the untrained network.  (The total loss keeps a floor: the state labels are means of
+    ten chain samples and the width labels single chain states.)"""
     from fdt_b200 import learned, lib, synth
 
     opts = Options.make(model=2, nfibres=3, rician=1, f0=1, ardf0=1)
