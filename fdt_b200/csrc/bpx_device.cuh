@@ -8,9 +8,7 @@
 
 namespace bpx {
 
-constexpr float kTwoPiGpu = 0.636619772f;  // CUDA/diffmodels_utils.h:13 (2/pi as the reference writes it)
-constexpr double kTwoPiGpuD = 0.636619772;
-constexpr float kFSmall = 0.001f;           // CUDA/diffmodels_utils.h:16
+constexpr double kTwoPiGpuD = 0.636619772;  // CUDA/diffmodels_utils.h:13 (2/pi as the reference writes it)
 constexpr float kUpperDiff = 0.005f;        // CUDA/runmcmc_kernels.cu:24
 constexpr float kMaxProp = 1e10f;           // CUDA/runmcmc_kernels.cu:23
 
@@ -55,11 +53,6 @@ __device__ __forceinline__ float lg2_approx(float x) {
 __device__ __forceinline__ float rsqrt_approx(float x) {
   float y;
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-__device__ __forceinline__ float rcp_approx(float x) {
-  float y;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
 
@@ -163,16 +156,5 @@ __device__ __forceinline__ float group_min(float x) {
   for (int o = G / 2; o >= 1; o >>= 1) x = fminf(x, __shfl_xor_sync(0xffffffffu, x, o));
   return x;
 }
-
-// transforms of CUDA/diffmodels_utils.h:19-41
-__device__ __forceinline__ float x2f(float x) { return fabsf(kTwoPiGpu * atanf(x)); }
-__device__ __forceinline__ float f2x(float f) { return tanf(f / kTwoPiGpu); }
-__device__ __forceinline__ float beta2f(float b) {
-  const float s = sinf(b);
-  return s * s;
-}
-__device__ __forceinline__ float f2beta(float f) { return asinf(sqrtf(f)); }
-__device__ __forceinline__ float sgnf(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }
-__device__ __forceinline__ float pm1(float x) { return x > 0.f ? 1.f : -1.f; }
 
 }  // namespace bpx
