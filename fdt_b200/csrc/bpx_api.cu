@@ -354,15 +354,31 @@ bpx_status bpx_fit_dev(const bpx_options* opts, const bpx_volume* vol, float* pa
   return fit_dev_scratch(opts, vol, params, tau, status, scratch, stream);
 }
 
-bpx_status bpx_mcmc_ex_dev(const bpx_options* opts, const bpx_volume* vol, const float* params, const float* tau,
-                           const float* props_in, float* props_out, int32_t freeze_props, float* records,
-                           uint32_t* status, void* stream) {
+}  // extern "C"
+
+namespace bpx {
+namespace {
+
+// One MCMC launch over a volume: the whole chain, or the stretch st describes (nullptr: all of it
+// from the LM parameters).
+struct Stretch {
+  int it_begin, it_end;
+  const float* state_in;
+  float* state_out;
+  const int32_t* acc_in;
+  int32_t* acc_out;
+};
+
+bpx_status mcmc_run(const bpx_options* opts, const bpx_volume* vol, const float* params, const float* tau,
+                    const float* props_in, float* props_out, int32_t freeze_props, float* records,
+                    uint32_t* status, void* stream, const Stretch* sp) {
   bpx_status st = check_opts(opts);
   if (st == BPX_OK) st = check_vol(vol, true);
   if (st != BPX_OK) return st;
   if (vol->nvox == 0) return BPX_OK;
-  if (!params || !records) return fail(BPX_ERR_INVALID_ARG, "params/records is NULL");
-  if (opts->rician && !tau) return fail(BPX_ERR_INVALID_ARG, "tau is NULL under rician");
+  const bool from_state = sp && sp->state_in;
+  if ((!params && !from_state) || !records) return fail(BPX_ERR_INVALID_ARG, "params/records is NULL");
+  if (opts->rician && !tau && !from_state) return fail(BPX_ERR_INVALID_ARG, "tau is NULL under rician");
   st = check_device();
   if (st != BPX_OK) return st;
   const McmcLayout lay = pick_layout(opts, vol->ndir);
@@ -399,8 +415,42 @@ bpx_status bpx_mcmc_ex_dev(const bpx_options* opts, const bpx_volume* vol, const
   a.props_out = props_out;
   if (freeze_props < 0 || freeze_props > 2) return fail(BPX_ERR_INVALID_ARG, "freeze_props must be 0, 1 or 2");
   a.freeze_props = freeze_props;
+  if (sp) {
+    a.it_begin = sp->it_begin;
+    a.it_end = sp->it_end;
+    a.state_in = sp->state_in;
+    a.state_out = sp->state_out;
+    a.acc_in = sp->acc_in;
+    a.acc_out = sp->acc_out;
+  }
   BPX_CUDA(launch_mcmc(a, opts->model, opts->nfibres, opts->rician != 0, lay, (cudaStream_t)stream));
   return BPX_OK;
+}
+
+}  // namespace
+}  // namespace bpx
+
+extern "C" {
+
+bpx_status bpx_mcmc_ex_dev(const bpx_options* opts, const bpx_volume* vol, const float* params, const float* tau,
+                           const float* props_in, float* props_out, int32_t freeze_props, float* records,
+                           uint32_t* status, void* stream) {
+  return mcmc_run(opts, vol, params, tau, props_in, props_out, freeze_props, records, status, stream, nullptr);
+}
+
+bpx_status bpx_mcmc_stretch_dev(const bpx_options* opts, const bpx_volume* vol, const float* params, const float* tau,
+                                const float* state_in, const float* props_in, const int32_t* acc_in,
+                                int32_t it_begin, int32_t it_end, int32_t freeze_props, float* records,
+                                float* state_out, float* props_out, int32_t* acc_out, uint32_t* status,
+                                void* stream) {
+  bpx_status st = check_opts(opts);
+  if (st != BPX_OK) return st;
+  const int total = opts->nburn + opts->njumps;
+  if (it_begin < 0 || it_end <= it_begin || it_end > total)
+    return fail(BPX_ERR_INVALID_ARG, "need 0 <= it_begin < it_end <= nburn + njumps");
+  if (it_begin > 0 && !state_in) return fail(BPX_ERR_INVALID_ARG, "a stretch that starts after iteration 0 needs state_in");
+  Stretch sp{it_begin, it_end, state_in, state_out, acc_in, acc_out};
+  return mcmc_run(opts, vol, params, tau, props_in, props_out, freeze_props, records, status, stream, &sp);
 }
 
 bpx_status bpx_mcmc_dev(const bpx_options* opts, const bpx_volume* vol, const float* params, const float* tau,

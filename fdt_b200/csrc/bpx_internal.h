@@ -86,6 +86,14 @@ struct McmcArgs {
   float* props_out;       // [6+3K][nvox] proposal widths after the last iteration, or NULL
   int freeze_props;       // 0: adapt (reference); 1: never adapt; 2: adapt during burn-in only
   const uint64_t* voxel_keys;  // [nvox] RNG voxel keys (packed batches), or NULL: voxel_offset + v
+  // a stretch of the chain: iterations [it_begin, it_end) (it_end 0: to the end), started from
+  // state_in [6+3K][nvox] (record rows) and acc_in [6+3K][nvox] when given; the state, acceptance
+  // counts since the last width update and widths at it_end go to state_out / acc_out / props_out
+  int it_begin, it_end;
+  const float* state_in;
+  float* state_out;
+  const int32_t* acc_in;
+  int32_t* acc_out;
 };
 
 struct EnergyArgs {

@@ -291,7 +291,9 @@ constexpr uint32_t slot_bits(int what) {
   return m;
 }
 
-template <int MODEL, int K, bool RIC, int TPV, int MPL>
+// STRETCH: compiled with the checkpoint/resume arguments of McmcArgs (it_begin/it_end, state and
+// acceptance counts in and out); without it the kernel runs the whole chain from the LM state.
+template <int MODEL, int K, bool RIC, int TPV, int MPL, bool STRETCH>
 __global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_kernel(McmcArgs a) {
   constexpr int NS = 6 + 3 * K;             // proposal slots
   constexpr int NR = (NS + TPV - 1) / TPV;  // Philox blocks per lane per iteration
@@ -405,27 +407,40 @@ __global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_ker
     for (int p = 0; p < NP; ++p) ywp[p * kMcmcThreads + tid] = make_float4(y2[p].x, y2[p].y, w2[p].x, w2[p].y);
     if (TAIL) ywt[tid] = make_float2(yt, wt);
 
-    // ---- init_Fibres_Multifibres (CUDA/runmcmc_kernels.cu:255-504) ----
-    const float* prm = a.params + (size_t)v * a.np_fit;
-    float S0 = prm[0];
-    float d = prm[1];
-    if (d < 0.f || d > kUpperDiff) d = 2e-3f;
-    float dstd = 0.f, R = 0.f;
-    if (MODEL >= 2) {
-      dstd = prm[2];
-      const float upper = MODEL == 3 ? 0.004f : 0.01f;
-      if (dstd < 0.f || dstd > upper) dstd = d / 10.f;
-      R = MODEL == 3 ? a.R_mean : 0.f;
+    // ---- init_Fibres_Multifibres (CUDA/runmcmc_kernels.cu:255-504), or a saved chain state ----
+    // (state_in rows as the records: d, f0, tau, d_std, R, S0, then th, ph, f per fibre)
+    const bool from_state = STRETCH && a.state_in != nullptr;
+    const float* prm = from_state ? nullptr : a.params + (size_t)v * a.np_fit;
+    auto srow = [&](int r) { return a.state_in[(size_t)r * a.nvox + v]; };
+    float S0, d, dstd = 0.f, R = 0.f, f0, tau;
+    if (from_state) {
+      S0 = srow(5);
+      d = srow(0);
+      if (MODEL >= 2) dstd = srow(3);
+      if (MODEL == 3) R = srow(4);
+      f0 = use_f0 ? srow(1) : 0.f;
+      tau = RIC ? srow(2) : 0.f;
+    } else {
+      S0 = prm[0];
+      d = prm[1];
+      if (d < 0.f || d > kUpperDiff) d = 2e-3f;
+      if (MODEL >= 2) {
+        dstd = prm[2];
+        const float upper = MODEL == 3 ? 0.004f : 0.01f;
+        if (dstd < 0.f || dstd > upper) dstd = d / 10.f;
+        R = MODEL == 3 ? a.R_mean : 0.f;
+      }
+      f0 = use_f0 ? prm[a.np_fit - 1] : 0.f;
+      tau = (RIC && a.tau) ? a.tau[v] : 0.f;
     }
-    float f0 = use_f0 ? prm[a.np_fit - 1] : 0.f;
-    float tau = (RIC && a.tau) ? a.tau[v] : 0.f;
     constexpr int add = MODEL >= 2 ? 1 : 0;
     float f[K];
     uint32_t lam = 0;  // ARD flag of fibre k in bit k
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      const float th0 = prm[2 + 3 * k + 1 + add], ph0 = prm[2 + 3 * k + 2 + add];
-      f[k] = prm[2 + 3 * k + add];
+      const float th0 = from_state ? srow(6 + 3 * k) : prm[2 + 3 * k + 1 + add];
+      const float ph0 = from_state ? srow(7 + 3 * k) : prm[2 + 3 * k + 2 + add];
+      f[k] = from_state ? srow(8 + 3 * k) : prm[2 + 3 * k + add];
       const bool lk = (k == 0) ? (a.all_ard != 0) : (a.no_ard == 0);
       lam |= lk ? 1u << k : 0u;
       float fp = 0.f;
@@ -569,13 +584,16 @@ __global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_ker
         if (q == kSlotR) pq = R / 10.f;
         if (a.props_in) pq = a.props_in[(size_t)q * a.nvox + v];
         sprop[q] = pq;
-        sacc[q] = 0;
+        sacc[q] = (STRETCH && a.acc_in) ? a.acc_in[(size_t)q * a.nvox + v] : 0;
       }
     }
     __syncwarp();
 
-    int sample = 0;
-    for (int it = 0; it < total; ++it) {
+    // iterations [it_begin, it_end) of the chain; samples recorded before it_begin keep their slots
+    const int it_begin = STRETCH ? a.it_begin : 0;
+    const int it_end = (STRETCH && a.it_end > 0) ? a.it_end : total;
+    int sample = it_begin > a.nburn ? min((it_begin - a.nburn) / a.sampleevery, ns) : 0;
+    for (int it = it_begin; it < it_end; ++it) {
       // this iteration's randoms: lane gl holds slots gl, gl+TPV, ...
       float rn[NR], rl[NR];
 #pragma unroll
@@ -818,6 +836,26 @@ __global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_ker
         __syncwarp();
       }
     }
+    if (STRETCH && valid && gl == 0 && a.state_out) {
+      const size_t n = a.nvox;
+      float* so = a.state_out + v;
+      so[0 * n] = d;
+      so[1 * n] = f0;
+      so[2 * n] = tau;
+      so[3 * n] = dstd;
+      so[4 * n] = R;
+      so[5 * n] = S0;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        so[(6 + 3 * k) * n] = fst[kFsTh * K + k];
+        so[(7 + 3 * k) * n] = fst[kFsPh * K + k];
+        so[(8 + 3 * k) * n] = f[k];
+      }
+    }
+    if (STRETCH && valid && gl == 0 && a.acc_out) {
+#pragma unroll
+      for (int q = 0; q < NS; ++q) a.acc_out[(size_t)q * a.nvox + v] = sacc[q];
+    }
     if (valid && gl == 0 && a.props_out) {
 #pragma unroll
       for (int q = 0; q < NS; ++q) a.props_out[(size_t)q * a.nvox + v] = sprop[q];
@@ -960,7 +998,8 @@ __global__ void __launch_bounds__(kMcmcThreads) energy_kernel(EnergyArgs a) {
 
 template <int MODEL, int K, bool RIC, int TPV, int MPL>
 cudaError_t launch_mcmc_t(const McmcArgs& a, cudaStream_t s) {
-  auto kern = mcmc_kernel<MODEL, K, RIC, TPV, MPL>;
+  const bool stretch = a.it_begin != 0 || a.it_end != 0 || a.state_in || a.state_out || a.acc_in || a.acc_out;
+  auto kern = stretch ? mcmc_kernel<MODEL, K, RIC, TPV, MPL, true> : mcmc_kernel<MODEL, K, RIC, TPV, MPL, false>;
   constexpr int NS = 6 + 3 * K, GPB = kMcmcThreads / TPV;
   constexpr int NP = MPL / 2;
   const size_t smem = (size_t)(a.gradnonlin ? GPB : 1) * TPV * MPL * sizeof(float4) +

@@ -41,6 +41,9 @@ _SIGS = {
     "bpx_xfibres_noalloc_dev": (C.c_int, [C.POINTER(Options), C.POINTER(Volume), C.POINTER(Outputs), C.c_void_p]),
     "bpx_mcmc_ex_dev": (C.c_int, [C.POINTER(Options), C.POINTER(Volume), C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "bpx_mcmc_stretch_dev": (C.c_int, [C.POINTER(Options), C.POINTER(Volume), C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "bpx_mlp_nin": (C.c_int32, [C.c_int32]),
     "bpx_mlp_nparams": (C.c_int64, [C.c_int32]),
     "bpx_mlp_features_dev": (C.c_int, [C.POINTER(Volume), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -165,6 +168,28 @@ def mcmc_ex(opts: Options, data, bvecs, bvals, params, tau=None, props_in=None, 
     _check(load().bpx_mcmc_ex_dev(C.byref(opts), C.byref(vol), _ptr(params), _ptr(tau), _ptr(props_in), _ptr(pout),
                                   int(freeze), _ptr(rec), _ptr(status), _stream(torch)), "bpx_mcmc_ex_dev")
     return rec, pout
+
+
+def mcmc_stretch(opts: Options, data, bvecs, bvals, it_begin: int, it_end: int, params=None, tau=None,
+                 state=None, records=None, voxel_offset: int = 0, freeze: int = 0):
+    """Iterations [it_begin, it_end) of the chain (bpx_mcmc_stretch_dev).  `state` is the previous
+    stretch's return value (a dict of state/props/acc tensors) or None to start from params/tau.
+    Returns (records, state at it_end); pass the same records tensor to every stretch of a chain."""
+    torch = _torch()
+    nvox = data.shape[0]
+    rows = 6 + 3 * opts.nfibres
+    if records is None:
+        records = torch.zeros((nrec(opts.nfibres), opts.nsamples, nvox), device="cuda", dtype=torch.float32)
+    out = {"state": torch.empty((rows, nvox), device="cuda", dtype=torch.float32),
+           "props": torch.empty((rows, nvox), device="cuda", dtype=torch.float32),
+           "acc": torch.empty((rows, nvox), device="cuda", dtype=torch.int32)}
+    vol = make_volume(data, bvecs, bvals, voxel_offset)
+    s_in = state or {}
+    _check(load().bpx_mcmc_stretch_dev(C.byref(opts), C.byref(vol), _ptr(params), _ptr(tau), _ptr(s_in.get("state")),
+                                       _ptr(s_in.get("props")), _ptr(s_in.get("acc")), int(it_begin), int(it_end),
+                                       int(freeze), _ptr(records), _ptr(out["state"]), _ptr(out["props"]),
+                                       _ptr(out["acc"]), None, _stream(torch)), "bpx_mcmc_stretch_dev")
+    return records, out
 
 
 def gemm_bf16(a, b, M: int, N: int, K: int, a_mn: bool = False, b_mn: bool = False):

@@ -252,6 +252,29 @@ bpx_status bpx_mcmc_ex_dev(const bpx_options* opts, const bpx_volume* vol, const
                            int32_t freeze_props, float* records, uint32_t* status, void* stream);
 
 /*
+ * A stretch of the chain, for checkpoint and resume (no counterpart in the reference, which
+ * restarts a part from its first iteration): iterations [it_begin, it_end) of the chain of
+ * opts->nburn + opts->njumps iterations.
+ *   state_in   [6+3*nfib][nvox] chain state at it_begin in the record rows (d, f0, tau, d_std, R,
+ *              S0, then th, ph, f per fibre); NULL = start from params/tau as bpx_mcmc_ex_dev
+ *              (required when it_begin > 0; params and tau are then not read).
+ *   props_in   widths as for bpx_mcmc_ex_dev; acc_in [6+3*nfib][nvox] acceptances since the last
+ *              width update (NULL = zeros).
+ *   records    [6+3*nfib][nsamples][nvox]: the samples recorded in the stretch are written at
+ *              their positions in the whole chain; the others are left as they are.
+ *   state_out, props_out, acc_out  the state, widths and acceptance counts at it_end (each may be
+ *              NULL).
+ * The RNG is keyed by the iteration and every signal, likelihood and prior is recomputed from
+ * the state, so consecutive stretches, each passed the previous one's state_out, props_out and
+ * acc_out, reproduce one call over the whole chain bit for bit.
+ */
+bpx_status bpx_mcmc_stretch_dev(const bpx_options* opts, const bpx_volume* vol, const float* params,
+                                const float* tau, const float* state_in, const float* props_in,
+                                const int32_t* acc_in, int32_t it_begin, int32_t it_end,
+                                int32_t freeze_props, float* records, float* state_out,
+                                float* props_out, int32_t* acc_out, uint32_t* status, void* stream);
+
+/*
  * ---- Learned initialiser (no counterpart in the reference) ----
  * A network nin -> 256 x 4 (GELU) -> 32 maps a voxel's signals, divided by the mean of its
  * b <= 50 s/mm^2 measurements (S0_hat) and zero-padded to nin = 8*ceil(ndir/8), to the MCMC's

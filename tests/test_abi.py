@@ -106,6 +106,17 @@ def test_host_argument_checks_reject_bad_input(libbpx):
     bad = Options.make(sampleevery=0)
     assert libbpx.bpx_finish_dev(C.byref(bad), 3, None, None, None) == abi.BPX_ERR_INVALID_ARG
     assert libbpx.bpx_prepare_data_dev(-1, 64, None, None) == abi.BPX_ERR_INVALID_ARG
+    # stretches of the chain: the iteration range, and a state when not starting at iteration 0
+    ok_s = Options.make(nburn=10, njumps=20)
+    st = libbpx.bpx_mcmc_stretch_dev
+    assert st(C.byref(ok_s), C.byref(vol), None, None, None, None, None, 0, 31, 0, None, None, None, None, None,
+              None) == abi.BPX_ERR_INVALID_ARG
+    assert b"it_begin" in libbpx.bpx_last_error()
+    assert st(C.byref(ok_s), C.byref(vol), None, None, None, None, None, 5, 5, 0, None, None, None, None, None,
+              None) == abi.BPX_ERR_INVALID_ARG
+    assert st(C.byref(ok_s), C.byref(vol), None, None, None, None, None, 5, 30, 0, None, None, None, None, None,
+              None) == abi.BPX_ERR_INVALID_ARG
+    assert b"state_in" in libbpx.bpx_last_error()
     # empty volumes are valid and do nothing
     vol.nvox = 0
     assert libbpx.bpx_fit_dev(C.byref(ok), C.byref(vol), None, None, None, None) == abi.BPX_OK
