@@ -20,6 +20,7 @@ BPX_ERR_BAD_DATA = 6
 BPX_VOX_NONFINITE_DATA = 1
 BPX_VOX_F0_REFIT = 2
 BPX_VOX_NONFINITE_ENERGY = 4
+BPX_VOX_LM_ITERATION_CAP = 8
 
 
 def nrec(nfib: int) -> int:

@@ -635,19 +635,19 @@ __device__ void normal_eqs(const Meas& ms, const Real (&p)[LmShape<KIND, K, F0>:
 // 2|dcf| <= 1e-8 (|cf_old|+|cf_new|+2e-16), stopped when lambda > 1e20 or after 200 successful
 // iterations (the iteration counter advances only on success).  Gradient 2 J^T r and Hessian
 // 2 J^T J come from normal_eqs after every successful step and stay in st between steps.
+// Returns false when the run stopped at the iteration cap (warp-uniform).
 template <int KIND, int K, bool F0>
-__device__ int lm_run(const Meas& ms, Real (&p)[LmShape<KIND, K, F0>::P], int lane, int gbo, Real R, Real invR,
+__device__ bool lm_run(const Meas& ms, Real (&p)[LmShape<KIND, K, F0>::P], int lane, int gbo, Real R, Real invR,
                       double* st) {
   constexpr int P = LmShape<KIND, K, F0>::P;
   double lambda = 0.1;
   const double cftol = 1.0e-8, ltol = 1.0e20;
   double pcf = cost<KIND, K, F0>(ms, p, lane, gbo, R, invR);
-  int niter = 0, iters = 0;
-  bool success = true;
+  int niter = 0;
+  bool success = true, stopped = false;
   double gsign = 1.0;  // PVM_multi's gradient S0 entry carries sign(S0) (CUDA/PVM_multi.cu:376)
   const int row = lane < P ? lane : 0;
   while (!(success && niter++ >= 200)) {
-    ++iters;
     if (success) {
       normal_eqs<KIND, K, F0>(ms, p, lane, gbo, R, invR, st);
       if (KIND == kMulti && lane == 0) gsign = pm1d(p[0]);
@@ -673,9 +673,12 @@ __device__ int lm_run(const Meas& ms, Real (&p)[LmShape<KIND, K, F0>::P], int la
       lambda *= 10.0;
       if (lambda > ltol) end = true;
     }
-    if (end) break;
+    if (end) {
+      stopped = true;
+      break;
+    }
   }
-  return iters;
+  return stopped;
 }
 
 // adjacent-swap sort of fibres by decreasing f (sort_PVM_*, CUDA/PVM_single.cu:86-104)
@@ -968,7 +971,8 @@ __device__ __forceinline__ Real predict_final(int model, const Real* q, int o, b
 // state in a flag word.  One warp per voxel; the warps of a block take voxels from a
 // shared-memory counter.
 // ------------------------------------------------------------------------------------------
-enum FitFlag : uint32_t { kFitBad = 1u, kFitRefit = 2u, kFitRefitted = 4u };
+// kFitCapped: the LM run that produced the voxel's current parameters stopped at its iteration cap
+enum FitFlag : uint32_t { kFitBad = 1u, kFitRefit = 2u, kFitRefitted = 4u, kFitCapped = 8u };
 
 struct VoxelMeas {
   Meas ms;
@@ -1024,16 +1028,16 @@ __device__ void stage_start(const FitArgs& a, int v, int lane, double* st) {
   if (a.model == 1 && !a.nonlin) {
     Real p[LmShape<kSingleC, K, F0>::P];
     start_single_c<K, F0>(dt, ms, lane, p);
-    lm_run<kSingleC, K, F0>(ms, p, lane, 0, R, invR, st);
+    if (!lm_run<kSingleC, K, F0>(ms, p, lane, 0, R, invR, st)) flag = kFitCapped;
     finalise<kSingleC, K, F0>(p);
-    if (F0 && needs_refit(p, 2)) flag = kFitRefit;
+    if (F0 && needs_refit(p, 2)) flag |= kFitRefit;
     store_res(res, p, lane);
   } else {
     Real p[LmShape<kSingle, K, F0>::P];
     start_single<K, F0>(dt, p);
-    lm_run<kSingle, K, F0>(ms, p, lane, 0, R, invR, st);
+    if (!lm_run<kSingle, K, F0>(ms, p, lane, 0, R, invR, st)) flag = kFitCapped;
     finalise<kSingle, K, F0>(p);
-    if (a.model == 1 && F0 && needs_refit(p, 2)) flag = kFitRefit;
+    if (a.model == 1 && F0 && needs_refit(p, 2)) flag |= kFitRefit;
     store_res(res, p, lane);
   }
   if (lane == 0) a.flags[v] = flag;
@@ -1049,10 +1053,14 @@ __device__ void stage_multi(const FitArgs& a, int v, int lane, double* st) {
   load_res(res, s);
   Real p[LmShape<kMulti, K, F0>::P];
   start_multi<K, F0>(s, p);
-  lm_run<kMulti, K, F0>(vm.ms, p, lane, a.model == 3 ? 2 : 0, R, invR, st);
+  const bool conv = lm_run<kMulti, K, F0>(vm.ms, p, lane, a.model == 3 ? 2 : 0, R, invR, st);
   finalise<kMulti, K, F0>(p);
   store_res(res, p, lane);
-  if (lane == 0 && F0 && needs_refit(p, 3)) a.flags[v] = kFitRefit;
+  if (lane == 0) {
+    uint32_t fl = (a.flags[v] & ~kFitCapped) | (conv ? 0u : kFitCapped);
+    if (F0 && needs_refit(p, 3)) fl |= kFitRefit;
+    a.flags[v] = fl;
+  }
 }
 
 // re-fit without f0 (f0 := 0.001): model 1 with the same start as A; models 2 and 3 through
@@ -1066,18 +1074,19 @@ __device__ void stage_refit(const FitArgs& a, int v, int lane, double* st) {
   double* res = a.scratch + (size_t)v * 16;
   Dti dt;
   dti_fit(ms, lane, dt);
+  bool conv;
   if (a.model == 1) {
     constexpr int NPOUT = 2 + 3 * K + 1;
     if (a.nonlin) {
       Real p[LmShape<kSingle, K, false>::P];
       start_single<K, false>(dt, p);
-      lm_run<kSingle, K, false>(ms, p, lane, 0, R, invR, st);
+      conv = lm_run<kSingle, K, false>(ms, p, lane, 0, R, invR, st);
       finalise<kSingle, K, false>(p);
       store_res(res, p, lane);
     } else {
       Real p[LmShape<kSingleC, K, false>::P];
       start_single_c<K, false>(dt, ms, lane, p);
-      lm_run<kSingleC, K, false>(ms, p, lane, 0, R, invR, st);
+      conv = lm_run<kSingleC, K, false>(ms, p, lane, 0, R, invR, st);
       finalise<kSingleC, K, false>(p);
       store_res(res, p, lane);
     }
@@ -1090,13 +1099,13 @@ __device__ void stage_refit(const FitArgs& a, int v, int lane, double* st) {
     finalise<kSingleC, K, false>(c);
     Real p[LmShape<kMulti, K, false>::P];
     start_multi<K, false>(c, p);
-    lm_run<kMulti, K, false>(ms, p, lane, a.model == 3 ? 2 : 0, R, invR, st);
+    conv = lm_run<kMulti, K, false>(ms, p, lane, a.model == 3 ? 2 : 0, R, invR, st);
     finalise<kMulti, K, false>(p);
     store_res(res, p, lane);
     if (lane == 0) res[NPM - 1] = 0.001;
   }
   __syncwarp();
-  if (lane == 0) a.flags[v] = kFitRefitted;
+  if (lane == 0) a.flags[v] = kFitRefitted | (conv ? 0u : kFitCapped);
 }
 
 // tau = 1 / var(y - prediction) (sample variance, n-1) and the FP32 outputs
@@ -1140,7 +1149,8 @@ __device__ void stage_finish(const FitArgs& a, int v, int lane, double*) {
     a.tau[v] = 0.f;
   }
   if (lane < npo) out[lane] = (float)res[lane];
-  if (lane == 0 && a.status) a.status[v] = refit ? BPX_VOX_F0_REFIT : 0u;
+  if (lane == 0 && a.status)
+    a.status[v] = (refit ? BPX_VOX_F0_REFIT : 0u) | ((flag & kFitCapped) ? BPX_VOX_LM_ITERATION_CAP : 0u);
 }
 
 // Each block owns kFitVoxPerBlock consecutive voxels; its warps take the next one from a

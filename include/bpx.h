@@ -59,6 +59,8 @@ typedef enum bpx_status {
 #define BPX_VOX_NONFINITE_DATA 1u  /* data held NaN/Inf: voxel skipped, outputs zero */
 #define BPX_VOX_F0_REFIT 2u        /* the f0 plausibility rule re-fitted this voxel without f0 */
 #define BPX_VOX_NONFINITE_ENERGY 4u /* the chain met a non-finite energy */
+#define BPX_VOX_LM_ITERATION_CAP 8u /* the LM fit that gave the start stopped at its 200-iteration cap,
+                                       not at the cost tolerance */
 
 /*
  * The xfibresOptions fields that act on the per-voxel path (xfibresoptions.h:104-149).

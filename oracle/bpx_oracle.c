@@ -611,12 +611,14 @@ static void lm_gradhess(const lmctx* c, const double* p, double* g, double* H) {
 }
 
 /* levenberg_marquardt_*_gpu (CUDA/levenberg_marquardt.cu:17-122): lambda0 0.1, x/÷10,
- * cftol 1e-8, ltol 1e20, at most 200 successful iterations. */
-static int lm_run(const lmctx* c, double* p) {
+ * cftol 1e-8, ltol 1e20, at most 200 successful iterations.  *capped (if given) is set when the
+ * run stopped at that cap instead of at the cost tolerance or the lambda limit. */
+static int lm_run(const lmctx* c, double* p, int* capped) {
   int np = c->np, niter = 0, maxiter = 200, success = 1, iters = 0;
   double lambda = 0.1, cftol = 1e-8, ltol = 1e20;
   double pcf = lm_cf(c, p), ncf;
   double g[MAXP], H[MAXP * MAXP], Hd[MAXP * MAXP], st[MAXP], step[MAXP];
+  int stopped = 0;
   while (!(success && niter++ >= maxiter)) {
     ++iters;
     if (success) lm_gradhess(c, p, g, H);
@@ -636,8 +638,12 @@ static int lm_run(const lmctx* c, double* p) {
       lambda *= 10.0;
       if (lambda > ltol) end = 1;
     }
-    if (end) break;
+    if (end) {
+      stopped = 1;
+      break;
+    }
   }
+  if (capped) *capped = !stopped;
   return iters;
 }
 
@@ -863,7 +869,7 @@ int orc_lm_start(int kind, int nfib, int f0, int ndir, const float* y, const flo
 
 /* fit one model from start values; returns finalised params */
 static int fit_model(int kind, int nfib, int f0, int gbo, double R, int ndir, const float* y,
-                     const float* bvecs, const float* bvals, const double* start, double* out) {
+                     const float* bvecs, const float* bvals, const double* start, double* out, int* capped) {
   lmctx c;
   lm_ctx_init(&c, kind, nfib, f0, gbo, R, ndir, y, bvecs, bvals);
   double p[MAXP];
@@ -881,7 +887,7 @@ static int fit_model(int kind, int nfib, int f0, int gbo, double R, int ndir, co
   } else {
     memcpy(p, start, sizeof(double) * c.np);
   }
-  int it = lm_run(&c, p);
+  int it = lm_run(&c, p, capped);
   lm_finalise(&c, p);
   memcpy(out, p, sizeof(double) * c.np);
   return it;
@@ -891,7 +897,7 @@ int orc_lm_fit(int kind, int nfib, int f0, int gamma_ball_only, double R, int nd
                const float* y, const float* bvecs, const float* bvals, const double* start,
                double* final_params) {
   return fit_model(kind, nfib, f0, gamma_ball_only, R, ndir, y, bvecs, bvals, start,
-                   final_params);
+                   final_params, NULL);
 }
 
 /* predicted signal from finalised params [S0, d, (dstd), (f,th,ph)*K, (f0)], as the
@@ -965,14 +971,14 @@ static void fit_voxel(const bpx_options* o, int ndir, const float* y, const floa
   dti_t dt;
   dti_for(w, y, bvecs, bvals, own_amat, &dt);
   double st[MAXP], out[MAXP];
-  int refit = 0;
+  int refit = 0, capped = 0; /* capped: the LM run that produced the final parameters hit its cap */
   if (model == 1) {
     int kind = o->nonlin ? KIND_SINGLE : KIND_SINGLE_C;
     if (kind == KIND_SINGLE)
       start_single(K, f0, &dt, st);
     else
       start_single_c(K, f0, &dt, ndir, y, bvecs, bvals, st);
-    fit_model(kind, K, f0, 0, R, ndir, y, bvecs, bvals, st, out);
+    fit_model(kind, K, f0, 0, R, ndir, y, bvecs, bvals, st, out, &capped);
     if (f0) {
       double md = out[1], mf = out[2], f0v = out[np - 1];
       if ((K > 0 && mf < 0.05) || md > 0.007 || f0v > 0.4) {
@@ -981,7 +987,7 @@ static void fit_voxel(const bpx_options* o, int ndir, const float* y, const floa
           start_single(K, 0, &dt, st2);
         else
           start_single_c(K, 0, &dt, ndir, y, bvecs, bvals, st2);
-        fit_model(kind, K, 0, 0, R, ndir, y, bvecs, bvals, st2, out2);
+        fit_model(kind, K, 0, 0, R, ndir, y, bvecs, bvals, st2, out2, &capped);
         memcpy(out, out2, sizeof(double) * (np - 1));
         out[np - 1] = 0.001; /* mix_params, CUDA/xfibres_gpu.cu:571 */
         refit = 1;
@@ -990,8 +996,8 @@ static void fit_voxel(const bpx_options* o, int ndir, const float* y, const floa
   } else {
     double s1[MAXP];
     start_single(K, f0, &dt, st);
-    fit_model(KIND_SINGLE, K, f0, 0, R, ndir, y, bvecs, bvals, st, s1);
-    fit_model(KIND_MULTI, K, f0, gbo, R, ndir, y, bvecs, bvals, s1, out);
+    fit_model(KIND_SINGLE, K, f0, 0, R, ndir, y, bvecs, bvals, st, s1, NULL);
+    fit_model(KIND_MULTI, K, f0, gbo, R, ndir, y, bvecs, bvals, s1, out, &capped);
     if (f0) {
       double md = out[1], mf = out[3], f0v = out[np - 1];
       if ((K > 0 && mf < 0.05) || md > 0.007 || f0v > 0.4) {
@@ -999,8 +1005,8 @@ static void fit_voxel(const bpx_options* o, int ndir, const float* y, const floa
          * the CPU path re-fits PVM_multi from PVM_single (xfibres.cc:681-693) instead */
         double st2[MAXP], c1[MAXP], out2[MAXP];
         start_single_c(K, 0, &dt, ndir, y, bvecs, bvals, st2);
-        fit_model(KIND_SINGLE_C, K, 0, 0, R, ndir, y, bvecs, bvals, st2, c1);
-        fit_model(KIND_MULTI, K, 0, gbo, R, ndir, y, bvecs, bvals, c1, out2);
+        fit_model(KIND_SINGLE_C, K, 0, 0, R, ndir, y, bvecs, bvals, st2, c1, NULL);
+        fit_model(KIND_MULTI, K, 0, gbo, R, ndir, y, bvecs, bvals, c1, out2, &capped);
         memcpy(out, out2, sizeof(double) * (np - 1));
         out[np - 1] = 0.001;
         refit = 1;
@@ -1009,6 +1015,7 @@ static void fit_voxel(const bpx_options* o, int ndir, const float* y, const floa
   }
   memcpy(params, out, sizeof(double) * np);
   if (status && refit) *status |= BPX_VOX_F0_REFIT;
+  if (status && capped) *status |= BPX_VOX_LM_ITERATION_CAP;
   if (o->rician && tau) {
     /* tau = 1/var(y - prediction), sample variance with n-1 (CUDA/diffmodels.cu:334-341) */
     int use_f0 = f0 && !refit;

@@ -90,6 +90,10 @@ def test_fit_parity(torch, lib, oracle, name, kw, protname, snr):
     ok = _fit_agreement(o, pg, po)
     # the f0 re-fit decision must agree wherever the fits agree
     assert np.all((((sg & 2) != 0) == ((so & 2) != 0))[ok])
+    # so must the iteration-cap flag of the final LM run, up to runs that end within a few
+    # iterations of the cap on one side and just past it on the other
+    cap_g, cap_o = (sg & 8) != 0, (so & 8) != 0
+    assert np.mean((cap_g == cap_o)[ok]) >= 0.9, (cap_g.mean(), cap_o.mean())
     assert ok.mean() >= 0.95, f"{name}: only {ok.mean():.3f} of voxels agree"
     if o.rician:
         rt = np.abs(tg - to) / to
