@@ -74,8 +74,13 @@ def read(path: str) -> tuple[np.ndarray, Header]:
     if not 1 <= nd <= 7:
         raise ValueError(f"{path}: bad dim[0] = {nd}")
     shape = tuple(int(d) for d in dim[1 : nd + 1])
+    if any(d < 1 for d in shape):
+        raise ValueError(f"{path}: bad dimensions {shape}")
     dt = np.dtype(_DTYPES[datatype]).newbyteorder(endian)
     count = int(np.prod(shape))
+    if vox_offset < HDR_SIZE or vox_offset + count * dt.itemsize > len(raw):
+        raise ValueError(f"{path}: truncated: {count} voxels of {dt.itemsize} bytes from offset {vox_offset} "
+                         f"need {vox_offset + count * dt.itemsize} bytes, the file has {len(raw)}")
     data = np.frombuffer(raw, dtype=dt, count=count, offset=vox_offset).reshape(shape, order="F")
     if slope != 0.0 and not (slope == 1.0 and inter == 0.0):
         data = data.astype(np.float32) * np.float32(slope) + np.float32(inter)
