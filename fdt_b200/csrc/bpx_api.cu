@@ -275,6 +275,7 @@ int32_t bpx_mcmc_layouts(int32_t* tpv, int32_t* mpl, int32_t max) {
 }
 
 bpx_status bpx_prepare_data_dev(int32_t nvox, int32_t ndir, float* data, void* stream) {
+  NvtxRange nvtx_range("bpx.prepare");
   if (nvox < 0 || ndir < 1 || (nvox > 0 && !data)) return fail(BPX_ERR_INVALID_ARG, "bad arguments to bpx_prepare_data_dev");
   if (nvox == 0) return BPX_OK;
   bpx_status st = check_device();
@@ -316,6 +317,7 @@ bpx_status fit_validate(const bpx_options* opts, const bpx_volume* vol, const fl
 
 bpx_status fit_dev_scratch(const bpx_options* opts, const bpx_volume* vol, float* params, float* tau, uint32_t* status,
                            void* scratch, void* stream) {
+  NvtxRange nvtx_range("bpx.fit");
   bpx_status st = fit_validate(opts, vol, params, tau);
   if (st != BPX_OK || vol->nvox == 0) return st;
   if (!scratch) return fail(BPX_ERR_INVALID_ARG, "fit stage scratch is NULL");
@@ -372,6 +374,7 @@ struct Stretch {
 bpx_status mcmc_run(const bpx_options* opts, const bpx_volume* vol, const float* params, const float* tau,
                     const float* props_in, float* props_out, int32_t freeze_props, float* records,
                     uint32_t* status, void* stream, const Stretch* sp) {
+  NvtxRange nvtx_range("bpx.mcmc");
   bpx_status st = check_opts(opts);
   if (st == BPX_OK) st = check_vol(vol, true);
   if (st != BPX_OK) return st;
@@ -459,6 +462,7 @@ bpx_status bpx_mcmc_dev(const bpx_options* opts, const bpx_volume* vol, const fl
 }
 
 bpx_status bpx_finish_dev(const bpx_options* opts, int32_t nvox, const float* records, bpx_outputs* out, void* stream) {
+  NvtxRange nvtx_range("bpx.finish");
   bpx_status st = check_opts(opts);
   if (st != BPX_OK) return st;
   if (nvox < 0 || !out) return fail(BPX_ERR_INVALID_ARG, "bad arguments to bpx_finish_dev");
@@ -480,6 +484,7 @@ bpx_status bpx_finish_dev(const bpx_options* opts, int32_t nvox, const float* re
 
 bpx_status bpx_postproc_dev(const bpx_options* opts, int32_t nvox, const bpx_outputs* out, float thr,
                             bpx_postproc* post, void* stream) {
+  NvtxRange nvtx_range("bpx.postproc");
   bpx_status st = check_opts(opts);
   if (st != BPX_OK) return st;
   if (nvox < 0 || !out || !post) return fail(BPX_ERR_INVALID_ARG, "bad arguments to bpx_postproc_dev");
@@ -536,6 +541,7 @@ bpx_status bpx_energy_dev(const bpx_options* opts, const bpx_volume* vol, const 
 }
 
 bpx_status bpx_xfibres_dev(const bpx_options* opts, const bpx_volume* vol, bpx_outputs* out, void* stream) {
+  NvtxRange nvtx_range("bpx.xfibres");
   bpx_status st = check_opts(opts);
   if (st == BPX_OK) st = check_vol(vol, true);
   if (st != BPX_OK) return st;
@@ -690,6 +696,7 @@ bpx_status xfibres_host_impl(const bpx_options* opts, const bpx_volume* vol, bpx
 extern "C" {
 
 bpx_status bpx_xfibres_host(const bpx_options* opts, const bpx_volume* vol, bpx_outputs* host_out) {
+  NvtxRange nvtx_range("bpx.xfibres_host");
   return xfibres_host_impl(opts, vol, host_out, nullptr, 0);
 }
 

@@ -566,6 +566,7 @@ bpx_status bpx_batch_create(const bpx_options* opts, const bpx_item* items, int3
 }
 
 bpx_status bpx_batch_run(bpx_batch* b, void* stream) {
+  NvtxRange nvtx_range("bpx.batch_run");
   if (!b || !b->exec) return api_fail(BPX_ERR_INVALID_ARG, "bpx_batch_run: no batch");
   BAT_CUDA(cudaGraphLaunch(b->exec, (cudaStream_t)stream));
   return BPX_OK;

@@ -4,10 +4,20 @@
 #include <cstdint>
 #include <string>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "bpx.h"
 
 namespace bpx {
+
+// Names a host-side stage for profilers (Nsight Systems shows the range and the kernels launched
+// inside it); NVTX v3 is header-only and costs a few instructions when no tool is attached.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 constexpr int kFitThreads = 128;   // 4 warps, one voxel per warp at a time
 constexpr int kFitVoxPerBlock = 32;  // voxels a fit block shares out among its warps

@@ -439,6 +439,7 @@ size_t mlp_weight_elems(int ndir) { return geom(ndir).nw; }
 
 bpx_status mlp_forward_buffers(int ndir, const float* params, int nvox, const uint16_t* x, float* out, uint16_t* wbf,
                                uint16_t* buf0, uint16_t* buf1, int chunk_rows, cudaStream_t s) {
+  NvtxRange nvtx_range("bpx.network");
   const Geom G = geom(ndir);
   int* err = nullptr;
   bpx_status st = error_word(&err);
@@ -635,6 +636,7 @@ bpx_status bpx_mlp_decode_dev(const bpx_options* opts, int32_t nvox, const float
 
 bpx_status bpx_xfibres_learned_dev(const bpx_options* opts, const bpx_volume* vol, const float* mlp_params,
                                    int32_t freeze_props, bpx_outputs* out, void* stream) {
+  NvtxRange nvtx_range("bpx.xfibres_learned");
   bpx_status st = api_check_opts(opts);
   if (st == BPX_OK) st = api_check_vol(vol);
   if (st != BPX_OK) return st;
