@@ -13,8 +13,13 @@
  * Functions named *_dev take DEVICE pointers and a cudaStream_t passed as void*; they are
  * asynchronous with respect to the host unless stated.  bpx_xfibres_host takes HOST pointers
  * and is synchronous.  Options are passed explicitly (the reference reads a process-wide
- * xfibresOptions singleton), so calls with different options may run concurrently on
- * different streams.
+ * xfibresOptions singleton).  Concurrency: the stage entries that take all their buffers from
+ * the caller (bpx_mcmc_*, bpx_finish_dev, bpx_postproc_dev, bpx_prepare_data_dev,
+ * bpx_gemm_bf16_dev) may run concurrently on different streams.  The entries that use the
+ * library's per-device workspace (bpx_fit_dev, bpx_xfibres_dev/_host, bpx_xfibres_learned_*,
+ * bpx_mlp_forward_dev, bpx_mlp_train_step_dev) share it between all callers on a device: issue
+ * them on one stream, or make a stream wait for the previous such call's work before the next
+ * call.  A bpx_batch owns its buffers; different batches may run concurrently.
  *
  * Array layouts (row-major, C order):
  *   data      [nvox][ndir]                 (voxel-major; CUDA/xfibres_gpu.cu:390-399)
@@ -167,7 +172,8 @@ bpx_status bpx_finish_dev(const bpx_options* opts, int32_t nvox, const float* re
 /*
  * Whole pipeline on device buffers: prepare (rician) -> fit -> mcmc -> finish, for one volume.
  * `data` is modified in place under --rician.  Workspace comes from a per-device cache
- * owned by the library (grown on demand, freed by bpx_release_workspace).
+ * owned by the library (grown on demand, freed by bpx_release_workspace) and shared by every
+ * workspace-using call on the device: see Concurrency above.
  */
 bpx_status bpx_xfibres_dev(const bpx_options* opts, const bpx_volume* vol, bpx_outputs* out,
                            void* stream);
