@@ -566,7 +566,6 @@ bpx_status bpx_xfibres_dev(const bpx_options* opts, const bpx_volume* vol, bpx_o
   float* tau = (float*)(p + b_params);
   float* rec = (float*)(p + b_params + b_tau);
   uint32_t* status = out->status ? out->status : (uint32_t*)(p + b_params + b_tau + b_rec);
-  cudaStream_t s = (cudaStream_t)stream;
   if (opts->rician) {
     st = bpx_prepare_data_dev(vol->nvox, vol->ndir, const_cast<float*>(vol->data), stream);
     if (st != BPX_OK) return st;
@@ -576,9 +575,7 @@ bpx_status bpx_xfibres_dev(const bpx_options* opts, const bpx_volume* vol, bpx_o
   st = bpx_mcmc_dev(opts, vol, params, tau, rec, status, stream);
   if (st != BPX_OK) return st;
   st = bpx_finish_dev(opts, vol->nvox, rec, out, stream);
-  if (st != BPX_OK) return st;
-  (void)s;
-  return BPX_OK;
+  return st;
 }
 
 }  // extern "C"
