@@ -593,7 +593,7 @@ def main():
         "frac": canon["frac"],
         "traffic": MCMC_DRAM_BYTES_PER_VOXEL * chunk if (o.model, o.nfibres, M, o.nsamples) == (2, 3, 288, 50) else None,
         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one mcmc_kernel launch "
-                          "(131072 voxels, this workload), scaled by voxels (profiles/mcmc_kernel_model2_k3_rician.md)",
+                          "on this workload's options, per voxel, scaled by the voxels of this launch",
         "kernel": f"mcmc_kernel (burn-in + recording), timed in the {rf} form's step",
         "counts": "canonical per-term counts (model-2 signal rcp+log2+exp2, Rician log2+rsqrt; FMA 6 per signal "
                   "term, K+4(+12 Rician) per likelihood term)",

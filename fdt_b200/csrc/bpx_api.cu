@@ -9,6 +9,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+
 #include "bpx.h"
 #include "bpx_device.cuh"
 #include "bpx_internal.h"
@@ -83,6 +85,7 @@ bpx_status check_vol(const bpx_volume* v, bool need_data) {
 struct Workspace {
   void* ptr = nullptr;
   size_t cap = 0;
+  uint64_t ctx = 0;  // context_id() the buffer was allocated in
 };
 std::mutex g_ws_mutex;
 Workspace g_ws[kWorkspaceSlots][kMaxDevices];
@@ -93,12 +96,17 @@ bpx_status workspace(size_t bytes, void** out, int slot = kWsPipeline) {
   BPX_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lk(g_ws_mutex);
   Workspace& w = g_ws[slot][dev % kMaxDevices];
+  if (w.ptr && w.ctx != context_id()) {  // allocated in a context that no longer exists: forget it
+    w.ptr = nullptr;
+    w.cap = 0;
+  }
   if (w.cap < bytes) {
     if (w.ptr) BPX_CUDA(cudaFree(w.ptr));
     w.ptr = nullptr;
     w.cap = 0;
     BPX_CUDA(cudaMalloc(&w.ptr, bytes));
     w.cap = bytes;
+    w.ctx = context_id();
   }
   *out = w.ptr;
   return BPX_OK;
@@ -120,6 +128,31 @@ bpx_status api_check_device() { return check_device(); }
 bpx_status api_check_opts(const bpx_options* o) { return check_opts(o); }
 bpx_status api_check_vol(const bpx_volume* v) { return check_vol(v, true); }
 bpx_status api_workspace(int slot, size_t bytes, void** out) { return workspace(bytes, out, slot); }
+
+uint64_t context_id() {
+  typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+  typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+  static std::once_flag once;
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(p);
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(p);
+  });
+  if (!get_current || !get_id) return 0;
+  CUcontext c = nullptr;
+  if (get_current(&c) != CUDA_SUCCESS || !c) return 0;
+  unsigned long long id = 0;
+  if (get_id(c, &id) != CUDA_SUCCESS) return 0;
+  return (uint64_t)id;
+}
 
 int sm_count() {
   int dev = 0;
@@ -745,7 +778,7 @@ bpx_status bpx_release_workspace(void) {
   std::lock_guard<std::mutex> lk(g_ws_mutex);
   for (int slot = 0; slot < kWorkspaceSlots; ++slot) {
     Workspace& w = g_ws[slot][dev % kMaxDevices];
-    if (w.ptr) BPX_CUDA(cudaFree(w.ptr));
+    if (w.ptr && w.ctx == context_id()) BPX_CUDA(cudaFree(w.ptr));
     w.ptr = nullptr;
     w.cap = 0;
   }

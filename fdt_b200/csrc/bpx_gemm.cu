@@ -25,6 +25,7 @@
 #include <mutex>
 
 #include "bpx_gemm.h"
+#include "bpx_internal.h"
 
 namespace bpx {
 namespace gemm {
@@ -263,6 +264,27 @@ static bool make_map(CUtensorMap* m, const uint16_t* ptr, int rows, int cols, in
 
 size_t smem_bytes(int ntile) { return 2 * (size_t)(kTileM * kChunkK * 2 + ntile * kChunkK * 2) + 1024 + sizeof(Smem) + 64; }
 
+// The kernel's dynamic shared-memory limit is raised once per device to what the widest tile
+// (256 columns) needs, and never lowered: a launch with a narrower tile needs less, and a CUDA graph
+// whose nodes were captured with different tile widths stays launchable whatever was set last.
+// (Setting the limit per launch to that launch's own need left it at the last layer's 42 KB after a
+// forward pass, below the 99 KB of the hidden layers' nodes.)
+constexpr int kMaxDevices = 64;
+cudaError_t set_smem_limit_once() {
+  static std::mutex mu;
+  static uint64_t done_ctx[kMaxDevices] = {0};  // context_id() the limit was set in (0: not set)
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(mu);
+  const uint64_t ctx = context_id();
+  if (ctx != 0 && done_ctx[dev] == ctx) return cudaSuccess;
+  e = cudaFuncSetAttribute(gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(256));
+  if (e == cudaSuccess) done_ctx[dev] = context_id();
+  return e;
+}
+
 const char* check(const GemmOperands& op, const GemmArgs& g) {
   if (g.M < 1 || g.N < 1 || g.K < 1) return "GEMM sizes must be positive";
   if (g.ntile != 32 && g.ntile != 64 && g.ntile != 128 && g.ntile != 256) return "GEMM tile width must be 32, 64, 128 or 256";
@@ -287,7 +309,7 @@ cudaError_t launch(const GemmOperands& op, const GemmArgs& g, cudaStream_t s, co
     return cudaErrorInvalidValue;
   }
   const size_t sm = smem_bytes(g.ntile);
-  const cudaError_t attr = cudaFuncSetAttribute(gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  const cudaError_t attr = set_smem_limit_once();
   if (attr != cudaSuccess) return attr;
   const dim3 grid((g.M + kTileM - 1) / kTileM, (g.N + g.ntile - 1) / g.ntile);
   gemm_kernel<<<grid, kThreads, sm, s>>>(ma, mb, g);

@@ -39,6 +39,11 @@ constexpr int mcmc_min_blocks() {
 }
 
 int sm_count();  // multiprocessors of the current device (cached per device)
+// Unique id of the CUDA context current on this thread (cuCtxGetId), 0 if none is current or the
+// driver lacks the call.  Per-device caches of device addresses (workspaces, the error word, the
+// allocation-free array) store it and treat a different id as a new context (after
+// cudaDeviceReset the old addresses are gone and must be neither used nor freed).
+uint64_t context_id();
 void set_last_error(const char* msg);  // message returned by bpx_last_error() on this thread
 
 // C-ABI helpers shared by the entry-point files (bpx_api.cu): status with message, device and

@@ -16,6 +16,8 @@
 // 15 f0*10, 16 ln(tau*S0_hat^2), 17.. ln of the normalised proposal width of MCMC slot q, in [-14, 2]
 // (q = 0..5+3K in the slot order f0, tau, d, d_std, R, S0, (th, ph, f)_k; widths of S0 are
 // divided by S0_hat, of d and d_std multiplied by 1e3, of tau divided by tau).
+#include <mutex>
+
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -376,15 +378,20 @@ bpx_status run_gemm(const uint16_t* a, int lda, int a_mn, const uint16_t* b, int
 }
 
 // per-device error word the GEMM's bounded waits write; read by bpx_mlp_poll_error
+std::mutex g_err_mutex;
 int* g_err[64] = {nullptr};
+uint64_t g_err_ctx[64] = {0};  // context_id() the word was allocated in
 
 bpx_status error_word(int** out) {
   int dev = 0;
   MLP_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return api_fail(BPX_ERR_NO_DEVICE, "device index out of range");
+  std::lock_guard<std::mutex> lk(g_err_mutex);
+  if (g_err[dev] && g_err_ctx[dev] != context_id()) g_err[dev] = nullptr;  // its context is gone
   if (!g_err[dev]) {
     MLP_CUDA(cudaMalloc(&g_err[dev], sizeof(int)));
     MLP_CUDA(cudaMemset(g_err[dev], 0, sizeof(int)));
+    g_err_ctx[dev] = context_id();
   }
   *out = g_err[dev];
   return BPX_OK;

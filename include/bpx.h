@@ -235,7 +235,11 @@ bpx_status bpx_measure_pipes(double* mufu_ops_per_s, double* fma_ops_per_s);
  * rician, 50 samples) that is 13,100 voxels, more than one 12,800-voxel subpart of xfibres_gpu.
  *
  * The first call on a device resolves the array's device address (cudaGetSymbolAddress, with that
- * device current); make that first call before any stream capture.  All calls share the one array
+ * device current); that is also when the CUDA runtime loads the array's module and takes its device
+ * memory.  Make that first call at start-up -- a call with vol->nvox == 0 does it and nothing else --
+ * before reserving a memory pool and before any stream capture.  The address is resolved again in a
+ * new context (after cudaDeviceReset).  Arguments are checked before anything runs, as by
+ * bpx_xfibres_dev; a rejected call leaves `data` untouched.  All calls share the one array
  * and it keeps the last call's contents; every element a call reads it has written first, so no
  * clearing is needed, but calls that overlap on the GPU (different streams, or threads) race on
  * the array and must be serialised by the caller.  Inputs and outputs are caller-owned device
