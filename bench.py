@@ -240,15 +240,17 @@ def batched_workload(scale: float, seed: int = 31):
     return items
 
 
-def run_batched(args):
-    """Times the batched form (one graph launch over all volumes) against the same items run one
-    after another through bpx_xfibres_dev with the default layouts."""
+def batched_record(scale: float, steps: int, warmup: int) -> dict:
+    """Times the batched form (one graph launch over all volumes of config C2 at voxel-count scale
+    `scale`) against the same items run one after another through bpx_xfibres_dev with the default
+    layouts.  Returns the measurement as a dict (the --workload batched line, or the C2 sub-record
+    of the default line)."""
     import torch
 
     from fdt_b200 import lib
 
     o = whole_brain_options()
-    items = batched_workload(args.batch_scale)
+    items = batched_workload(scale)
     protos = {}
     dev_items = []
     for it in items:
@@ -273,12 +275,12 @@ def run_batched(args):
         torch.cuda.synchronize()
         return sum(e0.elapsed_time(e1) for e0, e1 in evs) / 1e3 / k
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         batch.run()
     torch.cuda.synchronize()
     clocks = ClockSampler(0)
     clocks.start()
-    t_batch = timed(batch.run, args.steps)
+    t_batch = timed(batch.run, steps)
     ck = clocks.stop()
     work = [torch.empty_like(d["data"]) for d in dev_items]
     outs = []
@@ -297,19 +299,192 @@ def run_batched(args):
     t_seq = timed(sequential, 1)
     line = {
         "metric": "voxels/s, batched form (16 mixed volumes in one CUDA-graph launch)", "value": nvox / t_batch,
-        "unit": "voxels/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_batch,
+        "unit": "voxels/s", "n_gpus": 1, "steps": steps, "warmup": warmup, "ms_per_step": 1e3 * t_batch,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
         "config": {"workload": "C2 batch: 16 volumes, voxels log-uniform in [5k, 300k] x %g, ndir from "
                    "{33, 65, 129, 279}, models 1/2 per volume, 1..3 fibres per voxel, SNR U(10,40); "
-                   "rician+f0+ardf0, burnin 1000, njumps 1250" % args.batch_scale,
-                   "voxels": nvox, "items": len(items), "l2": "inputs larger than L2"},
+                   "rician+f0+ardf0, burnin 1000, njumps 1250" % scale,
+                   "scale": scale, "voxels": nvox, "items": len(items), "l2": "inputs larger than L2"},
         "sequential_per_item": {"value": nvox / t_seq, "unit": "voxels/s", "launches": 4 * len(items)},
         "batched_over_sequential": t_seq / t_batch,
         "buckets": batch.buckets(), "create_s": t_create,
         "gpu_launches": 1, "clocks": ck,
     }
-    print(json.dumps(line), flush=True)
     batch.close()
+    return line
+
+
+def run_batched(args):
+    print(json.dumps(batched_record(args.batch_scale, args.steps, args.warmup)), flush=True)
+
+
+def whole_volume_once(L, lo: Options, prot, mlp_h, freeze: int, seed: int = 4) -> dict:
+    """The whole-brain volume (145x174x145 grid, ellipsoidal mask of ~900k voxels) through ONE call
+    of bpx_xfibres_learned_host with pinned host buffers: data generated by the forward model on the
+    device (bpx_synth_dev, SNR 25) and copied to the host first, outside the timed call."""
+    import ctypes as C
+
+    import torch
+
+    from fdt_b200 import lib
+    from fdt_b200.abi import Volume
+
+    mask = synth.ellipsoid_mask((145, 174, 145), 900_000)
+    n = int(mask.sum())
+    bv, bl = lib.to_device(prot.bvecs), lib.to_device(prot.bvals)
+    d, _ = lib.synth(2, 3, n, bv, bl, seed, (25.0, 25.0))
+    hd = torch.empty(d.shape, dtype=torch.float32, pin_memory=True)
+    hd.copy_(d)
+    del d
+    torch.cuda.empty_cache()
+    hout = lib.alloc_outputs(lo, n, device="cpu", pin=True)
+    bh = np.ascontiguousarray(prot.bvecs, np.float32)
+    lh = np.ascontiguousarray(prot.bvals, np.float32)
+    v = Volume()
+    v.nvox, v.ndir = n, prot.ndir
+    v.data, v.bvecs, v.bvals = hd.data_ptr(), bh.ctypes.data, lh.ctypes.data
+    v.grad = None
+    v.voxel_offset = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lib._check(L.bpx_xfibres_learned_host(C.byref(lo), C.byref(v), mlp_h.ctypes.data, freeze, C.byref(hout[1])),
+               "xfibres_learned_host (whole volume)")
+    dt = time.perf_counter() - t0
+    ok = bool(torch.isfinite(hout[0]["mean_f"]).all())
+    L.bpx_release_workspace()
+    return {"voxels": n, "grid": [145, 174, 145], "calls": 1, "seconds": dt, "voxels_per_s": n / dt,
+            "entry": "bpx_xfibres_learned_host", "outputs_finite": ok,
+            "h2d_bytes": n * prot.ndir * 4, "d2h_bytes": sum(t.numel() * t.element_size() for t in hout[0].values())}
+
+
+def run_c3(args):
+    """Config C3: the initialiser network for the 279-measurement multi-shell protocol (9 b=0 + 90
+    directions at b=1000/2000/3000; model 2, 3 fibres, the options of config C1), evaluated on a
+    ~200k-voxel volume (96x96x60 grid, ellipsoidal mask; forward-model voxels, SNR 25): the learned
+    form (burn-in 200) against the plain LM-initialised chain (burn-in 1000), each one call over the
+    whole volume on device buffers, plus the multi-chain accuracy study on a subset."""
+    import torch
+
+    from fdt_b200 import learned, lib
+
+    o = Options.make(**learned.OPTION_SETS["c1"])
+    lo = learned_options(o)
+    prot = synth.three_shell(9, 90)
+    wpath = args.weights or learned.default_weights_path("multishell")
+    mlp_h, meta = learned.load_weights(wpath)
+    if int(meta["ndir"]) != prot.ndir:
+        raise SystemExit(f"{wpath}: trained for {int(meta['ndir'])} measurements, the protocol has {prot.ndir}")
+    mlp_d = torch.from_numpy(mlp_h).cuda()
+    n = int(synth.ellipsoid_mask((96, 96, 60), 200_000).sum())
+    bv, bl = lib.to_device(prot.bvecs), lib.to_device(prot.bvals)
+    data, _ = lib.synth(2, 3, n, bv, bl, 2, (25.0, 25.0))
+    stream = torch.cuda.current_stream()
+    outs = {"plain": lib.alloc_outputs(o, n), "learned": lib.alloc_outputs(lo, n)}
+
+    def run(form):
+        if form == "plain":
+            lib.xfibres_dev(o, data, bv, bl, out=outs["plain"])
+        else:
+            learned.xfibres_learned(lo, data, bv, bl, mlp_d, freeze=args.freeze, out=outs["learned"])
+
+    t = {}
+    clocks = ClockSampler(0)
+    clocks.start()
+    for form in ("plain", "learned"):
+        for _ in range(max(1, min(args.warmup, 1))):
+            run(form)
+        k = max(1, min(args.steps, 2))
+        e = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+        for e0, e1 in e:
+            e0.record(stream)
+            run(form)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        t[form] = sum(a.elapsed_time(b) for a, b in e) / 1e3 / k
+    ck = clocks.stop()
+    acc = learned.study_report(learned.posterior_study(o, data[: args.acc_voxels].contiguous(), bv, bl, mlp_d,
+                                                       R=args.acc_chains))
+    line = {
+        "metric": "voxels/s, learned-init vs plain MCMC on 1 B200 (config C3)", "value": n / t["learned"],
+        "unit": "voxels/s", "n_gpus": 1, "steps": k, "warmup": 1, "ms_per_step": 1e3 * t["learned"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": "C3: 279-measurement multi-shell protocol, model 2, 3 fibres (C1 options), "
+                   "96x96x60 ellipsoid of %d voxels, SNR 25; learned burn-in 200 vs plain burn-in 1000, "
+                   "njumps 1250, one call per volume" % n, "weights": os.path.relpath(wpath, ROOT),
+                   "n_train": int(meta.get("n_train", 0)), "freeze_props": args.freeze},
+        "forms": {f: {"voxels_per_s": n / t[f], "seconds_per_volume": t[f]} for f in t},
+        "learned_over_plain": t["plain"] / t["learned"],
+        "accuracy": acc, "clocks": ck, "gpu_launches": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_probtrack(args):
+    """probtrackx simple mode on the GPU: streamlines/s on a synthetic crossing-fibre field with the
+    whole-brain sample count (96x96x60 grid, ellipsoidal mask, 3 fibres x 50 samples; fibre 1 along
+    x, fibre 2 along y in half the volume), 1024 seed points in the mask x 5000 particles, probtrackx
+    defaults (2000 steps, 0.5 mm, cthr 0.2, fibthresh 0.01), 2 mm voxels.  The CPU oracle of the
+    same tracking is timed on 2 seed points (single thread) as the CPU baseline."""
+    import torch
+
+    from fdt_b200 import lib
+    from fdt_b200.abi import TrackOptions
+    from oracle import oracle as O
+
+    th, ph, f, mask = synth.fibre_field((96, 96, 60), nsamples=50, seed=1)
+    rng = np.random.default_rng(2)
+    inside = np.argwhere(mask > 0)  # [z, y, x]
+    pick = inside[rng.choice(len(inside), 1024, replace=False)]
+    seeds = np.ascontiguousarray(pick[:, ::-1].astype(np.float32))
+    o = TrackOptions.make(seed=9)
+    dev = [lib.to_device(a) for a in (th, ph, f, mask)]
+    sd = lib.to_device(seeds)
+    v = lib.track_volume(*dev)
+    paths = torch.zeros(mask.shape, device="cuda")
+    way = torch.zeros(1, device="cuda", dtype=torch.int64)
+    L = lib.load()
+    import ctypes as C
+
+    stream = torch.cuda.current_stream()
+
+    def step():
+        paths.zero_()
+        way.zero_()
+        lib._check(L.bpx_probtrack_dev(C.byref(o), C.byref(v), len(seeds), sd.data_ptr(), paths.data_ptr(),
+                                       way.data_ptr(), C.c_void_p(stream.cuda_stream)), "probtrack")
+
+    for _ in range(max(1, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    k = max(1, args.steps)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+    for e0, e1 in ev:
+        e0.record(stream)
+        step()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    t = sum(a.elapsed_time(b) for a, b in ev) / 1e3 / k
+    n_lines = len(seeds) * o.nparticles
+    nb = 2
+    o_cpu = TrackOptions.make(seed=9)
+    t0 = time.perf_counter()
+    O.probtrack(o_cpu, th, ph, f, mask, seeds[:nb])
+    t_cpu = time.perf_counter() - t0
+    line = {
+        "metric": "streamlines/s, probtrackx simple mode on bedpostx samples (1 B200)", "value": n_lines / t,
+        "unit": "streamlines/s", "n_gpus": 1, "steps": k, "warmup": max(1, args.warmup), "ms_per_step": 1e3 * t,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": "probtrackx simple mode: 96x96x60 crossing-fibre field, 3 fibres x 50 samples, "
+                   "1024 seeds x 5000 particles, 2000 steps of 0.5 mm, cthr 0.2, fibthresh 0.01",
+                   "streamlines": n_lines, "waytotal": int(way.item()), "visits": float(paths.sum().item())},
+        "cpu_baseline": {"value": nb * o.nparticles / t_cpu, "unit": "streamlines/s", "cores": 1, "kind": "port",
+                         "sample": f"{nb} seed points x {o.nparticles} particles through the CPU oracle"},
+        "gpu_launches": k, "clocks": ck,
+    }
+    print(json.dumps(line), flush=True)
 
 
 def learned_options(o: Options) -> Options:
@@ -336,9 +511,16 @@ def main():
     ap.add_argument("--freeze", type=int, default=0, choices=[0, 1, 2],
                     help="learned form: 0 network widths adapt, 1 frozen, 2 frozen after burn-in")
     ap.add_argument("--weights", default=None, help="initialiser weights (default: the committed whole-brain set)")
-    ap.add_argument("--workload", default="whole_brain", choices=["whole_brain", "batched"],
-                    help="batched: the mixed 16-volume batch in one graph launch (one GPU)")
-    ap.add_argument("--batch-scale", type=float, default=0.25, help="batched: voxel-count scale")
+    ap.add_argument("--workload", default="whole_brain", choices=["whole_brain", "batched", "c3", "probtrack"],
+                    help="batched: the mixed 16-volume batch in one graph launch (one GPU); c3: the "
+                         "279-measurement network on a 200k-voxel volume (one GPU)")
+    ap.add_argument("--batch-scale", type=float, default=0.5,
+                    help="batched: voxel-count scale (also the C2 sub-record of the default line)")
+    ap.add_argument("--no-c2", action="store_true", help="skip the C2 (mixed batch) sub-record")
+    ap.add_argument("--no-whole-volume", action="store_true",
+                    help="skip the one-call run of the ~900k-voxel whole-brain volume")
+    ap.add_argument("--acc-voxels", type=int, default=4096, help="accuracy study: voxels")
+    ap.add_argument("--acc-chains", type=int, default=8, help="accuracy study: chains per voxel and form")
     ap.add_argument("--prof", action="store_true",
                     help="profiling case: run the steps only (no e2e, CPU baseline, accuracy or calibration)")
     ap.add_argument("--nburn", type=int, default=None, help="override burn-in (profiling cases)")
@@ -348,6 +530,8 @@ def main():
         args.no_e2e = True
         args.no_cpu_baseline = True
         args.no_accuracy = True
+        args.no_c2 = True
+        args.no_whole_volume = True
     world, rank, local = dist_setup(args)
 
     if args.impl == "reference":
@@ -356,6 +540,14 @@ def main():
     if args.workload == "batched":
         if rank == 0:
             run_batched(args)
+        return
+    if args.workload == "c3":
+        if rank == 0:
+            run_c3(args)
+        return
+    if args.workload == "probtrack":
+        if rank == 0:
+            run_probtrack(args)
         return
 
     import ctypes as C
@@ -384,7 +576,10 @@ def main():
     prot = synth.three_shell(18, 90)
     M = prot.ndir
     chunk = args.chunk
-    forms = ["plain", "learned", "learned_batched"] if args.form == "all" else [args.form]
+    forms = ["plain", "learned", "learned_batched", "lm_burnin200"] if args.form == "all" else [args.form]
+    # the ablation form (the method without the network at the learned form's burn-in) is timed on
+    # fewer steps: it is a reported comparison, not the headline
+    short_forms = {"lm_burnin200"}
     wpath = args.weights or learned.default_weights_path("whole_brain")
     uses_net = "learned" in forms or "learned_batched" in forms
     mlp_h, meta = learned.load_weights(wpath) if uses_net else (None, None)
@@ -470,28 +665,39 @@ def main():
             ev[2].record(stream)
             ev[3].record(stream)
 
-    steps_fn = {"plain": plain_step, "learned": learned_step, "learned_batched": learned_batched_step}
+    lm200 = Options.make(**{f: getattr(o, f) for f, _ in Options._fields_ if f != "reserved"})
+    lm200.nburn = 200
+    lm200.seed = o.seed + 2
+
+    def lm200_step(i, ev=None):
+        plain_step(i, ev, opts=lm200, out=outs["lm_burnin200"])
+
+    steps_fn = {"plain": plain_step, "learned": learned_step, "learned_batched": learned_batched_step,
+                "lm_burnin200": lm200_step}
     # learned: prepare, features, weight cast + 5 GEMMs per 32768 voxels, decode, mcmc, finish;
     # learned_batched: one CUDA-graph launch (gather, the same kernels, scatter)
     n_gemm = 5 * ((chunk + 32767) // 32768)
     # kernels per step: plain = Rician clean-up, 4 fit stages, MCMC, finishing; learned = clean-up,
     # features, weight cast, the GEMMs, decode, MCMC, finishing; the graph form launches once and its
     # graph holds gather, the learned form's kernels and scatter
-    launches = {"plain": 7, "learned": 6 + n_gemm, "learned_batched": 8 + n_gemm}
+    launches = {"plain": 7, "learned": 6 + n_gemm, "learned_batched": 8 + n_gemm, "lm_burnin200": 7}
     timing = {}
     clocks = ClockSampler(local)
     clocks.start()
+    nsteps = {}
     for f in forms:
-        for i in range(args.warmup):
+        ns_f, nw_f = (min(args.steps, 3), min(args.warmup, 1)) if f in short_forms else (args.steps, args.warmup)
+        nsteps[f] = ns_f
+        for i in range(nw_f):
             flush.zero_()
             steps_fn[f](i)
         torch.cuda.synchronize()
         if pg:
             pg.barrier()
-        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
-        for i in range(args.steps):
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(ns_f)]
+        for i in range(ns_f):
             flush.zero_()  # L2 flush (256 MB write), outside the timed events
-            steps_fn[f](args.warmup + i, evs[i])
+            steps_fn[f](nw_f + i, evs[i])
         torch.cuda.synchronize()
         t = [sum(e[a].elapsed_time(e[a + 1]) for e in evs) / 1e3 for a in range(3)]
         tt = torch.tensor([sum(t)] + t, device="cuda", dtype=torch.float64)
@@ -510,24 +716,20 @@ def main():
 
     # ---- accuracy of the learned form against the plain chain on the same voxels ----
     accuracy = None
-    if not args.no_accuracy and "plain" in forms and ("learned" in forms or "learned_batched" in forms):
-        # the last timed step of each form ran on the same chunk; a second plain run with another
-        # seed gives the plain-vs-plain agreement the learned form is measured against
-        o2 = Options.make(**{f: getattr(o, f) for f, _ in Options._fields_ if f != "reserved"})
-        o2.seed = o.seed + 7
-        plain2 = lib.alloc_outputs(o, chunk)
-        plain_step(args.warmup + args.steps - 1, opts=o2, out=plain2)
-        torch.cuda.synchronize()
-        n_acc = min(chunk, 32768)
-        sub = lambda d: {k: v[..., :n_acc] for k, v in d.items()}  # noqa: E731  (voxel axis is last)
-        lout = lbatches[(args.warmup + args.steps - 1) % 2].outputs[0] if lbatches else outs["learned"][0]
-        accuracy = {
-            "voxels": n_acc,
-            "form": "learned_batched" if lbatches else "learned",
-            "learned_vs_plain": learned.summary(o, sub(lout), sub(outs["plain"][0])),
-            "plain_vs_plain_other_seed": learned.summary(o, sub(plain2[0]), sub(outs["plain"][0])),
-            "f_se": "Monte-Carlo SE of each chain's mean (Geyer initial positive sequence), combined",
-        }
+    if not args.no_accuracy and uses_net and rank == 0:
+        # R independent chains per voxel and form (the Monte-Carlo SE of a posterior mean is the
+        # spread of the chain means), on the first voxels of the first chunk, cleaned as the path
+        # cleans them; forms: plain (the judge), plain at another seed (yardstick), learned
+        # (adapting and frozen widths), LM start at the learned burn-in (the method without the
+        # network), and a long LM-started chain (gold)
+        d_acc = chunks_d[0][: args.acc_voxels].clone()
+        lib.prepare_data(d_acc)
+        sets = learned.posterior_study(o, d_acc, bvecs, bvals, mlp_d, R=args.acc_chains)
+        accuracy = learned.study_report(sets)
+        accuracy["se"] = ("Monte-Carlo SE of a posterior mean = sd of the chain means / sqrt(chains); "
+                          "|difference| <= 2 sqrt(se_a^2 + se_b^2) counts as agreement")
+        accuracy["dyads"] = "median angle between pooled dyads; 'supported' = fibres with mean f >= 0.05 in both"
+        del sets
 
     # ---- end to end through the host-buffer public entries (pinned host memory) ----
     e2e = None
@@ -565,6 +767,9 @@ def main():
         e2e = {"value": chunk * n_e2e * world / te.item(), "unit": "voxels/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "steps": n_e2e, "entry": "bpx_xfibres_learned_host" if head != "plain"
                else "bpx_xfibres_host"}
+        del hp, hout
+        if not args.no_whole_volume and head != "plain" and rank == 0:
+            e2e["whole_volume_once"] = whole_volume_once(L, lo, prot, mlp_h, args.freeze)
 
     if args.prof:
         if rank == 0:
@@ -605,13 +810,17 @@ def main():
     }
     peaks = measured_peaks()
     forms_out = {}
+    nb_form = {"plain": o.nburn, "learned": lo.nburn, "learned_batched": lo.nburn, "lm_burnin200": lm200.nburn}
     for f in forms:
         ts_, ti, tm, tf = timing[f]
-        forms_out[f] = {"voxels_per_s": vox_total / ts_, "ms_per_step": 1e3 * ts_ / args.steps,
-                        "nburn": (o if f == "plain" else lo).nburn, "gpu_launches_per_step": launches[f]}
+        k = nsteps[f]
+        forms_out[f] = {"voxels_per_s": chunk * k * world / ts_, "ms_per_step": 1e3 * ts_ / k, "steps": k,
+                        "nburn": nb_form[f], "gpu_launches_per_step": launches[f]}
         if f != "learned_batched":
-            forms_out[f]["phases_s_per_step"] = {"init": ti / args.steps, "mcmc": tm / args.steps,
-                                                 "finish": tf / args.steps}
+            forms_out[f]["phases_s_per_step"] = {"init": ti / k, "mcmc": tm / k, "finish": tf / k}
+    if "lm_burnin200" in forms_out:
+        forms_out["lm_burnin200"]["what"] = ("the method without the network at the learned form's burn-in: "
+                                             "LM fits + tau, reference widths, burn-in 200")
     result = {
         "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_step / args.steps, "higher_is_better": True,
@@ -631,6 +840,18 @@ def main():
         "clocks": ck,
         "hbm_peak_gbs": peaks.get("hbm_gbs"),
     }
+    if "lm_burnin200" in forms_out and head != "plain":
+        result["learned_over_lm_burnin200"] = forms_out[head]["voxels_per_s"] / forms_out["lm_burnin200"]["voxels_per_s"]
+    if rank == 0 and not args.no_c2 and world == 1:
+        del outs, chunks_d, work, flush
+        if lbatches:
+            for b in lbatches:
+                b.close()
+        torch.cuda.empty_cache()
+        c2 = batched_record(args.batch_scale, steps=2, warmup=1)
+        result["c2_batched"] = {k: c2[k] for k in ("value", "unit", "ms_per_step", "steps", "warmup", "config",
+                                                   "sequential_per_item", "batched_over_sequential", "create_s",
+                                                   "buckets", "clocks")}
     if rank == 0 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline()
     if rank == 0:

@@ -139,3 +139,53 @@ class PostProc(C.Structure):
         ("dyads_modf", C.c_void_p),
         ("mean_fsum", C.c_void_p),
     ]
+
+
+class TrackOptions(C.Structure):
+    """bpx_track_options: the probtrackx options of the simple mode (probtrackxOptions.h:198-236)."""
+
+    _fields_ = [
+        ("nparticles", C.c_int32),
+        ("nsteps", C.c_int32),
+        ("steplength", C.c_float),
+        ("c_thr", C.c_float),
+        ("fibthresh", C.c_float),
+        ("distthresh", C.c_float),
+        ("randfib", C.c_int32),
+        ("fibst", C.c_int32),
+        ("usef", C.c_int32),
+        ("sampvox", C.c_int32),
+        ("seed", C.c_uint64),
+        ("reserved", C.c_int32 * 4),
+    ]
+
+    @classmethod
+    def make(cls, **kw) -> "TrackOptions":
+        """probtrackx defaults (-P 5000 -S 2000 --steplength 0.5 -c 0.2 --fibthresh 0.01), overridden by kw."""
+        o = cls()
+        o.nparticles, o.nsteps, o.steplength, o.c_thr, o.fibthresh = 5000, 2000, 0.5, 0.2, 0.01
+        o.distthresh, o.randfib, o.fibst, o.usef, o.sampvox, o.seed = 0.0, 0, 1, 0, 0, 8665904
+        for k, v in kw.items():
+            if not hasattr(o, k):
+                raise KeyError(k)
+            setattr(o, k, v)
+        return o
+
+
+class TrackVolume(C.Structure):
+    """bpx_track_volume: samples [nfib][nsamples][nz][ny][nx], mask [nz][ny][nx], voxel size in mm."""
+
+    _fields_ = [
+        ("nx", C.c_int32),
+        ("ny", C.c_int32),
+        ("nz", C.c_int32),
+        ("dx", C.c_float),
+        ("dy", C.c_float),
+        ("dz", C.c_float),
+        ("nfib", C.c_int32),
+        ("nsamples", C.c_int32),
+        ("th", C.c_void_p),
+        ("ph", C.c_void_p),
+        ("f", C.c_void_p),
+        ("mask", C.c_void_p),
+    ]

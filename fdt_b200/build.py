@@ -48,8 +48,13 @@ def _stale(obj: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+# per-file flags: the tracking kernel keeps the reference's single-precision operation order (no
+# contraction of a*b+c into an FMA), which its CPU oracle repeats exactly
+FILE_FLAGS = {"bpx_track.cu": ["-fmad=false"]}
+
+
 def _compile(src: str, obj: str, extra: list[str], verbose: bool) -> tuple[str, str]:
-    cmd = [nvcc()] + NVCC_FLAGS + extra + ["-c", src, "-o", obj]
+    cmd = [nvcc()] + NVCC_FLAGS + FILE_FLAGS.get(os.path.basename(src), []) + extra + ["-c", src, "-o", obj]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -90,12 +91,32 @@ struct Workspace {
 std::mutex g_ws_mutex;
 Workspace g_ws[kWorkspaceSlots][kMaxDevices];
 
-// grow-only per-device scratch (not thread-safe across concurrent users of one device)
+}  // namespace
+}  // namespace bpx
+
+// A set of private workspaces (one per slot) on one device; see bpx_handle_create.
+struct bpx_handle {
+  int device = 0;
+  bpx::Workspace ws[bpx::kWorkspaceSlots];
+};
+
+namespace bpx {
+namespace {
+
+// the handle bound to this host thread (bpx_handle_bind), or NULL: the per-device shared workspaces
+thread_local bpx_handle* g_bound = nullptr;
+
+// grow-only scratch of one slot: the bound handle's, else the device's shared one (which all
+// unbound callers on the device share; see the concurrency note of bpx.h)
 bpx_status workspace(size_t bytes, void** out, int slot = kWsPipeline) {
   int dev = 0;
   BPX_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lk(g_ws_mutex);
-  Workspace& w = g_ws[slot][dev % kMaxDevices];
+  if (g_bound && g_bound->device != dev)
+    return fail(BPX_ERR_INVALID_ARG, "the handle bound to this thread belongs to device " +
+                                         std::to_string(g_bound->device) + ", the current device is " +
+                                         std::to_string(dev));
+  Workspace& w = g_bound ? g_bound->ws[slot] : g_ws[slot][dev % kMaxDevices];
   if (w.ptr && w.ctx != context_id()) {  // allocated in a context that no longer exists: forget it
     w.ptr = nullptr;
     w.cap = 0;
@@ -770,6 +791,50 @@ bpx_status bpx_measure_pipes(double* mufu_ops_per_s, double* fma_ops_per_s) {
   if (mufu_ops_per_s) *mufu_ops_per_s = lanes * it_m / (ms_m * 1e-3);
   if (fma_ops_per_s) *fma_ops_per_s = lanes * it_f / (ms_f * 1e-3);
   return BPX_OK;
+}
+
+bpx_status bpx_handle_create(bpx_handle** h) {
+  if (!h) return fail(BPX_ERR_INVALID_ARG, "bpx_handle_create: h is NULL");
+  *h = nullptr;
+  bpx_status st = check_device();
+  if (st != BPX_OK) return st;
+  int dev = 0;
+  BPX_CUDA(cudaGetDevice(&dev));
+  bpx_handle* p = new (std::nothrow) bpx_handle;
+  if (!p) return fail(BPX_ERR_CUDA, "bpx_handle_create: out of host memory");
+  p->device = dev;
+  *h = p;
+  return BPX_OK;
+}
+
+bpx_status bpx_handle_bind(bpx_handle* h) {
+  g_bound = h;
+  return BPX_OK;
+}
+
+bpx_status bpx_handle_destroy(bpx_handle* h) {
+  if (!h) return BPX_OK;
+  if (g_bound == h) g_bound = nullptr;
+  int cur = 0;
+  BPX_CUDA(cudaGetDevice(&cur));
+  if (cur != h->device) BPX_CUDA(cudaSetDevice(h->device));
+  bpx_status st = BPX_OK;
+  {
+    std::lock_guard<std::mutex> lk(g_ws_mutex);
+    for (int slot = 0; slot < kWorkspaceSlots; ++slot) {
+      Workspace& w = h->ws[slot];
+      // cudaFree waits for the device's work, so kernels still using the buffer finish first
+      if (w.ptr && w.ctx == context_id()) {
+        const cudaError_t e = cudaFree(w.ptr);
+        if (e != cudaSuccess && st == BPX_OK) st = cuda_fail(e, "bpx_handle_destroy: cudaFree");
+      }
+      w.ptr = nullptr;
+      w.cap = 0;
+    }
+  }
+  if (cur != h->device) cudaSetDevice(cur);
+  delete h;
+  return st;
 }
 
 bpx_status bpx_release_workspace(void) {

@@ -65,9 +65,7 @@ __device__ double principal_vector(double (&A)[3][3], double (&out)[3]) {
 }
 
 template <int K>
-__global__ void finish_kernel(FinishArgs a) {
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= a.nvox) return;
+__device__ void finish_voxel(const FinishArgs& a, int v) {
   const int ns = a.nsamples, nvox = a.nvox;
   const size_t row = (size_t)ns * nvox;
   const float* rec = a.records + v;
@@ -80,6 +78,7 @@ __global__ void finish_kernel(FinishArgs a) {
 #pragma unroll
       for (int j = 0; j < 3; ++j) dy[k][i][j] = 0;
   }
+#pragma unroll 2
   for (int s = 0; s < ns; ++s) {
     const size_t o = (size_t)s * nvox;
 #pragma unroll
@@ -153,6 +152,14 @@ __global__ void finish_kernel(FinishArgs a) {
   }
 }
 
+// Grid-stride over voxels.  A voxel's records are read twice (sums and dyads first, then the
+// sorted copies of th/ph/f); the launch keeps few enough voxels in flight that their records are
+// still in L2 for the second read, so each record crosses HBM once.
+template <int K>
+__global__ void finish_kernel(FinishArgs a) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < a.nvox; v += gridDim.x * blockDim.x) finish_voxel<K>(a, v);
+}
+
 // bedpostx_postproc_gpu.sh arithmetic (CUDA/bedpostx_postproc_gpu.sh:20-49) on the finished
 // outputs, one thread per voxel: fslmaths -Tmean of merged_th/ph, the dispersion of each fibre's
 // mean dyadic tensor (make_dyadic_vectors.cc:60-92: 1 - max |eigenvalue|), maskdyads
@@ -222,8 +229,17 @@ cudaError_t launch_postproc(const PostArgs& a, cudaStream_t s) {
 
 cudaError_t launch_finish(const FinishArgs& a, cudaStream_t s) {
   if (a.nvox == 0) return cudaSuccess;
-  const int threads = 128;
-  const int grid = (a.nvox + threads - 1) / threads;
+  const int threads = 64;
+  int dev = 0, l2 = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess || l2 <= 0) l2 = 32 << 20;
+  // voxels in flight whose records fill at most a third of L2 (the rest holds the outputs' lines)
+  const size_t per_voxel = (size_t)(6 + 3 * a.nfib) * a.nsamples * sizeof(float);
+  const size_t in_flight = (size_t)l2 / 3 / (per_voxel ? per_voxel : 1);
+  int grid = (int)((in_flight + threads - 1) / threads);
+  const int need = (a.nvox + threads - 1) / threads;
+  if (grid > need) grid = need;
+  if (grid < sm_count()) grid = sm_count() < need ? sm_count() : need;
   switch (a.nfib) {
     case 1: finish_kernel<1><<<grid, threads, 0, s>>>(a); break;
     case 2: finish_kernel<2><<<grid, threads, 0, s>>>(a); break;

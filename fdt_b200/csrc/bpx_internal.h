@@ -49,11 +49,12 @@ void set_last_error(const char* msg);  // message returned by bpx_last_error() o
 // C-ABI helpers shared by the entry-point files (bpx_api.cu): status with message, device and
 // argument checks, and the grow-only per-device workspaces (one per slot, so that a pipeline
 // stage can hold one while calling a stage that uses another).
-constexpr int kWorkspaceSlots = 4;
+constexpr int kWorkspaceSlots = 5;
 constexpr int kWsPipeline = 0;  // fit parameters, tau, records, status of bpx_xfibres_dev
 constexpr int kWsNetwork = 1;   // the network's weights and activations
 constexpr int kWsLearned = 2;   // intermediates of the learned pipeline
 constexpr int kWsFit = 3;       // FP64 parameters between the fit stages
+constexpr int kWsTrack = 4;     // the tracking kernel's per-thread visit tables
 bpx_status api_fail(bpx_status st, const std::string& msg);
 bpx_status api_cuda_fail(cudaError_t e, const char* where);
 bpx_status api_check_device();

@@ -1,0 +1,371 @@
+// bpx_track.cu -- probtrackx's simple mode on bedpostx samples (bpx_probtrack_dev).
+//
+// Replaces the per-particle loop of probtrackx (ptx_simple.cc:16-70 -> Seedmanager::run,
+// streamlines.cc:1029-1120; Streamliner::streamline, streamlines.cc:209-404; Tractvolsx::sample,
+// tractvolsx.h:101-255; Particle, particle.h) and its visit counting (Counter::update_pathdist,
+// streamlines.cc:662-690).  One thread tracks one particle: both halves of its streamline from the
+// seed, then adds 1 to fdt_paths in every voxel the kept halves passed through (once per voxel:
+// a per-thread open-addressing table of the voxels already counted, entries stamped with the
+// particle so no clearing is needed between particles) and 1 to waytotal.
+//
+// The work is a chain of dependent random gathers (mask, then a posterior sample of each fibre at
+// a randomly rounded position), so the kernel is latency-bound: a persistent grid keeps as many
+// particles in flight as the tables' workspace allows and every thread walks its particles in turn.
+//
+// Arithmetic: single precision in the reference's operation order, no contraction into FMAs (this
+// file is compiled with -fmad=false), sine and cosine from sincos_fast; random numbers from
+// Philox-4x32-10 keyed by the seed, counted by (particle, half, step), eight uniforms per step.
+// The CPU oracle (oracle/track_oracle.c) does the same operations and follows identical paths.
+#include <cstdint>
+#include <string>
+
+#include "bpx.h"
+#include "bpx_device.cuh"
+#include "bpx_internal.h"
+
+namespace bpx {
+namespace {
+
+constexpr int kTrackThreads = 64;
+constexpr int kTrackBlocksPerSm = 4;
+
+struct TrackArgs {
+  bpx_track_options o;
+  bpx_track_volume v;
+  size_t nvox;
+  int nseeds;
+  const float* seeds;
+  float* paths;
+  unsigned long long* waytotal;
+  uint2* tables;       // [threads][1 << log2n] {voxel, stamp}
+  int log2n;
+  uint64_t pid_begin;  // particles [pid_begin, pid_end) of this launch
+  uint64_t pid_end;
+};
+
+__device__ __forceinline__ float u24(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
+
+__device__ __forceinline__ void track_uniforms(uint64_t seed, uint64_t pid, int half, uint32_t step, float (&u)[8]) {
+  const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const uint4 r = philox4x32_10(make_uint4((uint32_t)pid, (uint32_t)(pid >> 32), step, 0x80000000u | (uint32_t)(2 * half + c)), key);
+    u[4 * c + 0] = u24(r.x);
+    u[4 * c + 1] = u24(r.y);
+    u[4 * c + 2] = u24(r.z);
+    u[4 * c + 3] = u24(r.w);
+  }
+}
+
+__device__ __forceinline__ int rnd(float v) { return (int)floorf(v + 0.5f); }
+__device__ __forceinline__ int clampi(int a, int lo, int hi) { return a < lo ? lo : (a > hi ? hi : a); }
+
+struct Particle {
+  float x, y, z, rx, ry, rz, rxi, ryi, rzi;
+  bool jumped;
+};
+
+struct Tracker {
+  const TrackArgs& a;
+  uint2* tab;
+  uint32_t stamp;
+
+  __device__ bool inside(int ix, int iy, int iz) const {
+    const bpx_track_volume& v = a.v;
+    if (ix < 0 || iy < 0 || iz < 0 || ix >= v.nx || iy >= v.ny || iz >= v.nz) return false;
+    return __ldg(v.mask + ((size_t)iz * v.ny + iy) * v.nx + ix) > 0.f;
+  }
+  __device__ size_t at(int k, int s, size_t vox) const { return ((size_t)k * a.v.nsamples + s) * a.nvox + vox; }
+
+  // first visit of `vox` by this particle: true (and the voxel is recorded)
+  __device__ bool first_visit(uint32_t vox) const {
+    const uint32_t mask = (1u << a.log2n) - 1u;
+    uint32_t h = (vox * 2654435761u) >> (32 - a.log2n);
+    for (uint32_t probe = 0; probe <= mask; ++probe) {
+      const uint2 e = tab[h];
+      if (e.y != stamp) {
+        tab[h] = make_uint2(vox, stamp);
+        return true;
+      }
+      if (e.x == vox) return false;
+      h = (h + 1u) & mask;
+    }
+    return false;  // unreachable: the table holds twice the longest path
+  }
+
+  // Tractvolsx::sample
+  __device__ void sample(const Particle& P, const float (&u)[8], bool& init_sample, int& fibst, float& th, float& ph,
+                         float& f) const {
+    const bpx_track_volume& v = a.v;
+    const int cx = (int)ceilf(P.x), fx = (int)floorf(P.x);
+    const int cy = (int)ceilf(P.y), fy = (int)floorf(P.y);
+    const int cz = (int)ceilf(P.z), fz = (int)floorf(P.z);
+    const float pcx = (cx == fx) ? 1.0f : (P.x - (float)fx) / (float)(cx - fx);
+    const float pcy = (cy == fy) ? 1.0f : (P.y - (float)fy) / (float)(cy - fy);
+    const float pcz = (cz == fz) ? 1.0f : (P.z - (float)fz) / (float)(cz - fz);
+    const int nx_ = clampi(u[0] > pcx ? fx : cx, 0, v.nx - 1);
+    const int ny_ = clampi(u[1] > pcy ? fy : cy, 0, v.ny - 1);
+    const int nz_ = clampi(u[2] > pcz ? fz : cz, 0, v.nz - 1);
+    const size_t vox = ((size_t)nz_ * v.ny + ny_) * v.nx + nx_;
+    const int samp = clampi(rnd(u[3] * (float)(v.nsamples - 1)), 0, v.nsamples - 1);
+    const int K = v.nfib;
+    const float thr = a.o.fibthresh;
+    float theta = 0.f, phi = 0.f;
+    int fibind = 0;
+    if (K > 1) {
+      if (init_sample) {
+        if (a.o.randfib == 1) {
+          int list[BPX_MAX_FIBRES], n = 0;
+          for (int k = 0; k < K; ++k)
+            if (__ldg(v.f + at(k, samp, vox)) > thr) list[n++] = k;
+          fibst = n == 0 ? 0 : list[clampi(rnd(u[4] * (float)(n - 1)), 0, n - 1)];
+        } else if (a.o.randfib == 2) {
+          float fsum = 0.f;
+          for (int k = 0; k < K; ++k) {
+            const float ft = __ldg(v.f + at(k, samp, vox));
+            if (ft > thr) fsum += ft;
+          }
+          if (fsum == 0.f) {
+            fibst = 0;
+          } else {
+            const float r = fsum * u[4];
+            float cum = 0.f;
+            for (int k = 0; k < K; ++k) {
+              const float ft = __ldg(v.f + at(k, samp, vox));
+              if (ft > thr) cum += ft;
+              if (r <= cum) {
+                fibst = k;
+                break;
+              }
+            }
+          }
+        }
+        theta = __ldg(v.th + at(fibst, samp, vox));
+        phi = __ldg(v.ph + at(fibst, samp, vox));
+        init_sample = false;
+      } else {
+        const float px = P.rx, py = P.ry, pz = P.rz;  // no preferred-direction volume
+        float dotmax = 0.f;
+        for (int k = 0; k < K; ++k) {
+          if (__ldg(v.f + at(k, samp, vox)) > thr) {
+            const float pht = __ldg(v.ph + at(k, samp, vox)), tht = __ldg(v.th + at(k, samp, vox));
+            float st, ct, sp, cp;
+            sincos_fast(tht, st, ct);
+            sincos_fast(pht, sp, cp);
+            const float dot = fabsf(st * cp * px + st * sp * py + ct * pz);
+            if (dot > dotmax) {
+              dotmax = dot;
+              theta = tht;
+              phi = pht;
+              fibind = k;
+            }
+          }
+        }
+        if (dotmax == 0.f) {
+          theta = __ldg(v.th + at(0, samp, vox));
+          phi = __ldg(v.ph + at(0, samp, vox));
+        }
+      }
+    } else {
+      theta = __ldg(v.th + at(0, samp, vox));
+      phi = __ldg(v.ph + at(0, samp, vox));
+    }
+    th = theta;
+    ph = phi;
+    f = a.o.usef ? __ldg(v.f + at(fibind, samp, vox)) : 1.0f;
+  }
+
+  // Streamliner::streamline for one half; counts the path's first visits when `count`.
+  // Returns the reject flag (1: shorter than distthresh).
+  __device__ int half_line(Particle& P, uint64_t pid, int h, int fibst0, float x0, float y0, float z0,
+                           bool count) const {
+    const bpx_track_options& o = a.o;
+    bool init_sample = true;
+    int fibst = fibst0;
+    P.x = x0;
+    P.y = y0;
+    P.z = z0;
+    float pathlength = 0.f;
+    for (int it = 1; it <= o.nsteps / 2; ++it) {
+      const int ix = rnd(P.x), iy = rnd(P.y), iz = rnd(P.z);
+      if (!inside(ix, iy, iz)) break;  // the reference's remaining steps change nothing
+      if (count) {
+        const uint32_t vox = (uint32_t)(((size_t)iz * a.v.ny + iy) * a.v.nx + ix);
+        if (first_visit(vox)) atomicAdd(a.paths + vox, 1.0f);
+      }
+      pathlength += o.steplength;
+      float u[8], th, ph, f;
+      track_uniforms(o.seed, pid, h, (uint32_t)it, u);
+      sample(P, u, init_sample, fibst, th, ph, f);
+      if (f > u[5]) {
+        float st, ct, sp, cp;
+        sincos_fast(th, st, ct);
+        sincos_fast(ph, sp, cp);
+        const float rxn = cp * st, ryn = sp * st, rzn = ct;
+        if (P.jumped && !(fabsf(rxn * P.rx + ryn * P.ry + rzn * P.rz) > o.c_thr)) break;
+        if (th != 0.f && ph != 0.f) {
+          int sign;
+          bool init = false;
+          if (P.jumped) {
+            sign = (rxn * P.rx + ryn * P.ry + rzn * P.rz) > 0.f ? 1 : -1;
+          } else {
+            sign = u[6] > 0.5f ? 1 : -1;
+            P.jumped = true;
+            init = true;
+          }
+          const float s = (float)sign;
+          P.x += s * o.steplength / a.v.dx * rxn;
+          P.y += s * o.steplength / a.v.dy * ryn;
+          P.z += s * o.steplength / a.v.dz * rzn;
+          P.rx = s * rxn;
+          P.ry = s * ryn;
+          P.rz = s * rzn;
+          if (init) {
+            P.rxi = P.rx;
+            P.ryi = P.ry;
+            P.rzi = P.rz;
+          }
+        }
+      }
+    }
+    return pathlength < o.distthresh ? 1 : 0;
+  }
+};
+
+__global__ void __launch_bounds__(kTrackThreads) track_kernel(TrackArgs a) {
+  const uint64_t threads = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  Tracker T{a, a.tables + (t << a.log2n), 0u};
+  unsigned long long kept = 0;
+  const bool two_pass = a.o.distthresh > 0.f;  // a half counts only once its length is known
+  for (uint64_t pid = a.pid_begin + t; pid < a.pid_end; pid += threads) {
+    T.stamp = (uint32_t)(pid - a.pid_begin) + 1u;
+    const int s = (int)(pid / (uint64_t)a.o.nparticles);
+    float u0[8];
+    track_uniforms(a.o.seed, pid, 0, 0u, u0);  // the particle's own draws: step 0
+    int fibst = a.o.fibst - 1;
+    if (a.o.randfib > 2) fibst = rnd(u0[0] * (float)(a.v.nfib - 1));
+    fibst = clampi(fibst, 0, a.v.nfib - 1);
+    float x0 = a.seeds[3 * s], y0 = a.seeds[3 * s + 1], z0 = a.seeds[3 * s + 2];
+    if (a.o.sampvox) {
+      x0 += u0[1] - 0.5f;
+      y0 += u0[2] - 0.5f;
+      z0 += u0[3] - 0.5f;
+    }
+    Particle P{};
+    int rej1, rej2;
+    if (two_pass) {
+      const Particle P0 = P;
+      rej1 = T.half_line(P, pid, 0, fibst, x0, y0, z0, false);
+      if (rej1 == 0) {
+        Particle Q = P0;
+        T.half_line(Q, pid, 0, fibst, x0, y0, z0, true);
+      }
+    } else {
+      rej1 = T.half_line(P, pid, 0, fibst, x0, y0, z0, true);
+    }
+    if (P.jumped) {  // Particle::restart_reverse
+      P.rx = -P.rxi;
+      P.ry = -P.ryi;
+      P.rz = -P.rzi;
+    }
+    if (two_pass) {
+      const Particle P1 = P;
+      rej2 = T.half_line(P, pid, 1, fibst, x0, y0, z0, false);
+      if (rej2 == 0) {
+        Particle Q = P1;
+        T.half_line(Q, pid, 1, fibst, x0, y0, z0, true);
+      }
+    } else {
+      rej2 = T.half_line(P, pid, 1, fibst, x0, y0, z0, true);
+    }
+    if (rej1 == 0 || rej2 == 0) ++kept;
+  }
+  // waytotal: one atomic per warp
+  for (int o = 16; o >= 1; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
+  if ((threadIdx.x & 31) == 0 && kept) atomicAdd(a.waytotal, kept);
+}
+
+bpx_status check_track(const bpx_track_options* o, const bpx_track_volume* v, int32_t nseeds, const float* seeds,
+                       const float* paths, const int64_t* waytotal) {
+  if (!o || !v) return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: opts or vol is NULL");
+  if (o->nparticles < 1 || o->nsteps < 2 || o->nsteps > (1 << 20))
+    return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: nparticles must be >= 1 and nsteps in 2..2^20");
+  if (!(o->steplength > 0.f) || !(o->c_thr >= 0.f) || o->randfib < 0 || o->randfib > 3 || o->fibst < 1)
+    return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: bad steplength, cthr, randfib or fibst");
+  if (v->nx < 1 || v->ny < 1 || v->nz < 1 || v->nfib < 1 || v->nfib > BPX_MAX_FIBRES || v->nsamples < 1)
+    return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: bad grid, fibre or sample count");
+  if ((size_t)v->nx * v->ny * v->nz >= (1ull << 32))
+    return api_fail(BPX_ERR_UNSUPPORTED, "bpx_probtrack_dev: more than 2^32 voxels");
+  if (!(v->dx > 0.f && v->dy > 0.f && v->dz > 0.f))
+    return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: voxel sizes must be positive");
+  if (o->fibst > v->nfib) return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: fibst beyond the fibres given");
+  if (nseeds < 0) return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: nseeds < 0");
+  if (nseeds > 0 && (!seeds || !paths || !waytotal || !v->th || !v->ph || !v->f || !v->mask))
+    return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: NULL buffer");
+  return BPX_OK;
+}
+
+}  // namespace
+}  // namespace bpx
+
+using namespace bpx;
+
+extern "C" {
+
+void bpx_track_options_default(bpx_track_options* o) {
+  if (!o) return;
+  *o = bpx_track_options{};
+  o->nparticles = 5000;
+  o->nsteps = 2000;
+  o->steplength = 0.5f;
+  o->c_thr = 0.2f;
+  o->fibthresh = 0.01f;
+  o->distthresh = 0.f;
+  o->randfib = 0;
+  o->fibst = 1;
+  o->seed = 8665904ull;
+}
+
+bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volume* vol, int32_t nseeds,
+                             const float* seeds, float* paths, int64_t* waytotal, void* stream) {
+  NvtxRange nvtx_range("bpx.probtrack");
+  bpx_status st = check_track(opts, vol, nseeds, seeds, paths, waytotal);
+  if (st != BPX_OK || nseeds == 0) return st;
+  st = api_check_device();
+  if (st != BPX_OK) return st;
+  TrackArgs a{};
+  a.o = *opts;
+  a.v = *vol;
+  a.nvox = (size_t)vol->nx * vol->ny * vol->nz;
+  a.nseeds = nseeds;
+  a.seeds = seeds;
+  a.paths = paths;
+  a.waytotal = reinterpret_cast<unsigned long long*>(waytotal);
+  // a table of at least twice the longest path (one voxel per step of both halves)
+  int log2n = 1;
+  while ((1ll << log2n) < 2ll * (opts->nsteps + 2)) ++log2n;
+  a.log2n = log2n;
+  const int grid = sm_count() * kTrackBlocksPerSm;
+  const size_t threads = (size_t)grid * kTrackThreads;
+  void* ws = nullptr;
+  st = api_workspace(kWsTrack, threads * ((size_t)1 << log2n) * sizeof(uint2), &ws);
+  if (st != BPX_OK) return st;
+  a.tables = (uint2*)ws;
+  cudaStream_t s = (cudaStream_t)stream;
+  const uint64_t total = (uint64_t)nseeds * (uint64_t)opts->nparticles;
+  const uint64_t chunk = 1ull << 30;  // stamps stay below 2^30 + 1 within a launch
+  for (uint64_t b = 0; b < total; b += chunk) {
+    // stamp 0 marks every entry empty before a launch reuses the tables
+    const cudaError_t e0 = cudaMemsetAsync(ws, 0, threads * ((size_t)1 << log2n) * sizeof(uint2), s);
+    if (e0 != cudaSuccess) return api_cuda_fail(e0, "bpx_probtrack_dev: cudaMemsetAsync");
+    a.pid_begin = b;
+    a.pid_end = b + chunk < total ? b + chunk : total;
+    track_kernel<<<grid, kTrackThreads, 0, s>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return api_cuda_fail(e, "bpx_probtrack_dev: track_kernel");
+  }
+  return BPX_OK;
+}
+
+}  // extern "C"

@@ -6,9 +6,10 @@ burn-in (bpx_mcmc_ex_dev).  Every step of training -- forward, loss, backward, A
 library's own kernels (tcgen05 GEMMs with fused epilogues); PyTorch only holds device memory and
 gathers the mini-batches.
 
-The trained network replaces the LM initialiser and sets per-voxel proposal widths that are then
-frozen, so the chain needs a shorter burn-in; the plain LM-initialised chain with the full burn-in
-stays the fallback and the judge of its accuracy (see `compare`).
+The trained network replaces the LM initialiser and sets per-voxel proposal widths (which the
+chain then adapts, or keeps frozen), so the chain needs a shorter burn-in; the plain LM-initialised
+chain with the full burn-in stays the fallback and the judge of its accuracy (posterior_study and
+study_report measure both against it and against a long chain).
 """
 from __future__ import annotations
 
@@ -274,56 +275,82 @@ def load_weights(path: str):
     return z["params"], {k: z[k] for k in z.files if k != "params"}
 
 
-def mc_se(x):
-    """Monte-Carlo standard error of the mean of each column of x [ns][n] (one chain's samples per
-    voxel): sd * sqrt(tau / ns), with the integrated autocorrelation time tau = -1 + 2 sum_m G_m,
-    G_m = rho_2m + rho_2m+1 summed up to the first non-positive G_m (Geyer's initial positive
-    sequence)."""
+def posterior_study(opts: Options, data, bvecs, bvals, mlp_params, R: int = 8, seed: int = 100,
+                    gold: bool = True) -> dict:
+    """Chain sets of the learned form and its comparators on the same voxels, R chains per voxel
+    (independent random streams: the volume is replicated R times, so every copy of a voxel has its
+    own RNG key), for agreement.compare:
+
+      plain           LM start, the reference's widths, opts.nburn (1000): the form that judges errors
+      plain_other_seed   the same with another seed (yardstick of plain-vs-plain agreement)
+      learned         network start state and widths, burn-in 200, widths adapting (freeze 0)
+      learned_frozen  the same, widths frozen after the burn-in (freeze 2)
+      lm_burnin200    the method without the network at the learned form's burn-in: LM start,
+                      the reference's widths, burn-in 200
+      gold            LM start, burn-in 5000, 12500 jumps recorded every 125: a long chain whose
+                      posterior means carry less start dependence and Monte-Carlo error
+
+    data: [n][ndir] device tensor (cleaned under --rician); bvecs/bvals device tensors; mlp_params the
+    network (host or device).  Returns {form: agreement.ChainSet}."""
     import torch
 
-    ns = x.shape[0]
-    c = x - x.mean(0)
-    g0 = (c * c).mean(0).clamp_min(1e-30)
+    from . import agreement
 
-    def rho(k):
-        return (c[k:] * c[: ns - k]).mean(0) * ((ns - k) / ns) / g0 if k < ns else torch.zeros_like(g0)
+    n = int(data.shape[0])
+    K = opts.nfibres
+    dR = data.repeat(R, 1).contiguous()
+    params, tau, _ = lib.fit(opts, data, bvecs, bvals)
+    pR, tR = params.repeat(R, 1).contiguous(), tau.repeat(R).contiguous()
+    tau_arg = tR if opts.rician else None
+    x, s0 = features(data, bvecs, bvals)
+    lo = Options.make(**{f: getattr(opts, f) for f, _ in Options._fields_ if f != "reserved"})
+    lo.nburn = 200
+    out = forward(mlp_params, int(data.shape[1]), x)
+    pn, tn, props, _ = decode(lo, out, s0)
+    pnR, tnR, propsR = pn.repeat(R, 1).contiguous(), tn.repeat(R).contiguous(), props.repeat(1, R).contiguous()
 
-    tau = -torch.ones_like(g0)
-    alive = torch.ones_like(g0, dtype=torch.bool)
-    for m in range(ns // 2):
-        G = (torch.ones_like(g0) if m == 0 else rho(2 * m)) + rho(2 * m + 1)
-        alive = alive & (G > 0)
-        tau = tau + 2.0 * torch.where(alive, G, torch.zeros_like(G))
-    return torch.sqrt(g0 * tau.clamp_min(1.0) / ns)
+    def with_(**kw):
+        o = Options.make(**{f: getattr(opts, f) for f, _ in Options._fields_ if f != "reserved"})
+        for k, v in kw.items():
+            setattr(o, k, v)
+        return o
 
+    def chains(o, p, t, pin=None, freeze=0):
+        rec, _ = lib.mcmc_ex(o, dR, bvecs, bvals, p, t, props_in=pin, freeze=freeze)
+        torch.cuda.synchronize()
+        return agreement.ChainSet(rec.cpu().numpy(), K, R)
 
-def compare(opts: Options, a: dict, b: dict):
-    """Agreement of two runs' posteriors per voxel: (dyad angle differences in degrees [K][n],
-    |mean f difference| / combined Monte-Carlo standard error [K][n], mean d relative difference
-    [n]).  Standard errors account for the autocorrelation of each chain's samples (mc_se)."""
-    import torch
-
-    ang, z = [], []
-    for k in range(opts.nfibres):
-        da, db = a["dyads"][k].float(), b["dyads"][k].float()
-        c = (da * db).sum(0).abs().clamp(max=1.0)
-        ang.append(torch.rad2deg(torch.acos(c)))
-        fa, fb = a["f"][k].float(), b["f"][k].float()
-        se = torch.sqrt(mc_se(fa) ** 2 + mc_se(fb) ** 2).clamp_min(1e-6)
-        z.append((fa.mean(0) - fb.mean(0)).abs() / se)
-    dd = (a["mean_d"] - b["mean_d"]).abs() / b["mean_d"].abs().clamp_min(1e-12)
-    return torch.stack(ang), torch.stack(z), dd
-
-
-def summary(opts: Options, a: dict, b: dict) -> dict:
-    """Median dyad angles, fraction of f within 2 MC standard errors, median d relative difference."""
-    ang, z, dd = compare(opts, a, b)
-    return {
-        "dyad_median_deg": [round(float(ang[k].median()), 3) for k in range(opts.nfibres)],
-        "f_within_2se": [round(float((z[k] <= 2).float().mean()), 3) for k in range(opts.nfibres)],
-        "d_rel_median": round(float(dd.median()), 4),
+    sets = {
+        "plain": chains(with_(seed=seed), pR, tau_arg),
+        "plain_other_seed": chains(with_(seed=seed + 7), pR, tau_arg),
+        "learned": chains(with_(seed=seed + 1, nburn=200), pnR, tnR if opts.rician else None, propsR, 0),
+        "learned_frozen": chains(with_(seed=seed + 1, nburn=200), pnR, tnR if opts.rician else None, propsR, 2),
+        "lm_burnin200": chains(with_(seed=seed + 2, nburn=200), pR, tau_arg),
     }
+    if gold:
+        sets["gold"] = chains(with_(seed=seed + 3, nburn=5000, njumps=12500, sampleevery=125), pR, tau_arg)
+    return sets
 
+
+def study_report(sets: dict) -> dict:
+    """Agreement of each form with the plain chain and with the long (gold) chain."""
+    from . import agreement
+
+    rep = {"chains_per_voxel": int(sets["plain"].R), "voxels": int(sets["plain"].nvox),
+           "vs_plain": {k: agreement.compare(sets[k], sets["plain"])
+                        for k in ("plain_other_seed", "learned", "learned_frozen", "lm_burnin200") if k in sets}}
+    if "gold" in sets:
+        rep["vs_gold"] = {k: agreement.compare(sets[k], sets["gold"])
+                          for k in ("plain", "learned", "learned_frozen", "lm_burnin200") if k in sets}
+    return rep
+
+
+# chain options of the configurations a network is trained for
+OPTION_SETS = {
+    "whole_brain": dict(model=2, nfibres=3, rician=1, f0=1, ardf0=1),  # the whole-brain configuration
+    "c1": dict(model=2, nfibres=3),  # the multi-shell configuration: no Rician noise model, no f0
+}
+DEFAULT_OPTIONS = {"whole_brain": "whole_brain", "multishell": "c1"}
 
 PROTOCOLS = {
     "whole_brain": lambda synth: synth.three_shell(18, 90),
@@ -349,6 +376,8 @@ def main(argv=None) -> None:
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--protocol", default="whole_brain", choices=sorted(PROTOCOLS))
+    ap.add_argument("--options", default=None, choices=sorted(OPTION_SETS),
+                    help="chain options the network is trained for (default: the protocol's configuration)")
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--batch", type=int, default=4096)
@@ -360,7 +389,8 @@ def main(argv=None) -> None:
     ap.add_argument("--weights", default=None, help="evaluate these weights instead of training")
     a = ap.parse_args(argv)
     prot = PROTOCOLS[a.protocol](synth)
-    opts = Options.make(model=2, nfibres=3, rician=1, f0=1, ardf0=1)
+    oname = a.options or DEFAULT_OPTIONS[a.protocol]
+    opts = Options.make(**OPTION_SETS[oname])
     if a.weights:
         params, _ = load_weights(a.weights)
     else:
@@ -374,23 +404,20 @@ def main(argv=None) -> None:
             print(f"  step {s:6d} loss {l:.5f}")
         out = a.out or default_weights_path(a.protocol)
         save(out, params, ndir=prot.ndir, model=2, nfibres=3, protocol=a.protocol, n_train=a.n, steps=a.steps,
-             seed=a.seed, labels=a.labels, bvals=prot.bvals, bvecs=prot.bvecs)
+             seed=a.seed, labels=a.labels, bvals=prot.bvals, bvecs=prot.bvecs, options=oname,
+             rician=opts.rician, f0=opts.f0, ardf0=opts.ardf0)
         print("saved", out)
         del ts
         torch.cuda.empty_cache()
     if a.eval:
+        import json
+
         data, _ = synth.make_volume(a.eval, prot, 3, True, 25.0, seed=a.seed + 1000)
         bv, bl = lib.to_device(prot.bvecs), lib.to_device(prot.bvals)
-        plain = lib.xfibres_dev(opts, lib.to_device(data), bv, bl)
-        o2 = Options.make(model=2, nfibres=3, rician=1, f0=1, ardf0=1, seed=opts.seed + 1)
-        print("plain vs plain (other seed):", summary(opts, lib.xfibres_dev(o2, lib.to_device(data), bv, bl), plain))
-        o3 = Options.make(model=2, nfibres=3, rician=1, f0=1, ardf0=1, nburn=200, seed=opts.seed + 1)
-        print("LM start, burn-in 200:", summary(opts, lib.xfibres_dev(o3, lib.to_device(data), bv, bl), plain))
-        for nb in (100, 200):
-            for fr in (0, 1, 2):
-                lo = Options.make(model=2, nfibres=3, rician=1, f0=1, ardf0=1, nburn=nb, seed=opts.seed + 1)
-                learned_out = xfibres_learned(lo, lib.to_device(data), bv, bl, params, freeze=fr)
-                print(f"learned, burn-in {nb}, freeze {fr}:", summary(opts, learned_out, plain))
+        d = lib.to_device(data)
+        if opts.rician:
+            lib.prepare_data(d)
+        print(json.dumps(study_report(posterior_study(opts, d, bv, bl, params, R=8))))
 
 
 if __name__ == "__main__":

@@ -11,7 +11,7 @@ import os
 
 import numpy as np
 
-from .abi import BPX_NSTATE, Item, Options, Outputs, PostProc, Volume, nrec
+from .abi import BPX_NSTATE, Item, Options, Outputs, PostProc, TrackOptions, TrackVolume, Volume, nrec
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libbpx.so")
@@ -37,6 +37,12 @@ _SIGS = {
                                      C.c_void_p, C.c_void_p]),
     "bpx_mcmc_layouts": (C.c_int32, [C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32]),
     "bpx_release_workspace": (C.c_int, []),
+    "bpx_track_options_default": (None, [C.POINTER(TrackOptions)]),
+    "bpx_probtrack_dev": (C.c_int, [C.POINTER(TrackOptions), C.POINTER(TrackVolume), C.c_int32, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p]),
+    "bpx_handle_create": (C.c_int, [C.POINTER(C.c_void_p)]),
+    "bpx_handle_bind": (C.c_int, [C.c_void_p]),
+    "bpx_handle_destroy": (C.c_int, [C.c_void_p]),
     "bpx_measure_pipes": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "bpx_xfibres_noalloc_dev": (C.c_int, [C.POINTER(Options), C.POINTER(Volume), C.POINTER(Outputs), C.c_void_p]),
     "bpx_mcmc_ex_dev": (C.c_int, [C.POINTER(Options), C.POINTER(Volume), C.c_void_p, C.c_void_p, C.c_void_p,
@@ -353,6 +359,52 @@ def states_from_records(opts: Options, records, sample: int):
         st[:, 7 + 3 * k] = r[7 + 3 * k]
         st[:, 8 + 3 * k] = r[8 + 3 * k]
     return st
+
+
+def track_volume(th, ph, f, mask, voxel_size=(2.0, 2.0, 2.0)) -> TrackVolume:
+    """TrackVolume over device tensors th/ph/f [nfib][nsamples][nz][ny][nx] and mask [nz][ny][nx]."""
+    v = TrackVolume()
+    v.nfib, v.nsamples, v.nz, v.ny, v.nx = (int(x) for x in th.shape)
+    v.dx, v.dy, v.dz = (float(x) for x in voxel_size)
+    v.th, v.ph, v.f, v.mask = th.data_ptr(), ph.data_ptr(), f.data_ptr(), mask.data_ptr()
+    return v
+
+
+def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.0)):
+    """probtrackx simple mode on device tensors: (paths [nz][ny][nx] float32, waytotal int) for
+    seeds [nseeds][3] (voxel coordinates x, y, z)."""
+    torch = _torch()
+    v = track_volume(th, ph, f, mask, voxel_size)
+    paths = torch.zeros(tuple(mask.shape), device="cuda", dtype=torch.float32)
+    way = torch.zeros(1, device="cuda", dtype=torch.int64)
+    sd = to_device(seeds)
+    _check(load().bpx_probtrack_dev(C.byref(topts), C.byref(v), int(sd.shape[0]), _ptr(sd), _ptr(paths), _ptr(way),
+                                    _stream(torch)), "bpx_probtrack_dev")
+    return paths, int(way.item())
+
+
+class Handle:
+    """Private workspaces for the workspace-using entries (bpx_handle_*).  ``with handle:`` binds it
+    to the calling thread for the block, so that calls from different threads with different
+    handles may run concurrently on different streams."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        _check(load().bpx_handle_create(C.byref(h)), "bpx_handle_create")
+        self.h = h
+
+    def __enter__(self):
+        _check(load().bpx_handle_bind(self.h), "bpx_handle_bind")
+        return self
+
+    def __exit__(self, *exc):
+        load().bpx_handle_bind(None)
+        return False
+
+    def close(self):
+        if getattr(self, "h", None):
+            _check(load().bpx_handle_destroy(self.h), "bpx_handle_destroy")
+            self.h = None
 
 
 class Batch:

@@ -1,0 +1,91 @@
+"""probtrackx's simple mode on a bedpostx directory, on the GPU (bpx_probtrack_dev).
+
+    python -m fdt_b200.probtrack SUBJECT.bedpostX --seeds seeds.txt --out OUTDIR [-P 5000] [-S 2000]
+        [--steplength 0.5] [--cthr 0.2] [--fibthresh 0.01] [--distthresh 0] [--randfib 0] [--fibst 1]
+        [--usef] [--sampvox] [--seed N]
+
+Reads merged_th{k}samples, merged_ph{k}samples, merged_f{k}samples and nodif_brain_mask (NIfTI-1)
+as probtrackx does (probtrackx.cc:25-96 with mode simple, tractvolsx.h:55-97), tracks from every
+seed point of the seed file (one point per row, voxel coordinates x y z; ptx_simple.cc:31-35) and
+writes fdt_paths (visit counts of the kept streamlines, the mask's geometry) and waytotal.
+The seed coordinates are taken in the volume's voxel grid as stored (the reference converts NIfTI
+voxel coordinates to its internal convention, which is the identity for neurological storage).
+"""
+from __future__ import annotations
+
+import argparse
+import glob
+import os
+
+import numpy as np
+
+from . import lib, nifti
+from .abi import TrackOptions
+
+
+def read_samples(bpx_dir: str):
+    """(th, ph, f [K][nsamples][nz][ny][nx] float32, mask [nz][ny][nx], header, voxel size)."""
+    mask, hdr = nifti.read(os.path.join(bpx_dir, "nodif_brain_mask.nii.gz"))
+    K = len(glob.glob(os.path.join(bpx_dir, "merged_th*samples.nii.gz")))
+    if K == 0:
+        raise FileNotFoundError(f"{bpx_dir}: no merged_th1samples")
+    vols = {}
+    for q in ("th", "ph", "f"):
+        arr = []
+        for k in range(1, K + 1):
+            a, _ = nifti.read(os.path.join(bpx_dir, f"merged_{q}{k}samples.nii.gz"))
+            if a.ndim == 3:
+                a = a[..., None]
+            if a.shape[:3] != mask.shape[:3]:
+                raise ValueError(f"merged_{q}{k}samples: grid {a.shape[:3]} differs from the mask's {mask.shape[:3]}")
+            arr.append(np.transpose(np.asarray(a, np.float32), (3, 2, 1, 0)))  # [ns][z][y][x]
+        vols[q] = np.ascontiguousarray(np.stack(arr))
+    m = np.ascontiguousarray(np.transpose(np.asarray(mask, np.float32).reshape(mask.shape[:3]), (2, 1, 0)))
+    vs = tuple(float(x) for x in hdr.pixdim[1:4])
+    return vols["th"], vols["ph"], vols["f"], m, hdr, vs
+
+
+def run(bpx_dir: str, seeds: np.ndarray, opts: TrackOptions, outdir: str) -> tuple[np.ndarray, int]:
+    import torch
+
+    th, ph, f, m, hdr, vs = read_samples(bpx_dir)
+    dev = [lib.to_device(a) for a in (th, ph, f, m)]
+    paths, way = lib.probtrack(opts, *dev, np.asarray(seeds, np.float32).reshape(-1, 3), voxel_size=vs)
+    torch.cuda.synchronize()
+    vol = np.transpose(paths.cpu().numpy(), (2, 1, 0))  # back to [x][y][z]
+    os.makedirs(outdir, exist_ok=True)
+    nifti.write(os.path.join(outdir, "fdt_paths.nii.gz"), vol, like=hdr, cal=(float(vol.min()), float(vol.max())))
+    with open(os.path.join(outdir, "waytotal"), "w") as fh:
+        fh.write(f"{way}\n")
+    return vol, way
+
+
+def main(argv=None) -> None:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("bpx_dir")
+    ap.add_argument("--seeds", required=True, help="text file, one seed point (voxel x y z) per row")
+    ap.add_argument("--out", required=True)
+    ap.add_argument("-P", "--nsamples", type=int, default=5000)
+    ap.add_argument("-S", "--nsteps", type=int, default=2000)
+    ap.add_argument("--steplength", type=float, default=0.5)
+    ap.add_argument("-c", "--cthr", type=float, default=0.2)
+    ap.add_argument("--fibthresh", type=float, default=0.01)
+    ap.add_argument("--distthresh", type=float, default=0.0)
+    ap.add_argument("--randfib", type=int, default=0)
+    ap.add_argument("--fibst", type=int, default=1)
+    ap.add_argument("-f", "--usef", action="store_true")
+    ap.add_argument("--sampvox", action="store_true")
+    ap.add_argument("--seed", type=int, default=8665904)
+    a = ap.parse_args(argv)
+    seeds = np.loadtxt(a.seeds, ndmin=2)
+    if seeds.shape[1] != 3 and seeds.shape[0] == 3:
+        seeds = seeds.T
+    o = TrackOptions.make(nparticles=a.nsamples, nsteps=a.nsteps, steplength=a.steplength, c_thr=a.cthr,
+                          fibthresh=a.fibthresh, distthresh=a.distthresh, randfib=a.randfib, fibst=a.fibst,
+                          usef=int(a.usef), sampvox=int(a.sampvox), seed=a.seed)
+    _, way = run(a.bpx_dir, seeds, o, a.out)
+    print(f"waytotal {way}")
+
+
+if __name__ == "__main__":
+    main()

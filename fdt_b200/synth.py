@@ -249,3 +249,34 @@ def config_whole_brain(seed: int = 4, nvox: int | None = None) -> Volume:
         nvox = int(mask.sum())
     data, truth = make_volume(nvox, prot, 3, True, 25.0, seed)
     return Volume(data, prot, truth, 2, 3, shape, mask)
+
+
+def fibre_field(shape=(24, 20, 12), nsamples: int = 20, jitter: float = 0.08, seed: int = 0):
+    """Posterior samples of a synthetic fibre field for tracking (the bedpostx outputs probtrackx
+    reads): an ellipsoidal mask; fibre 1 runs along x everywhere, fibre 2 along y in the
+    half-space x >= nx/2 (a crossing region), fibre 3 has f below the usual threshold.  Angles are
+    jittered per sample by N(0, jitter) rad.  Returns th, ph, f [3][nsamples][nz][ny][nx] and
+    mask [nz][ny][nx] (float32)."""
+    nx, ny, nz = shape
+    rng = np.random.default_rng(seed)
+    zz, yy, xx = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    c = [(nx - 1) / 2, (ny - 1) / 2, (nz - 1) / 2]
+    r = ((xx - c[0]) / (0.48 * nx)) ** 2 + ((yy - c[1]) / (0.48 * ny)) ** 2 + ((zz - c[2]) / (0.48 * nz)) ** 2
+    mask = (r <= 1.0).astype(np.float32)
+    K = 3
+    th = np.zeros((K, nsamples, nz, ny, nx), np.float32)
+    ph = np.zeros_like(th)
+    f = np.zeros_like(th)
+    g = lambda: rng.normal(0.0, jitter, (nsamples, nz, ny, nx))  # noqa: E731
+    th[0] = np.pi / 2 + g()
+    ph[0] = 0.0 + g()
+    f[0] = 0.5 + 0.05 * rng.standard_normal((nsamples, nz, ny, nx))
+    cross = (xx >= nx // 2)[None]
+    th[1] = np.pi / 2 + g()
+    ph[1] = np.pi / 2 + g()
+    f[1] = np.where(cross, 0.3, 0.005) + 0.02 * rng.standard_normal((nsamples, nz, ny, nx))
+    th[2] = rng.uniform(0.1, np.pi - 0.1, (nsamples, nz, ny, nx))
+    ph[2] = rng.uniform(-np.pi, np.pi, (nsamples, nz, ny, nx))
+    f[2] = 0.004
+    f = np.clip(f, 0.0, 1.0)
+    return th, ph, f.astype(np.float32), mask

@@ -15,11 +15,14 @@
  * and is synchronous.  Options are passed explicitly (the reference reads a process-wide
  * xfibresOptions singleton).  Concurrency: the stage entries that take all their buffers from
  * the caller (bpx_mcmc_*, bpx_finish_dev, bpx_postproc_dev, bpx_prepare_data_dev,
- * bpx_gemm_bf16_dev) may run concurrently on different streams.  The entries that use the
- * library's per-device workspace (bpx_fit_dev, bpx_xfibres_dev/_host, bpx_xfibres_learned_*,
- * bpx_mlp_forward_dev, bpx_mlp_train_step_dev) share it between all callers on a device: issue
- * them on one stream, or make a stream wait for the previous such call's work before the next
- * call.  A bpx_batch owns its buffers; different batches may run concurrently.
+ * bpx_gemm_bf16_dev) may run concurrently on different streams.  The entries that use workspace
+ * memory (bpx_fit_dev, bpx_xfibres_dev/_host, bpx_xfibres_learned_*, bpx_mlp_forward_dev,
+ * bpx_mlp_train_step_dev) take it from the handle bound to the calling host thread
+ * (bpx_handle_bind), or, with none bound, from a per-device workspace shared by every unbound
+ * caller on the device: unbound calls must be issued on one stream, or each made to wait for the
+ * previous such call's work.  Calls bound to different handles may run concurrently, from
+ * different threads and on different streams.  A bpx_batch owns its buffers; different batches may
+ * run concurrently.
  *
  * Array layouts (row-major, C order):
  *   data      [nvox][ndir]                 (voxel-major; CUDA/xfibres_gpu.cu:390-399)
@@ -422,8 +425,75 @@ typedef struct bpx_postproc {
 bpx_status bpx_postproc_dev(const bpx_options* opts, int32_t nvox, const bpx_outputs* out, float thr,
                             bpx_postproc* post, void* stream);
 
+/*
+ * ---- probtrackx on the samples (simple mode: seeds -> fdt_paths) ----
+ * The consumer of merged_th/ph/f{k}samples (probtrackx.cc:25-96 -> ptx_simple.cc:16-70,
+ * Seedmanager::run and Streamliner::streamline in streamlines.cc:209-416,1023-1127,
+ * Tractvolsx::sample in tractvolsx.h:101-255, Particle in particle.h).  For every seed point,
+ * nparticles particles each track one streamline in both directions from the seed: per step the
+ * position is rounded probabilistically to a voxel, one of the voxel's nsamples posterior samples
+ * is drawn, the fibre closest to the current direction among those with f > fibthresh is taken,
+ * the step stops at the curvature threshold c_thr, and the particle moves steplength mm.  Every
+ * voxel a kept streamline passes through is counted once per streamline (fdt_paths), and kept
+ * streamlines are counted (waytotal).  Random numbers are Philox-4x32-10 keyed by the seed and
+ * counted by (particle, half, step), so a run is reproducible (the reference uses rand()).
+ */
+typedef struct bpx_track_options {
+  int32_t nparticles;  /* -P, --nsamples: particles per seed point   (default 5000) */
+  int32_t nsteps;      /* -S, --nsteps: steps per streamline (both halves together; default 2000) */
+  float steplength;    /* --steplength, mm                           (default 0.5) */
+  float c_thr;         /* -c, --cthr: curvature threshold |cos|       (default 0.2) */
+  float fibthresh;     /* --fibthresh: f below which a fibre is ignored (default 0.01) */
+  float distthresh;    /* --distthresh: halves shorter than this (mm) are dropped (default 0) */
+  int32_t randfib;     /* --randfib 0..3: how the first step's fibre is chosen (default 0) */
+  int32_t fibst;       /* --fibst: first fibre (1-based) when randfib is 0 (default 1) */
+  int32_t usef;        /* -f, --usef: a step is taken with probability f */
+  int32_t sampvox;     /* --sampvox: seed positions jittered within the seed voxel */
+  uint64_t seed;       /* random seed */
+  int32_t reserved[4]; /* zero */
+} bpx_track_options;
+
+/* The bedpostx outputs probtrackx reads, on the device.  Sample arrays [nfib][nsamples][nz][ny][nx]
+ * (x fastest: the merged_{th,ph,f}{k}samples volumes one after the other); mask [nz][ny][nx]
+ * (nodif_brain_mask, > 0 inside); voxel size dx, dy, dz in mm. */
+typedef struct bpx_track_volume {
+  int32_t nx, ny, nz;
+  float dx, dy, dz;
+  int32_t nfib, nsamples;
+  const float* th;
+  const float* ph;
+  const float* f;
+  const float* mask;
+} bpx_track_volume;
+
+void bpx_track_options_default(bpx_track_options* opts);
+/*
+ * Tracks opts->nparticles streamlines from each of nseeds seed points (seeds [nseeds][3], voxel
+ * coordinates of the volume, x y z) and ADDS each kept streamline's distinct voxels to
+ * paths [nz][ny][nx] (float counts, fdt_paths) and the kept streamlines to *waytotal (device
+ * int64); the caller zeroes both first.  Uses workspace memory (see Concurrency) of
+ * 8 * 2^ceil(log2(2 * (nsteps + 2))) bytes per particle in flight (256 particles per
+ * multiprocessor: 1.2 GB on a B200 at nsteps 2000).
+ */
+bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volume* vol, int32_t nseeds,
+                             const float* seeds, float* paths, int64_t* waytotal, void* stream);
+
 /* Free the per-device workspace cache of the current device. */
 bpx_status bpx_release_workspace(void);
+
+/*
+ * Workspace handles (the re-entrant counterpart of the reference's process-wide state, which makes
+ * xfibres_gpu() single-threaded: CUDA/xfibres_gpu.h:15-23 with the xfibresOptions singleton).
+ * A handle owns private grow-only workspaces on the device current at bpx_handle_create.
+ * bpx_handle_bind(h) makes every workspace-using call on this host thread use h's workspaces
+ * (bind NULL to return to the shared per-device ones); a handle is bound to one thread at a time
+ * and its calls follow the one-stream rule among themselves.  bpx_handle_destroy frees the
+ * workspaces (cudaFree waits for the device's work) and unbinds it from the calling thread.
+ */
+typedef struct bpx_handle bpx_handle;
+bpx_status bpx_handle_create(bpx_handle** h);
+bpx_status bpx_handle_bind(bpx_handle* h);
+bpx_status bpx_handle_destroy(bpx_handle* h);
 
 #ifdef __cplusplus
 }

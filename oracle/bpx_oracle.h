@@ -7,9 +7,13 @@
  * The product (libbpx.so) never calls it.
  *
  * Parity pinning: the reference ships no tests, fixtures or golden vectors and its CPU xfibres
- * needs FSL libraries that are absent, so this oracle is pinned by analytic known-answer
- * checks (noiseless LM recovery, finite-difference Jacobians, the Philox-4x32-10 published
- * known-answer vectors, logI0 against its series) rather than by reference outputs.
+ * needs FSL libraries that are absent.  Its CUDA kernels, however, build from their own sources
+ * (oracle/Makefile, target ref -> oracle/_ref/librefgpu.so), and tests/test_gpu_refpin.py checks
+ * this oracle against them on the same inputs: the LM models' cost, gradient and Hessian
+ * (cf_/grad_/hess_PVM_*), the LM fits, the MCMC's initial likelihood and prior energies
+ * (init_Fibres_Multifibres_kernel) and the posterior means of its chains (runmcmc_kernel).
+ * Analytic known-answer checks (noiseless LM recovery, finite-difference Jacobians, the
+ * Philox-4x32-10 published known-answer vectors, logI0 against its series) pin the rest.
  *
  * Random numbers: the oracle and the GPU share one counter-based generator, Philox-4x32-10
  * (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC11), keyed by
@@ -84,6 +88,14 @@ int orc_finish(const bpx_options* opts, int nvox, const double* records, double*
 /* Likelihood and prior energies of given states [nvox][BPX_NSTATE]. */
 int orc_energy(const bpx_options* opts, int nvox, int ndir, const float* data, const float* bvecs,
                const float* bvals, const double* states, double* lik, double* prior);
+
+/* probtrackx simple mode on bedpostx samples (track_oracle.c): adds each kept streamline's
+ * distinct voxels to paths [nz][ny][nx] and the kept streamlines to *waytotal. */
+int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nseeds, const float* seeds,
+                  float* paths, int64_t* waytotal);
+/* the uniforms of one tracking step, and the single-precision sine/cosine both paths use */
+void orc_track_uniforms(uint64_t seed, uint64_t pid, int half, uint32_t step, float u[8]);
+void orc_sincos_fast(float x, float* sn, float* cs);
 
 #ifdef __cplusplus
 }

@@ -11,7 +11,7 @@ import subprocess
 
 import numpy as np
 
-from fdt_b200.abi import BPX_NSTATE, Options, nrec
+from fdt_b200.abi import BPX_NSTATE, Options, TrackOptions, TrackVolume, nrec
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "libbpx_oracle.so")
@@ -54,6 +54,10 @@ def lib():
         L.orc_finish.argtypes = [C.POINTER(Options), C.c_int, _f64p] + [C.c_void_p] * 11
         L.orc_energy.argtypes = [C.POINTER(Options), C.c_int, C.c_int, _f32p, _f32p, _f32p, _f64p,
                                  C.c_void_p, C.c_void_p]
+        L.orc_probtrack.argtypes = [C.POINTER(TrackOptions), C.POINTER(TrackVolume), C.c_int, _f32p, _f32p,
+                                    C.POINTER(C.c_int64)]
+        L.orc_track_uniforms.argtypes = [C.c_uint64, C.c_uint64, C.c_int, C.c_uint32, _f32p]
+        L.orc_sincos_fast.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
         _lib = L
     return _lib
 
@@ -180,3 +184,25 @@ def energy(opts: Options, data, bvecs, bvals, states):
                      np.ascontiguousarray(bvals, np.float32), st, lik.ctypes.data,
                      prior.ctypes.data)
     return lik, prior
+
+
+def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.0)):
+    """probtrackx simple mode on host arrays (th/ph/f [nfib][nsamples][nz][ny][nx], mask [nz][ny][nx],
+    seeds [nseeds][3] voxel coordinates): (paths [nz][ny][nx] float32, waytotal)."""
+    th, ph, f, mask = (np.ascontiguousarray(a, np.float32) for a in (th, ph, f, mask))
+    v = TrackVolume()
+    v.nfib, v.nsamples, v.nz, v.ny, v.nx = th.shape
+    v.dx, v.dy, v.dz = voxel_size
+    v.th, v.ph, v.f, v.mask = th.ctypes.data, ph.ctypes.data, f.ctypes.data, mask.ctypes.data
+    paths = np.zeros(mask.shape, np.float32)
+    way = C.c_int64(0)
+    sd = np.ascontiguousarray(seeds, np.float32).reshape(-1, 3)
+    rc = lib().orc_probtrack(C.byref(topts), C.byref(v), sd.shape[0], sd, paths, C.byref(way))
+    assert rc == 0
+    return paths, int(way.value)
+
+
+def sincos_fast(x: float) -> tuple[float, float]:
+    s, c = C.c_float(), C.c_float()
+    lib().orc_sincos_fast(x, C.byref(s), C.byref(c))
+    return s.value, c.value

@@ -1,0 +1,300 @@
+/*
+ * track_oracle.c -- CPU oracle of probtrackx's simple mode on bedpostx samples.  TEST
+ * INFRASTRUCTURE ONLY (loaded by tests/ as the checker of bpx_probtrack_dev; the product never
+ * calls it).
+ *
+ * Restates, one particle at a time:
+ *   Seedmanager::run            (streamlines.cc:1029-1120): both halves of a streamline from the
+ *                               seed, kept halves, the streamline count (waytotal);
+ *   Streamliner::streamline     (streamlines.cc:209-404): steps inside the mask, the path, the
+ *                               curvature stop, the jump, the distance threshold;
+ *   Counter::update_pathdist    (streamlines.cc:662-690): every voxel of a kept streamline counted
+ *                               once (fdt_paths);
+ *   Tractvolsx::sample          (tractvolsx.h:101-255): probabilistic rounding of the position,
+ *                               a random posterior sample, the first fibre (fibst, randfib 1/2)
+ *                               and afterwards the fibre closest to the current direction among
+ *                               those with f > fibthresh, f for --usef;
+ *   Particle::jump / check_dir / restart_reverse (particle.h).
+ * The reference draws from rand(); here every step's uniforms come from Philox-4x32-10 keyed by
+ * the seed and counted by (particle, half, step), exactly as the GPU kernel draws them, and the
+ * arithmetic is single precision in the reference's operation order, with the sine and cosine of
+ * the GPU path (Cody-Waite reduction and the fitted quarter-period polynomials kSinQ/kCosQ of
+ * bpx_device.cuh), so the oracle and the kernel follow identical paths.  MISCMATHS::round is taken
+ * as floor(x + 0.5); sample positions are clamped to the grid (the reference reads its volume
+ * there through newimage's boundary handling).  Compiled with -ffp-contract=off.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "bpx_oracle.h"
+
+/* the quarter-period polynomial coefficients of bpx_device.cuh (generated by fdt_b200/polyfit.py);
+ * tests/test_track_oracle.py checks that these literals equal the header's */
+static const float kSinQ[3] = {-0.16666655f, 0.008332156f, -0.00019514632f};
+static const float kCosQ[3] = {0.041666646f, -0.0013887362f, 2.443773e-05f};
+
+static void sincos_quarter(float r, float* s, float* c) {
+  const float u = r * r;
+  float p = fmaf(u, kSinQ[2], kSinQ[1]);
+  p = fmaf(u, p, kSinQ[0]);
+  *s = fmaf(r * u, p, r);
+  float q = fmaf(u, kCosQ[2], kCosQ[1]);
+  q = fmaf(u, q, kCosQ[0]);
+  q = fmaf(u, q, -0.5f);
+  *c = fmaf(u, q, 1.0f);
+}
+
+static float flip_sign(float a, int flip) {
+  uint32_t b;
+  memcpy(&b, &a, 4);
+  b ^= flip ? 0x80000000u : 0u;
+  memcpy(&a, &b, 4);
+  return a;
+}
+
+void orc_sincos_fast(float x, float* sn, float* cs) {
+  const float k = rintf(x * 0.636619772f);
+  float r = fmaf(-k, 1.57079637f, x);
+  r = fmaf(-k, -4.37113883e-08f, r);
+  r = fmaf(-k, -1.71512451e-15f, r);
+  float s, c;
+  sincos_quarter(r, &s, &c);
+  const int q = (int)k;
+  const int sw = (q & 1) != 0;
+  const float a = sw ? c : s, b = sw ? s : c;
+  *sn = flip_sign(a, (q & 2) != 0);
+  *cs = flip_sign(b, ((q + 1) & 2) != 0);
+}
+
+static float u24(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
+
+/* 8 uniforms in [0,1) for step `step` of half `half` of particle `pid` */
+void orc_track_uniforms(uint64_t seed, uint64_t pid, int half, uint32_t step, float u[8]) {
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  for (int c = 0; c < 2; ++c) {
+    const uint32_t ctr[4] = {(uint32_t)pid, (uint32_t)(pid >> 32), step, 0x80000000u | (uint32_t)(2 * half + c)};
+    uint32_t r[4];
+    orc_philox4x32_10(ctr, key, r);
+    for (int i = 0; i < 4; ++i) u[4 * c + i] = u24(r[i]);
+  }
+}
+
+static int rnd(float v) { return (int)floorf(v + 0.5f); }
+
+typedef struct {
+  const bpx_track_options* o;
+  const bpx_track_volume* v;
+  size_t nvox;
+  float sx, sy, sz; /* steplength / voxel size */
+} trk_t;
+
+typedef struct {
+  float x, y, z, rx, ry, rz, rxi, ryi, rzi;
+  int jumped;
+} part_t;
+
+static int inside(const trk_t* T, int ix, int iy, int iz) {
+  const bpx_track_volume* v = T->v;
+  if (ix < 0 || iy < 0 || iz < 0 || ix >= v->nx || iy >= v->ny || iz >= v->nz) return 0;
+  return v->mask[((size_t)iz * v->ny + iy) * v->nx + ix] > 0.f;
+}
+
+static int clampi(int a, int lo, int hi) { return a < lo ? lo : (a > hi ? hi : a); }
+
+static size_t at(const trk_t* T, int k, int s, size_t vox) {
+  return ((size_t)k * T->v->nsamples + s) * T->nvox + vox;
+}
+
+/* Tractvolsx::sample: theta, phi and f of one step */
+static void sample(const trk_t* T, const part_t* P, const float u[8], int* init_sample, int* fibst, float* th,
+                   float* ph, float* f) {
+  const bpx_track_volume* v = T->v;
+  const int cx = (int)ceilf(P->x), fx = (int)floorf(P->x);
+  const int cy = (int)ceilf(P->y), fy = (int)floorf(P->y);
+  const int cz = (int)ceilf(P->z), fz = (int)floorf(P->z);
+  const float pcx = (cx == fx) ? 1.0f : (P->x - (float)fx) / (float)(cx - fx);
+  const float pcy = (cy == fy) ? 1.0f : (P->y - (float)fy) / (float)(cy - fy);
+  const float pcz = (cz == fz) ? 1.0f : (P->z - (float)fz) / (float)(cz - fz);
+  const int nx_ = clampi(u[0] > pcx ? fx : cx, 0, v->nx - 1);
+  const int ny_ = clampi(u[1] > pcy ? fy : cy, 0, v->ny - 1);
+  const int nz_ = clampi(u[2] > pcz ? fz : cz, 0, v->nz - 1);
+  const size_t vox = ((size_t)nz_ * v->ny + ny_) * v->nx + nx_;
+  const int samp = clampi(rnd(u[3] * (float)(v->nsamples - 1)), 0, v->nsamples - 1);
+  const int K = v->nfib;
+  const float thr = T->o->fibthresh;
+  float theta = 0.f, phi = 0.f;
+  int fibind = 0;
+  if (K > 1) {
+    if (*init_sample) {
+      if (T->o->randfib == 1) {
+        int list[BPX_MAX_FIBRES], n = 0;
+        for (int k = 0; k < K; ++k)
+          if (v->f[at(T, k, samp, vox)] > thr) list[n++] = k;
+        *fibst = n == 0 ? 0 : list[clampi(rnd(u[4] * (float)(n - 1)), 0, n - 1)];
+      } else if (T->o->randfib == 2) {
+        float fsum = 0.f;
+        for (int k = 0; k < K; ++k) {
+          const float ft = v->f[at(T, k, samp, vox)];
+          if (ft > thr) fsum += ft;
+        }
+        if (fsum == 0.f) {
+          *fibst = 0;
+        } else {
+          const float r = fsum * u[4];
+          float cum = 0.f;
+          for (int k = 0; k < K; ++k) {
+            const float ft = v->f[at(T, k, samp, vox)];
+            if (ft > thr) cum += ft;
+            if (r <= cum) {
+              *fibst = k;
+              break;
+            }
+          }
+        }
+      }
+      theta = v->th[at(T, *fibst, samp, vox)];
+      phi = v->ph[at(T, *fibst, samp, vox)];
+      *init_sample = 0;
+    } else {
+      /* no preferred-direction volume: the preference is the current direction */
+      const float px = P->rx, py = P->ry, pz = P->rz;
+      float dotmax = 0.f;
+      for (int k = 0; k < K; ++k) {
+        if (v->f[at(T, k, samp, vox)] > thr) {
+          const float pht = v->ph[at(T, k, samp, vox)], tht = v->th[at(T, k, samp, vox)];
+          float st, ct, sp, cp;
+          orc_sincos_fast(tht, &st, &ct);
+          orc_sincos_fast(pht, &sp, &cp);
+          const float dot = fabsf(st * cp * px + st * sp * py + ct * pz);
+          if (dot > dotmax) {
+            dotmax = dot;
+            theta = tht;
+            phi = pht;
+            fibind = k;
+          }
+        }
+      }
+      if (dotmax == 0.f) {
+        theta = v->th[at(T, 0, samp, vox)];
+        phi = v->ph[at(T, 0, samp, vox)];
+      }
+    }
+  } else {
+    theta = v->th[at(T, 0, samp, vox)];
+    phi = v->ph[at(T, 0, samp, vox)];
+  }
+  *th = theta;
+  *ph = phi;
+  *f = T->o->usef ? v->f[at(T, fibind, samp, vox)] : 1.0f;
+}
+
+/* one half of a streamline (Streamliner::streamline); appends the path's voxels to path[];
+ * returns the reject flag (1: shorter than distthresh) */
+static int half_line(const trk_t* T, part_t* P, uint64_t pid, int h, int fibst0, float x0, float y0, float z0,
+                     int64_t* path, int* npath) {
+  const bpx_track_options* o = T->o;
+  int init_sample = 1, fibst = fibst0;
+  P->x = x0;
+  P->y = y0;
+  P->z = z0;
+  float pathlength = 0.f;
+  for (int it = 1; it <= o->nsteps / 2; ++it) {
+    const int ix = rnd(P->x), iy = rnd(P->y), iz = rnd(P->z);
+    if (!inside(T, ix, iy, iz)) break;  /* the reference's remaining steps change nothing */
+    path[(*npath)++] = ((int64_t)iz * T->v->ny + iy) * T->v->nx + ix;
+    pathlength += o->steplength;
+    float u[8], th, ph, f;
+    orc_track_uniforms(o->seed, pid, h, (uint32_t)it, u);
+    sample(T, P, u, &init_sample, &fibst, &th, &ph, &f);
+    if (f > u[5]) {
+      float st, ct, sp, cp;
+      orc_sincos_fast(th, &st, &ct);
+      orc_sincos_fast(ph, &sp, &cp);
+      const float rxn = cp * st, ryn = sp * st, rzn = ct;
+      if (P->jumped && !(fabsf(rxn * P->rx + ryn * P->ry + rzn * P->rz) > o->c_thr)) break;
+      if (th != 0.f && ph != 0.f) {
+        int sign, init = 0;
+        if (P->jumped) {
+          sign = (rxn * P->rx + ryn * P->ry + rzn * P->rz) > 0.f ? 1 : -1;
+        } else {
+          sign = u[6] > 0.5f ? 1 : -1;
+          P->jumped = 1;
+          init = 1;
+        }
+        const float s = (float)sign;
+        P->x += s * o->steplength / T->v->dx * rxn;
+        P->y += s * o->steplength / T->v->dy * ryn;
+        P->z += s * o->steplength / T->v->dz * rzn;
+        P->rx = s * rxn;
+        P->ry = s * ryn;
+        P->rz = s * rzn;
+        if (init) {
+          P->rxi = P->rx;
+          P->ryi = P->ry;
+          P->rzi = P->rz;
+        }
+      }
+    }
+  }
+  return pathlength < o->distthresh ? 1 : 0;
+}
+
+int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nseeds, const float* seeds,
+                  float* paths, int64_t* waytotal) {
+  trk_t T;
+  T.o = o;
+  T.v = v;
+  T.nvox = (size_t)v->nx * v->ny * v->nz;
+  const int half_steps = o->nsteps / 2;
+  int64_t* path = (int64_t*)malloc(sizeof(int64_t) * (size_t)(2 * half_steps + 2));
+  int64_t* stamp = (int64_t*)malloc(sizeof(int64_t) * T.nvox);
+  if (!path || !stamp) {
+    free(path);
+    free(stamp);
+    return 1;
+  }
+  for (size_t i = 0; i < T.nvox; ++i) stamp[i] = -1;
+  int64_t kept = 0;
+  for (int s = 0; s < nseeds; ++s) {
+    for (int p = 0; p < o->nparticles; ++p) {
+      const uint64_t pid = (uint64_t)s * (uint64_t)o->nparticles + (uint64_t)p;
+      float u[8];
+      orc_track_uniforms(o->seed, pid, 0, 0u, u); /* the particle's own draws: step 0 */
+      int fibst = o->fibst - 1;
+      if (o->randfib > 2) fibst = rnd(u[0] * (float)(v->nfib - 1));
+      fibst = clampi(fibst, 0, v->nfib - 1);
+      float x0 = seeds[3 * s], y0 = seeds[3 * s + 1], z0 = seeds[3 * s + 2];
+      if (o->sampvox) {
+        x0 += u[1] - 0.5f;
+        y0 += u[2] - 0.5f;
+        z0 += u[3] - 0.5f;
+      }
+      part_t P;
+      memset(&P, 0, sizeof(P));
+      int n1 = 0, n2 = 0;
+      const int rej1 = half_line(&T, &P, pid, 0, fibst, x0, y0, z0, path, &n1);
+      if (P.jumped) { /* Particle::restart_reverse */
+        P.rx = -P.rxi;
+        P.ry = -P.ryi;
+        P.rz = -P.rzi;
+      }
+      const int rej2 = half_line(&T, &P, pid, 1, fibst, x0, y0, z0, path + n1, &n2);
+      if (rej1 != 0 && rej2 != 0) continue;
+      ++kept;
+      const int from = rej1 == 0 ? 0 : n1, to = rej2 == 0 ? n1 + n2 : n1;
+      for (int i = from; i < to; ++i) {
+        const int64_t vx = path[i];
+        if (stamp[vx] != (int64_t)pid) {
+          stamp[vx] = (int64_t)pid;
+          paths[vx] += 1.0f;
+        }
+      }
+    }
+  }
+  *waytotal += kept;
+  free(path);
+  free(stamp);
+  return 0;
+}

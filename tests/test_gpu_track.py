@@ -1,0 +1,85 @@
+"""probtrackx simple mode on the GPU (bpx_probtrack_dev) against the CPU oracle, exactly.
+
+Both draw every step's random numbers from the same counter-based stream and do the same
+single-precision operations in the same order, so fdt_paths and waytotal must be identical, bit for
+bit (integer counts), for every option the kernel takes: the first fibre chosen by --fibst or at
+random (--randfib 1/2/3), --usef, --sampvox, --distthresh (the two-pass halves), short and long
+step counts, and on the outputs of this library's own bedpostx run.
+"""
+import numpy as np
+import pytest
+
+from fdt_b200 import synth
+from fdt_b200.abi import Options, TrackOptions
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+CASES = [
+    ("default", dict()),
+    ("randfib1", dict(randfib=1)),
+    ("randfib2", dict(randfib=2)),
+    ("randfib3", dict(randfib=3)),
+    ("usef", dict(usef=1)),
+    ("sampvox_fibst2", dict(sampvox=1, fibst=2)),
+    ("distthresh", dict(distthresh=6.0)),
+    ("short_steps_low_cthr", dict(nsteps=20, c_thr=0.0)),
+    ("steplength_1mm", dict(steplength=1.0)),
+]
+
+
+@pytest.mark.parametrize("name,kw", CASES, ids=[c[0] for c in CASES])
+def test_tracking_equals_oracle(torch, name, kw):
+    from fdt_b200 import lib
+
+    lib.load()
+    th, ph, f, mask = synth.fibre_field((20, 16, 10), nsamples=12, seed=4)
+    seeds = np.array([[5.0, 8.0, 5.0], [14.0, 7.0, 4.6], [10.3, 3.2, 5.5], [0.0, 0.0, 0.0]], np.float32)
+    o = TrackOptions.make(nparticles=200, nsteps=kw.pop("nsteps", 300), seed=17, **kw)
+    want_p, want_w = O.probtrack(o, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.5))
+    dev = [lib.to_device(a) for a in (th, ph, f, mask)]
+    got_p, got_w = lib.probtrack(o, *dev, seeds, voxel_size=(2.0, 2.0, 2.5))
+    torch.cuda.synchronize()
+    got_p = got_p.cpu().numpy()
+    assert got_w == want_w, (name, got_w, want_w)
+    assert np.array_equal(got_p, want_p), (name, np.argwhere(got_p != want_p)[:5])
+    assert want_p.sum() > 0
+
+
+def test_tracking_on_bedpostx_outputs_equals_oracle(torch):
+    from fdt_b200 import lib, nifti
+
+    lib.load()
+    # a small volume through this library's bedpostx, its merged samples tracked from two seeds
+    shape = (12, 10, 6)
+    mask = synth.ellipsoid_mask(shape, 400)
+    n = int(mask.sum())
+    prot = synth.three_shell(9, 90)
+    y, _ = synth.make_volume(n, prot, 2, True, 25.0, seed=8)
+    o = Options.make(model=2, nfibres=2, nburn=100, njumps=200, sampleevery=10)
+    out = lib.xfibres_dev(o, lib.to_device(y), lib.to_device(prot.bvecs), lib.to_device(prot.bvals))
+    torch.cuda.synchronize()
+    K, ns = 2, o.nsamples
+    vols = {}
+    for k in ("th", "ph", "f"):
+        a = out[k].cpu().numpy()  # [K][ns][n]
+        # merged_{k}{fibre}samples as volumes [x][y][z][ns], stored [fibre][ns][z][y][x]
+        v = np.stack([nifti.from_matrix(a[kk].T, mask) for kk in range(K)])  # [K][x][y][z][ns]
+        vols[k] = np.ascontiguousarray(np.transpose(v, (0, 4, 3, 2, 1)), np.float32)
+    m = np.ascontiguousarray(np.transpose(mask.astype(np.float32), (2, 1, 0)))
+    seeds = np.array([[6.0, 5.0, 3.0], [4.0, 4.0, 2.0]], np.float32)
+    t = TrackOptions.make(nparticles=300, nsteps=400, seed=5)
+    want_p, want_w = O.probtrack(t, vols["th"], vols["ph"], vols["f"], m, seeds)
+    got_p, got_w = lib.probtrack(t, *(lib.to_device(vols[k]) for k in ("th", "ph", "f")), lib.to_device(m), seeds)
+    torch.cuda.synchronize()
+    assert got_w == want_w and np.array_equal(got_p.cpu().numpy(), want_p)

@@ -1,0 +1,86 @@
+"""CPU checks of the probtrackx oracle (oracle/track_oracle.c): its sine/cosine is the GPU path's
+(same literals, single-precision accuracy), and tracking follows the reference's rules on fields
+whose answer is known: a straight tract is followed to the mask boundary in both directions and
+every voxel on it is counted once per streamline; the curvature threshold stops a streamline at a
+right-angle turn; the distance threshold drops short streamlines."""
+import os
+import re
+
+import numpy as np
+
+from fdt_b200 import synth
+from fdt_b200.abi import TrackOptions
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_sincos_literals_match_the_gpu_header():
+    hdr = open(os.path.join(ROOT, "fdt_b200", "csrc", "bpx_device.cuh")).read()
+    src = open(os.path.join(ROOT, "oracle", "track_oracle.c")).read()
+    for name in ("kSinQ", "kCosQ"):
+        h = re.search(name + r"\(int i\) \{ return (.*?); \}", hdr).group(1)
+        lits_h = [float(x.rstrip("f")) for x in re.findall(r"(-?[0-9.]+e?-?[0-9]*f)", h)]
+        c = re.search(r"static const float " + name + r"\[3\] = \{(.*?)\};", src).group(1)
+        lits_c = [float(x.strip().rstrip("f")) for x in c.split(",")]
+        assert np.array_equal(np.float32(lits_h), np.float32(lits_c)), name
+
+
+def test_sincos_fast_accuracy():
+    xs = np.concatenate([np.linspace(-50, 50, 2001), [0.0, np.pi / 2, np.pi, -np.pi / 4]]).astype(np.float32)
+    for x in xs:
+        s, c = O.sincos_fast(float(x))
+        assert abs(s - np.sin(np.float64(x))) < 3e-7 and abs(c - np.cos(np.float64(x))) < 3e-7, x
+
+
+def _straight_box(n=(30, 9, 9)):
+    nx, ny, nz = n
+    K, ns = 1, 10
+    th = np.full((K, ns, nz, ny, nx), np.pi / 2, np.float32)
+    # phi slightly off 0: the reference takes no step for a sample with theta or phi exactly 0
+    ph = np.full_like(th, 1e-4)
+    f = np.full_like(th, 0.6)
+    mask = np.zeros((nz, ny, nx), np.float32)
+    mask[2:7, 2:7, 3:27] = 1.0
+    return th, ph, f, mask
+
+
+def test_straight_tract_is_followed_both_ways_and_counted_once_per_streamline():
+    th, ph, f, mask = _straight_box()
+    o = TrackOptions.make(nparticles=50, nsteps=400, steplength=0.5, seed=3)
+    paths, way = O.probtrack(o, th, ph, f, mask, [[15.0, 4.0, 4.0]], voxel_size=(2.0, 2.0, 2.0))
+    assert way == 50
+    line = paths[4, 4, :]
+    assert np.all(line[3:27] == 50) and np.all(line[:3] == 0) and np.all(line[27:] == 0)
+    assert paths.sum() == line.sum()  # a straight path through voxel centres stays on its line
+
+
+def test_curvature_threshold_stops_at_a_right_angle_turn():
+    th, ph, f, mask = _straight_box()
+    ph[:, :, :, :, 20:] = np.pi / 2  # fibres turn to y at x = 20
+    mask[2:7, 2:7, 3:27] = 1.0
+    o = TrackOptions.make(nparticles=20, nsteps=400, c_thr=0.2, seed=5)
+    paths, way = O.probtrack(o, th, ph, f, mask, [[10.0, 4.0, 4.0]])
+    assert way == 20
+    # positions in [19.5, 20) round to the first turned voxel but may still draw their sample from
+    # voxel 19; no particle gets past x = 20, where both neighbours have turned
+    assert paths[4, 4, 19] == 20 and 0 < paths[4, 4, 20] <= 20 and paths[4, 4, 21:].sum() == 0
+    assert paths[4, 4, 3] == 20  # the other half reaches the boundary
+
+
+def test_distance_threshold_drops_short_halves():
+    th, ph, f, mask = _straight_box()
+    o = TrackOptions.make(nparticles=10, nsteps=400, distthresh=1000.0, seed=7)
+    paths, way = O.probtrack(o, th, ph, f, mask, [[15.0, 4.0, 4.0]])
+    assert way == 0 and paths.sum() == 0
+
+
+def test_crossing_field_options_run_and_conserve_counts():
+    th, ph, f, mask = synth.fibre_field((16, 14, 8), nsamples=8, seed=2)
+    seeds = [[4.0, 7.0, 4.0], [11.0, 6.0, 3.5]]
+    for kw in (dict(), dict(randfib=1), dict(randfib=2), dict(randfib=3), dict(usef=1), dict(sampvox=1),
+               dict(fibst=2)):
+        o = TrackOptions.make(nparticles=30, nsteps=200, seed=11, **kw)
+        paths, way = O.probtrack(o, th, ph, f, mask, seeds)
+        assert 0 < way <= 60, kw
+        assert paths.max() <= way and np.all(paths[mask == 0] == 0), kw
