@@ -434,7 +434,7 @@ def run_probtrack(args):
     th, ph, f, mask = synth.fibre_field((96, 96, 60), nsamples=50, seed=1)
     rng = np.random.default_rng(2)
     inside = np.argwhere(mask > 0)  # [z, y, x]
-    pick = inside[rng.choice(len(inside), 1024, replace=False)]
+    pick = inside[rng.choice(len(inside), args.track_seeds, replace=False)]
     seeds = np.ascontiguousarray(pick[:, ::-1].astype(np.float32))
     o = TrackOptions.make(seed=9)
     dev = [lib.to_device(a) for a in (th, ph, f, mask)]
@@ -478,7 +478,7 @@ def run_probtrack(args):
         "unit": "streamlines/s", "n_gpus": 1, "steps": k, "warmup": max(1, args.warmup), "ms_per_step": 1e3 * t,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
         "config": {"workload": "probtrackx simple mode: 96x96x60 crossing-fibre field, 3 fibres x 50 samples, "
-                   "1024 seeds x 5000 particles, 2000 steps of 0.5 mm, cthr 0.2, fibthresh 0.01",
+                   "%d seeds x 5000 particles, 2000 steps of 0.5 mm, cthr 0.2, fibthresh 0.01" % len(seeds),
                    "streamlines": n_lines, "waytotal": int(way.item()), "visits": float(paths.sum().item())},
         "cpu_baseline": {"value": nb * o.nparticles / t_cpu, "unit": "streamlines/s", "cores": 1, "kind": "port",
                          "sample": f"{nb} seed points x {o.nparticles} particles through the CPU oracle"},
@@ -517,6 +517,7 @@ def main():
     ap.add_argument("--batch-scale", type=float, default=0.5,
                     help="batched: voxel-count scale (also the C2 sub-record of the default line)")
     ap.add_argument("--no-c2", action="store_true", help="skip the C2 (mixed batch) sub-record")
+    ap.add_argument("--track-seeds", type=int, default=1024, help="probtrack: seed points")
     ap.add_argument("--no-whole-volume", action="store_true",
                     help="skip the one-call run of the ~900k-voxel whole-brain volume")
     ap.add_argument("--acc-voxels", type=int, default=4096, help="accuracy study: voxels")
