@@ -419,6 +419,81 @@ def run_c3(args):
     print(json.dumps(line), flush=True)
 
 
+def run_plain_config(args, name: str):
+    """The plain form (prepare, LM fits, MCMC burn-in 1000, finishing) on one whole volume of config
+    C0 (model 1, 2 fibres, 500 voxels, 64 measurements, SNR 20) or C1 (model 2, 3 fibres, 96x96x60
+    ellipsoid of ~200k voxels, 279 measurements, SNR 25), one call per step on device buffers, with
+    the fit and chain phases timed separately and the chain's roofline fraction."""
+    import ctypes as C
+
+    import torch
+
+    from fdt_b200 import lib
+
+    if name == "c0":
+        vol = synth.config_small_model1()
+        o = Options.make(model=1, nfibres=2)
+    else:
+        vol = synth.config_multishell_model2()
+        o = Options.make(model=2, nfibres=3)
+    prot, n, M = vol.prot, vol.nvox, vol.prot.ndir
+    L = lib.load()
+    d = lib.to_device(vol.data)
+    bv, bl = lib.to_device(prot.bvecs), lib.to_device(prot.bvals)
+    params = torch.empty((n, o.nparams_fit), device="cuda")
+    tau = torch.empty(n, device="cuda")
+    status = torch.zeros(n, device="cuda", dtype=torch.int32)
+    rec = torch.empty((6 + 3 * o.nfibres, o.nsamples, n), device="cuda")
+    out = lib.alloc_outputs(o, n)
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    vv = lib.make_volume(d, bv, bl)
+
+    def step(ev=None):
+        if ev:
+            ev[0].record(stream)
+        lib._check(L.bpx_fit_dev(C.byref(o), C.byref(vv), params.data_ptr(), tau.data_ptr(), status.data_ptr(), sp),
+                   "fit")
+        if ev:
+            ev[1].record(stream)
+        lib._check(L.bpx_mcmc_dev(C.byref(o), C.byref(vv), params.data_ptr(), tau.data_ptr(), rec.data_ptr(),
+                                  status.data_ptr(), sp), "mcmc")
+        if ev:
+            ev[2].record(stream)
+        lib._check(L.bpx_finish_dev(C.byref(o), n, rec.data_ptr(), C.byref(out[1]), sp), "finish")
+        if ev:
+            ev[3].record(stream)
+
+    for _ in range(max(1, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    k = max(1, args.steps)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(k)]
+    for e in evs:
+        step(e)
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ph = [sum(e[a].elapsed_time(e[a + 1]) for e in evs) / 1e3 / k for a in range(3)]
+    t = sum(ph)
+    mufu_peak, fma_peak = lib.measure_pipes()
+    mufu_v, fp32_v = mcmc_work_canonical(o, M)
+    frac = max(mufu_v * n / mufu_peak, fp32_v * n / fma_peak) / ph[1]
+    line = {
+        "metric": f"voxels/s, plain form on config {name.upper()} (1 B200)", "value": n / t, "unit": "voxels/s",
+        "n_gpus": 1, "steps": k, "warmup": max(1, args.warmup), "ms_per_step": 1e3 * t, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": f"config {name.upper()}: model {o.model}, {o.nfibres} fibres, {M} measurements, "
+                   f"{n} voxels, burnin 1000, njumps 1250, sampleevery 25, one call per volume"},
+        "phases_s": {"fit": ph[0], "mcmc": ph[1], "finish": ph[2]},
+        "mcmc_roofline": {"frac": frac, "bound": "fp32" if fp32_v / fma_peak > mufu_v / mufu_peak else "sfu",
+                          "counts": "canonical per-term counts, measured MUFU/FFMA peaks"},
+        "clocks": ck, "gpu_launches": 7 * k,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_probtrack(args):
     """probtrackx simple mode on the GPU: streamlines/s on a synthetic crossing-fibre field with the
     whole-brain sample count (96x96x60 grid, ellipsoidal mask, 3 fibres x 50 samples; fibre 1 along
@@ -511,7 +586,8 @@ def main():
     ap.add_argument("--freeze", type=int, default=0, choices=[0, 1, 2],
                     help="learned form: 0 network widths adapt, 1 frozen, 2 frozen after burn-in")
     ap.add_argument("--weights", default=None, help="initialiser weights (default: the committed whole-brain set)")
-    ap.add_argument("--workload", default="whole_brain", choices=["whole_brain", "batched", "c3", "probtrack"],
+    ap.add_argument("--workload", default="whole_brain",
+                    choices=["whole_brain", "batched", "c0", "c1", "c3", "probtrack"],
                     help="batched: the mixed 16-volume batch in one graph launch (one GPU); c3: the "
                          "279-measurement network on a 200k-voxel volume (one GPU)")
     ap.add_argument("--batch-scale", type=float, default=0.5,
@@ -549,6 +625,10 @@ def main():
     if args.workload == "probtrack":
         if rank == 0:
             run_probtrack(args)
+        return
+    if args.workload in ("c0", "c1"):
+        if rank == 0:
+            run_plain_config(args, args.workload)
         return
 
     import ctypes as C
