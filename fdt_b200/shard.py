@@ -45,26 +45,29 @@ def partition(nvox: int, world: int, cost: Sequence[float] | np.ndarray | None =
 def run_sharded(nvox: int, rank: int, world: int, run_range: Callable[[int, int], dict], dist=None,
                 cost=None) -> dict | None:
     """Runs `run_range(start, end)` for this rank's range and gathers the per-voxel outputs to
-    rank 0.  `run_range` returns a dict of CPU tensors whose LAST axis is the voxel axis (the
-    layout of every bpx output array).  Returns the assembled dict on rank 0, None elsewhere.
-    With world == 1 (or dist None) no collective is made."""
+    rank 0.  `run_range` returns a dict of tensors (CPU or CUDA) whose LAST axis is the voxel axis
+    (the layout of every bpx output array); the range's first voxel must key its chains
+    (bpx_volume.voxel_offset).  The gather goes through the process group's backend: CUDA tensors
+    for NCCL, CPU tensors for gloo.  Returns the assembled dict (CPU tensors) on rank 0, None
+    elsewhere.  With world == 1 (or dist None) no collective is made."""
     import torch
 
     ranges = partition(nvox, world, cost)
     start, end = ranges[rank]
     mine = run_range(start, end)
     if world == 1 or dist is None:
-        return mine
+        return {k: v.cpu() for k, v in mine.items()}
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend() == "nccl" else torch.device("cpu")
     keys = sorted(mine)
+    width = max(e - s for s, e in ranges)
     gathered = {}
     for k in keys:
-        t = mine[k].contiguous()
+        t = mine[k].contiguous().to(dev)
         # pad to the largest range so every rank sends the same shape
-        width = max(e - s for s, e in ranges)
-        pad = torch.zeros(t.shape[:-1] + (width,), dtype=t.dtype)
+        pad = torch.zeros(t.shape[:-1] + (width,), dtype=t.dtype, device=dev)
         pad[..., : t.shape[-1]] = t
         parts = [torch.zeros_like(pad) for _ in range(world)] if rank == 0 else None
         dist.gather(pad, gather_list=parts, dst=0)
         if rank == 0:
-            gathered[k] = torch.cat([parts[r][..., : ranges[r][1] - ranges[r][0]] for r in range(world)], dim=-1)
+            gathered[k] = torch.cat([parts[r][..., : ranges[r][1] - ranges[r][0]] for r in range(world)], dim=-1).cpu()
     return gathered if rank == 0 else None
