@@ -78,7 +78,8 @@ __device__ void finish_voxel(const FinishArgs& a, int v) {
 #pragma unroll
       for (int j = 0; j < 3; ++j) dy[k][i][j] = 0;
   }
-#pragma unroll 2
+  const bpx_outputs& out = a.out;
+  const bool copy = out.th || out.ph || out.f;
   for (int s = 0; s < ns; ++s) {
     const size_t o = (size_t)s * nvox;
 #pragma unroll
@@ -86,6 +87,7 @@ __device__ void finish_voxel(const FinishArgs& a, int v) {
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const float th = rec[(6 + 3 * k) * row + o], ph = rec[(7 + 3 * k) * row + o];
+      const float fk = rec[(8 + 3 * k) * row + o];
       float st, ct, sp, cp;
       sincosf(th, &st, &ct);
       sincosf(ph, &sp, &cp);
@@ -94,10 +96,15 @@ __device__ void finish_voxel(const FinishArgs& a, int v) {
       for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) dy[k][i][j] += x[i] * x[j];
-      sumf[k] += rec[(8 + 3 * k) * row + o];
+      sumf[k] += fk;
+      if (copy) {  // fibre k in output slot k: right unless the sort below moves it
+        const size_t oo = ((size_t)k * ns + s) * nvox + v;
+        if (out.th) out.th[oo] = th;
+        if (out.ph) out.ph[oo] = ph;
+        if (out.f) out.f[oo] = fk;
+      }
     }
   }
-  const bpx_outputs& out = a.out;
   const double inv = 1.0 / ns;
   if (out.mean_d) out.mean_d[v] = (float)(sums[0] * inv);
   if (out.mean_f0) out.mean_f0[v] = (float)(sums[1] * inv);
@@ -123,7 +130,7 @@ __device__ void finish_voxel(const FinishArgs& a, int v) {
 #pragma unroll
     for (int i = 0; i < K; ++i)
       if (order[o] == i) src = i;
-    if (out.th || out.ph || out.f) {
+    if (copy && src != o) {  // a fibre the sort moved: its samples are read again
       for (int s = 0; s < ns; ++s) {
         const size_t io = (size_t)s * nvox;
         const size_t oo = ((size_t)o * ns + s) * nvox + v;
@@ -152,9 +159,9 @@ __device__ void finish_voxel(const FinishArgs& a, int v) {
   }
 }
 
-// Grid-stride over voxels.  A voxel's records are read twice (sums and dyads first, then the
-// sorted copies of th/ph/f); the launch keeps few enough voxels in flight that their records are
-// still in L2 for the second read, so each record crosses HBM once.
+// One thread per voxel (grid-stride).  The records are read once: the samples are copied to the
+// outputs in fibre order as the sums are formed, and only the fibres the sort moves are copied
+// again (the chain keeps the fit's order, largest f first, in most voxels).
 template <int K>
 __global__ void finish_kernel(FinishArgs a) {
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < a.nvox; v += gridDim.x * blockDim.x) finish_voxel<K>(a, v);
@@ -229,17 +236,8 @@ cudaError_t launch_postproc(const PostArgs& a, cudaStream_t s) {
 
 cudaError_t launch_finish(const FinishArgs& a, cudaStream_t s) {
   if (a.nvox == 0) return cudaSuccess;
-  const int threads = 64;
-  int dev = 0, l2 = 0;
-  cudaGetDevice(&dev);
-  if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess || l2 <= 0) l2 = 32 << 20;
-  // voxels in flight whose records fill at most a third of L2 (the rest holds the outputs' lines)
-  const size_t per_voxel = (size_t)(6 + 3 * a.nfib) * a.nsamples * sizeof(float);
-  const size_t in_flight = (size_t)l2 / 3 / (per_voxel ? per_voxel : 1);
-  int grid = (int)((in_flight + threads - 1) / threads);
-  const int need = (a.nvox + threads - 1) / threads;
-  if (grid > need) grid = need;
-  if (grid < sm_count()) grid = sm_count() < need ? sm_count() : need;
+  const int threads = 128;
+  const int grid = (a.nvox + threads - 1) / threads;
   switch (a.nfib) {
     case 1: finish_kernel<1><<<grid, threads, 0, s>>>(a); break;
     case 2: finish_kernel<2><<<grid, threads, 0, s>>>(a); break;

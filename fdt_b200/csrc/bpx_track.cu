@@ -27,7 +27,7 @@ namespace bpx {
 namespace {
 
 constexpr int kTrackThreads = 64;
-constexpr int kTrackBlocksPerSm = 4;
+constexpr int kTrackBlocksPerSm = 8;  // 16 warps per SM to hide the gathers' latency (registers allow 10 blocks)
 
 struct TrackArgs {
   bpx_track_options o;
