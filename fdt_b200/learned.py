@@ -115,12 +115,13 @@ def state_from_record(opts: Options, rec, sample: int = 0):
 
 def make_training_set(opts: Options, bvecs: np.ndarray, bvals: np.ndarray, n: int, seed: int = 1,
                       snr=(10.0, 40.0), chunk: int = 131072, widths: bool = True,
-                      state_labels: str = "mean") -> TrainingSet:
+                      state_labels: str = "mean", label_samples: int = MEAN_LABEL_SAMPLES) -> TrainingSet:
     """n forward-model voxels (SNR ~ U(snr)) with their labels.  The plain chain is run from each
     voxel's LM fit through its full burn-in; its proposal widths at that point are the width
     labels, and the state labels are either that chain state (state_labels="chain": the state the
     LM-initialised chain reaches, which is where a chain with frozen widths must start), the
-    posterior mean over MEAN_LABEL_SAMPLES samples recorded after the burn-in ("mean", widths then
+    posterior mean over `label_samples` samples recorded after the burn-in ("mean"; with the plain
+    chain's 50 samples, the plain form's own posterior means; widths then
     taken at the end of that recording) or the LM fit itself ("lm")."""
     import torch
 
@@ -130,7 +131,7 @@ def make_training_set(opts: Options, bvecs: np.ndarray, bvals: np.ndarray, n: in
     x = torch.empty((n, nin(ndir)), device="cuda", dtype=torch.bfloat16)
     t = torch.empty((n, NOUT), device="cuda", dtype=torch.float32)
     w = torch.empty((n, NOUT), device="cuda", dtype=torch.float32)
-    lo = label_options(opts, MEAN_LABEL_SAMPLES if state_labels == "mean" else 1)
+    lo = label_options(opts, label_samples if state_labels == "mean" else 1)
     stream = lib._stream(torch)
     for s in range(0, n, chunk):
         m = min(chunk, n - s)
@@ -386,6 +387,8 @@ def main(argv=None) -> None:
     ap.add_argument("--out", default=None)
     ap.add_argument("--eval", type=int, default=8192, help="held-out voxels for the learned-vs-plain check")
     ap.add_argument("--labels", default="mean", choices=["chain", "mean", "lm"])
+    ap.add_argument("--label-samples", type=int, default=MEAN_LABEL_SAMPLES,
+                    help="--labels mean: samples (every sampleevery iterations) the labels average")
     ap.add_argument("--weights", default=None, help="evaluate these weights instead of training")
     a = ap.parse_args(argv)
     prot = PROTOCOLS[a.protocol](synth)
@@ -395,7 +398,8 @@ def main(argv=None) -> None:
         params, _ = load_weights(a.weights)
     else:
         t0 = time.time()
-        ts = make_training_set(opts, prot.bvecs, prot.bvals, a.n, seed=a.seed, state_labels=a.labels)
+        ts = make_training_set(opts, prot.bvecs, prot.bvals, a.n, seed=a.seed, state_labels=a.labels,
+                               label_samples=a.label_samples)
         t1 = time.time()
         params, losses = train(ts, a.steps, a.batch, a.lr, seed=a.seed, log_every=max(1, a.steps // 20))
         t2 = time.time()
@@ -404,7 +408,8 @@ def main(argv=None) -> None:
             print(f"  step {s:6d} loss {l:.5f}")
         out = a.out or default_weights_path(a.protocol)
         save(out, params, ndir=prot.ndir, model=2, nfibres=3, protocol=a.protocol, n_train=a.n, steps=a.steps,
-             seed=a.seed, labels=a.labels, bvals=prot.bvals, bvecs=prot.bvecs, options=oname,
+             seed=a.seed, labels=a.labels, label_samples=a.label_samples, bvals=prot.bvals, bvecs=prot.bvecs,
+             options=oname,
              rician=opts.rician, f0=opts.f0, ardf0=opts.ardf0)
         print("saved", out)
         del ts
