@@ -45,9 +45,10 @@ WORKLOAD_LEARNED = ("whole-brain: model 2, 3 fibres, rician+f0+ardf0, 288 measur
 
 
 # DRAM bytes (read + write) of one mcmc_kernel launch per voxel on the whole-brain workload, from
-# an ncu capture of a 131072-voxel launch: 313,204,224 B read + 441,731,584 B written.  The kernel
-# keeps its chain state on chip, so its traffic scales with voxels, not with iterations.
-MCMC_DRAM_BYTES_PER_VOXEL = (313204224 + 441731584) / 131072
+# an ncu capture of a 65536-voxel launch (the learned chain: 1450 iterations, 50 samples):
+# 122,633,984 B read + 169,972,992 B written.  The kernel keeps its chain state on chip, so its
+# traffic scales with voxels, not with iterations.
+MCMC_DRAM_BYTES_PER_VOXEL = (122633984 + 169972992) / 65536
 
 
 def whole_brain_options() -> Options:
@@ -878,8 +879,8 @@ def main():
         "bound": canon["bound"], "achieved": canon["achieved"], "peak": canon["peak"], "unit": "Gop/s",
         "frac": canon["frac"],
         "traffic": MCMC_DRAM_BYTES_PER_VOXEL * chunk if (o.model, o.nfibres, M, o.nsamples) == (2, 3, 288, 50) else None,
-        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one mcmc_kernel launch "
-                          "on this workload's options, per voxel, scaled by the voxels of this launch",
+        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 65536-voxel mcmc_kernel "
+                          "launch on this workload's options, per voxel, scaled by the voxels of this launch",
         "kernel": f"mcmc_kernel (burn-in + recording), timed in the {rf} form's step",
         "counts": "canonical per-term counts (model-2 signal rcp+log2+exp2, Rician log2+rsqrt; FMA 6 per signal "
                   "term, K+4(+12 Rician) per likelihood term)",

@@ -69,17 +69,34 @@ __device__ void finish_voxel(const FinishArgs& a, int v) {
   const int ns = a.nsamples, nvox = a.nvox;
   const size_t row = (size_t)ns * nvox;
   const float* rec = a.records + v;
-  double sums[6] = {0, 0, 0, 0, 0, 0}, sumf[K], dy[K][3][3];
+  // the fibre order first, from the sums of f over the samples (the f rows, a fifth of the
+  // records): sort (sum f, index) ascending and read it backwards (CUDA/samples.cu:299-330)
+  double sumf[K];
 #pragma unroll
-  for (int k = 0; k < K; ++k) {
-    sumf[k] = 0;
+  for (int k = 0; k < K; ++k) sumf[k] = 0;
+  for (int s = 0; s < ns; ++s) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) sumf[k] += rec[(8 + 3 * k) * row + (size_t)s * nvox];
+  }
+  int slot[K];  // output position of fibre k: the number of fibres that come before it
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    int rank = 0;
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+      if (j != i && (sumf[j] > sumf[i] || (sumf[j] == sumf[i] && j > i))) ++rank;
+    slot[i] = rank;
+  }
+  // one pass over the records: sums, dyadic tensors, and every sample copied to its sorted slot
+  // (each output row is written once, whole sectors at a time across the warp)
+  double sums[6] = {0, 0, 0, 0, 0, 0}, dy[K][3][3];
+#pragma unroll
+  for (int k = 0; k < K; ++k)
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
       for (int j = 0; j < 3; ++j) dy[k][i][j] = 0;
-  }
   const bpx_outputs& out = a.out;
-  const bool copy = out.th || out.ph || out.f;
   for (int s = 0; s < ns; ++s) {
     const size_t o = (size_t)s * nvox;
 #pragma unroll
@@ -87,7 +104,6 @@ __device__ void finish_voxel(const FinishArgs& a, int v) {
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const float th = rec[(6 + 3 * k) * row + o], ph = rec[(7 + 3 * k) * row + o];
-      const float fk = rec[(8 + 3 * k) * row + o];
       float st, ct, sp, cp;
       sincosf(th, &st, &ct);
       sincosf(ph, &sp, &cp);
@@ -96,13 +112,10 @@ __device__ void finish_voxel(const FinishArgs& a, int v) {
       for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) dy[k][i][j] += x[i] * x[j];
-      sumf[k] += fk;
-      if (copy) {  // fibre k in output slot k: right unless the sort below moves it
-        const size_t oo = ((size_t)k * ns + s) * nvox + v;
-        if (out.th) out.th[oo] = th;
-        if (out.ph) out.ph[oo] = ph;
-        if (out.f) out.f[oo] = fk;
-      }
+      const size_t oo = ((size_t)slot[k] * ns + s) * nvox + v;
+      if (out.th) out.th[oo] = th;
+      if (out.ph) out.ph[oo] = ph;
+      if (out.f) out.f[oo] = rec[(8 + 3 * k) * row + o];
     }
   }
   const double inv = 1.0 / ns;
@@ -112,33 +125,12 @@ __device__ void finish_voxel(const FinishArgs& a, int v) {
   if (out.mean_dstd) out.mean_dstd[v] = (float)(sums[3] * inv);
   if (out.mean_R) out.mean_R[v] = (float)(sums[4] * inv);
   if (out.mean_S0) out.mean_S0[v] = (float)(sums[5] * inv);
-  // order: sort (sum f, index) ascending and read it backwards (CUDA/samples.cu:299-330)
-  int order[K];
-#pragma unroll
-  for (int i = 0; i < K; ++i) {
-    int rank = 0;  // number of fibres that come before fibre i in the output
-#pragma unroll
-    for (int j = 0; j < K; ++j)
-      if (j != i && (sumf[j] > sumf[i] || (sumf[j] == sumf[i] && j > i))) ++rank;
-#pragma unroll
-    for (int o = 0; o < K; ++o)
-      if (o == rank) order[o] = i;
-  }
 #pragma unroll
   for (int o = 0; o < K; ++o) {
     int src = 0;
 #pragma unroll
     for (int i = 0; i < K; ++i)
-      if (order[o] == i) src = i;
-    if (copy && src != o) {  // a fibre the sort moved: its samples are read again
-      for (int s = 0; s < ns; ++s) {
-        const size_t io = (size_t)s * nvox;
-        const size_t oo = ((size_t)o * ns + s) * nvox + v;
-        if (out.th) out.th[oo] = rec[(6 + 3 * src) * row + io];
-        if (out.ph) out.ph[oo] = rec[(7 + 3 * src) * row + io];
-        if (out.f) out.f[oo] = rec[(8 + 3 * src) * row + io];
-      }
-    }
+      if (slot[i] == o) src = i;
     double sf = 0, A[3][3];
 #pragma unroll
     for (int i = 0; i < K; ++i)
@@ -159,9 +151,8 @@ __device__ void finish_voxel(const FinishArgs& a, int v) {
   }
 }
 
-// One thread per voxel (grid-stride).  The records are read once: the samples are copied to the
-// outputs in fibre order as the sums are formed, and only the fibres the sort moves are copied
-// again (the chain keeps the fit's order, largest f first, in most voxels).
+// One thread per voxel (grid-stride).  The f rows are read first to fix the fibre order, then
+// every record once more while the sums are formed and the samples copied to their sorted slots.
 template <int K>
 __global__ void finish_kernel(FinishArgs a) {
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < a.nvox; v += gridDim.x * blockDim.x) finish_voxel<K>(a, v);

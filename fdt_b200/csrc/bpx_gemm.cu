@@ -199,24 +199,62 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int col0 = n0 + c * 32;
     if (!done || row >= g.M || col0 >= g.N) continue;
     const int ncol = min(32, g.N - col0);
-    if (g.epi == kEpiStoreF32) {
+    // each lane owns one output row: a full, 16-byte aligned run of 32 columns is written with
+    // 16-byte stores (8 per FP32 row, 4 per BF16 row), anything else element by element
+    auto aligned16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+    if (g.epi == kEpiStoreF32 || g.epi == kEpiBias) {
       float* o = g.out_f32 + (size_t)row * g.ld_out + col0;
-      for (int j = 0; j < ncol; ++j) o[j] = v[j];
-    } else if (g.epi == kEpiBias) {
-      float* o = g.out_f32 + (size_t)row * g.ld_out + col0;
-      for (int j = 0; j < ncol; ++j) o[j] = v[j] + g.bias[col0 + j];
+      if (g.epi == kEpiBias)
+        for (int j = 0; j < ncol; ++j) v[j] += g.bias[col0 + j];
+      if (ncol == 32 && aligned16(o)) {
+#pragma unroll
+        for (int j = 0; j < 32; j += 4) *reinterpret_cast<float4*>(o + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+      } else {
+        for (int j = 0; j < ncol; ++j) o[j] = v[j];
+      }
     } else if (g.epi == kEpiBiasGelu) {
       uint16_t* a = g.out_bf16 + (size_t)row * g.ld_bf16 + col0;
       float* z = g.out_f32 ? g.out_f32 + (size_t)row * g.ld_out + col0 : nullptr;
-      for (int j = 0; j < ncol; ++j) {
-        const float zz = v[j] + g.bias[col0 + j];
-        if (z) z[j] = zz;
-        a[j] = to_bf16(gelu(zz));
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = j < ncol ? v[j] + g.bias[col0 + j] : 0.f;
+      if (z) {
+        if (ncol == 32 && aligned16(z)) {
+#pragma unroll
+          for (int j = 0; j < 32; j += 4) *reinterpret_cast<float4*>(z + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+        } else {
+          for (int j = 0; j < ncol; ++j) z[j] = v[j];
+        }
+      }
+      if (ncol == 32 && aligned16(a)) {
+#pragma unroll
+        for (int j = 0; j < 32; j += 8) {
+          uint4 q;
+          q.x = (uint32_t)to_bf16(gelu(v[j])) | ((uint32_t)to_bf16(gelu(v[j + 1])) << 16);
+          q.y = (uint32_t)to_bf16(gelu(v[j + 2])) | ((uint32_t)to_bf16(gelu(v[j + 3])) << 16);
+          q.z = (uint32_t)to_bf16(gelu(v[j + 4])) | ((uint32_t)to_bf16(gelu(v[j + 5])) << 16);
+          q.w = (uint32_t)to_bf16(gelu(v[j + 6])) | ((uint32_t)to_bf16(gelu(v[j + 7])) << 16);
+          *reinterpret_cast<uint4*>(a + j) = q;
+        }
+      } else {
+        for (int j = 0; j < ncol; ++j) a[j] = to_bf16(gelu(v[j]));
       }
     } else {  // kEpiGeluGrad: dZ = (dZ_next W) * gelu'(z)
       uint16_t* d = g.out_bf16 + (size_t)row * g.ld_bf16 + col0;
       const float* z = g.zin + (size_t)row * g.ld_zin + col0;
-      for (int j = 0; j < ncol; ++j) d[j] = to_bf16(v[j] * gelu_grad(z[j]));
+      if (ncol == 32 && aligned16(d) && aligned16(z)) {
+#pragma unroll
+        for (int j = 0; j < 32; j += 8) {
+          const float4 z0 = *reinterpret_cast<const float4*>(z + j), z1 = *reinterpret_cast<const float4*>(z + j + 4);
+          uint4 q;
+          q.x = (uint32_t)to_bf16(v[j] * gelu_grad(z0.x)) | ((uint32_t)to_bf16(v[j + 1] * gelu_grad(z0.y)) << 16);
+          q.y = (uint32_t)to_bf16(v[j + 2] * gelu_grad(z0.z)) | ((uint32_t)to_bf16(v[j + 3] * gelu_grad(z0.w)) << 16);
+          q.z = (uint32_t)to_bf16(v[j + 4] * gelu_grad(z1.x)) | ((uint32_t)to_bf16(v[j + 5] * gelu_grad(z1.y)) << 16);
+          q.w = (uint32_t)to_bf16(v[j + 6] * gelu_grad(z1.z)) | ((uint32_t)to_bf16(v[j + 7] * gelu_grad(z1.w)) << 16);
+          *reinterpret_cast<uint4*>(d + j) = q;
+        }
+      } else {
+        for (int j = 0; j < ncol; ++j) d[j] = to_bf16(v[j] * gelu_grad(z[j]));
+      }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
