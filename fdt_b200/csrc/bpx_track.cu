@@ -93,9 +93,10 @@ struct Tracker {
     return false;  // unreachable: the table holds twice the longest path
   }
 
-  // Tractvolsx::sample
-  __device__ void sample(const Particle& P, const float (&u)[8], bool& init_sample, int& fibst, float& th, float& ph,
-                         float& f) const {
+  // The voxel and posterior sample a step reads (the probabilistic rounding of Tractvolsx::sample):
+  // depends only on the position and the step's uniforms, so its loads can be issued together
+  // with the mask's.
+  __device__ void locate(const Particle& P, const float (&u)[8], size_t& vox, int& samp) const {
     const bpx_track_volume& v = a.v;
     const int cx = (int)ceilf(P.x), fx = (int)floorf(P.x);
     const int cy = (int)ceilf(P.y), fy = (int)floorf(P.y);
@@ -106,9 +107,15 @@ struct Tracker {
     const int nx_ = clampi(u[0] > pcx ? fx : cx, 0, v.nx - 1);
     const int ny_ = clampi(u[1] > pcy ? fy : cy, 0, v.ny - 1);
     const int nz_ = clampi(u[2] > pcz ? fz : cz, 0, v.nz - 1);
-    const size_t vox = ((size_t)nz_ * v.ny + ny_) * v.nx + nx_;
-    const int samp = clampi(rnd(u[3] * (float)(v.nsamples - 1)), 0, v.nsamples - 1);
-    const int K = v.nfib;
+    vox = ((size_t)nz_ * v.ny + ny_) * v.nx + nx_;
+    samp = clampi(rnd(u[3] * (float)(v.nsamples - 1)), 0, v.nsamples - 1);
+  }
+
+  // The fibre choice of Tractvolsx::sample on the voxel's sample (every fibre's th, ph, f loaded)
+  __device__ void choose(const Particle& P, const float (&u)[8], const float (&sth)[BPX_MAX_FIBRES],
+                         const float (&sph)[BPX_MAX_FIBRES], const float (&sf)[BPX_MAX_FIBRES], bool& init_sample,
+                         int& fibst, float& th, float& ph, float& f) const {
+    const int K = a.v.nfib;
     const float thr = a.o.fibthresh;
     float theta = 0.f, phi = 0.f;
     int fibind = 0;
@@ -116,63 +123,74 @@ struct Tracker {
       if (init_sample) {
         if (a.o.randfib == 1) {
           int list[BPX_MAX_FIBRES], n = 0;
-          for (int k = 0; k < K; ++k)
-            if (__ldg(v.f + at(k, samp, vox)) > thr) list[n++] = k;
+#pragma unroll
+          for (int k = 0; k < BPX_MAX_FIBRES; ++k)
+            if (k < K && sf[k] > thr) list[n++] = k;
           fibst = n == 0 ? 0 : list[clampi(rnd(u[4] * (float)(n - 1)), 0, n - 1)];
         } else if (a.o.randfib == 2) {
           float fsum = 0.f;
-          for (int k = 0; k < K; ++k) {
-            const float ft = __ldg(v.f + at(k, samp, vox));
-            if (ft > thr) fsum += ft;
-          }
+#pragma unroll
+          for (int k = 0; k < BPX_MAX_FIBRES; ++k)
+            if (k < K && sf[k] > thr) fsum += sf[k];
           if (fsum == 0.f) {
             fibst = 0;
           } else {
             const float r = fsum * u[4];
             float cum = 0.f;
-            for (int k = 0; k < K; ++k) {
-              const float ft = __ldg(v.f + at(k, samp, vox));
-              if (ft > thr) cum += ft;
-              if (r <= cum) {
-                fibst = k;
-                break;
+            bool found = false;
+#pragma unroll
+            for (int k = 0; k < BPX_MAX_FIBRES; ++k) {
+              if (k < K && !found) {
+                if (sf[k] > thr) cum += sf[k];
+                if (r <= cum) {
+                  fibst = k;
+                  found = true;
+                }
               }
             }
           }
         }
-        theta = __ldg(v.th + at(fibst, samp, vox));
-        phi = __ldg(v.ph + at(fibst, samp, vox));
+#pragma unroll
+        for (int k = 0; k < BPX_MAX_FIBRES; ++k)
+          if (k == fibst) {
+            theta = sth[k];
+            phi = sph[k];
+          }
         init_sample = false;
       } else {
         const float px = P.rx, py = P.ry, pz = P.rz;  // no preferred-direction volume
         float dotmax = 0.f;
-        for (int k = 0; k < K; ++k) {
-          if (__ldg(v.f + at(k, samp, vox)) > thr) {
-            const float pht = __ldg(v.ph + at(k, samp, vox)), tht = __ldg(v.th + at(k, samp, vox));
+#pragma unroll
+        for (int k = 0; k < BPX_MAX_FIBRES; ++k) {
+          if (k < K && sf[k] > thr) {
             float st, ct, sp, cp;
-            sincos_fast(tht, st, ct);
-            sincos_fast(pht, sp, cp);
+            sincos_fast(sth[k], st, ct);
+            sincos_fast(sph[k], sp, cp);
             const float dot = fabsf(st * cp * px + st * sp * py + ct * pz);
             if (dot > dotmax) {
               dotmax = dot;
-              theta = tht;
-              phi = pht;
+              theta = sth[k];
+              phi = sph[k];
               fibind = k;
             }
           }
         }
         if (dotmax == 0.f) {
-          theta = __ldg(v.th + at(0, samp, vox));
-          phi = __ldg(v.ph + at(0, samp, vox));
+          theta = sth[0];
+          phi = sph[0];
         }
       }
     } else {
-      theta = __ldg(v.th + at(0, samp, vox));
-      phi = __ldg(v.ph + at(0, samp, vox));
+      theta = sth[0];
+      phi = sph[0];
     }
     th = theta;
     ph = phi;
-    f = a.o.usef ? __ldg(v.f + at(fibind, samp, vox)) : 1.0f;
+    float ff = sf[0];
+#pragma unroll
+    for (int k = 1; k < BPX_MAX_FIBRES; ++k)
+      if (k == fibind) ff = sf[k];
+    f = a.o.usef ? ff : 1.0f;
   }
 
   // Streamliner::streamline for one half; counts the path's first visits when `count`.
@@ -186,17 +204,31 @@ struct Tracker {
     P.y = y0;
     P.z = z0;
     float pathlength = 0.f;
+    const int K = a.v.nfib;
     for (int it = 1; it <= o.nsteps / 2; ++it) {
       const int ix = rnd(P.x), iy = rnd(P.y), iz = rnd(P.z);
+      // this step's uniforms and sampled voxel, then the mask and every fibre's sample in one
+      // round of loads (the reference reads the sample only inside the mask: same values)
+      float u[8], th, ph, f;
+      track_uniforms(o.seed, pid, h, (uint32_t)it, u);
+      size_t svox;
+      int samp;
+      locate(P, u, svox, samp);
+      float sth[BPX_MAX_FIBRES], sph[BPX_MAX_FIBRES], sf[BPX_MAX_FIBRES];
+#pragma unroll
+      for (int k = 0; k < BPX_MAX_FIBRES; ++k) {
+        const size_t q = at(k < K ? k : 0, samp, svox);
+        sth[k] = __ldg(a.v.th + q);
+        sph[k] = __ldg(a.v.ph + q);
+        sf[k] = __ldg(a.v.f + q);
+      }
       if (!inside(ix, iy, iz)) break;  // the reference's remaining steps change nothing
       if (count) {
         const uint32_t vox = (uint32_t)(((size_t)iz * a.v.ny + iy) * a.v.nx + ix);
         if (first_visit(vox)) atomicAdd(a.paths + vox, 1.0f);
       }
       pathlength += o.steplength;
-      float u[8], th, ph, f;
-      track_uniforms(o.seed, pid, h, (uint32_t)it, u);
-      sample(P, u, init_sample, fibst, th, ph, f);
+      choose(P, u, sth, sph, sf, init_sample, fibst, th, ph, f);
       if (f > u[5]) {
         float st, ct, sp, cp;
         sincos_fast(th, st, ct);
@@ -346,10 +378,14 @@ bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volu
   int log2n = 1;
   while ((1ll << log2n) < 2ll * (opts->nsteps + 2)) ++log2n;
   a.log2n = log2n;
-  const int grid = sm_count() * kTrackBlocksPerSm;
+  // particles in flight: 8 blocks per SM, fewer when the tables of very long paths would pass 8 GB
+  const size_t table_bytes = ((size_t)1 << log2n) * sizeof(uint2);
+  const size_t max_blocks = ((size_t)8 << 30) / (table_bytes * kTrackThreads);
+  int grid = sm_count() * kTrackBlocksPerSm;
+  if ((size_t)grid > max_blocks) grid = max_blocks > 0 ? (int)max_blocks : 1;
   const size_t threads = (size_t)grid * kTrackThreads;
   void* ws = nullptr;
-  st = api_workspace(kWsTrack, threads * ((size_t)1 << log2n) * sizeof(uint2), &ws);
+  st = api_workspace(kWsTrack, threads * table_bytes, &ws);
   if (st != BPX_OK) return st;
   a.tables = (uint2*)ws;
   cudaStream_t s = (cudaStream_t)stream;
@@ -357,7 +393,7 @@ bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volu
   const uint64_t chunk = 1ull << 30;  // stamps stay below 2^30 + 1 within a launch
   for (uint64_t b = 0; b < total; b += chunk) {
     // stamp 0 marks every entry empty before a launch reuses the tables
-    const cudaError_t e0 = cudaMemsetAsync(ws, 0, threads * ((size_t)1 << log2n) * sizeof(uint2), s);
+    const cudaError_t e0 = cudaMemsetAsync(ws, 0, threads * table_bytes, s);
     if (e0 != cudaSuccess) return api_cuda_fail(e0, "bpx_probtrack_dev: cudaMemsetAsync");
     a.pid_begin = b;
     a.pid_end = b + chunk < total ? b + chunk : total;

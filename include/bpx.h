@@ -473,7 +473,7 @@ void bpx_track_options_default(bpx_track_options* opts);
  * paths [nz][ny][nx] (float counts, fdt_paths) and the kept streamlines to *waytotal (device
  * int64); the caller zeroes both first.  Uses workspace memory (see Concurrency) of
  * 8 * 2^ceil(log2(2 * (nsteps + 2))) bytes per particle in flight (512 particles per
- * multiprocessor: 2.5 GB on a B200 at nsteps 2000).
+ * multiprocessor, fewer if that passes 8 GB: 2.5 GB on a B200 at nsteps 2000).
  */
 bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volume* vol, int32_t nseeds,
                              const float* seeds, float* paths, int64_t* waytotal, void* stream);
