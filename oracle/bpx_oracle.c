@@ -867,6 +867,16 @@ int orc_lm_start(int kind, int nfib, int f0, int ndir, const float* y, const flo
   return 0;
 }
 
+/* orc_lm_start for every voxel of a volume [nvox][ndir] (OpenMP over voxels): p [nvox][np] */
+int orc_lm_starts(int kind, int nfib, int f0, int nvox, int ndir, const float* data, const float* bvecs,
+                  const float* bvals, double* p, int nthreads) {
+  const int np = 3 * nfib + 2 + (f0 ? 1 : 0);
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads)
+  for (int v = 0; v < nvox; ++v)
+    orc_lm_start(kind, nfib, f0, ndir, data + (size_t)v * ndir, bvecs, bvals, p + (size_t)v * np);
+  return 0;
+}
+
 /* fit one model from start values; returns finalised params */
 static int fit_model(int kind, int nfib, int f0, int gbo, double R, int ndir, const float* y,
                      const float* bvecs, const float* bvals, const double* start, double* out, int* capped) {

@@ -63,6 +63,9 @@ int orc_fit(const bpx_options* opts, int nvox, int ndir, const float* data, cons
 /* Start parameters of one LM model (before the fit): kind 0 PVM_single, 1 PVM_single_c. */
 int orc_lm_start(int kind, int nfib, int f0, int ndir, const float* y, const float* bvecs,
                  const float* bvals, double* p);
+/* orc_lm_start for every voxel of data [nvox][ndir]; p [nvox][np] */
+int orc_lm_starts(int kind, int nfib, int f0, int nvox, int ndir, const float* data, const float* bvecs,
+                  const float* bvals, double* p, int nthreads);
 /* One LM model fit from given start parameters, returning finalised parameters.
  * kind 0 single, 1 single_c, 2 multi (start = finalised PVM_single params), with
  * gamma_ball_only 0 (model 2) or 2 (model 3).  Returns the number of LM iterations. */

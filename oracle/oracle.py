@@ -44,6 +44,8 @@ def lib():
         L.orc_fit.argtypes = [C.POINTER(Options), C.c_int, C.c_int, _f32p, _f32p, _f32p, _f64p,
                               C.c_void_p, C.c_void_p, C.c_int]
         L.orc_lm_start.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p, _f64p]
+        L.orc_lm_starts.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p, _f64p,
+                                    C.c_int]
         L.orc_lm_fit.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, _f32p,
                                  _f32p, _f32p, _f64p, _f64p]
         L.orc_lm_eval.restype = C.c_double
@@ -121,6 +123,16 @@ def lm_start(kind: int, nfib: int, f0: bool, y, bvecs, bvals) -> np.ndarray:
     lib().orc_lm_start(kind, nfib, int(f0), len(y), np.ascontiguousarray(y, np.float32),
                        np.ascontiguousarray(bvecs, np.float32),
                        np.ascontiguousarray(bvals, np.float32), p)
+    return p
+
+
+def lm_starts(kind: int, nfib: int, f0: bool, data, bvecs, bvals, nthreads: int | None = None) -> np.ndarray:
+    """Start parameters of every voxel of data [nvox][ndir] (DTI + the model's start rule)."""
+    data = np.ascontiguousarray(data, np.float32)
+    nvox, ndir = data.shape
+    p = np.zeros((nvox, 3 * nfib + 2 + (1 if f0 else 0)))
+    lib().orc_lm_starts(kind, nfib, int(f0), nvox, ndir, data, np.ascontiguousarray(bvecs, np.float32),
+                        np.ascontiguousarray(bvals, np.float32), p, nthreads or nthreads_default())
     return p
 
 

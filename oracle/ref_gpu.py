@@ -57,6 +57,7 @@ def lib():
     if _lib is None:
         L = C.CDLL(LIB)
         L.refgpu_last_error.restype = C.c_char_p
+        L.refgpu_last_times.argtypes = [_f32p]
         L.refgpu_lm_eval.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int, _f32p, _f32p,
                                      _f32p, _f32p, _f64p, _f32p, _f32p]
         L.refgpu_fit.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int, _f32p, _f32p, _f32p,
@@ -129,3 +130,11 @@ def mcmc(opts: Options, data, bvecs, bvals, params, tau=None, seed: float = 8665
     _check(lib().refgpu_mcmc(C.byref(o), nvox, ndir, data, _f32(bvecs), _f32(bvals), _f32(params), t, None, None,
                              rec.ctypes.data), "refgpu_mcmc")
     return rec
+
+
+def last_times() -> tuple[float, float, float]:
+    """Device milliseconds of the last fit (fit kernels) and chain (init + randoms + burn-in;
+    recording) calls, CUDA events around the kernels only."""
+    ms = np.zeros(3, np.float32)
+    lib().refgpu_last_times(ms)
+    return float(ms[0]), float(ms[1]), float(ms[2])

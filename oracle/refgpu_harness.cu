@@ -45,6 +45,7 @@ namespace {
   } while (0)
 
 char g_err[512] = "";
+float g_ms[3] = {0.f, 0.f, 0.f};  // device time of the last call's kernels: fit; MCMC init + burn-in; recording
 
 // device buffer that frees itself
 template <typename T>
@@ -141,6 +142,12 @@ extern "C" {
 
 const char* refgpu_last_error(void) { return g_err; }
 
+// device milliseconds (CUDA events around the kernels only) of the last refgpu_fit (ms[0]) and
+// refgpu_mcmc (ms[1]: init_Fibres_Multifibres + randoms + burn-in; ms[2]: recording) calls
+void refgpu_last_times(float* ms) {
+  for (int i = 0; i < 3; ++i) ms[i] = g_ms[i];
+}
+
 // Cost (double), gradient and Hessian (float) of the reference's LM models at raw parameters
 // params [nvox][nparams]; see lm_eval_kernel.
 int refgpu_lm_eval(int kind, int nfib, int f0, int gbo, float R, int nvox, int ndir, const float* data,
@@ -187,6 +194,11 @@ int refgpu_fit(int kind, int nfib, int f0, int gbo, float R, int nvox, int ndir,
   RG_CUDA(d_in.put(start, (size_t)nvox * np_in));
   if (nvox == 0) return 0;
   const dim3 grid(nvox), block(THREADS_BLOCK_FIT);
+  if (kind == 2) RG_CUDA(d_out.alloc((size_t)nvox * np));
+  cudaEvent_t e0, e1;
+  RG_CUDA(cudaEventCreate(&e0));
+  RG_CUDA(cudaEventCreate(&e1));
+  RG_CUDA(cudaEventRecord(e0));
   if (kind == 0) {
     // CUDA/diffmodels.cu:98-104
     const int shared = 6 * sizeof(double) +
@@ -195,8 +207,6 @@ int refgpu_fit(int kind, int nfib, int f0, int gbo, float R, int nvox, int ndir,
     fit_PVM_single_kernel<<<grid, block, shared>>>(d_data.p, d_bvecs.p, d_bvals.p, nvox, ndir, nfib, np, f0 != 0,
                                                   false, d_in.p);
     RG_CUDA(cudaGetLastError());
-    RG_CUDA(cudaDeviceSynchronize());
-    RG_CUDA(d_in.get(params_out, (size_t)nvox * np));
   } else if (kind == 1) {
     // CUDA/diffmodels.cu:182-188
     const int shared = 6 * sizeof(double) +
@@ -206,11 +216,8 @@ int refgpu_fit(int kind, int nfib, int f0, int gbo, float R, int nvox, int ndir,
     fit_PVM_single_c_kernel<<<grid, block, shared>>>(d_data.p, d_bvecs.p, d_bvals.p, nvox, ndir, nfib, np, false,
                                                     f0 != 0, false, false, d_in.p);
     RG_CUDA(cudaGetLastError());
-    RG_CUDA(cudaDeviceSynchronize());
-    RG_CUDA(d_in.get(params_out, (size_t)nvox * np));
   } else {
     // CUDA/diffmodels.cu:232-240
-    RG_CUDA(d_out.alloc((size_t)nvox * np));
     const int shared = 6 * sizeof(double) +
                        (THREADS_BLOCK_FIT * np + THREADS_BLOCK_FIT + 5 * np + 2 * np * np + 4 * nfib + 3) * sizeof(float) +
                        (2 + np) * sizeof(int);
@@ -218,9 +225,13 @@ int refgpu_fit(int kind, int nfib, int f0, int gbo, float R, int nvox, int ndir,
     fit_PVM_multi_kernel<<<grid, block, shared>>>(d_data.p, d_in.p, d_bvecs.p, d_bvals.p, R, invR, nvox, ndir, nfib,
                                                  np, gbo, f0 != 0, false, d_out.p);
     RG_CUDA(cudaGetLastError());
-    RG_CUDA(cudaDeviceSynchronize());
-    RG_CUDA(d_out.get(params_out, (size_t)nvox * np));
   }
+  RG_CUDA(cudaEventRecord(e1));
+  RG_CUDA(cudaDeviceSynchronize());
+  RG_CUDA(cudaEventElapsedTime(&g_ms[0], e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  RG_CUDA((kind == 2 ? d_out : d_in).get(params_out, (size_t)nvox * np));
   return 0;
 }
 
@@ -274,6 +285,11 @@ int refgpu_mcmc(const refgpu_mcmc_opts* o, int nvox, int ndir, const float* data
   RG_CUDA(cudaMemset(d_fib.p, 0, sizeof(FibreGPU) * npad * K));
   RG_CUDA(cudaMemset(d_mf.p, 0, sizeof(MultifibreGPU) * npad));
   const dim3 grid(npad / VOXELS_BLOCK_MCMC), block(THREADS_VOXEL_MCMC * VOXELS_BLOCK_MCMC);
+  // event pairs around the kernels only (not the allocations between them): init, randoms, burn-in,
+  // recording
+  cudaEvent_t ev[8];
+  for (int i = 0; i < 8; ++i) RG_CUDA(cudaEventCreate(&ev[i]));
+  RG_CUDA(cudaEventRecord(ev[0]));
   // CUDA/runmcmc.cu:86-89
   const int sh_init =
       VOXELS_BLOCK_MCMC * ((THREADS_VOXEL_MCMC) * sizeof(double) + (3 * K + 9) * sizeof(float) + sizeof(int));
@@ -282,6 +298,7 @@ int refgpu_mcmc(const refgpu_mcmc_opts* o, int nvox, int ndir, const float* data
       o->model, o->fudge, o->f0 != 0, o->rician != 0, o->ardf0 != 0, o->all_ard != 0, o->no_ard != 0, false,
       d_angtmp.p, d_fib.p, d_mf.p, d_signals.p, d_iso.p);
   RG_CUDA(cudaGetLastError());
+  RG_CUDA(cudaEventRecord(ev[1]));
   RG_CUDA(cudaDeviceSynchronize());
   if (lik || prior) {
     std::vector<MultifibreGPU> mf(npad);
@@ -291,13 +308,18 @@ int refgpu_mcmc(const refgpu_mcmc_opts* o, int nvox, int ndir, const float* data
       if (prior) prior[v] = mf[v].m_prior_en;
     }
   }
-  if (!records) return 0;
+  if (!records) {
+    for (int i = 0; i < 8; ++i) cudaEventDestroy(ev[i]);
+    return 0;
+  }
   // setup_randoms_kernel (CUDA/runmcmc.cu:92-99)
   Buf<curandState> d_rand;
   RG_CUDA(d_rand.alloc(npad));
   const int rblocks = (npad + THREADS_BLOCK_RAND - 1) / THREADS_BLOCK_RAND;
+  RG_CUDA(cudaEventRecord(ev[2]));
   setup_randoms_kernel<<<rblocks, THREADS_BLOCK_RAND>>>(d_rand.p, o->seed, npad);
   RG_CUDA(cudaGetLastError());
+  RG_CUDA(cudaEventRecord(ev[3]));
   // runmcmc_kernel launches (CUDA/runmcmc.cu:135-200, 237-311)
   int nparams = (o->f0 ? 3 : 2) + 3 * K;
   if (o->model >= 2) nparams++;
@@ -324,6 +346,7 @@ int refgpu_mcmc(const refgpu_mcmc_opts* o, int nvox, int ndir, const float* data
     RG_CUDA(cudaMemset(b->p, 0, b->n * sizeof(float)));
   const int sh_mcmc = VOXELS_BLOCK_MCMC * ((THREADS_VOXEL_MCMC) * sizeof(double) + (10 * K + 27) * sizeof(float) +
                                            (7 * K + 20) * sizeof(int) + sizeof(curandState));
+  RG_CUDA(cudaEventRecord(ev[4]));
   if (o->nburn > 0) {
     runmcmc_kernel<<<grid, block, sh_mcmc>>>(
         d_data.p, d_bvals.p, d_alpha.p, d_beta.p, d_rand.p, o->R_mean, o->R_std, o->R_fudge, ndir, K, nparams, o->model,
@@ -332,13 +355,22 @@ int refgpu_mcmc(const refgpu_mcmc_opts* o, int nvox, int ndir, const float* data
         r_null.p, r_null.p, r_null.p, r_null.p, r_null.p, r_null.p);
     RG_CUDA(cudaGetLastError());
   }
+  RG_CUDA(cudaEventRecord(ev[5]));
   runmcmc_kernel<<<grid, block, sh_mcmc>>>(
       d_data.p, d_bvals.p, d_alpha.p, d_beta.p, d_rand.p, o->R_mean, o->R_std, o->R_fudge, ndir, K, nparams, o->model,
       o->fudge, o->f0 != 0, o->ardf0 != 0, !o->no_ard, o->rician != 0, false, o->upe, o->njumps, o->nburn,
       o->sampleevery, ns, d_oldsig.p, d_oldiso.p, d_angtmp.p, d_oldang.p, d_fib.p, d_mf.p, d_signals.p, d_iso.p,
       rf0.p, rtau.p, rs0.p, rd.p, rdstd.p, rR.p, rth.p, rph.p, rf.p);
   RG_CUDA(cudaGetLastError());
+  RG_CUDA(cudaEventRecord(ev[6]));
   RG_CUDA(cudaDeviceSynchronize());
+  float t_init = 0.f, t_rand = 0.f, t_burn = 0.f;
+  RG_CUDA(cudaEventElapsedTime(&t_init, ev[0], ev[1]));
+  RG_CUDA(cudaEventElapsedTime(&t_rand, ev[2], ev[3]));
+  RG_CUDA(cudaEventElapsedTime(&t_burn, ev[4], ev[5]));
+  RG_CUDA(cudaEventElapsedTime(&g_ms[2], ev[5], ev[6]));
+  g_ms[1] = t_init + t_rand + t_burn;
+  for (int i = 0; i < 8; ++i) cudaEventDestroy(ev[i]);
   // the reference's record arrays: r[vox*ns + s] and rk[vox*ns*K + k*ns + s]
   std::vector<float> h1(n1), hk(nk);
   const Buf<float>* rows1[6] = {&rd, &rf0, &rtau, &rdstd, &rR, &rs0};

@@ -265,3 +265,45 @@ def test_chains_match_reference(torch, name, kw, pname, gamma, n, r_orc):
             assert got_o["f_within_2se"][k] >= max(0.85, yard_o["f_within_2se"][k] - 0.04), (name, k, got_o, yard_o)
         assert got_o["d_within_2se"] >= max(0.85, yard_o["d_within_2se"] - 0.04), (name, got_o, yard_o)
         assert got_o["dyad_median_deg_supported"] < 1.0, (name, got_o)
+
+
+def test_speed_against_the_reference_kernels(torch):
+    """One xfibres_gpu subpart (12800 voxels, the reference's SIZE_SUB_PART) at the whole-brain
+    options: device time of the reference's own kernels -- fit_PVM_single_c and fit_PVM_multi from
+    the oracle's DTI/fit_pvf start values, then init_Fibres_Multifibres, the random setup and
+    runmcmc_kernel's burn-in (1000) and recording (1250) -- against this library's fit and chain
+    kernels on the same voxels (CUDA events around the kernels; the reference's host stages, DTI
+    start values, tau and Samples, are not counted).  Printed for the record; the test asks only
+    that this library be faster."""
+    from fdt_b200 import lib
+
+    n = 12800
+    o = Options.make(model=2, nfibres=3, rician=1, f0=1, ardf0=1)
+    prot = _protocol("wb")
+    y, _ = synth.make_volume(n, prot, 3, True, 25.0, seed=505)
+    y = O.prepare_data(y)
+    R = 0.13
+    start = O.lm_starts(1, 3, True, y, prot.bvecs, prot.bvals).astype(np.float32)
+    sc = ref_gpu.fit(1, 3, True, 0, R, y, prot.bvecs, prot.bvals, start)
+    t_fit = ref_gpu.last_times()[0]
+    pm = ref_gpu.fit(2, 3, True, 0, R, y, prot.bvecs, prot.bvals, sc)
+    t_fit += ref_gpu.last_times()[0]
+    d, bv, bl = (lib.to_device(a) for a in (y, prot.bvecs, prot.bvals))
+    for _ in range(2):  # the second pass is timed (modules loaded, workspaces grown)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        p, tau, _ = lib.fit(o, d, bv, bl)
+        e[1].record()
+        lib.mcmc(o, d, bv, bl, p, tau)
+        e[2].record()
+        torch.cuda.synchronize()
+    ours_fit, ours_mcmc = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+    ref_gpu.mcmc(o, y, prot.bvecs, prot.bvals, pm, tau.cpu().numpy(), seed=77.0)
+    _, t_burn, t_rec = ref_gpu.last_times()
+    ref_total, ours_total = t_fit + t_burn + t_rec, ours_fit + ours_mcmc
+    print(f"12800 whole-brain voxels, device ms: reference kernels fit {t_fit:.1f} + chain {t_burn + t_rec:.1f} = "
+          f"{ref_total:.1f} ({n / ref_total * 1e3:.0f} voxels/s); this library fit {ours_fit:.1f} + chain "
+          f"{ours_mcmc:.1f} = {ours_total:.1f} ({n / ours_total * 1e3:.0f} voxels/s); "
+          f"speed-up {ref_total / ours_total:.1f}x (fit {t_fit / ours_fit:.1f}x, chain "
+          f"{(t_burn + t_rec) / ours_mcmc:.1f}x)")
+    assert ours_total < ref_total
