@@ -188,4 +188,8 @@ class TrackVolume(C.Structure):
         ("ph", C.c_void_p),
         ("f", C.c_void_p),
         ("mask", C.c_void_p),
+        ("avoid", C.c_void_p),
+        ("stop", C.c_void_p),
+        ("waypoints", C.c_void_p),
+        ("nwaypoints", C.c_int32),
     ]

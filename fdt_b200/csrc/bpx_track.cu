@@ -6,7 +6,9 @@
 // streamlines.cc:662-690).  One thread tracks one particle: both halves of its streamline from the
 // seed, then adds 1 to fdt_paths in every voxel the kept halves passed through (once per voxel:
 // a per-thread open-addressing table of the voxels already counted, entries stamped with the
-// particle so no clearing is needed between particles) and 1 to waytotal.
+// particle so no clearing is needed between particles) and 1 to waytotal.  With an avoid mask,
+// waypoint masks or a distance threshold, the particle's halves are tracked once to learn which
+// are kept, then the kept ones again (the same draws, so the same path) to count them.
 //
 // The work is a chain of dependent random gathers (mask, then a posterior sample of each fibre at
 // a randomly rounded position), so the kernel is latency-bound: a persistent grid keeps as many
@@ -65,16 +67,20 @@ struct Particle {
   bool jumped;
 };
 
+// Particle::restart_reverse: the second half starts from the seed against the first half's first step
+__device__ __forceinline__ void reverse(Particle& P) {
+  if (P.jumped) {
+    P.rx = -P.rxi;
+    P.ry = -P.ryi;
+    P.rz = -P.rzi;
+  }
+}
+
 struct Tracker {
   const TrackArgs& a;
   uint2* tab;
   uint32_t stamp;
 
-  __device__ bool inside(int ix, int iy, int iz) const {
-    const bpx_track_volume& v = a.v;
-    if (ix < 0 || iy < 0 || iz < 0 || ix >= v.nx || iy >= v.ny || iz >= v.nz) return false;
-    return __ldg(v.mask + ((size_t)iz * v.ny + iy) * v.nx + ix) > 0.f;
-  }
   __device__ size_t at(int k, int s, size_t vox) const { return ((size_t)k * a.v.nsamples + s) * a.nvox + vox; }
 
   // first visit of `vox` by this particle: true (and the voxel is recorded)
@@ -193,41 +199,53 @@ struct Tracker {
     f = a.o.usef ? ff : 1.0f;
   }
 
-  // Streamliner::streamline for one half; counts the path's first visits when `count`.
-  // Returns the reject flag (1: shorter than distthresh).
+  // Streamliner::streamline for one half; counts the path's first visits when `count`.  `flags`
+  // accumulates the waypoint masks passed (over both halves of a particle).  Returns the reject
+  // flag: 1 (entered the avoid mask, passed no waypoint, or shorter than distthresh), 2 (passed
+  // some waypoints but not all), 0.
   __device__ int half_line(Particle& P, uint64_t pid, int h, int fibst0, float x0, float y0, float z0,
-                           bool count) const {
+                           bool count, uint32_t& flags) const {
     const bpx_track_options& o = a.o;
-    bool init_sample = true;
+    const bpx_track_volume& v = a.v;
+    bool init_sample = true, avoided = false;
     int fibst = fibst0;
     P.x = x0;
     P.y = y0;
     P.z = z0;
     float pathlength = 0.f;
-    const int K = a.v.nfib;
+    const int K = v.nfib;
     for (int it = 1; it <= o.nsteps / 2; ++it) {
       const int ix = rnd(P.x), iy = rnd(P.y), iz = rnd(P.z);
-      // this step's uniforms and sampled voxel, then the mask and every fibre's sample in one
-      // round of loads (the reference reads the sample only inside the mask: same values)
+      // this step's uniforms and sampled voxel, then the masks at the position and every fibre's
+      // sample in one round of loads (the reference reads them only inside the mask: same values)
       float u[8], th, ph, f;
       track_uniforms(o.seed, pid, h, (uint32_t)it, u);
       size_t svox;
       int samp;
       locate(P, u, svox, samp);
+      const bool in_grid = ix >= 0 && iy >= 0 && iz >= 0 && ix < v.nx && iy < v.ny && iz < v.nz;
+      const uint32_t vox = in_grid ? (uint32_t)(((size_t)iz * v.ny + iy) * v.nx + ix) : 0u;
+      const float m = __ldg(v.mask + vox);
+      const uint32_t way = v.waypoints ? __ldg(v.waypoints + vox) : 0u;
+      const bool avoid = v.avoid && __ldg(v.avoid + vox) != 0.f;
+      const bool stop = v.stop && __ldg(v.stop + vox) != 0.f;
       float sth[BPX_MAX_FIBRES], sph[BPX_MAX_FIBRES], sf[BPX_MAX_FIBRES];
 #pragma unroll
       for (int k = 0; k < BPX_MAX_FIBRES; ++k) {
         const size_t q = at(k < K ? k : 0, samp, svox);
-        sth[k] = __ldg(a.v.th + q);
-        sph[k] = __ldg(a.v.ph + q);
-        sf[k] = __ldg(a.v.f + q);
+        sth[k] = __ldg(v.th + q);
+        sph[k] = __ldg(v.ph + q);
+        sf[k] = __ldg(v.f + q);
       }
-      if (!inside(ix, iy, iz)) break;  // the reference's remaining steps change nothing
-      if (count) {
-        const uint32_t vox = (uint32_t)(((size_t)iz * a.v.ny + iy) * a.v.nx + ix);
-        if (first_visit(vox)) atomicAdd(a.paths + vox, 1.0f);
-      }
+      if (!(in_grid && m > 0.f)) break;  // the reference's remaining steps change nothing
+      flags |= way;
+      if (count && first_visit(vox)) atomicAdd(a.paths + vox, 1.0f);
       pathlength += o.steplength;
+      if (avoid) {
+        avoided = true;
+        break;
+      }
+      if (stop) break;
       choose(P, u, sth, sph, sf, init_sample, fibst, th, ph, f);
       if (f > u[5]) {
         float st, ct, sp, cp;
@@ -260,7 +278,14 @@ struct Tracker {
         }
       }
     }
-    return pathlength < o.distthresh ? 1 : 0;
+    int rej = 0;
+    if (v.nwaypoints > 0) {
+      const uint32_t all = v.nwaypoints >= 32 ? 0xffffffffu : ((1u << v.nwaypoints) - 1u);
+      const int passed = __popc(flags & all);
+      rej = passed == 0 ? 1 : (passed < v.nwaypoints ? 2 : 0);
+    }
+    if (avoided || pathlength < o.distthresh) rej = 1;
+    return rej;
   }
 };
 
@@ -269,7 +294,10 @@ __global__ void __launch_bounds__(kTrackThreads) track_kernel(TrackArgs a) {
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   Tracker T{a, a.tables + (t << a.log2n), 0u};
   unsigned long long kept = 0;
-  const bool two_pass = a.o.distthresh > 0.f;  // a half counts only once its length is known
+  // a half's fate waits on its length (distthresh), on the avoid mask, or on the waypoints both
+  // halves passed (Seedmanager::run keeps a first half with reject flag 2 when the second half
+  // completes the waypoints)
+  const bool decide = a.o.distthresh > 0.f || a.v.avoid != nullptr || a.v.nwaypoints > 0;
   for (uint64_t pid = a.pid_begin + t; pid < a.pid_end; pid += threads) {
     T.stamp = (uint32_t)(pid - a.pid_begin) + 1u;
     const int s = (int)(pid / (uint64_t)a.o.nparticles);
@@ -285,33 +313,30 @@ __global__ void __launch_bounds__(kTrackThreads) track_kernel(TrackArgs a) {
       z0 += u0[3] - 0.5f;
     }
     Particle P{};
-    int rej1, rej2;
-    if (two_pass) {
+    uint32_t flags = 0;  // waypoints passed by both halves (Streamliner::reset clears them per particle)
+    if (decide) {  // whether a half counts is known only once both halves have ended: track, then count
       const Particle P0 = P;
-      rej1 = T.half_line(P, pid, 0, fibst, x0, y0, z0, false);
-      if (rej1 == 0) {
-        Particle Q = P0;
-        T.half_line(Q, pid, 0, fibst, x0, y0, z0, true);
-      }
-    } else {
-      rej1 = T.half_line(P, pid, 0, fibst, x0, y0, z0, true);
-    }
-    if (P.jumped) {  // Particle::restart_reverse
-      P.rx = -P.rxi;
-      P.ry = -P.ryi;
-      P.rz = -P.rzi;
-    }
-    if (two_pass) {
+      const int rej1 = T.half_line(P, pid, 0, fibst, x0, y0, z0, false, flags);
+      reverse(P);
       const Particle P1 = P;
-      rej2 = T.half_line(P, pid, 1, fibst, x0, y0, z0, false);
-      if (rej2 == 0) {
-        Particle Q = P1;
-        T.half_line(Q, pid, 1, fibst, x0, y0, z0, true);
+      const int rej2 = T.half_line(P, pid, 1, fibst, x0, y0, z0, false, flags);
+      const bool fwd = (rej1 == 0 || rej1 == 2) && !(rej2 > 0 && rej1 > 0), bwd = rej2 == 0;
+      uint32_t unused = 0;
+      if (fwd) {
+        Particle Q = P0;
+        T.half_line(Q, pid, 0, fibst, x0, y0, z0, true, unused);
       }
-    } else {
-      rej2 = T.half_line(P, pid, 1, fibst, x0, y0, z0, true);
+      if (bwd) {
+        Particle Q = P1;
+        T.half_line(Q, pid, 1, fibst, x0, y0, z0, true, unused);
+      }
+      if (fwd || bwd) ++kept;
+    } else {  // every half is kept: count as it goes
+      T.half_line(P, pid, 0, fibst, x0, y0, z0, true, flags);
+      reverse(P);
+      T.half_line(P, pid, 1, fibst, x0, y0, z0, true, flags);
+      ++kept;
     }
-    if (rej1 == 0 || rej2 == 0) ++kept;
   }
   // waytotal: one atomic per warp
   for (int o = 16; o >= 1; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
@@ -333,7 +358,10 @@ bpx_status check_track(const bpx_track_options* o, const bpx_track_volume* v, in
     return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: voxel sizes must be positive");
   if (o->fibst > v->nfib) return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: fibst beyond the fibres given");
   if (nseeds < 0) return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: nseeds < 0");
-  if (nseeds > 0 && (!seeds || !paths || !waytotal || !v->th || !v->ph || !v->f || !v->mask))
+  if (v->nwaypoints < 0 || v->nwaypoints > 32)
+    return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: nwaypoints must be in 0..32");
+  if (nseeds > 0 && (!seeds || !paths || !waytotal || !v->th || !v->ph || !v->f || !v->mask ||
+                     (v->nwaypoints > 0 && !v->waypoints)))
     return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: NULL buffer");
   return BPX_OK;
 }

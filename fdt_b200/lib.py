@@ -361,20 +361,50 @@ def states_from_records(opts: Options, records, sample: int):
     return st
 
 
-def track_volume(th, ph, f, mask, voxel_size=(2.0, 2.0, 2.0)) -> TrackVolume:
-    """TrackVolume over device tensors th/ph/f [nfib][nsamples][nz][ny][nx] and mask [nz][ny][nx]."""
+def track_volume(th, ph, f, mask, voxel_size=(2.0, 2.0, 2.0), avoid=None, stop=None, waypoints=None,
+                 nwaypoints: int = 0) -> TrackVolume:
+    """TrackVolume over device tensors th/ph/f [nfib][nsamples][nz][ny][nx] and mask [nz][ny][nx];
+    optional avoid and stop masks (float32 [nz][ny][nx]) and waypoint bits (int32 [nz][ny][nx], bit w
+    for waypoint mask w < nwaypoints).  The tensors must outlive the call that uses the volume."""
     v = TrackVolume()
     v.nfib, v.nsamples, v.nz, v.ny, v.nx = (int(x) for x in th.shape)
     v.dx, v.dy, v.dz = (float(x) for x in voxel_size)
     v.th, v.ph, v.f, v.mask = th.data_ptr(), ph.data_ptr(), f.data_ptr(), mask.data_ptr()
+    for name, t in (("avoid", avoid), ("stop", stop), ("waypoints", waypoints)):
+        if t is not None:
+            if tuple(t.shape) != tuple(mask.shape) or t.element_size() != 4 or not t.is_contiguous():
+                raise ValueError(f"{name}: a contiguous 4-byte array of the mask's shape is needed")
+            setattr(v, name, t.data_ptr())
+    v.nwaypoints = int(nwaypoints) if waypoints is not None else 0
     return v
 
 
-def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.0)):
+def waypoint_bits(masks) -> np.ndarray:
+    """Waypoint masks ([nz][ny][nx] each, != 0 inside) packed as bpx_track_volume.waypoints:
+    int32 [nz][ny][nx] with bit w set inside mask w."""
+    masks = list(masks)
+    if not 1 <= len(masks) <= 32:
+        raise ValueError("1 to 32 waypoint masks")
+    bits = np.zeros(np.shape(masks[0]), np.uint32)
+    for w, m in enumerate(masks):
+        bits |= (np.asarray(m) != 0).astype(np.uint32) << np.uint32(w)
+    return bits.view(np.int32)
+
+
+def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.0), avoid=None, stop=None,
+              waypoints=None):
     """probtrackx simple mode on device tensors: (paths [nz][ny][nx] float32, waytotal int) for
-    seeds [nseeds][3] (voxel coordinates x, y, z)."""
+    seeds [nseeds][3] (voxel coordinates x, y, z).  `avoid` and `stop`: device masks of the mask's
+    shape (--avoid, --stop); `waypoints`: a list of 1 to 32 masks (host or device) that a kept
+    streamline must all pass (--waypoints)."""
     torch = _torch()
-    v = track_volume(th, ph, f, mask, voxel_size)
+    way_bits = None
+    nway = 0
+    if waypoints is not None:
+        nway = len(waypoints)
+        bits = waypoint_bits([w.cpu().numpy() if hasattr(w, "cpu") else w for w in waypoints])
+        way_bits = torch.from_numpy(bits).to("cuda")
+    v = track_volume(th, ph, f, mask, voxel_size, avoid=avoid, stop=stop, waypoints=way_bits, nwaypoints=nway)
     paths = torch.zeros(tuple(mask.shape), device="cuda", dtype=torch.float32)
     way = torch.zeros(1, device="cuda", dtype=torch.int64)
     sd = to_device(seeds)

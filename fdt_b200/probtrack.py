@@ -2,12 +2,15 @@
 
     python -m fdt_b200.probtrack SUBJECT.bedpostX --seeds seeds.txt --out OUTDIR [-P 5000] [-S 2000]
         [--steplength 0.5] [--cthr 0.2] [--fibthresh 0.01] [--distthresh 0] [--randfib 0] [--fibst 1]
-        [--usef] [--sampvox] [--seed N]
+        [--usef] [--sampvox] [--seed N] [--avoid MASK] [--stop MASK] [--waypoints MASK|LIST]
 
 Reads merged_th{k}samples, merged_ph{k}samples, merged_f{k}samples and nodif_brain_mask (NIfTI-1)
 as probtrackx does (probtrackx.cc:25-96 with mode simple, tractvolsx.h:55-97), tracks from every
 seed point of the seed file (one point per row, voxel coordinates x y z; ptx_simple.cc:31-35) and
 writes fdt_paths (visit counts of the kept streamlines, the mask's geometry) and waytotal.
+--avoid rejects a half that enters the mask, --stop ends a half where it enters it, and --waypoints
+(one mask, or a text file naming up to 32 masks one per line) keeps only streamlines whose halves
+together passed every mask (streamlines.cc:112-145, 279-330); all on the diffusion grid.
 The seed coordinates are taken in the volume's voxel grid as stored (the reference converts NIfTI
 voxel coordinates to its internal convention, which is the identity for neurological storage).
 """
@@ -45,12 +48,38 @@ def read_samples(bpx_dir: str):
     return vols["th"], vols["ph"], vols["f"], m, hdr, vs
 
 
-def run(bpx_dir: str, seeds: np.ndarray, opts: TrackOptions, outdir: str) -> tuple[np.ndarray, int]:
+def read_mask(path: str, grid: tuple[int, int, int]) -> np.ndarray:
+    """A mask on the diffusion grid as float32 [nz][ny][nx]."""
+    a, _ = nifti.read(path)
+    if a.shape[:3] != grid:
+        raise ValueError(f"{path}: grid {a.shape[:3]} differs from the mask's {grid}")
+    return np.ascontiguousarray(np.transpose(np.asarray(a, np.float32).reshape(grid), (2, 1, 0)))
+
+
+def waypoint_files(arg: str) -> list[str]:
+    """--waypoints: one image, or a text file naming one image per line (probtrackx's read_masks)."""
+    if arg.endswith((".nii", ".nii.gz")):
+        return [arg]
+    base = os.path.dirname(os.path.abspath(arg))
+    names = [ln.strip() for ln in open(arg) if ln.strip()]
+    return [n if os.path.isabs(n) else os.path.join(base, n) for n in names]
+
+
+def run(bpx_dir: str, seeds: np.ndarray, opts: TrackOptions, outdir: str, avoid: str | None = None,
+        stop: str | None = None, waypoints: str | None = None) -> tuple[np.ndarray, int]:
     import torch
 
     th, ph, f, m, hdr, vs = read_samples(bpx_dir)
+    grid = m.shape[::-1]
     dev = [lib.to_device(a) for a in (th, ph, f, m)]
-    paths, way = lib.probtrack(opts, *dev, np.asarray(seeds, np.float32).reshape(-1, 3), voxel_size=vs)
+    extra = {}
+    if avoid:
+        extra["avoid"] = lib.to_device(read_mask(avoid, grid))
+    if stop:
+        extra["stop"] = lib.to_device(read_mask(stop, grid))
+    if waypoints:
+        extra["waypoints"] = [read_mask(w, grid) for w in waypoint_files(waypoints)]
+    paths, way = lib.probtrack(opts, *dev, np.asarray(seeds, np.float32).reshape(-1, 3), voxel_size=vs, **extra)
     torch.cuda.synchronize()
     vol = np.transpose(paths.cpu().numpy(), (2, 1, 0))  # back to [x][y][z]
     os.makedirs(outdir, exist_ok=True)
@@ -76,6 +105,9 @@ def main(argv=None) -> None:
     ap.add_argument("-f", "--usef", action="store_true")
     ap.add_argument("--sampvox", action="store_true")
     ap.add_argument("--seed", type=int, default=8665904)
+    ap.add_argument("--avoid", help="reject pathways passing through this mask")
+    ap.add_argument("--stop", help="stop tracking at locations given by this mask")
+    ap.add_argument("--waypoints", help="waypoint mask, or a text file listing waypoint masks")
     a = ap.parse_args(argv)
     seeds = np.loadtxt(a.seeds, ndmin=2)
     if seeds.shape[1] != 3 and seeds.shape[0] == 3:
@@ -83,7 +115,7 @@ def main(argv=None) -> None:
     o = TrackOptions.make(nparticles=a.nsamples, nsteps=a.nsteps, steplength=a.steplength, c_thr=a.cthr,
                           fibthresh=a.fibthresh, distthresh=a.distthresh, randfib=a.randfib, fibst=a.fibst,
                           usef=int(a.usef), sampvox=int(a.sampvox), seed=a.seed)
-    _, way = run(a.bpx_dir, seeds, o, a.out)
+    _, way = run(a.bpx_dir, seeds, o, a.out, avoid=a.avoid, stop=a.stop, waypoints=a.waypoints)
     print(f"waytotal {way}")
 
 

@@ -280,3 +280,17 @@ def fibre_field(shape=(24, 20, 12), nsamples: int = 20, jitter: float = 0.08, se
     f[2] = 0.004
     f = np.clip(f, 0.0, 1.0)
     return th, ph, f.astype(np.float32), mask
+
+
+def write_bedpostx_dir(d: str, th, ph, f, mask) -> None:
+    """Writes th/ph/f [K][nsamples][nz][ny][nx] and mask [nz][ny][nx] as a bedpostX directory holds
+    them: merged_{th,ph,f}{k}samples ([x][y][z][nsamples]) and nodif_brain_mask, unit voxels."""
+    import os
+
+    from . import nifti
+
+    os.makedirs(d, exist_ok=True)
+    for q, a in (("th", th), ("ph", ph), ("f", f)):
+        for k in range(a.shape[0]):
+            nifti.write(os.path.join(d, f"merged_{q}{k + 1}samples.nii.gz"), np.transpose(a[k], (3, 2, 1, 0)))
+    nifti.write(os.path.join(d, "nodif_brain_mask.nii.gz"), np.transpose(mask, (2, 1, 0)))

@@ -455,7 +455,12 @@ typedef struct bpx_track_options {
 
 /* The bedpostx outputs probtrackx reads, on the device.  Sample arrays [nfib][nsamples][nz][ny][nx]
  * (x fastest: the merged_{th,ph,f}{k}samples volumes one after the other); mask [nz][ny][nx]
- * (nodif_brain_mask, > 0 inside); voxel size dx, dy, dz in mm. */
+ * (nodif_brain_mask, > 0 inside); voxel size dx, dy, dz in mm.  Optional masks on the same grid
+ * (NULL: none), tested at the rounded position of every step inside the brain mask
+ * (streamlines.cc:279-330): avoid (--avoid, the reference's rubbish mask, != 0 inside) rejects a
+ * half that enters it; stop (--stop) ends a half where it enters it; waypoints (--waypoints) holds
+ * bit w set inside waypoint mask w < nwaypoints (<= 32), and a streamline is kept only when its two
+ * halves together passed every one (Seedmanager::run's reject flags 0/1/2, streamlines.cc:1078-1098). */
 typedef struct bpx_track_volume {
   int32_t nx, ny, nz;
   float dx, dy, dz;
@@ -464,6 +469,10 @@ typedef struct bpx_track_volume {
   const float* ph;
   const float* f;
   const float* mask;
+  const float* avoid;
+  const float* stop;
+  const uint32_t* waypoints;
+  int32_t nwaypoints;
 } bpx_track_volume;
 
 void bpx_track_options_default(bpx_track_options* opts);

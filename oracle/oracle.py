@@ -198,14 +198,29 @@ def energy(opts: Options, data, bvecs, bvals, states):
     return lik, prior
 
 
-def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.0)):
+def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.0), avoid=None, stop=None,
+              waypoints=None):
     """probtrackx simple mode on host arrays (th/ph/f [nfib][nsamples][nz][ny][nx], mask [nz][ny][nx],
-    seeds [nseeds][3] voxel coordinates): (paths [nz][ny][nx] float32, waytotal)."""
+    seeds [nseeds][3] voxel coordinates; optional avoid and stop masks and a list of waypoint masks,
+    each [nz][ny][nx]): (paths [nz][ny][nx] float32, waytotal)."""
     th, ph, f, mask = (np.ascontiguousarray(a, np.float32) for a in (th, ph, f, mask))
     v = TrackVolume()
     v.nfib, v.nsamples, v.nz, v.ny, v.nx = th.shape
     v.dx, v.dy, v.dz = voxel_size
     v.th, v.ph, v.f, v.mask = th.ctypes.data, ph.ctypes.data, f.ctypes.data, mask.ctypes.data
+    keep = []
+    if avoid is not None:
+        keep.append(np.ascontiguousarray(avoid, np.float32))
+        v.avoid = keep[-1].ctypes.data
+    if stop is not None:
+        keep.append(np.ascontiguousarray(stop, np.float32))
+        v.stop = keep[-1].ctypes.data
+    if waypoints is not None:
+        bits = np.zeros(mask.shape, np.uint32)
+        for w, m in enumerate(waypoints):
+            bits |= (np.asarray(m) != 0).astype(np.uint32) << np.uint32(w)
+        keep.append(bits)
+        v.waypoints, v.nwaypoints = bits.ctypes.data, len(waypoints)
     paths = np.zeros(mask.shape, np.float32)
     way = C.c_int64(0)
     sd = np.ascontiguousarray(seeds, np.float32).reshape(-1, 3)

@@ -7,7 +7,8 @@
  *   Seedmanager::run            (streamlines.cc:1029-1120): both halves of a streamline from the
  *                               seed, kept halves, the streamline count (waytotal);
  *   Streamliner::streamline     (streamlines.cc:209-404): steps inside the mask, the path, the
- *                               curvature stop, the jump, the distance threshold;
+ *                               waypoint, avoid (rubbish) and stop masks, the curvature stop,
+ *                               the jump, the distance threshold;
  *   Counter::update_pathdist    (streamlines.cc:662-690): every voxel of a kept streamline counted
  *                               once (fdt_paths);
  *   Tractvolsx::sample          (tractvolsx.h:101-255): probabilistic rounding of the position,
@@ -191,11 +192,14 @@ static void sample(const trk_t* T, const part_t* P, const float u[8], int* init_
 }
 
 /* one half of a streamline (Streamliner::streamline); appends the path's voxels to path[];
- * returns the reject flag (1: shorter than distthresh) */
+ * *flags accumulates the waypoint masks passed (over both halves of a particle); returns the
+ * reject flag: 1 (entered the avoid mask, passed no waypoint, or shorter than distthresh), 2 (passed
+ * some waypoints but not all), 0 */
 static int half_line(const trk_t* T, part_t* P, uint64_t pid, int h, int fibst0, float x0, float y0, float z0,
-                     int64_t* path, int* npath) {
+                     int64_t* path, int* npath, uint32_t* flags) {
   const bpx_track_options* o = T->o;
-  int init_sample = 1, fibst = fibst0;
+  const bpx_track_volume* v = T->v;
+  int init_sample = 1, fibst = fibst0, avoided = 0;
   P->x = x0;
   P->y = y0;
   P->z = z0;
@@ -203,8 +207,15 @@ static int half_line(const trk_t* T, part_t* P, uint64_t pid, int h, int fibst0,
   for (int it = 1; it <= o->nsteps / 2; ++it) {
     const int ix = rnd(P->x), iy = rnd(P->y), iz = rnd(P->z);
     if (!inside(T, ix, iy, iz)) break;  /* the reference's remaining steps change nothing */
-    path[(*npath)++] = ((int64_t)iz * T->v->ny + iy) * T->v->nx + ix;
+    const int64_t vox = ((int64_t)iz * v->ny + iy) * v->nx + ix;
+    if (v->waypoints) *flags |= v->waypoints[vox];
+    path[(*npath)++] = vox;
     pathlength += o->steplength;
+    if (v->avoid && v->avoid[vox] != 0.f) {
+      avoided = 1;
+      break;
+    }
+    if (v->stop && v->stop[vox] != 0.f) break;
     float u[8], th, ph, f;
     orc_track_uniforms(o->seed, pid, h, (uint32_t)it, u);
     sample(T, P, u, &init_sample, &fibst, &th, &ph, &f);
@@ -238,7 +249,15 @@ static int half_line(const trk_t* T, part_t* P, uint64_t pid, int h, int fibst0,
       }
     }
   }
-  return pathlength < o->distthresh ? 1 : 0;
+  int rej = 0;
+  if (v->nwaypoints > 0) {
+    const uint32_t all = v->nwaypoints >= 32 ? 0xffffffffu : ((1u << v->nwaypoints) - 1u);
+    const int passed = __builtin_popcount(*flags & all);
+    rej = passed == 0 ? 1 : (passed < v->nwaypoints ? 2 : 0);
+  }
+  if (avoided) rej = 1;
+  if (pathlength < o->distthresh) rej = 1;
+  return rej;
 }
 
 int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nseeds, const float* seeds,
@@ -274,16 +293,21 @@ int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nse
       part_t P;
       memset(&P, 0, sizeof(P));
       int n1 = 0, n2 = 0;
-      const int rej1 = half_line(&T, &P, pid, 0, fibst, x0, y0, z0, path, &n1);
+      uint32_t flags = 0; /* waypoints passed, over both halves (Streamliner::reset clears them per particle) */
+      const int rej1 = half_line(&T, &P, pid, 0, fibst, x0, y0, z0, path, &n1, &flags);
       if (P.jumped) { /* Particle::restart_reverse */
         P.rx = -P.rxi;
         P.ry = -P.ryi;
         P.rz = -P.rzi;
       }
-      const int rej2 = half_line(&T, &P, pid, 1, fibst, x0, y0, z0, path + n1, &n2);
-      if (rej1 != 0 && rej2 != 0) continue;
+      const int rej2 = half_line(&T, &P, pid, 1, fibst, x0, y0, z0, path + n1, &n2, &flags);
+      /* Seedmanager::run: the first half is kept on flag 0, or on 2 when the second half completes
+       * the waypoints; the second half on flag 0 */
+      const int fwd = (rej1 == 0 || rej1 == 2) && !(rej2 > 0 && rej1 > 0);
+      const int bwd = rej2 == 0;
+      if (!fwd && !bwd) continue;
       ++kept;
-      const int from = rej1 == 0 ? 0 : n1, to = rej2 == 0 ? n1 + n2 : n1;
+      const int from = fwd ? 0 : n1, to = bwd ? n1 + n2 : n1;
       for (int i = from; i < to; ++i) {
         const int64_t vx = path[i];
         if (stamp[vx] != (int64_t)pid) {

@@ -3,8 +3,9 @@
 Both draw every step's random numbers from the same counter-based stream and do the same
 single-precision operations in the same order, so fdt_paths and waytotal must be identical, bit for
 bit (integer counts), for every option the kernel takes: the first fibre chosen by --fibst or at
-random (--randfib 1/2/3), --usef, --sampvox, --distthresh (the two-pass halves), short and long
-step counts, and on the outputs of this library's own bedpostx run.
+random (--randfib 1/2/3), --usef, --sampvox, --distthresh (the two-pass halves), the avoid, stop
+and waypoint masks, short and long step counts, and on the outputs of this library's own bedpostx
+run.
 """
 import numpy as np
 import pytest
@@ -35,7 +36,29 @@ CASES = [
     ("distthresh", dict(distthresh=6.0)),
     ("short_steps_low_cthr", dict(nsteps=20, c_thr=0.0)),
     ("steplength_1mm", dict(steplength=1.0)),
+    ("avoid", dict(masks=("avoid",))),
+    ("stop", dict(masks=("stop",))),
+    ("waypoints", dict(masks=("waypoints",))),
+    ("all_masks_distthresh", dict(masks=("avoid", "stop", "waypoints"), distthresh=4.0)),
 ]
+
+
+def _masks(mask, which):
+    """Slabs across the synthetic field: avoid at x = 17, stop at y = 13, two waypoints at x = 8 and
+    z = 3 (nz, ny, nx = 10, 16, 20)."""
+    out = {}
+    if "avoid" in which:
+        out["avoid"] = np.zeros_like(mask)
+        out["avoid"][:, :, 17] = 1.0
+    if "stop" in which:
+        out["stop"] = np.zeros_like(mask)
+        out["stop"][:, 13, :] = 2.0
+    if "waypoints" in which:
+        a, b = np.zeros_like(mask), np.zeros_like(mask)
+        a[:, :, 8] = 1.0
+        b[3, :, :] = 1.0
+        out["waypoints"] = [a, b]
+    return out
 
 
 @pytest.mark.parametrize("name,kw", CASES, ids=[c[0] for c in CASES])
@@ -45,10 +68,13 @@ def test_tracking_equals_oracle(torch, name, kw):
     lib.load()
     th, ph, f, mask = synth.fibre_field((20, 16, 10), nsamples=12, seed=4)
     seeds = np.array([[5.0, 8.0, 5.0], [14.0, 7.0, 4.6], [10.3, 3.2, 5.5], [0.0, 0.0, 0.0]], np.float32)
+    kw = dict(kw)
+    masks = _masks(mask, kw.pop("masks", ()))
     o = TrackOptions.make(nparticles=200, nsteps=kw.pop("nsteps", 300), seed=17, **kw)
-    want_p, want_w = O.probtrack(o, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.5))
+    want_p, want_w = O.probtrack(o, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.5), **masks)
     dev = [lib.to_device(a) for a in (th, ph, f, mask)]
-    got_p, got_w = lib.probtrack(o, *dev, seeds, voxel_size=(2.0, 2.0, 2.5))
+    dmasks = {k: (lib.to_device(v) if k != "waypoints" else v) for k, v in masks.items()}
+    got_p, got_w = lib.probtrack(o, *dev, seeds, voxel_size=(2.0, 2.0, 2.5), **dmasks)
     torch.cuda.synchronize()
     got_p = got_p.cpu().numpy()
     assert got_w == want_w, (name, got_w, want_w)
@@ -83,3 +109,32 @@ def test_tracking_on_bedpostx_outputs_equals_oracle(torch):
     got_p, got_w = lib.probtrack(t, *(lib.to_device(vols[k]) for k in ("th", "ph", "f")), lib.to_device(m), seeds)
     torch.cuda.synchronize()
     assert got_w == want_w and np.array_equal(got_p.cpu().numpy(), want_p)
+
+
+def test_probtrack_cli_with_masks_equals_oracle(torch, tmp_path):
+    """python -m fdt_b200.probtrack on a bedpostX directory with --avoid, --stop and a waypoint list:
+    fdt_paths and waytotal equal the oracle's on the same arrays."""
+    import os
+
+    from fdt_b200 import nifti, probtrack
+
+    th, ph, f, mask = synth.fibre_field((20, 16, 10), nsamples=12, seed=4)
+    d = str(tmp_path)
+    synth.write_bedpostx_dir(d, th, ph, f, mask)
+    masks = _masks(mask, ("avoid", "stop", "waypoints"))
+    for name, m in (("avoid", masks["avoid"]), ("stop", masks["stop"]), ("w1", masks["waypoints"][0]),
+                    ("w2", masks["waypoints"][1])):
+        nifti.write(os.path.join(d, name + ".nii.gz"), np.transpose(m, (2, 1, 0)))
+    with open(os.path.join(d, "ways.txt"), "w") as fh:
+        fh.write("w1.nii.gz\nw2.nii.gz\n")
+    seeds = np.array([[5.0, 8.0, 5.0], [14.0, 7.0, 4.6]], np.float32)
+    np.savetxt(os.path.join(d, "seeds.txt"), seeds)
+    out = os.path.join(d, "out")
+    probtrack.main([d, "--seeds", os.path.join(d, "seeds.txt"), "--out", out, "-P", "150", "-S", "300", "--seed", "23",
+                    "--avoid", os.path.join(d, "avoid.nii.gz"), "--stop", os.path.join(d, "stop.nii.gz"),
+                    "--waypoints", os.path.join(d, "ways.txt")])
+    o = TrackOptions.make(nparticles=150, nsteps=300, seed=23)
+    want_p, want_w = O.probtrack(o, th, ph, f, mask, seeds, **masks)
+    got, _ = nifti.read(os.path.join(out, "fdt_paths.nii.gz"))
+    assert int(open(os.path.join(out, "waytotal")).read()) == want_w > 0
+    assert np.array_equal(np.transpose(got, (2, 1, 0)), want_p)

@@ -2,7 +2,8 @@
 (same literals, single-precision accuracy), and tracking follows the reference's rules on fields
 whose answer is known: a straight tract is followed to the mask boundary in both directions and
 every voxel on it is counted once per streamline; the curvature threshold stops a streamline at a
-right-angle turn; the distance threshold drops short streamlines."""
+right-angle turn; the distance threshold drops short streamlines; the avoid, stop and waypoint
+masks reject, end and select halves as Seedmanager::run and Streamliner::streamline do."""
 import os
 import re
 
@@ -84,3 +85,79 @@ def test_crossing_field_options_run_and_conserve_counts():
         paths, way = O.probtrack(o, th, ph, f, mask, seeds)
         assert 0 < way <= 60, kw
         assert paths.max() <= way and np.all(paths[mask == 0] == 0), kw
+    # masks only ever remove streamlines or shorten them
+    o = TrackOptions.make(nparticles=30, nsteps=200, seed=11)
+    free, way0 = O.probtrack(o, th, ph, f, mask, seeds)
+    slab = np.zeros_like(mask)
+    slab[:, :, 8] = 1.0
+    for kw in (dict(avoid=slab), dict(stop=slab), dict(waypoints=[slab])):
+        paths, way = O.probtrack(o, th, ph, f, mask, seeds, **kw)
+        assert way <= way0 and np.all(paths <= free), list(kw)
+
+
+def _plane(mask, x):
+    m = np.zeros_like(mask)
+    m[:, :, x] = 1.0
+    return m
+
+
+def test_avoid_mask_rejects_the_half_that_enters_it():
+    th, ph, f, mask = _straight_box()
+    o = TrackOptions.make(nparticles=40, nsteps=400, seed=3)
+    paths, way = O.probtrack(o, th, ph, f, mask, [[15.0, 4.0, 4.0]], avoid=_plane(mask, 20))
+    line = paths[4, 4, :]
+    # one half of every particle runs into x = 20 and is dropped; the other reaches x = 3
+    assert way == 40 and np.all(line[3:16] == 40) and line[16:].sum() == 0 and line[:3].sum() == 0
+
+
+def test_stop_mask_ends_the_half_inside_it():
+    th, ph, f, mask = _straight_box()
+    o = TrackOptions.make(nparticles=40, nsteps=400, seed=3)
+    paths, way = O.probtrack(o, th, ph, f, mask, [[15.0, 4.0, 4.0]], stop=_plane(mask, 20))
+    line = paths[4, 4, :]
+    assert way == 40 and np.all(line[3:21] == 40) and line[21:].sum() == 0
+
+
+def test_one_waypoint_keeps_the_other_half_only_when_it_ran_second():
+    th, ph, f, mask = _straight_box()
+    o = TrackOptions.make(nparticles=60, nsteps=400, seed=9)
+    paths, way = O.probtrack(o, th, ph, f, mask, [[15.0, 4.0, 4.0]], waypoints=[_plane(mask, 20)])
+    line = paths[4, 4, :]
+    # the half towards the waypoint is always kept; the other only when it ran second, after the
+    # first had passed the waypoint (a first half that passed nothing gets reject flag 1 and is
+    # dropped, although the second half then passes the waypoint)
+    assert way == 60 and np.all(line[15:27] == 60)
+    assert 0 < line[3] < 60 and np.all(line[3:15] == line[3])
+
+
+def test_waypoints_passed_by_both_halves_together():
+    th, ph, f, mask = _straight_box()
+    o = TrackOptions.make(nparticles=30, nsteps=400, seed=9)
+    both = [_plane(mask, 8), _plane(mask, 22)]
+    paths, way = O.probtrack(o, th, ph, f, mask, [[15.0, 4.0, 4.0]], waypoints=both)
+    assert way == 30 and np.all(paths[4, 4, 3:27] == 30)
+    unreachable = np.zeros_like(mask)
+    unreachable[0, 0, :] = 1.0  # outside the brain mask
+    paths, way = O.probtrack(o, th, ph, f, mask, [[15.0, 4.0, 4.0]], waypoints=[both[0], unreachable])
+    assert way == 0 and paths.sum() == 0
+
+
+def test_probtrack_cli_reads_samples_masks_and_waypoint_lists(tmp_path):
+    from fdt_b200 import nifti, probtrack
+
+    th, ph, f, mask = synth.fibre_field((12, 10, 6), nsamples=4, seed=1)
+    synth.write_bedpostx_dir(str(tmp_path), th, ph, f, mask)
+    rth, rph, rf, rm, _, vs = probtrack.read_samples(str(tmp_path))
+    assert np.array_equal(rth, th) and np.array_equal(rph, ph) and np.array_equal(rf, f)
+    assert np.array_equal(rm, mask) and vs == (1.0, 1.0, 1.0)
+    w = np.zeros_like(mask)
+    w[:, :, 5] = 1.0
+    for name in ("w1.nii.gz", "w2.nii.gz"):
+        nifti.write(os.path.join(str(tmp_path), name), np.transpose(w, (2, 1, 0)))
+    lst = os.path.join(str(tmp_path), "waypoints.txt")
+    with open(lst, "w") as fh:
+        fh.write("w1.nii.gz\n\n" + os.path.join(str(tmp_path), "w2.nii.gz") + "\n")
+    files = probtrack.waypoint_files(lst)
+    assert [os.path.basename(p) for p in files] == ["w1.nii.gz", "w2.nii.gz"] and all(map(os.path.exists, files))
+    assert probtrack.waypoint_files(files[0]) == [files[0]]
+    assert np.array_equal(probtrack.read_mask(files[0], mask.shape[::-1]), w)
