@@ -214,6 +214,9 @@ struct Tracker {
     P.z = z0;
     float pathlength = 0.f;
     const int K = v.nfib;
+    // a step of steplength mm mostly stays in the voxel of the step before, which is counted
+    // already: the visit table is probed only when the voxel changes
+    uint32_t last = 0xffffffffu;
     for (int it = 1; it <= o.nsteps / 2; ++it) {
       const int ix = rnd(P.x), iy = rnd(P.y), iz = rnd(P.z);
       // this step's uniforms and sampled voxel, then the masks at the position and every fibre's
@@ -239,7 +242,10 @@ struct Tracker {
       }
       if (!(in_grid && m > 0.f)) break;  // the reference's remaining steps change nothing
       flags |= way;
-      if (count && first_visit(vox)) atomicAdd(a.paths + vox, 1.0f);
+      if (count && vox != last) {
+        last = vox;
+        if (first_visit(vox)) atomicAdd(a.paths + vox, 1.0f);
+      }
       pathlength += o.steplength;
       if (avoid) {
         avoided = true;
