@@ -10,9 +10,11 @@
 // waypoint masks or a distance threshold, the particle's halves are tracked once to learn which
 // are kept, then the kept ones again (the same draws, so the same path) to count them.
 //
-// The work is a chain of dependent random gathers (mask, then a posterior sample of each fibre at
-// a randomly rounded position), so the kernel is latency-bound: a persistent grid keeps as many
-// particles in flight as the tables' workspace allows and every thread walks its particles in turn.
+// The work is a chain of dependent random gathers (the mask at the position and a posterior sample
+// at a randomly rounded position, then the step), so the kernel is latency-bound: a persistent
+// grid keeps as many particles in flight as the tables' workspace allows and every thread walks its
+// particles in turn.  The samples are first repacked (pack_samples_kernel) so that one step reads
+// one record of every fibre's th, ph and f instead of 3K scattered words.
 //
 // Arithmetic: single precision in the reference's operation order, no contraction into FMAs (this
 // file is compiled with -fmad=false), sine and cosine from sincos_fast; random numbers from
@@ -41,6 +43,8 @@ struct TrackArgs {
   unsigned long long* waytotal;
   uint2* tables;       // [threads][1 << log2n] {voxel, stamp}
   int log2n;
+  const float4* packed;  // [nvox][nsamples][pk4] float4: th, ph, f of fibre 0, 1, 2 in turn, zero padded
+  int pk4;               // float4 entries per (voxel, sample): 1, 2 or 3
   uint64_t pid_begin;  // particles [pid_begin, pid_end) of this launch
   uint64_t pid_end;
 };
@@ -81,7 +85,6 @@ struct Tracker {
   uint2* tab;
   uint32_t stamp;
 
-  __device__ size_t at(int k, int s, size_t vox) const { return ((size_t)k * a.v.nsamples + s) * a.nvox + vox; }
 
   // first visit of `vox` by this particle: true (and the voxel is recorded)
   __device__ bool first_visit(uint32_t vox) const {
@@ -232,13 +235,17 @@ struct Tracker {
       const uint32_t way = v.waypoints ? __ldg(v.waypoints + vox) : 0u;
       const bool avoid = v.avoid && __ldg(v.avoid + vox) != 0.f;
       const bool stop = v.stop && __ldg(v.stop + vox) != 0.f;
+      // the sample: one 16- to 48-byte record (one or two sectors) instead of 3K scattered words
+      const float4* rec = a.packed + ((size_t)svox * v.nsamples + samp) * a.pk4;
+      const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 r0 = __ldg(rec), r1 = a.pk4 > 1 ? __ldg(rec + 1) : zero, r2 = a.pk4 > 2 ? __ldg(rec + 2) : zero;
+      const float e[12] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w};
       float sth[BPX_MAX_FIBRES], sph[BPX_MAX_FIBRES], sf[BPX_MAX_FIBRES];
 #pragma unroll
       for (int k = 0; k < BPX_MAX_FIBRES; ++k) {
-        const size_t q = at(k < K ? k : 0, samp, svox);
-        sth[k] = __ldg(v.th + q);
-        sph[k] = __ldg(v.ph + q);
-        sf[k] = __ldg(v.f + q);
+        sth[k] = e[3 * k];
+        sph[k] = e[3 * k + 1];
+        sf[k] = e[3 * k + 2];
       }
       if (!(in_grid && m > 0.f)) break;  // the reference's remaining steps change nothing
       flags |= way;
@@ -295,7 +302,7 @@ struct Tracker {
   }
 };
 
-__global__ void __launch_bounds__(kTrackThreads) track_kernel(TrackArgs a) {
+__global__ void __launch_bounds__(kTrackThreads, kTrackBlocksPerSm) track_kernel(TrackArgs a) {
   const uint64_t threads = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   Tracker T{a, a.tables + (t << a.log2n), 0u};
@@ -349,6 +356,41 @@ __global__ void __launch_bounds__(kTrackThreads) track_kernel(TrackArgs a) {
   if ((threadIdx.x & 31) == 0 && kept) atomicAdd(a.waytotal, kept);
 }
 
+// The samples [K][nsamples][nvox] of th, ph and f repacked as one record per (voxel, sample):
+// a 32 x 32 tile of (voxel, sample) per block, read along voxels and written along samples through
+// shared memory, so both sides are coalesced.
+constexpr int kPackTile = 32;
+__global__ void __launch_bounds__(256) pack_samples_kernel(const float* __restrict__ th, const float* __restrict__ ph,
+                                                           const float* __restrict__ f, int K, int ns, size_t nvox,
+                                                           int pk4, float4* __restrict__ out) {
+  __shared__ float tile[3 * BPX_MAX_FIBRES][kPackTile][kPackTile + 1];
+  const size_t v0 = (size_t)blockIdx.x * kPackTile;
+  const int s0 = blockIdx.y * kPackTile;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int c = 0; c < 3 * K; ++c) {
+    const float* src = (c % 3 == 0) ? th : (c % 3 == 1) ? ph : f;
+    const int k = c / 3;
+    for (int j = ty; j < kPackTile; j += blockDim.y) {
+      const int smp = s0 + j;
+      const size_t vx = v0 + tx;
+      tile[c][j][tx] = (smp < ns && vx < nvox) ? src[((size_t)k * ns + smp) * nvox + vx] : 0.f;
+    }
+  }
+  __syncthreads();
+  for (int i = ty; i < kPackTile; i += blockDim.y) {
+    const size_t vx = v0 + i;
+    const int smp = s0 + tx;
+    if (vx >= nvox || smp >= ns) continue;
+    float4* dst = out + (vx * ns + smp) * pk4;
+    for (int q = 0; q < pk4; ++q) {
+      float w[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) w[e] = (4 * q + e < 3 * K) ? tile[4 * q + e][tx][i] : 0.f;
+      dst[q] = make_float4(w[0], w[1], w[2], w[3]);
+    }
+  }
+}
+
 bpx_status check_track(const bpx_track_options* o, const bpx_track_volume* v, int32_t nseeds, const float* seeds,
                        const float* paths, const int64_t* waytotal) {
   if (!o || !v) return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: opts or vol is NULL");
@@ -360,6 +402,8 @@ bpx_status check_track(const bpx_track_options* o, const bpx_track_volume* v, in
     return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: bad grid, fibre or sample count");
   if ((size_t)v->nx * v->ny * v->nz >= (1ull << 32))
     return api_fail(BPX_ERR_UNSUPPORTED, "bpx_probtrack_dev: more than 2^32 voxels");
+  if ((size_t)v->nx * v->ny * v->nz * (size_t)v->nsamples >= (1ull << 36) || v->nsamples >= (1 << 26))
+    return api_fail(BPX_ERR_UNSUPPORTED, "bpx_probtrack_dev: more than 2^36 samples");
   if (!(v->dx > 0.f && v->dy > 0.f && v->dz > 0.f))
     return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: voxel sizes must be positive");
   if (o->fibst > v->nfib) return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: fibst beyond the fibres given");
@@ -418,11 +462,25 @@ bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volu
   int grid = sm_count() * kTrackBlocksPerSm;
   if ((size_t)grid > max_blocks) grid = max_blocks > 0 ? (int)max_blocks : 1;
   const size_t threads = (size_t)grid * kTrackThreads;
+  // workspace: the visit tables, then the repacked samples
+  const int pk4 = (3 * vol->nfib + 3) / 4;
+  const size_t tab_total = (threads * table_bytes + 255) & ~(size_t)255;
+  const size_t packed_bytes = a.nvox * (size_t)vol->nsamples * (size_t)pk4 * sizeof(float4);
   void* ws = nullptr;
-  st = api_workspace(kWsTrack, threads * table_bytes, &ws);
+  st = api_workspace(kWsTrack, tab_total + packed_bytes, &ws);
   if (st != BPX_OK) return st;
   a.tables = (uint2*)ws;
+  a.packed = (const float4*)((char*)ws + tab_total);
+  a.pk4 = pk4;
   cudaStream_t s = (cudaStream_t)stream;
+  {
+    const dim3 block(kPackTile, 8);
+    const dim3 pgrid((unsigned)((a.nvox + kPackTile - 1) / kPackTile), (unsigned)((vol->nsamples + kPackTile - 1) / kPackTile));
+    pack_samples_kernel<<<pgrid, block, 0, s>>>(vol->th, vol->ph, vol->f, vol->nfib, vol->nsamples, a.nvox, pk4,
+                                                 (float4*)a.packed);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return api_cuda_fail(e, "bpx_probtrack_dev: pack_samples_kernel");
+  }
   const uint64_t total = (uint64_t)nseeds * (uint64_t)opts->nparticles;
   const uint64_t chunk = 1ull << 30;  // stamps stay below 2^30 + 1 within a launch
   for (uint64_t b = 0; b < total; b += chunk) {

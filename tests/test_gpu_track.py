@@ -44,19 +44,19 @@ CASES = [
 
 
 def _masks(mask, which):
-    """Slabs across the synthetic field: avoid at x = 17, stop at y = 13, two waypoints at x = 8 and
-    z = 3 (nz, ny, nx = 10, 16, 20)."""
+    """Planes across the synthetic field's x-running tracts (nz, ny, nx = 10, 16, 20): avoid at
+    x = 17, stop at x = 3, two waypoints at x = 8 and x = 12 (each changes the oracle's counts)."""
     out = {}
     if "avoid" in which:
         out["avoid"] = np.zeros_like(mask)
         out["avoid"][:, :, 17] = 1.0
     if "stop" in which:
         out["stop"] = np.zeros_like(mask)
-        out["stop"][:, 13, :] = 2.0
+        out["stop"][:, :, 3] = 2.0
     if "waypoints" in which:
         a, b = np.zeros_like(mask), np.zeros_like(mask)
         a[:, :, 8] = 1.0
-        b[3, :, :] = 1.0
+        b[:, :, 12] = 1.0
         out["waypoints"] = [a, b]
     return out
 
