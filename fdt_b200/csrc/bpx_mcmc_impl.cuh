@@ -205,7 +205,7 @@ __device__ __forceinline__ void rician_pick(float z, float q, float pr, float& s
   sel = small ? q : pr;
   zs = small ? z : 0.f;
 }
-template <typename V, bool PADW = true>
+template <typename V>
 __device__ __forceinline__ void rician_acc(V y, V w, V base, V nS0, V tS0, V& rr, V& prod, V& zs) {
   const V r = vfma(nS0, base, y);
   const V z = vmul(tS0, vmul(y, base));
@@ -233,7 +233,7 @@ __device__ __forceinline__ void rician_acc(V y, V w, V base, V nS0, V tS0, V& rr
   }
   prod = vmul(prod, sel);
   zs = vadd(zs, zz);
-  rr = PADW ? vfma(vmul(r, w), r, rr) : vfma(r, r, rr);
+  rr = vfma(vmul(r, w), r, rr);
 }
 
 // signals of one or two measurements (compute_signal / compute_iso_signal, CUDA/runmcmc_kernels.cu:67-95).
@@ -262,13 +262,13 @@ __device__ __forceinline__ void with_signal_form(const SigParams<MODEL>& sp, F&&
 }
 
 // Gaussian likelihood contribution of one or two measurements, w (y - S0 base)^2
-template <int K, typename V, bool PADW = true>
+template <int K, typename V>
 __device__ __forceinline__ V gauss_v(V y, V w, V isov, const V (&sk)[K], V nS0, const V (&fk)[K], V f0, V wiso) {
   V base = vfma(wiso, isov, f0);
 #pragma unroll
   for (int k = 0; k < K; ++k) base = vfma(fk[k], sk[k], base);
   const V r = vfma(nS0, base, y);
-  return PADW ? vmul(vmul(r, w), r) : vmul(r, r);
+  return vmul(vmul(r, w), r);
 }
 
 // Rows of the per-group fibre state in shared memory (K entries each).
@@ -513,11 +513,8 @@ __global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_ker
         }
       });
     };
-    // the likelihood statistic of a state, summed over the group.  PADW: the lane's measurements
-    // include padding (M < TPV * MPL), whose weights w = 0 enter the Rician residual sum; without
-    // padding every w is 1 and the product is skipped (the same value, bit for bit).
-    auto lik_body = [&](auto padw, float S0x, const float (&fx)[K], float f0x, float taux) {
-      constexpr bool PADW = decltype(padw)::value;
+    // the likelihood statistic of a state, summed over the group
+    auto lik_of = [&](float S0x, const float (&fx)[K], float f0x, float taux) {
       float fsum = f0x;
 #pragma unroll
       for (int k = 0; k < K; ++k) fsum += fx[k];
@@ -537,7 +534,7 @@ __global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_ker
           float2 base = vfma(wiso2, i2[p], f02);
 #pragma unroll
           for (int k = 0; k < K; ++k) base = vfma(fk2[k], s2[k][p], base);
-          rician_acc<float2, PADW>(make_float2(yw.x, yw.y), make_float2(yw.z, yw.w), base, nS02, tS02, rr, prod, zs);
+          rician_acc<float2>(make_float2(yw.x, yw.y), make_float2(yw.z, yw.w), base, nS02, tS02, rr, prod, zs);
           if (p % 4 == 3 && p + 1 < NP) {
             lgp += lg2_approx(prod.x) + lg2_approx(prod.y);
             prod = make_float2(1.f, 1.f);
@@ -548,7 +545,7 @@ __global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_ker
           float base = fmaf(wiso, it_, f0x);
 #pragma unroll
           for (int k = 0; k < K; ++k) base = fmaf(fx[k], st[k], base);
-          rician_acc<float, PADW>(ytw.x, ytw.y, base, -S0x, taux * S0x, rr.x, prod.x, zs.x);
+          rician_acc<float>(ytw.x, ytw.y, base, -S0x, taux * S0x, rr.x, prod.x, zs.x);
         }
         acc = -0.5f * taux * (rr.x + rr.y) + kLn2 * (lgp + lg2_approx(prod.x) + lg2_approx(prod.y)) - (zs.x + zs.y);
       } else {
@@ -559,21 +556,16 @@ __global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_ker
 #pragma unroll
           for (int k = 0; k < K; ++k) sk[k] = s2[k][p];
           const float4 yw = ywp[p * kMcmcThreads + tid];
-          acc2 = vadd(acc2, gauss_v<K, float2, PADW>(make_float2(yw.x, yw.y), make_float2(yw.z, yw.w), i2[p], sk, nS02,
-                                                     fk2, f02, wiso2));
+          acc2 = vadd(acc2, gauss_v<K, float2>(make_float2(yw.x, yw.y), make_float2(yw.z, yw.w), i2[p], sk, nS02, fk2,
+                                               f02, wiso2));
         }
         acc = vhsum(acc2);
         if (TAIL) {
           const float2 ytw = ywt[tid];
-          acc += gauss_v<K, float, PADW>(ytw.x, ytw.y, it_, st, -S0x, fx, f0x, wiso);
+          acc += gauss_v<K, float>(ytw.x, ytw.y, it_, st, -S0x, fx, f0x, wiso);
         }
       }
       return group_sum<TPV>(acc);
-    };
-    const bool padded = M < TPV * MPL;
-    auto lik_of = [&](float S0x, const float (&fx)[K], float f0x, float taux) {
-      if (padded) return lik_body(std::true_type{}, S0x, fx, f0x, taux);
-      return lik_body(std::false_type{}, S0x, fx, f0x, taux);
     };
 
     // signal parameters of the current state (changed only by accepted d, d_std or R proposals)

@@ -134,8 +134,7 @@ def test_probtrack_cli_with_masks_equals_oracle(torch, tmp_path):
                     "--avoid", os.path.join(d, "avoid.nii.gz"), "--stop", os.path.join(d, "stop.nii.gz"),
                     "--waypoints", os.path.join(d, "ways.txt")])
     o = TrackOptions.make(nparticles=150, nsteps=300, seed=23)
-    # the directory's NIfTI files carry unit voxels
-    want_p, want_w = O.probtrack(o, th, ph, f, mask, seeds, voxel_size=(1.0, 1.0, 1.0), **masks)
+    want_p, want_w = O.probtrack(o, th, ph, f, mask, seeds, **masks)
     got, _ = nifti.read(os.path.join(out, "fdt_paths.nii.gz"))
     assert int(open(os.path.join(out, "waytotal")).read()) == want_w > 0
     assert np.array_equal(np.transpose(got, (2, 1, 0)), want_p)
