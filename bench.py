@@ -516,7 +516,7 @@ def run_probtrack(args):
     dev = [lib.to_device(a) for a in (th, ph, f, mask)]
     sd = lib.to_device(seeds)
     v = lib.track_volume(*dev)
-    paths = torch.zeros(mask.shape, device="cuda")
+    paths = torch.zeros(mask.shape, device="cuda", dtype=torch.int32)
     way = torch.zeros(1, device="cuda", dtype=torch.int64)
     L = lib.load()
     import ctypes as C
@@ -555,7 +555,7 @@ def run_probtrack(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
         "config": {"workload": "probtrackx simple mode: 96x96x60 crossing-fibre field, 3 fibres x 50 samples, "
                    "%d seeds x 5000 particles, 2000 steps of 0.5 mm, cthr 0.2, fibthresh 0.01" % len(seeds),
-                   "streamlines": n_lines, "waytotal": int(way.item()), "visits": float(paths.sum().item())},
+                   "streamlines": n_lines, "waytotal": int(way.item()), "visits": int(paths.sum(dtype=torch.int64).item())},
         "cpu_baseline": {"value": nb * o.nparticles / t_cpu, "unit": "streamlines/s", "cores": 1, "kind": "port",
                          "sample": f"{nb} seed points x {o.nparticles} particles through the CPU oracle"},
         "gpu_launches": k, "clocks": ck,

@@ -156,7 +156,8 @@ class TrackOptions(C.Structure):
         ("usef", C.c_int32),
         ("sampvox", C.c_int32),
         ("seed", C.c_uint64),
-        ("reserved", C.c_int32 * 4),
+        ("pathdist", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
     @classmethod

@@ -2,7 +2,7 @@
 
     python -m fdt_b200.probtrack SUBJECT.bedpostX --seeds seeds.txt --out OUTDIR [-P 5000] [-S 2000]
         [--steplength 0.5] [--cthr 0.2] [--fibthresh 0.01] [--distthresh 0] [--randfib 0] [--fibst 1]
-        [--usef] [--sampvox] [--seed N] [--avoid MASK] [--stop MASK] [--waypoints MASK|LIST]
+        [--usef] [--sampvox] [--pd] [--seed N] [--avoid MASK] [--stop MASK] [--waypoints MASK|LIST]
 
 Reads merged_th{k}samples, merged_ph{k}samples, merged_f{k}samples and nodif_brain_mask (NIfTI-1)
 as probtrackx does (probtrackx.cc:25-96 with mode simple, tractvolsx.h:55-97), tracks from every
@@ -83,7 +83,9 @@ def run(bpx_dir: str, seeds: np.ndarray, opts: TrackOptions, outdir: str, avoid:
     torch.cuda.synchronize()
     vol = np.transpose(paths.cpu().numpy(), (2, 1, 0))  # back to [x][y][z]
     os.makedirs(outdir, exist_ok=True)
-    nifti.write(os.path.join(outdir, "fdt_paths.nii.gz"), vol, like=hdr, cal=(float(vol.min()), float(vol.max())))
+    # an int32 volume, as the reference saves its volume<int> m_prob
+    nifti.write(os.path.join(outdir, "fdt_paths.nii.gz"), vol.astype(np.int32), like=hdr,
+                cal=(float(vol.min()), float(vol.max())))
     with open(os.path.join(outdir, "waytotal"), "w") as fh:
         fh.write(f"{way}\n")
     return vol, way
@@ -104,6 +106,7 @@ def main(argv=None) -> None:
     ap.add_argument("--fibst", type=int, default=1)
     ap.add_argument("-f", "--usef", action="store_true")
     ap.add_argument("--sampvox", action="store_true")
+    ap.add_argument("--pd", action="store_true", help="correct the path distribution for the length of the pathways")
     ap.add_argument("--seed", type=int, default=8665904)
     ap.add_argument("--avoid", help="reject pathways passing through this mask")
     ap.add_argument("--stop", help="stop tracking at locations given by this mask")
@@ -114,7 +117,7 @@ def main(argv=None) -> None:
         seeds = seeds.T
     o = TrackOptions.make(nparticles=a.nsamples, nsteps=a.nsteps, steplength=a.steplength, c_thr=a.cthr,
                           fibthresh=a.fibthresh, distthresh=a.distthresh, randfib=a.randfib, fibst=a.fibst,
-                          usef=int(a.usef), sampvox=int(a.sampvox), seed=a.seed)
+                          usef=int(a.usef), sampvox=int(a.sampvox), pathdist=int(a.pd), seed=a.seed)
     _, way = run(a.bpx_dir, seeds, o, a.out, avoid=a.avoid, stop=a.stop, waypoints=a.waypoints)
     print(f"waytotal {way}")
 

@@ -450,7 +450,9 @@ typedef struct bpx_track_options {
   int32_t usef;        /* -f, --usef: a step is taken with probability f */
   int32_t sampvox;     /* --sampvox: seed positions jittered within the seed voxel */
   uint64_t seed;       /* random seed */
-  int32_t reserved[4]; /* zero */
+  int32_t pathdist;    /* --pd: the d-th distinct voxel of a kept streamline adds d (path length
+                          correction), not 1 (Counter::update_pathdist, streamlines.cc:662-690) */
+  int32_t reserved[3]; /* zero */
 } bpx_track_options;
 
 /* The bedpostx outputs probtrackx reads, on the device.  Sample arrays [nfib][nsamples][nz][ny][nx]
@@ -479,13 +481,16 @@ void bpx_track_options_default(bpx_track_options* opts);
 /*
  * Tracks opts->nparticles streamlines from each of nseeds seed points (seeds [nseeds][3], voxel
  * coordinates of the volume, x y z) and ADDS each kept streamline's distinct voxels to
- * paths [nz][ny][nx] (float counts, fdt_paths) and the kept streamlines to *waytotal (device
- * int64); the caller zeroes both first.  Uses workspace memory (see Concurrency) of
- * 8 * 2^ceil(log2(2 * (nsteps + 2))) bytes per particle in flight (512 particles per
- * multiprocessor, fewer if that passes 8 GB: 2.5 GB on a B200 at nsteps 2000).
+ * paths [nz][ny][nx] (int32 counts, fdt_paths: the reference's volume<int> m_prob, wrapping past
+ * 2^31 as it does) and the kept streamlines to *waytotal (device int64); the caller zeroes both
+ * first.  Integer sums make the result independent of the order in which streamlines finish.
+ * Uses workspace memory (see Concurrency): the samples repacked, 16 * ceil(3 * nfib / 4) bytes per
+ * voxel and sample, and a visit table of 8 * 2^ceil(log2(2 * (nsteps + 2))) bytes per particle in
+ * flight (1024 particles per multiprocessor, fewer if the tables would pass 8 GB: 5 GB on a B200 at
+ * nsteps 2000).
  */
 bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volume* vol, int32_t nseeds,
-                             const float* seeds, float* paths, int64_t* waytotal, void* stream);
+                             const float* seeds, int32_t* paths, int64_t* waytotal, void* stream);
 
 /* Free the per-device workspace cache of the current device. */
 bpx_status bpx_release_workspace(void);

@@ -95,7 +95,7 @@ int orc_energy(const bpx_options* opts, int nvox, int ndir, const float* data, c
 /* probtrackx simple mode on bedpostx samples (track_oracle.c): adds each kept streamline's
  * distinct voxels to paths [nz][ny][nx] and the kept streamlines to *waytotal. */
 int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nseeds, const float* seeds,
-                  float* paths, int64_t* waytotal);
+                  int32_t* paths, int64_t* waytotal);
 /* the uniforms of one tracking step, and the single-precision sine/cosine both paths use */
 void orc_track_uniforms(uint64_t seed, uint64_t pid, int half, uint32_t step, float u[8]);
 void orc_sincos_fast(float x, float* sn, float* cs);

@@ -56,8 +56,8 @@ def lib():
         L.orc_finish.argtypes = [C.POINTER(Options), C.c_int, _f64p] + [C.c_void_p] * 11
         L.orc_energy.argtypes = [C.POINTER(Options), C.c_int, C.c_int, _f32p, _f32p, _f32p, _f64p,
                                  C.c_void_p, C.c_void_p]
-        L.orc_probtrack.argtypes = [C.POINTER(TrackOptions), C.POINTER(TrackVolume), C.c_int, _f32p, _f32p,
-                                    C.POINTER(C.c_int64)]
+        L.orc_probtrack.argtypes = [C.POINTER(TrackOptions), C.POINTER(TrackVolume), C.c_int, _f32p,
+                                    np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS"), C.POINTER(C.c_int64)]
         L.orc_track_uniforms.argtypes = [C.c_uint64, C.c_uint64, C.c_int, C.c_uint32, _f32p]
         L.orc_sincos_fast.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
         _lib = L
@@ -202,7 +202,7 @@ def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0,
               waypoints=None):
     """probtrackx simple mode on host arrays (th/ph/f [nfib][nsamples][nz][ny][nx], mask [nz][ny][nx],
     seeds [nseeds][3] voxel coordinates; optional avoid and stop masks and a list of waypoint masks,
-    each [nz][ny][nx]): (paths [nz][ny][nx] float32, waytotal)."""
+    each [nz][ny][nx]): (paths [nz][ny][nx] int32, waytotal)."""
     th, ph, f, mask = (np.ascontiguousarray(a, np.float32) for a in (th, ph, f, mask))
     v = TrackVolume()
     v.nfib, v.nsamples, v.nz, v.ny, v.nx = th.shape
@@ -221,7 +221,7 @@ def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0,
             bits |= (np.asarray(m) != 0).astype(np.uint32) << np.uint32(w)
         keep.append(bits)
         v.waypoints, v.nwaypoints = bits.ctypes.data, len(waypoints)
-    paths = np.zeros(mask.shape, np.float32)
+    paths = np.zeros(mask.shape, np.int32)
     way = C.c_int64(0)
     sd = np.ascontiguousarray(seeds, np.float32).reshape(-1, 3)
     rc = lib().orc_probtrack(C.byref(topts), C.byref(v), sd.shape[0], sd, paths, C.byref(way))

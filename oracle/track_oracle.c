@@ -261,7 +261,7 @@ static int half_line(const trk_t* T, part_t* P, uint64_t pid, int h, int fibst0,
 }
 
 int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nseeds, const float* seeds,
-                  float* paths, int64_t* waytotal) {
+                  int32_t* paths, int64_t* waytotal) {
   trk_t T;
   T.o = o;
   T.v = v;
@@ -307,12 +307,16 @@ int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nse
       const int bwd = rej2 == 0;
       if (!fwd && !bwd) continue;
       ++kept;
+      /* Counter::update_pathdist over the kept halves in order: each distinct voxel adds 1, or
+       * with --pd the d-th distinct voxel adds d (int32 sums wrap as the reference's int volume) */
       const int from = fwd ? 0 : n1, to = bwd ? n1 + n2 : n1;
+      uint32_t d = 0;
       for (int i = from; i < to; ++i) {
         const int64_t vx = path[i];
         if (stamp[vx] != (int64_t)pid) {
           stamp[vx] = (int64_t)pid;
-          paths[vx] += 1.0f;
+          ++d;
+          paths[vx] = (int32_t)((uint32_t)paths[vx] + (o->pathdist ? d : 1u));
         }
       }
     }

@@ -4,8 +4,8 @@ Both draw every step's random numbers from the same counter-based stream and do 
 single-precision operations in the same order, so fdt_paths and waytotal must be identical, bit for
 bit (integer counts), for every option the kernel takes: the first fibre chosen by --fibst or at
 random (--randfib 1/2/3), --usef, --sampvox, --distthresh (the two-pass halves), the avoid, stop
-and waypoint masks, short and long step counts, and on the outputs of this library's own bedpostx
-run.
+and waypoint masks, --pd, short and long step counts, and on the outputs of this library's own
+bedpostx run.
 """
 import numpy as np
 import pytest
@@ -40,6 +40,8 @@ CASES = [
     ("stop", dict(masks=("stop",))),
     ("waypoints", dict(masks=("waypoints",))),
     ("all_masks_distthresh", dict(masks=("avoid", "stop", "waypoints"), distthresh=4.0)),
+    ("pathdist", dict(pathdist=1)),
+    ("pathdist_waypoints", dict(pathdist=1, masks=("waypoints",))),
 ]
 
 
@@ -134,7 +136,8 @@ def test_probtrack_cli_with_masks_equals_oracle(torch, tmp_path):
                     "--avoid", os.path.join(d, "avoid.nii.gz"), "--stop", os.path.join(d, "stop.nii.gz"),
                     "--waypoints", os.path.join(d, "ways.txt")])
     o = TrackOptions.make(nparticles=150, nsteps=300, seed=23)
-    want_p, want_w = O.probtrack(o, th, ph, f, mask, seeds, **masks)
+    # the directory's NIfTI files carry unit voxels
+    want_p, want_w = O.probtrack(o, th, ph, f, mask, seeds, voxel_size=(1.0, 1.0, 1.0), **masks)
     got, _ = nifti.read(os.path.join(out, "fdt_paths.nii.gz"))
     assert int(open(os.path.join(out, "waytotal")).read()) == want_w > 0
     assert np.array_equal(np.transpose(got, (2, 1, 0)), want_p)

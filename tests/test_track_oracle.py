@@ -56,6 +56,18 @@ def test_straight_tract_is_followed_both_ways_and_counted_once_per_streamline():
     assert paths.sum() == line.sum()  # a straight path through voxel centres stays on its line
 
 
+def test_pathdist_weights_the_dth_distinct_voxel_by_d():
+    th, ph, f, mask = _straight_box()
+    o = TrackOptions.make(nparticles=20, nsteps=400, seed=3, pathdist=1)
+    paths, way = O.probtrack(o, th, ph, f, mask, [[15.0, 4.0, 4.0]])
+    # 24 distinct voxels per streamline, the seed's first: weights 1..24 whichever half runs first
+    assert way == 20 and paths.dtype == np.int32
+    assert paths[4, 4, 15] == 20 and paths.sum() == 20 * (24 * 25 // 2)
+    # k particles ran +x first (voxel 16 got 2, voxel 14 got 13), the others -x first (14, 2)
+    k, r = divmod(20 * 14 - int(paths[4, 4, 16]), 12)
+    assert r == 0 and 0 < k < 20 and paths[4, 4, 14] == 13 * k + 2 * (20 - k)
+
+
 def test_curvature_threshold_stops_at_a_right_angle_turn():
     th, ph, f, mask = _straight_box()
     ph[:, :, :, :, 20:] = np.pi / 2  # fibres turn to y at x = 20
