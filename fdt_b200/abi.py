@@ -157,7 +157,9 @@ class TrackOptions(C.Structure):
         ("sampvox", C.c_int32),
         ("seed", C.c_uint64),
         ("pathdist", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("loopcheck", C.c_int32),
+        ("modeuler", C.c_int32),
+        ("reserved", C.c_int32 * 1),
     ]
 
     @classmethod

@@ -48,6 +48,12 @@ struct TrackArgs {
   int log2n;
   const float4* packed;  // [nvox][nsamples][pk4] float4: th, ph, f of fibre 0, 1, 2 in turn, zero padded
   int pk4;               // float4 entries per (voxel, sample): 1, 2 or 3
+  // --loopcheck: per-thread tables [threads][1 << lc_log2n] of {coarse cell, stamp} and the
+  // direction last seen there; the coarse grid is lcnx x lcny x lcnz (5x coarser)
+  uint2* lc_keys;
+  float4* lc_dirs;
+  int lc_log2n;
+  int lcnx, lcny;
   uint64_t pid_begin;  // particles [pid_begin, pid_end) of this launch
   uint64_t pid_end;
 };
@@ -59,6 +65,20 @@ __device__ __forceinline__ void track_uniforms(uint64_t seed, uint64_t pid, int 
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
     const uint4 r = philox4x32_10(make_uint4((uint32_t)pid, (uint32_t)(pid >> 32), step, 0x80000000u | (uint32_t)(2 * half + c)), key);
+    u[4 * c + 0] = u24(r.x);
+    u[4 * c + 1] = u24(r.y);
+    u[4 * c + 2] = u24(r.z);
+    u[4 * c + 3] = u24(r.w);
+  }
+}
+
+// the 8 uniforms of a step's modified-Euler test sample: 0-3 its rounding and sample, 4 the test
+// jump's sign before the first jump
+__device__ __forceinline__ void euler_uniforms(uint64_t seed, uint64_t pid, int half, uint32_t step, float (&u)[8]) {
+  const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const uint4 r = philox4x32_10(make_uint4((uint32_t)pid, (uint32_t)(pid >> 32), step, 0xC0000000u | (uint32_t)(2 * half + c)), key);
     u[4 * c + 0] = u24(r.x);
     u[4 * c + 1] = u24(r.y);
     u[4 * c + 2] = u24(r.z);
@@ -83,10 +103,77 @@ __device__ __forceinline__ void reverse(Particle& P) {
   }
 }
 
+// Particle::jump along the unit vector (rxn, ryn, rzn): the sign keeps the direction of travel, or
+// is drawn (u6) on the first jump
+__device__ __forceinline__ void jump_dir(Particle& P, const TrackArgs& a, float rxn, float ryn, float rzn, float u6) {
+  int sign;
+  bool init = false;
+  if (P.jumped) {
+    sign = (rxn * P.rx + ryn * P.ry + rzn * P.rz) > 0.f ? 1 : -1;
+  } else {
+    sign = u6 > 0.5f ? 1 : -1;
+    P.jumped = true;
+    init = true;
+  }
+  const float s = (float)sign;
+  P.x += s * a.o.steplength / a.v.dx * rxn;
+  P.y += s * a.o.steplength / a.v.dy * ryn;
+  P.z += s * a.o.steplength / a.v.dz * rzn;
+  P.rx = s * rxn;
+  P.ry = s * ryn;
+  P.rz = s * rzn;
+  if (init) {
+    P.rxi = P.rx;
+    P.ryi = P.ry;
+    P.rzi = P.rz;
+  }
+}
+
 struct Tracker {
   const TrackArgs& a;
   uint2* tab;
   uint32_t stamp;
+  uint2* lck;        // this thread's loopcheck table
+  float4* lcd;
+  uint32_t lc_stamp;  // one per tracked half (the tables are cleared per launch)
+
+  // --loopcheck: the direction last stored in coarse cell `cell` this half (zero if none), which
+  // is then replaced by d
+  __device__ float3 loop_swap(uint32_t cell, float3 d) const {
+    const uint32_t mask = (1u << a.lc_log2n) - 1u;
+    uint32_t h = (cell * 2654435761u) >> (32 - a.lc_log2n);
+    for (uint32_t probe = 0; probe <= mask; ++probe) {
+      const uint2 e = lck[h];
+      if (e.y != lc_stamp) {
+        lck[h] = make_uint2(cell, lc_stamp);
+        lcd[h] = make_float4(d.x, d.y, d.z, 0.f);
+        return make_float3(0.f, 0.f, 0.f);
+      }
+      if (e.x == cell) {
+        const float4 o = lcd[h];
+        lcd[h] = make_float4(d.x, d.y, d.z, 0.f);
+        return make_float3(o.x, o.y, o.z);
+      }
+      h = (h + 1u) & mask;
+    }
+    return make_float3(0.f, 0.f, 0.f);  // unreachable: the table holds twice the cells of a half
+  }
+
+  // the sample record of voxel `svox`, sample `samp`, as th, ph, f per fibre
+  __device__ void load_record(size_t svox, int samp, float (&sth)[BPX_MAX_FIBRES], float (&sph)[BPX_MAX_FIBRES],
+                              float (&sf)[BPX_MAX_FIBRES]) const {
+    // one 16- to 48-byte record (one or two sectors) instead of 3K scattered words
+    const float4* rec = a.packed + ((size_t)svox * a.v.nsamples + samp) * a.pk4;
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 r0 = __ldg(rec), r1 = a.pk4 > 1 ? __ldg(rec + 1) : zero, r2 = a.pk4 > 2 ? __ldg(rec + 2) : zero;
+    const float e[12] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w};
+#pragma unroll
+    for (int k = 0; k < BPX_MAX_FIBRES; ++k) {
+      sth[k] = e[3 * k];
+      sph[k] = e[3 * k + 1];
+      sf[k] = e[3 * k + 2];
+    }
+  }
 
 
   // first visit of `vox` by this particle: true (and the voxel is recorded)
@@ -108,14 +195,14 @@ struct Tracker {
   // The voxel and posterior sample a step reads (the probabilistic rounding of Tractvolsx::sample):
   // depends only on the position and the step's uniforms, so its loads can be issued together
   // with the mask's.
-  __device__ void locate(const Particle& P, const float (&u)[8], size_t& vox, int& samp) const {
+  __device__ void locate(float x, float y, float z, const float (&u)[8], size_t& vox, int& samp) const {
     const bpx_track_volume& v = a.v;
-    const int cx = (int)ceilf(P.x), fx = (int)floorf(P.x);
-    const int cy = (int)ceilf(P.y), fy = (int)floorf(P.y);
-    const int cz = (int)ceilf(P.z), fz = (int)floorf(P.z);
-    const float pcx = (cx == fx) ? 1.0f : (P.x - (float)fx) / (float)(cx - fx);
-    const float pcy = (cy == fy) ? 1.0f : (P.y - (float)fy) / (float)(cy - fy);
-    const float pcz = (cz == fz) ? 1.0f : (P.z - (float)fz) / (float)(cz - fz);
+    const int cx = (int)ceilf(x), fx = (int)floorf(x);
+    const int cy = (int)ceilf(y), fy = (int)floorf(y);
+    const int cz = (int)ceilf(z), fz = (int)floorf(z);
+    const float pcx = (cx == fx) ? 1.0f : (x - (float)fx) / (float)(cx - fx);
+    const float pcy = (cy == fy) ? 1.0f : (y - (float)fy) / (float)(cy - fy);
+    const float pcz = (cz == fz) ? 1.0f : (z - (float)fz) / (float)(cz - fz);
     const int nx_ = clampi(u[0] > pcx ? fx : cx, 0, v.nx - 1);
     const int ny_ = clampi(u[1] > pcy ? fy : cy, 0, v.ny - 1);
     const int nz_ = clampi(u[2] > pcz ? fz : cz, 0, v.nz - 1);
@@ -210,8 +297,10 @@ struct Tracker {
   // accumulates the waypoint masks passed (over both halves of a particle).  Returns the reject
   // flag: 1 (entered the avoid mask, passed no waypoint, or shorter than distthresh), 2 (passed
   // some waypoints but not all), 0.
+  // EXT: compiled with --modeuler and --loopcheck (the plain form keeps its registers without them)
+  template <bool EXT>
   __device__ int half_line(Particle& P, uint64_t pid, int h, int fibst0, float x0, float y0, float z0,
-                           bool count, uint32_t& flags, int& nvisit) const {
+                           bool count, uint32_t& flags, int& nvisit) {
     const bpx_track_options& o = a.o;
     const bpx_track_volume& v = a.v;
     bool init_sample = true, avoided = false;
@@ -224,6 +313,7 @@ struct Tracker {
     // a step of steplength mm mostly stays in the voxel of the step before, which is counted
     // already: the visit table is probed only when the voxel changes
     uint32_t last = 0xffffffffu;
+    ++lc_stamp;  // every tracked half starts with an empty loopcheck volume
     for (int it = 1; it <= o.nsteps / 2; ++it) {
       const int ix = rnd(P.x), iy = rnd(P.y), iz = rnd(P.z);
       // this step's uniforms and sampled voxel, then the masks at the position and every fibre's
@@ -232,26 +322,23 @@ struct Tracker {
       track_uniforms(o.seed, pid, h, (uint32_t)it, u);
       size_t svox;
       int samp;
-      locate(P, u, svox, samp);
+      locate(P.x, P.y, P.z, u, svox, samp);
       const bool in_grid = ix >= 0 && iy >= 0 && iz >= 0 && ix < v.nx && iy < v.ny && iz < v.nz;
       const uint32_t vox = in_grid ? (uint32_t)(((size_t)iz * v.ny + iy) * v.nx + ix) : 0u;
       const float m = __ldg(v.mask + vox);
       const uint32_t way = v.waypoints ? __ldg(v.waypoints + vox) : 0u;
       const bool avoid = v.avoid && __ldg(v.avoid + vox) != 0.f;
       const bool stop = v.stop && __ldg(v.stop + vox) != 0.f;
-      // the sample: one 16- to 48-byte record (one or two sectors) instead of 3K scattered words
-      const float4* rec = a.packed + ((size_t)svox * v.nsamples + samp) * a.pk4;
-      const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-      const float4 r0 = __ldg(rec), r1 = a.pk4 > 1 ? __ldg(rec + 1) : zero, r2 = a.pk4 > 2 ? __ldg(rec + 2) : zero;
-      const float e[12] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w};
       float sth[BPX_MAX_FIBRES], sph[BPX_MAX_FIBRES], sf[BPX_MAX_FIBRES];
-#pragma unroll
-      for (int k = 0; k < BPX_MAX_FIBRES; ++k) {
-        sth[k] = e[3 * k];
-        sph[k] = e[3 * k + 1];
-        sf[k] = e[3 * k + 2];
-      }
+      load_record(svox, samp, sth, sph, sf);
       if (!(in_grid && m > 0.f)) break;  // the reference's remaining steps change nothing
+      if (EXT && o.loopcheck) {
+        // stop where the path runs against the direction it last had in this coarse cell
+        const int lx = rnd(P.x / 5.0f), ly = rnd(P.y / 5.0f), lz = rnd(P.z / 5.0f);
+        const uint32_t cell = ((uint32_t)lz * (uint32_t)a.lcny + (uint32_t)ly) * (uint32_t)a.lcnx + (uint32_t)lx;
+        const float3 old = loop_swap(cell, make_float3(P.rx, P.ry, P.rz));
+        if (P.rx * old.x + P.ry * old.y + P.rz * old.z < 0.f) break;
+      }
       flags |= way;
       if (count && vox != last) {
         last = vox;
@@ -271,26 +358,40 @@ struct Tracker {
         const float rxn = cp * st, ryn = sp * st, rzn = ct;
         if (P.jumped && !(fabsf(rxn * P.rx + ryn * P.ry + rzn * P.rz) > o.c_thr)) break;
         if (th != 0.f && ph != 0.f) {
-          int sign;
-          bool init = false;
-          if (P.jumped) {
-            sign = (rxn * P.rx + ryn * P.ry + rzn * P.rz) > 0.f ? 1 : -1;
+          if (!EXT || !o.modeuler) {
+            jump_dir(P, a, rxn, ryn, rzn, u[6]);
           } else {
-            sign = u[6] > 0.5f ? 1 : -1;
-            P.jumped = true;
-            init = true;
-          }
-          const float s = (float)sign;
-          P.x += s * o.steplength / a.v.dx * rxn;
-          P.y += s * o.steplength / a.v.dy * ryn;
-          P.z += s * o.steplength / a.v.dz * rzn;
-          P.rx = s * rxn;
-          P.ry = s * ryn;
-          P.rz = s * rzn;
-          if (init) {
-            P.rxi = P.rx;
-            P.ryi = P.ry;
-            P.rzi = P.rz;
+            // Particle::testjump, a sample there, and the jump along the mean of both directions
+            // (mean_sph_pol, streamlines.cc:12-27, as the normalised sum or difference)
+            float w[8];
+            euler_uniforms(o.seed, pid, h, (uint32_t)it, w);
+            int tsign;
+            if (P.jumped)
+              tsign = (rxn * P.rx + ryn * P.ry + rzn * P.rz) > 0.f ? 1 : -1;
+            else
+              tsign = w[4] > 0.5f ? 1 : -1;
+            const float ts = (float)tsign;
+            const float tx = P.x + ts * o.steplength / v.dx * rxn;
+            const float ty = P.y + ts * o.steplength / v.dy * ryn;
+            const float tz = P.z + ts * o.steplength / v.dz * rzn;
+            size_t tvox;
+            int tsamp;
+            locate(tx, ty, tz, w, tvox, tsamp);
+            float tth[BPX_MAX_FIBRES], tph[BPX_MAX_FIBRES], tf[BPX_MAX_FIBRES];
+            load_record(tvox, tsamp, tth, tph, tf);
+            float th2, ph2, f2;
+            choose(P, w, tth, tph, tf, init_sample, fibst, th2, ph2, f2);
+            float st2, ct2, sp2, cp2;
+            sincos_fast(th2, st2, ct2);
+            sincos_fast(ph2, sp2, cp2);
+            const float bx = cp2 * st2, by = sp2 * st2, bz = ct2;
+            const float same = (rxn * bx + ryn * by + rzn * bz) > 0.f ? 1.0f : -1.0f;
+            const float mx = (rxn + same * bx) * 0.5f, my = (ryn + same * by) * 0.5f, mz = (rzn + same * bz) * 0.5f;
+            const float n = sqrtf(mx * mx + my * my + mz * mz);
+            if (n > 0.f)
+              jump_dir(P, a, mx / n, my / n, mz / n, u[6]);
+            else
+              jump_dir(P, a, rxn, ryn, rzn, u[6]);
           }
         }
       }
@@ -306,10 +407,15 @@ struct Tracker {
   }
 };
 
+template <bool EXT>
 __global__ void __launch_bounds__(kTrackThreads, kTrackBlocksPerSm) track_kernel(TrackArgs a) {
   const uint64_t threads = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  Tracker T{a, a.tables + (t << a.log2n), 0u};
+  Tracker T{a, a.tables + (t << a.log2n), 0u, nullptr, nullptr, 0u};
+  if (a.o.loopcheck) {
+    T.lck = a.lc_keys + (t << a.lc_log2n);
+    T.lcd = a.lc_dirs + (t << a.lc_log2n);
+  }
   unsigned long long kept = 0;
   // a half's fate waits on its length (distthresh), on the avoid mask, or on the waypoints both
   // halves passed (Seedmanager::run keeps a first half with reject flag 2 when the second half
@@ -334,25 +440,25 @@ __global__ void __launch_bounds__(kTrackThreads, kTrackBlocksPerSm) track_kernel
     int nvisit = 0;      // distinct voxels counted so far (the first half's before the second's)
     if (decide) {  // whether a half counts is known only once both halves have ended: track, then count
       const Particle P0 = P;
-      const int rej1 = T.half_line(P, pid, 0, fibst, x0, y0, z0, false, flags, nvisit);
+      const int rej1 = T.template half_line<EXT>(P, pid, 0, fibst, x0, y0, z0, false, flags, nvisit);
       reverse(P);
       const Particle P1 = P;
-      const int rej2 = T.half_line(P, pid, 1, fibst, x0, y0, z0, false, flags, nvisit);
+      const int rej2 = T.template half_line<EXT>(P, pid, 1, fibst, x0, y0, z0, false, flags, nvisit);
       const bool fwd = (rej1 == 0 || rej1 == 2) && !(rej2 > 0 && rej1 > 0), bwd = rej2 == 0;
       uint32_t unused = 0;
       if (fwd) {
         Particle Q = P0;
-        T.half_line(Q, pid, 0, fibst, x0, y0, z0, true, unused, nvisit);
+        T.template half_line<EXT>(Q, pid, 0, fibst, x0, y0, z0, true, unused, nvisit);
       }
       if (bwd) {
         Particle Q = P1;
-        T.half_line(Q, pid, 1, fibst, x0, y0, z0, true, unused, nvisit);
+        T.template half_line<EXT>(Q, pid, 1, fibst, x0, y0, z0, true, unused, nvisit);
       }
       if (fwd || bwd) ++kept;
     } else {  // every half is kept: count as it goes
-      T.half_line(P, pid, 0, fibst, x0, y0, z0, true, flags, nvisit);
+      T.template half_line<EXT>(P, pid, 0, fibst, x0, y0, z0, true, flags, nvisit);
       reverse(P);
-      T.half_line(P, pid, 1, fibst, x0, y0, z0, true, flags, nvisit);
+      T.template half_line<EXT>(P, pid, 1, fibst, x0, y0, z0, true, flags, nvisit);
       ++kept;
     }
   }
@@ -461,22 +567,35 @@ bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volu
   int log2n = 1;
   while ((1ll << log2n) < 2ll * (opts->nsteps + 2)) ++log2n;
   a.log2n = log2n;
+  // --loopcheck: a table of at least twice the coarse cells one half can enter
+  a.lcnx = vol->nx / 5 + 2;
+  a.lcny = vol->ny / 5 + 2;
+  const long long lc_cells = (long long)a.lcnx * a.lcny * (vol->nz / 5 + 2);
+  const long long lc_max = lc_cells < opts->nsteps / 2 + 1 ? lc_cells : opts->nsteps / 2 + 1;
+  int lc_log2n = 1;
+  while ((1ll << lc_log2n) < 2 * lc_max) ++lc_log2n;
+  a.lc_log2n = lc_log2n;
+  const size_t lc_bytes = opts->loopcheck ? ((size_t)1 << lc_log2n) * (sizeof(uint2) + sizeof(float4)) : 0;
   // particles in flight: kTrackBlocksPerSm blocks per SM, fewer when the tables of very long paths
   // would pass 8 GB
   const size_t table_bytes = ((size_t)1 << log2n) * sizeof(uint2);
-  const size_t max_blocks = ((size_t)8 << 30) / (table_bytes * kTrackThreads);
+  const size_t max_blocks = ((size_t)8 << 30) / ((table_bytes + lc_bytes) * kTrackThreads);
   int grid = sm_count() * kTrackBlocksPerSm;
   if ((size_t)grid > max_blocks) grid = max_blocks > 0 ? (int)max_blocks : 1;
   const size_t threads = (size_t)grid * kTrackThreads;
-  // workspace: the visit tables, then the repacked samples
+  // workspace: the visit tables, the loopcheck tables (keys, then directions), the repacked samples
   const int pk4 = (3 * vol->nfib + 3) / 4;
   const size_t tab_total = (threads * table_bytes + 255) & ~(size_t)255;
+  const size_t lc_keys = opts->loopcheck ? (threads * ((size_t)1 << lc_log2n) * sizeof(uint2) + 255) & ~(size_t)255 : 0;
+  const size_t lc_dirs = opts->loopcheck ? threads * ((size_t)1 << lc_log2n) * sizeof(float4) : 0;
   const size_t packed_bytes = a.nvox * (size_t)vol->nsamples * (size_t)pk4 * sizeof(float4);
   void* ws = nullptr;
-  st = api_workspace(kWsTrack, tab_total + packed_bytes, &ws);
+  st = api_workspace(kWsTrack, tab_total + lc_keys + lc_dirs + packed_bytes, &ws);
   if (st != BPX_OK) return st;
   a.tables = (uint2*)ws;
-  a.packed = (const float4*)((char*)ws + tab_total);
+  a.lc_keys = opts->loopcheck ? (uint2*)((char*)ws + tab_total) : nullptr;
+  a.lc_dirs = opts->loopcheck ? (float4*)((char*)ws + tab_total + lc_keys) : nullptr;
+  a.packed = (const float4*)((char*)ws + tab_total + lc_keys + lc_dirs);
   a.pk4 = pk4;
   cudaStream_t s = (cudaStream_t)stream;
   {
@@ -491,11 +610,14 @@ bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volu
   const uint64_t chunk = 1ull << 30;  // stamps stay below 2^30 + 1 within a launch
   for (uint64_t b = 0; b < total; b += chunk) {
     // stamp 0 marks every entry empty before a launch reuses the tables
-    const cudaError_t e0 = cudaMemsetAsync(ws, 0, threads * table_bytes, s);
+    const cudaError_t e0 = cudaMemsetAsync(ws, 0, tab_total + lc_keys, s);
     if (e0 != cudaSuccess) return api_cuda_fail(e0, "bpx_probtrack_dev: cudaMemsetAsync");
     a.pid_begin = b;
     a.pid_end = b + chunk < total ? b + chunk : total;
-    track_kernel<<<grid, kTrackThreads, 0, s>>>(a);
+    if (opts->modeuler || opts->loopcheck)
+      track_kernel<true><<<grid, kTrackThreads, 0, s>>>(a);
+    else
+      track_kernel<false><<<grid, kTrackThreads, 0, s>>>(a);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return api_cuda_fail(e, "bpx_probtrack_dev: track_kernel");
   }

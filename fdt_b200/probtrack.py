@@ -2,7 +2,8 @@
 
     python -m fdt_b200.probtrack SUBJECT.bedpostX --seeds seeds.txt --out OUTDIR [-P 5000] [-S 2000]
         [--steplength 0.5] [--cthr 0.2] [--fibthresh 0.01] [--distthresh 0] [--randfib 0] [--fibst 1]
-        [--usef] [--sampvox] [--pd] [--seed N] [--avoid MASK] [--stop MASK] [--waypoints MASK|LIST]
+        [--usef] [--sampvox] [--pd] [-l] [--modeuler] [--seed N] [--avoid MASK] [--stop MASK]
+        [--waypoints MASK|LIST]
 
 Reads merged_th{k}samples, merged_ph{k}samples, merged_f{k}samples and nodif_brain_mask (NIfTI-1)
 as probtrackx does (probtrackx.cc:25-96 with mode simple, tractvolsx.h:55-97), tracks from every
@@ -107,6 +108,8 @@ def main(argv=None) -> None:
     ap.add_argument("-f", "--usef", action="store_true")
     ap.add_argument("--sampvox", action="store_true")
     ap.add_argument("--pd", action="store_true", help="correct the path distribution for the length of the pathways")
+    ap.add_argument("-l", "--loopcheck", action="store_true", help="perform loopchecks on paths")
+    ap.add_argument("--modeuler", action="store_true", help="use modified Euler streamlining")
     ap.add_argument("--seed", type=int, default=8665904)
     ap.add_argument("--avoid", help="reject pathways passing through this mask")
     ap.add_argument("--stop", help="stop tracking at locations given by this mask")
@@ -117,7 +120,8 @@ def main(argv=None) -> None:
         seeds = seeds.T
     o = TrackOptions.make(nparticles=a.nsamples, nsteps=a.nsteps, steplength=a.steplength, c_thr=a.cthr,
                           fibthresh=a.fibthresh, distthresh=a.distthresh, randfib=a.randfib, fibst=a.fibst,
-                          usef=int(a.usef), sampvox=int(a.sampvox), pathdist=int(a.pd), seed=a.seed)
+                          usef=int(a.usef), sampvox=int(a.sampvox), pathdist=int(a.pd), loopcheck=int(a.loopcheck),
+                          modeuler=int(a.modeuler), seed=a.seed)
     _, way = run(a.bpx_dir, seeds, o, a.out, avoid=a.avoid, stop=a.stop, waypoints=a.waypoints)
     print(f"waytotal {way}")
 

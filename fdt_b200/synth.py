@@ -294,3 +294,16 @@ def write_bedpostx_dir(d: str, th, ph, f, mask) -> None:
         for k in range(a.shape[0]):
             nifti.write(os.path.join(d, f"merged_{q}{k + 1}samples.nii.gz"), np.transpose(a[k], (3, 2, 1, 0)))
     nifti.write(os.path.join(d, "nodif_brain_mask.nii.gz"), np.transpose(mask, (2, 1, 0)))
+
+
+def circle_field(n: int = 24, nz: int = 6, nsamples: int = 8):
+    """Fibres along circles about the grid's central z axis (th, ph, f [1][nsamples][nz][n][n] and a
+    full mask): streamlines from a seed near the axis circle back through their own path."""
+    c = (n - 1) / 2.0
+    x = np.arange(n)[None, :]
+    y = np.arange(n)[:, None]
+    phi = (np.arctan2(y - c, x - c) + np.pi / 2).astype(np.float32)
+    th = np.full((1, nsamples, nz, n, n), np.pi / 2, np.float32)
+    ph = np.ascontiguousarray(np.broadcast_to(phi, th.shape))
+    f = np.full_like(th, 0.8)
+    return th, ph, f, np.ones((nz, n, n), np.float32)

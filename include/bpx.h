@@ -452,7 +452,11 @@ typedef struct bpx_track_options {
   uint64_t seed;       /* random seed */
   int32_t pathdist;    /* --pd: the d-th distinct voxel of a kept streamline adds d (path length
                           correction), not 1 (Counter::update_pathdist, streamlines.cc:662-690) */
-  int32_t reserved[3]; /* zero */
+  int32_t loopcheck;   /* -l, --loopcheck: a half stops where it runs against the direction it
+                          last had in the same cell of a 5x coarser grid (streamlines.cc:248-263) */
+  int32_t modeuler;    /* --modeuler: modified Euler steps, along the mean of the sampled direction
+                          and the one sampled a step ahead (streamlines.cc:352-361) */
+  int32_t reserved[1]; /* zero */
 } bpx_track_options;
 
 /* The bedpostx outputs probtrackx reads, on the device.  Sample arrays [nfib][nsamples][nz][ny][nx]

@@ -98,6 +98,7 @@ int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nse
                   int32_t* paths, int64_t* waytotal);
 /* the uniforms of one tracking step, and the single-precision sine/cosine both paths use */
 void orc_track_uniforms(uint64_t seed, uint64_t pid, int half, uint32_t step, float u[8]);
+void orc_track_uniforms_euler(uint64_t seed, uint64_t pid, int half, uint32_t step, float u[8]);
 void orc_sincos_fast(float x, float* sn, float* cs);
 
 #ifdef __cplusplus

@@ -15,7 +15,8 @@
  *                               a random posterior sample, the first fibre (fibst, randfib 1/2)
  *                               and afterwards the fibre closest to the current direction among
  *                               those with f > fibthresh, f for --usef;
- *   Particle::jump / check_dir / restart_reverse (particle.h).
+ *   Particle::jump / testjump / check_dir / restart_reverse (particle.h), --modeuler's test
+ *                               sample and mean direction, --loopcheck's coarse direction volume.
  * The reference draws from rand(); here every step's uniforms come from Philox-4x32-10 keyed by
  * the seed and counted by (particle, half, step), exactly as the GPU kernel draws them, and the
  * arithmetic is single precision in the reference's operation order, with the sine and cosine of
@@ -108,16 +109,16 @@ static size_t at(const trk_t* T, int k, int s, size_t vox) {
   return ((size_t)k * T->v->nsamples + s) * T->nvox + vox;
 }
 
-/* Tractvolsx::sample: theta, phi and f of one step */
-static void sample(const trk_t* T, const part_t* P, const float u[8], int* init_sample, int* fibst, float* th,
-                   float* ph, float* f) {
+/* Tractvolsx::sample at position (x, y, z) with the particle's direction P->r: theta, phi and f */
+static void sample(const trk_t* T, const part_t* P, float x, float y, float z, const float u[8], int* init_sample,
+                   int* fibst, float* th, float* ph, float* f) {
   const bpx_track_volume* v = T->v;
-  const int cx = (int)ceilf(P->x), fx = (int)floorf(P->x);
-  const int cy = (int)ceilf(P->y), fy = (int)floorf(P->y);
-  const int cz = (int)ceilf(P->z), fz = (int)floorf(P->z);
-  const float pcx = (cx == fx) ? 1.0f : (P->x - (float)fx) / (float)(cx - fx);
-  const float pcy = (cy == fy) ? 1.0f : (P->y - (float)fy) / (float)(cy - fy);
-  const float pcz = (cz == fz) ? 1.0f : (P->z - (float)fz) / (float)(cz - fz);
+  const int cx = (int)ceilf(x), fx = (int)floorf(x);
+  const int cy = (int)ceilf(y), fy = (int)floorf(y);
+  const int cz = (int)ceilf(z), fz = (int)floorf(z);
+  const float pcx = (cx == fx) ? 1.0f : (x - (float)fx) / (float)(cx - fx);
+  const float pcy = (cy == fy) ? 1.0f : (y - (float)fy) / (float)(cy - fy);
+  const float pcz = (cz == fz) ? 1.0f : (z - (float)fz) / (float)(cz - fz);
   const int nx_ = clampi(u[0] > pcx ? fx : cx, 0, v->nx - 1);
   const int ny_ = clampi(u[1] > pcy ? fy : cy, 0, v->ny - 1);
   const int nz_ = clampi(u[2] > pcz ? fz : cz, 0, v->nz - 1);
@@ -191,12 +192,57 @@ static void sample(const trk_t* T, const part_t* P, const float u[8], int* init_
   *f = T->o->usef ? v->f[at(T, fibind, samp, vox)] : 1.0f;
 }
 
+/* the 8 uniforms of a step's modified-Euler test sample (--modeuler): 0-3 its rounding and sample,
+ * 4 the test jump's sign before the first jump */
+void orc_track_uniforms_euler(uint64_t seed, uint64_t pid, int half, uint32_t step, float u[8]) {
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  for (int c = 0; c < 2; ++c) {
+    const uint32_t ctr[4] = {(uint32_t)pid, (uint32_t)(pid >> 32), step, 0xC0000000u | (uint32_t)(2 * half + c)};
+    uint32_t r[4];
+    orc_philox4x32_10(ctr, key, r);
+    for (int i = 0; i < 4; ++i) u[4 * c + i] = u24(r[i]);
+  }
+}
+
+/* Particle::jump along the unit vector (rxn, ryn, rzn); the sign keeps the direction of travel, or is
+ * drawn (u6) on the first jump */
+static void jump_dir(const trk_t* T, part_t* P, float rxn, float ryn, float rzn, float u6) {
+  const bpx_track_options* o = T->o;
+  int sign, init = 0;
+  if (P->jumped) {
+    sign = (rxn * P->rx + ryn * P->ry + rzn * P->rz) > 0.f ? 1 : -1;
+  } else {
+    sign = u6 > 0.5f ? 1 : -1;
+    P->jumped = 1;
+    init = 1;
+  }
+  const float s = (float)sign;
+  P->x += s * o->steplength / T->v->dx * rxn;
+  P->y += s * o->steplength / T->v->dy * ryn;
+  P->z += s * o->steplength / T->v->dz * rzn;
+  P->rx = s * rxn;
+  P->ry = s * ryn;
+  P->rz = s * rzn;
+  if (init) {
+    P->rxi = P->rx;
+    P->ryi = P->ry;
+    P->rzi = P->rz;
+  }
+}
+
+/* --loopcheck's volume of last directions on a 5x coarser grid (Streamliner::m_loopcheck,
+ * streamlines.cc:112-116,248-263), cleared after every half */
+typedef struct {
+  int nx, ny, nz;
+  float* dir; /* [nz][ny][nx][3] */
+} loopvol_t;
+
 /* one half of a streamline (Streamliner::streamline); appends the path's voxels to path[];
  * *flags accumulates the waypoint masks passed (over both halves of a particle); returns the
  * reject flag: 1 (entered the avoid mask, passed no waypoint, or shorter than distthresh), 2 (passed
  * some waypoints but not all), 0 */
 static int half_line(const trk_t* T, part_t* P, uint64_t pid, int h, int fibst0, float x0, float y0, float z0,
-                     int64_t* path, int* npath, uint32_t* flags) {
+                     int64_t* path, int* npath, uint32_t* flags, loopvol_t* lc) {
   const bpx_track_options* o = T->o;
   const bpx_track_volume* v = T->v;
   int init_sample = 1, fibst = fibst0, avoided = 0;
@@ -207,6 +253,15 @@ static int half_line(const trk_t* T, part_t* P, uint64_t pid, int h, int fibst0,
   for (int it = 1; it <= o->nsteps / 2; ++it) {
     const int ix = rnd(P->x), iy = rnd(P->y), iz = rnd(P->z);
     if (!inside(T, ix, iy, iz)) break;  /* the reference's remaining steps change nothing */
+    if (o->loopcheck) {
+      /* stop where the path runs against the direction it last had in this coarse cell */
+      const int lx = rnd(P->x / 5.0f), ly = rnd(P->y / 5.0f), lz = rnd(P->z / 5.0f);
+      float* d = lc->dir + 3 * (((size_t)lz * lc->ny + ly) * lc->nx + lx);
+      if (P->rx * d[0] + P->ry * d[1] + P->rz * d[2] < 0.f) break;
+      d[0] = P->rx;
+      d[1] = P->ry;
+      d[2] = P->rz;
+    }
     const int64_t vox = ((int64_t)iz * v->ny + iy) * v->nx + ix;
     if (v->waypoints) *flags |= v->waypoints[vox];
     path[(*npath)++] = vox;
@@ -218,7 +273,7 @@ static int half_line(const trk_t* T, part_t* P, uint64_t pid, int h, int fibst0,
     if (v->stop && v->stop[vox] != 0.f) break;
     float u[8], th, ph, f;
     orc_track_uniforms(o->seed, pid, h, (uint32_t)it, u);
-    sample(T, P, u, &init_sample, &fibst, &th, &ph, &f);
+    sample(T, P, P->x, P->y, P->z, u, &init_sample, &fibst, &th, &ph, &f);
     if (f > u[5]) {
       float st, ct, sp, cp;
       orc_sincos_fast(th, &st, &ct);
@@ -226,29 +281,40 @@ static int half_line(const trk_t* T, part_t* P, uint64_t pid, int h, int fibst0,
       const float rxn = cp * st, ryn = sp * st, rzn = ct;
       if (P->jumped && !(fabsf(rxn * P->rx + ryn * P->ry + rzn * P->rz) > o->c_thr)) break;
       if (th != 0.f && ph != 0.f) {
-        int sign, init = 0;
-        if (P->jumped) {
-          sign = (rxn * P->rx + ryn * P->ry + rzn * P->rz) > 0.f ? 1 : -1;
+        if (!o->modeuler) {
+          jump_dir(T, P, rxn, ryn, rzn, u[6]);
         } else {
-          sign = u[6] > 0.5f ? 1 : -1;
-          P->jumped = 1;
-          init = 1;
-        }
-        const float s = (float)sign;
-        P->x += s * o->steplength / T->v->dx * rxn;
-        P->y += s * o->steplength / T->v->dy * ryn;
-        P->z += s * o->steplength / T->v->dz * rzn;
-        P->rx = s * rxn;
-        P->ry = s * ryn;
-        P->rz = s * rzn;
-        if (init) {
-          P->rxi = P->rx;
-          P->ryi = P->ry;
-          P->rzi = P->rz;
+          /* Particle::testjump, a sample there, and the jump along the mean of both directions
+           * (mean_sph_pol, streamlines.cc:12-27, as the normalised sum or difference) */
+          float w[8];
+          orc_track_uniforms_euler(o->seed, pid, h, (uint32_t)it, w);
+          int tsign;
+          if (P->jumped)
+            tsign = (rxn * P->rx + ryn * P->ry + rzn * P->rz) > 0.f ? 1 : -1;
+          else
+            tsign = w[4] > 0.5f ? 1 : -1;
+          const float ts = (float)tsign;
+          const float tx = P->x + ts * o->steplength / v->dx * rxn;
+          const float ty = P->y + ts * o->steplength / v->dy * ryn;
+          const float tz = P->z + ts * o->steplength / v->dz * rzn;
+          float th2, ph2, f2;
+          sample(T, P, tx, ty, tz, w, &init_sample, &fibst, &th2, &ph2, &f2);
+          float st2, ct2, sp2, cp2;
+          orc_sincos_fast(th2, &st2, &ct2);
+          orc_sincos_fast(ph2, &sp2, &cp2);
+          const float bx = cp2 * st2, by = sp2 * st2, bz = ct2;
+          const float same = (rxn * bx + ryn * by + rzn * bz) > 0.f ? 1.0f : -1.0f;
+          const float mx = (rxn + same * bx) * 0.5f, my = (ryn + same * by) * 0.5f, mz = (rzn + same * bz) * 0.5f;
+          const float n = sqrtf(mx * mx + my * my + mz * mz);
+          if (n > 0.f)
+            jump_dir(T, P, mx / n, my / n, mz / n, u[6]);
+          else
+            jump_dir(T, P, rxn, ryn, rzn, u[6]);
         }
       }
     }
   }
+  if (o->loopcheck) memset(lc->dir, 0, sizeof(float) * 3 * (size_t)lc->nx * lc->ny * lc->nz);
   int rej = 0;
   if (v->nwaypoints > 0) {
     const uint32_t all = v->nwaypoints >= 32 ? 0xffffffffu : ((1u << v->nwaypoints) - 1u);
@@ -275,6 +341,16 @@ int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nse
     return 1;
   }
   for (size_t i = 0; i < T.nvox; ++i) stamp[i] = -1;
+  /* the coarse grid covers round(x / 5) for x in [-0.5, n - 0.5) */
+  loopvol_t lc = {v->nx / 5 + 2, v->ny / 5 + 2, v->nz / 5 + 2, NULL};
+  if (o->loopcheck) {
+    lc.dir = (float*)calloc(3 * (size_t)lc.nx * lc.ny * lc.nz, sizeof(float));
+    if (!lc.dir) {
+      free(path);
+      free(stamp);
+      return 1;
+    }
+  }
   int64_t kept = 0;
   for (int s = 0; s < nseeds; ++s) {
     for (int p = 0; p < o->nparticles; ++p) {
@@ -294,13 +370,13 @@ int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nse
       memset(&P, 0, sizeof(P));
       int n1 = 0, n2 = 0;
       uint32_t flags = 0; /* waypoints passed, over both halves (Streamliner::reset clears them per particle) */
-      const int rej1 = half_line(&T, &P, pid, 0, fibst, x0, y0, z0, path, &n1, &flags);
+      const int rej1 = half_line(&T, &P, pid, 0, fibst, x0, y0, z0, path, &n1, &flags, &lc);
       if (P.jumped) { /* Particle::restart_reverse */
         P.rx = -P.rxi;
         P.ry = -P.ryi;
         P.rz = -P.rzi;
       }
-      const int rej2 = half_line(&T, &P, pid, 1, fibst, x0, y0, z0, path + n1, &n2, &flags);
+      const int rej2 = half_line(&T, &P, pid, 1, fibst, x0, y0, z0, path + n1, &n2, &flags, &lc);
       /* Seedmanager::run: the first half is kept on flag 0, or on 2 when the second half completes
        * the waypoints; the second half on flag 0 */
       const int fwd = (rej1 == 0 || rej1 == 2) && !(rej2 > 0 && rej1 > 0);
@@ -324,5 +400,6 @@ int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nse
   *waytotal += kept;
   free(path);
   free(stamp);
+  free(lc.dir);
   return 0;
 }

@@ -4,8 +4,8 @@ Both draw every step's random numbers from the same counter-based stream and do 
 single-precision operations in the same order, so fdt_paths and waytotal must be identical, bit for
 bit (integer counts), for every option the kernel takes: the first fibre chosen by --fibst or at
 random (--randfib 1/2/3), --usef, --sampvox, --distthresh (the two-pass halves), the avoid, stop
-and waypoint masks, --pd, short and long step counts, and on the outputs of this library's own
-bedpostx run.
+and waypoint masks, --pd, --modeuler, --loopcheck (also on circling tracts, where it acts), short
+and long step counts, and on the outputs of this library's own bedpostx run.
 """
 import numpy as np
 import pytest
@@ -42,6 +42,10 @@ CASES = [
     ("all_masks_distthresh", dict(masks=("avoid", "stop", "waypoints"), distthresh=4.0)),
     ("pathdist", dict(pathdist=1)),
     ("pathdist_waypoints", dict(pathdist=1, masks=("waypoints",))),
+    ("modeuler", dict(modeuler=1)),
+    ("modeuler_randfib2_usef", dict(modeuler=1, randfib=2, usef=1)),
+    ("loopcheck_low_cthr", dict(loopcheck=1, c_thr=0.05)),
+    ("everything", dict(modeuler=1, loopcheck=1, pathdist=1, distthresh=3.0, masks=("avoid", "stop", "waypoints"))),
 ]
 
 
@@ -141,3 +145,20 @@ def test_probtrack_cli_with_masks_equals_oracle(torch, tmp_path):
     got, _ = nifti.read(os.path.join(out, "fdt_paths.nii.gz"))
     assert int(open(os.path.join(out, "waytotal")).read()) == want_w > 0
     assert np.array_equal(np.transpose(got, (2, 1, 0)), want_p)
+
+
+@pytest.mark.parametrize("modeuler", [0, 1])
+def test_loopcheck_on_circling_tracts_equals_oracle(torch, modeuler):
+    from fdt_b200 import lib
+
+    lib.load()
+    th, ph, f, mask = synth.circle_field()
+    seeds = np.array([[13.5, 11.5, 3.0], [17.5, 11.5, 2.0], [11.5, 14.2, 4.0]], np.float32)
+    o = TrackOptions.make(nparticles=300, nsteps=1000, seed=21, loopcheck=1, modeuler=modeuler)
+    want_p, want_w = O.probtrack(o, th, ph, f, mask, seeds)
+    got_p, got_w = lib.probtrack(o, *(lib.to_device(a) for a in (th, ph, f, mask)), seeds)
+    torch.cuda.synchronize()
+    assert got_w == want_w and np.array_equal(got_p.cpu().numpy(), want_p)
+    o.loopcheck = 0
+    free, _ = O.probtrack(o, th, ph, f, mask, seeds)
+    assert want_p.sum() < free.sum()  # the check acted

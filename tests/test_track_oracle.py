@@ -3,7 +3,9 @@
 whose answer is known: a straight tract is followed to the mask boundary in both directions and
 every voxel on it is counted once per streamline; the curvature threshold stops a streamline at a
 right-angle turn; the distance threshold drops short streamlines; the avoid, stop and waypoint
-masks reject, end and select halves as Seedmanager::run and Streamliner::streamline do."""
+masks reject, end and select halves as Seedmanager::run and Streamliner::streamline do; --pd
+weights voxels by their order on the path; --loopcheck stops paths that circle back on themselves;
+--modeuler follows a straight tract as the plain steps do."""
 import os
 import re
 
@@ -66,6 +68,38 @@ def test_pathdist_weights_the_dth_distinct_voxel_by_d():
     # k particles ran +x first (voxel 16 got 2, voxel 14 got 13), the others -x first (14, 2)
     k, r = divmod(20 * 14 - int(paths[4, 4, 16]), 12)
     assert r == 0 and 0 < k < 20 and paths[4, 4, 14] == 13 * k + 2 * (20 - k)
+
+
+def test_loopcheck_stops_paths_that_circle_back():
+    th, ph, f, mask = synth.circle_field()
+    seed = [[13.5, 11.5, 3.0]]  # two voxels from the axis: a circle fits in one coarse cell
+    o = TrackOptions.make(nparticles=40, nsteps=1000, seed=3)
+    free, way0 = O.probtrack(o, th, ph, f, mask, seed)
+    o.loopcheck = 1
+    checked, way1 = O.probtrack(o, th, ph, f, mask, seed)
+    assert way0 == way1 == 40 and checked.sum() < 0.4 * free.sum() and np.all(checked <= free)
+    # a straight tract never runs against itself
+    th, ph, f, mask = _straight_box()
+    o = TrackOptions.make(nparticles=20, nsteps=400, seed=3)
+    plain, _ = O.probtrack(o, th, ph, f, mask, [[15.0, 4.0, 4.0]])
+    o.loopcheck = 1
+    assert np.array_equal(O.probtrack(o, th, ph, f, mask, [[15.0, 4.0, 4.0]])[0], plain)
+
+
+def test_modeuler_follows_a_straight_tract_as_the_plain_steps_do():
+    th, ph, f, mask = _straight_box()
+    o = TrackOptions.make(nparticles=20, nsteps=400, seed=3)
+    plain, _ = O.probtrack(o, th, ph, f, mask, [[15.0, 4.0, 4.0]])
+    o.modeuler = 1
+    euler, way = O.probtrack(o, th, ph, f, mask, [[15.0, 4.0, 4.0]])
+    assert way == 20 and np.array_equal(euler, plain)
+    # on the circles the mean of the direction here and a step ahead differs from the plain step
+    th, ph, f, mask = synth.circle_field()
+    o = TrackOptions.make(nparticles=20, nsteps=300, seed=3)
+    a, _ = O.probtrack(o, th, ph, f, mask, [[17.5, 11.5, 3.0]])
+    o.modeuler = 1
+    b, _ = O.probtrack(o, th, ph, f, mask, [[17.5, 11.5, 3.0]])
+    assert not np.array_equal(a, b) and a.sum() > 0 and b.sum() > 0
 
 
 def test_curvature_threshold_stops_at_a_right_angle_turn():
