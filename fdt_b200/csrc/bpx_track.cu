@@ -60,24 +60,33 @@ struct TrackArgs {
 
 __device__ __forceinline__ float u24(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
 
-__device__ __forceinline__ void track_uniforms(uint64_t seed, uint64_t pid, int half, uint32_t step, float (&u)[8]) {
+// block c (0 or 1) of a step's uniforms: u[4c .. 4c+3]
+__device__ __forceinline__ void uniform_block(uint64_t seed, uint64_t pid, int half, uint32_t step, int c,
+                                              float (&u)[8]) {
   const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
-#pragma unroll
-  for (int c = 0; c < 2; ++c) {
-    const uint4 r = philox4x32_10(make_uint4((uint32_t)pid, (uint32_t)(pid >> 32), step, 0x80000000u | (uint32_t)(2 * half + c)), key);
-    u[4 * c + 0] = u24(r.x);
-    u[4 * c + 1] = u24(r.y);
-    u[4 * c + 2] = u24(r.z);
-    u[4 * c + 3] = u24(r.w);
-  }
+  const uint4 r = philox4x32_10(make_uint4((uint32_t)pid, (uint32_t)(pid >> 32), step, 0x80000000u | (uint32_t)(2 * half + c)), key);
+  u[4 * c + 0] = u24(r.x);
+  u[4 * c + 1] = u24(r.y);
+  u[4 * c + 2] = u24(r.z);
+  u[4 * c + 3] = u24(r.w);
 }
 
-// the 8 uniforms of a step's modified-Euler test sample: 0-3 its rounding and sample, 4 the test
-// jump's sign before the first jump
-__device__ __forceinline__ void euler_uniforms(uint64_t seed, uint64_t pid, int half, uint32_t step, float (&u)[8]) {
+__device__ __forceinline__ void track_uniforms(uint64_t seed, uint64_t pid, int half, uint32_t step, float (&u)[8]) {
+  uniform_block(seed, pid, half, step, 0, u);
+  uniform_block(seed, pid, half, step, 1, u);
+}
+
+// the uniforms of a step's modified-Euler test sample: 0-3 its rounding and sample, 4 the test
+// jump's sign before the first jump (the second block only when `second`; else 4-7 are zero)
+__device__ __forceinline__ void euler_uniforms(uint64_t seed, uint64_t pid, int half, uint32_t step, bool second,
+                                               float (&u)[8]) {
   const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
+    if (c == 1 && !second) {
+      u[4] = u[5] = u[6] = u[7] = 0.f;
+      break;
+    }
     const uint4 r = philox4x32_10(make_uint4((uint32_t)pid, (uint32_t)(pid >> 32), step, 0xC0000000u | (uint32_t)(2 * half + c)), key);
     u[4 * c + 0] = u24(r.x);
     u[4 * c + 1] = u24(r.y);
@@ -318,8 +327,15 @@ struct Tracker {
       const int ix = rnd(P.x), iy = rnd(P.y), iz = rnd(P.z);
       // this step's uniforms and sampled voxel, then the masks at the position and every fibre's
       // sample in one round of loads (the reference reads them only inside the mask: same values)
+      // this step's uniforms: the first block always (rounding, sample); the second (randfib's
+      // draw, the --usef test, the first jump's sign) only while one of its draws can be used
       float u[8], th, ph, f;
-      track_uniforms(o.seed, pid, h, (uint32_t)it, u);
+      uniform_block(o.seed, pid, h, (uint32_t)it, 0, u);
+      if (o.usef || !P.jumped || (init_sample && K > 1 && (o.randfib == 1 || o.randfib == 2))) {
+        uniform_block(o.seed, pid, h, (uint32_t)it, 1, u);
+      } else {
+        u[4] = u[5] = u[6] = u[7] = 0.f;  // f is 1 without --usef, so the step is taken
+      }
       size_t svox;
       int samp;
       locate(P.x, P.y, P.z, u, svox, samp);
@@ -364,7 +380,7 @@ struct Tracker {
             // Particle::testjump, a sample there, and the jump along the mean of both directions
             // (mean_sph_pol, streamlines.cc:12-27, as the normalised sum or difference)
             float w[8];
-            euler_uniforms(o.seed, pid, h, (uint32_t)it, w);
+            euler_uniforms(o.seed, pid, h, (uint32_t)it, !P.jumped, w);
             int tsign;
             if (P.jumped)
               tsign = (rxn * P.rx + ryn * P.ry + rzn * P.rz) > 0.f ? 1 : -1;
