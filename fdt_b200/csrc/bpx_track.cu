@@ -14,7 +14,8 @@
 // at a randomly rounded position, then the step), so the kernel is latency-bound: a persistent
 // grid keeps as many particles in flight as the tables' workspace allows and every thread walks its
 // particles in turn.  The samples are first repacked (pack_samples_kernel) so that one step reads
-// one record of every fibre's th, ph and f instead of 3K scattered words.
+// one record of every fibre's direction and f instead of 3K scattered words, and forms no sine or
+// cosine of the sampled angles.
 //
 // Arithmetic: single precision in the reference's operation order, no contraction into FMAs (this
 // file is compiled with -fmad=false), sine and cosine from sincos_fast; random numbers from
@@ -46,14 +47,18 @@ struct TrackArgs {
   unsigned long long* waytotal;
   uint2* tables;       // [threads][1 << log2n] {voxel, stamp}
   int log2n;
-  const float4* packed;  // [nvox][nsamples][pk4] float4: th, ph, f of fibre 0, 1, 2 in turn, zero padded
-  int pk4;               // float4 entries per (voxel, sample): 1, 2 or 3
+  // [nvox][nsamples][pk4] float4: per fibre k, {v_x, v_y, v_z, f} with v = (sin th cos ph,
+  // sin th sin ph, cos th) from sincos_fast; then one entry whose x holds bit k set when th_k and
+  // ph_k are both non-zero (the reference takes no step along a sample with either exactly 0)
+  const float4* packed;
+  int pk4;  // float4 entries per (voxel, sample): nfib + 1
   // --loopcheck: per-thread tables [threads][1 << lc_log2n] of {coarse cell, stamp} and the
   // direction last seen there; the coarse grid is lcnx x lcny x lcnz (5x coarser)
   uint2* lc_keys;
   float4* lc_dirs;
   int lc_log2n;
   int lcnx, lcny;
+  float sx, sy, sz;  // steplength / dx, dy, dz
   uint64_t pid_begin;  // particles [pid_begin, pid_end) of this launch
   uint64_t pid_end;
 };
@@ -125,9 +130,11 @@ __device__ __forceinline__ void jump_dir(Particle& P, const TrackArgs& a, float 
     init = true;
   }
   const float s = (float)sign;
-  P.x += s * a.o.steplength / a.v.dx * rxn;
-  P.y += s * a.o.steplength / a.v.dy * ryn;
-  P.z += s * a.o.steplength / a.v.dz * rzn;
+  // (s * steplength) / dx equals s * (steplength / dx) exactly for s = +-1: the quotients are
+  // formed once per launch (TrackArgs::sx, sy, sz)
+  P.x += s * a.sx * rxn;
+  P.y += s * a.sy * ryn;
+  P.z += s * a.sz * rzn;
   P.rx = s * rxn;
   P.ry = s * ryn;
   P.rz = s * rzn;
@@ -168,22 +175,30 @@ struct Tracker {
     return make_float3(0.f, 0.f, 0.f);  // unreachable: the table holds twice the cells of a half
   }
 
-  // the sample record of voxel `svox`, sample `samp`, as th, ph, f per fibre
-  __device__ void load_record(size_t svox, int samp, float (&sth)[BPX_MAX_FIBRES], float (&sph)[BPX_MAX_FIBRES],
-                              float (&sf)[BPX_MAX_FIBRES]) const {
-    // one 16- to 48-byte record (one or two sectors) instead of 3K scattered words
+  // the sample record of voxel `svox`, sample `samp`: every fibre's direction and f, and the
+  // non-zero-angle bits
+  struct Sample {
+    float vx[BPX_MAX_FIBRES], vy[BPX_MAX_FIBRES], vz[BPX_MAX_FIBRES], f[BPX_MAX_FIBRES];
+    uint32_t moves;  // bit k: th_k != 0 and ph_k != 0
+  };
+  __device__ void load_record(size_t svox, int samp, Sample& S) const {
+    // one 32- to 64-byte record (one or two sectors)
     const float4* rec = a.packed + ((size_t)svox * a.v.nsamples + samp) * a.pk4;
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 r0 = __ldg(rec), r1 = a.pk4 > 1 ? __ldg(rec + 1) : zero, r2 = a.pk4 > 2 ? __ldg(rec + 2) : zero;
-    const float e[12] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w};
+    float4 r[BPX_MAX_FIBRES + 1];
+#pragma unroll
+    for (int q = 0; q <= BPX_MAX_FIBRES; ++q) r[q] = a.pk4 > q ? __ldg(rec + q) : zero;
+    float4 fl = r[1];
 #pragma unroll
     for (int k = 0; k < BPX_MAX_FIBRES; ++k) {
-      sth[k] = e[3 * k];
-      sph[k] = e[3 * k + 1];
-      sf[k] = e[3 * k + 2];
+      S.vx[k] = r[k].x;
+      S.vy[k] = r[k].y;
+      S.vz[k] = r[k].z;
+      S.f[k] = r[k].w;
+      if (a.pk4 == k + 2) fl = r[k + 1];
     }
+    S.moves = __float_as_uint(fl.x);
   }
-
 
   // first visit of `vox` by this particle: true (and the voxel is recorded)
   __device__ bool first_visit(uint32_t vox) const {
@@ -209,9 +224,10 @@ struct Tracker {
     const int cx = (int)ceilf(x), fx = (int)floorf(x);
     const int cy = (int)ceilf(y), fy = (int)floorf(y);
     const int cz = (int)ceilf(z), fz = (int)floorf(z);
-    const float pcx = (cx == fx) ? 1.0f : (x - (float)fx) / (float)(cx - fx);
-    const float pcy = (cy == fy) ? 1.0f : (y - (float)fy) / (float)(cy - fy);
-    const float pcz = (cz == fz) ? 1.0f : (z - (float)fz) / (float)(cz - fz);
+    // (x - fx) / (cx - fx) with cx - fx = 1 whenever it is formed: the quotient is x - fx exactly
+    const float pcx = (cx == fx) ? 1.0f : (x - (float)fx);
+    const float pcy = (cy == fy) ? 1.0f : (y - (float)fy);
+    const float pcz = (cz == fz) ? 1.0f : (z - (float)fz);
     const int nx_ = clampi(u[0] > pcx ? fx : cx, 0, v.nx - 1);
     const int ny_ = clampi(u[1] > pcy ? fy : cy, 0, v.ny - 1);
     const int nz_ = clampi(u[2] > pcz ? fz : cz, 0, v.nz - 1);
@@ -219,38 +235,37 @@ struct Tracker {
     samp = clampi(rnd(u[3] * (float)(v.nsamples - 1)), 0, v.nsamples - 1);
   }
 
-  // The fibre choice of Tractvolsx::sample on the voxel's sample (every fibre's th, ph, f loaded)
-  __device__ void choose(const Particle& P, const float (&u)[8], const float (&sth)[BPX_MAX_FIBRES],
-                         const float (&sph)[BPX_MAX_FIBRES], const float (&sf)[BPX_MAX_FIBRES], bool& init_sample,
-                         int& fibst, float& th, float& ph, float& f) const {
+  // The fibre choice of Tractvolsx::sample on the voxel's sample: the chosen fibre's direction
+  // (r), whether its angles are both non-zero (moves) and f (1 without --usef)
+  __device__ void choose(const Particle& P, const float (&u)[8], const Sample& S, bool& init_sample, int& fibst,
+                         float3& r, bool& moves, float& f) const {
     const int K = a.v.nfib;
     const float thr = a.o.fibthresh;
-    float theta = 0.f, phi = 0.f;
-    int fibind = 0;
+    int sel = 0, fibind = 0;
     if (K > 1) {
       if (init_sample) {
         if (a.o.randfib == 1) {
           int list[BPX_MAX_FIBRES], n = 0;
 #pragma unroll
           for (int k = 0; k < BPX_MAX_FIBRES; ++k)
-            if (k < K && sf[k] > thr) list[n++] = k;
+            if (k < K && S.f[k] > thr) list[n++] = k;
           fibst = n == 0 ? 0 : list[clampi(rnd(u[4] * (float)(n - 1)), 0, n - 1)];
         } else if (a.o.randfib == 2) {
           float fsum = 0.f;
 #pragma unroll
           for (int k = 0; k < BPX_MAX_FIBRES; ++k)
-            if (k < K && sf[k] > thr) fsum += sf[k];
+            if (k < K && S.f[k] > thr) fsum += S.f[k];
           if (fsum == 0.f) {
             fibst = 0;
           } else {
-            const float r = fsum * u[4];
+            const float rr = fsum * u[4];
             float cum = 0.f;
             bool found = false;
 #pragma unroll
             for (int k = 0; k < BPX_MAX_FIBRES; ++k) {
               if (k < K && !found) {
-                if (sf[k] > thr) cum += sf[k];
-                if (r <= cum) {
+                if (S.f[k] > thr) cum += S.f[k];
+                if (rr <= cum) {
                   fibst = k;
                   found = true;
                 }
@@ -258,46 +273,35 @@ struct Tracker {
             }
           }
         }
-#pragma unroll
-        for (int k = 0; k < BPX_MAX_FIBRES; ++k)
-          if (k == fibst) {
-            theta = sth[k];
-            phi = sph[k];
-          }
+        sel = fibst;
         init_sample = false;
       } else {
-        const float px = P.rx, py = P.ry, pz = P.rz;  // no preferred-direction volume
+        // no preferred-direction volume: the preference is the current direction;
+        // |sin th cos ph px + sin th sin ph py + cos th pz| in the reference's order
+        const float px = P.rx, py = P.ry, pz = P.rz;
         float dotmax = 0.f;
 #pragma unroll
         for (int k = 0; k < BPX_MAX_FIBRES; ++k) {
-          if (k < K && sf[k] > thr) {
-            float st, ct, sp, cp;
-            sincos_fast(sth[k], st, ct);
-            sincos_fast(sph[k], sp, cp);
-            const float dot = fabsf(st * cp * px + st * sp * py + ct * pz);
+          if (k < K && S.f[k] > thr) {
+            const float dot = fabsf(S.vx[k] * px + S.vy[k] * py + S.vz[k] * pz);
             if (dot > dotmax) {
               dotmax = dot;
-              theta = sth[k];
-              phi = sph[k];
+              sel = k;
               fibind = k;
             }
           }
         }
-        if (dotmax == 0.f) {
-          theta = sth[0];
-          phi = sph[0];
-        }
+        if (dotmax == 0.f) sel = 0;
       }
-    } else {
-      theta = sth[0];
-      phi = sph[0];
     }
-    th = theta;
-    ph = phi;
-    float ff = sf[0];
+    r = make_float3(S.vx[0], S.vy[0], S.vz[0]);
+    float ff = S.f[0];
 #pragma unroll
-    for (int k = 1; k < BPX_MAX_FIBRES; ++k)
-      if (k == fibind) ff = sf[k];
+    for (int k = 1; k < BPX_MAX_FIBRES; ++k) {
+      if (k == sel) r = make_float3(S.vx[k], S.vy[k], S.vz[k]);
+      if (k == fibind) ff = S.f[k];
+    }
+    moves = (S.moves >> sel) & 1u;
     f = a.o.usef ? ff : 1.0f;
   }
 
@@ -329,7 +333,7 @@ struct Tracker {
       // sample in one round of loads (the reference reads them only inside the mask: same values)
       // this step's uniforms: the first block always (rounding, sample); the second (randfib's
       // draw, the --usef test, the first jump's sign) only while one of its draws can be used
-      float u[8], th, ph, f;
+      float u[8], f;
       uniform_block(o.seed, pid, h, (uint32_t)it, 0, u);
       if (o.usef || !P.jumped || (init_sample && K > 1 && (o.randfib == 1 || o.randfib == 2))) {
         uniform_block(o.seed, pid, h, (uint32_t)it, 1, u);
@@ -345,8 +349,8 @@ struct Tracker {
       const uint32_t way = v.waypoints ? __ldg(v.waypoints + vox) : 0u;
       const bool avoid = v.avoid && __ldg(v.avoid + vox) != 0.f;
       const bool stop = v.stop && __ldg(v.stop + vox) != 0.f;
-      float sth[BPX_MAX_FIBRES], sph[BPX_MAX_FIBRES], sf[BPX_MAX_FIBRES];
-      load_record(svox, samp, sth, sph, sf);
+      Sample S;
+      load_record(svox, samp, S);
       if (!(in_grid && m > 0.f)) break;  // the reference's remaining steps change nothing
       if (EXT && o.loopcheck) {
         // stop where the path runs against the direction it last had in this coarse cell
@@ -366,14 +370,14 @@ struct Tracker {
         break;
       }
       if (stop) break;
-      choose(P, u, sth, sph, sf, init_sample, fibst, th, ph, f);
+      float3 rn;
+      bool moves;
+      choose(P, u, S, init_sample, fibst, rn, moves, f);
       if (f > u[5]) {
-        float st, ct, sp, cp;
-        sincos_fast(th, st, ct);
-        sincos_fast(ph, sp, cp);
-        const float rxn = cp * st, ryn = sp * st, rzn = ct;
+        // (cos ph sin th, sin ph sin th, cos th): the record's vector, products commuted
+        const float rxn = rn.x, ryn = rn.y, rzn = rn.z;
         if (P.jumped && !(fabsf(rxn * P.rx + ryn * P.ry + rzn * P.rz) > o.c_thr)) break;
-        if (th != 0.f && ph != 0.f) {
+        if (moves) {
           if (!EXT || !o.modeuler) {
             jump_dir(P, a, rxn, ryn, rzn, u[6]);
           } else {
@@ -387,20 +391,19 @@ struct Tracker {
             else
               tsign = w[4] > 0.5f ? 1 : -1;
             const float ts = (float)tsign;
-            const float tx = P.x + ts * o.steplength / v.dx * rxn;
-            const float ty = P.y + ts * o.steplength / v.dy * ryn;
-            const float tz = P.z + ts * o.steplength / v.dz * rzn;
+            const float tx = P.x + ts * a.sx * rxn;
+            const float ty = P.y + ts * a.sy * ryn;
+            const float tz = P.z + ts * a.sz * rzn;
             size_t tvox;
             int tsamp;
             locate(tx, ty, tz, w, tvox, tsamp);
-            float tth[BPX_MAX_FIBRES], tph[BPX_MAX_FIBRES], tf[BPX_MAX_FIBRES];
-            load_record(tvox, tsamp, tth, tph, tf);
-            float th2, ph2, f2;
-            choose(P, w, tth, tph, tf, init_sample, fibst, th2, ph2, f2);
-            float st2, ct2, sp2, cp2;
-            sincos_fast(th2, st2, ct2);
-            sincos_fast(ph2, sp2, cp2);
-            const float bx = cp2 * st2, by = sp2 * st2, bz = ct2;
+            Sample T2;
+            load_record(tvox, tsamp, T2);
+            float3 b;
+            bool moves2;
+            float f2;
+            choose(P, w, T2, init_sample, fibst, b, moves2, f2);
+            const float bx = b.x, by = b.y, bz = b.z;
             const float same = (rxn * bx + ryn * by + rzn * bz) > 0.f ? 1.0f : -1.0f;
             const float mx = (rxn + same * bx) * 0.5f, my = (ryn + same * by) * 0.5f, mz = (rzn + same * bz) * 0.5f;
             const float n = sqrtf(mx * mx + my * my + mz * mz);
@@ -483,9 +486,10 @@ __global__ void __launch_bounds__(kTrackThreads, kTrackBlocksPerSm) track_kernel
   if ((threadIdx.x & 31) == 0 && kept) atomicAdd(a.waytotal, kept);
 }
 
-// The samples [K][nsamples][nvox] of th, ph and f repacked as one record per (voxel, sample):
-// a 32 x 32 tile of (voxel, sample) per block, read along voxels and written along samples through
-// shared memory, so both sides are coalesced.
+// The samples [K][nsamples][nvox] of th, ph and f repacked as one record per (voxel, sample)
+// (TrackArgs::packed): a 32 x 32 tile of (voxel, sample) per block, read along voxels and written
+// along samples through shared memory, so both sides are coalesced.  Each fibre's direction is
+// formed here once, with the sine and cosine every step would otherwise form again.
 constexpr int kPackTile = 32;
 __global__ void __launch_bounds__(256) pack_samples_kernel(const float* __restrict__ th, const float* __restrict__ ph,
                                                            const float* __restrict__ f, int K, int ns, size_t nvox,
@@ -509,12 +513,16 @@ __global__ void __launch_bounds__(256) pack_samples_kernel(const float* __restri
     const int smp = s0 + tx;
     if (vx >= nvox || smp >= ns) continue;
     float4* dst = out + (vx * ns + smp) * pk4;
-    for (int q = 0; q < pk4; ++q) {
-      float w[4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) w[e] = (4 * q + e < 3 * K) ? tile[4 * q + e][tx][i] : 0.f;
-      dst[q] = make_float4(w[0], w[1], w[2], w[3]);
+    uint32_t moves = 0;
+    for (int k = 0; k < K; ++k) {
+      const float t = tile[3 * k][tx][i], p = tile[3 * k + 1][tx][i];
+      float st, ct, sp, cp;
+      sincos_fast(t, st, ct);
+      sincos_fast(p, sp, cp);
+      dst[k] = make_float4(st * cp, st * sp, ct, tile[3 * k + 2][tx][i]);
+      if (t != 0.f && p != 0.f) moves |= 1u << k;
     }
+    dst[K] = make_float4(__uint_as_float(moves), 0.f, 0.f, 0.f);
   }
 }
 
@@ -575,6 +583,9 @@ bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volu
   a.o = *opts;
   a.v = *vol;
   a.nvox = (size_t)vol->nx * vol->ny * vol->nz;
+  a.sx = opts->steplength / vol->dx;
+  a.sy = opts->steplength / vol->dy;
+  a.sz = opts->steplength / vol->dz;
   a.nseeds = nseeds;
   a.seeds = seeds;
   a.paths = reinterpret_cast<int*>(paths);
@@ -600,7 +611,7 @@ bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volu
   if ((size_t)grid > max_blocks) grid = max_blocks > 0 ? (int)max_blocks : 1;
   const size_t threads = (size_t)grid * kTrackThreads;
   // workspace: the visit tables, the loopcheck tables (keys, then directions), the repacked samples
-  const int pk4 = (3 * vol->nfib + 3) / 4;
+  const int pk4 = vol->nfib + 1;
   const size_t tab_total = (threads * table_bytes + 255) & ~(size_t)255;
   const size_t lc_keys = opts->loopcheck ? (threads * ((size_t)1 << lc_log2n) * sizeof(uint2) + 255) & ~(size_t)255 : 0;
   const size_t lc_dirs = opts->loopcheck ? threads * ((size_t)1 << lc_log2n) * sizeof(float4) : 0;
