@@ -537,8 +537,8 @@ bpx_status check_track(const bpx_track_options* o, const bpx_track_volume* v, in
     return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: bad grid, fibre or sample count");
   if ((size_t)v->nx * v->ny * v->nz >= (1ull << 32))
     return api_fail(BPX_ERR_UNSUPPORTED, "bpx_probtrack_dev: more than 2^32 voxels");
-  if ((size_t)v->nx * v->ny * v->nz * (size_t)v->nsamples >= (1ull << 36) || v->nsamples >= (1 << 26))
-    return api_fail(BPX_ERR_UNSUPPORTED, "bpx_probtrack_dev: more than 2^36 samples");
+  if ((size_t)v->nx * v->ny * v->nz * (size_t)v->nsamples >= (1ull << 36) || v->nsamples > (1 << 20))
+    return api_fail(BPX_ERR_UNSUPPORTED, "bpx_probtrack_dev: more than 2^36 samples, or 2^20 per voxel");
   if (!(v->dx > 0.f && v->dy > 0.f && v->dz > 0.f))
     return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: voxel sizes must be positive");
   if (o->fibst > v->nfib) return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: fibst beyond the fibres given");

@@ -45,8 +45,12 @@ int main(void) {
   printf("bpx_options size %zu\n", sizeof(bpx_options));
   printf("bpx_volume size %zu\n", sizeof(bpx_volume));
   printf("bpx_outputs size %zu\n", sizeof(bpx_outputs));
+  printf("bpx_track_options size %zu\n", sizeof(bpx_track_options));
+  printf("bpx_track_volume size %zu\n", sizeof(bpx_track_volume));
   F(bpx_options, seed) F(bpx_options, gradnonlin) F(bpx_options, mcmc_tpv) F(bpx_options, R_prior_fudge)
   F(bpx_volume, data) F(bpx_volume, voxel_offset) F(bpx_outputs, dyads) F(bpx_outputs, status)
+  F(bpx_track_options, seed) F(bpx_track_options, pathdist) F(bpx_track_options, modeuler)
+  F(bpx_track_volume, mask) F(bpx_track_volume, waypoints) F(bpx_track_volume, nwaypoints)
   return 0;
 }
 """
@@ -64,10 +68,13 @@ int main(void) {
     assert got[("bpx_options", "size")] == C.sizeof(Options)
     assert got[("bpx_volume", "size")] == C.sizeof(Volume)
     assert got[("bpx_outputs", "size")] == C.sizeof(Outputs)
+    assert got[("bpx_track_options", "size")] == C.sizeof(abi.TrackOptions)
+    assert got[("bpx_track_volume", "size")] == C.sizeof(abi.TrackVolume)
     for (t, m), v in got.items():
         if m == "size":
             continue
-        cls = {"bpx_options": Options, "bpx_volume": Volume, "bpx_outputs": Outputs}[t]
+        cls = {"bpx_options": Options, "bpx_volume": Volume, "bpx_outputs": Outputs,
+               "bpx_track_options": abi.TrackOptions, "bpx_track_volume": abi.TrackVolume}[t]
         assert getattr(cls, m).offset == v, (t, m)
 
 
@@ -117,6 +124,23 @@ def test_host_argument_checks_reject_bad_input(libbpx):
     assert st(C.byref(ok_s), C.byref(vol), None, None, None, None, None, 5, 30, 0, None, None, None, None, None,
               None) == abi.BPX_ERR_INVALID_ARG
     assert b"state_in" in libbpx.bpx_last_error()
+    # tracking: options, grid and buffers are checked first
+    t = abi.TrackOptions.make()
+    tv = abi.TrackVolume()
+    tv.nx, tv.ny, tv.nz, tv.dx, tv.dy, tv.dz, tv.nfib, tv.nsamples = 8, 8, 8, 2.0, 2.0, 2.0, 3, 50
+    pt = libbpx.bpx_probtrack_dev
+    assert pt(C.byref(t), C.byref(tv), 1, None, None, None, None) == abi.BPX_ERR_INVALID_ARG  # NULL buffers
+    assert b"NULL" in libbpx.bpx_last_error()
+    tv.nwaypoints = 33
+    assert pt(C.byref(t), C.byref(tv), 1, None, None, None, None) == abi.BPX_ERR_INVALID_ARG
+    assert b"nwaypoints" in libbpx.bpx_last_error()
+    tv.nwaypoints, tv.nsamples = 0, (1 << 20) + 1
+    assert pt(C.byref(t), C.byref(tv), 1, None, None, None, None) == abi.BPX_ERR_UNSUPPORTED
+    tv.nsamples, tv.nfib = 50, 4
+    assert pt(C.byref(t), C.byref(tv), 1, None, None, None, None) == abi.BPX_ERR_INVALID_ARG
+    tv.nfib = 3
+    assert pt(C.byref(abi.TrackOptions.make(nsteps=1)), C.byref(tv), 1, None, None, None, None) == abi.BPX_ERR_INVALID_ARG
+    assert pt(C.byref(t), C.byref(tv), 0, None, None, None, None) == abi.BPX_OK  # no seeds: nothing to do
     # empty volumes are valid and do nothing
     vol.nvox = 0
     assert libbpx.bpx_fit_dev(C.byref(ok), C.byref(vol), None, None, None, None) == abi.BPX_OK
