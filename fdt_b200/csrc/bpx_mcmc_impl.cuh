@@ -205,7 +205,7 @@ __device__ __forceinline__ void rician_pick(float z, float q, float pr, float& s
   sel = small ? q : pr;
   zs = small ? z : 0.f;
 }
-template <typename V>
+template <typename V, bool W = true>
 __device__ __forceinline__ void rician_acc(V y, V w, V base, V nS0, V tS0, V& rr, V& prod, V& zs) {
   const V r = vfma(nS0, base, y);
   const V z = vmul(tS0, vmul(y, base));
@@ -233,7 +233,7 @@ __device__ __forceinline__ void rician_acc(V y, V w, V base, V nS0, V tS0, V& rr
   }
   prod = vmul(prod, sel);
   zs = vadd(zs, zz);
-  rr = vfma(vmul(r, w), r, rr);
+  rr = W ? vfma(vmul(r, w), r, rr) : vfma(r, r, rr);  // w is 1 wherever W is false
 }
 
 // signals of one or two measurements (compute_signal / compute_iso_signal, CUDA/runmcmc_kernels.cu:67-95).
@@ -262,13 +262,13 @@ __device__ __forceinline__ void with_signal_form(const SigParams<MODEL>& sp, F&&
 }
 
 // Gaussian likelihood contribution of one or two measurements, w (y - S0 base)^2
-template <int K, typename V>
+template <int K, typename V, bool W = true>
 __device__ __forceinline__ V gauss_v(V y, V w, V isov, const V (&sk)[K], V nS0, const V (&fk)[K], V f0, V wiso) {
   V base = vfma(wiso, isov, f0);
 #pragma unroll
   for (int k = 0; k < K; ++k) base = vfma(fk[k], sk[k], base);
   const V r = vfma(nS0, base, y);
-  return vmul(vmul(r, w), r);
+  return W ? vmul(vmul(r, w), r) : vmul(r, r);  // w is 1 wherever W is false
 }
 
 // Rows of the per-group fibre state in shared memory (K entries each).
@@ -293,7 +293,10 @@ constexpr uint32_t slot_bits(int what) {
 
 // STRETCH: compiled with the checkpoint/resume arguments of McmcArgs (it_begin/it_end, state and
 // acceptance counts in and out); without it the kernel runs the whole chain from the LM state.
-template <int MODEL, int K, bool RIC, int TPV, int MPL, bool STRETCH>
+// PAIRW: the measurement pairs may hold padding (M < 2 * (MPL / 2) * TPV), so their residuals carry
+// the padding weights; without it only the unpaired measurement can be padding and the pairs skip
+// the multiply by w = 1 (the same sums, bit for bit).
+template <int MODEL, int K, bool RIC, int TPV, int MPL, bool STRETCH, bool PAIRW = true>
 __global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_kernel(McmcArgs a) {
   constexpr int NS = 6 + 3 * K;             // proposal slots
   constexpr int NR = (NS + TPV - 1) / TPV;  // Philox blocks per lane per iteration
@@ -534,7 +537,7 @@ __global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_ker
           float2 base = vfma(wiso2, i2[p], f02);
 #pragma unroll
           for (int k = 0; k < K; ++k) base = vfma(fk2[k], s2[k][p], base);
-          rician_acc<float2>(make_float2(yw.x, yw.y), make_float2(yw.z, yw.w), base, nS02, tS02, rr, prod, zs);
+          rician_acc<float2, PAIRW>(make_float2(yw.x, yw.y), make_float2(yw.z, yw.w), base, nS02, tS02, rr, prod, zs);
           if (p % 4 == 3 && p + 1 < NP) {
             lgp += lg2_approx(prod.x) + lg2_approx(prod.y);
             prod = make_float2(1.f, 1.f);
@@ -556,8 +559,8 @@ __global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_ker
 #pragma unroll
           for (int k = 0; k < K; ++k) sk[k] = s2[k][p];
           const float4 yw = ywp[p * kMcmcThreads + tid];
-          acc2 = vadd(acc2, gauss_v<K, float2>(make_float2(yw.x, yw.y), make_float2(yw.z, yw.w), i2[p], sk, nS02, fk2,
-                                               f02, wiso2));
+          acc2 = vadd(acc2, gauss_v<K, float2, PAIRW>(make_float2(yw.x, yw.y), make_float2(yw.z, yw.w), i2[p], sk, nS02,
+                                                      fk2, f02, wiso2));
         }
         acc = vhsum(acc2);
         if (TAIL) {
@@ -999,9 +1002,12 @@ __global__ void __launch_bounds__(kMcmcThreads) energy_kernel(EnergyArgs a) {
 template <int MODEL, int K, bool RIC, int TPV, int MPL>
 cudaError_t launch_mcmc_t(const McmcArgs& a, cudaStream_t s) {
   const bool stretch = a.it_begin != 0 || a.it_end != 0 || a.state_in || a.state_out || a.acc_in || a.acc_out;
-  auto kern = stretch ? mcmc_kernel<MODEL, K, RIC, TPV, MPL, true> : mcmc_kernel<MODEL, K, RIC, TPV, MPL, false>;
   constexpr int NS = 6 + 3 * K, GPB = kMcmcThreads / TPV;
   constexpr int NP = MPL / 2;
+  auto kern = stretch ? mcmc_kernel<MODEL, K, RIC, TPV, MPL, true> : mcmc_kernel<MODEL, K, RIC, TPV, MPL, false>;
+  // the whole-brain layout without padding in its pairs (M > 256), the plain chain: pairs skip w
+  if constexpr (TPV == 32 && MPL == 9)
+    if (!stretch && a.ndir >= 2 * NP * TPV) kern = mcmc_kernel<MODEL, K, RIC, TPV, MPL, false, false>;
   const size_t smem = (size_t)(a.gradnonlin ? GPB : 1) * TPV * MPL * sizeof(float4) +
                       (size_t)NP * kMcmcThreads * sizeof(float4) + (size_t)kMcmcThreads * sizeof(float2) +
                       (size_t)(2 * NP + 1) * (K + 1) * kMcmcThreads * sizeof(float) + (size_t)GPB * NS * 8 +
