@@ -293,10 +293,10 @@ constexpr uint32_t slot_bits(int what) {
 
 // STRETCH: compiled with the checkpoint/resume arguments of McmcArgs (it_begin/it_end, state and
 // acceptance counts in and out); without it the kernel runs the whole chain from the LM state.
-// PAIRW: the measurement pairs may hold padding (M < 2 * (MPL / 2) * TPV), so their residuals carry
-// the padding weights; without it only the unpaired measurement can be padding and the pairs skip
-// the multiply by w = 1 (the same sums, bit for bit).
-template <int MODEL, int K, bool RIC, int TPV, int MPL, bool STRETCH, bool PAIRW = true>
+// WPAD: which residuals carry the padding weights w.  2: all (the general case); 1: only the
+// unpaired measurement's (M >= 2 * (MPL / 2) * TPV: the pairs hold no padding); 0: none
+// (M = TPV * MPL).  Where w is 1 the multiply is skipped: the same sums, bit for bit.
+template <int MODEL, int K, bool RIC, int TPV, int MPL, bool STRETCH, int WPAD = 2>
 __global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_kernel(McmcArgs a) {
   constexpr int NS = 6 + 3 * K;             // proposal slots
   constexpr int NR = (NS + TPV - 1) / TPV;  // Philox blocks per lane per iteration
@@ -537,7 +537,8 @@ __global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_ker
           float2 base = vfma(wiso2, i2[p], f02);
 #pragma unroll
           for (int k = 0; k < K; ++k) base = vfma(fk2[k], s2[k][p], base);
-          rician_acc<float2, PAIRW>(make_float2(yw.x, yw.y), make_float2(yw.z, yw.w), base, nS02, tS02, rr, prod, zs);
+          rician_acc<float2, (WPAD >= 2)>(make_float2(yw.x, yw.y), make_float2(yw.z, yw.w), base, nS02, tS02, rr, prod,
+                                          zs);
           if (p % 4 == 3 && p + 1 < NP) {
             lgp += lg2_approx(prod.x) + lg2_approx(prod.y);
             prod = make_float2(1.f, 1.f);
@@ -548,7 +549,7 @@ __global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_ker
           float base = fmaf(wiso, it_, f0x);
 #pragma unroll
           for (int k = 0; k < K; ++k) base = fmaf(fx[k], st[k], base);
-          rician_acc<float>(ytw.x, ytw.y, base, -S0x, taux * S0x, rr.x, prod.x, zs.x);
+          rician_acc<float, (WPAD >= 1)>(ytw.x, ytw.y, base, -S0x, taux * S0x, rr.x, prod.x, zs.x);
         }
         acc = -0.5f * taux * (rr.x + rr.y) + kLn2 * (lgp + lg2_approx(prod.x) + lg2_approx(prod.y)) - (zs.x + zs.y);
       } else {
@@ -559,13 +560,13 @@ __global__ void __launch_bounds__(kMcmcThreads, mcmc_min_blocks<MPL>()) mcmc_ker
 #pragma unroll
           for (int k = 0; k < K; ++k) sk[k] = s2[k][p];
           const float4 yw = ywp[p * kMcmcThreads + tid];
-          acc2 = vadd(acc2, gauss_v<K, float2, PAIRW>(make_float2(yw.x, yw.y), make_float2(yw.z, yw.w), i2[p], sk, nS02,
-                                                      fk2, f02, wiso2));
+          acc2 = vadd(acc2, gauss_v<K, float2, (WPAD >= 2)>(make_float2(yw.x, yw.y), make_float2(yw.z, yw.w), i2[p], sk,
+                                                            nS02, fk2, f02, wiso2));
         }
         acc = vhsum(acc2);
         if (TAIL) {
           const float2 ytw = ywt[tid];
-          acc += gauss_v<K, float>(ytw.x, ytw.y, it_, st, -S0x, fx, f0x, wiso);
+          acc += gauss_v<K, float, (WPAD >= 1)>(ytw.x, ytw.y, it_, st, -S0x, fx, f0x, wiso);
         }
       }
       return group_sum<TPV>(acc);
@@ -1005,9 +1006,14 @@ cudaError_t launch_mcmc_t(const McmcArgs& a, cudaStream_t s) {
   constexpr int NS = 6 + 3 * K, GPB = kMcmcThreads / TPV;
   constexpr int NP = MPL / 2;
   auto kern = stretch ? mcmc_kernel<MODEL, K, RIC, TPV, MPL, true> : mcmc_kernel<MODEL, K, RIC, TPV, MPL, false>;
-  // the whole-brain layout without padding in its pairs (M > 256), the plain chain: pairs skip w
-  if constexpr (TPV == 32 && MPL == 9)
-    if (!stretch && a.ndir >= 2 * NP * TPV) kern = mcmc_kernel<MODEL, K, RIC, TPV, MPL, false, false>;
+  // the whole-brain layout with no padding in its pairs (M >= 256) or none at all (M = 288), the
+  // whole chain: those residuals skip w
+  if constexpr (TPV == 32 && MPL == 9) {
+    if (!stretch && a.ndir == TPV * MPL)
+      kern = mcmc_kernel<MODEL, K, RIC, TPV, MPL, false, 0>;
+    else if (!stretch && a.ndir >= 2 * NP * TPV)
+      kern = mcmc_kernel<MODEL, K, RIC, TPV, MPL, false, 1>;
+  }
   const size_t smem = (size_t)(a.gradnonlin ? GPB : 1) * TPV * MPL * sizeof(float4) +
                       (size_t)NP * kMcmcThreads * sizeof(float4) + (size_t)kMcmcThreads * sizeof(float2) +
                       (size_t)(2 * NP + 1) * (K + 1) * kMcmcThreads * sizeof(float) + (size_t)GPB * NS * 8 +
