@@ -326,6 +326,9 @@ static int half_line(const trk_t* T, part_t* P, uint64_t pid, int h, int fibst0,
   return rej;
 }
 
+/* Particles are independent: OpenMP threads take them in chunks, each with its own path, visit
+ * stamps and loopcheck volume; the int32 counts and waytotal are integer sums, so the result does
+ * not depend on the number of threads or the order. */
 int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nseeds, const float* seeds,
                   int32_t* paths, int64_t* waytotal) {
   trk_t T;
@@ -333,28 +336,26 @@ int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nse
   T.v = v;
   T.nvox = (size_t)v->nx * v->ny * v->nz;
   const int half_steps = o->nsteps / 2;
-  int64_t* path = (int64_t*)malloc(sizeof(int64_t) * (size_t)(2 * half_steps + 2));
-  int64_t* stamp = (int64_t*)malloc(sizeof(int64_t) * T.nvox);
-  if (!path || !stamp) {
-    free(path);
-    free(stamp);
-    return 1;
-  }
-  for (size_t i = 0; i < T.nvox; ++i) stamp[i] = -1;
-  /* the coarse grid covers round(x / 5) for x in [-0.5, n - 0.5) */
-  loopvol_t lc = {v->nx / 5 + 2, v->ny / 5 + 2, v->nz / 5 + 2, NULL};
-  if (o->loopcheck) {
-    lc.dir = (float*)calloc(3 * (size_t)lc.nx * lc.ny * lc.nz, sizeof(float));
-    if (!lc.dir) {
-      free(path);
-      free(stamp);
-      return 1;
-    }
-  }
+  const int64_t total = (int64_t)nseeds * (int64_t)o->nparticles;
+  uint32_t* counts = (uint32_t*)paths;
   int64_t kept = 0;
-  for (int s = 0; s < nseeds; ++s) {
-    for (int p = 0; p < o->nparticles; ++p) {
-      const uint64_t pid = (uint64_t)s * (uint64_t)o->nparticles + (uint64_t)p;
+  int failed = 0;
+#pragma omp parallel reduction(+ : kept) reduction(| : failed)
+  {
+    int64_t* path = (int64_t*)malloc(sizeof(int64_t) * (size_t)(2 * half_steps + 2));
+    int64_t* stamp = (int64_t*)malloc(sizeof(int64_t) * T.nvox);
+    /* the coarse grid covers round(x / 5) for x in [-0.5, n - 0.5) */
+    loopvol_t lc = {v->nx / 5 + 2, v->ny / 5 + 2, v->nz / 5 + 2, NULL};
+    if (o->loopcheck) lc.dir = (float*)calloc(3 * (size_t)lc.nx * lc.ny * lc.nz, sizeof(float));
+    const int ok = path && stamp && (!o->loopcheck || lc.dir);
+    if (!ok) failed = 1;
+    if (ok)
+      for (size_t i = 0; i < T.nvox; ++i) stamp[i] = -1;
+#pragma omp for schedule(dynamic, 16)
+    for (int64_t q = 0; q < total; ++q) {
+      if (!ok) continue;
+      const int s = (int)(q / o->nparticles);
+      const uint64_t pid = (uint64_t)q;
       float u[8];
       orc_track_uniforms(o->seed, pid, 0, 0u, u); /* the particle's own draws: step 0 */
       int fibst = o->fibst - 1;
@@ -392,14 +393,17 @@ int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nse
         if (stamp[vx] != (int64_t)pid) {
           stamp[vx] = (int64_t)pid;
           ++d;
-          paths[vx] = (int32_t)((uint32_t)paths[vx] + (o->pathdist ? d : 1u));
+          const uint32_t add = o->pathdist ? d : 1u;
+#pragma omp atomic
+          counts[vx] += add;
         }
       }
     }
+    free(path);
+    free(stamp);
+    free(lc.dir);
   }
+  if (failed) return 1;
   *waytotal += kept;
-  free(path);
-  free(stamp);
-  free(lc.dir);
   return 0;
 }
