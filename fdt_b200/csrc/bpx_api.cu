@@ -4,6 +4,7 @@
 // host-buffer drop-in for xfibres_gpu() (CUDA/xfibres_gpu.cu:29-146).  No entry point calls
 // exit(); failures return a bpx_status and leave a message for bpx_last_error().
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -636,8 +637,20 @@ bpx_status bpx_xfibres_dev(const bpx_options* opts, const bpx_volume* vol, bpx_o
 
 namespace {
 
-// Host-buffer pipeline: copies in, runs the plain (mlp == NULL) or the learned pipeline on a
-// private stream, copies the outputs back and synchronises.
+// Host-buffer pipeline: the plain (mlp == NULL) or the learned pipeline over the volume in
+// sub-volumes of kHostChunk voxels, each through one of two device buffer sets, so that the copies
+// of one sub-volume (host to device on one copy stream, device to host on another) overlap the
+// computation of the next on the compute stream.  Every voxel's result is independent of the
+// others and its chain is keyed by its global index (voxel_offset + position), so the outputs are
+// those of one call over the whole volume, bit for bit.  Synchronous.  The sub-volume size is
+// 65536 voxels (about 14 waves of the whole-brain chain on a B200), or BPX_HOST_CHUNK from the
+// environment.
+size_t host_chunk() {
+  const char* e = std::getenv("BPX_HOST_CHUNK");
+  const long long v = e ? std::atoll(e) : 0;
+  return v > 0 ? (size_t)v : (size_t)65536;
+}
+
 bpx_status xfibres_host_impl(const bpx_options* opts, const bpx_volume* vol, bpx_outputs* host_out, const float* mlp,
                              int32_t freeze_props) {
   bpx_status st = check_opts(opts);
@@ -651,25 +664,49 @@ bpx_status xfibres_host_impl(const bpx_options* opts, const bpx_volume* vol, bpx
   st = check_device();
   if (st != BPX_OK) return st;
   const size_t nvox = vol->nvox, ndir = vol->ndir, K = opts->nfibres;
+  const size_t chunk = host_chunk();
+  const size_t C = nvox < chunk ? nvox : chunk;  // voxels per sub-volume
   const bool gn = opts->gradnonlin != 0;
-  // device buffers: inputs, per-voxel b-matrix under gradnonlin, outputs
-  const size_t b_data = align256(nvox * ndir * 4);
+  // device buffers: the shared b-table and weights, then two sets of per-sub-volume buffers
   const size_t b_bvec = align256(3 * ndir * 4), b_bval = align256(ndir * 4);
-  const size_t b_grad = gn ? align256(nvox * 9 * 4) : 0;
-  const size_t b_bvec_v = gn ? align256(nvox * 3 * ndir * 4) : 0, b_bval_v = gn ? align256(nvox * ndir * 4) : 0;
-  const size_t b_samp = align256(K * ns * nvox * 4);
-  const size_t b_vox = align256(nvox * 4);
-  const size_t b_vk = align256(K * nvox * 4), b_dy = align256(K * 3 * nvox * 4);
   const size_t b_mlp = mlp ? align256((size_t)bpx_mlp_nparams(vol->ndir) * 4) : 0;
-  const size_t total =
-      b_data + b_bvec + b_bval + b_grad + b_bvec_v + b_bval_v + 3 * b_samp + 7 * b_vox + b_vk + b_dy + b_mlp;
+  const size_t b_data = align256(C * ndir * 4);
+  const size_t b_grad = gn ? align256(C * 9 * 4) : 0;
+  const size_t b_bvec_v = gn ? align256(C * 3 * ndir * 4) : 0, b_bval_v = gn ? align256(C * ndir * 4) : 0;
+  const size_t b_samp = align256(K * ns * C * 4);
+  const size_t b_vox = align256(C * 4);
+  const size_t b_vk = align256(K * C * 4), b_dy = align256(K * 3 * C * 4);
+  const size_t per_set = b_data + b_grad + b_bvec_v + b_bval_v + 3 * b_samp + 7 * b_vox + b_vk + b_dy;
+  const size_t total = b_bvec + b_bval + b_mlp + 2 * per_set;
   char* base = nullptr;
   BPX_CUDA(cudaMalloc(&base, total));
-  cudaStream_t s = nullptr;
-  cudaError_t ce = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-  if (ce != cudaSuccess) {
+  cudaStream_t sc = nullptr, sin = nullptr, sout = nullptr;
+  cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
+  cudaError_t ce = cudaStreamCreateWithFlags(&sc, cudaStreamNonBlocking);
+  if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&sin, cudaStreamNonBlocking);
+  if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&sout, cudaStreamNonBlocking);
+  for (int b = 0; b < 2 && ce == cudaSuccess; ++b) {
+    ce = cudaEventCreateWithFlags(&ev_in[b], cudaEventDisableTiming);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&ev_done[b], cudaEventDisableTiming);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&ev_free[b], cudaEventDisableTiming);
+  }
+  auto release = [&]() {
+    if (sc) cudaStreamSynchronize(sc);
+    if (sin) cudaStreamSynchronize(sin);
+    if (sout) cudaStreamSynchronize(sout);
+    for (int b = 0; b < 2; ++b) {
+      if (ev_in[b]) cudaEventDestroy(ev_in[b]);
+      if (ev_done[b]) cudaEventDestroy(ev_done[b]);
+      if (ev_free[b]) cudaEventDestroy(ev_free[b]);
+    }
+    if (sc) cudaStreamDestroy(sc);
+    if (sin) cudaStreamDestroy(sin);
+    if (sout) cudaStreamDestroy(sout);
     cudaFree(base);
-    return cuda_fail(ce, "cudaStreamCreate");
+  };
+  if (ce != cudaSuccess) {
+    release();
+    return cuda_fail(ce, "xfibres_host: streams and events");
   }
   char* p = base;
   auto take = [&](size_t b) {
@@ -677,68 +714,92 @@ bpx_status xfibres_host_impl(const bpx_options* opts, const bpx_volume* vol, bpx
     p += b;
     return r;
   };
-  float* d_data = (float*)take(b_data);
   float* d_bvec = (float*)take(b_bvec);
   float* d_bval = (float*)take(b_bval);
-  float* d_grad = gn ? (float*)take(b_grad) : nullptr;
-  float* d_bvec_v = gn ? (float*)take(b_bvec_v) : nullptr;
-  float* d_bval_v = gn ? (float*)take(b_bval_v) : nullptr;
-  bpx_outputs d_out;
-  std::memset(&d_out, 0, sizeof(d_out));
-  d_out.th = (float*)take(b_samp);
-  d_out.ph = (float*)take(b_samp);
-  d_out.f = (float*)take(b_samp);
-  d_out.mean_d = (float*)take(b_vox);
-  d_out.mean_dstd = (float*)take(b_vox);
-  d_out.mean_R = (float*)take(b_vox);
-  d_out.mean_f0 = (float*)take(b_vox);
-  d_out.mean_tau = (float*)take(b_vox);
-  d_out.mean_S0 = (float*)take(b_vox);
-  d_out.status = (uint32_t*)take(b_vox);
-  d_out.mean_f = (float*)take(b_vk);
-  d_out.dyads = (float*)take(b_dy);
   float* d_mlp = mlp ? (float*)take(b_mlp) : nullptr;
+  struct Set {
+    float *data, *grad, *bvec_v, *bval_v;
+    bpx_outputs out;
+  } set[2];
+  for (int b = 0; b < 2; ++b) {
+    Set& q = set[b];
+    q.data = (float*)take(b_data);
+    q.grad = gn ? (float*)take(b_grad) : nullptr;
+    q.bvec_v = gn ? (float*)take(b_bvec_v) : nullptr;
+    q.bval_v = gn ? (float*)take(b_bval_v) : nullptr;
+    std::memset(&q.out, 0, sizeof(q.out));
+    q.out.th = (float*)take(b_samp);
+    q.out.ph = (float*)take(b_samp);
+    q.out.f = (float*)take(b_samp);
+    q.out.mean_d = (float*)take(b_vox);
+    q.out.mean_dstd = (float*)take(b_vox);
+    q.out.mean_R = (float*)take(b_vox);
+    q.out.mean_f0 = (float*)take(b_vox);
+    q.out.mean_tau = (float*)take(b_vox);
+    q.out.mean_S0 = (float*)take(b_vox);
+    q.out.status = (uint32_t*)take(b_vox);
+    q.out.mean_f = (float*)take(b_vk);
+    q.out.dyads = (float*)take(b_dy);
+  }
   auto run = [&]() -> bpx_status {
-    if (mlp) BPX_CUDA(cudaMemcpyAsync(d_mlp, mlp, (size_t)bpx_mlp_nparams(vol->ndir) * 4, cudaMemcpyHostToDevice, s));
-    BPX_CUDA(cudaMemcpyAsync(d_data, vol->data, nvox * ndir * 4, cudaMemcpyHostToDevice, s));
-    BPX_CUDA(cudaMemcpyAsync(d_bvec, vol->bvecs, 3 * ndir * 4, cudaMemcpyHostToDevice, s));
-    BPX_CUDA(cudaMemcpyAsync(d_bval, vol->bvals, ndir * 4, cudaMemcpyHostToDevice, s));
-    bpx_volume dv = *vol;
-    dv.data = d_data;
-    dv.bvecs = d_bvec;
-    dv.bvals = d_bval;
-    dv.grad = nullptr;
-    if (gn) {
-      BPX_CUDA(cudaMemcpyAsync(d_grad, vol->grad, nvox * 9 * 4, cudaMemcpyHostToDevice, s));
-      bpx_status s2 = bpx_gradnonlin_dev(vol->nvox, vol->ndir, d_grad, d_bvec, d_bval, d_bvec_v, d_bval_v, s);
-      if (s2 != BPX_OK) return s2;
-      dv.bvecs = d_bvec_v;
-      dv.bvals = d_bval_v;
-    }
-    bpx_status s3 = mlp ? bpx_xfibres_learned_dev(opts, &dv, d_mlp, freeze_props, &d_out, s)
-                        : bpx_xfibres_dev(opts, &dv, &d_out, s);
-    if (s3 != BPX_OK) return s3;
+    if (mlp) BPX_CUDA(cudaMemcpyAsync(d_mlp, mlp, (size_t)bpx_mlp_nparams(vol->ndir) * 4, cudaMemcpyHostToDevice, sin));
+    BPX_CUDA(cudaMemcpyAsync(d_bvec, vol->bvecs, 3 * ndir * 4, cudaMemcpyHostToDevice, sin));
+    BPX_CUDA(cudaMemcpyAsync(d_bval, vol->bvals, ndir * 4, cudaMemcpyHostToDevice, sin));
     const bpx_outputs& h = *host_out;
-    const size_t samp = K * ns * nvox * 4, vox = nvox * 4;
-    if (h.th) BPX_CUDA(cudaMemcpyAsync(h.th, d_out.th, samp, cudaMemcpyDeviceToHost, s));
-    if (h.ph) BPX_CUDA(cudaMemcpyAsync(h.ph, d_out.ph, samp, cudaMemcpyDeviceToHost, s));
-    if (h.f) BPX_CUDA(cudaMemcpyAsync(h.f, d_out.f, samp, cudaMemcpyDeviceToHost, s));
-    if (h.mean_d) BPX_CUDA(cudaMemcpyAsync(h.mean_d, d_out.mean_d, vox, cudaMemcpyDeviceToHost, s));
-    if (h.mean_dstd) BPX_CUDA(cudaMemcpyAsync(h.mean_dstd, d_out.mean_dstd, vox, cudaMemcpyDeviceToHost, s));
-    if (h.mean_R) BPX_CUDA(cudaMemcpyAsync(h.mean_R, d_out.mean_R, vox, cudaMemcpyDeviceToHost, s));
-    if (h.mean_f0) BPX_CUDA(cudaMemcpyAsync(h.mean_f0, d_out.mean_f0, vox, cudaMemcpyDeviceToHost, s));
-    if (h.mean_tau) BPX_CUDA(cudaMemcpyAsync(h.mean_tau, d_out.mean_tau, vox, cudaMemcpyDeviceToHost, s));
-    if (h.mean_S0) BPX_CUDA(cudaMemcpyAsync(h.mean_S0, d_out.mean_S0, vox, cudaMemcpyDeviceToHost, s));
-    if (h.status) BPX_CUDA(cudaMemcpyAsync(h.status, d_out.status, vox, cudaMemcpyDeviceToHost, s));
-    if (h.mean_f) BPX_CUDA(cudaMemcpyAsync(h.mean_f, d_out.mean_f, K * vox, cudaMemcpyDeviceToHost, s));
-    if (h.dyads) BPX_CUDA(cudaMemcpyAsync(h.dyads, d_out.dyads, 3 * K * vox, cudaMemcpyDeviceToHost, s));
-    BPX_CUDA(cudaStreamSynchronize(s));
+    int k = 0;
+    for (size_t v0 = 0; v0 < nvox; v0 += C, ++k) {
+      const size_t c = nvox - v0 < C ? nvox - v0 : C;
+      Set& q = set[k & 1];
+      // inputs of this sub-volume, once its buffer set's previous outputs have been copied out
+      if (k >= 2) BPX_CUDA(cudaStreamWaitEvent(sin, ev_free[k & 1], 0));
+      BPX_CUDA(cudaMemcpyAsync(q.data, vol->data + v0 * ndir, c * ndir * 4, cudaMemcpyHostToDevice, sin));
+      if (gn) BPX_CUDA(cudaMemcpyAsync(q.grad, vol->grad + v0 * 9, c * 9 * 4, cudaMemcpyHostToDevice, sin));
+      BPX_CUDA(cudaEventRecord(ev_in[k & 1], sin));
+      // the pipeline on the compute stream
+      BPX_CUDA(cudaStreamWaitEvent(sc, ev_in[k & 1], 0));
+      bpx_volume dv = *vol;
+      dv.nvox = (int32_t)c;
+      dv.voxel_offset = vol->voxel_offset + v0;
+      dv.data = q.data;
+      dv.bvecs = d_bvec;
+      dv.bvals = d_bval;
+      dv.grad = nullptr;
+      if (gn) {
+        bpx_status s2 = bpx_gradnonlin_dev((int32_t)c, vol->ndir, q.grad, d_bvec, d_bval, q.bvec_v, q.bval_v, sc);
+        if (s2 != BPX_OK) return s2;
+        dv.bvecs = q.bvec_v;
+        dv.bvals = q.bval_v;
+      }
+      bpx_status s3 = mlp ? bpx_xfibres_learned_dev(opts, &dv, d_mlp, freeze_props, &q.out, sc)
+                          : bpx_xfibres_dev(opts, &dv, &q.out, sc);
+      if (s3 != BPX_OK) return s3;
+      BPX_CUDA(cudaEventRecord(ev_done[k & 1], sc));
+      // the outputs back, into the host arrays' columns v0 .. v0 + c (pitched copies of the rows)
+      BPX_CUDA(cudaStreamWaitEvent(sout, ev_done[k & 1], 0));
+      auto rows_back = [&](void* dst, const void* src, size_t rows) -> cudaError_t {
+        if (!dst) return cudaSuccess;
+        return cudaMemcpy2DAsync((char*)dst + v0 * 4, nvox * 4, src, c * 4, c * 4, rows, cudaMemcpyDeviceToHost, sout);
+      };
+      BPX_CUDA(rows_back(h.th, q.out.th, K * ns));
+      BPX_CUDA(rows_back(h.ph, q.out.ph, K * ns));
+      BPX_CUDA(rows_back(h.f, q.out.f, K * ns));
+      BPX_CUDA(rows_back(h.mean_d, q.out.mean_d, 1));
+      BPX_CUDA(rows_back(h.mean_dstd, q.out.mean_dstd, 1));
+      BPX_CUDA(rows_back(h.mean_R, q.out.mean_R, 1));
+      BPX_CUDA(rows_back(h.mean_f0, q.out.mean_f0, 1));
+      BPX_CUDA(rows_back(h.mean_tau, q.out.mean_tau, 1));
+      BPX_CUDA(rows_back(h.mean_S0, q.out.mean_S0, 1));
+      BPX_CUDA(rows_back(h.status, q.out.status, 1));
+      BPX_CUDA(rows_back(h.mean_f, q.out.mean_f, K));
+      BPX_CUDA(rows_back(h.dyads, q.out.dyads, 3 * K));
+      BPX_CUDA(cudaEventRecord(ev_free[k & 1], sout));
+    }
+    BPX_CUDA(cudaStreamSynchronize(sout));
+    BPX_CUDA(cudaStreamSynchronize(sc));
     return BPX_OK;
   };
   st = run();
-  cudaStreamSynchronize(s);
-  cudaStreamDestroy(s);
-  cudaFree(base);
+  release();
   return st;
 }
 

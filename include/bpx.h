@@ -185,7 +185,11 @@ bpx_status bpx_xfibres_dev(const bpx_options* opts, const bpx_volume* vol, bpx_o
  * Drop-in for xfibres_gpu() with HOST buffers: copies data/bvecs/bvals (and grad under
  * gradnonlin) to the current device, corrects the b-matrix per voxel when vol->grad is given
  * (correct_bvals_bvecs, CUDA/xfibres_gpu.cu:151-170), runs the pipeline and copies the
- * outputs back into host buffers.  Synchronous.
+ * outputs back into host buffers.  Synchronous.  The volume goes through in sub-volumes of 65536
+ * voxels (or BPX_HOST_CHUNK from the environment) on two alternating device buffer sets, the
+ * copies of one overlapping the computation of the next (pinned host buffers let them run
+ * asynchronously); the outputs equal those of one pass over the whole volume, bit for bit, and
+ * the device memory held is that of two sub-volumes.
  */
 bpx_status bpx_xfibres_host(const bpx_options* opts, const bpx_volume* vol, bpx_outputs* host_out);
 

@@ -39,8 +39,10 @@ def setup(torch):
     return dict(params=params, prot=prot, data=data, bv=bv, bl=bl, base=base)
 
 
-def test_learned_host_entry_matches_device_entry(torch, setup):
+def test_learned_host_entry_matches_device_entry(torch, setup, monkeypatch):
     import ctypes as C
+
+    monkeypatch.setenv("BPX_HOST_CHUNK", "300")  # four sub-volumes through the two buffer sets
 
     from fdt_b200 import learned, lib
     from fdt_b200.abi import Volume

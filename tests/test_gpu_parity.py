@@ -279,15 +279,32 @@ def test_posterior_means_agree_with_oracle_small_config(torch, lib, oracle):
     assert np.median(np.degrees(np.arccos(np.clip(dots, 0, 1)))) < 1.0
 
 
-def test_host_entry_matches_device_entry(torch, lib):
+@pytest.mark.parametrize("chunk", [None, "16"])
+def test_host_entry_matches_device_entry(torch, lib, monkeypatch, chunk):
+    """The host entry equals the device pipeline bit for bit, in one sub-volume or (BPX_HOST_CHUNK
+    16: 16, 16, 16, 2 voxels through the two alternating buffer sets, copies overlapping compute)."""
+    if chunk:
+        monkeypatch.setenv("BPX_HOST_CHUNK", chunk)
     o = Options.make(model=2, nfibres=2, nburn=50, njumps=100, sampleevery=10, rician=1, f0=1)
     prot = synth.three_shell(9, 90)
     y, _ = synth.make_volume(50, prot, 2, True, 25.0, seed=51)
     h = lib.xfibres_host(o, y, prot.bvecs, prot.bvals)
     d, bv, bl = _dev(torch, y, prot.bvecs, prot.bvals)
     g = lib.xfibres_dev(o, d, bv, bl)
-    for k in ("th", "ph", "f", "mean_d", "mean_S0", "mean_f", "dyads", "status"):
+    for k in ("th", "ph", "f", "mean_d", "mean_S0", "mean_tau", "mean_f0", "mean_dstd", "mean_f", "dyads", "status"):
         assert np.array_equal(h[k].numpy(), g[k].cpu().numpy()), k
+
+
+def test_host_entry_with_gradnonlin_in_sub_volumes(torch, lib, monkeypatch):
+    o = Options.make(model=1, nfibres=2, nburn=50, njumps=100, sampleevery=10, gradnonlin=1)
+    prot = synth.single_shell_64()
+    y, _ = synth.make_volume(40, prot, 2, False, 20.0, seed=62)
+    grad = np.random.default_rng(3).normal(0, 0.02, (40, 9)).astype(np.float32)
+    whole = lib.xfibres_host(o, y, prot.bvecs, prot.bvals, grad=grad)
+    monkeypatch.setenv("BPX_HOST_CHUNK", "15")
+    parts = lib.xfibres_host(o, y, prot.bvecs, prot.bvals, grad=grad)
+    for k in ("th", "ph", "f", "mean_d", "mean_S0", "mean_f", "dyads", "status"):
+        assert np.array_equal(whole[k].numpy(), parts[k].numpy()), k
 
 
 def test_gradnonlin_zero_tensor_is_identity(torch, lib):
