@@ -804,7 +804,7 @@ def main():
     if not args.no_accuracy and uses_net and rank == 0:
         # R independent chains per voxel and form (the Monte-Carlo SE of a posterior mean is the
         # spread of the chain means), on the first voxels of the first chunk, cleaned as the path
-        # cleans them; forms: plain (the judge), plain at another seed (yardstick), learned
+        # cleans them; forms: plain (the comparator), plain at another seed (yardstick), learned
         # (adapting and frozen widths), LM start at the learned burn-in (the method without the
         # network), and a long LM-started chain (gold)
         d_acc = chunks_d[0][: args.acc_voxels].clone()

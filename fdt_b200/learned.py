@@ -8,7 +8,7 @@ gathers the mini-batches.
 
 The trained network replaces the LM initialiser and sets per-voxel proposal widths (which the
 chain then adapts, or keeps frozen), so the chain needs a shorter burn-in; the plain LM-initialised
-chain with the full burn-in stays the fallback and the judge of its accuracy (posterior_study and
+chain with the full burn-in stays the fallback and the comparator for its accuracy (posterior_study and
 study_report measure both against it and against a long chain).
 """
 from __future__ import annotations
@@ -282,7 +282,7 @@ def posterior_study(opts: Options, data, bvecs, bvals, mlp_params, R: int = 8, s
     (independent random streams: the volume is replicated R times, so every copy of a voxel has its
     own RNG key), for agreement.compare:
 
-      plain           LM start, the reference's widths, opts.nburn (1000): the form that judges errors
+      plain           LM start, the reference's widths, opts.nburn (1000): the comparator for the others
       plain_other_seed   the same with another seed (yardstick of plain-vs-plain agreement)
       learned         network start state and widths, burn-in 200, widths adapting (freeze 0)
       learned_frozen  the same, widths frozen after the burn-in (freeze 2)
