@@ -159,6 +159,7 @@ class TrackOptions(C.Structure):
         ("pathdist", C.c_int32),
         ("loopcheck", C.c_int32),
         ("modeuler", C.c_int32),
+        ("per_seed", C.c_int32),
         ("reserved", C.c_int32 * 1),
     ]
 

@@ -149,6 +149,7 @@ struct Tracker {
   const TrackArgs& a;
   uint2* tab;
   uint32_t stamp;
+  int* paths;  // the volume this particle's visits go to (its seed's with per_seed)
   uint2* lck;        // this thread's loopcheck table
   float4* lcd;
   uint32_t lc_stamp;  // one per tracked half (the tables are cleared per launch)
@@ -362,7 +363,7 @@ struct Tracker {
       flags |= way;
       if (count && vox != last) {
         last = vox;
-        if (first_visit(vox)) atomicAdd(a.paths + vox, o.pathdist ? ++nvisit : 1);
+        if (first_visit(vox)) atomicAdd(paths + vox, o.pathdist ? ++nvisit : 1);
       }
       pathlength += o.steplength;
       if (avoid) {
@@ -430,7 +431,7 @@ template <bool EXT>
 __global__ void __launch_bounds__(kTrackThreads, kTrackBlocksPerSm) track_kernel(TrackArgs a) {
   const uint64_t threads = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  Tracker T{a, a.tables + (t << a.log2n), 0u, nullptr, nullptr, 0u};
+  Tracker T{a, a.tables + (t << a.log2n), 0u, a.paths, nullptr, nullptr, 0u};
   if (a.o.loopcheck) {
     T.lck = a.lc_keys + (t << a.lc_log2n);
     T.lcd = a.lc_dirs + (t << a.lc_log2n);
@@ -443,6 +444,7 @@ __global__ void __launch_bounds__(kTrackThreads, kTrackBlocksPerSm) track_kernel
   for (uint64_t pid = a.pid_begin + t; pid < a.pid_end; pid += threads) {
     T.stamp = (uint32_t)(pid - a.pid_begin) + 1u;
     const int s = (int)(pid / (uint64_t)a.o.nparticles);
+    if (a.o.per_seed) T.paths = a.paths + (size_t)s * a.nvox;
     float u0[8];
     track_uniforms(a.o.seed, pid, 0, 0u, u0);  // the particle's own draws: step 0
     int fibst = a.o.fibst - 1;

@@ -393,7 +393,8 @@ def waypoint_bits(masks) -> np.ndarray:
 
 def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.0), avoid=None, stop=None,
               waypoints=None):
-    """probtrackx simple mode on device tensors: (paths [nz][ny][nx] int32, waytotal int) for
+    """probtrackx on device tensors: (paths [nz][ny][nx] int32, or [nseeds][nz][ny][nx] with
+    topts.per_seed; waytotal int) for
     seeds [nseeds][3] (voxel coordinates x, y, z).  `avoid` and `stop`: device masks of the mask's
     shape (--avoid, --stop); `waypoints`: a list of 1 to 32 masks (host or device) that a kept
     streamline must all pass (--waypoints)."""
@@ -405,9 +406,10 @@ def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0,
         bits = waypoint_bits([w.cpu().numpy() if hasattr(w, "cpu") else w for w in waypoints])
         way_bits = torch.from_numpy(bits).to("cuda")
     v = track_volume(th, ph, f, mask, voxel_size, avoid=avoid, stop=stop, waypoints=way_bits, nwaypoints=nway)
-    paths = torch.zeros(tuple(mask.shape), device="cuda", dtype=torch.int32)
+    sd = to_device(np.asarray(seeds, np.float32).reshape(-1, 3))
+    lead = (int(sd.shape[0]),) if topts.per_seed else ()
+    paths = torch.zeros(lead + tuple(mask.shape), device="cuda", dtype=torch.int32)
     way = torch.zeros(1, device="cuda", dtype=torch.int64)
-    sd = to_device(seeds)
     _check(load().bpx_probtrack_dev(C.byref(topts), C.byref(v), int(sd.shape[0]), _ptr(sd), _ptr(paths), _ptr(way),
                                     _stream(torch)), "bpx_probtrack_dev")
     return paths, int(way.item())

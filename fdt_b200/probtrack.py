@@ -1,14 +1,18 @@
-"""probtrackx's simple mode on a bedpostx directory, on the GPU (bpx_probtrack_dev).
+"""probtrackx on a bedpostx directory, on the GPU (bpx_probtrack_dev): simple and seedmask modes.
 
-    python -m fdt_b200.probtrack SUBJECT.bedpostX --seeds seeds.txt --out OUTDIR [-P 5000] [-S 2000]
-        [--steplength 0.5] [--cthr 0.2] [--fibthresh 0.01] [--distthresh 0] [--randfib 0] [--fibst 1]
-        [--usef] [--sampvox] [--pd] [-l] [--modeuler] [--seed N] [--avoid MASK] [--stop MASK]
-        [--waypoints MASK|LIST]
+    python -m fdt_b200.probtrack SUBJECT.bedpostX --seeds SEEDS --out OUTDIR [-o fdt_paths] [-P 5000]
+        [-S 2000] [--steplength 0.5] [--cthr 0.2] [--fibthresh 0.01] [--distthresh 0] [--randfib 0]
+        [--fibst 1] [--usef] [--sampvox] [--pd] [-l] [--modeuler] [--seed N] [--avoid MASK]
+        [--stop MASK] [--waypoints MASK|LIST]
 
 Reads merged_th{k}samples, merged_ph{k}samples, merged_f{k}samples and nodif_brain_mask (NIfTI-1)
-as probtrackx does (probtrackx.cc:25-96 with mode simple, tractvolsx.h:55-97), tracks from every
-seed point of the seed file (one point per row, voxel coordinates x y z; ptx_simple.cc:31-35) and
-writes fdt_paths (visit counts of the kept streamlines, the mask's geometry) and waytotal.
+as probtrackx does (probtrackx.cc:25-96, tractvolsx.h:55-97) and tracks from the seeds:
+  * SEEDS a text file of points (one per row, voxel coordinates x y z): simple mode
+    (ptx_simple.cc:16-70, as run with --opd): one path distribution per point,
+    OUTDIR/<out>_<x>_<y>_<z>.nii.gz, counts reset between points;
+  * SEEDS a NIfTI mask on the diffusion grid: seedmask mode (ptx_seedmask.cc): every voxel with a
+    non-zero value is a seed point, in z, y, x order, and OUTDIR/<out>.nii.gz sums them all.
+OUTDIR/waytotal holds the number of kept streamlines over all seeds (Counter::save_total).
 --avoid rejects a half that enters the mask, --stop ends a half where it enters it, and --waypoints
 (one mask, or a text file naming up to 32 masks one per line) keeps only streamlines whose halves
 together passed every mask (streamlines.cc:112-145, 279-330); all on the diffusion grid.
@@ -66,12 +70,34 @@ def waypoint_files(arg: str) -> list[str]:
     return [n if os.path.isabs(n) else os.path.join(base, n) for n in names]
 
 
-def run(bpx_dir: str, seeds: np.ndarray, opts: TrackOptions, outdir: str, avoid: str | None = None,
-        stop: str | None = None, waypoints: str | None = None) -> tuple[np.ndarray, int]:
+def seed_points(arg: str, grid: tuple[int, int, int]) -> tuple[np.ndarray, bool]:
+    """(seed points [n][3] as voxel x y z, per_seed): a text file of points (simple mode, one
+    output per point) or a NIfTI mask whose non-zero voxels, in z, y, x order, are the seeds
+    (seedmask mode, one output over all)."""
+    if arg.endswith((".nii", ".nii.gz")):
+        m = read_mask(arg, grid)  # [z][y][x]
+        zyx = np.argwhere(np.abs(m) > 0)
+        return np.ascontiguousarray(zyx[:, ::-1].astype(np.float32)), False
+    pts = np.loadtxt(arg, ndmin=2)
+    if pts.shape[1] != 3 and pts.shape[0] == 3:
+        pts = pts.T
+    return np.ascontiguousarray(pts, np.float32), True
+
+
+def run(bpx_dir: str, seeds, opts: TrackOptions, outdir: str, avoid: str | None = None,
+        stop: str | None = None, waypoints: str | None = None, outname: str = "fdt_paths") -> tuple[np.ndarray, int]:
+    """Tracks from `seeds` (a seed file or mask path, or an array of points for simple mode) and
+    writes the path distributions and waytotal; returns (paths [x][y][z], or [nseeds][x][y][z] in
+    simple mode, waytotal)."""
     import torch
 
     th, ph, f, m, hdr, vs = read_samples(bpx_dir)
     grid = m.shape[::-1]
+    if isinstance(seeds, str):
+        seeds, per_seed = seed_points(seeds, grid)
+    else:
+        seeds, per_seed = np.ascontiguousarray(seeds, np.float32).reshape(-1, 3), True
+    opts.per_seed = int(per_seed)
     dev = [lib.to_device(a) for a in (th, ph, f, m)]
     extra = {}
     if avoid:
@@ -80,23 +106,35 @@ def run(bpx_dir: str, seeds: np.ndarray, opts: TrackOptions, outdir: str, avoid:
         extra["stop"] = lib.to_device(read_mask(stop, grid))
     if waypoints:
         extra["waypoints"] = [read_mask(w, grid) for w in waypoint_files(waypoints)]
-    paths, way = lib.probtrack(opts, *dev, np.asarray(seeds, np.float32).reshape(-1, 3), voxel_size=vs, **extra)
+    paths, way = lib.probtrack(opts, *dev, seeds, voxel_size=vs, **extra)
     torch.cuda.synchronize()
-    vol = np.transpose(paths.cpu().numpy(), (2, 1, 0))  # back to [x][y][z]
     os.makedirs(outdir, exist_ok=True)
-    # an int32 volume, as the reference saves its volume<int> m_prob
-    nifti.write(os.path.join(outdir, "fdt_paths.nii.gz"), vol.astype(np.int32), like=hdr,
-                cal=(float(vol.min()), float(vol.max())))
+
+    def save(vol_zyx: np.ndarray, name: str) -> np.ndarray:
+        vol = np.transpose(vol_zyx, (2, 1, 0))  # back to [x][y][z]
+        # an int32 volume, as the reference saves its volume<int> m_prob
+        nifti.write(os.path.join(outdir, name + ".nii.gz"), vol.astype(np.int32), like=hdr,
+                    cal=(float(vol.min()), float(vol.max())))
+        return vol
+
+    p = paths.cpu().numpy()
+    if per_seed:
+        # Counter::save_pathdist(add): the basename, then _x_y_z as the seed file gives them
+        vols = np.stack([save(p[i], f"{outname}_{x:g}_{y:g}_{z:g}") for i, (x, y, z) in enumerate(seeds)])
+    else:
+        vols = save(p, outname)
     with open(os.path.join(outdir, "waytotal"), "w") as fh:
         fh.write(f"{way}\n")
-    return vol, way
+    return vols, way
 
 
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("bpx_dir")
-    ap.add_argument("--seeds", required=True, help="text file, one seed point (voxel x y z) per row")
-    ap.add_argument("--out", required=True)
+    ap.add_argument("--seeds", required=True,
+                    help="text file of seed points (voxel x y z per row: simple mode) or a seed mask (seedmask mode)")
+    ap.add_argument("--out", required=True, help="output directory")
+    ap.add_argument("-o", "--outname", default="fdt_paths", help="basename of the path distributions")
     ap.add_argument("-P", "--nsamples", type=int, default=5000)
     ap.add_argument("-S", "--nsteps", type=int, default=2000)
     ap.add_argument("--steplength", type=float, default=0.5)
@@ -115,14 +153,11 @@ def main(argv=None) -> None:
     ap.add_argument("--stop", help="stop tracking at locations given by this mask")
     ap.add_argument("--waypoints", help="waypoint mask, or a text file listing waypoint masks")
     a = ap.parse_args(argv)
-    seeds = np.loadtxt(a.seeds, ndmin=2)
-    if seeds.shape[1] != 3 and seeds.shape[0] == 3:
-        seeds = seeds.T
     o = TrackOptions.make(nparticles=a.nsamples, nsteps=a.nsteps, steplength=a.steplength, c_thr=a.cthr,
                           fibthresh=a.fibthresh, distthresh=a.distthresh, randfib=a.randfib, fibst=a.fibst,
                           usef=int(a.usef), sampvox=int(a.sampvox), pathdist=int(a.pd), loopcheck=int(a.loopcheck),
                           modeuler=int(a.modeuler), seed=a.seed)
-    _, way = run(a.bpx_dir, seeds, o, a.out, avoid=a.avoid, stop=a.stop, waypoints=a.waypoints)
+    _, way = run(a.bpx_dir, a.seeds, o, a.out, avoid=a.avoid, stop=a.stop, waypoints=a.waypoints, outname=a.outname)
     print(f"waytotal {way}")
 
 

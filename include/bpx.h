@@ -460,6 +460,10 @@ typedef struct bpx_track_options {
                           last had in the same cell of a 5x coarser grid (streamlines.cc:248-263) */
   int32_t modeuler;    /* --modeuler: modified Euler steps, along the mean of the sampled direction
                           and the one sampled a step ahead (streamlines.cc:352-361) */
+  int32_t per_seed;    /* 1: paths holds one volume per seed point, [nseeds][nz][ny][nx] (simple
+                          mode's fdt_paths_<x>_<y>_<z>, counts reset between seeds: ptx_simple.cc:
+                          50-62); 0: one volume summed over the seeds (seedmask mode's fdt_paths,
+                          ptx_seedmask.cc) */
   int32_t reserved[1]; /* zero */
 } bpx_track_options;
 
@@ -489,9 +493,9 @@ void bpx_track_options_default(bpx_track_options* opts);
 /*
  * Tracks opts->nparticles streamlines from each of nseeds seed points (seeds [nseeds][3], voxel
  * coordinates of the volume, x y z) and ADDS each kept streamline's distinct voxels to
- * paths [nz][ny][nx] (int32 counts, fdt_paths: the reference's volume<int> m_prob, wrapping past
- * 2^31 as it does) and the kept streamlines to *waytotal (device int64); the caller zeroes both
- * first.  Integer sums make the result independent of the order in which streamlines finish.
+ * paths [nz][ny][nx], or to its seed's volume of paths [nseeds][nz][ny][nx] with opts->per_seed
+ * (int32 counts, fdt_paths: the reference's volume<int> m_prob, wrapping past 2^31 as it does), and
+ * the kept streamlines to *waytotal (device int64); the caller zeroes both first.  Integer sums make the result independent of the order in which streamlines finish.
  * Uses workspace memory (see Concurrency): the samples repacked, 16 * ceil(3 * nfib / 4) bytes per
  * voxel and sample, and a visit table of 8 * 2^ceil(log2(2 * (nsteps + 2))) bytes per particle in
  * flight (1024 particles per multiprocessor, fewer if the tables would pass 8 GB: 5 GB on a B200 at

@@ -202,7 +202,8 @@ def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0,
               waypoints=None):
     """probtrackx simple mode on host arrays (th/ph/f [nfib][nsamples][nz][ny][nx], mask [nz][ny][nx],
     seeds [nseeds][3] voxel coordinates; optional avoid and stop masks and a list of waypoint masks,
-    each [nz][ny][nx]): (paths [nz][ny][nx] int32, waytotal)."""
+    each [nz][ny][nx]): (paths [nz][ny][nx] int32, or [nseeds][nz][ny][nx] with topts.per_seed,
+    waytotal)."""
     th, ph, f, mask = (np.ascontiguousarray(a, np.float32) for a in (th, ph, f, mask))
     v = TrackVolume()
     v.nfib, v.nsamples, v.nz, v.ny, v.nx = th.shape
@@ -221,9 +222,9 @@ def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0,
             bits |= (np.asarray(m) != 0).astype(np.uint32) << np.uint32(w)
         keep.append(bits)
         v.waypoints, v.nwaypoints = bits.ctypes.data, len(waypoints)
-    paths = np.zeros(mask.shape, np.int32)
-    way = C.c_int64(0)
     sd = np.ascontiguousarray(seeds, np.float32).reshape(-1, 3)
+    paths = np.zeros(((sd.shape[0],) if topts.per_seed else ()) + tuple(mask.shape), np.int32)
+    way = C.c_int64(0)
     rc = lib().orc_probtrack(C.byref(topts), C.byref(v), sd.shape[0], sd, paths, C.byref(way))
     assert rc == 0
     return paths, int(way.value)

@@ -10,7 +10,7 @@
  *                               waypoint, avoid (rubbish) and stop masks, the curvature stop,
  *                               the jump, the distance threshold;
  *   Counter::update_pathdist    (streamlines.cc:662-690): every voxel of a kept streamline counted
- *                               once (fdt_paths);
+ *                               once (fdt_paths), per seed point with per_seed (ptx_simple.cc:50-62);
  *   Tractvolsx::sample          (tractvolsx.h:101-255): probabilistic rounding of the position,
  *                               a random posterior sample, the first fibre (fibst, randfib 1/2)
  *                               and afterwards the fibre closest to the current direction among
@@ -394,8 +394,9 @@ int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nse
           stamp[vx] = (int64_t)pid;
           ++d;
           const uint32_t add = o->pathdist ? d : 1u;
+          const size_t at_vx = (o->per_seed ? (size_t)s * T.nvox : 0) + (size_t)vx;
 #pragma omp atomic
-          counts[vx] += add;
+          counts[at_vx] += add;
         }
       }
     }

@@ -46,6 +46,8 @@ CASES = [
     ("modeuler_randfib2_usef", dict(modeuler=1, randfib=2, usef=1)),
     ("loopcheck_low_cthr", dict(loopcheck=1, c_thr=0.05)),
     ("everything", dict(modeuler=1, loopcheck=1, pathdist=1, distthresh=3.0, masks=("avoid", "stop", "waypoints"))),
+    ("per_seed", dict(per_seed=1)),
+    ("per_seed_pathdist_waypoints", dict(per_seed=1, pathdist=1, masks=("waypoints",))),
 ]
 
 
@@ -118,8 +120,9 @@ def test_tracking_on_bedpostx_outputs_equals_oracle(torch):
 
 
 def test_probtrack_cli_with_masks_equals_oracle(torch, tmp_path):
-    """python -m fdt_b200.probtrack on a bedpostX directory with --avoid, --stop and a waypoint list:
-    fdt_paths and waytotal equal the oracle's on the same arrays."""
+    """python -m fdt_b200.probtrack on a bedpostX directory with --avoid, --stop and a waypoint list,
+    in simple mode (a seed file: one path distribution per point) and seedmask mode (a seed mask:
+    one over all its voxels): the volumes and waytotal equal the oracle's on the same arrays."""
     import os
 
     from fdt_b200 import nifti, probtrack
@@ -133,15 +136,29 @@ def test_probtrack_cli_with_masks_equals_oracle(torch, tmp_path):
         nifti.write(os.path.join(d, name + ".nii.gz"), np.transpose(m, (2, 1, 0)))
     with open(os.path.join(d, "ways.txt"), "w") as fh:
         fh.write("w1.nii.gz\nw2.nii.gz\n")
-    seeds = np.array([[5.0, 8.0, 5.0], [14.0, 7.0, 4.6]], np.float32)
+    common = ["-P", "150", "-S", "300", "--seed", "23", "--avoid", os.path.join(d, "avoid.nii.gz"), "--stop",
+              os.path.join(d, "stop.nii.gz"), "--waypoints", os.path.join(d, "ways.txt")]
+    # simple mode
+    seeds = np.array([[5.0, 8.0, 5.0], [14.0, 7.0, 4.5]], np.float32)
     np.savetxt(os.path.join(d, "seeds.txt"), seeds)
-    out = os.path.join(d, "out")
-    probtrack.main([d, "--seeds", os.path.join(d, "seeds.txt"), "--out", out, "-P", "150", "-S", "300", "--seed", "23",
-                    "--avoid", os.path.join(d, "avoid.nii.gz"), "--stop", os.path.join(d, "stop.nii.gz"),
-                    "--waypoints", os.path.join(d, "ways.txt")])
-    o = TrackOptions.make(nparticles=150, nsteps=300, seed=23)
+    out = os.path.join(d, "simple")
+    probtrack.main([d, "--seeds", os.path.join(d, "seeds.txt"), "--out", out] + common)
+    o = TrackOptions.make(nparticles=150, nsteps=300, seed=23, per_seed=1)
     # the directory's NIfTI files carry unit voxels
     want_p, want_w = O.probtrack(o, th, ph, f, mask, seeds, voxel_size=(1.0, 1.0, 1.0), **masks)
+    assert int(open(os.path.join(out, "waytotal")).read()) == want_w > 0
+    for i, name in enumerate(("fdt_paths_5_8_5", "fdt_paths_14_7_4.5")):
+        got, _ = nifti.read(os.path.join(out, name + ".nii.gz"))
+        assert np.array_equal(np.transpose(got, (2, 1, 0)), want_p[i]), name
+    # seedmask mode
+    sm = np.zeros_like(mask)
+    sm[5, 8, 5] = sm[4, 7, 14] = sm[5, 3, 10] = 1.0
+    nifti.write(os.path.join(d, "seedmask.nii.gz"), np.transpose(sm, (2, 1, 0)))
+    out = os.path.join(d, "seedmask")
+    probtrack.main([d, "--seeds", os.path.join(d, "seedmask.nii.gz"), "--out", out] + common)
+    pts = np.argwhere(sm > 0)[:, ::-1].astype(np.float32)  # z, y, x order of the voxels, as x y z
+    o.per_seed = 0
+    want_p, want_w = O.probtrack(o, th, ph, f, mask, pts, voxel_size=(1.0, 1.0, 1.0), **masks)
     got, _ = nifti.read(os.path.join(out, "fdt_paths.nii.gz"))
     assert int(open(os.path.join(out, "waytotal")).read()) == want_w > 0
     assert np.array_equal(np.transpose(got, (2, 1, 0)), want_p)

@@ -70,6 +70,18 @@ def test_pathdist_weights_the_dth_distinct_voxel_by_d():
     assert r == 0 and 0 < k < 20 and paths[4, 4, 14] == 13 * k + 2 * (20 - k)
 
 
+def test_per_seed_volumes_sum_to_the_volume_over_all_seeds():
+    th, ph, f, mask = synth.fibre_field((16, 14, 8), nsamples=8, seed=2)
+    seeds = [[4.0, 7.0, 4.0], [11.0, 6.0, 3.5], [8.0, 8.0, 4.0]]
+    o = TrackOptions.make(nparticles=40, nsteps=200, seed=13)
+    total, way = O.probtrack(o, th, ph, f, mask, seeds)
+    o.per_seed = 1
+    each, way_each = O.probtrack(o, th, ph, f, mask, seeds)
+    assert each.shape == (3,) + mask.shape and way_each == way
+    assert np.array_equal(each.sum(axis=0), total) and all(e.sum() > 0 for e in each)
+    assert np.all(each[:, mask == 0] == 0)
+
+
 def test_loopcheck_stops_paths_that_circle_back():
     th, ph, f, mask = synth.circle_field()
     seed = [[13.5, 11.5, 3.0]]  # two voxels from the axis: a circle fits in one coarse cell
@@ -207,3 +219,12 @@ def test_probtrack_cli_reads_samples_masks_and_waypoint_lists(tmp_path):
     assert [os.path.basename(p) for p in files] == ["w1.nii.gz", "w2.nii.gz"] and all(map(os.path.exists, files))
     assert probtrack.waypoint_files(files[0]) == [files[0]]
     assert np.array_equal(probtrack.read_mask(files[0], mask.shape[::-1]), w)
+    # seeds: a text file of points (simple mode), or a mask's voxels in z, y, x order (seedmask mode)
+    np.savetxt(os.path.join(str(tmp_path), "pts.txt"), [[1.0, 2.0, 3.0], [4.5, 5.0, 1.0]])
+    pts, per_seed = probtrack.seed_points(os.path.join(str(tmp_path), "pts.txt"), mask.shape[::-1])
+    assert per_seed and np.array_equal(pts, [[1, 2, 3], [4.5, 5, 1]])
+    sm = np.zeros_like(mask)
+    sm[1, 2, 3] = sm[0, 4, 5] = -2.0
+    nifti.write(os.path.join(str(tmp_path), "sm.nii.gz"), np.transpose(sm, (2, 1, 0)))
+    pts, per_seed = probtrack.seed_points(os.path.join(str(tmp_path), "sm.nii.gz"), mask.shape[::-1])
+    assert not per_seed and np.array_equal(pts, [[5, 4, 0], [3, 2, 1]])
