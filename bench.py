@@ -496,7 +496,7 @@ def run_plain_config(args, name: str):
 
 
 def run_probtrack(args):
-    """probtrackx simple mode on the GPU: streamlines/s on a synthetic crossing-fibre field with the
+    """probtrackx on the GPU: streamlines/s on a synthetic crossing-fibre field with the
     whole-brain sample count (96x96x60 grid, ellipsoidal mask, 3 fibres x 50 samples; fibre 1 along
     x, fibre 2 along y in half the volume), 1024 seed points in the mask x 5000 particles, probtrackx
     defaults (2000 steps, 0.5 mm, cthr 0.2, fibthresh 0.01), 2 mm voxels.  The CPU oracle of the
@@ -552,10 +552,11 @@ def run_probtrack(args):
     O.probtrack(o_cpu, th, ph, f, mask, seeds[:nb])
     t_cpu = time.perf_counter() - t0
     line = {
-        "metric": "streamlines/s, probtrackx simple mode on bedpostx samples (1 B200)", "value": n_lines / t,
+        "metric": "streamlines/s, probtrackx on bedpostx samples (1 B200)", "value": n_lines / t,
         "unit": "streamlines/s", "n_gpus": 1, "steps": k, "warmup": max(1, args.warmup), "ms_per_step": 1e3 * t,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-        "config": {"workload": "probtrackx simple mode: 96x96x60 crossing-fibre field, 3 fibres x 50 samples, "
+        "config": {"workload": "probtrackx (one path distribution over all seeds, as seedmask mode): 96x96x60 "
+                   "crossing-fibre field, 3 fibres x 50 samples, "
                    "%d seeds x 5000 particles, 2000 steps of 0.5 mm, cthr 0.2, fibthresh 0.01" % len(seeds),
                    "streamlines": n_lines, "waytotal": int(way.item()), "visits": int(paths.sum(dtype=torch.int64).item())},
         "cpu_baseline": {"value": nb * o.nparticles / t_cpu, "unit": "streamlines/s", "cores": cores, "kind": "port",
