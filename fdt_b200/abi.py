@@ -196,4 +196,7 @@ class TrackVolume(C.Structure):
         ("stop", C.c_void_p),
         ("waypoints", C.c_void_p),
         ("nwaypoints", C.c_int32),
+        ("ntargets", C.c_int32),
+        ("targets", C.c_void_p),
+        ("seeds_to_targets", C.c_void_p),
     ]

@@ -36,6 +36,9 @@ constexpr int kTrackThreads = 64;
 // (no spills); measured on 1024 seeds x 5000 particles, 8 / 10 / 12 / 16 blocks per SM took
 // 93.7 / 81.9 / 75.1 / 67.6 ms
 constexpr int kTrackBlocksPerSm = 16;
+// the extended form (--modeuler, --loopcheck, seeds to targets) carries more state: 12 blocks,
+// 85 registers
+constexpr int kTrackBlocksPerSmExt = 12;
 
 struct TrackArgs {
   bpx_track_options o;
@@ -144,6 +147,14 @@ __device__ __forceinline__ void jump_dir(Particle& P, const TrackArgs& a, float 
     P.rzi = P.rz;
   }
 }
+
+// what the counting passes of one particle carry over its kept halves: the path length so far on
+// the counted path, the targets already entered, the particle's seed
+struct Counted {
+  float length;
+  uint32_t tflags;
+  int seed;
+};
 
 struct Tracker {
   const TrackArgs& a;
@@ -311,10 +322,11 @@ struct Tracker {
   // accumulates the waypoint masks passed (over both halves of a particle).  Returns the reject
   // flag: 1 (entered the avoid mask, passed no waypoint, or shorter than distthresh), 2 (passed
   // some waypoints but not all), 0.
-  // EXT: compiled with --modeuler and --loopcheck (the plain form keeps its registers without them)
+  // EXT: compiled with --modeuler, --loopcheck and seeds to targets (the plain form keeps its
+  // registers without them)
   template <bool EXT>
   __device__ int half_line(Particle& P, uint64_t pid, int h, int fibst0, float x0, float y0, float z0,
-                           bool count, uint32_t& flags, int& nvisit) {
+                           bool count, uint32_t& flags, int& nvisit, Counted& cnt) {
     const bpx_track_options& o = a.o;
     const bpx_track_volume& v = a.v;
     bool init_sample = true, avoided = false;
@@ -364,7 +376,18 @@ struct Tracker {
       if (count && vox != last) {
         last = vox;
         if (first_visit(vox)) atomicAdd(paths + vox, o.pathdist ? ++nvisit : 1);
+        if (EXT && v.ntargets > 0) {
+          // a target is counted at its first entry on the counted path (a voxel change), if the path
+          // is by then at least distthresh long (Counter::update_seedcounts)
+          const uint32_t tb = __ldg(v.targets + vox) & ~cnt.tflags;
+          if (tb) {
+            if (cnt.length >= o.distthresh)
+              for (uint32_t b = tb; b; b &= b - 1) atomicAdd(v.seeds_to_targets + (size_t)(__ffs(b) - 1) * a.nseeds + cnt.seed, 1);
+            cnt.tflags |= tb;
+          }
+        }
       }
+      if (EXT && count) cnt.length += o.steplength;
       pathlength += o.steplength;
       if (avoid) {
         avoided = true;
@@ -428,7 +451,7 @@ struct Tracker {
 };
 
 template <bool EXT>
-__global__ void __launch_bounds__(kTrackThreads, kTrackBlocksPerSm) track_kernel(TrackArgs a) {
+__global__ void __launch_bounds__(kTrackThreads, EXT ? kTrackBlocksPerSmExt : kTrackBlocksPerSm) track_kernel(TrackArgs a) {
   const uint64_t threads = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   Tracker T{a, a.tables + (t << a.log2n), 0u, a.paths, nullptr, nullptr, 0u};
@@ -459,27 +482,28 @@ __global__ void __launch_bounds__(kTrackThreads, kTrackBlocksPerSm) track_kernel
     Particle P{};
     uint32_t flags = 0;  // waypoints passed by both halves (Streamliner::reset clears them per particle)
     int nvisit = 0;      // distinct voxels counted so far (the first half's before the second's)
+    Counted cnt{0.f, 0u, s};
     if (decide) {  // whether a half counts is known only once both halves have ended: track, then count
       const Particle P0 = P;
-      const int rej1 = T.template half_line<EXT>(P, pid, 0, fibst, x0, y0, z0, false, flags, nvisit);
+      const int rej1 = T.template half_line<EXT>(P, pid, 0, fibst, x0, y0, z0, false, flags, nvisit, cnt);
       reverse(P);
       const Particle P1 = P;
-      const int rej2 = T.template half_line<EXT>(P, pid, 1, fibst, x0, y0, z0, false, flags, nvisit);
+      const int rej2 = T.template half_line<EXT>(P, pid, 1, fibst, x0, y0, z0, false, flags, nvisit, cnt);
       const bool fwd = (rej1 == 0 || rej1 == 2) && !(rej2 > 0 && rej1 > 0), bwd = rej2 == 0;
       uint32_t unused = 0;
       if (fwd) {
         Particle Q = P0;
-        T.template half_line<EXT>(Q, pid, 0, fibst, x0, y0, z0, true, unused, nvisit);
+        T.template half_line<EXT>(Q, pid, 0, fibst, x0, y0, z0, true, unused, nvisit, cnt);
       }
       if (bwd) {
         Particle Q = P1;
-        T.template half_line<EXT>(Q, pid, 1, fibst, x0, y0, z0, true, unused, nvisit);
+        T.template half_line<EXT>(Q, pid, 1, fibst, x0, y0, z0, true, unused, nvisit, cnt);
       }
       if (fwd || bwd) ++kept;
     } else {  // every half is kept: count as it goes
-      T.template half_line<EXT>(P, pid, 0, fibst, x0, y0, z0, true, flags, nvisit);
+      T.template half_line<EXT>(P, pid, 0, fibst, x0, y0, z0, true, flags, nvisit, cnt);
       reverse(P);
-      T.template half_line<EXT>(P, pid, 1, fibst, x0, y0, z0, true, flags, nvisit);
+      T.template half_line<EXT>(P, pid, 1, fibst, x0, y0, z0, true, flags, nvisit, cnt);
       ++kept;
     }
   }
@@ -547,6 +571,12 @@ bpx_status check_track(const bpx_track_options* o, const bpx_track_volume* v, in
   if (nseeds < 0) return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: nseeds < 0");
   if (v->nwaypoints < 0 || v->nwaypoints > 32)
     return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: nwaypoints must be in 0..32");
+  if (v->ntargets < 0 || v->ntargets > 32)
+    return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: ntargets must be in 0..32");
+  if (v->ntargets > 0 && o->pathdist)
+    return api_fail(BPX_ERR_UNSUPPORTED, "bpx_probtrack_dev: seeds to targets with pathdist");
+  if (nseeds > 0 && v->ntargets > 0 && (!v->targets || !v->seeds_to_targets))
+    return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: NULL targets or seeds_to_targets");
   if (nseeds > 0 && (!seeds || !paths || !waytotal || !v->th || !v->ph || !v->f || !v->mask ||
                      (v->nwaypoints > 0 && !v->waypoints)))
     return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: NULL buffer");
@@ -609,7 +639,8 @@ bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volu
   // would pass 8 GB
   const size_t table_bytes = ((size_t)1 << log2n) * sizeof(uint2);
   const size_t max_blocks = ((size_t)8 << 30) / ((table_bytes + lc_bytes) * kTrackThreads);
-  int grid = sm_count() * kTrackBlocksPerSm;
+  const bool ext = opts->modeuler || opts->loopcheck || vol->ntargets > 0;
+  int grid = sm_count() * (ext ? kTrackBlocksPerSmExt : kTrackBlocksPerSm);
   if ((size_t)grid > max_blocks) grid = max_blocks > 0 ? (int)max_blocks : 1;
   const size_t threads = (size_t)grid * kTrackThreads;
   // workspace: the visit tables, the loopcheck tables (keys, then directions), the repacked samples
@@ -643,7 +674,7 @@ bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volu
     if (e0 != cudaSuccess) return api_cuda_fail(e0, "bpx_probtrack_dev: cudaMemsetAsync");
     a.pid_begin = b;
     a.pid_end = b + chunk < total ? b + chunk : total;
-    if (opts->modeuler || opts->loopcheck)
+    if (ext)
       track_kernel<true><<<grid, kTrackThreads, 0, s>>>(a);
     else
       track_kernel<false><<<grid, kTrackThreads, 0, s>>>(a);

@@ -392,12 +392,13 @@ def waypoint_bits(masks) -> np.ndarray:
 
 
 def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.0), avoid=None, stop=None,
-              waypoints=None):
+              waypoints=None, targets=None):
     """probtrackx on device tensors: (paths [nz][ny][nx] int32, or [nseeds][nz][ny][nx] with
     topts.per_seed; waytotal int) for
     seeds [nseeds][3] (voxel coordinates x, y, z).  `avoid` and `stop`: device masks of the mask's
     shape (--avoid, --stop); `waypoints`: a list of 1 to 32 masks (host or device) that a kept
-    streamline must all pass (--waypoints)."""
+    streamline must all pass (--waypoints); `targets`: a list of 1 to 32 target masks, for which
+    seeds_to_targets [ntargets][nseeds] (int32, host) is returned third (--targetmasks --os2t)."""
     torch = _torch()
     way_bits = None
     nway = 0
@@ -410,8 +411,15 @@ def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0,
     lead = (int(sd.shape[0]),) if topts.per_seed else ()
     paths = torch.zeros(lead + tuple(mask.shape), device="cuda", dtype=torch.int32)
     way = torch.zeros(1, device="cuda", dtype=torch.int64)
+    s2t = None
+    if targets is not None:
+        tb = torch.from_numpy(waypoint_bits([t.cpu().numpy() if hasattr(t, "cpu") else t for t in targets])).to("cuda")
+        s2t = torch.zeros((len(targets), int(sd.shape[0])), device="cuda", dtype=torch.int32)
+        v.ntargets, v.targets, v.seeds_to_targets = len(targets), tb.data_ptr(), s2t.data_ptr()
     _check(load().bpx_probtrack_dev(C.byref(topts), C.byref(v), int(sd.shape[0]), _ptr(sd), _ptr(paths), _ptr(way),
                                     _stream(torch)), "bpx_probtrack_dev")
+    if targets is not None:
+        return paths, int(way.item()), s2t.cpu().numpy()
     return paths, int(way.item())
 
 

@@ -3,7 +3,7 @@
     python -m fdt_b200.probtrack SUBJECT.bedpostX --seeds SEEDS --out OUTDIR [-o fdt_paths] [-P 5000]
         [-S 2000] [--steplength 0.5] [--cthr 0.2] [--fibthresh 0.01] [--distthresh 0] [--randfib 0]
         [--fibst 1] [--usef] [--sampvox] [--pd] [-l] [--modeuler] [--seed N] [--avoid MASK]
-        [--stop MASK] [--waypoints MASK|LIST]
+        [--stop MASK] [--waypoints MASK|LIST] [--targetmasks LIST --os2t]
 
 Reads merged_th{k}samples, merged_ph{k}samples, merged_f{k}samples and nodif_brain_mask (NIfTI-1)
 as probtrackx does (probtrackx.cc:25-96, tractvolsx.h:55-97) and tracks from the seeds:
@@ -13,6 +13,9 @@ as probtrackx does (probtrackx.cc:25-96, tractvolsx.h:55-97) and tracks from the
   * SEEDS a NIfTI mask on the diffusion grid: seedmask mode (ptx_seedmask.cc): every voxel with a
     non-zero value is a seed point, in z, y, x order, and OUTDIR/<out>.nii.gz sums them all.
 OUTDIR/waytotal holds the number of kept streamlines over all seeds (Counter::save_total).
+--targetmasks LIST --os2t (a text file naming up to 32 masks one per line) adds
+OUTDIR/seeds_to_<mask>.nii.gz: at every seed voxel, the kept streamlines from it that enter the
+mask (Counter::update_seedcounts, save_seedcounts; streamlines.cc:700-748, 900-930).
 --avoid rejects a half that enters the mask, --stop ends a half where it enters it, and --waypoints
 (one mask, or a text file naming up to 32 masks one per line) keeps only streamlines whose halves
 together passed every mask (streamlines.cc:112-145, 279-330); all on the diffusion grid.
@@ -85,7 +88,8 @@ def seed_points(arg: str, grid: tuple[int, int, int]) -> tuple[np.ndarray, bool]
 
 
 def run(bpx_dir: str, seeds, opts: TrackOptions, outdir: str, avoid: str | None = None,
-        stop: str | None = None, waypoints: str | None = None, outname: str = "fdt_paths") -> tuple[np.ndarray, int]:
+        stop: str | None = None, waypoints: str | None = None, outname: str = "fdt_paths",
+        targets: str | None = None) -> tuple[np.ndarray, int]:
     """Tracks from `seeds` (a seed file or mask path, or an array of points for simple mode) and
     writes the path distributions and waytotal; returns (paths [x][y][z], or [nseeds][x][y][z] in
     simple mode, waytotal)."""
@@ -106,7 +110,11 @@ def run(bpx_dir: str, seeds, opts: TrackOptions, outdir: str, avoid: str | None 
         extra["stop"] = lib.to_device(read_mask(stop, grid))
     if waypoints:
         extra["waypoints"] = [read_mask(w, grid) for w in waypoint_files(waypoints)]
-    paths, way = lib.probtrack(opts, *dev, seeds, voxel_size=vs, **extra)
+    target_files = waypoint_files(targets) if targets else []
+    if target_files:
+        extra["targets"] = [read_mask(t, grid) for t in target_files]
+    res = lib.probtrack(opts, *dev, seeds, voxel_size=vs, **extra)
+    paths, way = res[0], res[1]
     torch.cuda.synchronize()
     os.makedirs(outdir, exist_ok=True)
 
@@ -125,6 +133,20 @@ def run(bpx_dir: str, seeds, opts: TrackOptions, outdir: str, avoid: str | None 
         vols = save(p, outname)
     with open(os.path.join(outdir, "waytotal"), "w") as fh:
         fh.write(f"{way}\n")
+    if target_files:
+        # seeds_to_<target>: each seed's count at its (rounded) voxel, float as the reference saves it
+        s2t = res[2]
+        idx = np.floor(seeds + 0.5).astype(np.int64)
+        inside = np.all((idx >= 0) & (idx < np.array(grid)), axis=1)
+        for t, name in enumerate(target_files):
+            vol = np.zeros(grid, np.float32)
+            vol[idx[inside, 0], idx[inside, 1], idx[inside, 2]] = s2t[t][inside]
+            stem = os.path.basename(name)
+            for ext in (".nii.gz", ".nii"):
+                if stem.endswith(ext):
+                    stem = stem[: -len(ext)]
+            nifti.write(os.path.join(outdir, f"seeds_to_{stem}.nii.gz"), vol, like=hdr,
+                        cal=(0.0, float(opts.nparticles)))
     return vols, way
 
 
@@ -152,12 +174,17 @@ def main(argv=None) -> None:
     ap.add_argument("--avoid", help="reject pathways passing through this mask")
     ap.add_argument("--stop", help="stop tracking at locations given by this mask")
     ap.add_argument("--waypoints", help="waypoint mask, or a text file listing waypoint masks")
+    ap.add_argument("--targetmasks", help="text file listing target masks (seeds_to_targets)")
+    ap.add_argument("--os2t", action="store_true", help="output seeds_to_targets")
     a = ap.parse_args(argv)
     o = TrackOptions.make(nparticles=a.nsamples, nsteps=a.nsteps, steplength=a.steplength, c_thr=a.cthr,
                           fibthresh=a.fibthresh, distthresh=a.distthresh, randfib=a.randfib, fibst=a.fibst,
                           usef=int(a.usef), sampvox=int(a.sampvox), pathdist=int(a.pd), loopcheck=int(a.loopcheck),
                           modeuler=int(a.modeuler), seed=a.seed)
-    _, way = run(a.bpx_dir, a.seeds, o, a.out, avoid=a.avoid, stop=a.stop, waypoints=a.waypoints, outname=a.outname)
+    if a.os2t and not a.targetmasks:
+        ap.error("--os2t needs --targetmasks")
+    _, way = run(a.bpx_dir, a.seeds, o, a.out, avoid=a.avoid, stop=a.stop, waypoints=a.waypoints, outname=a.outname,
+                 targets=a.targetmasks if a.os2t else None)
     print(f"waytotal {way}")
 
 

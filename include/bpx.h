@@ -487,6 +487,14 @@ typedef struct bpx_track_volume {
   const float* stop;
   const uint32_t* waypoints;
   int32_t nwaypoints;
+  /* seeds to targets (--targetmasks with --os2t; Counter::update_seedcounts, streamlines.cc:700-748):
+   * targets holds bit t set inside target mask t < ntargets (<= 32), and seeds_to_targets
+   * [ntargets][nseeds] (OUTPUT, int32, added to) counts for every seed the kept streamlines whose
+   * path (first kept half, then second) enters target t at a path length >= distthresh.  Not with
+   * pathdist (the reference then adds path lengths). */
+  int32_t ntargets;
+  const uint32_t* targets;
+  int32_t* seeds_to_targets;
 } bpx_track_volume;
 
 void bpx_track_options_default(bpx_track_options* opts);

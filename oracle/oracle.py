@@ -199,11 +199,12 @@ def energy(opts: Options, data, bvecs, bvals, states):
 
 
 def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.0), avoid=None, stop=None,
-              waypoints=None):
+              waypoints=None, targets=None):
     """probtrackx simple mode on host arrays (th/ph/f [nfib][nsamples][nz][ny][nx], mask [nz][ny][nx],
     seeds [nseeds][3] voxel coordinates; optional avoid and stop masks and a list of waypoint masks,
-    each [nz][ny][nx]): (paths [nz][ny][nx] int32, or [nseeds][nz][ny][nx] with topts.per_seed,
-    waytotal)."""
+    each [nz][ny][nx]; target masks, each [nz][ny][nx]): (paths [nz][ny][nx] int32, or
+    [nseeds][nz][ny][nx] with topts.per_seed, waytotal[, seeds_to_targets [ntargets][nseeds] int32
+    when targets are given])."""
     th, ph, f, mask = (np.ascontiguousarray(a, np.float32) for a in (th, ph, f, mask))
     v = TrackVolume()
     v.nfib, v.nsamples, v.nz, v.ny, v.nx = th.shape
@@ -223,10 +224,20 @@ def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0,
         keep.append(bits)
         v.waypoints, v.nwaypoints = bits.ctypes.data, len(waypoints)
     sd = np.ascontiguousarray(seeds, np.float32).reshape(-1, 3)
+    s2t = None
+    if targets is not None:
+        tb = np.zeros(mask.shape, np.uint32)
+        for t, m in enumerate(targets):
+            tb |= (np.asarray(m) != 0).astype(np.uint32) << np.uint32(t)
+        s2t = np.zeros((len(targets), sd.shape[0]), np.int32)
+        keep += [tb, s2t]
+        v.ntargets, v.targets, v.seeds_to_targets = len(targets), tb.ctypes.data, s2t.ctypes.data
     paths = np.zeros(((sd.shape[0],) if topts.per_seed else ()) + tuple(mask.shape), np.int32)
     way = C.c_int64(0)
     rc = lib().orc_probtrack(C.byref(topts), C.byref(v), sd.shape[0], sd, paths, C.byref(way))
     assert rc == 0
+    if targets is not None:
+        return paths, int(way.value), s2t
     return paths, int(way.value)
 
 

@@ -11,6 +11,7 @@
  *                               the jump, the distance threshold;
  *   Counter::update_pathdist    (streamlines.cc:662-690): every voxel of a kept streamline counted
  *                               once (fdt_paths), per seed point with per_seed (ptx_simple.cc:50-62);
+ *   Counter::update_seedcounts  (streamlines.cc:700-748): seeds to targets;
  *   Tractvolsx::sample          (tractvolsx.h:101-255): probabilistic rounding of the position,
  *                               a random posterior sample, the first fibre (fibst, randfib 1/2)
  *                               and afterwards the fibre closest to the current direction among
@@ -387,9 +388,25 @@ int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nse
       /* Counter::update_pathdist over the kept halves in order: each distinct voxel adds 1, or
        * with --pd the d-th distinct voxel adds d (int32 sums wrap as the reference's int volume) */
       const int from = fwd ? 0 : n1, to = bwd ? n1 + n2 : n1;
-      uint32_t d = 0;
+      uint32_t d = 0, tflags = 0;
+      float clen = 0.f; /* path length along the counted path (Counter::update_seedcounts) */
       for (int i = from; i < to; ++i) {
         const int64_t vx = path[i];
+        if (v->ntargets > 0) {
+          /* seeds to targets: each target once per streamline, at its first entry, if the path is by
+           * then at least distthresh long */
+          const uint32_t tb = v->targets[vx] & ~tflags;
+          if (tb) {
+            if (clen >= o->distthresh)
+              for (int m = 0; m < v->ntargets; ++m)
+                if ((tb >> m) & 1u) {
+#pragma omp atomic
+                  v->seeds_to_targets[(size_t)m * nseeds + s] += 1;
+                }
+            tflags |= tb;
+          }
+        }
+        clen += o->steplength;
         if (stamp[vx] != (int64_t)pid) {
           stamp[vx] = (int64_t)pid;
           ++d;

@@ -155,13 +155,38 @@ def test_probtrack_cli_with_masks_equals_oracle(torch, tmp_path):
     sm[5, 8, 5] = sm[4, 7, 14] = sm[5, 3, 10] = 1.0
     nifti.write(os.path.join(d, "seedmask.nii.gz"), np.transpose(sm, (2, 1, 0)))
     out = os.path.join(d, "seedmask")
-    probtrack.main([d, "--seeds", os.path.join(d, "seedmask.nii.gz"), "--out", out] + common)
+    probtrack.main([d, "--seeds", os.path.join(d, "seedmask.nii.gz"), "--out", out, "--targetmasks",
+                    os.path.join(d, "ways.txt"), "--os2t"] + common)
     pts = np.argwhere(sm > 0)[:, ::-1].astype(np.float32)  # z, y, x order of the voxels, as x y z
     o.per_seed = 0
-    want_p, want_w = O.probtrack(o, th, ph, f, mask, pts, voxel_size=(1.0, 1.0, 1.0), **masks)
+    want_p, want_w, want_s = O.probtrack(o, th, ph, f, mask, pts, voxel_size=(1.0, 1.0, 1.0),
+                                         targets=masks["waypoints"], **masks)
     got, _ = nifti.read(os.path.join(out, "fdt_paths.nii.gz"))
     assert int(open(os.path.join(out, "waytotal")).read()) == want_w > 0
     assert np.array_equal(np.transpose(got, (2, 1, 0)), want_p)
+    # seeds_to_<target>: each seed voxel's count
+    for t, name in enumerate(("w1", "w2")):
+        vol, _ = nifti.read(os.path.join(out, f"seeds_to_{name}.nii.gz"))
+        at = vol[pts[:, 0].astype(int), pts[:, 1].astype(int), pts[:, 2].astype(int)]
+        assert np.array_equal(at, want_s[t]) and vol.sum() == want_s[t].sum(), name
+    assert want_s.sum() > 0
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(distthresh=6.0), dict(modeuler=1, per_seed=1)], ids=["plain", "distthresh",
+                                                                                           "modeuler_per_seed"])
+def test_seeds_to_targets_equal_oracle(torch, kw):
+    from fdt_b200 import lib
+
+    lib.load()
+    th, ph, f, mask = synth.fibre_field((20, 16, 10), nsamples=12, seed=4)
+    seeds = np.array([[5.0, 8.0, 5.0], [14.0, 7.0, 4.6], [10.3, 3.2, 5.5]], np.float32)
+    targets = _masks(mask, ("waypoints",))["waypoints"] + [_masks(mask, ("avoid",))["avoid"]]
+    o = TrackOptions.make(nparticles=200, nsteps=300, seed=31, **kw)
+    want_p, want_w, want_s = O.probtrack(o, th, ph, f, mask, seeds, targets=targets)
+    got_p, got_w, got_s = lib.probtrack(o, *(lib.to_device(a) for a in (th, ph, f, mask)), seeds, targets=targets)
+    torch.cuda.synchronize()
+    assert got_w == want_w and np.array_equal(got_p.cpu().numpy(), want_p)
+    assert np.array_equal(got_s, want_s) and want_s.sum() > 0, (got_s, want_s)
 
 
 @pytest.mark.parametrize("modeuler", [0, 1])

@@ -82,6 +82,22 @@ def test_per_seed_volumes_sum_to_the_volume_over_all_seeds():
     assert np.all(each[:, mask == 0] == 0)
 
 
+def test_seeds_to_targets_count_streamlines_entering_each_target():
+    th, ph, f, mask = _straight_box()
+    o = TrackOptions.make(nparticles=40, nsteps=400, seed=3)
+    far = np.zeros_like(mask)
+    far[0, 0, :] = 1.0  # outside the brain mask: never reached
+    paths, way, s2t = O.probtrack(o, th, ph, f, mask, [[15.0, 4.0, 4.0], [10.0, 4.0, 4.0]],
+                                  targets=[_plane(mask, 20), _plane(mask, 5), far])
+    assert way == 80 and s2t.shape == (3, 2) and s2t.dtype == np.int32
+    assert np.array_equal(s2t, [[40, 40], [40, 40], [0, 0]])
+    # with distthresh 20 mm the x = 20 plane counts only where the counted path (first kept half,
+    # then the second) is that long on arrival: after the -x half (24 mm), not straight from the seed
+    o.distthresh = 20.0
+    _, way, s2t = O.probtrack(o, th, ph, f, mask, [[15.0, 4.0, 4.0]], targets=[_plane(mask, 20)])
+    assert way == 40 and 0 < s2t[0, 0] < 40
+
+
 def test_loopcheck_stops_paths_that_circle_back():
     th, ph, f, mask = synth.circle_field()
     seed = [[13.5, 11.5, 3.0]]  # two voxels from the axis: a circle fits in one coarse cell
