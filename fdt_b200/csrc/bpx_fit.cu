@@ -546,7 +546,7 @@ __device__ __forceinline__ Real point(const Pre<KIND, K, F0>& q, const Real (&p)
     J[2] += q.sgn2 * q.S0 * wiso * iso_b;
     if (F0) J[P - 1] = q.S0 * (1.0 - iso) * q.dfx0;
     J0h = full / p[0];
-    J[0] = pm1d(p[0]) * full / p[0];
+    J[0] = pm1d(p[0]) * J0h;  // (+-full) / p0 = +-(full / p0) exactly: one division
     return full;
   }
 }
