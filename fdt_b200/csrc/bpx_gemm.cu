@@ -13,9 +13,8 @@
 //   K-major tile  [K/8 groups][rows][8]  -> LBO (K direction) = rows*16 B, SBO (rows) = 128 B
 //   MN-major tile [MN/8 groups][K][8]    -> LBO (K direction) = 128 B,    SBO (MN)   = K*16 B
 // One thread issues TMA and MMA (M = 128, N = tile width <= 256, K = 16 per instruction) through
-// a two-stage mbarrier ring; eight warps then read the accumulator (tcgen05.ld: warp w reaches TMEM
-// lanes 32 (w mod 4) .. +31, and warps w and w + 4 take alternate 32-column chunks) and run the
-// epilogue.  Every mbarrier wait is bounded (about a second), after which the kernel records
+// a two-stage mbarrier ring; four warps then read their 32 TMEM lanes each (tcgen05.ld) and run
+// the epilogue.  Every mbarrier wait is bounded (about a second), after which the kernel records
 // an error code, waits (bounded) for its own MMAs and releases its tensor memory.
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -33,7 +32,7 @@ namespace gemm {
 
 constexpr int kTileM = 128;
 constexpr int kChunkK = 64;
-constexpr int kThreads = 256;  // warp 0's lane 0 issues TMA and MMA; all eight warps run the epilogue
+constexpr int kThreads = 128;
 constexpr long long kWaitCycles = 2000000000ll;  // ~1 s at 2 GHz
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -191,14 +190,12 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (!done && g.error) atomicExch(g.error, 2);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
-  // epilogue: warp w owns accumulator rows 32 (w mod 4) .. +31 (its TMEM lanes) and every other
-  // 32-column chunk, starting at chunk w / 4
-  const int quad = warp & 3;
-  const int row = m0 + 32 * quad + lane;
-  for (int c = warp >> 2; c < nt / 32; c += 2) {
+  // epilogue: warp w owns accumulator rows 32w..32w+31 (TMEM lanes), 32 columns at a time
+  const int row = m0 + 32 * warp + lane;
+  for (int c = 0; c < nt / 32; ++c) {
     float v[32];
     __syncwarp();
-    tmem_ld32(tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(c * 32), v);
+    tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(c * 32), v);
     const int col0 = n0 + c * 32;
     if (!done || row >= g.M || col0 >= g.N) continue;
     const int ncol = min(32, g.N - col0);
