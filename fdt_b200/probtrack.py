@@ -3,7 +3,7 @@
     python -m fdt_b200.probtrack SUBJECT.bedpostX --seeds SEEDS --out OUTDIR [-o fdt_paths] [-P 5000]
         [-S 2000] [--steplength 0.5] [--cthr 0.2] [--fibthresh 0.01] [--distthresh 0] [--randfib 0]
         [--fibst 1] [--usef] [--sampvox] [--pd] [-l] [--modeuler] [--seed N] [--avoid MASK]
-        [--stop MASK] [--waypoints MASK|LIST] [--targetmasks LIST --os2t]
+        [--stop MASK] [--waypoints MASK|LIST] [--targetmasks LIST --os2t] [--network]
 
 Reads merged_th{k}samples, merged_ph{k}samples, merged_f{k}samples and nodif_brain_mask (NIfTI-1)
 as probtrackx does (probtrackx.cc:25-96, tractvolsx.h:55-97) and tracks from the seeds:
@@ -12,6 +12,9 @@ as probtrackx does (probtrackx.cc:25-96, tractvolsx.h:55-97) and tracks from the
     OUTDIR/<out>_<x>_<y>_<z>.nii.gz, counts reset between points;
   * SEEDS a NIfTI mask on the diffusion grid: seedmask mode (ptx_seedmask.cc): every voxel with a
     non-zero value is a seed point, in z, y, x order, and OUTDIR/<out>.nii.gz sums them all.
+  * --network with SEEDS a text file naming several masks: network mode (ptx_nmasks.cc): each
+    mask's voxels are seeds in turn, keeping only streamlines that reach the union of the other
+    masks (one extra waypoint mask); OUTDIR/<out>.nii.gz sums all, waytotal has one line per mask.
 OUTDIR/waytotal holds the number of kept streamlines over all seeds (Counter::save_total).
 --targetmasks LIST --os2t (a text file naming up to 32 masks one per line) adds
 OUTDIR/seeds_to_<mask>.nii.gz: at every seed voxel, the kept streamlines from it that enter the
@@ -150,6 +153,50 @@ def run(bpx_dir: str, seeds, opts: TrackOptions, outdir: str, avoid: str | None 
     return vols, way
 
 
+def run_network(bpx_dir: str, mask_list: str, opts: TrackOptions, outdir: str, avoid: str | None = None,
+                stop: str | None = None, waypoints: str | None = None,
+                outname: str = "fdt_paths") -> tuple[np.ndarray, list[int]]:
+    """Network mode (ptx_nmasks.cc): for each mask of the list, its voxels (z, y, x order) are the
+    seeds and the union of the other masks is one more waypoint mask (Streamliner::add_waymask);
+    the path counts of all masks add into one volume and waytotal has one entry per mask."""
+    import torch
+
+    th, ph, f, m, hdr, vs = read_samples(bpx_dir)
+    grid = m.shape[::-1]
+    masks = [np.abs(read_mask(n, grid)) > 0 for n in waypoint_files(mask_list)]
+    if len(masks) < 2:
+        raise ValueError("network mode needs at least two masks")
+    dev = [lib.to_device(a) for a in (th, ph, f, m)]
+    extra = {}
+    if avoid:
+        extra["avoid"] = lib.to_device(read_mask(avoid, grid))
+    if stop:
+        extra["stop"] = lib.to_device(read_mask(stop, grid))
+    user_ways = [read_mask(w, grid) for w in waypoint_files(waypoints)] if waypoints else []
+    if len(user_ways) > 31:
+        raise ValueError("network mode takes at most 31 waypoint masks of its own")
+    opts.per_seed = 0
+    total = np.zeros(m.shape, np.int64)
+    ways = []
+    for i, mi in enumerate(masks):
+        others = np.zeros(m.shape, bool)
+        for j, mj in enumerate(masks):
+            if j != i:
+                others |= mj
+        seeds = np.ascontiguousarray(np.argwhere(mi)[:, ::-1].astype(np.float32))
+        paths, way = lib.probtrack(opts, *dev, seeds, voxel_size=vs, waypoints=user_ways + [others.astype(np.float32)],
+                                   **extra)
+        torch.cuda.synchronize()
+        total += paths.cpu().numpy()
+        ways.append(way)
+    os.makedirs(outdir, exist_ok=True)
+    vol = np.transpose(total.astype(np.int32), (2, 1, 0))
+    nifti.write(os.path.join(outdir, outname + ".nii.gz"), vol, like=hdr, cal=(float(vol.min()), float(vol.max())))
+    with open(os.path.join(outdir, "waytotal"), "w") as fh:
+        fh.write("".join(f"{w}\n" for w in ways))
+    return vol, ways
+
+
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("bpx_dir")
@@ -176,6 +223,7 @@ def main(argv=None) -> None:
     ap.add_argument("--waypoints", help="waypoint mask, or a text file listing waypoint masks")
     ap.add_argument("--targetmasks", help="text file listing target masks (seeds_to_targets)")
     ap.add_argument("--os2t", action="store_true", help="output seeds_to_targets")
+    ap.add_argument("--network", action="store_true", help="network mode: --seeds lists several masks")
     a = ap.parse_args(argv)
     o = TrackOptions.make(nparticles=a.nsamples, nsteps=a.nsteps, steplength=a.steplength, c_thr=a.cthr,
                           fibthresh=a.fibthresh, distthresh=a.distthresh, randfib=a.randfib, fibst=a.fibst,
@@ -183,6 +231,13 @@ def main(argv=None) -> None:
                           modeuler=int(a.modeuler), seed=a.seed)
     if a.os2t and not a.targetmasks:
         ap.error("--os2t needs --targetmasks")
+    if a.network:
+        if a.os2t:
+            ap.error("seeds_to_targets is not available in network mode")
+        _, ways = run_network(a.bpx_dir, a.seeds, o, a.out, avoid=a.avoid, stop=a.stop, waypoints=a.waypoints,
+                              outname=a.outname)
+        print("waytotal " + " ".join(map(str, ways)))
+        return
     _, way = run(a.bpx_dir, a.seeds, o, a.out, avoid=a.avoid, stop=a.stop, waypoints=a.waypoints, outname=a.outname,
                  targets=a.targetmasks if a.os2t else None)
     print(f"waytotal {way}")

@@ -204,3 +204,38 @@ def test_loopcheck_on_circling_tracts_equals_oracle(torch, modeuler):
     o.loopcheck = 0
     free, _ = O.probtrack(o, th, ph, f, mask, seeds)
     assert want_p.sum() < free.sum()  # the check acted
+
+
+def test_probtrack_network_mode_equals_oracle(torch, tmp_path):
+    """--network: each mask seeds in turn, keeping streamlines that reach another mask; the summed
+    fdt_paths and the per-mask waytotal equal the oracle run mask by mask."""
+    import os
+
+    from fdt_b200 import nifti, probtrack
+
+    th, ph, f, mask = synth.fibre_field((20, 16, 10), nsamples=12, seed=4)
+    d = str(tmp_path)
+    synth.write_bedpostx_dir(d, th, ph, f, mask)
+    masks = []
+    for i, (z, y, x) in enumerate([(5, 8, 4), (5, 8, 10), (4, 7, 15)]):
+        mk = np.zeros_like(mask)
+        mk[z - 1:z + 1, y - 1:y + 1, x] = 1.0
+        masks.append(mk)
+        nifti.write(os.path.join(d, f"m{i}.nii.gz"), np.transpose(mk, (2, 1, 0)))
+    with open(os.path.join(d, "masks.txt"), "w") as fh:
+        fh.write("m0.nii.gz\nm1.nii.gz\nm2.nii.gz\n")
+    out = os.path.join(d, "net")
+    probtrack.main([d, "--seeds", os.path.join(d, "masks.txt"), "--network", "--out", out, "-P", "100", "-S", "300",
+                    "--seed", "41"])
+    o = TrackOptions.make(nparticles=100, nsteps=300, seed=41)
+    total = np.zeros(mask.shape, np.int64)
+    ways = []
+    for i, mi in enumerate(masks):
+        others = sum(mj for j, mj in enumerate(masks) if j != i)
+        pts = np.argwhere(mi > 0)[:, ::-1].astype(np.float32)
+        p, w = O.probtrack(o, th, ph, f, mask, pts, voxel_size=(1.0, 1.0, 1.0), waypoints=[others])
+        total += p
+        ways.append(w)
+    got, _ = nifti.read(os.path.join(out, "fdt_paths.nii.gz"))
+    assert [int(x) for x in open(os.path.join(out, "waytotal")).read().split()] == ways and sum(ways) > 0
+    assert np.array_equal(np.transpose(got, (2, 1, 0)), total)
