@@ -3,7 +3,7 @@
     python -m fdt_b200.probtrack SUBJECT.bedpostX --seeds SEEDS --out OUTDIR [-o fdt_paths] [-P 5000]
         [-S 2000] [--steplength 0.5] [--cthr 0.2] [--fibthresh 0.01] [--distthresh 0] [--randfib 0]
         [--fibst 1] [--usef] [--sampvox] [--pd] [-l] [--modeuler] [--seed N] [--avoid MASK]
-        [--stop MASK] [--waypoints MASK|LIST] [--targetmasks LIST --os2t] [--network]
+        [--stop MASK] [--waypoints MASK|LIST] [--targetmasks LIST --os2t] [--network] [--mask2 MASK]
 
 Reads merged_th{k}samples, merged_ph{k}samples, merged_f{k}samples and nodif_brain_mask (NIfTI-1)
 as probtrackx does (probtrackx.cc:25-96, tractvolsx.h:55-97) and tracks from the seeds:
@@ -14,7 +14,8 @@ as probtrackx does (probtrackx.cc:25-96, tractvolsx.h:55-97) and tracks from the
     non-zero value is a seed point, in z, y, x order, and OUTDIR/<out>.nii.gz sums them all.
   * --network with SEEDS a text file naming several masks: network mode (ptx_nmasks.cc): each
     mask's voxels are seeds in turn, keeping only streamlines that reach the union of the other
-    masks (one extra waypoint mask); OUTDIR/<out>.nii.gz sums all, waytotal has one line per mask.
+    masks (one extra waypoint mask); OUTDIR/<out>.nii.gz sums all, waytotal has one line per mask;
+  * SEEDS a mask and --mask2 a second one: twomasks mode (ptx_twomasks.cc), the same with two.
 OUTDIR/waytotal holds the number of kept streamlines over all seeds (Counter::save_total).
 --targetmasks LIST --os2t (a text file naming up to 32 masks one per line) adds
 OUTDIR/seeds_to_<mask>.nii.gz: at every seed voxel, the kept streamlines from it that enter the
@@ -153,17 +154,19 @@ def run(bpx_dir: str, seeds, opts: TrackOptions, outdir: str, avoid: str | None 
     return vols, way
 
 
-def run_network(bpx_dir: str, mask_list: str, opts: TrackOptions, outdir: str, avoid: str | None = None,
+def run_network(bpx_dir: str, mask_list, opts: TrackOptions, outdir: str, avoid: str | None = None,
                 stop: str | None = None, waypoints: str | None = None,
                 outname: str = "fdt_paths") -> tuple[np.ndarray, list[int]]:
-    """Network mode (ptx_nmasks.cc): for each mask of the list, its voxels (z, y, x order) are the
+    """Network mode (ptx_nmasks.cc; with two masks, twomasks mode, ptx_twomasks.cc): for each mask
+    of the list (a text file naming them, or a list of paths), its voxels (z, y, x order) are the
     seeds and the union of the other masks is one more waypoint mask (Streamliner::add_waymask);
     the path counts of all masks add into one volume and waytotal has one entry per mask."""
     import torch
 
     th, ph, f, m, hdr, vs = read_samples(bpx_dir)
     grid = m.shape[::-1]
-    masks = [np.abs(read_mask(n, grid)) > 0 for n in waypoint_files(mask_list)]
+    names = waypoint_files(mask_list) if isinstance(mask_list, str) else list(mask_list)
+    masks = [np.abs(read_mask(n, grid)) > 0 for n in names]
     if len(masks) < 2:
         raise ValueError("network mode needs at least two masks")
     dev = [lib.to_device(a) for a in (th, ph, f, m)]
@@ -224,6 +227,7 @@ def main(argv=None) -> None:
     ap.add_argument("--targetmasks", help="text file listing target masks (seeds_to_targets)")
     ap.add_argument("--os2t", action="store_true", help="output seeds_to_targets")
     ap.add_argument("--network", action="store_true", help="network mode: --seeds lists several masks")
+    ap.add_argument("--mask2", help="second seed mask (twomasks mode, with a seed mask)")
     a = ap.parse_args(argv)
     o = TrackOptions.make(nparticles=a.nsamples, nsteps=a.nsteps, steplength=a.steplength, c_thr=a.cthr,
                           fibthresh=a.fibthresh, distthresh=a.distthresh, randfib=a.randfib, fibst=a.fibst,
@@ -231,10 +235,11 @@ def main(argv=None) -> None:
                           modeuler=int(a.modeuler), seed=a.seed)
     if a.os2t and not a.targetmasks:
         ap.error("--os2t needs --targetmasks")
-    if a.network:
+    if a.network or a.mask2:
         if a.os2t:
-            ap.error("seeds_to_targets is not available in network mode")
-        _, ways = run_network(a.bpx_dir, a.seeds, o, a.out, avoid=a.avoid, stop=a.stop, waypoints=a.waypoints,
+            ap.error("seeds_to_targets is not available in multiple seed tractography")
+        masks = [a.seeds, a.mask2] if a.mask2 else a.seeds
+        _, ways = run_network(a.bpx_dir, masks, o, a.out, avoid=a.avoid, stop=a.stop, waypoints=a.waypoints,
                               outname=a.outname)
         print("waytotal " + " ".join(map(str, ways)))
         return

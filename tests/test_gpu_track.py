@@ -239,3 +239,28 @@ def test_probtrack_network_mode_equals_oracle(torch, tmp_path):
     got, _ = nifti.read(os.path.join(out, "fdt_paths.nii.gz"))
     assert [int(x) for x in open(os.path.join(out, "waytotal")).read().split()] == ways and sum(ways) > 0
     assert np.array_equal(np.transpose(got, (2, 1, 0)), total)
+
+
+def test_probtrack_twomasks_mode_is_network_mode_of_two(torch, tmp_path):
+    import os
+
+    from fdt_b200 import nifti, probtrack
+
+    th, ph, f, mask = synth.fibre_field((20, 16, 10), nsamples=12, seed=4)
+    d = str(tmp_path)
+    synth.write_bedpostx_dir(d, th, ph, f, mask)
+    for i, x in enumerate((4, 12)):
+        mk = np.zeros_like(mask)
+        mk[4:6, 7:9, x] = 1.0
+        nifti.write(os.path.join(d, f"m{i}.nii.gz"), np.transpose(mk, (2, 1, 0)))
+    with open(os.path.join(d, "two.txt"), "w") as fh:
+        fh.write("m0.nii.gz\nm1.nii.gz\n")
+    common = ["-P", "80", "-S", "300", "--seed", "5"]
+    probtrack.main([d, "--seeds", os.path.join(d, "m0.nii.gz"), "--mask2", os.path.join(d, "m1.nii.gz"), "--out",
+                    os.path.join(d, "two")] + common)
+    probtrack.main([d, "--seeds", os.path.join(d, "two.txt"), "--network", "--out", os.path.join(d, "net")] + common)
+    a, _ = nifti.read(os.path.join(d, "two", "fdt_paths.nii.gz"))
+    b, _ = nifti.read(os.path.join(d, "net", "fdt_paths.nii.gz"))
+    wa = open(os.path.join(d, "two", "waytotal")).read().split()
+    assert np.array_equal(a, b) and a.sum() > 0 and wa == open(os.path.join(d, "net", "waytotal")).read().split()
+    assert len(wa) == 2
