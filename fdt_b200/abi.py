@@ -199,4 +199,13 @@ class TrackVolume(C.Structure):
         ("ntargets", C.c_int32),
         ("targets", C.c_void_p),
         ("seeds_to_targets", C.c_void_p),
+        ("m2_ncols", C.c_int32),
+        ("lr_nx", C.c_int32),
+        ("lr_ny", C.c_int32),
+        ("lr_nz", C.c_int32),
+        ("lr_dx", C.c_float),
+        ("lr_dy", C.c_float),
+        ("lr_dz", C.c_float),
+        ("m2_lookup", C.c_void_p),
+        ("matrix2", C.c_void_p),
     ]

@@ -149,12 +149,17 @@ __device__ __forceinline__ void jump_dir(Particle& P, const TrackArgs& a, float 
 }
 
 // what the counting passes of one particle carry over its kept halves: the path length so far on
-// the counted path, the targets already entered, the particle's seed
+// the counted path, the targets already entered, the particle's seed, the tract-space columns
+// counted so far (--omatrix2 with --pd)
 struct Counted {
   float length;
   uint32_t tflags;
   int seed;
+  int nvisit2;
 };
+
+// --omatrix2's tract-space voxel keys share the visit table with the diffusion voxels
+constexpr uint32_t kLrKey = 0x80000000u;
 
 struct Tracker {
   const TrackArgs& a;
@@ -322,7 +327,7 @@ struct Tracker {
   // accumulates the waypoint masks passed (over both halves of a particle).  Returns the reject
   // flag: 1 (entered the avoid mask, passed no waypoint, or shorter than distthresh), 2 (passed
   // some waypoints but not all), 0.
-  // EXT: compiled with --modeuler, --loopcheck and seeds to targets (the plain form keeps its
+  // EXT: compiled with --modeuler, --loopcheck, seeds to targets and matrix2 (the plain form keeps its
   // registers without them)
   template <bool EXT>
   __device__ int half_line(Particle& P, uint64_t pid, int h, int fibst0, float x0, float y0, float z0,
@@ -338,7 +343,7 @@ struct Tracker {
     const int K = v.nfib;
     // a step of steplength mm mostly stays in the voxel of the step before, which is counted
     // already: the visit table is probed only when the voxel changes
-    uint32_t last = 0xffffffffu;
+    uint32_t last = 0xffffffffu, last_lr = 0xffffffffu;
     ++lc_stamp;  // every tracked half starts with an empty loopcheck volume
     for (int it = 1; it <= o.nsteps / 2; ++it) {
       const int ix = rnd(P.x), iy = rnd(P.y), iz = rnd(P.z);
@@ -384,6 +389,23 @@ struct Tracker {
             if (cnt.length >= o.distthresh)
               for (uint32_t b = tb; b; b &= b - 1) atomicAdd(v.seeds_to_targets + (size_t)(__ffs(b) - 1) * a.nseeds + cnt.seed, 1);
             cnt.tflags |= tb;
+          }
+        }
+      }
+      if (EXT && count && v.m2_ncols > 0) {
+        // --omatrix2: the tract-space voxel of the position (vox_to_vox in double, rounded to float,
+        // then MISCMATHS::round), counted once per particle when its column is not 0
+        // (Counter::update_matrix2_row); it can change inside a diffusion voxel
+        const int lx = rnd((float)(((double)P.x * (double)v.dx) / (double)v.lr_dx));
+        const int ly = rnd((float)(((double)P.y * (double)v.dy) / (double)v.lr_dy));
+        const int lz = rnd((float)(((double)P.z * (double)v.dz) / (double)v.lr_dz));
+        if (lx >= 0 && ly >= 0 && lz >= 0 && lx < v.lr_nx && ly < v.lr_ny && lz < v.lr_nz) {
+          const uint32_t lr = ((uint32_t)lz * (uint32_t)v.lr_ny + (uint32_t)ly) * (uint32_t)v.lr_nx + (uint32_t)lx;
+          if (lr != last_lr) {
+            last_lr = lr;
+            const int col = __ldg(v.m2_lookup + lr);
+            if (col > 0 && first_visit(lr | kLrKey))
+              atomicAdd(v.matrix2 + (size_t)cnt.seed * v.m2_ncols + col, o.pathdist ? ++cnt.nvisit2 : 1);
           }
         }
       }
@@ -482,7 +504,7 @@ __global__ void __launch_bounds__(kTrackThreads, EXT ? kTrackBlocksPerSmExt : kT
     Particle P{};
     uint32_t flags = 0;  // waypoints passed by both halves (Streamliner::reset clears them per particle)
     int nvisit = 0;      // distinct voxels counted so far (the first half's before the second's)
-    Counted cnt{0.f, 0u, s};
+    Counted cnt{0.f, 0u, s, 0};
     if (decide) {  // whether a half counts is known only once both halves have ended: track, then count
       const Particle P0 = P;
       const int rej1 = T.template half_line<EXT>(P, pid, 0, fibst, x0, y0, z0, false, flags, nvisit, cnt);
@@ -577,6 +599,17 @@ bpx_status check_track(const bpx_track_options* o, const bpx_track_volume* v, in
     return api_fail(BPX_ERR_UNSUPPORTED, "bpx_probtrack_dev: seeds to targets with pathdist");
   if (nseeds > 0 && v->ntargets > 0 && (!v->targets || !v->seeds_to_targets))
     return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: NULL targets or seeds_to_targets");
+  if (v->m2_ncols < 0) return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: m2_ncols < 0");
+  if (v->m2_ncols > 0) {
+    if (v->lr_nx < 1 || v->lr_ny < 1 || v->lr_nz < 1 || !(v->lr_dx > 0.f && v->lr_dy > 0.f && v->lr_dz > 0.f))
+      return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: bad tract-space grid for matrix2");
+    if ((size_t)v->nx * v->ny * v->nz >= (1ull << 31) || (size_t)v->lr_nx * v->lr_ny * v->lr_nz >= (1ull << 31))
+      return api_fail(BPX_ERR_UNSUPPORTED, "bpx_probtrack_dev: matrix2 with 2^31 or more voxels in either grid");
+    if ((size_t)nseeds * (size_t)v->m2_ncols >= (1ull << 40))
+      return api_fail(BPX_ERR_UNSUPPORTED, "bpx_probtrack_dev: matrix2 of 2^40 or more entries");
+    if (nseeds > 0 && (!v->m2_lookup || !v->matrix2))
+      return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: NULL m2_lookup or matrix2");
+  }
   if (nseeds > 0 && (!seeds || !paths || !waytotal || !v->th || !v->ph || !v->f || !v->mask ||
                      (v->nwaypoints > 0 && !v->waypoints)))
     return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: NULL buffer");
@@ -622,9 +655,11 @@ bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volu
   a.seeds = seeds;
   a.paths = reinterpret_cast<int*>(paths);
   a.waytotal = reinterpret_cast<unsigned long long*>(waytotal);
-  // a table of at least twice the longest path (one voxel per step of both halves)
+  // a table of at least twice the longest path (one voxel per step of both halves, and one
+  // tract-space voxel per step with matrix2)
+  const long long keys = (long long)(opts->nsteps + 2) * (vol->m2_ncols > 0 ? 2 : 1);
   int log2n = 1;
-  while ((1ll << log2n) < 2ll * (opts->nsteps + 2)) ++log2n;
+  while ((1ll << log2n) < 2ll * keys) ++log2n;
   a.log2n = log2n;
   // --loopcheck: a table of at least twice the coarse cells one half can enter
   a.lcnx = vol->nx / 5 + 2;
@@ -639,7 +674,7 @@ bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volu
   // would pass 8 GB
   const size_t table_bytes = ((size_t)1 << log2n) * sizeof(uint2);
   const size_t max_blocks = ((size_t)8 << 30) / ((table_bytes + lc_bytes) * kTrackThreads);
-  const bool ext = opts->modeuler || opts->loopcheck || vol->ntargets > 0;
+  const bool ext = opts->modeuler || opts->loopcheck || vol->ntargets > 0 || vol->m2_ncols > 0;
   int grid = sm_count() * (ext ? kTrackBlocksPerSmExt : kTrackBlocksPerSm);
   if ((size_t)grid > max_blocks) grid = max_blocks > 0 ? (int)max_blocks : 1;
   const size_t threads = (size_t)grid * kTrackThreads;

@@ -391,14 +391,26 @@ def waypoint_bits(masks) -> np.ndarray:
     return bits.view(np.int32)
 
 
+def matrix2_lookup(lrmask) -> np.ndarray:
+    """bpx_track_volume.m2_lookup for a tract-space mask [lz][ly][lx]: int32 of the same shape, the
+    column of every voxel inside the mask (0, 1, ... in z, y, x order, as Counter::initialise_matrix2
+    numbers them, streamlines.cc:515-549) and -1 outside."""
+    m = np.asarray(lrmask) != 0
+    lut = np.full(m.shape, -1, np.int32)
+    lut[m] = np.arange(int(m.sum()), dtype=np.int32)
+    return lut
+
+
 def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.0), avoid=None, stop=None,
-              waypoints=None, targets=None):
+              waypoints=None, targets=None, matrix2=None):
     """probtrackx on device tensors: (paths [nz][ny][nx] int32, or [nseeds][nz][ny][nx] with
     topts.per_seed; waytotal int) for
     seeds [nseeds][3] (voxel coordinates x, y, z).  `avoid` and `stop`: device masks of the mask's
     shape (--avoid, --stop); `waypoints`: a list of 1 to 32 masks (host or device) that a kept
     streamline must all pass (--waypoints); `targets`: a list of 1 to 32 target masks, for which
-    seeds_to_targets [ntargets][nseeds] (int32, host) is returned third (--targetmasks --os2t)."""
+    seeds_to_targets [ntargets][nseeds] (int32, host) follows waytotal (--targetmasks --os2t);
+    `matrix2`: (tract-space mask [lz][ly][lx], its voxel size in mm), for which fdt_matrix2
+    [nseeds][columns] (int32, host) comes last (--omatrix2 --lrmask)."""
     torch = _torch()
     way_bits = None
     nway = 0
@@ -416,11 +428,25 @@ def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0,
         tb = torch.from_numpy(waypoint_bits([t.cpu().numpy() if hasattr(t, "cpu") else t for t in targets])).to("cuda")
         s2t = torch.zeros((len(targets), int(sd.shape[0])), device="cuda", dtype=torch.int32)
         v.ntargets, v.targets, v.seeds_to_targets = len(targets), tb.data_ptr(), s2t.data_ptr()
+    m2 = None
+    if matrix2 is not None:
+        lrmask, lr_size = matrix2
+        lut = matrix2_lookup(lrmask.cpu().numpy() if hasattr(lrmask, "cpu") else lrmask)
+        ncols = int((lut >= 0).sum())
+        lut_d = torch.from_numpy(lut).to("cuda")
+        m2 = torch.zeros((int(sd.shape[0]), ncols), device="cuda", dtype=torch.int32)
+        v.m2_ncols = ncols
+        v.lr_nz, v.lr_ny, v.lr_nx = (int(x) for x in lut.shape)
+        v.lr_dx, v.lr_dy, v.lr_dz = (float(x) for x in lr_size)
+        v.m2_lookup, v.matrix2 = lut_d.data_ptr(), m2.data_ptr()
     _check(load().bpx_probtrack_dev(C.byref(topts), C.byref(v), int(sd.shape[0]), _ptr(sd), _ptr(paths), _ptr(way),
                                     _stream(torch)), "bpx_probtrack_dev")
+    out = (paths, int(way.item()))
     if targets is not None:
-        return paths, int(way.item()), s2t.cpu().numpy()
-    return paths, int(way.item())
+        out += (s2t.cpu().numpy(),)
+    if matrix2 is not None:
+        out += (m2.cpu().numpy(),)
+    return out
 
 
 class Handle:

@@ -3,7 +3,8 @@
     python -m fdt_b200.probtrack SUBJECT.bedpostX --seeds SEEDS --out OUTDIR [-o fdt_paths] [-P 5000]
         [-S 2000] [--steplength 0.5] [--cthr 0.2] [--fibthresh 0.01] [--distthresh 0] [--randfib 0]
         [--fibst 1] [--usef] [--sampvox] [--pd] [-l] [--modeuler] [--seed N] [--avoid MASK]
-        [--stop MASK] [--waypoints MASK|LIST] [--targetmasks LIST --os2t] [--network] [--mask2 MASK]
+        [--stop MASK] [--waypoints MASK|LIST] [--targetmasks LIST --os2t] [--omatrix2 --lrmask MASK]
+        [--network] [--mask2 MASK]
 
 Reads merged_th{k}samples, merged_ph{k}samples, merged_f{k}samples and nodif_brain_mask (NIfTI-1)
 as probtrackx does (probtrackx.cc:25-96, tractvolsx.h:55-97) and tracks from the seeds:
@@ -20,6 +21,11 @@ OUTDIR/waytotal holds the number of kept streamlines over all seeds (Counter::sa
 --targetmasks LIST --os2t (a text file naming up to 32 masks one per line) adds
 OUTDIR/seeds_to_<mask>.nii.gz: at every seed voxel, the kept streamlines from it that enter the
 mask (Counter::update_seedcounts, save_seedcounts; streamlines.cc:700-748, 900-930).
+--omatrix2 --lrmask MASK (a mask on a tract-space grid of its own voxel size, in line with the
+diffusion grid) adds OUTDIR/fdt_matrix2.nii.gz, seeds x tract-space voxels: for every seed, the
+kept streamlines from it through each voxel of the mask, and its coordinate and lookup files
+(Counter::initialise_matrix2, update_matrix2_row, save_matrix2; streamlines.cc:515-560, 772-808,
+970-980).
 --avoid rejects a half that enters the mask, --stop ends a half where it enters it, and --waypoints
 (one mask, or a text file naming up to 32 masks one per line) keeps only streamlines whose halves
 together passed every mask (streamlines.cc:112-145, 279-330); all on the diffusion grid.
@@ -93,7 +99,7 @@ def seed_points(arg: str, grid: tuple[int, int, int]) -> tuple[np.ndarray, bool]
 
 def run(bpx_dir: str, seeds, opts: TrackOptions, outdir: str, avoid: str | None = None,
         stop: str | None = None, waypoints: str | None = None, outname: str = "fdt_paths",
-        targets: str | None = None) -> tuple[np.ndarray, int]:
+        targets: str | None = None, lrmask: str | None = None) -> tuple[np.ndarray, int]:
     """Tracks from `seeds` (a seed file or mask path, or an array of points for simple mode) and
     writes the path distributions and waytotal; returns (paths [x][y][z], or [nseeds][x][y][z] in
     simple mode, waytotal)."""
@@ -117,6 +123,10 @@ def run(bpx_dir: str, seeds, opts: TrackOptions, outdir: str, avoid: str | None 
     target_files = waypoint_files(targets) if targets else []
     if target_files:
         extra["targets"] = [read_mask(t, grid) for t in target_files]
+    if lrmask:
+        lr, lr_hdr = nifti.read(lrmask)
+        lr_zyx = np.ascontiguousarray(np.transpose(np.asarray(lr, np.float32).reshape(lr.shape[:3]), (2, 1, 0)))
+        extra["matrix2"] = (lr_zyx, tuple(float(x) for x in lr_hdr.pixdim[1:4]))
     res = lib.probtrack(opts, *dev, seeds, voxel_size=vs, **extra)
     paths, way = res[0], res[1]
     torch.cuda.synchronize()
@@ -151,7 +161,26 @@ def run(bpx_dir: str, seeds, opts: TrackOptions, outdir: str, avoid: str | None 
                     stem = stem[: -len(ext)]
             nifti.write(os.path.join(outdir, f"seeds_to_{stem}.nii.gz"), vol, like=hdr,
                         cal=(0.0, float(opts.nparticles)))
+    if lrmask:
+        save_matrix2(outdir, res[-1], seeds, lr_zyx, lr_hdr)
     return vols, way
+
+
+def save_matrix2(outdir: str, m2: np.ndarray, seeds: np.ndarray, lr_zyx: np.ndarray, lr_hdr) -> None:
+    """Counter::save_matrix2 (streamlines.cc:970-980): fdt_matrix2 (seeds along x, tract-space
+    columns along y), coords_for_fdt_matrix2 (each seed's voxel x y z), tract_space_coords_for_fdt_matrix2
+    (each column's tract-space voxel), lookup_tractspace_fdt_matrix2 (each tract-space voxel's
+    column, 0 outside the mask); int32 as the reference's volume<int>."""
+    m2 = np.asarray(m2, np.int32)
+    nifti.write(os.path.join(outdir, "fdt_matrix2.nii.gz"), m2[:, :, None], cal=(0.0, float(m2.max(initial=0))))
+    seed_vox = np.floor(np.asarray(seeds, np.float64) + 0.5).astype(np.int32)
+    nifti.write(os.path.join(outdir, "coords_for_fdt_matrix2.nii.gz"), seed_vox[:, :, None])
+    inside = lr_zyx != 0
+    tract = np.ascontiguousarray(np.argwhere(inside)[:, ::-1].astype(np.int32))  # z, y, x order -> x y z
+    nifti.write(os.path.join(outdir, "tract_space_coords_for_fdt_matrix2.nii.gz"), tract[:, :, None])
+    lut = np.maximum(lib.matrix2_lookup(lr_zyx), 0)
+    nifti.write(os.path.join(outdir, "lookup_tractspace_fdt_matrix2.nii.gz"), np.transpose(lut, (2, 1, 0)),
+                like=lr_hdr, cal=(0.0, float(lut.max(initial=0))))
 
 
 def run_network(bpx_dir: str, mask_list, opts: TrackOptions, outdir: str, avoid: str | None = None,
@@ -226,6 +255,8 @@ def main(argv=None) -> None:
     ap.add_argument("--waypoints", help="waypoint mask, or a text file listing waypoint masks")
     ap.add_argument("--targetmasks", help="text file listing target masks (seeds_to_targets)")
     ap.add_argument("--os2t", action="store_true", help="output seeds_to_targets")
+    ap.add_argument("--omatrix2", action="store_true", help="output matrix2 (seeds x tract-space voxels)")
+    ap.add_argument("--lrmask", help="tract-space (low resolution) mask for matrix2")
     ap.add_argument("--network", action="store_true", help="network mode: --seeds lists several masks")
     ap.add_argument("--mask2", help="second seed mask (twomasks mode, with a seed mask)")
     a = ap.parse_args(argv)
@@ -235,16 +266,18 @@ def main(argv=None) -> None:
                           modeuler=int(a.modeuler), seed=a.seed)
     if a.os2t and not a.targetmasks:
         ap.error("--os2t needs --targetmasks")
+    if a.omatrix2 and not a.lrmask:
+        ap.error("--omatrix2 needs --lrmask")
     if a.network or a.mask2:
-        if a.os2t:
-            ap.error("seeds_to_targets is not available in multiple seed tractography")
+        if a.os2t or a.omatrix2:
+            ap.error("seeds_to_targets and matrix2 are not available in multiple seed tractography")
         masks = [a.seeds, a.mask2] if a.mask2 else a.seeds
         _, ways = run_network(a.bpx_dir, masks, o, a.out, avoid=a.avoid, stop=a.stop, waypoints=a.waypoints,
                               outname=a.outname)
         print("waytotal " + " ".join(map(str, ways)))
         return
     _, way = run(a.bpx_dir, a.seeds, o, a.out, avoid=a.avoid, stop=a.stop, waypoints=a.waypoints, outname=a.outname,
-                 targets=a.targetmasks if a.os2t else None)
+                 targets=a.targetmasks if a.os2t else None, lrmask=a.lrmask if a.omatrix2 else None)
     print(f"waytotal {way}")
 
 

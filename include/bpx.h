@@ -495,6 +495,18 @@ typedef struct bpx_track_volume {
   int32_t ntargets;
   const uint32_t* targets;
   int32_t* seeds_to_targets;
+  /* --omatrix2 (Counter::update_matrix2_row, streamlines.cc:772-808): a tract-space grid of
+   * lr_nx x lr_ny x lr_nz voxels of lr_dx x lr_dy x lr_dz mm, to which a path position maps by its
+   * mm coordinates (vox_to_vox with the identity: round(x * dx / lr_dx)); m2_lookup
+   * [lr_nz][lr_ny][lr_nx] gives each tract-space voxel's column (-1 outside the --target2 mask);
+   * matrix2 [nseeds][m2_ncols] (OUTPUT, int32, added to) counts for every seed the kept
+   * streamlines through each column, once per streamline (with pathdist the d-th new column adds
+   * d).  Column 0 is never counted, as in the reference, whose test is "column != 0". */
+  int32_t m2_ncols;
+  int32_t lr_nx, lr_ny, lr_nz;
+  float lr_dx, lr_dy, lr_dz;
+  const int32_t* m2_lookup;
+  int32_t* matrix2;
 } bpx_track_volume;
 
 void bpx_track_options_default(bpx_track_options* opts);

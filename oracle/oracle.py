@@ -199,12 +199,13 @@ def energy(opts: Options, data, bvecs, bvals, states):
 
 
 def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.0), avoid=None, stop=None,
-              waypoints=None, targets=None):
+              waypoints=None, targets=None, matrix2=None):
     """probtrackx simple mode on host arrays (th/ph/f [nfib][nsamples][nz][ny][nx], mask [nz][ny][nx],
     seeds [nseeds][3] voxel coordinates; optional avoid and stop masks and a list of waypoint masks,
-    each [nz][ny][nx]; target masks, each [nz][ny][nx]): (paths [nz][ny][nx] int32, or
-    [nseeds][nz][ny][nx] with topts.per_seed, waytotal[, seeds_to_targets [ntargets][nseeds] int32
-    when targets are given])."""
+    each [nz][ny][nx]; target masks, each [nz][ny][nx]; matrix2 = (tract-space mask [lz][ly][lx], its
+    voxel size)): (paths [nz][ny][nx] int32, or [nseeds][nz][ny][nx] with topts.per_seed,
+    waytotal[, seeds_to_targets [ntargets][nseeds] int32 when targets are given][, fdt_matrix2
+    [nseeds][columns] int32 when matrix2 is given])."""
     th, ph, f, mask = (np.ascontiguousarray(a, np.float32) for a in (th, ph, f, mask))
     v = TrackVolume()
     v.nfib, v.nsamples, v.nz, v.ny, v.nx = th.shape
@@ -232,13 +233,28 @@ def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0,
         s2t = np.zeros((len(targets), sd.shape[0]), np.int32)
         keep += [tb, s2t]
         v.ntargets, v.targets, v.seeds_to_targets = len(targets), tb.ctypes.data, s2t.ctypes.data
+    m2 = None
+    if matrix2 is not None:
+        lrmask, lr_size = matrix2
+        inside = np.asarray(lrmask) != 0
+        lut = np.full(inside.shape, -1, np.int32)  # columns in z, y, x order (Counter::initialise_matrix2)
+        lut[inside] = np.arange(int(inside.sum()), dtype=np.int32)
+        m2 = np.zeros((sd.shape[0], int(inside.sum())), np.int32)
+        keep += [lut, m2]
+        v.m2_ncols = m2.shape[1]
+        v.lr_nz, v.lr_ny, v.lr_nx = lut.shape
+        v.lr_dx, v.lr_dy, v.lr_dz = lr_size
+        v.m2_lookup, v.matrix2 = lut.ctypes.data, m2.ctypes.data
     paths = np.zeros(((sd.shape[0],) if topts.per_seed else ()) + tuple(mask.shape), np.int32)
     way = C.c_int64(0)
     rc = lib().orc_probtrack(C.byref(topts), C.byref(v), sd.shape[0], sd, paths, C.byref(way))
     assert rc == 0
+    out = (paths, int(way.value))
     if targets is not None:
-        return paths, int(way.value), s2t
-    return paths, int(way.value)
+        out += (s2t,)
+    if matrix2 is not None:
+        out += (m2,)
+    return out
 
 
 def sincos_fast(x: float) -> tuple[float, float]:

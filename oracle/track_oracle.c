@@ -12,6 +12,7 @@
  *   Counter::update_pathdist    (streamlines.cc:662-690): every voxel of a kept streamline counted
  *                               once (fdt_paths), per seed point with per_seed (ptx_simple.cc:50-62);
  *   Counter::update_seedcounts  (streamlines.cc:700-748): seeds to targets;
+ *   Counter::update_matrix2_row (streamlines.cc:772-808): --omatrix2;
  *   Tractvolsx::sample          (tractvolsx.h:101-255): probabilistic rounding of the position,
  *                               a random posterior sample, the first fibre (fibst, randfib 1/2)
  *                               and afterwards the fibre closest to the current direction among
@@ -242,8 +243,18 @@ typedef struct {
  * *flags accumulates the waypoint masks passed (over both halves of a particle); returns the
  * reject flag: 1 (entered the avoid mask, passed no waypoint, or shorter than distthresh), 2 (passed
  * some waypoints but not all), 0 */
+/* --omatrix2: the tract-space voxel of a path position (vox_to_vox with the identity, then
+ * MISCMATHS::round), or -1 off the tract-space grid */
+static int64_t lr_voxel(const bpx_track_volume* v, float x, float y, float z) {
+  /* vox_to_vox works in double (NEWMAT) and the result is rounded to float before MISCMATHS::round */
+  const int lx = rnd((float)(((double)x * v->dx) / v->lr_dx)), ly = rnd((float)(((double)y * v->dy) / v->lr_dy)),
+            lz = rnd((float)(((double)z * v->dz) / v->lr_dz));
+  if (lx < 0 || ly < 0 || lz < 0 || lx >= v->lr_nx || ly >= v->lr_ny || lz >= v->lr_nz) return -1;
+  return ((int64_t)lz * v->lr_ny + ly) * v->lr_nx + lx;
+}
+
 static int half_line(const trk_t* T, part_t* P, uint64_t pid, int h, int fibst0, float x0, float y0, float z0,
-                     int64_t* path, int* npath, uint32_t* flags, loopvol_t* lc) {
+                     int64_t* path, int64_t* lrpath, int* npath, uint32_t* flags, loopvol_t* lc) {
   const bpx_track_options* o = T->o;
   const bpx_track_volume* v = T->v;
   int init_sample = 1, fibst = fibst0, avoided = 0;
@@ -265,6 +276,7 @@ static int half_line(const trk_t* T, part_t* P, uint64_t pid, int h, int fibst0,
     }
     const int64_t vox = ((int64_t)iz * v->ny + iy) * v->nx + ix;
     if (v->waypoints) *flags |= v->waypoints[vox];
+    if (v->m2_ncols > 0) lrpath[*npath] = lr_voxel(v, P->x, P->y, P->z);
     path[(*npath)++] = vox;
     pathlength += o->steplength;
     if (v->avoid && v->avoid[vox] != 0.f) {
@@ -344,14 +356,19 @@ int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nse
 #pragma omp parallel reduction(+ : kept) reduction(| : failed)
   {
     int64_t* path = (int64_t*)malloc(sizeof(int64_t) * (size_t)(2 * half_steps + 2));
+    int64_t* lrpath = (int64_t*)malloc(sizeof(int64_t) * (size_t)(2 * half_steps + 2));
+    const size_t lr_nvox = v->m2_ncols > 0 ? (size_t)v->lr_nx * v->lr_ny * v->lr_nz : 1;
+    int64_t* stamp2 = (int64_t*)malloc(sizeof(int64_t) * lr_nvox); /* beenhere2 */
     int64_t* stamp = (int64_t*)malloc(sizeof(int64_t) * T.nvox);
     /* the coarse grid covers round(x / 5) for x in [-0.5, n - 0.5) */
     loopvol_t lc = {v->nx / 5 + 2, v->ny / 5 + 2, v->nz / 5 + 2, NULL};
     if (o->loopcheck) lc.dir = (float*)calloc(3 * (size_t)lc.nx * lc.ny * lc.nz, sizeof(float));
-    const int ok = path && stamp && (!o->loopcheck || lc.dir);
+    const int ok = path && lrpath && stamp && stamp2 && (!o->loopcheck || lc.dir);
     if (!ok) failed = 1;
-    if (ok)
+    if (ok) {
       for (size_t i = 0; i < T.nvox; ++i) stamp[i] = -1;
+      for (size_t i = 0; i < lr_nvox; ++i) stamp2[i] = -1;
+    }
 #pragma omp for schedule(dynamic, 16)
     for (int64_t q = 0; q < total; ++q) {
       if (!ok) continue;
@@ -372,13 +389,13 @@ int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nse
       memset(&P, 0, sizeof(P));
       int n1 = 0, n2 = 0;
       uint32_t flags = 0; /* waypoints passed, over both halves (Streamliner::reset clears them per particle) */
-      const int rej1 = half_line(&T, &P, pid, 0, fibst, x0, y0, z0, path, &n1, &flags, &lc);
+      const int rej1 = half_line(&T, &P, pid, 0, fibst, x0, y0, z0, path, lrpath, &n1, &flags, &lc);
       if (P.jumped) { /* Particle::restart_reverse */
         P.rx = -P.rxi;
         P.ry = -P.ryi;
         P.rz = -P.rzi;
       }
-      const int rej2 = half_line(&T, &P, pid, 1, fibst, x0, y0, z0, path + n1, &n2, &flags, &lc);
+      const int rej2 = half_line(&T, &P, pid, 1, fibst, x0, y0, z0, path + n1, lrpath + n1, &n2, &flags, &lc);
       /* Seedmanager::run: the first half is kept on flag 0, or on 2 when the second half completes
        * the waypoints; the second half on flag 0 */
       const int fwd = (rej1 == 0 || rej1 == 2) && !(rej2 > 0 && rej1 > 0);
@@ -388,10 +405,23 @@ int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nse
       /* Counter::update_pathdist over the kept halves in order: each distinct voxel adds 1, or
        * with --pd the d-th distinct voxel adds d (int32 sums wrap as the reference's int volume) */
       const int from = fwd ? 0 : n1, to = bwd ? n1 + n2 : n1;
-      uint32_t d = 0, tflags = 0;
+      uint32_t d = 0, d2 = 0, tflags = 0;
       float clen = 0.f; /* path length along the counted path (Counter::update_seedcounts) */
       for (int i = from; i < to; ++i) {
         const int64_t vx = path[i];
+        if (v->m2_ncols > 0 && lrpath[i] >= 0) {
+          /* matrix2: each tract-space voxel once per streamline; column 0 and voxels outside the
+           * mask are not counted (the reference's m_lookup2 test is "!= 0") */
+          const int32_t col = v->m2_lookup[lrpath[i]];
+          if (col > 0 && stamp2[lrpath[i]] != (int64_t)pid) {
+            stamp2[lrpath[i]] = (int64_t)pid;
+            ++d2;
+            const uint32_t add = o->pathdist ? d2 : 1u;
+            uint32_t* m2 = (uint32_t*)v->matrix2;
+#pragma omp atomic
+            m2[(size_t)s * v->m2_ncols + col] += add;
+          }
+        }
         if (v->ntargets > 0) {
           /* seeds to targets: each target once per streamline, at its first entry, if the path is by
            * then at least distthresh long */
@@ -418,7 +448,9 @@ int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nse
       }
     }
     free(path);
+    free(lrpath);
     free(stamp);
+    free(stamp2);
     free(lc.dir);
   }
   if (failed) return 1;

@@ -170,6 +170,26 @@ def test_probtrack_cli_with_masks_equals_oracle(torch, tmp_path):
         at = vol[pts[:, 0].astype(int), pts[:, 1].astype(int), pts[:, 2].astype(int)]
         assert np.array_equal(at, want_s[t]) and vol.sum() == want_s[t].sum(), name
     assert want_s.sum() > 0
+    # --omatrix2 --lrmask: a tract-space mask of 2 mm voxels (the directory's voxels are 1 mm)
+    lr = np.zeros((5, 8, 10), np.float32)
+    lr[1:4, 2:6, 1:9] = 1.0
+    lr_x = np.transpose(lr, (2, 1, 0))
+    nifti.write(os.path.join(d, "lr.nii.gz"), lr_x, like=nifti.Header(dim=lr_x.shape, pixdim=(1.0, 2.0, 2.0, 2.0) + (1.0,) * 4))
+    out = os.path.join(d, "matrix2")
+    probtrack.main([d, "--seeds", os.path.join(d, "seedmask.nii.gz"), "--out", out, "--omatrix2", "--lrmask",
+                    os.path.join(d, "lr.nii.gz")] + common)
+    _, lr_hdr = nifti.read(os.path.join(d, "lr.nii.gz"))
+    lr_vs = tuple(float(x) for x in lr_hdr.pixdim[1:4])
+    _, _, want_m2 = O.probtrack(o, th, ph, f, mask, pts, voxel_size=(1.0, 1.0, 1.0), matrix2=(lr, lr_vs), **masks)
+    got, _ = nifti.read(os.path.join(out, "fdt_matrix2.nii.gz"))
+    assert got.shape[:2] == want_m2.shape and np.array_equal(got.reshape(want_m2.shape), want_m2)
+    assert want_m2.sum() > 0
+    lut, _ = nifti.read(os.path.join(out, "lookup_tractspace_fdt_matrix2.nii.gz"))
+    tc, _ = nifti.read(os.path.join(out, "tract_space_coords_for_fdt_matrix2.nii.gz"))
+    tc = tc.reshape(-1, 3)
+    assert tc.shape[0] == want_m2.shape[1] and np.array_equal(lut[tc[:, 0], tc[:, 1], tc[:, 2]], np.arange(tc.shape[0]))
+    sc, _ = nifti.read(os.path.join(out, "coords_for_fdt_matrix2.nii.gz"))
+    assert np.array_equal(sc.reshape(-1, 3), pts.astype(int))
 
 
 @pytest.mark.parametrize("kw", [dict(), dict(distthresh=6.0), dict(modeuler=1, per_seed=1)], ids=["plain", "distthresh",
@@ -187,6 +207,42 @@ def test_seeds_to_targets_equal_oracle(torch, kw):
     torch.cuda.synchronize()
     assert got_w == want_w and np.array_equal(got_p.cpu().numpy(), want_p)
     assert np.array_equal(got_s, want_s) and want_s.sum() > 0, (got_s, want_s)
+
+
+M2_CASES = [
+    ("plain", dict()),
+    ("pathdist", dict(pathdist=1)),
+    ("masks_distthresh", dict(masks=("avoid", "stop", "waypoints"), distthresh=3.0)),
+    ("modeuler_loopcheck_per_seed", dict(modeuler=1, loopcheck=1, per_seed=1)),
+    ("with_targets", dict(targets=True, randfib=2)),
+]
+
+
+@pytest.mark.parametrize("name,kw", M2_CASES, ids=[c[0] for c in M2_CASES])
+def test_matrix2_equals_oracle(torch, name, kw):
+    """--omatrix2 on a tract-space grid of 3 mm voxels over a field of 2 x 2 x 2.5 mm voxels (the
+    tract-space voxel changes inside diffusion voxels), a mask of about 70% of it."""
+    from fdt_b200 import lib
+
+    lib.load()
+    th, ph, f, mask = synth.fibre_field((20, 16, 10), nsamples=12, seed=4)
+    seeds = np.array([[5.0, 8.0, 5.0], [14.0, 7.0, 4.6], [10.3, 3.2, 5.5]], np.float32)
+    lr = (np.random.default_rng(3).random((9, 11, 14)) < 0.7).astype(np.float32)
+    kw = dict(kw)
+    extra = _masks(mask, kw.pop("masks", ()))
+    if kw.pop("targets", False):
+        extra["targets"] = _masks(mask, ("waypoints",))["waypoints"]
+    o = TrackOptions.make(nparticles=200, nsteps=300, seed=41, **kw)
+    m2 = (lr, (3.0, 3.0, 3.0))
+    want = O.probtrack(o, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.5), matrix2=m2, **extra)
+    dev = [lib.to_device(a) for a in (th, ph, f, mask)]
+    dextra = {k: (lib.to_device(v) if k in ("avoid", "stop") else v) for k, v in extra.items()}
+    got = lib.probtrack(o, *dev, seeds, voxel_size=(2.0, 2.0, 2.5), matrix2=m2, **dextra)
+    torch.cuda.synchronize()
+    assert got[1] == want[1] and np.array_equal(got[0].cpu().numpy(), want[0])
+    for g, w in zip(got[2:], want[2:]):
+        assert np.array_equal(g, w), (name, np.argwhere(g != w)[:5])
+    assert want[-1].sum() > 0 and want[-1].shape == (3, int(lr.sum()))
 
 
 @pytest.mark.parametrize("modeuler", [0, 1])

@@ -5,7 +5,8 @@ every voxel on it is counted once per streamline; the curvature threshold stops 
 right-angle turn; the distance threshold drops short streamlines; the avoid, stop and waypoint
 masks reject, end and select halves as Seedmanager::run and Streamliner::streamline do; --pd
 weights voxels by their order on the path; --loopcheck stops paths that circle back on themselves;
---modeuler follows a straight tract as the plain steps do."""
+--modeuler follows a straight tract as the plain steps do; --omatrix2 counts every tract-space voxel
+once per streamline (column 0 never, as the reference's "column != 0" test has it)."""
 import os
 import re
 
@@ -173,6 +174,44 @@ def _plane(mask, x):
     m = np.zeros_like(mask)
     m[:, :, x] = 1.0
     return m
+
+
+def test_matrix2_on_the_diffusion_grid_is_the_per_seed_path_counts_inside_the_mask():
+    # with the tract space equal to the diffusion grid every path position maps to its own voxel, so
+    # a seed's matrix2 row is its path distribution read at the tract-space mask's voxels (z, y, x
+    # order), column 0 excepted
+    th, ph, f, mask = synth.fibre_field((16, 14, 8), nsamples=8, seed=2)
+    seeds = [[4.0, 7.0, 4.0], [11.0, 6.0, 3.5], [8.0, 8.0, 4.0]]
+    o = TrackOptions.make(nparticles=40, nsteps=200, seed=13, per_seed=1)
+    lr = mask.copy()
+    each, way, m2 = O.probtrack(o, th, ph, f, mask, seeds, matrix2=(lr, (2.0, 2.0, 2.0)))
+    want = each[:, lr != 0]
+    want[:, 0] = 0
+    assert m2.shape == (3, int((lr != 0).sum())) and m2.dtype == np.int32
+    assert np.array_equal(m2, want) and m2.sum() > 0
+    # a tract-space mask of part of the grid keeps only its own columns
+    lr2 = np.zeros_like(mask)
+    lr2[:, 4:10, :] = mask[:, 4:10, :]
+    _, _, m2b = O.probtrack(o, th, ph, f, mask, seeds, matrix2=(lr2, (2.0, 2.0, 2.0)))
+    want = each[:, lr2 != 0]
+    want[:, 0] = 0
+    assert np.array_equal(m2b, want)
+
+
+def test_matrix2_on_a_coarser_grid_counts_each_tract_space_voxel_once_per_streamline():
+    th, ph, f, mask = _straight_box()  # 30 x 9 x 9 voxels of 2 mm, the tract along x at y = z = 4
+    # tract space of 4 mm voxels: positions 2.5 <= x < 26.5 map to x_lr = round(x / 2) = 1 .. 13 at
+    # y_lr = z_lr = 2; the mask holds x_lr = 1 .. 14 there, so x_lr = 1 is column 0 and never counted
+    lr = np.zeros((5, 5, 15), np.float32)
+    lr[2, 2, 1:15] = 1.0
+    o = TrackOptions.make(nparticles=50, nsteps=400, seed=3)
+    paths, way, m2 = O.probtrack(o, th, ph, f, mask, [[15.0, 4.0, 4.0]], matrix2=(lr, (4.0, 4.0, 4.0)))
+    assert way == 50 and m2.shape == (1, 14)
+    assert m2[0, 0] == 0 and np.all(m2[0, 1:13] == 50) and m2[0, 13] == 0
+    # --pd: the d-th tract-space voxel counted on a streamline adds d (12 counted columns)
+    o.pathdist = 1
+    _, _, m2 = O.probtrack(o, th, ph, f, mask, [[15.0, 4.0, 4.0]], matrix2=(lr, (4.0, 4.0, 4.0)))
+    assert m2.sum() == 50 * (12 * 13 // 2) and m2[0, 0] == 0
 
 
 def test_avoid_mask_rejects_the_half_that_enters_it():
