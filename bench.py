@@ -512,10 +512,39 @@ def run_probtrack(args):
     inside = np.argwhere(mask > 0)  # [z, y, x]
     pick = inside[rng.choice(len(inside), args.track_seeds, replace=False)]
     seeds = np.ascontiguousarray(pick[:, ::-1].astype(np.float32))
-    o = TrackOptions.make(seed=9)
+    # --track-options: loopcheck, modeuler (options), targets (3 target planes across the x-running
+    # tracts, seeds to targets), matrix2 (a tract space of 4 mm voxels over the whole grid)
+    topts = [t for t in args.track_options.split(",") if t]
+    for t in topts:
+        if t not in ("loopcheck", "modeuler", "targets", "matrix2"):
+            raise SystemExit(f"--track-options: unknown option {t}")
+    o = TrackOptions.make(seed=9, loopcheck=int("loopcheck" in topts), modeuler=int("modeuler" in topts))
+    extra = {}
+    if "targets" in topts:
+        planes = []
+        for x in (20, 48, 70):
+            pl = np.zeros_like(mask)
+            pl[:, :, x] = 1.0
+            planes.append(pl)
+        extra["targets"] = planes
+    if "matrix2" in topts:
+        extra["matrix2"] = (np.ones((30, 48, 48), np.float32), (4.0, 4.0, 4.0))
     dev = [lib.to_device(a) for a in (th, ph, f, mask)]
     sd = lib.to_device(seeds)
     v = lib.track_volume(*dev)
+    outs = []  # per-option outputs, zeroed every step
+    if "targets" in topts:
+        tb = torch.from_numpy(lib.waypoint_bits(extra["targets"])).cuda()
+        s2t = torch.zeros((3, len(seeds)), device="cuda", dtype=torch.int32)
+        v.ntargets, v.targets, v.seeds_to_targets = 3, tb.data_ptr(), s2t.data_ptr()
+        outs.append(s2t)
+    if "matrix2" in topts:
+        lut = torch.from_numpy(lib.matrix2_lookup(extra["matrix2"][0])).cuda()
+        m2 = torch.zeros((len(seeds), int(lut.numel())), device="cuda", dtype=torch.int32)
+        v.m2_ncols, v.lr_nx, v.lr_ny, v.lr_nz = int(lut.numel()), 48, 48, 30
+        v.lr_dx = v.lr_dy = v.lr_dz = 4.0
+        v.m2_lookup, v.matrix2 = lut.data_ptr(), m2.data_ptr()
+        outs.append(m2)
     paths = torch.zeros(mask.shape, device="cuda", dtype=torch.int32)
     way = torch.zeros(1, device="cuda", dtype=torch.int64)
     L = lib.load()
@@ -526,6 +555,8 @@ def run_probtrack(args):
     def step():
         paths.zero_()
         way.zero_()
+        for t in outs:
+            t.zero_()
         lib._check(L.bpx_probtrack_dev(C.byref(o), C.byref(v), len(seeds), sd.data_ptr(), paths.data_ptr(),
                                        way.data_ptr(), C.c_void_p(stream.cuda_stream)), "probtrack")
 
@@ -547,9 +578,9 @@ def run_probtrack(args):
     # the CPU oracle on all host threads (OpenMP over particles), 4 seed points per thread
     cores = os.cpu_count() or 1
     nb = min(len(seeds), 4 * cores)
-    o_cpu = TrackOptions.make(seed=9)
+    o_cpu = TrackOptions.make(seed=9, loopcheck=o.loopcheck, modeuler=o.modeuler)
     t0 = time.perf_counter()
-    O.probtrack(o_cpu, th, ph, f, mask, seeds[:nb])
+    O.probtrack(o_cpu, th, ph, f, mask, seeds[:nb], **extra)
     t_cpu = time.perf_counter() - t0
     line = {
         "metric": "streamlines/s, probtrackx on bedpostx samples (1 B200)", "value": n_lines / t,
@@ -557,7 +588,8 @@ def run_probtrack(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
         "config": {"workload": "probtrackx (one path distribution over all seeds, as seedmask mode): 96x96x60 "
                    "crossing-fibre field, 3 fibres x 50 samples, "
-                   "%d seeds x 5000 particles, 2000 steps of 0.5 mm, cthr 0.2, fibthresh 0.01" % len(seeds),
+                   "%d seeds x 5000 particles, 2000 steps of 0.5 mm, cthr 0.2, fibthresh 0.01" % len(seeds)
+                   + "".join(", " + t for t in topts),
                    "streamlines": n_lines, "waytotal": int(way.item()), "visits": int(paths.sum(dtype=torch.int64).item())},
         "cpu_baseline": {"value": nb * o.nparticles / t_cpu, "unit": "streamlines/s", "cores": cores, "kind": "port",
                          "sample": f"{nb} seed points x {o.nparticles} particles through the CPU oracle, "
@@ -599,6 +631,8 @@ def main():
                     help="batched: voxel-count scale (also the C2 sub-record of the default line)")
     ap.add_argument("--no-c2", action="store_true", help="skip the C2 (mixed batch) sub-record")
     ap.add_argument("--track-seeds", type=int, default=1024, help="probtrack: seed points")
+    ap.add_argument("--track-options", default="",
+                    help="probtrack: comma list of loopcheck, modeuler, targets, matrix2 (default: none)")
     ap.add_argument("--no-whole-volume", action="store_true",
                     help="skip the one-call run of the ~900k-voxel whole-brain volume")
     ap.add_argument("--acc-voxels", type=int, default=4096, help="accuracy study: voxels")

@@ -21,6 +21,7 @@
 // file is compiled with -fmad=false), sine and cosine from sincos_fast; random numbers from
 // Philox-4x32-10 keyed by the seed, counted by (particle, half, step), eight uniforms per step.
 // The CPU oracle (oracle/track_oracle.c) does the same operations and follows identical paths.
+#include <cmath>
 #include <cstdint>
 #include <string>
 
@@ -36,9 +37,15 @@ constexpr int kTrackThreads = 64;
 // (no spills); measured on 1024 seeds x 5000 particles, 8 / 10 / 12 / 16 blocks per SM took
 // 93.7 / 81.9 / 75.1 / 67.6 ms
 constexpr int kTrackBlocksPerSm = 16;
-// the extended form (--modeuler, --loopcheck, seeds to targets) carries more state: 12 blocks,
-// 85 registers
-constexpr int kTrackBlocksPerSmExt = 12;
+
+// The options that carry state of their own compile into instantiations of the kernel of their
+// own (a feature set), so each spills only what it must at the same launch bound: the plain form
+// none (62 registers).  Measured on 1024 seeds x 5000 particles, 8 / 12 / 16 blocks per SM: 120 /
+// 96 / 86 ms with --modeuler, 102 / 75 / 64 ms with --loopcheck, 86 / 64 / 57 ms with 3 targets,
+// 255 / 219 / 204 ms with all of them and matrix2 (14 blocks: 204 ms).
+constexpr int kFeatEuler = 1;  // --modeuler
+constexpr int kFeatLoop = 2;   // --loopcheck
+constexpr int kFeatCount = 4;  // seeds to targets, matrix2
 
 struct TrackArgs {
   bpx_track_options o;
@@ -62,6 +69,7 @@ struct TrackArgs {
   int lc_log2n;
   int lcnx, lcny;
   float sx, sy, sz;  // steplength / dx, dy, dz
+  float lrx, lry, lrz;  // matrix2: dx / lr_dx, dy / lr_dy, dz / lr_dz
   uint64_t pid_begin;  // particles [pid_begin, pid_end) of this launch
   uint64_t pid_end;
 };
@@ -161,6 +169,30 @@ struct Counted {
 // --omatrix2's tract-space voxel keys share the visit table with the diffusion voxels
 constexpr uint32_t kLrKey = 0x80000000u;
 
+// Rounding of a quotient without the division: q, a float product within 3e-7 |q| of the exact
+// quotient, decides floor(quotient + 1/2) wherever it lies farther than 1e-5 (|q| + 1) from a
+// rounding boundary k + 1/2 (the quotient, and its correctly rounded float, then lie on the same
+// side of it); returns false where it does not, and the caller forms the quotient itself.
+__device__ __forceinline__ bool round_clear(float q, int& r) {
+  r = (int)floorf(q + 0.5f);
+  return fabsf((q - floorf(q)) - 0.5f) > 1e-5f * (fabsf(q) + 1.0f);
+}
+
+// --omatrix2's tract-space coordinate: round(float(x * d / lr_d)) as the reference forms it
+// (vox_to_vox in double, the result rounded to float, then MISCMATHS::round); ratio = d / lr_d
+__device__ __forceinline__ int lr_round(float x, float d, float lr_d, float ratio) {
+  int r;
+  if (round_clear(x * ratio, r)) return r;
+  return rnd((float)(((double)x * (double)d) / (double)lr_d));
+}
+
+// --loopcheck's coarse coordinate round(x / 5)
+__device__ __forceinline__ int lc_round(float x) {
+  int r;
+  if (round_clear(x * 0.2f, r)) return r;
+  return rnd(x / 5.0f);
+}
+
 struct Tracker {
   const TrackArgs& a;
   uint2* tab;
@@ -170,26 +202,34 @@ struct Tracker {
   float4* lcd;
   uint32_t lc_stamp;  // one per tracked half (the tables are cleared per launch)
 
-  // --loopcheck: the direction last stored in coarse cell `cell` this half (zero if none), which
-  // is then replaced by d
-  __device__ float3 loop_swap(uint32_t cell, float3 d) const {
+  // --loopcheck: the direction stored for coarse cell `cell` this half (zero if none)
+  __device__ float3 loop_get(uint32_t cell) const {
     const uint32_t mask = (1u << a.lc_log2n) - 1u;
     uint32_t h = (cell * 2654435761u) >> (32 - a.lc_log2n);
     for (uint32_t probe = 0; probe <= mask; ++probe) {
       const uint2 e = lck[h];
-      if (e.y != lc_stamp) {
-        lck[h] = make_uint2(cell, lc_stamp);
-        lcd[h] = make_float4(d.x, d.y, d.z, 0.f);
-        return make_float3(0.f, 0.f, 0.f);
-      }
+      if (e.y != lc_stamp) break;  // an empty entry ends the probe sequence: not stored
       if (e.x == cell) {
         const float4 o = lcd[h];
-        lcd[h] = make_float4(d.x, d.y, d.z, 0.f);
         return make_float3(o.x, o.y, o.z);
       }
       h = (h + 1u) & mask;
     }
-    return make_float3(0.f, 0.f, 0.f);  // unreachable: the table holds twice the cells of a half
+    return make_float3(0.f, 0.f, 0.f);
+  }
+  // --loopcheck: stores d as the direction of coarse cell `cell` this half
+  __device__ void loop_put(uint32_t cell, float3 d) const {
+    const uint32_t mask = (1u << a.lc_log2n) - 1u;
+    uint32_t h = (cell * 2654435761u) >> (32 - a.lc_log2n);
+    for (uint32_t probe = 0; probe <= mask; ++probe) {
+      const uint2 e = lck[h];
+      if (e.y != lc_stamp || e.x == cell) {
+        lck[h] = make_uint2(cell, lc_stamp);
+        lcd[h] = make_float4(d.x, d.y, d.z, 0.f);
+        return;
+      }
+      h = (h + 1u) & mask;
+    }  // unreachable: the table holds twice the cells of a half
   }
 
   // the sample record of voxel `svox`, sample `samp`: every fibre's direction and f, and the
@@ -327,9 +367,8 @@ struct Tracker {
   // accumulates the waypoint masks passed (over both halves of a particle).  Returns the reject
   // flag: 1 (entered the avoid mask, passed no waypoint, or shorter than distthresh), 2 (passed
   // some waypoints but not all), 0.
-  // EXT: compiled with --modeuler, --loopcheck, seeds to targets and matrix2 (the plain form keeps its
-  // registers without them)
-  template <bool EXT>
+  // FEAT: the feature set compiled in (kFeatEuler, kFeatLoop, kFeatCount)
+  template <int FEAT>
   __device__ int half_line(Particle& P, uint64_t pid, int h, int fibst0, float x0, float y0, float z0,
                            bool count, uint32_t& flags, int& nvisit, Counted& cnt) {
     const bpx_track_options& o = a.o;
@@ -345,6 +384,11 @@ struct Tracker {
     // already: the visit table is probed only when the voxel changes
     uint32_t last = 0xffffffffu, last_lr = 0xffffffffu;
     ++lc_stamp;  // every tracked half starts with an empty loopcheck volume
+    // --loopcheck: the coarse cell of the step before and the direction stored for it since; the
+    // table is read and written only when the cell changes (about every 20 steps of 0.5 mm in 2 mm
+    // voxels), which stores and finds the same directions as a table access every step
+    uint32_t lc_cell = 0xffffffffu;
+    float3 lc_dir = make_float3(0.f, 0.f, 0.f);
     for (int it = 1; it <= o.nsteps / 2; ++it) {
       const int ix = rnd(P.x), iy = rnd(P.y), iz = rnd(P.z);
       // this step's uniforms and sampled voxel, then the masks at the position and every fibre's
@@ -365,26 +409,48 @@ struct Tracker {
       const uint32_t vox = in_grid ? (uint32_t)(((size_t)iz * v.ny + iy) * v.nx + ix) : 0u;
       const float m = __ldg(v.mask + vox);
       const uint32_t way = v.waypoints ? __ldg(v.waypoints + vox) : 0u;
+      // what the counting below reads, in the same round: the target bits of a new voxel, the
+      // matrix2 column of a new tract-space voxel (lr: its index, or ~0 off the tract-space grid)
+      uint32_t tgt = 0u, lr = 0xffffffffu;
+      int col = 0;
+      if ((FEAT & kFeatCount) && count) {
+        if (v.ntargets > 0 && vox != last) tgt = __ldg(v.targets + vox);
+        if (v.m2_ncols > 0) {
+          const int lx = lr_round(P.x, v.dx, v.lr_dx, a.lrx);
+          const int ly = lr_round(P.y, v.dy, v.lr_dy, a.lry);
+          const int lz = lr_round(P.z, v.dz, v.lr_dz, a.lrz);
+          if (lx >= 0 && ly >= 0 && lz >= 0 && lx < v.lr_nx && ly < v.lr_ny && lz < v.lr_nz) {
+            lr = ((uint32_t)lz * (uint32_t)v.lr_ny + (uint32_t)ly) * (uint32_t)v.lr_nx + (uint32_t)lx;
+            if (lr != last_lr) col = __ldg(v.m2_lookup + lr);
+          }
+        }
+      }
       const bool avoid = v.avoid && __ldg(v.avoid + vox) != 0.f;
       const bool stop = v.stop && __ldg(v.stop + vox) != 0.f;
       Sample S;
       load_record(svox, samp, S);
       if (!(in_grid && m > 0.f)) break;  // the reference's remaining steps change nothing
-      if (EXT && o.loopcheck) {
+      if ((FEAT & kFeatLoop) && o.loopcheck) {
         // stop where the path runs against the direction it last had in this coarse cell
-        const int lx = rnd(P.x / 5.0f), ly = rnd(P.y / 5.0f), lz = rnd(P.z / 5.0f);
+        const int lx = lc_round(P.x), ly = lc_round(P.y), lz = lc_round(P.z);
         const uint32_t cell = ((uint32_t)lz * (uint32_t)a.lcny + (uint32_t)ly) * (uint32_t)a.lcnx + (uint32_t)lx;
-        const float3 old = loop_swap(cell, make_float3(P.rx, P.ry, P.rz));
+        float3 old = lc_dir;
+        if (cell != lc_cell) {
+          if (lc_cell != 0xffffffffu) loop_put(lc_cell, lc_dir);
+          old = loop_get(cell);
+          lc_cell = cell;
+        }
         if (P.rx * old.x + P.ry * old.y + P.rz * old.z < 0.f) break;
+        lc_dir = make_float3(P.rx, P.ry, P.rz);
       }
       flags |= way;
       if (count && vox != last) {
         last = vox;
         if (first_visit(vox)) atomicAdd(paths + vox, o.pathdist ? ++nvisit : 1);
-        if (EXT && v.ntargets > 0) {
+        if ((FEAT & kFeatCount) && v.ntargets > 0) {
           // a target is counted at its first entry on the counted path (a voxel change), if the path
           // is by then at least distthresh long (Counter::update_seedcounts)
-          const uint32_t tb = __ldg(v.targets + vox) & ~cnt.tflags;
+          const uint32_t tb = tgt & ~cnt.tflags;
           if (tb) {
             if (cnt.length >= o.distthresh)
               for (uint32_t b = tb; b; b &= b - 1) atomicAdd(v.seeds_to_targets + (size_t)(__ffs(b) - 1) * a.nseeds + cnt.seed, 1);
@@ -392,24 +458,14 @@ struct Tracker {
           }
         }
       }
-      if (EXT && count && v.m2_ncols > 0) {
-        // --omatrix2: the tract-space voxel of the position (vox_to_vox in double, rounded to float,
-        // then MISCMATHS::round), counted once per particle when its column is not 0
-        // (Counter::update_matrix2_row); it can change inside a diffusion voxel
-        const int lx = rnd((float)(((double)P.x * (double)v.dx) / (double)v.lr_dx));
-        const int ly = rnd((float)(((double)P.y * (double)v.dy) / (double)v.lr_dy));
-        const int lz = rnd((float)(((double)P.z * (double)v.dz) / (double)v.lr_dz));
-        if (lx >= 0 && ly >= 0 && lz >= 0 && lx < v.lr_nx && ly < v.lr_ny && lz < v.lr_nz) {
-          const uint32_t lr = ((uint32_t)lz * (uint32_t)v.lr_ny + (uint32_t)ly) * (uint32_t)v.lr_nx + (uint32_t)lx;
-          if (lr != last_lr) {
-            last_lr = lr;
-            const int col = __ldg(v.m2_lookup + lr);
-            if (col > 0 && first_visit(lr | kLrKey))
-              atomicAdd(v.matrix2 + (size_t)cnt.seed * v.m2_ncols + col, o.pathdist ? ++cnt.nvisit2 : 1);
-          }
-        }
+      if ((FEAT & kFeatCount) && count && lr != 0xffffffffu && lr != last_lr) {
+        // --omatrix2: the tract-space voxel of the position, counted once per particle when its
+        // column is not 0 (Counter::update_matrix2_row); it can change inside a diffusion voxel
+        last_lr = lr;
+        if (col > 0 && first_visit(lr | kLrKey))
+          atomicAdd(v.matrix2 + (size_t)cnt.seed * v.m2_ncols + col, o.pathdist ? ++cnt.nvisit2 : 1);
       }
-      if (EXT && count) cnt.length += o.steplength;
+      if ((FEAT & kFeatCount) && count) cnt.length += o.steplength;
       pathlength += o.steplength;
       if (avoid) {
         avoided = true;
@@ -424,7 +480,7 @@ struct Tracker {
         const float rxn = rn.x, ryn = rn.y, rzn = rn.z;
         if (P.jumped && !(fabsf(rxn * P.rx + ryn * P.ry + rzn * P.rz) > o.c_thr)) break;
         if (moves) {
-          if (!EXT || !o.modeuler) {
+          if (!(FEAT & kFeatEuler) || !o.modeuler) {
             jump_dir(P, a, rxn, ryn, rzn, u[6]);
           } else {
             // Particle::testjump, a sample there, and the jump along the mean of both directions
@@ -472,8 +528,8 @@ struct Tracker {
   }
 };
 
-template <bool EXT>
-__global__ void __launch_bounds__(kTrackThreads, EXT ? kTrackBlocksPerSmExt : kTrackBlocksPerSm) track_kernel(TrackArgs a) {
+template <int FEAT>
+__global__ void __launch_bounds__(kTrackThreads, kTrackBlocksPerSm) track_kernel(TrackArgs a) {
   const uint64_t threads = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   Tracker T{a, a.tables + (t << a.log2n), 0u, a.paths, nullptr, nullptr, 0u};
@@ -507,25 +563,25 @@ __global__ void __launch_bounds__(kTrackThreads, EXT ? kTrackBlocksPerSmExt : kT
     Counted cnt{0.f, 0u, s, 0};
     if (decide) {  // whether a half counts is known only once both halves have ended: track, then count
       const Particle P0 = P;
-      const int rej1 = T.template half_line<EXT>(P, pid, 0, fibst, x0, y0, z0, false, flags, nvisit, cnt);
+      const int rej1 = T.template half_line<FEAT>(P, pid, 0, fibst, x0, y0, z0, false, flags, nvisit, cnt);
       reverse(P);
       const Particle P1 = P;
-      const int rej2 = T.template half_line<EXT>(P, pid, 1, fibst, x0, y0, z0, false, flags, nvisit, cnt);
+      const int rej2 = T.template half_line<FEAT>(P, pid, 1, fibst, x0, y0, z0, false, flags, nvisit, cnt);
       const bool fwd = (rej1 == 0 || rej1 == 2) && !(rej2 > 0 && rej1 > 0), bwd = rej2 == 0;
       uint32_t unused = 0;
       if (fwd) {
         Particle Q = P0;
-        T.template half_line<EXT>(Q, pid, 0, fibst, x0, y0, z0, true, unused, nvisit, cnt);
+        T.template half_line<FEAT>(Q, pid, 0, fibst, x0, y0, z0, true, unused, nvisit, cnt);
       }
       if (bwd) {
         Particle Q = P1;
-        T.template half_line<EXT>(Q, pid, 1, fibst, x0, y0, z0, true, unused, nvisit, cnt);
+        T.template half_line<FEAT>(Q, pid, 1, fibst, x0, y0, z0, true, unused, nvisit, cnt);
       }
       if (fwd || bwd) ++kept;
     } else {  // every half is kept: count as it goes
-      T.template half_line<EXT>(P, pid, 0, fibst, x0, y0, z0, true, flags, nvisit, cnt);
+      T.template half_line<FEAT>(P, pid, 0, fibst, x0, y0, z0, true, flags, nvisit, cnt);
       reverse(P);
-      T.template half_line<EXT>(P, pid, 1, fibst, x0, y0, z0, true, flags, nvisit, cnt);
+      T.template half_line<FEAT>(P, pid, 1, fibst, x0, y0, z0, true, flags, nvisit, cnt);
       ++kept;
     }
   }
@@ -651,6 +707,11 @@ bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volu
   a.sx = opts->steplength / vol->dx;
   a.sy = opts->steplength / vol->dy;
   a.sz = opts->steplength / vol->dz;
+  if (vol->m2_ncols > 0) {
+    a.lrx = vol->dx / vol->lr_dx;
+    a.lry = vol->dy / vol->lr_dy;
+    a.lrz = vol->dz / vol->lr_dz;
+  }
   a.nseeds = nseeds;
   a.seeds = seeds;
   a.paths = reinterpret_cast<int*>(paths);
@@ -661,21 +722,28 @@ bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volu
   int log2n = 1;
   while ((1ll << log2n) < 2ll * keys) ++log2n;
   a.log2n = log2n;
-  // --loopcheck: a table of at least twice the coarse cells one half can enter
+  // --loopcheck: a table of at least twice the coarse cells one half can enter.  A half's path is at
+  // most l = (nsteps / 2) * steplength / min(dx, dy, dz) voxels long; cut into pieces of at most 4
+  // voxels, each piece meets at most 8 cells of 5 voxels, so it enters at most 8 (ceil(l / 4) + 1)
   a.lcnx = vol->nx / 5 + 2;
   a.lcny = vol->ny / 5 + 2;
   const long long lc_cells = (long long)a.lcnx * a.lcny * (vol->nz / 5 + 2);
-  const long long lc_max = lc_cells < opts->nsteps / 2 + 1 ? lc_cells : opts->nsteps / 2 + 1;
+  const float dmin = fminf(vol->dx, fminf(vol->dy, vol->dz));
+  const double half_len = (double)(opts->nsteps / 2) * (double)opts->steplength / (double)dmin;
+  const double lc_geom = 8.0 * (std::ceil(half_len / 4.0) + 1.0);
+  long long lc_max = lc_cells < opts->nsteps / 2 + 1 ? lc_cells : opts->nsteps / 2 + 1;
+  if (lc_geom < (double)lc_max) lc_max = (long long)lc_geom;
   int lc_log2n = 1;
   while ((1ll << lc_log2n) < 2 * lc_max) ++lc_log2n;
   a.lc_log2n = lc_log2n;
   const size_t lc_bytes = opts->loopcheck ? ((size_t)1 << lc_log2n) * (sizeof(uint2) + sizeof(float4)) : 0;
   // particles in flight: kTrackBlocksPerSm blocks per SM, fewer when the tables of very long paths
-  // would pass 8 GB
+  // would pass 16 GB
   const size_t table_bytes = ((size_t)1 << log2n) * sizeof(uint2);
-  const size_t max_blocks = ((size_t)8 << 30) / ((table_bytes + lc_bytes) * kTrackThreads);
-  const bool ext = opts->modeuler || opts->loopcheck || vol->ntargets > 0 || vol->m2_ncols > 0;
-  int grid = sm_count() * (ext ? kTrackBlocksPerSmExt : kTrackBlocksPerSm);
+  const size_t max_blocks = ((size_t)16 << 30) / ((table_bytes + lc_bytes) * kTrackThreads);
+  const int feat = (opts->modeuler ? kFeatEuler : 0) | (opts->loopcheck ? kFeatLoop : 0) |
+                   ((vol->ntargets > 0 || vol->m2_ncols > 0) ? kFeatCount : 0);
+  int grid = sm_count() * kTrackBlocksPerSm;
   if ((size_t)grid > max_blocks) grid = max_blocks > 0 ? (int)max_blocks : 1;
   const size_t threads = (size_t)grid * kTrackThreads;
   // workspace: the visit tables, the loopcheck tables (keys, then directions), the repacked samples
@@ -709,10 +777,16 @@ bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volu
     if (e0 != cudaSuccess) return api_cuda_fail(e0, "bpx_probtrack_dev: cudaMemsetAsync");
     a.pid_begin = b;
     a.pid_end = b + chunk < total ? b + chunk : total;
-    if (ext)
-      track_kernel<true><<<grid, kTrackThreads, 0, s>>>(a);
-    else
-      track_kernel<false><<<grid, kTrackThreads, 0, s>>>(a);
+    switch (feat) {
+      case 0: track_kernel<0><<<grid, kTrackThreads, 0, s>>>(a); break;
+      case 1: track_kernel<1><<<grid, kTrackThreads, 0, s>>>(a); break;
+      case 2: track_kernel<2><<<grid, kTrackThreads, 0, s>>>(a); break;
+      case 3: track_kernel<3><<<grid, kTrackThreads, 0, s>>>(a); break;
+      case 4: track_kernel<4><<<grid, kTrackThreads, 0, s>>>(a); break;
+      case 5: track_kernel<5><<<grid, kTrackThreads, 0, s>>>(a); break;
+      case 6: track_kernel<6><<<grid, kTrackThreads, 0, s>>>(a); break;
+      default: track_kernel<7><<<grid, kTrackThreads, 0, s>>>(a); break;
+    }
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return api_cuda_fail(e, "bpx_probtrack_dev: track_kernel");
   }

@@ -516,10 +516,11 @@ void bpx_track_options_default(bpx_track_options* opts);
  * paths [nz][ny][nx], or to its seed's volume of paths [nseeds][nz][ny][nx] with opts->per_seed
  * (int32 counts, fdt_paths: the reference's volume<int> m_prob, wrapping past 2^31 as it does), and
  * the kept streamlines to *waytotal (device int64); the caller zeroes both first.  Integer sums make the result independent of the order in which streamlines finish.
- * Uses workspace memory (see Concurrency): the samples repacked, 16 * ceil(3 * nfib / 4) bytes per
- * voxel and sample, and a visit table of 8 * 2^ceil(log2(2 * (nsteps + 2))) bytes per particle in
- * flight (1024 particles per multiprocessor, fewer if the tables would pass 8 GB: 5 GB on a B200 at
- * nsteps 2000).
+ * Uses workspace memory (see Concurrency): the samples repacked, 16 * (nfib + 1) bytes per voxel
+ * and sample, and per particle in flight a visit table of 8 * 2^ceil(log2(2 * (nsteps + 2))) bytes
+ * (twice that with matrix2) and with loopcheck a coarse-cell table of 24 bytes per entry; 1024
+ * particles in flight per multiprocessor, fewer if the tables would pass 16 GB (5 GB on a B200 at
+ * nsteps 2000 without options).
  */
 bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volume* vol, int32_t nseeds,
                              const float* seeds, int32_t* paths, int64_t* waytotal, void* stream);
