@@ -378,7 +378,7 @@ def run_c3(args):
     mlp_d = torch.from_numpy(mlp_h).cuda()
     n = int(synth.ellipsoid_mask((96, 96, 60), 200_000).sum())
     bv, bl = lib.to_device(prot.bvecs), lib.to_device(prot.bvals)
-    data, _ = lib.synth(2, 3, n, bv, bl, 2, (25.0, 25.0))
+    data, truth_d = lib.synth(2, 3, n, bv, bl, 2, (25.0, 25.0))
     stream = torch.cuda.current_stream()
     outs = {"plain": lib.alloc_outputs(o, n), "learned": lib.alloc_outputs(lo, n)}
 
@@ -403,8 +403,13 @@ def run_c3(args):
         torch.cuda.synchronize()
         t[form] = sum(a.elapsed_time(b) for a, b in e) / 1e3 / k
     ck = clocks.stop()
+    # ground truth of the study's voxels (state rows: S0, d, d_std, R, tau, f0, then th, ph, f per fibre)
+    tr = truth_d[: args.acc_voxels].double().cpu().numpy()
+    th, ph = tr[:, 6::3][:, :3], tr[:, 7::3][:, :3]
+    v = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], -1)
+    truth = synth.Truth(tr[:, 0], tr[:, 1], tr[:, 2], tr[:, 8::3][:, :3], v)
     acc = learned.study_report(learned.posterior_study(o, data[: args.acc_voxels].contiguous(), bv, bl, mlp_d,
-                                                       R=args.acc_chains))
+                                                       R=args.acc_chains), truth)
     line = {
         "metric": "voxels/s, learned-init vs plain MCMC on 1 B200 (config C3)", "value": n / t["learned"],
         "unit": "voxels/s", "n_gpus": 1, "steps": k, "warmup": 1, "ms_per_step": 1e3 * t["learned"],
@@ -708,9 +713,11 @@ def main():
     mlp_d = torch.from_numpy(mlp_h).cuda() if mlp_h is not None else None
     # two distinct chunks per rank, alternated between steps
     chunks_h = []
+    truth0 = None  # ground truth of the first chunk (the accuracy study's voxels)
     for c in range(2):
-        y, _ = synth.make_volume(chunk, prot, 3, True, 25.0, seed=9000 + 17 * rank + c)
+        y, tr = synth.make_volume(chunk, prot, 3, True, 25.0, seed=9000 + 17 * rank + c)
         chunks_h.append(y)
+        truth0 = tr if c == 0 else truth0
     bvecs = lib.to_device(prot.bvecs)
     bvals = lib.to_device(prot.bvals)
     chunks_d = [lib.to_device(y) for y in chunks_h]
@@ -845,10 +852,12 @@ def main():
         d_acc = chunks_d[0][: args.acc_voxels].clone()
         lib.prepare_data(d_acc)
         sets = learned.posterior_study(o, d_acc, bvecs, bvals, mlp_d, R=args.acc_chains)
-        accuracy = learned.study_report(sets)
+        accuracy = learned.study_report(sets, truth0)
         accuracy["se"] = ("Monte-Carlo SE of a posterior mean = sd of the chain means / sqrt(chains); "
                           "|difference| <= 2 sqrt(se_a^2 + se_b^2) counts as agreement")
         accuracy["dyads"] = "median angle between pooled dyads; 'supported' = fibres with mean f >= 0.05 in both"
+        accuracy["truth"] = ("vs_truth: each form's pooled posterior means against the synthetic ground truth, "
+                             "fibres ranked by fraction; dyad angles over fibres with true f >= 0.05")
         del sets
 
     # ---- end to end through the host-buffer public entries (pinned host memory) ----

@@ -101,3 +101,34 @@ def compare(a: ChainSet, b: ChainSet, fmin: float = 0.05) -> dict:
 def replicate(x: np.ndarray, R: int) -> np.ndarray:
     """Stack R copies of per-voxel rows (axis 0): chain r of voxel v becomes row r*nvox + v."""
     return np.ascontiguousarray(np.concatenate([x] * R, axis=0))
+
+
+def truth_errors(s: ChainSet, f_true: np.ndarray, v_true: np.ndarray, d_true: np.ndarray,
+                 fmin: float = 0.05) -> dict:
+    """Errors of a chain set's pooled posterior means against the ground truth of synthetic voxels.
+
+    f_true [nvox][K], v_true [nvox][K][3] (unit vectors), d_true [nvox].  True fibres are ranked by
+    their fraction (largest first), as the finished outputs rank the estimated ones, and compared
+    rank by rank:
+      f_abs_median[k]: median |mean f_k - true f_k|;
+      dyad_deg_median[k]: median angle between the pooled dyad and the true direction of rank k,
+        over voxels whose true f_k >= fmin (a fibre below the post-processing threshold has no
+        direction to recover);
+      d_rel_median: median |mean d - true d| / true d.
+    """
+    p = s.pooled()
+    K = s.K
+    order = np.argsort(-f_true, axis=1, kind="stable")  # [nvox][K]
+    ft = np.take_along_axis(f_true, order, axis=1).T  # [K][nvox]
+    vt = np.take_along_axis(v_true, order[:, :, None], axis=1).transpose(1, 0, 2)  # [K][nvox][3]
+    fe = np.abs(p["f"] - ft)
+    cosang = np.clip(np.abs(np.sum(p["dyad"] * vt, -1)), 0.0, 1.0)
+    ang = np.degrees(np.arccos(cosang))
+    return {
+        "voxels": int(s.nvox),
+        "f_abs_median": [round(float(np.median(fe[k])), 4) for k in range(K)],
+        "dyad_deg_median": [round(float(np.median(ang[k][ft[k] >= fmin])), 3) if np.any(ft[k] >= fmin) else None
+                            for k in range(K)],
+        "dyad_voxels": [int(np.sum(ft[k] >= fmin)) for k in range(K)],
+        "d_rel_median": round(float(np.median(np.abs(p["d"] - d_true) / d_true)), 4),
+    }

@@ -333,8 +333,9 @@ def posterior_study(opts: Options, data, bvecs, bvals, mlp_params, R: int = 8, s
     return sets
 
 
-def study_report(sets: dict) -> dict:
-    """Agreement of each form with the plain chain and with the long (gold) chain."""
+def study_report(sets: dict, truth=None) -> dict:
+    """Agreement of each form with the plain chain and with the long (gold) chain; with the ground
+    truth of synthetic voxels (truth: synth.Truth of the same voxels), each form's errors against it."""
     from . import agreement
 
     rep = {"chains_per_voxel": int(sets["plain"].R), "voxels": int(sets["plain"].nvox),
@@ -343,6 +344,9 @@ def study_report(sets: dict) -> dict:
     if "gold" in sets:
         rep["vs_gold"] = {k: agreement.compare(sets[k], sets["gold"])
                           for k in ("plain", "learned", "learned_frozen", "lm_burnin200") if k in sets}
+    if truth is not None:
+        n = int(sets["plain"].nvox)
+        rep["vs_truth"] = {k: agreement.truth_errors(v, truth.f[:n], truth.v[:n], truth.d[:n]) for k, v in sets.items()}
     return rep
 
 

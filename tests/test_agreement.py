@@ -54,3 +54,22 @@ def test_replicate_orders_chains_by_block():
     x = np.arange(6).reshape(3, 2)
     r = agreement.replicate(x, 2)
     assert r.shape == (6, 2) and np.array_equal(r[3:], x) and np.array_equal(r[:3], x)
+
+
+def test_truth_errors_rank_fibres_and_measure_angles():
+    rng = np.random.default_rng(2)
+    nvox, K, ns, R = 400, 2, 30, 4
+    f_true = np.stack([rng.uniform(0.1, 0.25, nvox), rng.uniform(0.4, 0.6, nvox)])  # second fibre the larger
+    rec = _records(rng, nvox, R, K, ns, f_true)
+    s = agreement.ChainSet(rec, K, R)
+    # true directions: the larger fibre (record fibre 1) at (th, ph) = (0.5, 2.0), the smaller at (0.5, 1.0)
+    d2 = lambda th, ph: np.array([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)])
+    v = np.zeros((nvox, K, 3))
+    v[:, 0], v[:, 1] = d2(0.5, 1.0), d2(0.5, 2.0)
+    e = agreement.truth_errors(s, f_true.T, v, np.full(nvox, 1e-3))
+    assert e["f_abs_median"][0] < 0.01 and e["f_abs_median"][1] < 0.01, e
+    assert e["dyad_deg_median"][0] < 1.0 and e["dyad_deg_median"][1] < 1.0, e
+    assert e["d_rel_median"] < 0.01 and e["dyad_voxels"] == [nvox, nvox]
+    # directions swapped between the ranks: the angle between them (~27 degrees) shows up
+    e2 = agreement.truth_errors(s, f_true.T, v[:, ::-1], np.full(nvox, 1e-3))
+    assert min(e2["dyad_deg_median"]) > 20.0, e2

@@ -33,10 +33,10 @@ def setup(torch):
     params, meta = learned.load_weights(learned.default_weights_path("whole_brain"))
     prot = synth.three_shell(18, 90)
     assert int(meta["ndir"]) == prot.ndir
-    data, _ = synth.make_volume(4096, prot, 3, True, 25.0, seed=777)
+    data, truth = synth.make_volume(4096, prot, 3, True, 25.0, seed=777)
     bv, bl = lib.to_device(prot.bvecs), lib.to_device(prot.bvals)
     base = dict(model=2, nfibres=3, rician=1, f0=1, ardf0=1)
-    return dict(params=params, prot=prot, data=data, bv=bv, bl=bl, base=base)
+    return dict(params=params, prot=prot, data=data, truth=truth, bv=bv, bl=bl, base=base)
 
 
 def test_learned_host_entry_matches_device_entry(torch, setup, monkeypatch):
@@ -77,7 +77,11 @@ def test_learned_form_against_plain_gold_and_the_method_without_the_network(torc
       * the method without the network at the same burn-in (LM start, the reference's widths,
         burn-in 200) against a long chain (burn-in 5000, 12500 jumps): the learned form is about as
         close to it (f1 within 0.08), so what the network buys is time -- the LM fits it replaces
-        (more than 1.8x the voxels/s of the LM start at burn-in 200)."""
+        (more than 1.8x the voxels/s of the LM start at burn-in 200);
+      * against the ground truth of these synthetic voxels (agreement.truth_errors), the learned
+        form's posterior means are at least as accurate as the plain form's and the LM start's at
+        burn-in 200 for the two largest fibres (f error and dyad angle) -- measured on 4096
+        whole-brain voxels: f1 0.0145 vs 0.0164 (plain), first dyad 1.27 vs 1.37 degrees."""
     from fdt_b200 import learned, lib
 
     s = setup
@@ -86,7 +90,7 @@ def test_learned_form_against_plain_gold_and_the_method_without_the_network(torc
     lib.prepare_data(d)
     o = Options.make(**s["base"])
     sets = learned.posterior_study(o, d, s["bv"], s["bl"], s["params"], R=8, seed=300)
-    rep = learned.study_report(sets)
+    rep = learned.study_report(sets, s["truth"])
     yard, acc, lm = (rep["vs_plain"][k] for k in ("plain_other_seed", "learned", "lm_burnin200"))
     print("learned vs plain", acc, "\nplain vs plain", yard, "\nLM burn-in 200 vs plain", lm)
     print("vs gold", rep["vs_gold"])
@@ -97,6 +101,12 @@ def test_learned_form_against_plain_gold_and_the_method_without_the_network(torc
     g = rep["vs_gold"]
     assert g["learned"]["f_within_2se"][0] >= g["lm_burnin200"]["f_within_2se"][0] - 0.08, g
     assert g["learned"]["dyad_median_deg_supported"] < 1.0, g
+    t = rep["vs_truth"]
+    print("vs truth", t)
+    for k in (0, 1):
+        for other in ("plain", "lm_burnin200"):
+            assert t["learned"]["f_abs_median"][k] <= 1.1 * t[other]["f_abs_median"][k], (k, other, t)
+            assert t["learned"]["dyad_deg_median"][k] <= 1.1 * t[other]["dyad_deg_median"][k], (k, other, t)
 
     # speed: the learned pipeline against the LM-started chain at the same burn-in
     lo = Options.make(**s["base"], nburn=200, seed=12)
