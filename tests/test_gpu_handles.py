@@ -91,3 +91,40 @@ def test_unbound_calls_use_the_shared_workspace_after_a_handle_is_unbound(torch)
     assert np.all(np.isfinite(t["mean_f"].cpu().numpy()))
     h.close()
     assert L.bpx_handle_destroy(None) == 0
+
+
+def test_released_shared_workspace_is_made_again_with_the_same_outputs(torch):
+    """bpx_release_workspace frees the device's shared workspaces; the next call allocates them
+    again and gives the same outputs bit for bit."""
+    from fdt_b200 import lib
+
+    L = lib.load()
+    o = Options.make(model=2, nfibres=3, rician=1, f0=1, ardf0=1, nburn=20, njumps=40, sampleevery=8)
+    prot = synth.three_shell(18, 90)
+    y, _ = synth.make_volume(257, prot, 3, True, 25.0, seed=91)
+    bv, bl = lib.to_device(prot.bvecs), lib.to_device(prot.bvals)
+    first = lib.xfibres_dev(o, lib.to_device(y), bv, bl)
+    torch.cuda.synchronize()
+    assert L.bpx_release_workspace() == 0, L.bpx_last_error()
+    assert L.bpx_release_workspace() == 0  # nothing left to free: still fine
+    again = lib.xfibres_dev(o, lib.to_device(y), bv, bl)
+    torch.cuda.synchronize()
+    for k in first:
+        assert torch.equal(first[k], again[k]), k
+
+
+def test_measure_pipes_reports_plausible_issue_rates(torch):
+    """bpx_measure_pipes (the roofline denominators of the bench): MUFU ex2 and FP32 FMA rates are
+    positive, the FMA rate well above the MUFU rate, and both below 2x the B200's nominal figures
+    (148 SMs x 16 MUFU lanes and 128 FMA lanes per clock at up to 1.965 GHz)."""
+    import ctypes as C
+
+    from fdt_b200 import lib
+
+    L = lib.load()
+    m, f = C.c_double(), C.c_double()
+    assert L.bpx_measure_pipes(C.byref(m), C.byref(f)) == 0, L.bpx_last_error()
+    nominal_mufu, nominal_fma = 148 * 16 * 1.965e9, 148 * 128 * 1.965e9
+    assert 0.2 * nominal_mufu < m.value < 2 * nominal_mufu, m.value
+    assert 0.2 * nominal_fma < f.value < 2 * nominal_fma, f.value
+    assert f.value > 4 * m.value
