@@ -69,9 +69,14 @@ class TrainingSet:
 MEAN_LABEL_SAMPLES = 10
 
 
-def label_options(opts: Options, samples: int = 1) -> Options:
-    """Options of the labelling chain: the plain chain's burn-in, then `samples` recorded samples."""
+def label_options(opts: Options, samples: int = 1, burnin: int | None = None, every: int | None = None) -> Options:
+    """Options of the labelling chain: the plain chain's burn-in (or `burnin` iterations), then
+    `samples` samples recorded every sampleevery (or `every`) iterations."""
     o = Options.make(**{f: getattr(opts, f) for f, _ in Options._fields_ if f != "reserved"})
+    if burnin is not None:
+        o.nburn = burnin
+    if every is not None:
+        o.sampleevery = every
     o.njumps = o.sampleevery * samples
     return o
 
@@ -115,14 +120,16 @@ def state_from_record(opts: Options, rec, sample: int = 0):
 
 def make_training_set(opts: Options, bvecs: np.ndarray, bvals: np.ndarray, n: int, seed: int = 1,
                       snr=(10.0, 40.0), chunk: int = 131072, widths: bool = True,
-                      state_labels: str = "mean", label_samples: int = MEAN_LABEL_SAMPLES) -> TrainingSet:
+                      state_labels: str = "mean", label_samples: int = MEAN_LABEL_SAMPLES,
+                      label_burnin: int | None = None, label_every: int | None = None) -> TrainingSet:
     """n forward-model voxels (SNR ~ U(snr)) with their labels.  The plain chain is run from each
     voxel's LM fit through its full burn-in; its proposal widths at that point are the width
     labels, and the state labels are either that chain state (state_labels="chain": the state the
     LM-initialised chain reaches, which is where a chain with frozen widths must start), the
     posterior mean over `label_samples` samples recorded after the burn-in ("mean"; with the plain
     chain's 50 samples, the plain form's own posterior means; widths then
-    taken at the end of that recording) or the LM fit itself ("lm")."""
+    taken at the end of that recording) or the LM fit itself ("lm").  label_burnin / label_every
+    replace the labelling chain's burn-in and sample spacing (default: the plain chain's)."""
     import torch
 
     L = lib.load()
@@ -131,7 +138,7 @@ def make_training_set(opts: Options, bvecs: np.ndarray, bvals: np.ndarray, n: in
     x = torch.empty((n, nin(ndir)), device="cuda", dtype=torch.bfloat16)
     t = torch.empty((n, NOUT), device="cuda", dtype=torch.float32)
     w = torch.empty((n, NOUT), device="cuda", dtype=torch.float32)
-    lo = label_options(opts, label_samples if state_labels == "mean" else 1)
+    lo = label_options(opts, label_samples if state_labels == "mean" else 1, label_burnin, label_every)
     stream = lib._stream(torch)
     for s in range(0, n, chunk):
         m = min(chunk, n - s)
@@ -393,6 +400,10 @@ def main(argv=None) -> None:
     ap.add_argument("--labels", default="mean", choices=["chain", "mean", "lm"])
     ap.add_argument("--label-samples", type=int, default=MEAN_LABEL_SAMPLES,
                     help="--labels mean: samples (every sampleevery iterations) the labels average")
+    ap.add_argument("--label-burnin", type=int, default=None,
+                    help="burn-in of the labelling chain (default: the plain chain's)")
+    ap.add_argument("--label-every", type=int, default=None,
+                    help="sample spacing of the labelling chain (default: the plain chain's)")
     ap.add_argument("--weights", default=None, help="evaluate these weights instead of training")
     a = ap.parse_args(argv)
     prot = PROTOCOLS[a.protocol](synth)
@@ -403,7 +414,8 @@ def main(argv=None) -> None:
     else:
         t0 = time.time()
         ts = make_training_set(opts, prot.bvecs, prot.bvals, a.n, seed=a.seed, state_labels=a.labels,
-                               label_samples=a.label_samples)
+                               label_samples=a.label_samples, label_burnin=a.label_burnin,
+                               label_every=a.label_every)
         t1 = time.time()
         params, losses = train(ts, a.steps, a.batch, a.lr, seed=a.seed, log_every=max(1, a.steps // 20))
         t2 = time.time()
@@ -412,7 +424,10 @@ def main(argv=None) -> None:
             print(f"  step {s:6d} loss {l:.5f}")
         out = a.out or default_weights_path(a.protocol)
         save(out, params, ndir=prot.ndir, model=2, nfibres=3, protocol=a.protocol, n_train=a.n, steps=a.steps,
-             seed=a.seed, labels=a.labels, label_samples=a.label_samples, bvals=prot.bvals, bvecs=prot.bvecs,
+             seed=a.seed, labels=a.labels, label_samples=a.label_samples,
+             label_burnin=opts.nburn if a.label_burnin is None else a.label_burnin,
+             label_every=opts.sampleevery if a.label_every is None else a.label_every,
+             bvals=prot.bvals, bvecs=prot.bvecs,
              options=oname,
              rician=opts.rician, f0=opts.f0, ardf0=opts.ardf0)
         print("saved", out)
