@@ -44,11 +44,14 @@ WORKLOAD_LEARNED = ("whole-brain: model 2, 3 fibres, rician+f0+ardf0, 288 measur
                     "launch per step) against the plain LM-initialised chain (burnin 1000)")
 
 
-# DRAM bytes (read + write) of one mcmc_kernel launch per voxel on the whole-brain workload, from
-# an ncu capture of a 65536-voxel launch (the learned chain: 1450 iterations, 50 samples):
-# 122,633,984 B read + 169,972,992 B written.  The kernel keeps its chain state on chip, so its
-# traffic scales with voxels, not with iterations.
-MCMC_DRAM_BYTES_PER_VOXEL = (122633984 + 169972992) / 65536
+# DRAM bytes (read + write) of one mcmc_kernel launch on the whole-brain workload at this bench's
+# launch size, from an ncu capture of a 131072-voxel launch (the learned chain: 1450 iterations,
+# 50 samples): 278,176,512 B read + 420,939,776 B written, 5334 B per voxel against 4224 B of
+# inputs, start state and samples.  The chain state stays on chip, so the traffic does not grow
+# with iterations; per voxel it grows with the launch size (4465 B at 65536 voxels), since the
+# one-word record stores of neighbouring voxels reach L2 further apart in time.
+MCMC_DRAM_BYTES_LAUNCH = 278176512 + 420939776
+MCMC_DRAM_LAUNCH_VOXELS = 131072
 
 
 def whole_brain_options() -> Options:
@@ -925,9 +928,12 @@ def main():
     roofline = {
         "bound": canon["bound"], "achieved": canon["achieved"], "peak": canon["peak"], "unit": "Gop/s",
         "frac": canon["frac"],
-        "traffic": MCMC_DRAM_BYTES_PER_VOXEL * chunk if (o.model, o.nfibres, M, o.nsamples) == (2, 3, 288, 50) else None,
-        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 65536-voxel mcmc_kernel "
-                          "launch on this workload's options, per voxel, scaled by the voxels of this launch",
+        "traffic": (MCMC_DRAM_BYTES_LAUNCH if chunk == MCMC_DRAM_LAUNCH_VOXELS else
+                    MCMC_DRAM_BYTES_LAUNCH / MCMC_DRAM_LAUNCH_VOXELS * chunk)
+        if (o.model, o.nfibres, M, o.nsamples) == (2, 3, 288, 50) else None,
+        "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one 131072-voxel mcmc_kernel launch "
+                           "on this workload's options" + ("" if chunk == MCMC_DRAM_LAUNCH_VOXELS else
+                                                           ", per voxel, scaled by the voxels of this launch")),
         "kernel": f"mcmc_kernel (burn-in + recording), timed in the {rf} form's step",
         "counts": "canonical per-term counts (model-2 signal rcp+log2+exp2, Rician log2+rsqrt; FMA 6 per signal "
                   "term, K+4(+12 Rician) per likelihood term)",
