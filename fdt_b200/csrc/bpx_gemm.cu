@@ -34,6 +34,14 @@ constexpr int kTileM = 128;
 constexpr int kChunkK = 64;
 constexpr int kThreads = 128;
 constexpr long long kWaitCycles = 2000000000ll;  // ~1 s at 2 GHz
+// epilogue staging per warp: a 32 x 32 fp32 block (rows padded to 36 floats) and a 32 x 32 bf16
+// block (rows padded to 80 bytes); both pitches keep 16-byte alignment and spread a quarter-warp's
+// 16-byte accesses over distinct banks
+constexpr int kPitchF = 36;
+constexpr int kPitchB = 80;
+constexpr int kEpiWarpBytes = 32 * kPitchF * 4 + 32 * kPitchB;
+static_assert((kThreads / 32) * kEpiWarpBytes <= 2 * kTileM * kChunkK * 2, "epilogue tiles must fit the A stages");
+static_assert(kEpiWarpBytes % 16 == 0 && (32 * kPitchF * 4) % 16 == 0, "epilogue tiles must stay 16-byte aligned");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -104,6 +112,7 @@ __device__ __forceinline__ uint16_t to_bf16(float x) {
 }
 
 struct Smem {
+  float bias[256];  // the tile's bias columns, staged once for the epilogue (16-byte aligned)
   uint64_t full[2], empty[2], done;
   uint32_t tmem_base;
 };
@@ -188,73 +197,139 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncwarp();
   const bool done = mbar_wait(smem_u32(&sm->done), 0);
   if (!done && g.error) atomicExch(g.error, 2);
+  // every lane of a warp adds the same bias columns: stage them in shared memory once, so the
+  // epilogue reads them as broadcast 16-byte loads instead of 32 global loads per column chunk
+  const bool use_bias = g.bias && (g.epi == kEpiBias || g.epi == kEpiBiasGelu);
+  if (use_bias)
+    for (int t = threadIdx.x; t < nt; t += kThreads) sm->bias[t] = n0 + t < g.N ? g.bias[n0 + t] : 0.f;
+  __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
-  // epilogue: warp w owns accumulator rows 32w..32w+31 (TMEM lanes), 32 columns at a time
-  const int row = m0 + 32 * warp + lane;
+  // epilogue: warp w owns accumulator rows 32w..32w+31 (TMEM lanes), 32 columns at a time.  A lane
+  // holds one row of a 32x32 block, so it is turned around through a per-warp shared-memory tile:
+  // lanes write their rows, then read the block back so that consecutive lanes cover consecutive
+  // columns of a row, and the global stores (and the GELU-derivative's loads of z) are whole
+  // 128-byte lines instead of 32 rows touched per instruction.  The tiles reuse the operand stages,
+  // idle once every MMA has completed (the done barrier above).
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  float* tf = reinterpret_cast<float*>(base + warp * kEpiWarpBytes);  // [32][kPitchF] fp32 block
+  unsigned char* tb = base + warp * kEpiWarpBytes + 32 * kPitchF * 4;  // [32][kPitchB] bytes, bf16 block
+  const bool all_done = __all_sync(0xffffffffu, done);
+  const int row0 = m0 + 32 * warp;
+  auto aligned16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+  // the block's 32 rows x 32 fp32 columns, lane = row, to out (row-major, leading dimension ld)
+  auto put_f32 = [&](const float (&v)[32], float* out, int ld, int col0) {
+    float4* t4 = reinterpret_cast<float4*>(tf + lane * kPitchF);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) t4[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int r = 4 * i + (lane >> 3), q = lane & 7;
+      const int grow = row0 + r, gcol = col0 + 4 * q;
+      const float4 x = reinterpret_cast<const float4*>(tf + r * kPitchF)[q];
+      if (grow < g.M && gcol < g.N) {
+        float* o = out + (size_t)grow * ld + gcol;
+        if (gcol + 3 < g.N && aligned16(o)) {
+          *reinterpret_cast<float4*>(o) = x;
+        } else {
+          const float e[4] = {x.x, x.y, x.z, x.w};
+          for (int j = 0; j < 4 && gcol + j < g.N; ++j) o[j] = e[j];
+        }
+      }
+    }
+    __syncwarp();
+  };
+  // the same for bf16 values (32 per lane, packed in pairs)
+  auto put_bf16 = [&](const uint32_t (&h)[16], uint16_t* out, int ld, int col0) {
+    uint4* t4 = reinterpret_cast<uint4*>(tb + lane * kPitchB);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) t4[q] = make_uint4(h[4 * q], h[4 * q + 1], h[4 * q + 2], h[4 * q + 3]);
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = 8 * i + (lane >> 2), q = lane & 3;
+      const int grow = row0 + r, gcol = col0 + 8 * q;
+      const uint4 x = reinterpret_cast<const uint4*>(tb + r * kPitchB)[q];
+      if (grow < g.M && gcol < g.N) {
+        uint16_t* o = out + (size_t)grow * ld + gcol;
+        if (gcol + 7 < g.N && aligned16(o)) {
+          *reinterpret_cast<uint4*>(o) = x;
+        } else {
+          const uint32_t w[4] = {x.x, x.y, x.z, x.w};
+          for (int j = 0; j < 8 && gcol + j < g.N; ++j) o[j] = (uint16_t)(w[j >> 1] >> (16 * (j & 1)));
+        }
+      }
+    }
+    __syncwarp();
+  };
+  // z of the GELU derivative for the block's rows: coalesced loads into the fp32 tile, then each
+  // lane reads its own row (columns past N read as 0)
+  auto get_f32 = [&](const float* in, int ld, int col0, float (&zv)[32]) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int r = 4 * i + (lane >> 3), q = lane & 7;
+      const int grow = row0 + r, gcol = col0 + 4 * q;
+      float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (grow < g.M && gcol < g.N) {
+        const float* z = in + (size_t)grow * ld + gcol;
+        if (gcol + 3 < g.N && aligned16(z)) {
+          x = *reinterpret_cast<const float4*>(z);
+        } else {
+          float e[4] = {0.f, 0.f, 0.f, 0.f};
+          for (int j = 0; j < 4 && gcol + j < g.N; ++j) e[j] = z[j];
+          x = make_float4(e[0], e[1], e[2], e[3]);
+        }
+      }
+      reinterpret_cast<float4*>(tf + r * kPitchF)[q] = x;
+    }
+    __syncwarp();
+    const float4* t4 = reinterpret_cast<const float4*>(tf + lane * kPitchF);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float4 x = t4[q];
+      zv[4 * q] = x.x;
+      zv[4 * q + 1] = x.y;
+      zv[4 * q + 2] = x.z;
+      zv[4 * q + 3] = x.w;
+    }
+    __syncwarp();
+  };
   for (int c = 0; c < nt / 32; ++c) {
     float v[32];
     __syncwarp();
     tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(c * 32), v);
     const int col0 = n0 + c * 32;
-    if (!done || row >= g.M || col0 >= g.N) continue;
-    const int ncol = min(32, g.N - col0);
-    // each lane owns one output row: a full, 16-byte aligned run of 32 columns is written with
-    // 16-byte stores (8 per FP32 row, 4 per BF16 row), anything else element by element
-    auto aligned16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+    if (!all_done || row0 >= g.M || col0 >= g.N) continue;  // warp-uniform
+    const float4* sb4 = reinterpret_cast<const float4*>(sm->bias + c * 32);
+    if (use_bias) {
+#pragma unroll
+      for (int j = 0; j < 32; j += 4) {
+        const float4 b4 = sb4[j / 4];
+        v[j] += b4.x;
+        v[j + 1] += b4.y;
+        v[j + 2] += b4.z;
+        v[j + 3] += b4.w;
+      }
+    }
     if (g.epi == kEpiStoreF32 || g.epi == kEpiBias) {
-      float* o = g.out_f32 + (size_t)row * g.ld_out + col0;
-      if (g.epi == kEpiBias)
-        for (int j = 0; j < ncol; ++j) v[j] += g.bias[col0 + j];
-      if (ncol == 32 && aligned16(o)) {
-#pragma unroll
-        for (int j = 0; j < 32; j += 4) *reinterpret_cast<float4*>(o + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
-      } else {
-        for (int j = 0; j < ncol; ++j) o[j] = v[j];
-      }
+      put_f32(v, g.out_f32, g.ld_out, col0);
     } else if (g.epi == kEpiBiasGelu) {
-      uint16_t* a = g.out_bf16 + (size_t)row * g.ld_bf16 + col0;
-      float* z = g.out_f32 ? g.out_f32 + (size_t)row * g.ld_out + col0 : nullptr;
+      if (g.out_f32) put_f32(v, g.out_f32, g.ld_out, col0);
+      uint32_t h[16];
 #pragma unroll
-      for (int j = 0; j < 32; ++j) v[j] = j < ncol ? v[j] + g.bias[col0 + j] : 0.f;
-      if (z) {
-        if (ncol == 32 && aligned16(z)) {
-#pragma unroll
-          for (int j = 0; j < 32; j += 4) *reinterpret_cast<float4*>(z + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
-        } else {
-          for (int j = 0; j < ncol; ++j) z[j] = v[j];
-        }
-      }
-      if (ncol == 32 && aligned16(a)) {
-#pragma unroll
-        for (int j = 0; j < 32; j += 8) {
-          uint4 q;
-          q.x = (uint32_t)to_bf16(gelu(v[j])) | ((uint32_t)to_bf16(gelu(v[j + 1])) << 16);
-          q.y = (uint32_t)to_bf16(gelu(v[j + 2])) | ((uint32_t)to_bf16(gelu(v[j + 3])) << 16);
-          q.z = (uint32_t)to_bf16(gelu(v[j + 4])) | ((uint32_t)to_bf16(gelu(v[j + 5])) << 16);
-          q.w = (uint32_t)to_bf16(gelu(v[j + 6])) | ((uint32_t)to_bf16(gelu(v[j + 7])) << 16);
-          *reinterpret_cast<uint4*>(a + j) = q;
-        }
-      } else {
-        for (int j = 0; j < ncol; ++j) a[j] = to_bf16(gelu(v[j]));
-      }
+      for (int j = 0; j < 16; ++j)
+        h[j] = (uint32_t)to_bf16(gelu(v[2 * j])) | ((uint32_t)to_bf16(gelu(v[2 * j + 1])) << 16);
+      put_bf16(h, g.out_bf16, g.ld_bf16, col0);
     } else {  // kEpiGeluGrad: dZ = (dZ_next W) * gelu'(z)
-      uint16_t* d = g.out_bf16 + (size_t)row * g.ld_bf16 + col0;
-      const float* z = g.zin + (size_t)row * g.ld_zin + col0;
-      if (ncol == 32 && aligned16(d) && aligned16(z)) {
+      float zv[32];
+      get_f32(g.zin, g.ld_zin, col0, zv);
+      uint32_t h[16];
 #pragma unroll
-        for (int j = 0; j < 32; j += 8) {
-          const float4 z0 = *reinterpret_cast<const float4*>(z + j), z1 = *reinterpret_cast<const float4*>(z + j + 4);
-          uint4 q;
-          q.x = (uint32_t)to_bf16(v[j] * gelu_grad(z0.x)) | ((uint32_t)to_bf16(v[j + 1] * gelu_grad(z0.y)) << 16);
-          q.y = (uint32_t)to_bf16(v[j + 2] * gelu_grad(z0.z)) | ((uint32_t)to_bf16(v[j + 3] * gelu_grad(z0.w)) << 16);
-          q.z = (uint32_t)to_bf16(v[j + 4] * gelu_grad(z1.x)) | ((uint32_t)to_bf16(v[j + 5] * gelu_grad(z1.y)) << 16);
-          q.w = (uint32_t)to_bf16(v[j + 6] * gelu_grad(z1.z)) | ((uint32_t)to_bf16(v[j + 7] * gelu_grad(z1.w)) << 16);
-          *reinterpret_cast<uint4*>(d + j) = q;
-        }
-      } else {
-        for (int j = 0; j < ncol; ++j) d[j] = to_bf16(v[j] * gelu_grad(z[j]));
-      }
+      for (int j = 0; j < 16; ++j)
+        h[j] = (uint32_t)to_bf16(v[2 * j] * gelu_grad(zv[2 * j])) |
+               ((uint32_t)to_bf16(v[2 * j + 1] * gelu_grad(zv[2 * j + 1])) << 16);
+      put_bf16(h, g.out_bf16, g.ld_bf16, col0);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
