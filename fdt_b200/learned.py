@@ -405,8 +405,32 @@ def main(argv=None) -> None:
     ap.add_argument("--label-every", type=int, default=None,
                     help="sample spacing of the labelling chain (default: the plain chain's)")
     ap.add_argument("--weights", default=None, help="evaluate these weights instead of training")
+    ap.add_argument("--time-forward", type=int, default=0, metavar="ROWS",
+                    help="only time the network's forward pass on ROWS inputs (CUDA events) and exit")
     a = ap.parse_args(argv)
     prot = PROTOCOLS[a.protocol](synth)
+    if a.time_forward:
+        import json
+
+        params, _ = load_weights(a.weights or default_weights_path(a.protocol))
+        g = torch.Generator(device="cuda").manual_seed(a.seed)
+        x = (1.2 * torch.rand((a.time_forward, nin(prot.ndir)), device="cuda", generator=g)).to(torch.bfloat16)
+        p = torch.from_numpy(np.ascontiguousarray(params, np.float32)).cuda()
+        for _ in range(3):
+            forward(p, prot.ndir, x)
+        ts = []
+        for _ in range(20):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            forward(p, prot.ndir, x)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        if lib.poll_error() != 0:
+            raise SystemExit("a tensor-core kernel reported a timed-out wait")
+        print(json.dumps({"rows": a.time_forward, "layers": 5, "forward_ms_min": min(ts),
+                          "forward_ms_median": float(np.median(ts))}))
+        return
     oname = a.options or DEFAULT_OPTIONS[a.protocol]
     opts = Options.make(**OPTION_SETS[oname])
     if a.weights:
