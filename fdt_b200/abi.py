@@ -208,4 +208,7 @@ class TrackVolume(C.Structure):
         ("lr_dz", C.c_float),
         ("m2_lookup", C.c_void_p),
         ("matrix2", C.c_void_p),
+        ("m1_ncols", C.c_int32),
+        ("m1_lookup", C.c_void_p),
+        ("matrix1", C.c_void_p),
     ]

@@ -45,7 +45,7 @@ constexpr int kTrackBlocksPerSm = 16;
 // 255 / 219 / 204 ms with all of them and matrix2 (14 blocks: 204 ms).
 constexpr int kFeatEuler = 1;  // --modeuler
 constexpr int kFeatLoop = 2;   // --loopcheck
-constexpr int kFeatCount = 4;  // seeds to targets, matrix2
+constexpr int kFeatCount = 4;  // seeds to targets, matrix2, matrix1
 
 struct TrackArgs {
   bpx_track_options o;
@@ -446,7 +446,15 @@ struct Tracker {
       flags |= way;
       if (count && vox != last) {
         last = vox;
-        if (first_visit(vox)) atomicAdd(paths + vox, o.pathdist ? ++nvisit : 1);
+        if (first_visit(vox)) {
+          const int add = o.pathdist ? ++nvisit : 1;
+          atomicAdd(paths + vox, add);
+          if ((FEAT & kFeatCount) && v.m1_ncols > 0) {
+            // --omatrix1: a seed-mask voxel's fdt_paths count also goes to the seed's row
+            const int c1 = __ldg(v.m1_lookup + vox);
+            if (c1 >= 0 && c1 < v.m1_ncols) atomicAdd(v.matrix1 + (size_t)cnt.seed * v.m1_ncols + c1, add);
+          }
+        }
         if ((FEAT & kFeatCount) && v.ntargets > 0) {
           // a target is counted at its first entry on the counted path (a voxel change), if the path
           // is by then at least distthresh long (Counter::update_seedcounts)
@@ -462,7 +470,7 @@ struct Tracker {
         // --omatrix2: the tract-space voxel of the position, counted once per particle when its
         // column is not 0 (Counter::update_matrix2_row); it can change inside a diffusion voxel
         last_lr = lr;
-        if (col > 0 && first_visit(lr | kLrKey))
+        if (col > 0 && col < v.m2_ncols && first_visit(lr | kLrKey))
           atomicAdd(v.matrix2 + (size_t)cnt.seed * v.m2_ncols + col, o.pathdist ? ++cnt.nvisit2 : 1);
       }
       if ((FEAT & kFeatCount) && count) cnt.length += o.steplength;
@@ -666,6 +674,13 @@ bpx_status check_track(const bpx_track_options* o, const bpx_track_volume* v, in
     if (nseeds > 0 && (!v->m2_lookup || !v->matrix2))
       return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: NULL m2_lookup or matrix2");
   }
+  if (v->m1_ncols < 0) return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: m1_ncols < 0");
+  if (v->m1_ncols > 0) {
+    if ((size_t)nseeds * (size_t)v->m1_ncols >= (1ull << 40))
+      return api_fail(BPX_ERR_UNSUPPORTED, "bpx_probtrack_dev: matrix1 of 2^40 or more entries");
+    if (nseeds > 0 && (!v->m1_lookup || !v->matrix1))
+      return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: NULL m1_lookup or matrix1");
+  }
   if (nseeds > 0 && (!seeds || !paths || !waytotal || !v->th || !v->ph || !v->f || !v->mask ||
                      (v->nwaypoints > 0 && !v->waypoints)))
     return api_fail(BPX_ERR_INVALID_ARG, "bpx_probtrack_dev: NULL buffer");
@@ -742,7 +757,7 @@ bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volu
   const size_t table_bytes = ((size_t)1 << log2n) * sizeof(uint2);
   const size_t max_blocks = ((size_t)16 << 30) / ((table_bytes + lc_bytes) * kTrackThreads);
   const int feat = (opts->modeuler ? kFeatEuler : 0) | (opts->loopcheck ? kFeatLoop : 0) |
-                   ((vol->ntargets > 0 || vol->m2_ncols > 0) ? kFeatCount : 0);
+                   ((vol->ntargets > 0 || vol->m2_ncols > 0 || vol->m1_ncols > 0) ? kFeatCount : 0);
   int grid = sm_count() * kTrackBlocksPerSm;
   if ((size_t)grid > max_blocks) grid = max_blocks > 0 ? (int)max_blocks : 1;
   const size_t threads = (size_t)grid * kTrackThreads;

@@ -402,7 +402,7 @@ def matrix2_lookup(lrmask) -> np.ndarray:
 
 
 def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.0), avoid=None, stop=None,
-              waypoints=None, targets=None, matrix2=None):
+              waypoints=None, targets=None, matrix2=None, matrix1=None):
     """probtrackx on device tensors: (paths [nz][ny][nx] int32, or [nseeds][nz][ny][nx] with
     topts.per_seed; waytotal int) for
     seeds [nseeds][3] (voxel coordinates x, y, z).  `avoid` and `stop`: device masks of the mask's
@@ -410,7 +410,9 @@ def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0,
     streamline must all pass (--waypoints); `targets`: a list of 1 to 32 target masks, for which
     seeds_to_targets [ntargets][nseeds] (int32, host) follows waytotal (--targetmasks --os2t);
     `matrix2`: (tract-space mask [lz][ly][lx], its voxel size in mm), for which fdt_matrix2
-    [nseeds][columns] (int32, host) comes last (--omatrix2 --lrmask)."""
+    [nseeds][columns] (int32, host) follows (--omatrix2 --lrmask); `matrix1`: the seed mask
+    [nz][ny][nx], for which fdt_matrix1 [nseeds][seed-mask voxels] (int32, host) comes last
+    (--omatrix1: each seed's path distribution at the seed-mask voxels, in z, y, x order)."""
     torch = _torch()
     way_bits = None
     nway = 0
@@ -439,6 +441,15 @@ def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0,
         v.lr_nz, v.lr_ny, v.lr_nx = (int(x) for x in lut.shape)
         v.lr_dx, v.lr_dy, v.lr_dz = (float(x) for x in lr_size)
         v.m2_lookup, v.matrix2 = lut_d.data_ptr(), m2.data_ptr()
+    m1 = None
+    if matrix1 is not None:
+        lut1 = matrix2_lookup(matrix1.cpu().numpy() if hasattr(matrix1, "cpu") else matrix1)
+        if lut1.shape != tuple(mask.shape):
+            raise BpxError("matrix1: the seed mask must have the mask's shape")
+        lut1_d = torch.from_numpy(lut1).to("cuda")
+        m1 = torch.zeros((int(sd.shape[0]), int((lut1 >= 0).sum())), device="cuda", dtype=torch.int32)
+        v.m1_ncols = int(m1.shape[1])
+        v.m1_lookup, v.matrix1 = lut1_d.data_ptr(), m1.data_ptr()
     _check(load().bpx_probtrack_dev(C.byref(topts), C.byref(v), int(sd.shape[0]), _ptr(sd), _ptr(paths), _ptr(way),
                                     _stream(torch)), "bpx_probtrack_dev")
     out = (paths, int(way.item()))
@@ -446,6 +457,8 @@ def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0,
         out += (s2t.cpu().numpy(),)
     if matrix2 is not None:
         out += (m2.cpu().numpy(),)
+    if matrix1 is not None:
+        out += (m1.cpu().numpy(),)
     return out
 
 

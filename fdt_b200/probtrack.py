@@ -4,7 +4,7 @@
         [-S 2000] [--steplength 0.5] [--cthr 0.2] [--fibthresh 0.01] [--distthresh 0] [--randfib 0]
         [--fibst 1] [--usef] [--sampvox] [--pd] [-l] [--modeuler] [--seed N] [--avoid MASK]
         [--stop MASK] [--waypoints MASK|LIST] [--targetmasks LIST --os2t] [--omatrix2 --lrmask MASK]
-        [--network] [--mask2 MASK]
+        [--omatrix1] [--network] [--mask2 MASK]
 
 Reads merged_th{k}samples, merged_ph{k}samples, merged_f{k}samples and nodif_brain_mask (NIfTI-1)
 as probtrackx does (probtrackx.cc:25-96, tractvolsx.h:55-97) and tracks from the seeds:
@@ -26,6 +26,11 @@ diffusion grid) adds OUTDIR/fdt_matrix2.nii.gz, seeds x tract-space voxels: for 
 kept streamlines from it through each voxel of the mask, and its coordinate and lookup files
 (Counter::initialise_matrix2, update_matrix2_row, save_matrix2; streamlines.cc:515-560, 772-808,
 970-980).
+--omatrix1 (seedmask mode) adds OUTDIR/fdt_matrix1.nii.gz, seeds x seeds: for every seed, the kept
+streamlines from it through each seed voxel (its path distribution read at the seed mask), and
+coords_for_fdt_matrix1 (Counter::initialise_matrix1, update_matrix1, save_matrix1;
+streamlines.cc:493-510, 751-770, 963-968).  The reference clears its path distribution after each
+seed when it builds matrix1, so its fdt_paths comes out empty then; here fdt_paths keeps the sum.
 --avoid rejects a half that enters the mask, --stop ends a half where it enters it, and --waypoints
 (one mask, or a text file naming up to 32 masks one per line) keeps only streamlines whose halves
 together passed every mask (streamlines.cc:112-145, 279-330); all on the diffusion grid.
@@ -99,7 +104,7 @@ def seed_points(arg: str, grid: tuple[int, int, int]) -> tuple[np.ndarray, bool]
 
 def run(bpx_dir: str, seeds, opts: TrackOptions, outdir: str, avoid: str | None = None,
         stop: str | None = None, waypoints: str | None = None, outname: str = "fdt_paths",
-        targets: str | None = None, lrmask: str | None = None) -> tuple[np.ndarray, int]:
+        targets: str | None = None, lrmask: str | None = None, omatrix1: bool = False) -> tuple[np.ndarray, int]:
     """Tracks from `seeds` (a seed file or mask path, or an array of points for simple mode) and
     writes the path distributions and waytotal; returns (paths [x][y][z], or [nseeds][x][y][z] in
     simple mode, waytotal)."""
@@ -107,6 +112,7 @@ def run(bpx_dir: str, seeds, opts: TrackOptions, outdir: str, avoid: str | None 
 
     th, ph, f, m, hdr, vs = read_samples(bpx_dir)
     grid = m.shape[::-1]
+    seeds_arg = seeds
     if isinstance(seeds, str):
         seeds, per_seed = seed_points(seeds, grid)
     else:
@@ -127,6 +133,11 @@ def run(bpx_dir: str, seeds, opts: TrackOptions, outdir: str, avoid: str | None 
         lr, lr_hdr = nifti.read(lrmask)
         lr_zyx = np.ascontiguousarray(np.transpose(np.asarray(lr, np.float32).reshape(lr.shape[:3]), (2, 1, 0)))
         extra["matrix2"] = (lr_zyx, tuple(float(x) for x in lr_hdr.pixdim[1:4]))
+    if omatrix1:
+        if per_seed or not isinstance(seeds_arg, str):
+            raise ValueError("--omatrix1 needs a seed mask (seedmask mode)")
+        # the columns: the seed voxels, in the order seed_points gives the seeds (z, y, x)
+        extra["matrix1"] = (np.abs(read_mask(seeds_arg, grid)) > 0).astype(np.float32)
     res = lib.probtrack(opts, *dev, seeds, voxel_size=vs, **extra)
     paths, way = res[0], res[1]
     torch.cuda.synchronize()
@@ -162,8 +173,20 @@ def run(bpx_dir: str, seeds, opts: TrackOptions, outdir: str, avoid: str | None 
             nifti.write(os.path.join(outdir, f"seeds_to_{stem}.nii.gz"), vol, like=hdr,
                         cal=(0.0, float(opts.nparticles)))
     if lrmask:
-        save_matrix2(outdir, res[-1], seeds, lr_zyx, lr_hdr)
+        save_matrix2(outdir, res[2 + bool(target_files)], seeds, lr_zyx, lr_hdr)
+    if omatrix1:
+        save_matrix1(outdir, res[-1], seeds)
     return vols, way
+
+
+def save_matrix1(outdir: str, m1: np.ndarray, seeds: np.ndarray) -> None:
+    """Counter::save_matrix1 (streamlines.cc:963-968): fdt_matrix1 (seeds along x, seed-voxel columns
+    along y, int32 as the reference's volume<int>) and coords_for_fdt_matrix1 (each seed's voxel
+    x y z)."""
+    m1 = np.asarray(m1, np.int32)
+    nifti.write(os.path.join(outdir, "fdt_matrix1.nii.gz"), m1[:, :, None], cal=(0.0, float(m1.max(initial=0))))
+    seed_vox = np.floor(np.asarray(seeds, np.float64) + 0.5).astype(np.int32)
+    nifti.write(os.path.join(outdir, "coords_for_fdt_matrix1.nii.gz"), seed_vox[:, :, None])
 
 
 def save_matrix2(outdir: str, m2: np.ndarray, seeds: np.ndarray, lr_zyx: np.ndarray, lr_hdr) -> None:
@@ -257,6 +280,7 @@ def main(argv=None) -> None:
     ap.add_argument("--os2t", action="store_true", help="output seeds_to_targets")
     ap.add_argument("--omatrix2", action="store_true", help="output matrix2 (seeds x tract-space voxels)")
     ap.add_argument("--lrmask", help="tract-space (low resolution) mask for matrix2")
+    ap.add_argument("--omatrix1", action="store_true", help="output matrix1 (seeds x seed voxels; seedmask mode)")
     ap.add_argument("--network", action="store_true", help="network mode: --seeds lists several masks")
     ap.add_argument("--mask2", help="second seed mask (twomasks mode, with a seed mask)")
     a = ap.parse_args(argv)
@@ -269,15 +293,18 @@ def main(argv=None) -> None:
     if a.omatrix2 and not a.lrmask:
         ap.error("--omatrix2 needs --lrmask")
     if a.network or a.mask2:
-        if a.os2t or a.omatrix2:
-            ap.error("seeds_to_targets and matrix2 are not available in multiple seed tractography")
+        if a.os2t or a.omatrix2 or a.omatrix1:
+            ap.error("seeds_to_targets, matrix1 and matrix2 are not available in multiple seed tractography")
         masks = [a.seeds, a.mask2] if a.mask2 else a.seeds
         _, ways = run_network(a.bpx_dir, masks, o, a.out, avoid=a.avoid, stop=a.stop, waypoints=a.waypoints,
                               outname=a.outname)
         print("waytotal " + " ".join(map(str, ways)))
         return
+    if a.omatrix1 and not a.seeds.endswith((".nii", ".nii.gz")):
+        ap.error("--omatrix1 needs a seed mask (seedmask mode)")
     _, way = run(a.bpx_dir, a.seeds, o, a.out, avoid=a.avoid, stop=a.stop, waypoints=a.waypoints, outname=a.outname,
-                 targets=a.targetmasks if a.os2t else None, lrmask=a.lrmask if a.omatrix2 else None)
+                 targets=a.targetmasks if a.os2t else None, lrmask=a.lrmask if a.omatrix2 else None,
+                 omatrix1=a.omatrix1)
     print(f"waytotal {way}")
 
 

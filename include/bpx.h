@@ -507,6 +507,15 @@ typedef struct bpx_track_volume {
   float lr_dx, lr_dy, lr_dz;
   const int32_t* m2_lookup;
   int32_t* matrix2;
+  /* --omatrix1 (Counter::initialise_matrix1, update_matrix1, streamlines.cc:493-510, 751-770): m1_lookup
+   * [nz][ny][nx] gives each seed-mask voxel its column (-1 elsewhere: m1_ncols columns, numbered in
+   * z, y, x order as the seeds of seedmask mode are); matrix1 [nseeds][m1_ncols] (OUTPUT, int32,
+   * added to) counts for every seed the kept streamlines through each seed-mask voxel, once per
+   * streamline, adding what that voxel's fdt_paths count gets (with pathdist the d-th new voxel adds
+   * d): the reference's per-seed path distribution read at the seed mask. */
+  int32_t m1_ncols;
+  const int32_t* m1_lookup;
+  int32_t* matrix1;
 } bpx_track_volume;
 
 void bpx_track_options_default(bpx_track_options* opts);

@@ -199,13 +199,14 @@ def energy(opts: Options, data, bvecs, bvals, states):
 
 
 def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.0), avoid=None, stop=None,
-              waypoints=None, targets=None, matrix2=None):
+              waypoints=None, targets=None, matrix2=None, matrix1=None):
     """probtrackx simple mode on host arrays (th/ph/f [nfib][nsamples][nz][ny][nx], mask [nz][ny][nx],
     seeds [nseeds][3] voxel coordinates; optional avoid and stop masks and a list of waypoint masks,
     each [nz][ny][nx]; target masks, each [nz][ny][nx]; matrix2 = (tract-space mask [lz][ly][lx], its
-    voxel size)): (paths [nz][ny][nx] int32, or [nseeds][nz][ny][nx] with topts.per_seed,
-    waytotal[, seeds_to_targets [ntargets][nseeds] int32 when targets are given][, fdt_matrix2
-    [nseeds][columns] int32 when matrix2 is given])."""
+    voxel size); matrix1 = the seed mask [nz][ny][nx]): (paths [nz][ny][nx] int32, or
+    [nseeds][nz][ny][nx] with topts.per_seed, waytotal[, seeds_to_targets [ntargets][nseeds] int32
+    when targets are given][, fdt_matrix2 [nseeds][columns] int32 when matrix2 is given][,
+    fdt_matrix1 [nseeds][seed-mask voxels] int32 when matrix1 is given])."""
     th, ph, f, mask = (np.ascontiguousarray(a, np.float32) for a in (th, ph, f, mask))
     v = TrackVolume()
     v.nfib, v.nsamples, v.nz, v.ny, v.nx = th.shape
@@ -245,6 +246,16 @@ def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0,
         v.lr_nz, v.lr_ny, v.lr_nx = lut.shape
         v.lr_dx, v.lr_dy, v.lr_dz = lr_size
         v.m2_lookup, v.matrix2 = lut.ctypes.data, m2.ctypes.data
+    m1 = None
+    if matrix1 is not None:
+        inside1 = np.asarray(matrix1) != 0
+        assert inside1.shape == mask.shape
+        lut1 = np.full(inside1.shape, -1, np.int32)  # columns in z, y, x order (Counter::initialise_matrix1)
+        lut1[inside1] = np.arange(int(inside1.sum()), dtype=np.int32)
+        m1 = np.zeros((sd.shape[0], int(inside1.sum())), np.int32)
+        keep += [lut1, m1]
+        v.m1_ncols = m1.shape[1]
+        v.m1_lookup, v.matrix1 = lut1.ctypes.data, m1.ctypes.data
     paths = np.zeros(((sd.shape[0],) if topts.per_seed else ()) + tuple(mask.shape), np.int32)
     way = C.c_int64(0)
     rc = lib().orc_probtrack(C.byref(topts), C.byref(v), sd.shape[0], sd, paths, C.byref(way))
@@ -254,6 +265,8 @@ def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0,
         out += (s2t,)
     if matrix2 is not None:
         out += (m2,)
+    if matrix1 is not None:
+        out += (m1,)
     return out
 
 

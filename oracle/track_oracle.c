@@ -13,6 +13,8 @@
  *                               once (fdt_paths), per seed point with per_seed (ptx_simple.cc:50-62);
  *   Counter::update_seedcounts  (streamlines.cc:700-748): seeds to targets;
  *   Counter::update_matrix2_row (streamlines.cc:772-808): --omatrix2;
+ *   Counter::update_matrix1     (streamlines.cc:751-770): --omatrix1, the per-seed path
+ *                               distribution read at the seed-mask voxels;
  *   Tractvolsx::sample          (tractvolsx.h:101-255): probabilistic rounding of the position,
  *                               a random posterior sample, the first fibre (fibst, randfib 1/2)
  *                               and afterwards the fibre closest to the current direction among
@@ -413,7 +415,7 @@ int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nse
           /* matrix2: each tract-space voxel once per streamline; column 0 and voxels outside the
            * mask are not counted (the reference's m_lookup2 test is "!= 0") */
           const int32_t col = v->m2_lookup[lrpath[i]];
-          if (col > 0 && stamp2[lrpath[i]] != (int64_t)pid) {
+          if (col > 0 && col < v->m2_ncols && stamp2[lrpath[i]] != (int64_t)pid) {
             stamp2[lrpath[i]] = (int64_t)pid;
             ++d2;
             const uint32_t add = o->pathdist ? d2 : 1u;
@@ -444,6 +446,15 @@ int orc_probtrack(const bpx_track_options* o, const bpx_track_volume* v, int nse
           const size_t at_vx = (o->per_seed ? (size_t)s * T.nvox : 0) + (size_t)vx;
 #pragma omp atomic
           counts[at_vx] += add;
+          if (v->m1_ncols > 0) {
+            /* matrix1 (Counter::update_matrix1): the seed's path distribution read at the seed mask */
+            const int32_t c1 = v->m1_lookup[vx];
+            if (c1 >= 0 && c1 < v->m1_ncols) {
+              uint32_t* m1 = (uint32_t*)v->matrix1;
+#pragma omp atomic
+              m1[(size_t)s * v->m1_ncols + c1] += add;
+            }
+          }
         }
       }
     }

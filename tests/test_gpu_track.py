@@ -190,6 +190,18 @@ def test_probtrack_cli_with_masks_equals_oracle(torch, tmp_path):
     assert tc.shape[0] == want_m2.shape[1] and np.array_equal(lut[tc[:, 0], tc[:, 1], tc[:, 2]], np.arange(tc.shape[0]))
     sc, _ = nifti.read(os.path.join(out, "coords_for_fdt_matrix2.nii.gz"))
     assert np.array_equal(sc.reshape(-1, 3), pts.astype(int))
+    # --omatrix1 (with --omatrix2 beside it): seeds x seed voxels
+    out = os.path.join(d, "matrix1")
+    probtrack.main([d, "--seeds", os.path.join(d, "seedmask.nii.gz"), "--out", out, "--omatrix1", "--omatrix2",
+                    "--lrmask", os.path.join(d, "lr.nii.gz")] + common)
+    _, _, want_m2b, want_m1 = O.probtrack(o, th, ph, f, mask, pts, voxel_size=(1.0, 1.0, 1.0), matrix2=(lr, lr_vs),
+                                          matrix1=sm, **masks)
+    got, _ = nifti.read(os.path.join(out, "fdt_matrix1.nii.gz"))
+    assert got.shape[:2] == (3, 3) and np.array_equal(got.reshape(3, 3), want_m1) and want_m1.sum() > 0
+    got, _ = nifti.read(os.path.join(out, "fdt_matrix2.nii.gz"))
+    assert np.array_equal(got.reshape(want_m2b.shape), want_m2b)
+    sc, _ = nifti.read(os.path.join(out, "coords_for_fdt_matrix1.nii.gz"))
+    assert np.array_equal(sc.reshape(-1, 3), pts.astype(int))
 
 
 @pytest.mark.parametrize("kw", [dict(), dict(distthresh=6.0), dict(modeuler=1, per_seed=1)], ids=["plain", "distthresh",
@@ -243,6 +255,42 @@ def test_matrix2_equals_oracle(torch, name, kw):
     for g, w in zip(got[2:], want[2:]):
         assert np.array_equal(g, w), (name, np.argwhere(g != w)[:5])
     assert want[-1].sum() > 0 and want[-1].shape == (3, int(lr.sum()))
+
+
+M1_CASES = [
+    ("plain", dict()),
+    ("pathdist", dict(pathdist=1)),
+    ("masks_distthresh", dict(masks=("avoid", "stop", "waypoints"), distthresh=3.0)),
+    ("modeuler_loopcheck", dict(modeuler=1, loopcheck=1)),
+    ("with_matrix2", dict(matrix2=True)),
+]
+
+
+@pytest.mark.parametrize("name,kw", M1_CASES, ids=[c[0] for c in M1_CASES])
+def test_matrix1_equals_oracle(torch, name, kw):
+    """--omatrix1 in seedmask mode: every voxel of a seed mask seeds, and each seed's row counts its
+    kept streamlines through every seed-mask voxel (bit for bit against the oracle)."""
+    from fdt_b200 import lib
+
+    lib.load()
+    th, ph, f, mask = synth.fibre_field((20, 16, 10), nsamples=12, seed=4)
+    seedmask = np.zeros_like(mask)
+    seedmask[4:6, 6:10, 6:13] = mask[4:6, 6:10, 6:13]
+    seeds = np.argwhere(seedmask != 0)[:, ::-1].astype(np.float32)
+    kw = dict(kw)
+    extra = _masks(mask, kw.pop("masks", ()))
+    if kw.pop("matrix2", False):
+        extra["matrix2"] = ((np.random.default_rng(5).random((9, 11, 14)) < 0.7).astype(np.float32), (3.0, 3.0, 3.0))
+    o = TrackOptions.make(nparticles=50, nsteps=300, seed=43, **kw)
+    want = O.probtrack(o, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.5), matrix1=seedmask, **extra)
+    dev = [lib.to_device(a) for a in (th, ph, f, mask)]
+    dextra = {k: (lib.to_device(v) if k in ("avoid", "stop") else v) for k, v in extra.items()}
+    got = lib.probtrack(o, *dev, seeds, voxel_size=(2.0, 2.0, 2.5), matrix1=seedmask, **dextra)
+    torch.cuda.synchronize()
+    assert got[1] == want[1] and np.array_equal(got[0].cpu().numpy(), want[0])
+    for g, w in zip(got[2:], want[2:]):
+        assert np.array_equal(g, w), (name, np.argwhere(g != w)[:5])
+    assert want[-1].sum() > 0 and want[-1].shape == (len(seeds), len(seeds))
 
 
 @pytest.mark.parametrize("modeuler", [0, 1])

@@ -6,7 +6,8 @@ right-angle turn; the distance threshold drops short streamlines; the avoid, sto
 masks reject, end and select halves as Seedmanager::run and Streamliner::streamline do; --pd
 weights voxels by their order on the path; --loopcheck stops paths that circle back on themselves;
 --modeuler follows a straight tract as the plain steps do; --omatrix2 counts every tract-space voxel
-once per streamline (column 0 never, as the reference's "column != 0" test has it)."""
+once per streamline (column 0 never, as the reference's "column != 0" test has it); --omatrix1 is
+each seed's path distribution read at the seed mask."""
 import os
 import re
 
@@ -196,6 +197,26 @@ def test_matrix2_on_the_diffusion_grid_is_the_per_seed_path_counts_inside_the_ma
     want = each[:, lr2 != 0]
     want[:, 0] = 0
     assert np.array_equal(m2b, want)
+
+
+def test_matrix1_is_the_per_seed_path_counts_at_the_seed_mask():
+    # Counter::update_matrix1 copies the seed's path distribution at every seed-mask voxel (z, y, x
+    # order) into the seed's row, column 0 included; with --pd the same weighted counts
+    th, ph, f, mask = synth.fibre_field((16, 14, 8), nsamples=8, seed=2)
+    seedmask = np.zeros_like(mask)
+    seedmask[3:6, 5:9, 4:12] = mask[3:6, 5:9, 4:12]
+    zyx = np.argwhere(seedmask != 0)
+    seeds = zyx[:, ::-1].astype(np.float32)  # seedmask mode's seeds: x y z, in z, y, x order
+    for pd in (0, 1):
+        o = TrackOptions.make(nparticles=20, nsteps=200, seed=17, per_seed=1, pathdist=pd)
+        each, way, m1 = O.probtrack(o, th, ph, f, mask, seeds, matrix1=seedmask)
+        assert m1.shape == (len(seeds), len(seeds)) and m1.dtype == np.int32
+        assert np.array_equal(m1, each[:, seedmask != 0]) and m1.sum() > 0, pd
+        assert np.all(np.diag(m1) > 0)  # every seed's streamlines start in its own voxel
+        # the summed volume: the same matrix
+        o.per_seed = 0
+        paths, way2, m1b = O.probtrack(o, th, ph, f, mask, seeds, matrix1=seedmask)
+        assert way2 == way and np.array_equal(m1b, m1) and np.array_equal(paths, each.sum(0))
 
 
 def test_matrix2_on_a_coarser_grid_counts_each_tract_space_voxel_once_per_streamline():
