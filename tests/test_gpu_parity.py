@@ -191,8 +191,12 @@ def _run_both(torch, lib, oracle, o, y, prot, n_vox, voxel_offset=0):
 
 @pytest.mark.parametrize("kw", [dict(model=1, nfibres=2), dict(model=2, nfibres=3, rician=1, f0=1, ardf0=1),
                                 dict(model=2, nfibres=3, rician=1, f0=1, ardf0=1, mcmc_tpv=32, mcmc_mpl=16),
-                                dict(model=3, nfibres=2, rician=1), dict(model=3, nfibres=2, R_prior_fudge=1.0)],
-                         ids=["m1", "m2_ric_f0", "m2_ric_f0_32x16", "m3_ric", "m3_Rfudge"])
+                                dict(model=3, nfibres=2, rician=1), dict(model=3, nfibres=2, R_prior_fudge=1.0),
+                                dict(model=1, nfibres=2, all_ard=1), dict(model=2, nfibres=3, rician=1, no_ard=1),
+                                dict(model=2, nfibres=2, fudge=5.0, f0=1),
+                                dict(model=1, nfibres=1, updateproposalevery=7)],
+                         ids=["m1", "m2_ric_f0", "m2_ric_f0_32x16", "m3_ric", "m3_Rfudge", "m1_allard", "m2_ric_noard",
+                              "m2_fudge5_f0", "m1_K1_upe7"])
 def test_short_chains_track_the_oracle(torch, lib, oracle, kw):
     """Same random stream: the GPU chain reproduces the FP64 chain step by step (se=1) until an
     accept decision lands within FP32 rounding of its threshold."""
