@@ -65,6 +65,9 @@ FIT_CASES = [
     ("m2_K3", dict(model=2, nfibres=3), "multi", 25.0),
     ("m2_K3_f0_rician_ardf0", dict(model=2, nfibres=3, f0=1, rician=1, ardf0=1), "brain", 25.0),
     ("m3_K2", dict(model=3, nfibres=2), "multi", 25.0),
+    ("m1_cnonlin_K1", dict(model=1, nfibres=1), "small", 20.0),
+    ("m2_K2_f0", dict(model=2, nfibres=2, f0=1), "multi", 25.0),
+    ("m3_K3_f0_rician", dict(model=3, nfibres=3, f0=1, rician=1), "brain", 25.0),
 ]
 
 
@@ -140,6 +143,8 @@ ENERGY_CASES = [
     dict(model=2, nfibres=3),
     dict(model=2, nfibres=3, rician=1, f0=1, ardf0=1),
     dict(model=3, nfibres=2, rician=1),
+    dict(model=3, nfibres=3, f0=1),
+    dict(model=1, nfibres=1, rician=1),
 ]
 
 
