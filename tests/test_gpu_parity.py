@@ -336,6 +336,41 @@ def test_gradnonlin_zero_tensor_is_identity(torch, lib):
     assert np.allclose(a["mean_f"].numpy(), b["mean_f"].numpy(), atol=0.05)
 
 
+@pytest.mark.parametrize("kw", [dict(model=1, nfibres=2), dict(model=2, nfibres=3, rician=1, f0=1, ardf0=1)],
+                         ids=["m1", "m2_ric_f0"])
+def test_gradnonlin_fits_and_chains_track_the_oracle(torch, lib, oracle, kw):
+    """With a coil tensor per voxel (--gradnonlin) every voxel has its own b-matrix: the LM fits agree
+    with the FP64 oracle's on the same corrected b-matrices (criterion (a)) and short chains from the
+    same start track the oracle's step by step, through the kernel's per-voxel b-matrix tables."""
+    o = Options.make(nburn=0, njumps=30, sampleevery=1, gradnonlin=1, **kw)
+    prot = synth.three_shell(18, 90) if o.model >= 2 else synth.single_shell_64()
+    n = 64
+    y, _ = synth.make_volume(n, prot, o.nfibres, o.model >= 2, 25.0, seed=71)
+    if o.rician:
+        y = oracle.prepare_data(y)
+    grad = np.random.default_rng(5).normal(0, 0.02, (n, 9)).astype(np.float32)
+    g, d, bv, bl = _dev(torch, grad, y, prot.bvecs, prot.bvals)
+    bvv, blv = lib.gradnonlin(g, bv, bl)  # [n][3][ndir], [n][ndir]
+    bvv_h, blv_h = bvv.cpu().numpy(), blv.cpu().numpy()
+    assert not np.allclose(bvv_h, np.broadcast_to(prot.bvecs, bvv_h.shape), atol=1e-3)  # really per voxel
+    pg, tg, _ = lib.fit(o, d, bvv, blv)
+    po, _, _ = oracle.fit(o, y, bvv_h, blv_h)
+    pg64 = pg.cpu().numpy().astype(np.float64)
+    assert _fit_agreement(o, pg64, po).mean() >= 0.95
+    rec_g = lib.mcmc(o, d, bvv, blv, pg, tg).cpu().numpy()
+    rec_o = oracle.mcmc(o, y, bvv_h, blv_h, pg64, tg.cpu().numpy().astype(np.float64))
+    rows = [0, 5] + [6 + i for i in range(3 * o.nfibres)] + ([3] if o.model >= 2 else [])
+    agree_until = np.zeros(n, int)
+    for v in range(n):
+        for s_ in range(o.nsamples):
+            a, b = rec_g[rows, s_, v], rec_o[rows, s_, v]
+            if not np.all(np.abs(a - b) <= 1e-3 * np.abs(b) + 1e-6):
+                break
+            agree_until[v] += 1
+    assert np.mean(agree_until >= 10) >= 0.9, agree_until
+    assert np.median(agree_until) >= 20
+
+
 def test_gradnonlin_correction_matches_numpy(torch, lib):
     prot = synth.single_shell_64()
     rng = np.random.default_rng(0)
