@@ -211,4 +211,5 @@ class TrackVolume(C.Structure):
         ("m1_ncols", C.c_int32),
         ("m1_lookup", C.c_void_p),
         ("matrix1", C.c_void_p),
+        ("prefdir", C.c_void_p),
     ]

@@ -46,6 +46,7 @@ constexpr int kTrackBlocksPerSm = 16;
 constexpr int kFeatEuler = 1;  // --modeuler
 constexpr int kFeatLoop = 2;   // --loopcheck
 constexpr int kFeatCount = 4;  // seeds to targets, matrix2, matrix1
+constexpr int kFeatPref = 8;   // --prefdir
 
 struct TrackArgs {
   bpx_track_options o;
@@ -294,8 +295,8 @@ struct Tracker {
 
   // The fibre choice of Tractvolsx::sample on the voxel's sample: the chosen fibre's direction
   // (r), whether its angles are both non-zero (moves) and f (1 without --usef)
-  __device__ void choose(const Particle& P, const float (&u)[8], const Sample& S, bool& init_sample, int& fibst,
-                         float3& r, bool& moves, float& f) const {
+  __device__ void choose(const Particle& P, const float (&u)[8], const Sample& S, float3 pref, bool& init_sample,
+                         int& fibst, float3& r, bool& moves, float& f) const {
     const int K = a.v.nfib;
     const float thr = a.o.fibthresh;
     int sel = 0, fibind = 0;
@@ -333,9 +334,11 @@ struct Tracker {
         sel = fibst;
         init_sample = false;
       } else {
-        // no preferred-direction volume: the preference is the current direction;
-        // |sin th cos ph px + sin th sin ph py + cos th pz| in the reference's order
-        const float px = P.rx, py = P.ry, pz = P.rz;
+        // the preferred direction of the step's voxel, or where it is zero (always, without
+        // --prefdir) the current direction; |sin th cos ph px + sin th sin ph py + cos th pz| in the
+        // reference's order
+        const bool nopref = (fabsf(pref.x) + fabsf(pref.y) + fabsf(pref.z)) == 0.f;
+        const float px = nopref ? P.rx : pref.x, py = nopref ? P.ry : pref.y, pz = nopref ? P.rz : pref.z;
         float dotmax = 0.f;
 #pragma unroll
         for (int k = 0; k < BPX_MAX_FIBRES; ++k) {
@@ -409,6 +412,9 @@ struct Tracker {
       const uint32_t vox = in_grid ? (uint32_t)(((size_t)iz * v.ny + iy) * v.nx + ix) : 0u;
       const float m = __ldg(v.mask + vox);
       const uint32_t way = v.waypoints ? __ldg(v.waypoints + vox) : 0u;
+      float3 pref = make_float3(0.f, 0.f, 0.f);  // --prefdir at the rounded position
+      if ((FEAT & kFeatPref) && v.prefdir)
+        pref = make_float3(__ldg(v.prefdir + vox), __ldg(v.prefdir + a.nvox + vox), __ldg(v.prefdir + 2 * a.nvox + vox));
       // what the counting below reads, in the same round: the target bits of a new voxel, the
       // matrix2 column of a new tract-space voxel (lr: its index, or ~0 off the tract-space grid)
       uint32_t tgt = 0u, lr = 0xffffffffu;
@@ -482,7 +488,7 @@ struct Tracker {
       if (stop) break;
       float3 rn;
       bool moves;
-      choose(P, u, S, init_sample, fibst, rn, moves, f);
+      choose(P, u, S, pref, init_sample, fibst, rn, moves, f);
       if (f > u[5]) {
         // (cos ph sin th, sin ph sin th, cos th): the record's vector, products commuted
         const float rxn = rn.x, ryn = rn.y, rzn = rn.z;
@@ -512,7 +518,7 @@ struct Tracker {
             float3 b;
             bool moves2;
             float f2;
-            choose(P, w, T2, init_sample, fibst, b, moves2, f2);
+            choose(P, w, T2, pref, init_sample, fibst, b, moves2, f2);
             const float bx = b.x, by = b.y, bz = b.z;
             const float same = (rxn * bx + ryn * by + rzn * bz) > 0.f ? 1.0f : -1.0f;
             const float mx = (rxn + same * bx) * 0.5f, my = (ryn + same * by) * 0.5f, mz = (rzn + same * bz) * 0.5f;
@@ -757,7 +763,8 @@ bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volu
   const size_t table_bytes = ((size_t)1 << log2n) * sizeof(uint2);
   const size_t max_blocks = ((size_t)16 << 30) / ((table_bytes + lc_bytes) * kTrackThreads);
   const int feat = (opts->modeuler ? kFeatEuler : 0) | (opts->loopcheck ? kFeatLoop : 0) |
-                   ((vol->ntargets > 0 || vol->m2_ncols > 0 || vol->m1_ncols > 0) ? kFeatCount : 0);
+                   ((vol->ntargets > 0 || vol->m2_ncols > 0 || vol->m1_ncols > 0) ? kFeatCount : 0) |
+                   (vol->prefdir ? kFeatPref : 0);
   int grid = sm_count() * kTrackBlocksPerSm;
   if ((size_t)grid > max_blocks) grid = max_blocks > 0 ? (int)max_blocks : 1;
   const size_t threads = (size_t)grid * kTrackThreads;
@@ -800,7 +807,15 @@ bpx_status bpx_probtrack_dev(const bpx_track_options* opts, const bpx_track_volu
       case 4: track_kernel<4><<<grid, kTrackThreads, 0, s>>>(a); break;
       case 5: track_kernel<5><<<grid, kTrackThreads, 0, s>>>(a); break;
       case 6: track_kernel<6><<<grid, kTrackThreads, 0, s>>>(a); break;
-      default: track_kernel<7><<<grid, kTrackThreads, 0, s>>>(a); break;
+      case 7: track_kernel<7><<<grid, kTrackThreads, 0, s>>>(a); break;
+      case 8: track_kernel<8><<<grid, kTrackThreads, 0, s>>>(a); break;
+      case 9: track_kernel<9><<<grid, kTrackThreads, 0, s>>>(a); break;
+      case 10: track_kernel<10><<<grid, kTrackThreads, 0, s>>>(a); break;
+      case 11: track_kernel<11><<<grid, kTrackThreads, 0, s>>>(a); break;
+      case 12: track_kernel<12><<<grid, kTrackThreads, 0, s>>>(a); break;
+      case 13: track_kernel<13><<<grid, kTrackThreads, 0, s>>>(a); break;
+      case 14: track_kernel<14><<<grid, kTrackThreads, 0, s>>>(a); break;
+      default: track_kernel<15><<<grid, kTrackThreads, 0, s>>>(a); break;
     }
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return api_cuda_fail(e, "bpx_probtrack_dev: track_kernel");

@@ -402,7 +402,7 @@ def matrix2_lookup(lrmask) -> np.ndarray:
 
 
 def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.0), avoid=None, stop=None,
-              waypoints=None, targets=None, matrix2=None, matrix1=None):
+              waypoints=None, targets=None, matrix2=None, matrix1=None, prefdir=None):
     """probtrackx on device tensors: (paths [nz][ny][nx] int32, or [nseeds][nz][ny][nx] with
     topts.per_seed; waytotal int) for
     seeds [nseeds][3] (voxel coordinates x, y, z).  `avoid` and `stop`: device masks of the mask's
@@ -412,7 +412,8 @@ def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0,
     `matrix2`: (tract-space mask [lz][ly][lx], its voxel size in mm), for which fdt_matrix2
     [nseeds][columns] (int32, host) follows (--omatrix2 --lrmask); `matrix1`: the seed mask
     [nz][ny][nx], for which fdt_matrix1 [nseeds][seed-mask voxels] (int32, host) comes last
-    (--omatrix1: each seed's path distribution at the seed-mask voxels, in z, y, x order)."""
+    (--omatrix1: each seed's path distribution at the seed-mask voxels, in z, y, x order); `prefdir`:
+    a preferred direction per voxel, [3][nz][ny][nx] (--prefdir)."""
     torch = _torch()
     way_bits = None
     nway = 0
@@ -450,6 +451,12 @@ def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0,
         m1 = torch.zeros((int(sd.shape[0]), int((lut1 >= 0).sum())), device="cuda", dtype=torch.int32)
         v.m1_ncols = int(m1.shape[1])
         v.m1_lookup, v.matrix1 = lut1_d.data_ptr(), m1.data_ptr()
+    pd = None
+    if prefdir is not None:
+        pd = to_device(prefdir.cpu().numpy() if hasattr(prefdir, "cpu") else np.asarray(prefdir))
+        if tuple(pd.shape) != (3,) + tuple(mask.shape):
+            raise BpxError("prefdir: expected [3][nz][ny][nx] on the mask's grid")
+        v.prefdir = pd.data_ptr()
     _check(load().bpx_probtrack_dev(C.byref(topts), C.byref(v), int(sd.shape[0]), _ptr(sd), _ptr(paths), _ptr(way),
                                     _stream(torch)), "bpx_probtrack_dev")
     out = (paths, int(way.item()))

@@ -4,7 +4,7 @@
         [-S 2000] [--steplength 0.5] [--cthr 0.2] [--fibthresh 0.01] [--distthresh 0] [--randfib 0]
         [--fibst 1] [--usef] [--sampvox] [--pd] [-l] [--modeuler] [--seed N] [--avoid MASK]
         [--stop MASK] [--waypoints MASK|LIST] [--targetmasks LIST --os2t] [--omatrix2 --lrmask MASK]
-        [--omatrix1] [--network] [--mask2 MASK]
+        [--omatrix1] [--prefdir VOL4D] [--network] [--mask2 MASK]
 
 Reads merged_th{k}samples, merged_ph{k}samples, merged_f{k}samples and nodif_brain_mask (NIfTI-1)
 as probtrackx does (probtrackx.cc:25-96, tractvolsx.h:55-97) and tracks from the seeds:
@@ -31,6 +31,9 @@ streamlines from it through each seed voxel (its path distribution read at the s
 coords_for_fdt_matrix1 (Counter::initialise_matrix1, update_matrix1, save_matrix1;
 streamlines.cc:493-510, 751-770, 963-968).  The reference clears its path distribution after each
 seed when it builds matrix1, so its fdt_paths comes out empty then; here fdt_paths keeps the sum.
+--prefdir VOL4D (x, y, z components per voxel) makes every step after a streamline's first take the
+fibre closest to the voxel's preferred direction, where it is non-zero (streamlines.cc:286-291,
+tractvolsx.h:209-225).
 --avoid rejects a half that enters the mask, --stop ends a half where it enters it, and --waypoints
 (one mask, or a text file naming up to 32 masks one per line) keeps only streamlines whose halves
 together passed every mask (streamlines.cc:112-145, 279-330); all on the diffusion grid.
@@ -88,6 +91,15 @@ def waypoint_files(arg: str) -> list[str]:
     return [n if os.path.isabs(n) else os.path.join(base, n) for n in names]
 
 
+def read_prefdir(path: str, grid: tuple[int, int, int]) -> np.ndarray:
+    """--prefdir: a 4D NIfTI [x][y][z][3] of preferred directions on the diffusion grid, as float32
+    [3][nz][ny][nx] (read_volume4D of streamlines.cc:124-125)."""
+    a, _ = nifti.read(path)
+    if a.ndim != 4 or a.shape[:3] != grid or a.shape[3] != 3:
+        raise ValueError(f"{path}: expected a 4D volume of 3 components on the grid {grid}, got {a.shape}")
+    return np.ascontiguousarray(np.transpose(np.asarray(a, np.float32), (3, 2, 1, 0)))
+
+
 def seed_points(arg: str, grid: tuple[int, int, int]) -> tuple[np.ndarray, bool]:
     """(seed points [n][3] as voxel x y z, per_seed): a text file of points (simple mode, one
     output per point) or a NIfTI mask whose non-zero voxels, in z, y, x order, are the seeds
@@ -104,7 +116,8 @@ def seed_points(arg: str, grid: tuple[int, int, int]) -> tuple[np.ndarray, bool]
 
 def run(bpx_dir: str, seeds, opts: TrackOptions, outdir: str, avoid: str | None = None,
         stop: str | None = None, waypoints: str | None = None, outname: str = "fdt_paths",
-        targets: str | None = None, lrmask: str | None = None, omatrix1: bool = False) -> tuple[np.ndarray, int]:
+        targets: str | None = None, lrmask: str | None = None, omatrix1: bool = False,
+        prefdir: str | None = None) -> tuple[np.ndarray, int]:
     """Tracks from `seeds` (a seed file or mask path, or an array of points for simple mode) and
     writes the path distributions and waytotal; returns (paths [x][y][z], or [nseeds][x][y][z] in
     simple mode, waytotal)."""
@@ -133,6 +146,8 @@ def run(bpx_dir: str, seeds, opts: TrackOptions, outdir: str, avoid: str | None 
         lr, lr_hdr = nifti.read(lrmask)
         lr_zyx = np.ascontiguousarray(np.transpose(np.asarray(lr, np.float32).reshape(lr.shape[:3]), (2, 1, 0)))
         extra["matrix2"] = (lr_zyx, tuple(float(x) for x in lr_hdr.pixdim[1:4]))
+    if prefdir:
+        extra["prefdir"] = read_prefdir(prefdir, grid)
     if omatrix1:
         if per_seed or not isinstance(seeds_arg, str):
             raise ValueError("--omatrix1 needs a seed mask (seedmask mode)")
@@ -208,7 +223,7 @@ def save_matrix2(outdir: str, m2: np.ndarray, seeds: np.ndarray, lr_zyx: np.ndar
 
 def run_network(bpx_dir: str, mask_list, opts: TrackOptions, outdir: str, avoid: str | None = None,
                 stop: str | None = None, waypoints: str | None = None,
-                outname: str = "fdt_paths") -> tuple[np.ndarray, list[int]]:
+                outname: str = "fdt_paths", prefdir: str | None = None) -> tuple[np.ndarray, list[int]]:
     """Network mode (ptx_nmasks.cc; with two masks, twomasks mode, ptx_twomasks.cc): for each mask
     of the list (a text file naming them, or a list of paths), its voxels (z, y, x order) are the
     seeds and the union of the other masks is one more waypoint mask (Streamliner::add_waymask);
@@ -227,6 +242,8 @@ def run_network(bpx_dir: str, mask_list, opts: TrackOptions, outdir: str, avoid:
         extra["avoid"] = lib.to_device(read_mask(avoid, grid))
     if stop:
         extra["stop"] = lib.to_device(read_mask(stop, grid))
+    if prefdir:
+        extra["prefdir"] = read_prefdir(prefdir, grid)
     user_ways = [read_mask(w, grid) for w in waypoint_files(waypoints)] if waypoints else []
     if len(user_ways) > 31:
         raise ValueError("network mode takes at most 31 waypoint masks of its own")
@@ -281,6 +298,7 @@ def main(argv=None) -> None:
     ap.add_argument("--omatrix2", action="store_true", help="output matrix2 (seeds x tract-space voxels)")
     ap.add_argument("--lrmask", help="tract-space (low resolution) mask for matrix2")
     ap.add_argument("--omatrix1", action="store_true", help="output matrix1 (seeds x seed voxels; seedmask mode)")
+    ap.add_argument("--prefdir", help="4D volume of preferred directions (x, y, z) on the diffusion grid")
     ap.add_argument("--network", action="store_true", help="network mode: --seeds lists several masks")
     ap.add_argument("--mask2", help="second seed mask (twomasks mode, with a seed mask)")
     a = ap.parse_args(argv)
@@ -297,14 +315,14 @@ def main(argv=None) -> None:
             ap.error("seeds_to_targets, matrix1 and matrix2 are not available in multiple seed tractography")
         masks = [a.seeds, a.mask2] if a.mask2 else a.seeds
         _, ways = run_network(a.bpx_dir, masks, o, a.out, avoid=a.avoid, stop=a.stop, waypoints=a.waypoints,
-                              outname=a.outname)
+                              outname=a.outname, prefdir=a.prefdir)
         print("waytotal " + " ".join(map(str, ways)))
         return
     if a.omatrix1 and not a.seeds.endswith((".nii", ".nii.gz")):
         ap.error("--omatrix1 needs a seed mask (seedmask mode)")
     _, way = run(a.bpx_dir, a.seeds, o, a.out, avoid=a.avoid, stop=a.stop, waypoints=a.waypoints, outname=a.outname,
                  targets=a.targetmasks if a.os2t else None, lrmask=a.lrmask if a.omatrix2 else None,
-                 omatrix1=a.omatrix1)
+                 omatrix1=a.omatrix1, prefdir=a.prefdir)
     print(f"waytotal {way}")
 
 

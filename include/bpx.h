@@ -516,6 +516,11 @@ typedef struct bpx_track_volume {
   int32_t m1_ncols;
   const int32_t* m1_lookup;
   int32_t* matrix1;
+  /* --prefdir (streamlines.cc:124-125, 286-291; Tractvolsx::sample, tractvolsx.h:209-225): a preferred
+   * direction per voxel, [3][nz][ny][nx] (x, y, z components), or NULL.  After a streamline's first
+   * sample, each step takes the fibre closest to the vector at its rounded position, or to the
+   * current direction where that vector is zero (the rule without --prefdir). */
+  const float* prefdir;
 } bpx_track_volume;
 
 void bpx_track_options_default(bpx_track_options* opts);

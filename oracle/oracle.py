@@ -199,14 +199,15 @@ def energy(opts: Options, data, bvecs, bvals, states):
 
 
 def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0, 2.0), avoid=None, stop=None,
-              waypoints=None, targets=None, matrix2=None, matrix1=None):
+              waypoints=None, targets=None, matrix2=None, matrix1=None, prefdir=None):
     """probtrackx simple mode on host arrays (th/ph/f [nfib][nsamples][nz][ny][nx], mask [nz][ny][nx],
     seeds [nseeds][3] voxel coordinates; optional avoid and stop masks and a list of waypoint masks,
     each [nz][ny][nx]; target masks, each [nz][ny][nx]; matrix2 = (tract-space mask [lz][ly][lx], its
     voxel size); matrix1 = the seed mask [nz][ny][nx]): (paths [nz][ny][nx] int32, or
     [nseeds][nz][ny][nx] with topts.per_seed, waytotal[, seeds_to_targets [ntargets][nseeds] int32
     when targets are given][, fdt_matrix2 [nseeds][columns] int32 when matrix2 is given][,
-    fdt_matrix1 [nseeds][seed-mask voxels] int32 when matrix1 is given])."""
+    fdt_matrix1 [nseeds][seed-mask voxels] int32 when matrix1 is given]); prefdir: a preferred
+    direction volume [3][nz][ny][nx] (--prefdir)."""
     th, ph, f, mask = (np.ascontiguousarray(a, np.float32) for a in (th, ph, f, mask))
     v = TrackVolume()
     v.nfib, v.nsamples, v.nz, v.ny, v.nx = th.shape
@@ -256,6 +257,11 @@ def probtrack(topts: TrackOptions, th, ph, f, mask, seeds, voxel_size=(2.0, 2.0,
         keep += [lut1, m1]
         v.m1_ncols = m1.shape[1]
         v.m1_lookup, v.matrix1 = lut1.ctypes.data, m1.ctypes.data
+    if prefdir is not None:
+        pd = np.ascontiguousarray(prefdir, np.float32)
+        assert pd.shape == (3,) + mask.shape
+        keep.append(pd)
+        v.prefdir = pd.ctypes.data
     paths = np.zeros(((sd.shape[0],) if topts.per_seed else ()) + tuple(mask.shape), np.int32)
     way = C.c_int64(0)
     rc = lib().orc_probtrack(C.byref(topts), C.byref(v), sd.shape[0], sd, paths, C.byref(way))

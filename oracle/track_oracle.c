@@ -15,6 +15,8 @@
  *   Counter::update_matrix2_row (streamlines.cc:772-808): --omatrix2;
  *   Counter::update_matrix1     (streamlines.cc:751-770): --omatrix1, the per-seed path
  *                               distribution read at the seed-mask voxels;
+ *   --prefdir                   (streamlines.cc:286-291, tractvolsx.h:209-225): the fibre closest
+ *                               to a preferred direction per voxel after the first sample;
  *   Tractvolsx::sample          (tractvolsx.h:101-255): probabilistic rounding of the position,
  *                               a random posterior sample, the first fibre (fibst, randfib 1/2)
  *                               and afterwards the fibre closest to the current direction among
@@ -113,9 +115,10 @@ static size_t at(const trk_t* T, int k, int s, size_t vox) {
   return ((size_t)k * T->v->nsamples + s) * T->nvox + vox;
 }
 
-/* Tractvolsx::sample at position (x, y, z) with the particle's direction P->r: theta, phi and f */
-static void sample(const trk_t* T, const part_t* P, float x, float y, float z, const float u[8], int* init_sample,
-                   int* fibst, float* th, float* ph, float* f) {
+/* Tractvolsx::sample at position (x, y, z) with the particle's direction P->r and the preferred
+ * direction pref of the step's voxel (zero without --prefdir): theta, phi and f */
+static void sample(const trk_t* T, const part_t* P, float x, float y, float z, const float u[8], const float pref[3],
+                   int* init_sample, int* fibst, float* th, float* ph, float* f) {
   const bpx_track_volume* v = T->v;
   const int cx = (int)ceilf(x), fx = (int)floorf(x);
   const int cy = (int)ceilf(y), fy = (int)floorf(y);
@@ -164,8 +167,9 @@ static void sample(const trk_t* T, const part_t* P, float x, float y, float z, c
       phi = v->ph[at(T, *fibst, samp, vox)];
       *init_sample = 0;
     } else {
-      /* no preferred-direction volume: the preference is the current direction */
-      const float px = P->rx, py = P->ry, pz = P->rz;
+      /* the preferred direction, or where it is zero (always, without --prefdir) the current one */
+      const int nopref = (fabsf(pref[0]) + fabsf(pref[1]) + fabsf(pref[2])) == 0.f;
+      const float px = nopref ? P->rx : pref[0], py = nopref ? P->ry : pref[1], pz = nopref ? P->rz : pref[2];
       float dotmax = 0.f;
       for (int k = 0; k < K; ++k) {
         if (v->f[at(T, k, samp, vox)] > thr) {
@@ -287,8 +291,11 @@ static int half_line(const trk_t* T, part_t* P, uint64_t pid, int h, int fibst0,
     }
     if (v->stop && v->stop[vox] != 0.f) break;
     float u[8], th, ph, f;
+    float pref[3] = {0.f, 0.f, 0.f}; /* --prefdir at the rounded position (streamlines.cc:286-291) */
+    if (v->prefdir)
+      for (int c = 0; c < 3; ++c) pref[c] = v->prefdir[(size_t)c * T->nvox + (size_t)vox];
     orc_track_uniforms(o->seed, pid, h, (uint32_t)it, u);
-    sample(T, P, P->x, P->y, P->z, u, &init_sample, &fibst, &th, &ph, &f);
+    sample(T, P, P->x, P->y, P->z, u, pref, &init_sample, &fibst, &th, &ph, &f);
     if (f > u[5]) {
       float st, ct, sp, cp;
       orc_sincos_fast(th, &st, &ct);
@@ -313,7 +320,7 @@ static int half_line(const trk_t* T, part_t* P, uint64_t pid, int h, int fibst0,
           const float ty = P->y + ts * o->steplength / v->dy * ryn;
           const float tz = P->z + ts * o->steplength / v->dz * rzn;
           float th2, ph2, f2;
-          sample(T, P, tx, ty, tz, w, &init_sample, &fibst, &th2, &ph2, &f2);
+          sample(T, P, tx, ty, tz, w, pref, &init_sample, &fibst, &th2, &ph2, &f2);
           float st2, ct2, sp2, cp2;
           orc_sincos_fast(th2, &st2, &ct2);
           orc_sincos_fast(ph2, &sp2, &cp2);

@@ -293,6 +293,49 @@ def test_matrix1_equals_oracle(torch, name, kw):
     assert want[-1].sum() > 0 and want[-1].shape == (len(seeds), len(seeds))
 
 
+PREF_CASES = [
+    ("plain", dict()),
+    ("modeuler", dict(modeuler=1)),
+    ("loopcheck_pathdist", dict(loopcheck=1, pathdist=1)),
+    ("randfib_usef_masks", dict(randfib=2, usef=1, masks=("avoid", "waypoints"))),
+    ("with_matrix1", dict(matrix1=True)),
+]
+
+
+@pytest.mark.parametrize("name,kw", PREF_CASES, ids=[c[0] for c in PREF_CASES])
+def test_prefdir_equals_oracle(torch, name, kw):
+    """--prefdir on the crossing field: a preferred direction per voxel (unit vectors, zero in a
+    third of the voxels, where the current direction decides); bit for bit against the oracle."""
+    from fdt_b200 import lib
+
+    lib.load()
+    th, ph, f, mask = synth.fibre_field((20, 16, 10), nsamples=12, seed=4)
+    rng = np.random.default_rng(9)
+    pref = rng.normal(size=(3,) + mask.shape).astype(np.float32)
+    pref /= np.linalg.norm(pref, axis=0, keepdims=True)
+    pref[:, rng.random(mask.shape) < 1 / 3] = 0.0
+    seeds = np.array([[5.0, 8.0, 5.0], [14.0, 7.0, 4.6], [10.3, 3.2, 5.5]], np.float32)
+    kw = dict(kw)
+    extra = _masks(mask, kw.pop("masks", ()))
+    if kw.pop("matrix1", False):
+        sm = np.zeros_like(mask)
+        sm[4:6, 6:10, 6:13] = mask[4:6, 6:10, 6:13]
+        seeds = np.argwhere(sm != 0)[:, ::-1].astype(np.float32)
+        extra["matrix1"] = sm
+    o = TrackOptions.make(nparticles=100, nsteps=300, seed=47, **kw)
+    want = O.probtrack(o, th, ph, f, mask, seeds, prefdir=pref, **extra)
+    dev = [lib.to_device(a) for a in (th, ph, f, mask)]
+    dextra = {k: (lib.to_device(v) if k in ("avoid", "stop") else v) for k, v in extra.items()}
+    got = lib.probtrack(o, *dev, seeds, prefdir=pref, **dextra)
+    torch.cuda.synchronize()
+    assert got[1] == want[1] > 0 and np.array_equal(got[0].cpu().numpy(), want[0]), name
+    for g, w in zip(got[2:], want[2:]):
+        assert np.array_equal(g, w), name
+    # the preferred directions change the paths
+    plain = O.probtrack(o, th, ph, f, mask, seeds, **extra)
+    assert not np.array_equal(plain[0], want[0])
+
+
 @pytest.mark.parametrize("modeuler", [0, 1])
 def test_loopcheck_on_circling_tracts_equals_oracle(torch, modeuler):
     from fdt_b200 import lib

@@ -219,6 +219,32 @@ def test_matrix1_is_the_per_seed_path_counts_at_the_seed_mask():
         assert way2 == way and np.array_equal(m1b, m1) and np.array_equal(paths, each.sum(0))
 
 
+def test_prefdir_chooses_the_fibre_closest_to_the_preferred_direction():
+    # two fibres everywhere, along x (fibre 1) and along y (fibre 2); the first step follows fibre 1
+    th, ph, f, mask = _straight_box()
+    th = np.concatenate([th, th])
+    ph = np.concatenate([ph, np.full_like(ph, np.pi / 2)])
+    f = np.concatenate([f, f]) * np.float32(0.6)
+    o = TrackOptions.make(nparticles=40, nsteps=400, seed=5)
+    seed = [[15.0, 4.0, 4.0]]
+    free, way = O.probtrack(o, th, ph, f, mask, seed)
+    assert way == 40 and np.all(free[4, 4, 3:27] == 40)  # the current direction keeps it along x
+    pref = np.zeros((3,) + mask.shape, np.float32)
+    same, way0 = O.probtrack(o, th, ph, f, mask, seed, prefdir=pref)  # zero vectors: the current direction
+    assert way0 == way and np.array_equal(same, free)
+    pref[0] = 1.0  # along x: the same choice at every step
+    alongx, _ = O.probtrack(o, th, ph, f, mask, seed, prefdir=pref)
+    assert np.array_equal(alongx, free)
+    pref[0], pref[1] = 0.0, 1.0  # along y: the second step turns by 90 degrees and the curvature test stops it
+    alongy, wy = O.probtrack(o, th, ph, f, mask, seed, prefdir=pref)
+    assert wy == 40 and alongy[4, 4, 3:13].sum() == 0 and alongy[4, 4, 18:27].sum() == 0
+    assert 0 < alongy.sum() <= 40 * 4
+    # with a curvature threshold that lets it turn, it follows y instead and leaves the x line
+    o.c_thr = 0.0
+    turned, _ = O.probtrack(o, th, ph, f, mask, seed, prefdir=pref)
+    assert turned[4, 4, 3:13].sum() == 0 and turned[:, 2:7, 15].sum() > turned[4, 4, 15]
+
+
 def test_matrix2_on_a_coarser_grid_counts_each_tract_space_voxel_once_per_streamline():
     th, ph, f, mask = _straight_box()  # 30 x 9 x 9 voxels of 2 mm, the tract along x at y = z = 4
     # tract space of 4 mm voxels: positions 2.5 <= x < 26.5 map to x_lr = round(x / 2) = 1 .. 13 at
