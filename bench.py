@@ -521,10 +521,11 @@ def run_probtrack(args):
     pick = inside[rng.choice(len(inside), args.track_seeds, replace=False)]
     seeds = np.ascontiguousarray(pick[:, ::-1].astype(np.float32))
     # --track-options: loopcheck, modeuler (options), targets (3 target planes across the x-running
-    # tracts, seeds to targets), matrix2 (a tract space of 4 mm voxels over the whole grid)
+    # tracts, seeds to targets), matrix2 (a tract space of 4 mm voxels over the whole grid), prefdir
+    # (a preferred direction along x in every voxel of the mask's lower half, zero elsewhere)
     topts = [t for t in args.track_options.split(",") if t]
     for t in topts:
-        if t not in ("loopcheck", "modeuler", "targets", "matrix2"):
+        if t not in ("loopcheck", "modeuler", "targets", "matrix2", "prefdir"):
             raise SystemExit(f"--track-options: unknown option {t}")
     o = TrackOptions.make(seed=9, loopcheck=int("loopcheck" in topts), modeuler=int("modeuler" in topts))
     extra = {}
@@ -537,9 +538,16 @@ def run_probtrack(args):
         extra["targets"] = planes
     if "matrix2" in topts:
         extra["matrix2"] = (np.ones((30, 48, 48), np.float32), (4.0, 4.0, 4.0))
+    if "prefdir" in topts:
+        pref = np.zeros((3,) + mask.shape, np.float32)
+        pref[0, : mask.shape[0] // 2] = 1.0
+        extra["prefdir"] = pref
     dev = [lib.to_device(a) for a in (th, ph, f, mask)]
     sd = lib.to_device(seeds)
     v = lib.track_volume(*dev)
+    if "prefdir" in topts:
+        pref_d = lib.to_device(extra["prefdir"])
+        v.prefdir = pref_d.data_ptr()
     outs = []  # per-option outputs, zeroed every step
     if "targets" in topts:
         tb = torch.from_numpy(lib.waypoint_bits(extra["targets"])).cuda()
