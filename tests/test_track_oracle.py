@@ -330,3 +330,30 @@ def test_probtrack_cli_reads_samples_masks_and_waypoint_lists(tmp_path):
     nifti.write(os.path.join(str(tmp_path), "sm.nii.gz"), np.transpose(sm, (2, 1, 0)))
     pts, per_seed = probtrack.seed_points(os.path.join(str(tmp_path), "sm.nii.gz"), mask.shape[::-1])
     assert not per_seed and np.array_equal(pts, [[5, 4, 0], [3, 2, 1]])
+
+
+def test_probtrack_cli_reads_prefdir_and_checks_matrix1_arguments(tmp_path):
+    import pytest
+
+    from fdt_b200 import nifti, probtrack
+
+    th, ph, f, mask = synth.fibre_field((12, 10, 6), nsamples=4, seed=1)
+    synth.write_bedpostx_dir(str(tmp_path), th, ph, f, mask)
+    grid = mask.shape[::-1]
+    # --prefdir: a 4D [x][y][z][3] volume becomes [3][z][y][x]
+    pref = np.random.default_rng(0).normal(size=(3,) + mask.shape).astype(np.float32)
+    path = os.path.join(str(tmp_path), "pref.nii.gz")
+    nifti.write(path, np.transpose(pref, (3, 2, 1, 0)))
+    assert np.array_equal(probtrack.read_prefdir(path, grid), pref)
+    bad = os.path.join(str(tmp_path), "pref2.nii.gz")
+    nifti.write(bad, np.transpose(pref[:2], (3, 2, 1, 0)))  # two components
+    with pytest.raises(ValueError):
+        probtrack.read_prefdir(bad, grid)
+    # --omatrix1 needs seedmask mode; matrix1 and matrix2 are not for multiple seed tractography
+    np.savetxt(os.path.join(str(tmp_path), "pts.txt"), [[1.0, 2.0, 3.0]])
+    with pytest.raises(SystemExit):
+        probtrack.main([str(tmp_path), "--seeds", os.path.join(str(tmp_path), "pts.txt"), "--out",
+                        os.path.join(str(tmp_path), "o"), "--omatrix1"])
+    with pytest.raises(SystemExit):
+        probtrack.main([str(tmp_path), "--seeds", os.path.join(str(tmp_path), "pts.txt"), "--out",
+                        os.path.join(str(tmp_path), "o"), "--network", "--omatrix1"])
