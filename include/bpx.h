@@ -549,7 +549,8 @@ bpx_status bpx_release_workspace(void);
  * bpx_handle_bind(h) makes every workspace-using call on this host thread use h's workspaces
  * (bind NULL to return to the shared per-device ones); a handle is bound to one thread at a time
  * and its calls follow the one-stream rule among themselves.  bpx_handle_destroy frees the
- * workspaces (cudaFree waits for the device's work) and unbinds it from the calling thread.
+ * workspaces (cudaFree waits for the device's work) and unbinds it from the calling thread; a handle
+ * bound on another thread must be unbound there (bpx_handle_bind(NULL)) before it is destroyed.
  */
 typedef struct bpx_handle bpx_handle;
 bpx_status bpx_handle_create(bpx_handle** h);
